@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Benchmark: BN254 G1 MSM over 2^20 points (SRS bases [tau^i]G1, uniform Fr
+scalars), the operator-level headline of the reference's prover hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--log-n 20] [--impl ours|reference]
+
+One JSON line on stdout (rank 0).  A step is one complete MSM: device
+conversion and validation of the bases, signed-digit bucket sort, bucket
+accumulation and reduction, window combination and normalisation to a
+canonical affine point in host memory.
+
+  value / ms_per_step : device time per MSM (CUDA events on the launching
+                        stream), inputs resident in HBM, L2 flushed (256 MB
+                        write) between steps; the sum over K steps / K.
+                        With N GPUs the ranks run independent replicas;
+                        value = max-over-ranks time / (N * K) (ms per MSM
+                        of the whole job).
+  e2e                 : the same MSM through the reference-facing C-ABI
+                        call dvgpu_bn254_msm with pinned HOST buffers
+                        (H2D of 96 bytes/point inside the timed region).
+  roofline            : the bucket-accumulation kernel (the dominant one):
+                        N * windows XYZZ mixed additions x 10 Fq
+                        multiplications x 136 32x32->64 multiply-accumulates
+                        per launch, over its CUDA-event duration, against
+                        the IMAD rate measured in this run.
+  cpu_baseline        : the CPU oracle (C++ restatement of arkworks
+                        semantics, window-parallel Pippenger) on the same
+                        inputs, one full MSM, all host threads.
+  --impl reference    : times that CPU implementation alone (the reference
+                        itself, Rust + arkworks + ICICLE, cannot be built here).
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "G1 MSM 2^20 ms"
+UNIT = "ms"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--log-n", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def msm_fme(n):
+    """Algorithmic work of a G1 MSM in Fq multiplications:
+    min over c of ceil(254/c) * (10 n + 14 * 2^c)."""
+    return min(math.ceil(254 / c) * (10 * n + 14 * (1 << c)) for c in range(2, 24))
+
+
+class ClockSampler:
+    """nvidia-smi samples of one GPU during the timed region."""
+
+    FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id):
+        self.bus_id = (bus_id or "").lower()
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        rows = []
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 10:
+                continue
+            bus = parts[1].lower()
+            if self.bus_id and not (bus.endswith(self.bus_id[-12:]) or self.bus_id.endswith(bus[-12:])):
+                continue
+            rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = sorted(v for v in (num(r[2]) for r in rows) if v is not None)
+        mx = max(v for v in (num(r[3]) for r in rows) if v is not None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def load_traffic():
+    """DRAM bytes per launch of the accumulation kernel from the committed
+    ncu summary (profiles/msm_g1_accum_2p20.txt), or None."""
+    path = os.path.join(ROOT, "profiles", "msm_g1_accum_2p20.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_reference_msm(points: bytes, scalars: bytes, threads: int):
+    from oracle import oracle
+    t0 = time.perf_counter()
+    out = oracle.msm_g1(points, scalars, threads=threads)
+    return out, (time.perf_counter() - t0) * 1e3
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU implementation of the path on host cores."""
+    if rank != 0:
+        return
+    from oracle import oracle
+    n = 1 << args.log_n
+    threads = os.cpu_count() or 1
+    tau = oracle.uniform_fr(2812, 1)
+    points = oracle.fixed_base_g1(oracle.fr_powers(tau, n), threads=threads)
+    scalars = oracle.uniform_fr(2813, n)
+    # warm-up (bounded) then timed steps, bounded to ~90 s of wall time
+    _, first = cpu_reference_msm(points, scalars, threads)
+    budget_ms = 90e3
+    steps = max(1, min(args.steps, int(budget_ms // max(first, 1.0))))
+    times = []
+    for _ in range(steps):
+        _, ms = cpu_reference_msm(points, scalars, threads)
+        times.append(ms)
+    value = sum(times) / len(times)
+    sample = f"{steps} full 2^{args.log_n}-point MSMs (after 1 warm-up), window-parallel Pippenger"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 limbs (Fq/Fr, exact)", "data": "synthetic",
+        "config": {"workload": f"G1 MSM 2^{args.log_n}: bases [tau^i]G1 affine (seeded tau), uniform Fr scalars",
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("reference = C++ restatement of arkworks 0.4 semantics (oracle/); the reference's own "
+                 "Rust/arkworks/ICICLE code cannot be built in this image"),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    from __graft_entry__ import load_package
+    dv = load_package()
+    b = dv.DvgpuBackend()
+    n = 1 << args.log_n
+    stream = torch.cuda.current_stream()
+    s = stream.cuda_stream
+
+    # ---- inputs, generated on the device (seeded): SRS bases and scalars
+    tau = torch.empty(32, dtype=torch.uint8, device="cuda")
+    b.random_fr_device(2812, 1, tau.data_ptr(), s)
+    powers = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+    b.fr_powers_device(tau.data_ptr(), n, powers.data_ptr(), s)
+    points = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
+    b.fixed_base_device(powers.data_ptr(), n, False, points.data_ptr(), s)
+    scalars = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+    b.random_fr_device(2813 + rank, n, scalars.data_ptr(), s)
+    del powers
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        result = b.msm_device(points.data_ptr(), scalars.data_ptr(), n, stream=s)
+
+    try:
+        bus = torch.cuda.get_device_properties(dev).pci_bus_id
+    except AttributeError:
+        bus = None
+    sampler = ClockSampler(bus if isinstance(bus, str) else None)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = b.launch_count()
+    b.msm_timeline(True)
+    step_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = b.msm_device(points.data_ptr(), scalars.data_ptr(), n, stream=s)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        if r != result:
+            raise RuntimeError("MSM result changed between steps")
+    torch.cuda.synchronize()
+    tl = b.msm_timeline(False)
+    launches = b.launch_count() - launches0
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_msm = total_ms / args.steps
+    value = total_ms / (args.steps * world)
+
+    # ---- end to end through the C-ABI with pinned host buffers
+    h_points = torch.empty(n * 64, dtype=torch.uint8, pin_memory=True)
+    h_scalars = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
+    h_points.copy_(points)
+    h_scalars.copy_(scalars)
+    torch.cuda.synchronize()
+    L = dv.lib()
+    out = bytearray(64)
+    import ctypes
+    outbuf = (ctypes.c_char * 64).from_buffer(out)
+    err = ctypes.create_string_buffer(256)
+    rc = L.dvgpu_bn254_msm(b.handle, h_points.data_ptr(), h_scalars.data_ptr(), n, outbuf, err, 256)
+    if rc != 0 or bytes(out) != result:
+        raise RuntimeError(f"e2e MSM failed or differs: {rc} {err.value}")
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        L.dvgpu_bn254_msm(b.handle, h_points.data_ptr(), h_scalars.data_ptr(), n, outbuf, err, 256)
+    e2e_total = (time.perf_counter() - t0) * 1e3
+    if world > 1:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_ms = e2e_total / (args.e2e_steps * world)
+    c = b.window_for(n)
+    windows = math.ceil(255 / c)
+
+    # ---- roofline of the dominant kernel (bucket accumulation)
+    imad_peak = b.probe_imad_rate()  # MAC/s
+    accum_ms = tl.ms[3] / max(1, tl.calls)
+    adds_per_launch = tl.accum_mixed_adds / max(1, tl.calls)
+    accum_macs = adds_per_launch * 10 * 136
+    achieved = accum_macs / (accum_ms * 1e-3) / 1e12
+    peak = imad_peak / 1e12
+    traffic = load_traffic()
+    phases = {name: tl.ms[k] / max(1, tl.calls) for k, name in enumerate(dv.MSM_PHASE_NAMES)}
+    msm_macs = msm_fme(n) * 136
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_msm, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 limbs (Fq/Fr Montgomery, exact)", "data": "synthetic",
+        "config": {"workload": f"G1 MSM 2^{args.log_n}: bases [tau^i]G1 affine (seeded tau), uniform Fr scalars",
+                   "points": n, "window_bits": c, "windows": windows,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed between steps (256 MB write)"},
+        "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": n * 96,
+                "d2h_bytes_per_step": 64 + windows * 128,
+                "call": "dvgpu_bn254_msm (pinned host buffers)"},
+        "roofline": {"bound": "imad", "kernel": "k_accum (bucket accumulation)",
+                     "achieved": achieved, "peak": peak, "unit": "TMAC/s", "frac": achieved / peak,
+                     "traffic": traffic, "algorithmic_macs_per_launch": accum_macs,
+                     "peak_source": "dvgpu_probe_imad_rate in this run (madc.lo/hi chains on all SMs)",
+                     "launch_ms": accum_ms},
+        "msm_roofline": {"algorithmic_macs": msm_macs, "achieved_tmacs": msm_macs / (ms_per_msm * 1e-3) / 1e12,
+                         "frac": msm_macs / (ms_per_msm * 1e-3) / imad_peak},
+        "phases_ms": phases,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        host_pts = bytes(h_points.numpy().tobytes())
+        host_sc = bytes(h_scalars.numpy().tobytes())
+        threads = os.cpu_count() or 1
+        cpu_out, cpu_ms = cpu_reference_msm(host_pts, host_sc, threads)
+        line["cpu_baseline"] = {"value": cpu_ms, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"one full 2^{args.log_n}-point MSM on the same inputs",
+                                "matches_gpu": cpu_out == result}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,208 @@
+/* dvgpu C-ABI: BN254 prover operators on NVIDIA B200 (sm_100a).
+ *
+ * Drop-in for the reference's native ABI, native/include/dynaverse_gpu.h,
+ * whose symbols the Rust crate binds in crates/gpu/src/icicle.rs:35-57,
+ * crates/gpu/src/setup.rs:47-52 and crates/gpu/src/g2_validation.rs:84-93.
+ * Every entry point of the reference that this library implements keeps its
+ * exact signature, argument meaning and status codes:
+ *
+ *    0  success (outputs written)
+ *   -1  invalid argument; nothing written, owner unchanged
+ *   -2  CUDA failure; the owner is retired
+ *   -3  unknown native exception; the owner is retired
+ *   -4  owner already retired (create a new owner to recover)
+ *   -5  G2 content rejected; only the report is published
+ *
+ * Wire formats (crates/gpu/src/codec.rs:25-111, crates/gpu/src/resident.rs:419-431):
+ * Fr and Fq elements are 32-byte little-endian canonical integers (NOT
+ * Montgomery), G1 points 64 bytes x||y, G2 points 128 bytes
+ * x.c0||x.c1||y.c0||y.c1, infinity all zero.  Host-buffer calls are
+ * synchronous and retain no caller pointer.  Error text is NUL-terminated
+ * into (error, error_capacity) when capacity > 0.
+ *
+ * Differences from the reference, all additive:
+ *  - size caps are lifted: MSM up to DVGPU_MAX_MSM_SIZE points, NTT up to
+ *    DVGPU_MAX_NTT_SIZE, fixed base and G2 validation up to
+ *    DVGPU_MAX_SETUP_SIZE per call (the reference stops at 2^20 / 2^20 /
+ *    4096);
+ *  - owners share the device's primary context, so the *_device entry points
+ *    accept device pointers from any runtime user on the same device;
+ *  - new entry points below the reference set are marked "additive".
+ */
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+enum { DVGPU_MAX_MSM_SIZE = 1 << 26 };
+enum { DVGPU_MAX_NTT_SIZE = 1 << 26 };
+enum { DVGPU_MAX_SETUP_SIZE = 1 << 26 };
+enum { DVGPU_MAX_MSM_BATCH_SIZE = 1 << 20 };
+enum { DVGPU_MAX_LARGE_BUCKET_FACTOR = 100 };
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- owner lifecycle (native/include/dynaverse_gpu.h:15-27) ------------ */
+int dvgpu_backend_create(void** backend, char* error, size_t error_capacity);
+/* factor 0..100 is validated and recorded; bucket load balancing is always on
+ * in this engine, so the value does not change results or the algorithm. */
+int dvgpu_backend_create_with_large_bucket_factor(uint32_t factor, void** backend, char* error,
+                                                  size_t error_capacity);
+void dvgpu_backend_destroy(void* backend);
+int dvgpu_backend_device_identity(void* backend, char* output, size_t output_capacity, char* error,
+                                  size_t error_capacity);
+
+/* ---- MSM (native/include/dynaverse_gpu.h:28-38, 46-52) ----------------- */
+int dvgpu_bn254_msm(void* backend, const uint8_t* points, const uint8_t* scalars, size_t length, uint8_t* result,
+                    char* error, size_t error_capacity);
+int dvgpu_bn254_g2_msm(void* backend, const uint8_t* points, const uint8_t* scalars, size_t length, uint8_t* result,
+                       char* error, size_t error_capacity);
+/* count sets, each padded to `length` points (points_size = length * count). */
+int dvgpu_bn254_msm_batch(void* backend, const uint8_t* points, const uint8_t* scalars, size_t length, size_t count,
+                          uint8_t* results, char* error, size_t error_capacity);
+
+/* ---- NTT (native/include/dynaverse_gpu.h:39-45) ------------------------ */
+/* root: the canonical primitive 2^20-th root of unity of the CPU reference;
+ * checked to have order exactly 2^20.  length: power of two. */
+int dvgpu_bn254_ntt(void* backend, const uint8_t* values, size_t length, int inverse, const uint8_t* root,
+                    uint8_t* result, char* error, size_t error_capacity);
+
+typedef struct DvgpuBatchStats {
+    uint64_t icicle_calls; /* native batch launches */
+    uint64_t buffer_grows;
+    uint64_t max_batch_size;
+    uint64_t input_capacity;
+} DvgpuBatchStats;
+typedef struct DvgpuSetupStats {
+    uint64_t table_builds[2], calls[2], points[2], table_bytes;
+    uint64_t device_ns[5], native_wall_ns;
+} DvgpuSetupStats;
+/* native/include/dynaverse_gpu.h:59-66: mode 0..2 is validated and recorded;
+ * this engine always uses the table + batch-normalise path (mode 2). */
+int dvgpu_setup_mode(void* backend, int mode);
+int dvgpu_setup_stats(void* backend, DvgpuSetupStats* stats);
+
+/* ---- G2 validation (native/include/dynaverse_gpu.h:67-89) -------------- */
+typedef struct DvgpuG2ValidationReport {
+    uint64_t checked_points, invalid_points, first_invalid;
+    uint32_t failure_mask, algorithm;
+} DvgpuG2ValidationReport;
+typedef struct DvgpuG2ValidationStats {
+    uint64_t parse_curve_device_ns, subgroup_device_ns, reduce_device_ns;
+    uint64_t h2d_device_ns, d2h_device_ns, native_wall_ns;
+    uint64_t checked_points, accepted_points;
+} DvgpuG2ValidationStats;
+/* masks: 1 encoding, 2 off-curve, 4 outside the subgroup; algorithm 1/2/3. */
+int dvgpu_bn254_g2_validation_inspect(void* owner, const uint8_t* wire, size_t n, uint32_t algorithm,
+                                      uint32_t* point_masks, DvgpuG2ValidationReport* report, char* error,
+                                      size_t error_capacity);
+int dvgpu_g2_validation_stats(void* owner, DvgpuG2ValidationStats* stats);
+typedef struct DvgpuG2ValidationTraffic {
+    uint64_t scalar_h2d_bytes, point_h2d_bytes, point_d2h_bytes, status_d2h_bytes;
+} DvgpuG2ValidationTraffic;
+int dvgpu_g2_validation_traffic(void* owner, DvgpuG2ValidationTraffic* stats);
+/* Fixed-base G2 generation validated on the device; -5 publishes only the report. */
+int dvgpu_bn254_fixed_base_g2_checked(void* owner, const uint8_t* scalars, size_t n, uint32_t algorithm,
+                                      uint8_t* output, DvgpuG2ValidationReport* report, char* error,
+                                      size_t error_capacity);
+int dvgpu_backend_batch_stats(void* backend, DvgpuBatchStats* stats);
+typedef struct DvgpuMemoryInfo {
+    uint64_t free_bytes;
+    uint64_t total_bytes;
+} DvgpuMemoryInfo;
+int dvgpu_backend_memory_info(void* backend, DvgpuMemoryInfo* info, char* error, size_t error_capacity);
+
+/* ---- fixed base (crates/gpu/src/setup.rs:47-52; icicle_msm.cu:494-521) --- */
+/* [s_i] G for the standard G1 (g2 = 0) or G2 (g2 = 1) generator. */
+int dvgpu_bn254_fixed_base(void* backend, const uint8_t* scalars, size_t length, int g2, uint8_t* output, char* error,
+                           size_t error_capacity);
+int dvgpu_reserve_batch(void* backend, size_t points, char* error, size_t error_capacity);
+
+/* ---- diagnostics (native/include/dynaverse_gpu.h:159-168) -------------- */
+typedef struct DvgpuMsmTimings {
+    uint64_t conversion_ns; /* host-side argument handling */
+    uint64_t icicle_ns;     /* device work incl. transfers and synchronisation */
+    uint64_t output_ns;     /* host-side window combination and normalisation */
+} DvgpuMsmTimings;
+int dvgpu_bn254_msm_profiled(void* backend, const uint8_t* points, const uint8_t* scalars, size_t length,
+                             uint8_t* result, DvgpuMsmTimings* timings, char* error, size_t error_capacity);
+
+/* ======================= additive entry points ========================= */
+
+/* NTT of any kind: 0 forward, 1 inverse, 2 coset forward, 3 coset inverse
+ * (coset offset g = 5, the Fr multiplicative generator).  The domain root is
+ * the arkworks one (GENERATOR^((r-1)/2^28) squared down to order length). */
+int dvgpu_bn254_ntt_ex(void* backend, const uint8_t* values, size_t length, int kind, uint8_t* result, char* error,
+                       size_t error_capacity);
+
+/* count independent G1 MSMs of uneven sizes in one launch sequence:
+ * set k uses points/scalars [set_offsets[k], set_offsets[k+1]). */
+int dvgpu_bn254_msm_batch_uneven(void* backend, const uint8_t* points, const uint8_t* scalars,
+                                 const uint64_t* set_offsets, size_t count, uint8_t* results, char* error,
+                                 size_t error_capacity);
+
+/* Resident MSM bases (an SRS table kept in HBM across calls).  points are
+ * validated (canonical, on curve) and converted once.  g2 selects G2. */
+int dvgpu_bases_register(void* backend, const uint8_t* points, size_t n, int g2, uint64_t* handle, char* error,
+                         size_t error_capacity);
+int dvgpu_bases_release(void* backend, uint64_t handle);
+
+/* Sparse-index G1 MSM over resident bases (OperatorBackend::msm_sparse_batch,
+ * crates/protocol/src/types.rs:262-345): request k sums
+ * values[j] * bases[indices[j]] for j in [request_offsets[k], request_offsets[k+1]).
+ * Order, repeated indices and zero values are preserved; an index >= n of
+ * the registered table is rejected (-1) before any result is written. */
+int dvgpu_bn254_msm_sparse_batch(void* backend, uint64_t bases_handle, const uint64_t* indices, const uint8_t* values,
+                                 const uint64_t* request_offsets, size_t count, uint8_t* results, char* error,
+                                 size_t error_capacity);
+
+/* Device-pointer forms (inputs already in HBM, canonical wire layout).
+ * stream: a cudaStream_t, or NULL for the owner's stream.  The call returns
+ * after the device work on `stream` completed.  result_host: host memory. */
+int dvgpu_bn254_msm_device(void* backend, const uint8_t* d_points, const uint8_t* d_scalars, size_t length, int g2,
+                           uint8_t* result_host, void* stream, char* error, size_t error_capacity);
+/* MSM over a registered base table (first `length` bases) with device scalars. */
+int dvgpu_bn254_msm_resident(void* backend, uint64_t bases_handle, const uint8_t* d_scalars, size_t length,
+                             uint8_t* result_host, void* stream, char* error, size_t error_capacity);
+int dvgpu_bn254_ntt_device(void* backend, const uint8_t* d_values, size_t length, int kind, uint8_t* d_result,
+                           void* stream, char* error, size_t error_capacity);
+int dvgpu_bn254_fixed_base_device(void* backend, const uint8_t* d_scalars, size_t length, int g2, uint8_t* d_output,
+                                  void* stream, char* error, size_t error_capacity);
+int dvgpu_bn254_g2_check_device(void* backend, const uint8_t* d_wire, size_t n, uint32_t algorithm,
+                                uint32_t* d_masks, DvgpuG2ValidationReport* report_host, void* stream, char* error,
+                                size_t error_capacity);
+
+/* Tuning: force the Pippenger window width c (0 = cost-model choice). */
+int dvgpu_msm_set_window(void* backend, int c);
+int dvgpu_msm_get_window(void* backend, size_t points_per_set, int* c);
+
+/* Integer-multiply roofline probe: runs a dependent-chain-free kernel of
+ * mad.lo.cc / madc.hi.cc pairs on every SM and reports the achieved
+ * 32x32->64-bit multiply-accumulate rate (MAC/s). */
+int dvgpu_probe_imad_rate(void* backend, double* macs_per_second, char* error, size_t error_capacity);
+
+/* Diagnostics: kernel launches of this library since load (all owners). */
+uint64_t dvgpu_launch_count(void);
+/* Per-phase MSM device time, accumulated over calls while enabled (CUDA
+ * events on the launching stream).  ms[]: 0 digit histogram, 1 offsets scan,
+ * 2 scatter, 3 bucket accumulation, 4 split-bucket merge, 5 segment
+ * reduction, 6 window sums, 7 tail (window D2H + host Horner).  enable = 1
+ * resets and starts, 0 stops; out (may be NULL) receives the totals so far. */
+typedef struct DvgpuMsmPhaseTimes {
+    double ms[8];
+    uint64_t calls;
+    uint64_t accum_mixed_adds; /* points x windows accumulated while enabled */
+} DvgpuMsmPhaseTimes;
+int dvgpu_msm_timeline(void* backend, int enable, DvgpuMsmPhaseTimes* out);
+
+/* Seeded synthetic inputs on the device: n uniform Fr scalars (canonical),
+ * and the powers tau^0..tau^(n-1) of a canonical device scalar. */
+int dvgpu_random_fr_device(void* backend, uint64_t seed, size_t n, uint8_t* d_out, void* stream, char* error,
+                           size_t error_capacity);
+int dvgpu_fr_powers_device(void* backend, const uint8_t* d_tau, size_t n, uint8_t* d_out, void* stream, char* error,
+                           size_t error_capacity);
+
+#ifdef __cplusplus
+}
+#endif

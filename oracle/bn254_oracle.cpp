@@ -1,0 +1,1035 @@
+// BN254 CPU oracle -- TEST INFRASTRUCTURE ONLY.
+//
+// This file is the checker for the CUDA library, never part of it: only the
+// tests, the smoke check and the CPU-baseline leg of the benchmark load it.
+// It restates, in plain C++ on 4 x 64-bit Montgomery limbs, the arithmetic
+// that the reference reaches through arkworks 0.4 (ark-ff 0.4.2, ark-ec
+// 0.4.2, ark-poly 0.4.2, ark-bn254 0.4.0; pinned in Cargo.lock) and ICICLE
+// v2.8.0 -- neither of which is vendored in the reference tree:
+//
+//  * G1/G2 variable-base MSM: OperatorBackend::msm / msm_g2_host
+//    (crates/protocol/src/types.rs:295-356), CPU reference straight_msm
+//    (crates/gpu/src/lib.rs:122-139) and VariableBaseMSM::msm_unchecked
+//    (crates/gpu/src/arkworks.rs:19-25).  The result is a group element, so
+//    any correct algorithm yields the same normalised affine point.
+//  * Sparse MSM: SparseMsmRequest semantics (types.rs:262-277): each entry
+//    adds value * bases[index]; order, repeats and zeros preserved.
+//  * Fr NTT: Radix2EvaluationDomain fft/ifft (crates/gpu/src/lib.rs:99-118),
+//    natural order in and out, inverse scaled by 1/n, root = GENERATOR^((r-1)
+//    /2^28) squared down to order n (crates/gpu/src/icicle.rs:440-443); coset
+//    with offset g = 5 as in arkworks get_coset (crates/protocol/src/kzg.rs:498).
+//  * Fixed base [s]G1 / [s]G2: protocol/src/setup.rs:13-31 and
+//    crates/gpu/src/fixed_base_cpu.rs:25-58 (4-bit windows, as the reference's
+//    table in native/include/icicle_setup.cuh:44-65).
+//  * G2 wire parse + on-curve + subgroup predicates (masks 1/2/4):
+//    crates/gpu/src/g2_validation.rs:214-299, native/include/icicle_g2_wire.cuh.
+//  * Codec: canonical little-endian, all-zero = infinity
+//    (crates/gpu/src/codec.rs:25-111, crates/gpu/src/resident.rs:419-431).
+//
+// Build: see oracle/Makefile (g++ -O3, shared object under oracle/build/).
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+typedef unsigned __int128 u128;
+
+namespace {
+
+// ------------------------------------------------------------------ field
+struct Fe { uint64_t v[4]; };
+
+struct Field {
+    uint64_t p[4];
+    uint64_t inv;   // -p^{-1} mod 2^64
+    Fe r2;          // R^2 mod p
+    Fe one;         // R mod p (Montgomery one)
+};
+
+static inline bool geq(const uint64_t* a, const uint64_t* b) {
+    for (int i = 3; i >= 0; --i) {
+        if (a[i] > b[i]) return true;
+        if (a[i] < b[i]) return false;
+    }
+    return true;
+}
+static inline void sub_raw(uint64_t* a, const uint64_t* b) {
+    uint64_t borrow = 0;
+    for (int i = 0; i < 4; ++i) {
+        u128 d = (u128)a[i] - b[i] - borrow;
+        a[i] = (uint64_t)d;
+        borrow = (uint64_t)(d >> 64) & 1;
+    }
+}
+
+static inline void fmul(const Field& F, Fe& out, const Fe& a, const Fe& b) {
+    // CIOS Montgomery multiplication (Koc, Acar, Kaliski 1996).
+    uint64_t t[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < 4; ++i) {
+        u128 c = 0;
+        for (int j = 0; j < 4; ++j) {
+            c += (u128)a.v[j] * b.v[i] + t[j];
+            t[j] = (uint64_t)c;
+            c >>= 64;
+        }
+        c += t[4];
+        t[4] = (uint64_t)c;
+        t[5] = (uint64_t)(c >> 64);
+        uint64_t m = t[0] * F.inv;
+        c = (u128)m * F.p[0] + t[0];
+        c >>= 64;
+        for (int j = 1; j < 4; ++j) {
+            c += (u128)m * F.p[j] + t[j];
+            t[j - 1] = (uint64_t)c;
+            c >>= 64;
+        }
+        c += t[4];
+        t[3] = (uint64_t)c;
+        t[4] = t[5] + (uint64_t)(c >> 64);
+    }
+    Fe r = {{t[0], t[1], t[2], t[3]}};
+    if (t[4] || geq(r.v, F.p)) sub_raw(r.v, F.p);
+    out = r;
+}
+static inline void fadd(const Field& F, Fe& out, const Fe& a, const Fe& b) {
+    Fe r;
+    uint64_t carry = 0;
+    for (int i = 0; i < 4; ++i) {
+        u128 s = (u128)a.v[i] + b.v[i] + carry;
+        r.v[i] = (uint64_t)s;
+        carry = (uint64_t)(s >> 64);
+    }
+    if (carry || geq(r.v, F.p)) sub_raw(r.v, F.p);
+    out = r;
+}
+static inline void fsub(const Field& F, Fe& out, const Fe& a, const Fe& b) {
+    Fe r = a;
+    if (geq(a.v, b.v)) {
+        sub_raw(r.v, b.v);
+    } else {
+        // a - b + p
+        uint64_t carry = 0;
+        for (int i = 0; i < 4; ++i) {
+            u128 s = (u128)r.v[i] + F.p[i] + carry;
+            r.v[i] = (uint64_t)s;
+            carry = (uint64_t)(s >> 64);
+        }
+        sub_raw(r.v, b.v);
+    }
+    out = r;
+}
+static inline bool fzero(const Fe& a) { return !(a.v[0] | a.v[1] | a.v[2] | a.v[3]); }
+static inline bool feq(const Fe& a, const Fe& b) {
+    return a.v[0] == b.v[0] && a.v[1] == b.v[1] && a.v[2] == b.v[2] && a.v[3] == b.v[3];
+}
+static inline void fneg(const Field& F, Fe& out, const Fe& a) {
+    if (fzero(a)) { out = a; return; }
+    Fe r = {{F.p[0], F.p[1], F.p[2], F.p[3]}};
+    sub_raw(r.v, a.v);
+    out = r;
+}
+static void fpow(const Field& F, Fe& out, const Fe& a, const uint64_t* e, int words) {
+    Fe r = F.one;
+    for (int i = words * 64 - 1; i >= 0; --i) {
+        fmul(F, r, r, r);
+        if ((e[i / 64] >> (i % 64)) & 1) fmul(F, r, r, a);
+    }
+    out = r;
+}
+static void finv(const Field& F, Fe& out, const Fe& a) {
+    uint64_t e[4] = {F.p[0] - 2, F.p[1], F.p[2], F.p[3]};
+    fpow(F, out, a, e, 4);
+}
+static void to_mont(const Field& F, Fe& out, const uint64_t* canon) {
+    Fe a = {{canon[0], canon[1], canon[2], canon[3]}};
+    fmul(F, out, a, F.r2);
+}
+static void from_mont(const Field& F, uint64_t* canon, const Fe& a) {
+    Fe one = {{1, 0, 0, 0}};
+    Fe r;
+    fmul(F, r, a, one);
+    memcpy(canon, r.v, 32);
+}
+static Field make_field(const uint64_t* p) {
+    Field F;
+    memcpy(F.p, p, 32);
+    uint64_t x = 1;  // Newton iteration for p^{-1} mod 2^64
+    for (int i = 0; i < 7; ++i) x *= 2 - p[0] * x;
+    F.inv = (uint64_t)0 - x;
+    // R mod p by reducing 2^256: compute 2^256 - k*p via repeated doubling of 1.
+    Fe r = {{1, 0, 0, 0}};
+    for (int i = 0; i < 512; ++i) {
+        // r = 2r mod p
+        uint64_t carry = 0;
+        for (int j = 0; j < 4; ++j) {
+            uint64_t nc = r.v[j] >> 63;
+            r.v[j] = (r.v[j] << 1) | carry;
+            carry = nc;
+        }
+        if (carry || geq(r.v, F.p)) sub_raw(r.v, F.p);
+        if (i == 255) F.one = r;
+    }
+    F.r2 = r;
+    return F;
+}
+
+const uint64_t Q_LIMBS[4] = {0x3c208c16d87cfd47ull, 0x97816a916871ca8dull,
+                             0xb85045b68181585dull, 0x30644e72e131a029ull};
+const uint64_t R_LIMBS[4] = {0x43e1f593f0000001ull, 0x2833e84879b97091ull,
+                             0xb85045b68181585dull, 0x30644e72e131a029ull};
+const Field FQ = make_field(Q_LIMBS);
+const Field FR = make_field(R_LIMBS);
+
+static bool read_canon(const uint8_t* bytes, uint64_t* out, const uint64_t* modulus, bool mask_flags = false) {
+    for (int i = 0; i < 4; ++i) {
+        uint64_t w = 0;
+        for (int b = 7; b >= 0; --b) w = (w << 8) | bytes[8 * i + b];
+        out[i] = w;
+    }
+    if (mask_flags) out[3] &= 0x3fffffffffffffffull;
+    return !geq(out, modulus);
+}
+static void write_canon(uint8_t* bytes, const uint64_t* v) {
+    for (int i = 0; i < 4; ++i)
+        for (int b = 0; b < 8; ++b) bytes[8 * i + b] = (uint8_t)(v[i] >> (8 * b));
+}
+static void fe_to_bytes(const Field& F, uint8_t* out, const Fe& a) {
+    uint64_t c[4];
+    from_mont(F, c, a);
+    write_canon(out, c);
+}
+
+// ------------------------------------------------------------------ Fq2
+struct Fe2 { Fe c0, c1; };
+
+struct OpsFq {
+    typedef Fe T;
+    static void mul(T& o, const T& a, const T& b) { fmul(FQ, o, a, b); }
+    static void sqr(T& o, const T& a) { fmul(FQ, o, a, a); }
+    static void add(T& o, const T& a, const T& b) { fadd(FQ, o, a, b); }
+    static void sub(T& o, const T& a, const T& b) { fsub(FQ, o, a, b); }
+    static void neg(T& o, const T& a) { fneg(FQ, o, a); }
+    static bool zero(const T& a) { return fzero(a); }
+    static bool eq(const T& a, const T& b) { return feq(a, b); }
+    static T one() { return FQ.one; }
+    static T zero_v() { T z = {{0, 0, 0, 0}}; return z; }
+    static void inv(T& o, const T& a) { finv(FQ, o, a); }
+};
+struct OpsFq2 {
+    typedef Fe2 T;
+    static void mul(T& o, const T& a, const T& b) {
+        Fe t0, t1, t2, s0, s1;
+        fmul(FQ, t0, a.c0, b.c0);
+        fmul(FQ, t1, a.c1, b.c1);
+        fadd(FQ, s0, a.c0, a.c1);
+        fadd(FQ, s1, b.c0, b.c1);
+        fmul(FQ, t2, s0, s1);
+        fsub(FQ, o.c0, t0, t1);
+        fsub(FQ, t2, t2, t0);
+        fsub(FQ, o.c1, t2, t1);
+    }
+    static void sqr(T& o, const T& a) { mul(o, a, a); }
+    static void add(T& o, const T& a, const T& b) { fadd(FQ, o.c0, a.c0, b.c0); fadd(FQ, o.c1, a.c1, b.c1); }
+    static void sub(T& o, const T& a, const T& b) { fsub(FQ, o.c0, a.c0, b.c0); fsub(FQ, o.c1, a.c1, b.c1); }
+    static void neg(T& o, const T& a) { fneg(FQ, o.c0, a.c0); fneg(FQ, o.c1, a.c1); }
+    static bool zero(const T& a) { return fzero(a.c0) && fzero(a.c1); }
+    static bool eq(const T& a, const T& b) { return feq(a.c0, b.c0) && feq(a.c1, b.c1); }
+    static T one() { T r; r.c0 = FQ.one; r.c1 = OpsFq::zero_v(); return r; }
+    static T zero_v() { T r; r.c0 = OpsFq::zero_v(); r.c1 = OpsFq::zero_v(); return r; }
+    static void inv(T& o, const T& a) {
+        Fe n, t, ni;
+        fmul(FQ, n, a.c0, a.c0);
+        fmul(FQ, t, a.c1, a.c1);
+        fadd(FQ, n, n, t);
+        finv(FQ, ni, n);
+        fmul(FQ, o.c0, a.c0, ni);
+        fmul(FQ, t, a.c1, ni);
+        fneg(FQ, o.c1, t);
+    }
+};
+
+// ------------------------------------------------------------------ curves
+// Jacobian coordinates (X, Y, Z), x = X/Z^2, y = Y/Z^3, Z = 0 is infinity.
+template <class O>
+struct Jac { typename O::T x, y, z; };
+template <class O>
+struct Aff { typename O::T x, y; bool inf; };
+
+template <class O>
+static Jac<O> jac_zero() { Jac<O> r; r.x = O::one(); r.y = O::one(); r.z = O::zero_v(); return r; }
+
+template <class O>
+static void jac_dbl(Jac<O>& r, const Jac<O>& p) {
+    typedef typename O::T T;
+    if (O::zero(p.z)) { r = p; return; }
+    T a, b, c, d, e, f, t;
+    O::sqr(a, p.x);
+    O::sqr(b, p.y);
+    O::sqr(c, b);
+    O::add(t, p.x, b);
+    O::sqr(t, t);
+    O::sub(t, t, a);
+    O::sub(t, t, c);
+    O::add(d, t, t);
+    O::add(e, a, a);
+    O::add(e, e, a);
+    O::sqr(f, e);
+    T x3, y3, z3;
+    O::sub(x3, f, d);
+    O::sub(x3, x3, d);
+    O::sub(t, d, x3);
+    O::mul(y3, e, t);
+    O::add(c, c, c);
+    O::add(c, c, c);
+    O::add(c, c, c);
+    O::sub(y3, y3, c);
+    O::mul(z3, p.y, p.z);
+    O::add(z3, z3, z3);
+    r.x = x3; r.y = y3; r.z = z3;
+}
+
+template <class O>
+static void jac_add(Jac<O>& r, const Jac<O>& p, const Jac<O>& q) {
+    typedef typename O::T T;
+    if (O::zero(p.z)) { r = q; return; }
+    if (O::zero(q.z)) { r = p; return; }
+    T z1z1, z2z2, u1, u2, s1, s2, t;
+    O::sqr(z1z1, p.z);
+    O::sqr(z2z2, q.z);
+    O::mul(u1, p.x, z2z2);
+    O::mul(u2, q.x, z1z1);
+    O::mul(t, q.z, z2z2);
+    O::mul(s1, p.y, t);
+    O::mul(t, p.z, z1z1);
+    O::mul(s2, q.y, t);
+    T h, rr;
+    O::sub(h, u2, u1);
+    O::sub(rr, s2, s1);
+    if (O::zero(h)) {
+        if (O::zero(rr)) { jac_dbl(r, p); return; }
+        r = jac_zero<O>();
+        return;
+    }
+    T i, j, v, x3, y3, z3;
+    O::add(i, h, h);
+    O::sqr(i, i);
+    O::mul(j, h, i);
+    O::add(rr, rr, rr);
+    O::mul(v, u1, i);
+    O::sqr(x3, rr);
+    O::sub(x3, x3, j);
+    O::sub(x3, x3, v);
+    O::sub(x3, x3, v);
+    O::sub(t, v, x3);
+    O::mul(y3, rr, t);
+    O::mul(t, s1, j);
+    O::add(t, t, t);
+    O::sub(y3, y3, t);
+    O::add(z3, p.z, q.z);
+    O::sqr(z3, z3);
+    O::sub(z3, z3, z1z1);
+    O::sub(z3, z3, z2z2);
+    O::mul(z3, z3, h);
+    r.x = x3; r.y = y3; r.z = z3;
+}
+
+template <class O>
+static void jac_add_aff(Jac<O>& r, const Jac<O>& p, const Aff<O>& q) {
+    if (q.inf) { r = p; return; }
+    Jac<O> qq;
+    qq.x = q.x; qq.y = q.y; qq.z = O::one();
+    jac_add(r, p, qq);
+}
+
+template <class O>
+static void jac_neg(Jac<O>& r, const Jac<O>& p) { r = p; O::neg(r.y, p.y); }
+
+template <class O>
+static bool jac_eq(const Jac<O>& a, const Jac<O>& b) {
+    typedef typename O::T T;
+    bool az = O::zero(a.z), bz = O::zero(b.z);
+    if (az || bz) return az && bz;
+    T za2, zb2, t1, t2, za3, zb3;
+    O::sqr(za2, a.z);
+    O::sqr(zb2, b.z);
+    O::mul(t1, a.x, zb2);
+    O::mul(t2, b.x, za2);
+    if (!O::eq(t1, t2)) return false;
+    O::mul(za3, za2, a.z);
+    O::mul(zb3, zb2, b.z);
+    O::mul(t1, a.y, zb3);
+    O::mul(t2, b.y, za3);
+    return O::eq(t1, t2);
+}
+
+template <class O>
+static Aff<O> jac_to_aff(const Jac<O>& p) {
+    typedef typename O::T T;
+    Aff<O> a;
+    if (O::zero(p.z)) { a.x = O::zero_v(); a.y = O::zero_v(); a.inf = true; return a; }
+    T zi, zi2, zi3;
+    O::inv(zi, p.z);
+    O::sqr(zi2, zi);
+    O::mul(zi3, zi2, zi);
+    O::mul(a.x, p.x, zi2);
+    O::mul(a.y, p.y, zi3);
+    a.inf = false;
+    return a;
+}
+
+// Batch normalisation (Montgomery's simultaneous inversion trick).
+template <class O>
+static void batch_to_aff(const Jac<O>* in, Aff<O>* out, size_t n) {
+    typedef typename O::T T;
+    std::vector<T> prefix(n);
+    T acc = O::one();
+    for (size_t i = 0; i < n; ++i) {
+        prefix[i] = acc;
+        if (!O::zero(in[i].z)) O::mul(acc, acc, in[i].z);
+    }
+    T inv;
+    O::inv(inv, acc);
+    for (size_t i = n; i-- > 0;) {
+        if (O::zero(in[i].z)) {
+            out[i].x = O::zero_v(); out[i].y = O::zero_v(); out[i].inf = true;
+            continue;
+        }
+        T zi, zi2, zi3;
+        O::mul(zi, inv, prefix[i]);
+        O::mul(inv, inv, in[i].z);
+        O::sqr(zi2, zi);
+        O::mul(zi3, zi2, zi);
+        O::mul(out[i].x, in[i].x, zi2);
+        O::mul(out[i].y, in[i].y, zi3);
+        out[i].inf = false;
+    }
+}
+
+// ------------------------------------------------------------------ codecs
+static bool g1_read(const uint8_t* b, Aff<OpsFq>& p) {
+    bool all_zero = true;
+    for (int i = 0; i < 64; ++i) all_zero &= b[i] == 0;
+    if (all_zero) { p.inf = true; p.x = OpsFq::zero_v(); p.y = OpsFq::zero_v(); return true; }
+    uint64_t x[4], y[4];
+    if (!read_canon(b, x, Q_LIMBS) || !read_canon(b + 32, y, Q_LIMBS)) return false;
+    to_mont(FQ, p.x, x);
+    to_mont(FQ, p.y, y);
+    p.inf = false;
+    return true;
+}
+static void g1_write(uint8_t* b, const Aff<OpsFq>& p) {
+    if (p.inf) { memset(b, 0, 64); return; }
+    fe_to_bytes(FQ, b, p.x);
+    fe_to_bytes(FQ, b + 32, p.y);
+}
+static bool g2_read(const uint8_t* b, Aff<OpsFq2>& p) {
+    bool all_zero = true;
+    for (int i = 0; i < 128; ++i) all_zero &= b[i] == 0;
+    if (all_zero) { p.inf = true; p.x = OpsFq2::zero_v(); p.y = OpsFq2::zero_v(); return true; }
+    uint64_t c[4][4];
+    for (int j = 0; j < 4; ++j)
+        if (!read_canon(b + 32 * j, c[j], Q_LIMBS)) return false;
+    to_mont(FQ, p.x.c0, c[0]);
+    to_mont(FQ, p.x.c1, c[1]);
+    to_mont(FQ, p.y.c0, c[2]);
+    to_mont(FQ, p.y.c1, c[3]);
+    p.inf = false;
+    return true;
+}
+static void g2_write(uint8_t* b, const Aff<OpsFq2>& p) {
+    if (p.inf) { memset(b, 0, 128); return; }
+    fe_to_bytes(FQ, b, p.x.c0);
+    fe_to_bytes(FQ, b + 32, p.x.c1);
+    fe_to_bytes(FQ, b + 64, p.y.c0);
+    fe_to_bytes(FQ, b + 96, p.y.c1);
+}
+static void scalar_read(const uint8_t* b, uint64_t* s) { read_canon(b, s, R_LIMBS); }
+
+// Curve coefficient b (Montgomery form).
+static Fe g1_b() { uint64_t c[4] = {3, 0, 0, 0}; Fe r; to_mont(FQ, r, c); return r; }
+static Fe2 g2_b() {
+    Fe2 nine_u, three, inv, r;
+    uint64_t c9[4] = {9, 0, 0, 0}, c1[4] = {1, 0, 0, 0}, c3[4] = {3, 0, 0, 0};
+    to_mont(FQ, nine_u.c0, c9);
+    to_mont(FQ, nine_u.c1, c1);
+    to_mont(FQ, three.c0, c3);
+    three.c1 = OpsFq::zero_v();
+    OpsFq2::inv(inv, nine_u);
+    OpsFq2::mul(r, three, inv);
+    return r;
+}
+
+template <class O>
+static bool on_curve(const Aff<O>& p, const typename O::T& b) {
+    if (p.inf) return true;
+    typename O::T l, r;
+    O::sqr(l, p.y);
+    O::sqr(r, p.x);
+    O::mul(r, r, p.x);
+    O::add(r, r, b);
+    return O::eq(l, r);
+}
+
+template <class O>
+static Aff<O> generator();
+template <>
+Aff<OpsFq> generator<OpsFq>() {
+    Aff<OpsFq> g;
+    uint64_t x[4] = {1, 0, 0, 0}, y[4] = {2, 0, 0, 0};
+    to_mont(FQ, g.x, x);
+    to_mont(FQ, g.y, y);
+    g.inf = false;
+    return g;
+}
+template <>
+Aff<OpsFq2> generator<OpsFq2>() {
+    // Standard BN254 G2 generator (ark-bn254 0.4.0 G2 GENERATOR_X/Y), as
+    // canonical 64-bit limbs of x.c0, x.c1, y.c0, y.c1.
+    static const uint64_t L[4][4] = {
+        {0x46debd5cd992f6edull, 0x674322d4f75edaddull, 0x426a00665e5c4479ull, 0x1800deef121f1e76ull},
+        {0x97e485b7aef312c2ull, 0xf1aa493335a9e712ull, 0x7260bfb731fb5d25ull, 0x198e9393920d483aull},
+        {0x4ce6cc0166fa7daaull, 0xe3d1e7690c43d37bull, 0x4aab71808dcb408full, 0x12c85ea5db8c6debull},
+        {0x55acdadcd122975bull, 0xbc4b313370b38ef3ull, 0xec9e99ad690c3395ull, 0x090689d0585ff075ull}};
+    Aff<OpsFq2> g;
+    to_mont(FQ, g.x.c0, L[0]);
+    to_mont(FQ, g.x.c1, L[1]);
+    to_mont(FQ, g.y.c0, L[2]);
+    to_mont(FQ, g.y.c1, L[3]);
+    g.inf = false;
+    return g;
+}
+
+// ------------------------------------------------------------------ scalar mul
+template <class O>
+static Jac<O> mul_bits(const Aff<O>& p, const uint64_t* k, int bits) {
+    Jac<O> r = jac_zero<O>();
+    for (int i = bits - 1; i >= 0; --i) {
+        jac_dbl(r, r);
+        if ((k[i / 64] >> (i % 64)) & 1) jac_add_aff(r, r, p);
+    }
+    return r;
+}
+template <class O>
+static Jac<O> mul_bits_jac(const Jac<O>& p, const uint64_t* k, int bits) {
+    Jac<O> r = jac_zero<O>();
+    for (int i = bits - 1; i >= 0; --i) {
+        jac_dbl(r, r);
+        if ((k[i / 64] >> (i % 64)) & 1) jac_add(r, r, p);
+    }
+    return r;
+}
+
+static int num_threads(int requested) {
+    if (requested > 0) return requested;
+    unsigned h = std::thread::hardware_concurrency();
+    return h ? (int)h : 1;
+}
+
+template <class F>
+static void parallel_for(size_t n, int threads, F fn) {
+    threads = std::max(1, std::min<int>(threads, (int)std::max<size_t>(n, 1)));
+    if (threads == 1) { fn(0, n); return; }
+    std::vector<std::thread> ts;
+    size_t chunk = (n + threads - 1) / threads;
+    for (int t = 0; t < threads; ++t) {
+        size_t lo = t * chunk, hi = std::min(n, lo + chunk);
+        if (lo >= hi) break;
+        ts.emplace_back([=]() { fn(lo, hi); });
+    }
+    for (auto& t : ts) t.join();
+}
+
+// ------------------------------------------------------------------ MSM
+// Straight double-and-add, the shape of crates/gpu/src/lib.rs:122-139.
+template <class O>
+static Jac<O> msm_naive(const Aff<O>* pts, const uint64_t (*sc)[4], size_t n) {
+    Jac<O> acc = jac_zero<O>();
+    for (size_t i = 0; i < n; ++i) {
+        Jac<O> cur;
+        if (pts[i].inf) continue;
+        cur.x = pts[i].x; cur.y = pts[i].y; cur.z = O::one();
+        for (int b = 0; b < 254; ++b) {
+            if ((sc[i][b / 64] >> (b % 64)) & 1) jac_add(acc, acc, cur);
+            jac_dbl(cur, cur);
+        }
+    }
+    return acc;
+}
+
+static inline uint32_t window_digit(const uint64_t* s, int start, int c) {
+    uint64_t v = s[start / 64] >> (start % 64);
+    int have = 64 - start % 64;
+    if (have < c && start / 64 + 1 < 4) v |= s[start / 64 + 1] << have;
+    return (uint32_t)(v & ((1ull << c) - 1));
+}
+
+// Unsigned-window Pippenger; windows are distributed over threads.
+template <class O>
+static Jac<O> msm_pippenger(const Aff<O>* pts, const uint64_t (*sc)[4], size_t n, int threads) {
+    int c = 1;
+    double best = 1e300;
+    for (int cc = 2; cc <= 20; ++cc) {
+        double cost = ((254 + cc - 1) / cc) * ((double)n + 2.0 * (1u << cc));
+        if (cost < best) { best = cost; c = cc; }
+    }
+    int windows = (254 + c - 1) / c;
+    std::vector<Jac<O>> sums(windows);
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        std::vector<Jac<O>> buckets(((size_t)1 << c));
+        for (;;) {
+            int w = next.fetch_add(1);
+            if (w >= windows) break;
+            for (auto& bkt : buckets) bkt = jac_zero<O>();
+            for (size_t i = 0; i < n; ++i) {
+                uint32_t d = window_digit(sc[i], w * c, std::min(c, 254 - w * c));
+                if (d) jac_add_aff(buckets[d], buckets[d], pts[i]);
+            }
+            Jac<O> running = jac_zero<O>(), total = jac_zero<O>();
+            for (size_t b = buckets.size() - 1; b >= 1; --b) {
+                jac_add(running, running, buckets[b]);
+                jac_add(total, total, running);
+            }
+            sums[w] = total;
+        }
+    };
+    int nt = std::max(1, std::min(num_threads(threads), windows));
+    std::vector<std::thread> ts;
+    for (int t = 1; t < nt; ++t) ts.emplace_back(work);
+    work();
+    for (auto& t : ts) t.join();
+    Jac<O> acc = jac_zero<O>();
+    for (int w = windows - 1; w >= 0; --w) {
+        for (int k = 0; k < c; ++k) jac_dbl(acc, acc);
+        jac_add(acc, acc, sums[w]);
+    }
+    return acc;
+}
+
+template <class O>
+static int msm_bytes(const uint8_t* pbytes, const uint8_t* sbytes, size_t n, uint8_t* out, int threads,
+                     int naive, bool (*rd)(const uint8_t*, Aff<O>&), void (*wr)(uint8_t*, const Aff<O>&),
+                     size_t psize) {
+    std::vector<Aff<O>> pts(n);
+    std::vector<uint64_t[4]> sc(n);
+    for (size_t i = 0; i < n; ++i) {
+        if (!rd(pbytes + psize * i, pts[i])) return -1;
+        scalar_read(sbytes + 32 * i, sc[i]);
+    }
+    Jac<O> r = (naive || n < 32) ? msm_naive<O>(pts.data(), sc.data(), n)
+                                 : msm_pippenger<O>(pts.data(), sc.data(), n, threads);
+    wr(out, jac_to_aff(r));
+    return 0;
+}
+
+// ------------------------------------------------------------------ fixed base
+template <class O>
+static void fixed_base(const uint8_t* sbytes, size_t n, uint8_t* out, int threads,
+                       void (*wr)(uint8_t*, const Aff<O>&), size_t psize) {
+    // 64 windows of 4 bits: table[w][d] = [d * 16^w] G.
+    const int W = 64;
+    std::vector<Jac<O>> tj(W * 16);
+    Jac<O> base;
+    Aff<O> g = generator<O>();
+    base.x = g.x; base.y = g.y; base.z = O::one();
+    for (int w = 0; w < W; ++w) {
+        Jac<O> acc = jac_zero<O>();
+        for (int d = 0; d < 16; ++d) { tj[w * 16 + d] = acc; jac_add(acc, acc, base); }
+        for (int k = 0; k < 4; ++k) jac_dbl(base, base);
+    }
+    std::vector<Aff<O>> table(W * 16);
+    batch_to_aff(tj.data(), table.data(), tj.size());
+    parallel_for(n, num_threads(threads), [&](size_t lo, size_t hi) {
+        std::vector<Jac<O>> res(hi - lo);
+        for (size_t i = lo; i < hi; ++i) {
+            uint64_t s[4];
+            scalar_read(sbytes + 32 * i, s);
+            Jac<O> acc = jac_zero<O>();
+            for (int w = 0; w < W; ++w) {
+                uint32_t d = (s[w / 16] >> (4 * (w % 16))) & 15;
+                if (d) jac_add_aff(acc, acc, table[w * 16 + d]);
+            }
+            res[i - lo] = acc;
+        }
+        std::vector<Aff<O>> aff(hi - lo);
+        batch_to_aff(res.data(), aff.data(), res.size());
+        for (size_t i = lo; i < hi; ++i) wr(out + psize * i, aff[i - lo]);
+    });
+}
+
+// ------------------------------------------------------------------ G2 subgroup
+static Fe2 PSI_CX, PSI_CY;
+static void init_psi() {
+    // xi = 9 + u; cx = xi^((q-1)/3), cy = xi^((q-1)/2), computed on the integer q-1.
+    Fe2 xi;
+    uint64_t c9[4] = {9, 0, 0, 0}, c1[4] = {1, 0, 0, 0};
+    to_mont(FQ, xi.c0, c9);
+    to_mont(FQ, xi.c1, c1);
+    auto divide = [](uint64_t d, uint64_t* out) {
+        uint64_t qm1[4] = {Q_LIMBS[0] - 1, Q_LIMBS[1], Q_LIMBS[2], Q_LIMBS[3]};
+        u128 rem = 0;
+        for (int i = 3; i >= 0; --i) {
+            u128 v = (rem << 64) | qm1[i];
+            out[i] = (uint64_t)(v / d);
+            rem = v % d;
+        }
+    };
+    uint64_t e3[4], e2[4];
+    divide(3, e3);
+    divide(2, e2);
+    auto pw = [&](const uint64_t* e) {
+        Fe2 r = OpsFq2::one(), base = xi;
+        for (int i = 0; i < 256; ++i) {
+            if ((e[i / 64] >> (i % 64)) & 1) OpsFq2::mul(r, r, base);
+            OpsFq2::mul(base, base, base);
+        }
+        return r;
+    };
+    PSI_CX = pw(e3);
+    PSI_CY = pw(e2);
+}
+static Jac<OpsFq2> psi(const Jac<OpsFq2>& p) {
+    if (OpsFq2::zero(p.z)) return p;
+    // Jacobian form: psi(X, Y, Z) = (conj(X) cx, conj(Y) cy, conj(Z)), valid
+    // because conj commutes with the Jacobian scaling.
+    Jac<OpsFq2> r;
+    Fe2 t;
+    t = p.x; fneg(FQ, t.c1, p.x.c1); OpsFq2::mul(r.x, t, PSI_CX);
+    t = p.y; fneg(FQ, t.c1, p.y.c1); OpsFq2::mul(r.y, t, PSI_CY);
+    r.z = p.z; fneg(FQ, r.z.c1, p.z.c1);
+    return r;
+}
+static const uint64_t BN_SEED = 4965661367192848881ull;
+
+static bool subgroup_check(const Aff<OpsFq2>& a, uint32_t algorithm) {
+    Jac<OpsFq2> p;
+    p.x = a.x; p.y = a.y; p.z = OpsFq2::one();
+    if (algorithm == 1) {
+        Jac<OpsFq2> r = mul_bits_jac(p, R_LIMBS, 254);
+        return OpsFq2::zero(r.z);
+    }
+    if (algorithm == 2) {
+        u128 lam = (u128)6 * BN_SEED * BN_SEED;
+        uint64_t l[4] = {(uint64_t)lam, (uint64_t)(lam >> 64), 0, 0};
+        Jac<OpsFq2> r = mul_bits_jac(p, l, 128);
+        return jac_eq(psi(p), r);
+    }
+    uint64_t s[4] = {BN_SEED, 0, 0, 0};
+    Jac<OpsFq2> x = mul_bits_jac(p, s, 63);
+    Jac<OpsFq2> b = psi(x), c = psi(b), lhs, rhs;
+    jac_add(lhs, x, p);
+    jac_add(lhs, lhs, b);
+    jac_add(lhs, lhs, c);
+    rhs = psi(c);
+    jac_dbl(rhs, rhs);
+    return jac_eq(lhs, rhs);
+}
+
+static uint32_t g2_wire_mask(const uint8_t* b, uint32_t algorithm, const Fe2& curve_b) {
+    bool all_zero = true;
+    for (int i = 0; i < 128; ++i) all_zero &= b[i] == 0;
+    if (all_zero) return 0;
+    unsigned flags = b[127] & 0xc0;
+    if (flags == 0xc0) return 1;
+    uint64_t c[4][4];
+    for (int j = 0; j < 4; ++j)
+        if (!read_canon(b + 32 * j, c[j], Q_LIMBS, j == 3)) return 1;
+    if (flags == 0x40) return 0;
+    Aff<OpsFq2> p;
+    to_mont(FQ, p.x.c0, c[0]);
+    to_mont(FQ, p.x.c1, c[1]);
+    to_mont(FQ, p.y.c0, c[2]);
+    to_mont(FQ, p.y.c1, c[3]);
+    p.inf = false;
+    if (!on_curve(p, curve_b)) return 2;
+    return subgroup_check(p, algorithm) ? 0 : 4;
+}
+
+// ------------------------------------------------------------------ NTT
+static void ntt_inplace(std::vector<Fe>& a, const Fe& omega) {
+    size_t n = a.size();
+    int logn = 0;
+    while (((size_t)1 << logn) < n) ++logn;
+    for (size_t i = 0; i < n; ++i) {
+        size_t j = 0;
+        for (int b = 0; b < logn; ++b) j |= ((i >> b) & 1) << (logn - 1 - b);
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (size_t len = 2; len <= n; len <<= 1) {
+        Fe wlen = omega;
+        for (size_t k = len; k < n; k <<= 1) fmul(FR, wlen, wlen, wlen);
+        std::vector<Fe> tw(len / 2);
+        tw[0] = FR.one;
+        for (size_t j = 1; j < len / 2; ++j) fmul(FR, tw[j], tw[j - 1], wlen);
+        for (size_t i = 0; i < n; i += len) {
+            for (size_t j = 0; j < len / 2; ++j) {
+                Fe u = a[i + j], v;
+                fmul(FR, v, a[i + j + len / 2], tw[j]);
+                fadd(FR, a[i + j], u, v);
+                fsub(FR, a[i + j + len / 2], u, v);
+            }
+        }
+    }
+}
+static Fe root_of_unity(size_t n) {
+    // GENERATOR^((r-1)/2^28), squared (28 - log2 n) times.
+    uint64_t e[4] = {R_LIMBS[0] - 1, R_LIMBS[1], R_LIMBS[2], R_LIMBS[3]};
+    for (int k = 0; k < 28; ++k) {
+        for (int i = 0; i < 3; ++i) e[i] = (e[i] >> 1) | (e[i + 1] << 63);
+        e[3] >>= 1;
+    }
+    uint64_t g[4] = {5, 0, 0, 0};
+    Fe gm, w;
+    to_mont(FR, gm, g);
+    fpow(FR, w, gm, e, 4);
+    int logn = 0;
+    while (((size_t)1 << logn) < n) ++logn;
+    for (int k = logn; k < 28; ++k) fmul(FR, w, w, w);
+    return w;
+}
+
+struct Init { Init() { init_psi(); } } init_once;
+
+// ------------------------------------------------------------------ ChaCha20
+static inline uint32_t rotl(uint32_t v, int c) { return (v << c) | (v >> (32 - c)); }
+static void chacha_block(const uint32_t* key, uint32_t counter, uint8_t* out) {
+    uint32_t init[16] = {0x61707865, 0x3320646e, 0x79622d32, 0x6b206574, key[0], key[1], key[2], key[3],
+                         key[4], key[5], key[6], key[7], counter, 0, 0, 0};
+    uint32_t s[16];
+    memcpy(s, init, sizeof s);
+#define QR(a, b, c, d)                                \
+    s[a] += s[b]; s[d] = rotl(s[d] ^ s[a], 16);       \
+    s[c] += s[d]; s[b] = rotl(s[b] ^ s[c], 12);       \
+    s[a] += s[b]; s[d] = rotl(s[d] ^ s[a], 8);        \
+    s[c] += s[d]; s[b] = rotl(s[b] ^ s[c], 7);
+    for (int i = 0; i < 10; ++i) {
+        QR(0, 4, 8, 12) QR(1, 5, 9, 13) QR(2, 6, 10, 14) QR(3, 7, 11, 15)
+        QR(0, 5, 10, 15) QR(1, 6, 11, 12) QR(2, 7, 8, 13) QR(3, 4, 9, 14)
+    }
+#undef QR
+    for (int i = 0; i < 16; ++i) {
+        uint32_t v = s[i] + init[i];
+        for (int b = 0; b < 4; ++b) out[4 * i + b] = (uint8_t)(v >> (8 * b));
+    }
+}
+struct ChaCha {
+    uint32_t key[8];
+    uint32_t counter = 0;
+    uint8_t buf[64];
+    int pos = 64;
+    explicit ChaCha(uint64_t seed) {
+        memset(key, 0, sizeof key);
+        key[0] = (uint32_t)seed;
+        key[1] = (uint32_t)(seed >> 32);
+    }
+    void read(uint8_t* out, size_t n) {
+        for (size_t i = 0; i < n; ++i) {
+            if (pos == 64) { chacha_block(key, counter++, buf); pos = 0; }
+            out[i] = buf[pos++];
+        }
+    }
+    void uniform(const uint64_t* modulus, uint8_t* out) {
+        for (;;) {
+            read(out, 32);
+            out[31] &= 0x3f;
+            uint64_t v[4];
+            read_canon(out, v, modulus);
+            if (!geq(v, modulus)) return;
+        }
+    }
+};
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+int oracle_msm_g1(const uint8_t* points, const uint8_t* scalars, size_t n, uint8_t* out, int threads, int naive) {
+    return msm_bytes<OpsFq>(points, scalars, n, out, threads, naive, g1_read, g1_write, 64);
+}
+int oracle_msm_g2(const uint8_t* points, const uint8_t* scalars, size_t n, uint8_t* out, int threads, int naive) {
+    return msm_bytes<OpsFq2>(points, scalars, n, out, threads, naive, g2_read, g2_write, 128);
+}
+
+// Sparse MSM: sum_j values[j] * bases[indices[j]] (types.rs:262-277).
+int oracle_sparse_msm_g1(const uint8_t* bases, size_t nbases, const uint64_t* indices, const uint8_t* values,
+                         size_t k, uint8_t* out, int threads) {
+    std::vector<uint8_t> pts(64 * k);
+    for (size_t j = 0; j < k; ++j) {
+        if (indices[j] >= nbases) return -1;
+        memcpy(&pts[64 * j], bases + 64 * indices[j], 64);
+    }
+    return oracle_msm_g1(pts.data(), values, k, out, threads, 0);
+}
+
+// kind: 0 forward, 1 inverse, 2 coset forward, 3 coset inverse.
+int oracle_ntt(uint8_t* values, size_t n, int kind) {
+    if (n == 0 || (n & (n - 1)) || n > ((size_t)1 << 28) || kind < 0 || kind > 3) return -1;
+    std::vector<Fe> a(n);
+    for (size_t i = 0; i < n; ++i) {
+        uint64_t c[4];
+        if (!read_canon(values + 32 * i, c, R_LIMBS)) return -1;
+        to_mont(FR, a[i], c);
+    }
+    bool inverse = kind & 1, coset = kind >= 2;
+    uint64_t g5[4] = {5, 0, 0, 0};
+    Fe g;
+    to_mont(FR, g, g5);
+    if (coset && !inverse) {
+        Fe pw = FR.one;
+        for (size_t i = 0; i < n; ++i) { fmul(FR, a[i], a[i], pw); fmul(FR, pw, pw, g); }
+    }
+    Fe w = root_of_unity(n);
+    if (inverse) finv(FR, w, w);
+    if (n > 1) ntt_inplace(a, w);
+    if (inverse) {
+        uint64_t nc[4] = {(uint64_t)n, 0, 0, 0};
+        Fe nm, ni;
+        to_mont(FR, nm, nc);
+        finv(FR, ni, nm);
+        for (auto& v : a) fmul(FR, v, v, ni);
+        if (coset) {
+            Fe gi, pw = FR.one;
+            finv(FR, gi, g);
+            for (size_t i = 0; i < n; ++i) { fmul(FR, a[i], a[i], pw); fmul(FR, pw, pw, gi); }
+        }
+    }
+    for (size_t i = 0; i < n; ++i) fe_to_bytes(FR, values + 32 * i, a[i]);
+    return 0;
+}
+
+void oracle_fixed_base_g1(const uint8_t* scalars, size_t n, uint8_t* out, int threads) {
+    fixed_base<OpsFq>(scalars, n, out, threads, g1_write, 64);
+}
+void oracle_fixed_base_g2(const uint8_t* scalars, size_t n, uint8_t* out, int threads) {
+    fixed_base<OpsFq2>(scalars, n, out, threads, g2_write, 128);
+}
+
+void oracle_g2_check(const uint8_t* wire, size_t n, uint32_t algorithm, uint32_t* masks, int threads) {
+    Fe2 b = g2_b();
+    parallel_for(n, num_threads(threads), [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) masks[i] = g2_wire_mask(wire + 128 * i, algorithm, b);
+    });
+}
+
+int oracle_g1_on_curve(const uint8_t* point) {
+    Aff<OpsFq> p;
+    if (!g1_read(point, p)) return 0;
+    return on_curve(p, g1_b());
+}
+int oracle_g2_on_curve(const uint8_t* point) {
+    Aff<OpsFq2> p;
+    if (!g2_read(point, p)) return 0;
+    return on_curve(p, g2_b());
+}
+
+// Uniform field elements from the seeded ChaCha20 stream (key = seed LE).
+// which: 0 = Fr, 1 = Fq.
+void oracle_chacha_uniform(uint64_t seed, size_t n, int which, uint8_t* out) {
+    ChaCha rng(seed);
+    for (size_t i = 0; i < n; ++i) rng.uniform(which ? Q_LIMBS : R_LIMBS, out + 32 * i);
+}
+
+// Powers tau^0 .. tau^{n-1} in Fr (canonical bytes).
+void oracle_fr_powers(const uint8_t* tau, size_t n, uint8_t* out) {
+    uint64_t c[4];
+    read_canon(tau, c, R_LIMBS);
+    Fe t, acc = FR.one;
+    to_mont(FR, t, c);
+    for (size_t i = 0; i < n; ++i) { fe_to_bytes(FR, out + 32 * i, acc); fmul(FR, acc, acc, t); }
+}
+
+// Twist points from x (Fq2 x given), y = sqrt(x^3 + b') when it exists; writes
+// found points consecutively and returns how many.  Uses q = 3 mod 4.
+size_t oracle_g2_twist_points(uint64_t seed, size_t want, uint8_t* out) {
+    ChaCha rng(seed);
+    Fe2 b = g2_b();
+    size_t got = 0;
+    uint64_t e34[4] = {Q_LIMBS[0], Q_LIMBS[1], Q_LIMBS[2], Q_LIMBS[3]};
+    // (q-3)/4
+    {
+        u128 s = (u128)e34[0] - 3;
+        e34[0] = (uint64_t)s;
+        for (int i = 0; i < 3; ++i) e34[i] = (e34[i] >> 2) | (e34[i + 1] << 62);
+        e34[3] >>= 2;
+    }
+    uint64_t eh[4] = {Q_LIMBS[0] - 1, Q_LIMBS[1], Q_LIMBS[2], Q_LIMBS[3]};
+    for (int i = 0; i < 3; ++i) eh[i] = (eh[i] >> 1) | (eh[i + 1] << 63);
+    eh[3] >>= 1;
+    auto pw2 = [](const Fe2& a, const uint64_t* e) {
+        Fe2 r = OpsFq2::one(), base = a;
+        for (int i = 0; i < 256; ++i) {
+            if ((e[i / 64] >> (i % 64)) & 1) OpsFq2::mul(r, r, base);
+            OpsFq2::mul(base, base, base);
+        }
+        return r;
+    };
+    Fe2 minus_one = OpsFq2::one();
+    fneg(FQ, minus_one.c0, minus_one.c0);
+    while (got < want) {
+        uint8_t xb[64];
+        rng.uniform(Q_LIMBS, xb);
+        rng.uniform(Q_LIMBS, xb + 32);
+        Aff<OpsFq2> p;
+        uint64_t c0[4], c1[4];
+        read_canon(xb, c0, Q_LIMBS);
+        read_canon(xb + 32, c1, Q_LIMBS);
+        to_mont(FQ, p.x.c0, c0);
+        to_mont(FQ, p.x.c1, c1);
+        Fe2 rhs, a1, alpha, x0, y, t;
+        OpsFq2::sqr(rhs, p.x);
+        OpsFq2::mul(rhs, rhs, p.x);
+        OpsFq2::add(rhs, rhs, b);
+        a1 = pw2(rhs, e34);
+        OpsFq2::mul(t, a1, rhs);
+        OpsFq2::mul(alpha, a1, t);
+        x0 = t;
+        if (OpsFq2::eq(alpha, minus_one)) {
+            Fe2 uu = OpsFq2::zero_v();
+            uu.c1 = FQ.one;
+            OpsFq2::mul(y, uu, x0);
+        } else {
+            Fe2 onep = OpsFq2::one(), bb;
+            OpsFq2::add(bb, onep, alpha);
+            bb = pw2(bb, eh);
+            OpsFq2::mul(y, bb, x0);
+        }
+        OpsFq2::sqr(t, y);
+        if (!OpsFq2::eq(t, rhs)) continue;
+        p.y = y;
+        p.inf = false;
+        g2_write(out + 128 * got, p);
+        ++got;
+    }
+    return got;
+}
+
+// out = a + b (affine, canonical bytes) for G1 and G2, and [k]P.
+int oracle_g1_add(const uint8_t* a, const uint8_t* b, uint8_t* out) {
+    Aff<OpsFq> pa, pb;
+    if (!g1_read(a, pa) || !g1_read(b, pb)) return -1;
+    Jac<OpsFq> ja = jac_zero<OpsFq>();
+    jac_add_aff(ja, ja, pa);
+    jac_add_aff(ja, ja, pb);
+    g1_write(out, jac_to_aff(ja));
+    return 0;
+}
+int oracle_g2_add(const uint8_t* a, const uint8_t* b, uint8_t* out) {
+    Aff<OpsFq2> pa, pb;
+    if (!g2_read(a, pa) || !g2_read(b, pb)) return -1;
+    Jac<OpsFq2> ja = jac_zero<OpsFq2>();
+    jac_add_aff(ja, ja, pa);
+    jac_add_aff(ja, ja, pb);
+    g2_write(out, jac_to_aff(ja));
+    return 0;
+}
+int oracle_g2_mul_r(const uint8_t* a, uint8_t* out) {
+    Aff<OpsFq2> pa;
+    if (!g2_read(a, pa)) return -1;
+    g2_write(out, jac_to_aff(mul_bits(pa, R_LIMBS, 254)));
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+"""CPU-only checks of the boundary: the C-ABI library loads, exports every
+symbol include/dynaverse_gpu.h declares, and the field constants embedded in
+the CUDA sources equal the values computed here with Python integers."""
+import ctypes
+import os
+import re
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+import bn254_py as b  # noqa: E402
+
+HEADER = os.path.join(ROOT, "include", "dynaverse_gpu.h")
+CSRC = os.path.join(ROOT, "zkp-dynaverse_b200", "csrc")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dvgpu_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_reference_entry_points():
+    names = set(declared_functions())
+    # the entry points the reference's Rust crate binds (icicle.rs:35-57,
+    # setup.rs:47-52, g2_validation.rs:84-93)
+    for n in ["dvgpu_backend_create", "dvgpu_backend_create_with_large_bucket_factor", "dvgpu_backend_destroy",
+              "dvgpu_backend_device_identity", "dvgpu_backend_batch_stats", "dvgpu_backend_memory_info",
+              "dvgpu_bn254_msm", "dvgpu_bn254_msm_batch", "dvgpu_bn254_g2_msm", "dvgpu_bn254_ntt",
+              "dvgpu_bn254_msm_profiled", "dvgpu_bn254_fixed_base", "dvgpu_setup_mode", "dvgpu_setup_stats",
+              "dvgpu_bn254_g2_validation_inspect", "dvgpu_g2_validation_stats", "dvgpu_g2_validation_traffic",
+              "dvgpu_bn254_fixed_base_g2_checked", "dvgpu_reserve_batch"]:
+        assert n in names, n
+
+
+def test_library_exports_every_declared_symbol(dv):
+    lib = dv.lib()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_signatures_cover_header(dv):
+    bound = {s[0] for s in dv.SIGNATURES}
+    assert set(declared_functions()) <= bound
+
+
+def _limbs32(v):
+    return [(v >> (32 * i)) & 0xFFFFFFFF for i in range(8)]
+
+
+def _cfg_values(text, cfg, prefix):
+    body = text[text.index(f"struct {cfg}"):]
+    body = body[:body.index("};")]
+    vals = {}
+    for name, val in re.findall(r"\b([A-Z0-9]+)\s*=\s*(0x[0-9a-fA-F]+)u", body):
+        vals[name] = int(val, 16)
+    return [vals[f"{prefix}{i}"] for i in range(8)], vals
+
+
+@pytest.mark.parametrize("cfg,p", [("FqCfg", b.Q), ("FrCfg", b.R)])
+def test_device_field_constants(cfg, p):
+    text = open(os.path.join(CSRC, "field.cuh")).read()
+    pl, vals = _cfg_values(text, cfg, "P")
+    assert pl == _limbs32(p)
+    assert vals["INV"] == (-pow(p, -1, 1 << 32)) % (1 << 32)
+    one, _ = _cfg_values(text, cfg, "ONE")
+    r2, _ = _cfg_values(text, cfg, "R2")
+    assert one == _limbs32((1 << 256) % p)
+    assert r2 == _limbs32((1 << 512) % p)
+
+
+def _c_array(text, name):
+    m = re.search(name + r"[^=]*=\s*\{(.*?)\};", text, flags=re.S)
+    return [int(x, 16) for x in re.findall(r"0x[0-9a-fA-F]+", m.group(1))]
+
+
+def _int_of(words):
+    return sum(w << (32 * i) for i, w in enumerate(words))
+
+
+def test_device_curve_and_psi_constants():
+    g2 = open(os.path.join(CSRC, "g2.cu")).read()
+    psi = _c_array(g2, "PSI_C")
+    assert _int_of(psi[0:8]) == b.PSI_CX[0] and _int_of(psi[8:16]) == b.PSI_CX[1]
+    assert _int_of(psi[16:24]) == b.PSI_CY[0] and _int_of(psi[24:32]) == b.PSI_CY[1]
+    assert _int_of(_c_array(g2, "R_INT")) == b.R
+    assert _int_of(_c_array(g2, "LAMBDA")) == 6 * b.BN_SEED ** 2
+    assert _int_of(_c_array(g2, "SEED")) == b.BN_SEED
+    gen = _c_array(g2, "G2_GEN")
+    assert (_int_of(gen[0:8]), _int_of(gen[8:16])) == b.G2_GEN[0]
+    assert (_int_of(gen[16:24]), _int_of(gen[24:32])) == b.G2_GEN[1]
+    curve = open(os.path.join(CSRC, "curve.cuh")).read()
+    body = curve[curve.index("Fq2 g2_b()"):]
+    assert _int_of(_c_array(body, "c0")) == b.B2[0]
+    assert _int_of(_c_array(body, "c1")) == b.B2[1]
+    ntt = open(os.path.join(CSRC, "ntt.cu")).read()
+    assert _int_of(_c_array(ntt, "ROOT28")) == b.root_of_unity(1 << 28)

@@ -1,0 +1,443 @@
+"""dynaverse-b200: BN254 prover operators on B200, behind the dvgpu C-ABI.
+
+Host-side mirror of the reference's operator plugin interface
+(`OperatorBackend`, crates/protocol/src/types.rs:281-359, implemented for the
+GPU by `IcicleBackend`, crates/gpu/src/icicle.rs:342-457).  Method names,
+argument meaning and error behaviour follow the trait:
+
+* results in caller order, element-identical to the CPU reference;
+* inputs validated before any dispatch; errors raise DvgpuError and never
+  fall back to a CPU path;
+* a failed call leaves caller data untouched.
+
+All compute runs in libdvgpu.so (hand-written sm_100a kernels); this module
+only marshals bytes.  Wire formats: Fr 32-byte LE canonical, G1 64 bytes,
+G2 128 bytes, infinity all zero (crates/gpu/src/codec.rs:25-111).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libdvgpu.so")
+
+FR_BYTES = 32
+G1_BYTES = 64
+G2_BYTES = 128
+R_MODULUS = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+Q_MODULUS = 0x30644E72E131A029B85045B68181585D97816A916871CA8D3C208C16D87CFD47
+
+NTT_FORWARD, NTT_INVERSE, NTT_COSET_FORWARD, NTT_COSET_INVERSE = 0, 1, 2, 3
+
+_lib = None
+
+
+class DvgpuError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"dvgpu error {status}: {message}")
+        self.status = status
+        self.message = message
+
+
+class G2ValidationReport(ctypes.Structure):
+    _fields_ = [("checked_points", ctypes.c_uint64), ("invalid_points", ctypes.c_uint64),
+                ("first_invalid", ctypes.c_uint64), ("failure_mask", ctypes.c_uint32),
+                ("algorithm", ctypes.c_uint32)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("icicle_calls", ctypes.c_uint64), ("buffer_grows", ctypes.c_uint64),
+                ("max_batch_size", ctypes.c_uint64), ("input_capacity", ctypes.c_uint64)]
+
+
+class MemoryInfo(ctypes.Structure):
+    _fields_ = [("free_bytes", ctypes.c_uint64), ("total_bytes", ctypes.c_uint64)]
+
+
+class MsmPhaseTimes(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double * 8), ("calls", ctypes.c_uint64), ("accum_mixed_adds", ctypes.c_uint64)]
+
+
+MSM_PHASE_NAMES = ["hist", "scan", "scatter", "accum", "fixup", "segments", "wsum", "tail"]
+
+
+class SetupStats(ctypes.Structure):
+    _fields_ = [("table_builds", ctypes.c_uint64 * 2), ("calls", ctypes.c_uint64 * 2),
+                ("points", ctypes.c_uint64 * 2), ("table_bytes", ctypes.c_uint64),
+                ("device_ns", ctypes.c_uint64 * 5), ("native_wall_ns", ctypes.c_uint64)]
+
+
+# (name, restype, argtypes)
+_P = ctypes.c_void_p
+_B = ctypes.c_char_p
+_SZ = ctypes.c_size_t
+_E = [ctypes.c_char_p, ctypes.c_size_t]
+SIGNATURES = [
+    ("dvgpu_backend_create", ctypes.c_int, [ctypes.POINTER(_P)] + _E),
+    ("dvgpu_backend_create_with_large_bucket_factor", ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(_P)] + _E),
+    ("dvgpu_backend_destroy", None, [_P]),
+    ("dvgpu_backend_device_identity", ctypes.c_int, [_P, _B, _SZ] + _E),
+    ("dvgpu_backend_memory_info", ctypes.c_int, [_P, ctypes.POINTER(MemoryInfo)] + _E),
+    ("dvgpu_backend_batch_stats", ctypes.c_int, [_P, ctypes.POINTER(BatchStats)]),
+    ("dvgpu_bn254_msm", ctypes.c_int, [_P, _P, _P, _SZ, _B] + _E),
+    ("dvgpu_bn254_g2_msm", ctypes.c_int, [_P, _P, _P, _SZ, _B] + _E),
+    ("dvgpu_bn254_msm_batch", ctypes.c_int, [_P, _P, _P, _SZ, _SZ, _B] + _E),
+    ("dvgpu_bn254_ntt", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _B, _B] + _E),
+    ("dvgpu_setup_mode", ctypes.c_int, [_P, ctypes.c_int]),
+    ("dvgpu_setup_stats", ctypes.c_int, [_P, ctypes.POINTER(SetupStats)]),
+    ("dvgpu_bn254_g2_validation_inspect", ctypes.c_int,
+     [_P, _P, _SZ, ctypes.c_uint32, _P, ctypes.POINTER(G2ValidationReport)] + _E),
+    ("dvgpu_g2_validation_stats", ctypes.c_int, [_P, _P]),
+    ("dvgpu_g2_validation_traffic", ctypes.c_int, [_P, _P]),
+    ("dvgpu_bn254_fixed_base_g2_checked", ctypes.c_int,
+     [_P, _P, _SZ, ctypes.c_uint32, _B, ctypes.POINTER(G2ValidationReport)] + _E),
+    ("dvgpu_bn254_fixed_base", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _B] + _E),
+    ("dvgpu_reserve_batch", ctypes.c_int, [_P, _SZ] + _E),
+    ("dvgpu_bn254_msm_profiled", ctypes.c_int, [_P, _P, _P, _SZ, _B, _P] + _E),
+    ("dvgpu_bn254_ntt_ex", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _B] + _E),
+    ("dvgpu_bn254_msm_batch_uneven", ctypes.c_int, [_P, _P, _P, _P, _SZ, _B] + _E),
+    ("dvgpu_bases_register", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)] + _E),
+    ("dvgpu_bases_release", ctypes.c_int, [_P, ctypes.c_uint64]),
+    ("dvgpu_bn254_msm_sparse_batch", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _P, _SZ, _B] + _E),
+    ("dvgpu_bn254_msm_device", ctypes.c_int, [_P, _P, _P, _SZ, ctypes.c_int, _B, _P] + _E),
+    ("dvgpu_bn254_msm_resident", ctypes.c_int, [_P, ctypes.c_uint64, _P, _SZ, _B, _P] + _E),
+    ("dvgpu_bn254_ntt_device", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _P, _P] + _E),
+    ("dvgpu_bn254_fixed_base_device", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _P, _P] + _E),
+    ("dvgpu_bn254_g2_check_device", ctypes.c_int,
+     [_P, _P, _SZ, ctypes.c_uint32, _P, ctypes.POINTER(G2ValidationReport), _P] + _E),
+    ("dvgpu_msm_set_window", ctypes.c_int, [_P, ctypes.c_int]),
+    ("dvgpu_msm_get_window", ctypes.c_int, [_P, _SZ, ctypes.POINTER(ctypes.c_int)]),
+    ("dvgpu_probe_imad_rate", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)] + _E),
+    ("dvgpu_launch_count", ctypes.c_uint64, []),
+    ("dvgpu_msm_timeline", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(MsmPhaseTimes)]),
+    ("dvgpu_random_fr_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
+    ("dvgpu_fr_powers_device", ctypes.c_int, [_P, _P, _SZ, _P, _P] + _E),
+]
+
+
+def lib():
+    """Load libdvgpu.so.  Fails loudly when the CUDA library is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libdvgpu.so not built ({LIB_PATH}); run zkp-dynaverse_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(data):
+    """Pointer to a bytes / bytearray / numpy buffer (None for empty)."""
+    if data is None:
+        return None
+    if isinstance(data, np.ndarray):
+        return data.ctypes.data if data.size else None
+    if isinstance(data, (bytes, bytearray, memoryview)):
+        if len(data) == 0:
+            return None
+        arr = np.frombuffer(data, dtype=np.uint8)
+        return arr.ctypes.data
+    raise TypeError(f"unsupported buffer type {type(data)}")
+
+
+def _as_bytes(data):
+    if isinstance(data, np.ndarray):
+        return data.tobytes()
+    return bytes(data)
+
+
+def encode_fr(v: int) -> bytes:
+    if not 0 <= v < R_MODULUS:
+        raise ValueError("scalar out of range")
+    return v.to_bytes(32, "little")
+
+
+def decode_fr(b: bytes) -> int:
+    """Rejects non-canonical encodings (crates/gpu/src/codec.rs:43-49)."""
+    if len(b) != FR_BYTES:
+        raise ValueError("scalar must be exactly 32 bytes")
+    v = int.from_bytes(b, "little")
+    if v >= R_MODULUS:
+        raise ValueError("non-canonical or invalid scalar bytes")
+    return v
+
+
+class DvgpuBackend:
+    """One native owner (crates/gpu/src/icicle.rs:98-110 IcicleBackend).
+
+    Not thread-safe: one backend per caller thread, as in the reference."""
+
+    def __init__(self, large_bucket_factor=0):
+        self._L = lib()
+        self._err = ctypes.create_string_buffer(512)
+        h = ctypes.c_void_p()
+        rc = self._L.dvgpu_backend_create_with_large_bucket_factor(large_bucket_factor, ctypes.byref(h),
+                                                                    self._err, len(self._err))
+        self._check(rc)
+        if not h.value:
+            raise DvgpuError(-3, "native backend returned a null owner")
+        self.handle = h
+        self.large_bucket_factor = large_bucket_factor
+
+    # ------------------------------------------------------------------ plumbing
+    def _check(self, rc):
+        if rc != 0:
+            raise DvgpuError(rc, self._err.value.decode(errors="replace"))
+
+    def _call(self, name, *args):
+        rc = getattr(self._L, name)(self.handle, *args, self._err, len(self._err))
+        self._check(rc)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._L.dvgpu_backend_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------ info
+    def device_identity(self) -> str:
+        out = ctypes.create_string_buffer(320)
+        self._call("dvgpu_backend_device_identity", out, len(out))
+        return out.value.decode()
+
+    def memory_info(self):
+        info = MemoryInfo()
+        self._call("dvgpu_backend_memory_info", ctypes.byref(info))
+        return info.free_bytes, info.total_bytes
+
+    def batch_stats(self) -> BatchStats:
+        s = BatchStats()
+        rc = self._L.dvgpu_backend_batch_stats(self.handle, ctypes.byref(s))
+        if rc != 0:
+            raise DvgpuError(rc, "invalid native batch stats owner")
+        return s
+
+    def gpu_capabilities(self):
+        return {"g1_msm": True, "fr_ntt": True, "g2_msm": True}
+
+    # ------------------------------------------------------------------ MSM
+    def msm(self, points: bytes, scalars: bytes) -> bytes:
+        """G1 sum s_i P_i -> 64-byte affine (types.rs:295-299)."""
+        n = len(scalars) // FR_BYTES
+        if len(points) != n * G1_BYTES or len(scalars) != n * FR_BYTES:
+            raise ValueError("MSM length mismatch")
+        out = ctypes.create_string_buffer(G1_BYTES)
+        self._call("dvgpu_bn254_msm", _ptr(points), _ptr(scalars), n, out)
+        return out.raw
+
+    def msm_g2_host(self, points: bytes, scalars: bytes) -> bytes:
+        """G2 sum s_i Q_i -> 128-byte affine (types.rs:351-356)."""
+        n = len(scalars) // FR_BYTES
+        if len(points) != n * G2_BYTES or len(scalars) != n * FR_BYTES:
+            raise ValueError("G2 MSM length mismatch")
+        out = ctypes.create_string_buffer(G2_BYTES)
+        self._call("dvgpu_bn254_g2_msm", _ptr(points), _ptr(scalars), n, out)
+        return out.raw
+
+    def msm_batch(self, point_sets, shared_scalars: bytes, offsets, lengths):
+        """BatchMsmRequest (types.rs:254-259): set i uses point_sets[i][:lengths[i]]
+        against shared_scalars[offsets[i] : offsets[i] + lengths[i]].  Uneven
+        sets run in one native launch sequence, without padding."""
+        count = len(point_sets)
+        if len(offsets) != count or len(lengths) != count:
+            raise ValueError("batch shape mismatch")
+        n_sc = len(shared_scalars) // FR_BYTES
+        pts, scs, set_off = [], [], [0]
+        for i in range(count):
+            L = lengths[i]
+            if offsets[i] + L > n_sc:
+                raise ValueError("scalar range out of bounds")
+            if L * G1_BYTES > len(point_sets[i]):
+                raise ValueError("point range out of bounds")
+            pts.append(bytes(point_sets[i][:L * G1_BYTES]))
+            scs.append(bytes(shared_scalars[offsets[i] * FR_BYTES:(offsets[i] + L) * FR_BYTES]))
+            set_off.append(set_off[-1] + L)
+        return self.msm_batch_uneven(b"".join(pts), b"".join(scs), set_off)
+
+    def msm_batch_uneven(self, points: bytes, scalars: bytes, set_offsets):
+        count = len(set_offsets) - 1
+        if count <= 0:
+            return []
+        offs = np.ascontiguousarray(np.asarray(set_offsets, dtype=np.uint64))
+        if len(points) != int(offs[-1]) * G1_BYTES or len(scalars) != int(offs[-1]) * FR_BYTES:
+            raise ValueError("batch buffer length mismatch")
+        out = ctypes.create_string_buffer(count * G1_BYTES)
+        self._call("dvgpu_bn254_msm_batch_uneven", _ptr(points), _ptr(scalars), offs.ctypes.data, count, out)
+        raw = out.raw
+        return [raw[i * G1_BYTES:(i + 1) * G1_BYTES] for i in range(count)]
+
+    def msm_batch_padded(self, points: bytes, scalars: bytes, length: int, count: int):
+        """The reference's native padded batch (dvgpu_bn254_msm_batch)."""
+        out = ctypes.create_string_buffer(count * G1_BYTES)
+        self._call("dvgpu_bn254_msm_batch", _ptr(points), _ptr(scalars), length, count, out)
+        raw = out.raw
+        return [raw[i * G1_BYTES:(i + 1) * G1_BYTES] for i in range(count)]
+
+    def msm_sparse_batch(self, requests):
+        """SparseMsmRequest list (types.rs:262-345): each request is
+        (bases: bytes, entries: [(index, scalar_bytes)]).  Every index is
+        validated before any dispatch; results in request order."""
+        lengths = []
+        pts, scs, set_off = [], [], [0]
+        for bases, entries in requests:
+            nb = len(bases) // G1_BYTES
+            for idx, _ in entries:
+                if not 0 <= idx < nb:
+                    raise ValueError("sparse MSM index out of range")
+            for idx, val in entries:
+                pts.append(bases[idx * G1_BYTES:(idx + 1) * G1_BYTES])
+                scs.append(bytes(val))
+            lengths.append(len(entries))
+            set_off.append(set_off[-1] + len(entries))
+        if not requests:
+            return []
+        return self.msm_batch_uneven(b"".join(pts), b"".join(scs), set_off)
+
+    # resident bases + sparse-index MSM over them (no host gather)
+    def register_bases(self, points: bytes, g2=False) -> int:
+        size = G2_BYTES if g2 else G1_BYTES
+        h = ctypes.c_uint64()
+        self._call("dvgpu_bases_register", _ptr(points), len(points) // size, int(g2), ctypes.byref(h))
+        return h.value
+
+    def release_bases(self, handle: int):
+        self._L.dvgpu_bases_release(self.handle, handle)
+
+    def sparse_msm_resident(self, handle: int, indices, values: bytes, request_offsets):
+        idx = np.ascontiguousarray(np.asarray(indices, dtype=np.uint64))
+        offs = np.ascontiguousarray(np.asarray(request_offsets, dtype=np.uint64))
+        count = len(offs) - 1
+        out = ctypes.create_string_buffer(max(1, count) * G1_BYTES)
+        self._call("dvgpu_bn254_msm_sparse_batch", handle, idx.ctypes.data if idx.size else None,
+                   _ptr(values), offs.ctypes.data, count, out)
+        raw = out.raw
+        return [raw[i * G1_BYTES:(i + 1) * G1_BYTES] for i in range(count)]
+
+    def set_window(self, c: int):
+        if self._L.dvgpu_msm_set_window(self.handle, c) != 0:
+            raise DvgpuError(-1, "invalid window width")
+
+    def window_for(self, points_per_set: int) -> int:
+        c = ctypes.c_int()
+        self._L.dvgpu_msm_get_window(self.handle, points_per_set, ctypes.byref(c))
+        return c.value
+
+    # ------------------------------------------------------------------ NTT
+    def ntt(self, values: bytes, inverse: bool) -> bytes:
+        """Natural-order Fr transform, inverse includes 1/n (types.rs:347)."""
+        n = len(values) // FR_BYTES
+        if n == 0 or n & (n - 1) or len(values) != n * FR_BYTES:
+            raise ValueError(f"ntt size {n} is not a power of two")
+        out = ctypes.create_string_buffer(n * FR_BYTES)
+        self._call("dvgpu_bn254_ntt_ex", _ptr(values), n, int(bool(inverse)), out)
+        return out.raw
+
+    def ntt_with_root(self, values: bytes, inverse: bool, root: bytes) -> bytes:
+        """The reference ABI form with the explicit 2^20 root (icicle.rs:440-446)."""
+        n = len(values) // FR_BYTES
+        out = ctypes.create_string_buffer(max(1, n) * FR_BYTES)
+        self._call("dvgpu_bn254_ntt", _ptr(values), n, int(bool(inverse)), root, out)
+        return out.raw[:n * FR_BYTES]
+
+    def ntt_coset(self, values: bytes, inverse: bool) -> bytes:
+        n = len(values) // FR_BYTES
+        if n == 0 or n & (n - 1):
+            raise ValueError(f"ntt size {n} is not a power of two")
+        out = ctypes.create_string_buffer(n * FR_BYTES)
+        self._call("dvgpu_bn254_ntt_ex", _ptr(values), n, NTT_COSET_INVERSE if inverse else NTT_COSET_FORWARD, out)
+        return out.raw
+
+    # ------------------------------------------------------------------ fixed base
+    def fixed_base_g1(self, scalars: bytes) -> bytes:
+        n = len(scalars) // FR_BYTES
+        out = ctypes.create_string_buffer(max(1, n) * G1_BYTES)
+        self._call("dvgpu_bn254_fixed_base", _ptr(scalars), n, 0, out)
+        return out.raw[:n * G1_BYTES]
+
+    def fixed_base_g2(self, scalars: bytes) -> bytes:
+        n = len(scalars) // FR_BYTES
+        out = ctypes.create_string_buffer(max(1, n) * G2_BYTES)
+        self._call("dvgpu_bn254_fixed_base", _ptr(scalars), n, 1, out)
+        return out.raw[:n * G2_BYTES]
+
+    def setup_stats(self) -> SetupStats:
+        s = SetupStats()
+        self._L.dvgpu_setup_stats(self.handle, ctypes.byref(s))
+        return s
+
+    # ------------------------------------------------------------------ G2 validation
+    def inspect_g2_validation(self, wire: bytes, algorithm: int):
+        """Status-only batched inspector (g2_validation.rs:124-135,191-203)."""
+        if len(wire) % G2_BYTES or algorithm not in (1, 2, 3):
+            raise ValueError("invalid G2 validation input")
+        n = len(wire) // G2_BYTES
+        masks = np.zeros(max(1, n), dtype=np.uint32)
+        rep = G2ValidationReport()
+        self._call("dvgpu_bn254_g2_validation_inspect", _ptr(wire), n, algorithm, masks.ctypes.data,
+                   ctypes.byref(rep))
+        return masks[:n], rep
+
+    def fixed_base_g2_checked(self, scalars: bytes, algorithm: int):
+        n = len(scalars) // FR_BYTES
+        out = ctypes.create_string_buffer(max(1, n) * G2_BYTES)
+        rep = G2ValidationReport()
+        self._call("dvgpu_bn254_fixed_base_g2_checked", _ptr(scalars), n, algorithm, out, ctypes.byref(rep))
+        return out.raw[:n * G2_BYTES], rep
+
+    # ------------------------------------------------------------------ device forms
+    def msm_device(self, d_points: int, d_scalars: int, n: int, g2=False, stream=None) -> bytes:
+        out = ctypes.create_string_buffer(G2_BYTES if g2 else G1_BYTES)
+        self._call("dvgpu_bn254_msm_device", d_points, d_scalars, n, int(g2), out, stream)
+        return out.raw
+
+    def msm_resident(self, handle: int, d_scalars: int, n: int, stream=None, g2=False) -> bytes:
+        out = ctypes.create_string_buffer(G2_BYTES if g2 else G1_BYTES)
+        self._call("dvgpu_bn254_msm_resident", handle, d_scalars, n, out, stream)
+        return out.raw
+
+    def ntt_device(self, d_values: int, n: int, kind: int, d_out: int, stream=None):
+        self._call("dvgpu_bn254_ntt_device", d_values, n, kind, d_out, stream)
+
+    def fixed_base_device(self, d_scalars: int, n: int, g2: bool, d_out: int, stream=None):
+        self._call("dvgpu_bn254_fixed_base_device", d_scalars, n, int(g2), d_out, stream)
+
+    def g2_check_device(self, d_wire: int, n: int, algorithm: int, d_masks: int, stream=None):
+        rep = G2ValidationReport()
+        self._call("dvgpu_bn254_g2_check_device", d_wire, n, algorithm, d_masks, ctypes.byref(rep), stream)
+        return rep
+
+    def launch_count(self) -> int:
+        return int(self._L.dvgpu_launch_count())
+
+    def msm_timeline(self, enable: bool) -> MsmPhaseTimes:
+        t = MsmPhaseTimes()
+        if self._L.dvgpu_msm_timeline(self.handle, int(enable), ctypes.byref(t)) != 0:
+            raise DvgpuError(-1, "timeline unavailable")
+        return t
+
+    def random_fr_device(self, seed: int, n: int, d_out: int, stream=None):
+        self._call("dvgpu_random_fr_device", seed, n, d_out, stream)
+
+    def fr_powers_device(self, d_tau: int, n: int, d_out: int, stream=None):
+        self._call("dvgpu_fr_powers_device", d_tau, n, d_out, stream)
+
+    def probe_imad_rate(self) -> float:
+        v = ctypes.c_double()
+        self._call("dvgpu_probe_imad_rate", ctypes.byref(v))
+        return v.value

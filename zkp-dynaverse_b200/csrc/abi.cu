@@ -1,0 +1,818 @@
+// extern "C" entry points of libdvgpu (declared in include/dynaverse_gpu.h).
+//
+// Status discipline follows native/src/icicle_msm.cu:38-45,188-238,424-432:
+// invalid arguments return -1 and leave the owner healthy; CUDA failures
+// retire the owner (-2/-3), later calls return -4; outputs are written only
+// on success; C++ exceptions never cross the ABI.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "backend.hpp"
+#include "g2.cuh"
+#include "host_curve.hpp"
+
+using namespace dv;
+
+namespace {
+
+int fail(int status, const std::string& msg, char* error, size_t cap) {
+    if (error && cap) {
+        const size_t n = std::min(cap - 1, msg.size());
+        memcpy(error, msg.data(), n);
+        error[n] = '\0';
+    }
+    return status;
+}
+
+template <class Fn>
+int guarded(void* opaque, char* error, size_t cap, Fn&& fn) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b) return fail(-1, "null backend", error, cap);
+    if (b->retired) return fail(-4, "backend retired after an error; create a new backend", error, cap);
+    try {
+        DV_CUDA(cudaSetDevice(b->device));
+        fn(*b);
+        return 0;
+    } catch (const InvalidArgument& e) {
+        return fail(-1, e.what(), error, cap);
+    } catch (const std::exception& e) {
+        b->retired = true;
+        b->release_all();
+        return fail(-2, e.what(), error, cap);
+    } catch (...) {
+        b->retired = true;
+        b->release_all();
+        return fail(-3, "unknown native exception", error, cap);
+    }
+}
+
+inline cudaStream_t pick(Backend& b, void* s) { return s ? static_cast<cudaStream_t>(s) : b.stream; }
+
+void require(bool ok, const char* msg) {
+    if (!ok) throw InvalidArgument(msg);
+}
+
+uint32_t read_err_word(Backend& b, uint32_t* d_word, cudaStream_t st) {
+    uint32_t* h = b.pin_err.as<uint32_t>(1);
+    DV_CUDA(cudaMemcpyAsync(h, d_word, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaStreamSynchronize(st));
+    return *h;
+}
+
+// MSM over canonical device points/scalars, count sets (offsets host u32).
+template <class F>
+void msm_sets_device(Backend& b, const uint8_t* d_points, const uint8_t* d_scalars, const std::vector<uint32_t>& offs,
+                     uint8_t* result, cudaStream_t st) {
+    const uint32_t count = (uint32_t)offs.size() - 1;
+    const uint64_t n = offs[count];
+    const size_t psize = 2 * sizeof(F);
+    std::vector<uint8_t> tmp((size_t)count * psize);
+    if (n == 0) {
+        memset(result, 0, tmp.size());
+        return;
+    }
+    Affine<F>* conv = b.conv_points.as<Affine<F>>(n);
+    uint32_t* bad = b.err.as<uint32_t>(1);
+    DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
+    convert_points<F>(d_points, conv, n, bad, st);
+    msm_run<F>(b.msm, conv, reinterpret_cast<const uint32_t*>(d_scalars), offs.data(), count, b.force_c, st,
+               tmp.data(), &b.msm_stats);
+    const uint32_t first_bad = read_err_word(b, bad, st);
+    if (first_bad != 0xffffffffu) throw InvalidArgument("invalid point at index " + std::to_string(first_bad));
+    memcpy(result, tmp.data(), tmp.size());
+}
+
+template <class F>
+void msm_sets_host(Backend& b, const uint8_t* points, const uint8_t* scalars, const std::vector<uint32_t>& offs,
+                   uint8_t* result) {
+    const uint64_t n = offs.back();
+    const size_t psize = 2 * sizeof(F);
+    if (n == 0) {
+        memset(result, 0, (offs.size() - 1) * psize);
+        return;
+    }
+    uint8_t* d_pts = b.in_points.as<uint8_t>(n * psize);
+    uint8_t* d_sc = b.in_scalars.as<uint8_t>(n * 32);
+    DV_CUDA(cudaMemcpyAsync(d_pts, points, n * psize, cudaMemcpyHostToDevice, b.stream));
+    DV_CUDA(cudaMemcpyAsync(d_sc, scalars, n * 32, cudaMemcpyHostToDevice, b.stream));
+    msm_sets_device<F>(b, d_pts, d_sc, offs, result, b.stream);
+}
+
+std::vector<uint32_t> single_set(size_t n) { return {0u, (uint32_t)n}; }
+
+// ---- host Fr check of the reference's explicit NTT root -----------------
+const uint64_t FR_P[4] = {0x43e1f593f0000001ull, 0x2833e84879b97091ull, 0xb85045b68181585dull, 0x30644e72e131a029ull};
+const uint64_t FR_INV64 = 0xc2e1f593efffffffull;  // -r^{-1} mod 2^64
+const uint64_t FR_R2[4] = {0x1bb8e645ae216da7ull, 0x53fe3ab1e35c59e3ull, 0x8c49833d53bb8085ull, 0x0216d0b17f4e44a5ull};
+
+void fr_mul(uint64_t* out, const uint64_t* a, const uint64_t* b) {
+    typedef unsigned __int128 u128;
+    uint64_t t[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < 4; ++i) {
+        u128 c = 0;
+        for (int j = 0; j < 4; ++j) {
+            c += (u128)a[j] * b[i] + t[j];
+            t[j] = (uint64_t)c;
+            c >>= 64;
+        }
+        c += t[4];
+        t[4] = (uint64_t)c;
+        t[5] = (uint64_t)(c >> 64);
+        const uint64_t m = t[0] * FR_INV64;
+        c = ((u128)m * FR_P[0] + t[0]) >> 64;
+        for (int j = 1; j < 4; ++j) {
+            c += (u128)m * FR_P[j] + t[j];
+            t[j - 1] = (uint64_t)c;
+            c >>= 64;
+        }
+        c += t[4];
+        t[3] = (uint64_t)c;
+        t[4] = t[5] + (uint64_t)(c >> 64);
+    }
+    uint64_t r[4] = {t[0], t[1], t[2], t[3]};
+    bool ge = t[4] != 0;
+    if (!ge) {
+        ge = true;
+        for (int i = 3; i >= 0; --i)
+            if (r[i] != FR_P[i]) { ge = r[i] > FR_P[i]; break; }
+    }
+    if (ge) {
+        unsigned __int128 br = 0;
+        for (int i = 0; i < 4; ++i) {
+            unsigned __int128 d = (unsigned __int128)r[i] - FR_P[i] - (uint64_t)br;
+            r[i] = (uint64_t)d;
+            br = (d >> 64) & 1;
+        }
+    }
+    memcpy(out, r, 32);
+}
+
+// root (canonical bytes) has multiplicative order exactly 2^20.
+bool root_has_order_2_20(const uint8_t* root) {
+    uint64_t c[4];
+    for (int i = 0; i < 4; ++i) {
+        uint64_t w = 0;
+        for (int k = 7; k >= 0; --k) w = (w << 8) | root[8 * i + k];
+        c[i] = w;
+    }
+    for (int i = 3; i >= 0; --i) {
+        if (c[i] < FR_P[i]) break;
+        if (c[i] > FR_P[i] || i == 0) return false;
+    }
+    uint64_t x[4], one_m[4], one_raw[4] = {1, 0, 0, 0};
+    fr_mul(x, c, FR_R2);          // Montgomery form
+    fr_mul(one_m, one_raw, FR_R2);  // R mod r
+    for (int i = 0; i < 19; ++i) fr_mul(x, x, x);
+    const bool half_is_one = !memcmp(x, one_m, 32);
+    fr_mul(x, x, x);
+    return !half_is_one && !memcmp(x, one_m, 32);
+}
+
+// The arkworks root of order 2^20 (TWO_ADIC_ROOT_OF_UNITY squared 8 times).
+bool is_default_root20(const uint8_t* root) {
+    static uint8_t expect[32];
+    static bool init = false;
+    if (!init) {
+        const uint64_t r28[4] = {0x9bd61b6e725b19f0ull, 0x402d111e41112ed4ull, 0x00e0a7eb8ef62abcull,
+                                 0x2a3c09f0a58a7e85ull};
+        uint64_t x[4], one_raw[4] = {1, 0, 0, 0};
+        fr_mul(x, r28, FR_R2);
+        for (int i = 0; i < 8; ++i) fr_mul(x, x, x);
+        fr_mul(x, x, one_raw);
+        for (int i = 0; i < 4; ++i)
+            for (int k = 0; k < 8; ++k) expect[8 * i + k] = (uint8_t)(x[i] >> (8 * k));
+        init = true;
+    }
+    return !memcmp(root, expect, 32);
+}
+
+// IMAD roofline probe kernels: 16 independent accumulator rows per thread.
+__global__ void k_probe_madc(uint32_t seed, uint32_t iters, uint32_t* sink) {
+    uint32_t a0 = seed ^ threadIdx.x, a1 = a0 * 3u, a2 = a0 * 5u, a3 = a0 * 7u;
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0, t8 = 0;
+    const uint32_t b = seed * 0x9e3779b9u + blockIdx.x;
+    for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            asm volatile(
+                "mad.lo.cc.u32 %0, %9, %13, %0;\n\t"
+                "madc.hi.cc.u32 %1, %9, %13, %1;\n\t"
+                "madc.lo.cc.u32 %2, %10, %13, %2;\n\t"
+                "madc.hi.cc.u32 %3, %10, %13, %3;\n\t"
+                "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"
+                "madc.hi.cc.u32 %5, %11, %13, %5;\n\t"
+                "madc.lo.cc.u32 %6, %12, %13, %6;\n\t"
+                "madc.hi.cc.u32 %7, %12, %13, %7;\n\t"
+                "addc.u32 %8, %8, 0;"
+                : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)
+                : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b + r));
+        }
+    }
+    if ((t0 ^ t1 ^ t2 ^ t3 ^ t4 ^ t5 ^ t6 ^ t7 ^ t8) == 0x12345678u) sink[0] = 1;
+}
+
+}  // namespace
+
+void Backend::release_all() noexcept {
+    bases.clear();
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+        stream = nullptr;
+    }
+}
+
+// ============================================================ lifecycle
+extern "C" int dvgpu_backend_create_with_large_bucket_factor(uint32_t factor, void** output, char* error,
+                                                             size_t cap) {
+    if (!output) return fail(-1, "null backend output", error, cap);
+    *output = nullptr;
+    if (factor > DVGPU_MAX_LARGE_BUCKET_FACTOR)
+        return fail(-1, "large bucket factor must be within 0..=100", error, cap);
+    try {
+        int count = 0;
+        DV_CUDA(cudaGetDeviceCount(&count));
+        if (!count) throw CudaFailure("no visible CUDA device");
+        auto b = std::make_unique<Backend>();
+        // The calling thread's current device: visible device 0 unless the
+        // caller selected another (one owner per GPU, e.g. one per rank).
+        int dev = 0;
+        DV_CUDA(cudaGetDevice(&dev));
+        b->device = dev;
+        b->large_bucket_factor = factor;
+        DV_CUDA(cudaSetDevice(dev));
+        cudaDeviceProp p{};
+        DV_CUDA(cudaGetDeviceProperties(&p, dev));
+        b->identity = std::string(p.name) + "/sm_" + std::to_string(p.major) + std::to_string(p.minor);
+        DV_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        *output = b.release();
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(-2, e.what(), error, cap);
+    } catch (...) {
+        return fail(-3, "unknown native exception", error, cap);
+    }
+}
+
+extern "C" int dvgpu_backend_create(void** output, char* error, size_t cap) {
+    return dvgpu_backend_create_with_large_bucket_factor(0, output, error, cap);
+}
+
+extern "C" void dvgpu_backend_destroy(void* backend) {
+    auto* b = static_cast<Backend*>(backend);
+    if (!b) return;
+    cudaSetDevice(b->device);
+    delete b;
+}
+
+extern "C" int dvgpu_backend_device_identity(void* opaque, char* output, size_t output_capacity, char* error,
+                                             size_t cap) {
+    const auto* b = static_cast<const Backend*>(opaque);
+    if (!b || !output || output_capacity <= b->identity.size())
+        return fail(-1, "invalid device identity output", error, cap);
+    memcpy(output, b->identity.c_str(), b->identity.size() + 1);
+    return 0;
+}
+
+extern "C" int dvgpu_backend_memory_info(void* opaque, DvgpuMemoryInfo* info, char* error, size_t cap) {
+    if (!info) return fail(-1, "null memory info output", error, cap);
+    return guarded(opaque, error, cap, [&](Backend&) {
+        size_t f = 0, t = 0;
+        DV_CUDA(cudaMemGetInfo(&f, &t));
+        *info = {(uint64_t)f, (uint64_t)t};
+    });
+}
+
+extern "C" int dvgpu_backend_batch_stats(void* opaque, DvgpuBatchStats* stats) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || !stats) return -1;
+    *stats = b->batch_stats;
+    return 0;
+}
+
+// ============================================================ MSM
+extern "C" int dvgpu_bn254_msm(void* opaque, const uint8_t* points, const uint8_t* scalars, size_t length,
+                               uint8_t* result, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(result && length <= DVGPU_MAX_MSM_SIZE && (!length || (points && scalars)),
+                "invalid MSM buffers or length");
+        msm_sets_host<Fq>(b, points, scalars, single_set(length), result);
+    });
+}
+
+extern "C" int dvgpu_bn254_msm_profiled(void* opaque, const uint8_t* points, const uint8_t* scalars, size_t length,
+                                        uint8_t* result, DvgpuMsmTimings* timings, char* error, size_t cap) {
+    if (!timings) return fail(-1, "null diagnostic timings", error, cap);
+    *timings = {};
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(result && length <= DVGPU_MAX_MSM_SIZE && (!length || (points && scalars)),
+                "invalid MSM buffers or length");
+        const auto t0 = std::chrono::steady_clock::now();
+        msm_sets_host<Fq>(b, points, scalars, single_set(length), result);
+        timings->icicle_ns = (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                 std::chrono::steady_clock::now() - t0)
+                                 .count();
+    });
+}
+
+extern "C" int dvgpu_bn254_g2_msm(void* opaque, const uint8_t* points, const uint8_t* scalars, size_t length,
+                                  uint8_t* result, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(result && length <= DVGPU_MAX_MSM_SIZE && (!length || (points && scalars)),
+                "invalid G2 MSM buffers or length");
+        msm_sets_host<Fq2>(b, points, scalars, single_set(length), result);
+    });
+}
+
+extern "C" int dvgpu_bn254_msm_batch(void* opaque, const uint8_t* points, const uint8_t* scalars, size_t length,
+                                     size_t count, uint8_t* results, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(points && scalars && results && length && count && count <= DVGPU_MAX_MSM_BATCH_SIZE &&
+                    length <= DVGPU_MAX_MSM_SIZE / count,
+                "invalid batch buffers or bounded work size");
+        std::vector<uint32_t> offs(count + 1);
+        for (size_t k = 0; k <= count; ++k) offs[k] = (uint32_t)(k * length);
+        b.batch_stats.icicle_calls++;
+        b.batch_stats.max_batch_size = std::max<uint64_t>(b.batch_stats.max_batch_size, count);
+        const size_t before = b.in_points.cap;
+        msm_sets_host<Fq>(b, points, scalars, offs, results);
+        if (b.in_points.cap != before) b.batch_stats.buffer_grows++;
+        b.batch_stats.input_capacity = b.in_points.cap / 64;
+    });
+}
+
+extern "C" int dvgpu_reserve_batch(void* opaque, size_t points, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(points <= DVGPU_MAX_MSM_SIZE, "invalid batch reserve capacity");
+        const size_t before = b.in_points.cap;
+        b.in_points.get(points * 64);
+        b.in_scalars.get(points * 32);
+        if (b.in_points.cap != before) b.batch_stats.buffer_grows++;
+        b.batch_stats.input_capacity = b.in_points.cap / 64;
+    });
+}
+
+extern "C" int dvgpu_bn254_msm_batch_uneven(void* opaque, const uint8_t* points, const uint8_t* scalars,
+                                            const uint64_t* set_offsets, size_t count, uint8_t* results,
+                                            char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(set_offsets && results && count <= DVGPU_MAX_MSM_BATCH_SIZE, "invalid uneven batch arguments");
+        std::vector<uint32_t> offs(count + 1);
+        require(set_offsets[0] == 0, "set offsets must start at 0");
+        for (size_t k = 0; k <= count; ++k) {
+            require(k == 0 || set_offsets[k] >= set_offsets[k - 1], "set offsets must be non-decreasing");
+            require(set_offsets[k] <= DVGPU_MAX_MSM_SIZE, "batch exceeds the MSM size bound");
+            offs[k] = (uint32_t)set_offsets[k];
+        }
+        require(!offs[count] || (points && scalars), "null point or scalar buffer");
+        b.batch_stats.icicle_calls++;
+        b.batch_stats.max_batch_size = std::max<uint64_t>(b.batch_stats.max_batch_size, count);
+        if (count) msm_sets_host<Fq>(b, points, scalars, offs, results);
+    });
+}
+
+extern "C" int dvgpu_bases_register(void* opaque, const uint8_t* points, size_t n, int g2, uint64_t* handle,
+                                    char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(handle && (g2 == 0 || g2 == 1) && n <= DVGPU_MAX_MSM_SIZE && (!n || points),
+                "invalid base registration");
+        auto rb = std::make_unique<ResidentBases>();
+        rb->n = n;
+        rb->g2 = g2;
+        const size_t psize = g2 ? 128 : 64;
+        if (n) {
+            uint8_t* d_canon = b.in_points.as<uint8_t>(n * psize);
+            DV_CUDA(cudaMemcpyAsync(d_canon, points, n * psize, cudaMemcpyHostToDevice, b.stream));
+            uint32_t* bad = b.err.as<uint32_t>(1);
+            DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), b.stream));
+            if (g2) convert_points<Fq2>(d_canon, rb->points.as<G2A>(n), n, bad, b.stream);
+            else convert_points<Fq>(d_canon, rb->points.as<G1A>(n), n, bad, b.stream);
+            const uint32_t first_bad = read_err_word(b, bad, b.stream);
+            if (first_bad != 0xffffffffu) throw InvalidArgument("invalid base at index " + std::to_string(first_bad));
+        }
+        *handle = b.next_handle++;
+        b.bases[*handle] = std::move(rb);
+    });
+}
+
+extern "C" int dvgpu_bases_release(void* opaque, uint64_t handle) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b) return -1;
+    return b->bases.erase(handle) ? 0 : -1;
+}
+
+extern "C" int dvgpu_bn254_msm_sparse_batch(void* opaque, uint64_t bases_handle, const uint64_t* indices,
+                                            const uint8_t* values, const uint64_t* request_offsets, size_t count,
+                                            uint8_t* results, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        auto it = b.bases.find(bases_handle);
+        require(it != b.bases.end() && !it->second->g2, "unknown G1 base handle");
+        require(request_offsets && results && count <= DVGPU_MAX_MSM_BATCH_SIZE && request_offsets[0] == 0,
+                "invalid sparse request arguments");
+        std::vector<uint32_t> offs(count + 1);
+        for (size_t k = 0; k <= count; ++k) {
+            require(k == 0 || request_offsets[k] >= request_offsets[k - 1], "request offsets must be non-decreasing");
+            require(request_offsets[k] <= DVGPU_MAX_MSM_SIZE, "sparse batch exceeds the MSM size bound");
+            offs[k] = (uint32_t)request_offsets[k];
+        }
+        const uint64_t k_total = offs[count];
+        require(!k_total || (indices && values), "null index or value buffer");
+        const ResidentBases& rb = *it->second;
+        for (uint64_t j = 0; j < k_total; ++j)
+            require(indices[j] < rb.n, "sparse MSM index out of range");
+        if (!count) return;
+        if (!k_total) {
+            memset(results, 0, count * 64);
+            return;
+        }
+        uint64_t* d_idx = b.idx.as<uint64_t>(k_total);
+        uint8_t* d_vals = b.in_scalars.as<uint8_t>(k_total * 32);
+        DV_CUDA(cudaMemcpyAsync(d_idx, indices, k_total * 8, cudaMemcpyHostToDevice, b.stream));
+        DV_CUDA(cudaMemcpyAsync(d_vals, values, k_total * 32, cudaMemcpyHostToDevice, b.stream));
+        G1A* gathered = b.conv_points.as<G1A>(k_total);
+        uint32_t* bad = b.err.as<uint32_t>(1);
+        DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), b.stream));
+        gather_points<Fq>(rb.points.view<G1A>(), rb.n, d_idx, k_total, gathered, bad, b.stream);
+        std::vector<uint8_t> tmp(count * 64);
+        msm_run<Fq>(b.msm, gathered, reinterpret_cast<const uint32_t*>(d_vals), offs.data(), (uint32_t)count,
+                    b.force_c, b.stream, tmp.data(), &b.msm_stats);
+        require(read_err_word(b, bad, b.stream) == 0xffffffffu, "sparse MSM index out of range");
+        b.batch_stats.icicle_calls++;
+        b.batch_stats.max_batch_size = std::max<uint64_t>(b.batch_stats.max_batch_size, count);
+        memcpy(results, tmp.data(), tmp.size());
+    });
+}
+
+extern "C" int dvgpu_bn254_msm_device(void* opaque, const uint8_t* d_points, const uint8_t* d_scalars, size_t length,
+                                      int g2, uint8_t* result_host, void* stream, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(result_host && (g2 == 0 || g2 == 1) && length <= DVGPU_MAX_MSM_SIZE &&
+                    (!length || (d_points && d_scalars)),
+                "invalid device MSM arguments");
+        if (g2) msm_sets_device<Fq2>(b, d_points, d_scalars, single_set(length), result_host, pick(b, stream));
+        else msm_sets_device<Fq>(b, d_points, d_scalars, single_set(length), result_host, pick(b, stream));
+    });
+}
+
+extern "C" int dvgpu_bn254_msm_resident(void* opaque, uint64_t bases_handle, const uint8_t* d_scalars, size_t length,
+                                        uint8_t* result_host, void* stream, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        auto it = b.bases.find(bases_handle);
+        require(it != b.bases.end(), "unknown base handle");
+        const ResidentBases& rb = *it->second;
+        require(result_host && length <= rb.n && (!length || d_scalars), "invalid resident MSM arguments");
+        const cudaStream_t st = pick(b, stream);
+        const auto offs = single_set(length);
+        if (!length) {
+            memset(result_host, 0, rb.g2 ? 128 : 64);
+            return;
+        }
+        if (rb.g2) {
+            uint8_t tmp[128];
+            msm_run<Fq2>(b.msm, rb.points.view<G2A>(), reinterpret_cast<const uint32_t*>(d_scalars), offs.data(), 1,
+                         b.force_c, st, tmp, &b.msm_stats);
+            memcpy(result_host, tmp, 128);
+        } else {
+            uint8_t tmp[64];
+            msm_run<Fq>(b.msm, rb.points.view<G1A>(), reinterpret_cast<const uint32_t*>(d_scalars), offs.data(), 1,
+                        b.force_c, st, tmp, &b.msm_stats);
+            memcpy(result_host, tmp, 64);
+        }
+    });
+}
+
+extern "C" int dvgpu_msm_set_window(void* opaque, int c) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || c < 0 || c == 1 || c > 20 || (c && c < 4)) return -1;
+    b->force_c = c;
+    return 0;
+}
+
+extern "C" int dvgpu_msm_get_window(void* opaque, size_t points, int* c) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || !c) return -1;
+    *c = msm_plan(points, b->force_c).c;
+    return 0;
+}
+
+// ============================================================ NTT
+namespace {
+void ntt_host(Backend& b, const uint8_t* values, size_t length, int kind, uint8_t* result) {
+    require(values && result && length && length <= DVGPU_MAX_NTT_SIZE && !(length & (length - 1)),
+            "invalid NTT buffers, direction or length");
+    int logn = 0;
+    while ((1ull << logn) < length) ++logn;
+    uint8_t* d = b.in_scalars.as<uint8_t>(length * 32);
+    DV_CUDA(cudaMemcpyAsync(d, values, length * 32, cudaMemcpyHostToDevice, b.stream));
+    uint8_t* d_out = b.out_buf.as<uint8_t>(length * 32);
+    ntt_run(b.ntt, d, d_out, logn, kind, b.stream);  // synchronises and checks
+    uint8_t* h = b.pin_out.as<uint8_t>(length * 32);
+    DV_CUDA(cudaMemcpyAsync(h, d_out, length * 32, cudaMemcpyDeviceToHost, b.stream));
+    DV_CUDA(cudaStreamSynchronize(b.stream));
+    memcpy(result, h, length * 32);
+}
+}  // namespace
+
+extern "C" int dvgpu_bn254_ntt(void* opaque, const uint8_t* values, size_t length, int inverse, const uint8_t* root,
+                               uint8_t* result, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(values && result && root && length && length <= DVGPU_MAX_NTT_SIZE && !(length & (length - 1)) &&
+                    (inverse == 0 || inverse == 1),
+                "invalid NTT buffers, direction or length");
+        require(root_has_order_2_20(root), "NTT root must have order 2^20");
+        // Orientation is pinned to the CPU reference's root; another root of
+        // the same order would define a different (conjugate) transform.
+        require(is_default_root20(root), "NTT root differs from the arkworks 2^20 root of unity");
+        ntt_host(b, values, length, inverse, result);
+    });
+}
+
+extern "C" int dvgpu_bn254_ntt_ex(void* opaque, const uint8_t* values, size_t length, int kind, uint8_t* result,
+                                  char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(kind >= 0 && kind <= 3, "invalid NTT kind");
+        ntt_host(b, values, length, kind, result);
+    });
+}
+
+extern "C" int dvgpu_bn254_ntt_device(void* opaque, const uint8_t* d_values, size_t length, int kind,
+                                      uint8_t* d_result, void* stream, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(d_values && d_result && length && length <= DVGPU_MAX_NTT_SIZE && !(length & (length - 1)) &&
+                    kind >= 0 && kind <= 3,
+                "invalid device NTT arguments");
+        int logn = 0;
+        while ((1ull << logn) < length) ++logn;
+        ntt_run(b.ntt, d_values, d_result, logn, kind, pick(b, stream));
+    });
+}
+
+// ============================================================ fixed base
+namespace {
+void fixed_base_device(Backend& b, const uint8_t* d_scalars, size_t n, int g2, uint8_t* d_out, cudaStream_t st) {
+    uint32_t* bad = b.err.as<uint32_t>(1);
+    DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
+    FixedBaseTables& t = b.fixed_base;
+    const bool had = g2 ? t.g2_ready : t.g1_ready;
+    fixed_base_launch(t, d_scalars, n, g2, d_out, bad, st);
+    if (!had) {
+        b.setup_stats.table_builds[g2]++;
+        b.setup_stats.table_bytes += 64 * 16 * (g2 ? 128 : 64);
+    }
+    const uint32_t first_bad = read_err_word(b, bad, st);
+    if (first_bad != 0xffffffffu) throw InvalidArgument("non-canonical scalar at index " + std::to_string(first_bad));
+    b.setup_stats.calls[g2]++;
+    b.setup_stats.points[g2] += n;
+}
+}  // namespace
+
+extern "C" int dvgpu_bn254_fixed_base(void* opaque, const uint8_t* scalars, size_t length, int g2, uint8_t* output,
+                                      char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(length <= DVGPU_MAX_SETUP_SIZE && (g2 == 0 || g2 == 1) && (!length || (scalars && output)),
+                "invalid fixed-base buffers or chunk length");
+        if (!length) return;
+        const size_t psize = g2 ? 128 : 64;
+        const auto t0 = std::chrono::steady_clock::now();
+        uint8_t* d_sc = b.in_scalars.as<uint8_t>(length * 32);
+        uint8_t* d_out = b.out_buf.as<uint8_t>(length * psize);
+        DV_CUDA(cudaMemcpyAsync(d_sc, scalars, length * 32, cudaMemcpyHostToDevice, b.stream));
+        fixed_base_device(b, d_sc, length, g2, d_out, b.stream);
+        uint8_t* h = b.pin_out.as<uint8_t>(length * psize);
+        DV_CUDA(cudaMemcpyAsync(h, d_out, length * psize, cudaMemcpyDeviceToHost, b.stream));
+        DV_CUDA(cudaStreamSynchronize(b.stream));
+        memcpy(output, h, length * psize);
+        b.setup_stats.native_wall_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                            std::chrono::steady_clock::now() - t0)
+                                            .count();
+        if (g2) {
+            b.g2_traffic.scalar_h2d_bytes += length * 32;
+            b.g2_traffic.point_d2h_bytes += length * 128;
+        }
+    });
+}
+
+extern "C" int dvgpu_bn254_fixed_base_device(void* opaque, const uint8_t* d_scalars, size_t length, int g2,
+                                             uint8_t* d_output, void* stream, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(length <= DVGPU_MAX_SETUP_SIZE && (g2 == 0 || g2 == 1) && (!length || (d_scalars && d_output)),
+                "invalid device fixed-base arguments");
+        if (length) fixed_base_device(b, d_scalars, length, g2, d_output, pick(b, stream));
+    });
+}
+
+extern "C" int dvgpu_setup_mode(void* opaque, int mode) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || b->retired || mode < 0 || mode > 2) return -1;
+    b->setup_mode = mode;
+    return 0;
+}
+
+extern "C" int dvgpu_setup_stats(void* opaque, DvgpuSetupStats* stats) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || !stats) return -1;
+    *stats = b->setup_stats;
+    return 0;
+}
+
+// ============================================================ G2 validation
+namespace {
+DvgpuG2ValidationReport g2_check_device(Backend& b, const uint8_t* d_wire, size_t n, uint32_t algorithm,
+                                        uint32_t* d_masks, cudaStream_t st) {
+    G2CheckAccum* acc = b.aux.as<G2CheckAccum>(1);
+    const G2CheckAccum init = {0ull, ~0ull, 0u, 0u};
+    G2CheckAccum* h = b.pin_out.as<G2CheckAccum>(1);
+    *h = init;
+    DV_CUDA(cudaMemcpyAsync(acc, h, sizeof(init), cudaMemcpyHostToDevice, st));
+    g2_check_launch(d_wire, n, algorithm, d_masks, acc, st);
+    DV_CUDA(cudaMemcpyAsync(h, acc, sizeof(init), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaStreamSynchronize(st));
+    DvgpuG2ValidationReport r;
+    r.checked_points = n;
+    r.invalid_points = h->invalid;
+    r.first_invalid = h->invalid ? h->first : UINT64_MAX;
+    r.failure_mask = h->mask;
+    r.algorithm = algorithm;
+    b.g2_stats.checked_points += n;
+    return r;
+}
+}  // namespace
+
+extern "C" int dvgpu_bn254_g2_validation_inspect(void* opaque, const uint8_t* wire, size_t n, uint32_t algorithm,
+                                                 uint32_t* masks, DvgpuG2ValidationReport* report, char* error,
+                                                 size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(n <= DVGPU_MAX_SETUP_SIZE && algorithm >= 1 && algorithm <= 3 && report && (!n || (wire && masks)),
+                "invalid G2 validation buffers, algorithm or chunk length");
+        if (!n) {
+            *report = {0, 0, UINT64_MAX, 0, algorithm};
+            return;
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        uint8_t* d_wire = b.in_points.as<uint8_t>(n * 128);
+        uint32_t* d_masks = b.out_buf.as<uint32_t>(n);
+        DV_CUDA(cudaMemcpyAsync(d_wire, wire, n * 128, cudaMemcpyHostToDevice, b.stream));
+        const DvgpuG2ValidationReport r = g2_check_device(b, d_wire, n, algorithm, d_masks, b.stream);
+        std::vector<uint32_t> tmp(n);
+        DV_CUDA(cudaMemcpyAsync(tmp.data(), d_masks, n * 4, cudaMemcpyDeviceToHost, b.stream));
+        DV_CUDA(cudaStreamSynchronize(b.stream));
+        memcpy(masks, tmp.data(), n * 4);
+        *report = r;
+        b.g2_traffic.point_h2d_bytes += n * 128;
+        b.g2_traffic.status_d2h_bytes += n * 4 + sizeof(r);
+        b.g2_stats.native_wall_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                         std::chrono::steady_clock::now() - t0)
+                                         .count();
+    });
+}
+
+extern "C" int dvgpu_bn254_g2_check_device(void* opaque, const uint8_t* d_wire, size_t n, uint32_t algorithm,
+                                           uint32_t* d_masks, DvgpuG2ValidationReport* report_host, void* stream,
+                                           char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(n <= DVGPU_MAX_SETUP_SIZE && algorithm >= 1 && algorithm <= 3 && report_host &&
+                    (!n || (d_wire && d_masks)),
+                "invalid device G2 check arguments");
+        if (!n) {
+            *report_host = {0, 0, UINT64_MAX, 0, algorithm};
+            return;
+        }
+        *report_host = g2_check_device(b, d_wire, n, algorithm, d_masks, pick(b, stream));
+    });
+}
+
+extern "C" int dvgpu_bn254_fixed_base_g2_checked(void* opaque, const uint8_t* scalars, size_t n, uint32_t algorithm,
+                                                 uint8_t* output, DvgpuG2ValidationReport* report, char* error,
+                                                 size_t cap) {
+    auto* b0 = static_cast<Backend*>(opaque);
+    int rejected = 0;
+    const int rc = guarded(opaque, error, cap, [&](Backend& b) {
+        require(n <= DVGPU_MAX_SETUP_SIZE && algorithm >= 1 && algorithm <= 3 && report && (!n || (scalars && output)),
+                "invalid checked G2 buffers or algorithm");
+        if (!n) {
+            *report = {0, 0, UINT64_MAX, 0, algorithm};
+            return;
+        }
+        uint8_t* d_sc = b.in_scalars.as<uint8_t>(n * 32);
+        uint8_t* d_out = b.in_points.as<uint8_t>(n * 128);
+        uint32_t* d_masks = b.out_buf.as<uint32_t>(n);
+        DV_CUDA(cudaMemcpyAsync(d_sc, scalars, n * 32, cudaMemcpyHostToDevice, b.stream));
+        fixed_base_device(b, d_sc, n, 1, d_out, b.stream);
+        const DvgpuG2ValidationReport r = g2_check_device(b, d_out, n, algorithm, d_masks, b.stream);
+        *report = r;
+        b.g2_traffic.scalar_h2d_bytes += n * 32;
+        b.g2_traffic.status_d2h_bytes += sizeof(r);
+        if (r.invalid_points) {
+            rejected = 1;
+            return;
+        }
+        uint8_t* h = b.pin_out.as<uint8_t>(n * 128);
+        DV_CUDA(cudaMemcpyAsync(h, d_out, n * 128, cudaMemcpyDeviceToHost, b.stream));
+        DV_CUDA(cudaStreamSynchronize(b.stream));
+        memcpy(output, h, n * 128);
+        b.g2_traffic.point_d2h_bytes += n * 128;
+        b.g2_stats.accepted_points += n;
+    });
+    (void)b0;
+    if (rc == 0 && rejected) return fail(-5, "G2 content validation rejected", error, cap);
+    return rc;
+}
+
+extern "C" int dvgpu_g2_validation_stats(void* opaque, DvgpuG2ValidationStats* stats) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || !stats) return -1;
+    *stats = b->g2_stats;
+    return 0;
+}
+
+extern "C" int dvgpu_g2_validation_traffic(void* opaque, DvgpuG2ValidationTraffic* stats) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || !stats) return -1;
+    *stats = b->g2_traffic;
+    return 0;
+}
+
+// ============================================================ IMAD probe
+extern "C" int dvgpu_probe_imad_rate(void* opaque, double* macs_per_second, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(macs_per_second, "null output");
+        uint32_t* sink = b.err.as<uint32_t>(1);
+        const unsigned blocks = (unsigned)sm_count() * 8, threads = 256;
+        const uint32_t iters = 4096;
+        cudaEvent_t e0, e1;
+        DV_CUDA(cudaEventCreate(&e0));
+        DV_CUDA(cudaEventCreate(&e1));
+        k_probe_madc<<<blocks, threads, 0, b.stream>>>(1u, 64, sink);  // warm-up
+        DV_LAUNCH();
+        float best = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            DV_CUDA(cudaEventRecord(e0, b.stream));
+            k_probe_madc<<<blocks, threads, 0, b.stream>>>(2u + rep, iters, sink);
+            DV_LAUNCH();
+            DV_CUDA(cudaEventRecord(e1, b.stream));
+            DV_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            DV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            best = std::min(best, ms);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        // per iteration: 4 rows x 4 wide multiplies (lo + hi = one 32x32->64 MAC each)
+        const double macs = (double)blocks * threads * iters * 4.0 * 4.0;
+        *macs_per_second = macs / (best * 1e-3);
+    });
+}
+
+// ============================================================ diagnostics
+namespace dv {
+void random_fr_launch(uint64_t seed, uint64_t n, uint8_t* d_out, cudaStream_t st);
+void powers_launch(const uint8_t* d_tau, uint64_t n, uint8_t* d_out, cudaStream_t st);
+}  // namespace dv
+
+extern "C" uint64_t dvgpu_launch_count(void) { return __atomic_load_n(&dv::launch_counter(), __ATOMIC_RELAXED); }
+
+extern "C" int dvgpu_msm_timeline(void* opaque, int enable, DvgpuMsmPhaseTimes* out) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || b->retired) return -1;
+    MsmTimeline& tl = b->msm.timeline;
+    try {
+        DV_CUDA(cudaSetDevice(b->device));
+        if (out) {
+            for (int k = 0; k < MSM_PHASES; ++k) out->ms[k] = tl.ms[k];
+            out->calls = tl.calls;
+            out->accum_mixed_adds = tl.accum_mixed_adds;
+        }
+        if (enable) {
+            if (!tl.ev[0])
+                for (auto& e : tl.ev) DV_CUDA(cudaEventCreate(&e));
+            for (auto& m : tl.ms) m = 0;
+            tl.calls = 0;
+            tl.accum_mixed_adds = 0;
+            tl.enabled = true;
+        } else {
+            tl.enabled = false;
+        }
+        return 0;
+    } catch (...) {
+        return -2;
+    }
+}
+
+extern "C" int dvgpu_random_fr_device(void* opaque, uint64_t seed, size_t n, uint8_t* d_out, void* stream,
+                                      char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(!n || d_out, "null output");
+        dv::random_fr_launch(seed, n, d_out, pick(b, stream));
+    });
+}
+
+extern "C" int dvgpu_fr_powers_device(void* opaque, const uint8_t* d_tau, size_t n, uint8_t* d_out, void* stream,
+                                      char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(d_tau && (!n || d_out), "null buffers");
+        dv::powers_launch(d_tau, n, d_out, pick(b, stream));
+    });
+}

@@ -1,0 +1,59 @@
+// Owner ("backend") object behind the opaque void* of the C-ABI.
+//
+// Mirrors the reference owner (native/src/icicle_msm.cu:92-144): created on
+// visible device 0, used by one caller thread at a time, retired by any CUDA
+// failure (later calls return -4), destroyed by dvgpu_backend_destroy.
+// Unlike the reference it uses the device's primary context, so device
+// pointers from other runtime users (e.g. torch) are valid in the
+// device-pointer entry points; each owner has its own non-blocking stream and
+// grow-only workspaces.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+
+#include "../../include/dynaverse_gpu.h"
+#include "engine.hpp"
+#include "g2.cuh"
+#include "msm.cuh"
+#include "ntt.cuh"
+
+namespace dv {
+
+struct ResidentBases {
+    DevBuf points;  // Montgomery affine
+    uint64_t n = 0;
+    int g2 = 0;
+};
+
+struct Backend {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool retired = false;
+    uint32_t large_bucket_factor = 0;
+    std::string identity;
+
+    MsmWorkspace msm;
+    MsmStats msm_stats;
+    NttWorkspace ntt;
+    FixedBaseTables fixed_base;
+    DevBuf in_points, in_scalars, conv_points, idx, out_buf, aux, err;
+    PinnedBuf pin_in, pin_out, pin_err;
+    DvgpuBatchStats batch_stats{};
+    DvgpuSetupStats setup_stats{};
+    DvgpuG2ValidationStats g2_stats{};
+    DvgpuG2ValidationTraffic g2_traffic{};
+    int setup_mode = 2;
+    int force_c = 0;
+
+    std::map<uint64_t, std::unique_ptr<ResidentBases>> bases;
+    uint64_t next_handle = 1;
+
+    void release_all() noexcept;
+    ~Backend() { release_all(); }
+};
+
+}  // namespace dv

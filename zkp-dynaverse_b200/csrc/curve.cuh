@@ -1,0 +1,169 @@
+// BN254 G1 (y^2 = x^3 + 3 over Fq) and G2 (twist y^2 = x^3 + 3/(9+u) over
+// Fq2) in XYZZ coordinates: x = X/ZZ, y = Y/ZZZ, ZZ^3 = ZZZ^2, ZZ = 0 is the
+// point at infinity.  Formulas are the a = 0 specialisations of the
+// Explicit-Formulas Database "xyzz" family (madd-2008-s, add-2008-s,
+// dbl-2008-s-1, mdbl-2008-s-1): mixed add 8M+2S, full add 12M+2S,
+// double 6M+3S.  Affine infinity is encoded as (0, 0), which is on neither
+// curve.
+#pragma once
+#include "field.cuh"
+
+namespace dv {
+
+template <class F>
+struct Affine {
+    F x, y;
+    DV_INL bool is_inf() const { return x.is_zero() && y.is_zero(); }
+    DV_INL static Affine inf() { return {F::zero(), F::zero()}; }
+    DV_INL Affine neg() const { return {x, F::neg(y)}; }
+};
+
+template <class F>
+struct XYZZ {
+    F x, y, zz, zzz;
+
+    DV_INL static XYZZ inf() { return {F::one(), F::one(), F::zero(), F::zero()}; }
+    DV_INL bool is_inf() const { return zz.is_zero(); }
+    DV_INL static XYZZ from_affine(const Affine<F>& a) {
+        if (a.is_inf()) return inf();
+        return {a.x, a.y, F::one(), F::one()};
+    }
+    DV_INL XYZZ neg() const { return {x, F::neg(y), zz, zzz}; }
+
+    // 2 * (x, y) for an affine point (mdbl-2008-s-1).
+    DV_INL static XYZZ dbl_affine(const Affine<F>& a) {
+        const F u = F::dbl(a.y);
+        const F v = F::sqr(u);
+        const F w = F::mul(u, v);
+        const F s = F::mul(a.x, v);
+        const F x2 = F::sqr(a.x);
+        const F m = F::add(F::dbl(x2), x2);
+        const F x3 = F::sub(F::sqr(m), F::dbl(s));
+        const F y3 = F::sub(F::mul(m, F::sub(s, x3)), F::mul(w, a.y));
+        return {x3, y3, v, w};
+    }
+
+    // dbl-2008-s-1 (a = 0)
+    DV_INL static XYZZ dbl(const XYZZ& p) {
+        if (p.is_inf()) return p;
+        const F u = F::dbl(p.y);
+        const F v = F::sqr(u);
+        const F w = F::mul(u, v);
+        const F s = F::mul(p.x, v);
+        const F x2 = F::sqr(p.x);
+        const F m = F::add(F::dbl(x2), x2);
+        const F x3 = F::sub(F::sqr(m), F::dbl(s));
+        const F y3 = F::sub(F::mul(m, F::sub(s, x3)), F::mul(w, p.y));
+        return {x3, y3, F::mul(v, p.zz), F::mul(w, p.zzz)};
+    }
+
+    // p + a with a affine (madd-2008-s).
+    DV_INL static XYZZ add_affine(const XYZZ& p, const Affine<F>& a) {
+        if (a.is_inf()) return p;
+        if (p.is_inf()) return from_affine(a);
+        const F u2 = F::mul(a.x, p.zz);
+        const F s2 = F::mul(a.y, p.zzz);
+        const F pp_ = F::sub(u2, p.x);
+        const F r = F::sub(s2, p.y);
+        if (pp_.is_zero()) {
+            if (r.is_zero()) return dbl_affine(a);
+            return inf();
+        }
+        const F pp = F::sqr(pp_);
+        const F ppp = F::mul(pp_, pp);
+        const F q = F::mul(p.x, pp);
+        const F x3 = F::sub(F::sub(F::sqr(r), ppp), F::dbl(q));
+        const F y3 = F::sub(F::mul(r, F::sub(q, x3)), F::mul(p.y, ppp));
+        return {x3, y3, F::mul(p.zz, pp), F::mul(p.zzz, ppp)};
+    }
+
+    // p + q (add-2008-s).
+    DV_INL static XYZZ add(const XYZZ& p, const XYZZ& q) {
+        if (p.is_inf()) return q;
+        if (q.is_inf()) return p;
+        const F u1 = F::mul(p.x, q.zz);
+        const F u2 = F::mul(q.x, p.zz);
+        const F s1 = F::mul(p.y, q.zzz);
+        const F s2 = F::mul(q.y, p.zzz);
+        const F pp_ = F::sub(u2, u1);
+        const F r = F::sub(s2, s1);
+        if (pp_.is_zero()) {
+            if (r.is_zero()) return dbl(p);
+            return inf();
+        }
+        const F pp = F::sqr(pp_);
+        const F ppp = F::mul(pp_, pp);
+        const F qq = F::mul(u1, pp);
+        const F x3 = F::sub(F::sub(F::sqr(r), ppp), F::dbl(qq));
+        const F y3 = F::sub(F::mul(r, F::sub(qq, x3)), F::mul(s1, ppp));
+        return {x3, y3, F::mul(F::mul(p.zz, q.zz), pp), F::mul(F::mul(p.zzz, q.zzz), ppp)};
+    }
+
+    // Projective equality without normalisation.
+    DV_INL static bool equal(const XYZZ& p, const XYZZ& q) {
+        const bool pi = p.is_inf(), qi = q.is_inf();
+        if (pi || qi) return pi && qi;
+        return F::mul(p.x, q.zz) == F::mul(q.x, p.zz) && F::mul(p.y, q.zzz) == F::mul(q.y, p.zzz);
+    }
+
+    DV_INL Affine<F> to_affine() const {
+        if (is_inf()) return Affine<F>::inf();
+        const F d = F::inv(F::mul(zz, zzz));     // 1 / (ZZ * ZZZ)
+        const F izz = F::mul(d, zzz);            // 1 / ZZ
+        const F izzz = F::mul(d, zz);            // 1 / ZZZ
+        return {F::mul(x, izz), F::mul(y, izzz)};
+    }
+};
+
+typedef Affine<Fq> G1A;
+typedef XYZZ<Fq> G1X;
+typedef Affine<Fq2> G2A;
+typedef XYZZ<Fq2> G2X;
+
+// ------------------------------------------------------------- canonical I/O
+// Canonical little-endian 32-byte field elements, read as 8 u32 words.
+
+DV_INL void load_words(const uint8_t* p, uint32_t* w) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    const uint4 a = q[0], b = q[1];
+    w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+    w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+}
+DV_INL void store_words(uint8_t* p, const uint32_t* w) {
+    uint4* q = reinterpret_cast<uint4*>(p);
+    q[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    q[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+// Curve equations (Montgomery constants).
+DV_INL Fq g1_b() {
+    uint32_t c[8] = {3, 0, 0, 0, 0, 0, 0, 0};
+    return Fq::from_canonical(c);
+}
+DV_INL Fq2 g2_b() {
+    // 3 / (9 + u), canonical limbs.
+    const uint32_t c0[8] = {0x24a138e5u, 0x3267e6dcu, 0x59dbefa3u, 0xb5b4c5e5u,
+                            0x1be06ac3u, 0x81be1899u, 0xceb8aaaeu, 0x2b149d40u};
+    const uint32_t c1[8] = {0x85c315d2u, 0xe4a2bd06u, 0xe52d1852u, 0xa74fa084u,
+                            0xeed8fdf4u, 0xcd2cafadu, 0x3af0fed4u, 0x009713b0u};
+    return {Fq::from_canonical(c0), Fq::from_canonical(c1)};
+}
+
+template <class F>
+struct CurveOps;
+template <>
+struct CurveOps<Fq> {
+    DV_INL static bool on_curve(const Affine<Fq>& a) {
+        if (a.is_inf()) return true;
+        return Fq::sqr(a.y) == Fq::add(Fq::mul(Fq::sqr(a.x), a.x), g1_b());
+    }
+};
+template <>
+struct CurveOps<Fq2> {
+    DV_INL static bool on_curve(const Affine<Fq2>& a) {
+        if (a.is_inf()) return true;
+        return Fq2::sqr(a.y) == Fq2::add(Fq2::mul(Fq2::sqr(a.x), a.x), g2_b());
+    }
+};
+
+}  // namespace dv

@@ -1,0 +1,101 @@
+// Host-side plumbing shared by the kernels' launch code: error type,
+// grow-only device workspace buffers, CUDA status checks.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace dv {
+
+// Invalid caller input: reported as status -1, the owner stays healthy.
+struct InvalidArgument : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+// CUDA failure: reported as status -2, the owner is retired.
+struct CudaFailure : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+inline void cuda_check(cudaError_t s, const char* what) {
+    if (s != cudaSuccess) throw CudaFailure(std::string(what) + ": " + cudaGetErrorString(s));
+}
+// Number of this library's kernel launches since load (all owners).
+uint64_t& launch_counter();
+inline void launched() {
+    cuda_check(cudaGetLastError(), "kernel launch");
+    __atomic_add_fetch(&launch_counter(), 1, __ATOMIC_RELAXED);
+}
+#define DV_CUDA(call) ::dv::cuda_check((call), #call)
+#define DV_LAUNCH() ::dv::launched()
+
+// Grow-only device buffer.  Contents are scratch between calls.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t cap = 0;
+    void* get(size_t bytes) {
+        if (bytes <= cap && ptr) return ptr;
+        release();
+        size_t want = bytes < 256 ? 256 : bytes;
+        DV_CUDA(cudaMalloc(&ptr, want));
+        cap = want;
+        return ptr;
+    }
+    template <class T>
+    T* as(size_t count) {
+        return static_cast<T*>(get(count * sizeof(T)));
+    }
+    template <class T>
+    T* view() const {
+        return static_cast<T*>(ptr);
+    }
+    void release() noexcept {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+    ~DevBuf() { release(); }
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+// Grow-only pinned host buffer.
+struct PinnedBuf {
+    void* ptr = nullptr;
+    size_t cap = 0;
+    void* get(size_t bytes) {
+        if (bytes <= cap && ptr) return ptr;
+        release();
+        size_t want = bytes < 256 ? 256 : bytes;
+        DV_CUDA(cudaMallocHost(&ptr, want));
+        cap = want;
+        return ptr;
+    }
+    template <class T>
+    T* as(size_t count) {
+        return static_cast<T*>(get(count * sizeof(T)));
+    }
+    void release() noexcept {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+    ~PinnedBuf() { release(); }
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+};
+
+inline int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        DV_CUDA(cudaGetDevice(&dev));
+        DV_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return n;
+}
+
+}  // namespace dv

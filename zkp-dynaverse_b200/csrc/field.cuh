@@ -1,0 +1,285 @@
+// BN254 prime fields on sm_100a: 8 x 32-bit limbs, Montgomery form R = 2^256.
+//
+// Multiplication is CIOS (Koc, Acar, Kaliski, "Analyzing and comparing
+// Montgomery multiplication algorithms", 1996) written as PTX carry chains.
+// Each row "t += x * v" is split into an even-limb chain (lo of v0,v2,.. into
+// t0,t2,..; hi into t1,t3,..) and an odd-limb chain, so every chain is a
+// single uninterrupted mad.lo.cc / madc.hi.cc sequence.  p < 2^254, so the
+// 9-limb accumulator never overflows (T < 2p before each row, and
+// T + a*b_i + m*p < 2^288).
+//
+// Values are kept fully reduced in [0, p).
+#pragma once
+#include <cstdint>
+
+namespace dv {
+
+struct FqCfg {
+    static constexpr uint32_t P0 = 0xd87cfd47u, P1 = 0x3c208c16u, P2 = 0x6871ca8du, P3 = 0x97816a91u,
+                              P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
+    static constexpr uint32_t INV = 0xe4866389u;  // -p^{-1} mod 2^32
+    static constexpr uint32_t ONE0 = 0xc58f0d9du, ONE1 = 0xd35d438du, ONE2 = 0xf5c70b3du, ONE3 = 0x0a78eb28u, ONE4 = 0x7879462cu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
+    static constexpr uint32_t R20 = 0x538afa89u, R21 = 0xf32cfc5bu, R22 = 0xd44501fbu, R23 = 0xb5e71911u, R24 = 0x0a417ff6u, R25 = 0x47ab1effu, R26 = 0xcab8351fu, R27 = 0x06d89f71u;
+};
+struct FrCfg {
+    static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u,
+                              P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
+    static constexpr uint32_t INV = 0xefffffffu;
+    static constexpr uint32_t ONE0 = 0x4ffffffbu, ONE1 = 0xac96341cu, ONE2 = 0x9f60cd29u, ONE3 = 0x36fc7695u, ONE4 = 0x7879462eu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
+    static constexpr uint32_t R20 = 0xae216da7u, R21 = 0x1bb8e645u, R22 = 0xe35c59e3u, R23 = 0x53fe3ab1u, R24 = 0x53bb8085u, R25 = 0x8c49833du, R26 = 0x7f4e44a5u, R27 = 0x0216d0b1u;
+};
+
+#define DV_INL __device__ __forceinline__
+
+template <class C>
+struct Fp {
+    uint32_t v[8];
+
+    DV_INL static Fp zero() {
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) r.v[i] = 0;
+        return r;
+    }
+    DV_INL static Fp one() {
+        Fp r;
+        r.v[0] = C::ONE0; r.v[1] = C::ONE1; r.v[2] = C::ONE2; r.v[3] = C::ONE3;
+        r.v[4] = C::ONE4; r.v[5] = C::ONE5; r.v[6] = C::ONE6; r.v[7] = C::ONE7;
+        return r;
+    }
+    // R^2 mod p: the Montgomery form of R.
+    DV_INL static Fp r2() {
+        Fp r;
+        r.v[0] = C::R20; r.v[1] = C::R21; r.v[2] = C::R22; r.v[3] = C::R23;
+        r.v[4] = C::R24; r.v[5] = C::R25; r.v[6] = C::R26; r.v[7] = C::R27;
+        return r;
+    }
+    DV_INL bool is_zero() const {
+        uint32_t x = v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7];
+        return x == 0;
+    }
+    DV_INL bool operator==(const Fp& o) const {
+        uint32_t x = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x |= v[i] ^ o.v[i];
+        return x == 0;
+    }
+
+    // r = a - p if a >= p else a   (a < 2^256)
+    DV_INL static void reduce_once(uint32_t* t) {
+        uint32_t s[8], borrow;
+        asm("sub.cc.u32 %0, %9, %17;\n\t"
+            "subc.cc.u32 %1, %10, %18;\n\t"
+            "subc.cc.u32 %2, %11, %19;\n\t"
+            "subc.cc.u32 %3, %12, %20;\n\t"
+            "subc.cc.u32 %4, %13, %21;\n\t"
+            "subc.cc.u32 %5, %14, %22;\n\t"
+            "subc.cc.u32 %6, %15, %23;\n\t"
+            "subc.cc.u32 %7, %16, %24;\n\t"
+            "subc.u32 %8, 0, 0;"
+            : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]),
+              "=r"(s[7]), "=r"(borrow)
+            : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]),
+              "n"(C::P0), "n"(C::P1), "n"(C::P2), "n"(C::P3), "n"(C::P4), "n"(C::P5), "n"(C::P6),
+              "n"(C::P7));
+        // borrow == 0xffffffff  <=>  t < p  -> keep t
+#pragma unroll
+        for (int i = 0; i < 8; ++i) t[i] = borrow ? t[i] : s[i];
+    }
+
+    DV_INL static Fp add(const Fp& a, const Fp& b) {
+        Fp r;
+        asm("add.cc.u32 %0, %8, %16;\n\t"
+            "addc.cc.u32 %1, %9, %17;\n\t"
+            "addc.cc.u32 %2, %10, %18;\n\t"
+            "addc.cc.u32 %3, %11, %19;\n\t"
+            "addc.cc.u32 %4, %12, %20;\n\t"
+            "addc.cc.u32 %5, %13, %21;\n\t"
+            "addc.cc.u32 %6, %14, %22;\n\t"
+            "addc.u32 %7, %15, %23;"
+            : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]),
+              "=r"(r.v[6]), "=r"(r.v[7])
+            : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]),
+              "r"(a.v[7]), "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]),
+              "r"(b.v[6]), "r"(b.v[7]));
+        reduce_once(r.v);
+        return r;
+    }
+
+    DV_INL static Fp sub(const Fp& a, const Fp& b) {
+        Fp r;
+        uint32_t borrow;
+        asm("sub.cc.u32 %0, %9, %17;\n\t"
+            "subc.cc.u32 %1, %10, %18;\n\t"
+            "subc.cc.u32 %2, %11, %19;\n\t"
+            "subc.cc.u32 %3, %12, %20;\n\t"
+            "subc.cc.u32 %4, %13, %21;\n\t"
+            "subc.cc.u32 %5, %14, %22;\n\t"
+            "subc.cc.u32 %6, %15, %23;\n\t"
+            "subc.cc.u32 %7, %16, %24;\n\t"
+            "subc.u32 %8, 0, 0;"
+            : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]),
+              "=r"(r.v[6]), "=r"(r.v[7]), "=r"(borrow)
+            : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]),
+              "r"(a.v[7]), "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]),
+              "r"(b.v[6]), "r"(b.v[7]));
+        // add back p & borrow
+        asm("add.cc.u32 %0, %0, %8;\n\t"
+            "addc.cc.u32 %1, %1, %9;\n\t"
+            "addc.cc.u32 %2, %2, %10;\n\t"
+            "addc.cc.u32 %3, %3, %11;\n\t"
+            "addc.cc.u32 %4, %4, %12;\n\t"
+            "addc.cc.u32 %5, %5, %13;\n\t"
+            "addc.cc.u32 %6, %6, %14;\n\t"
+            "addc.u32 %7, %7, %15;"
+            : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]),
+              "+r"(r.v[6]), "+r"(r.v[7])
+            : "r"(C::P0 & borrow), "r"(C::P1 & borrow), "r"(C::P2 & borrow), "r"(C::P3 & borrow),
+              "r"(C::P4 & borrow), "r"(C::P5 & borrow), "r"(C::P6 & borrow), "r"(C::P7 & borrow));
+        return r;
+    }
+
+    DV_INL static Fp dbl(const Fp& a) { return add(a, a); }
+
+    DV_INL static Fp neg(const Fp& a) {
+        Fp z = zero();
+        return a.is_zero() ? a : sub(z, a);
+    }
+
+    DV_INL static Fp mul(const Fp& a, const Fp& b) {
+        uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0, t8 = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t bi = b.v[i];
+            asm("mad.lo.cc.u32 %0, %9, %13, %0;\n\t"
+                "madc.hi.cc.u32 %1, %9, %13, %1;\n\t"
+                "madc.lo.cc.u32 %2, %10, %13, %2;\n\t"
+                "madc.hi.cc.u32 %3, %10, %13, %3;\n\t"
+                "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"
+                "madc.hi.cc.u32 %5, %11, %13, %5;\n\t"
+                "madc.lo.cc.u32 %6, %12, %13, %6;\n\t"
+                "madc.hi.cc.u32 %7, %12, %13, %7;\n\t"
+                "addc.u32 %8, %8, 0;"
+                : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)
+                : "r"(a.v[0]), "r"(a.v[2]), "r"(a.v[4]), "r"(a.v[6]), "r"(bi));
+            asm("mad.lo.cc.u32 %0, %8, %12, %0;\n\t"
+                "madc.hi.cc.u32 %1, %8, %12, %1;\n\t"
+                "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"
+                "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"
+                "madc.lo.cc.u32 %4, %10, %12, %4;\n\t"
+                "madc.hi.cc.u32 %5, %10, %12, %5;\n\t"
+                "madc.lo.cc.u32 %6, %11, %12, %6;\n\t"
+                "madc.hi.u32 %7, %11, %12, %7;"
+                : "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)
+                : "r"(a.v[1]), "r"(a.v[3]), "r"(a.v[5]), "r"(a.v[7]), "r"(bi));
+            const uint32_t m = t0 * C::INV;
+            asm("mad.lo.cc.u32 %0, %9, %10, %0;\n\t"
+                "madc.hi.cc.u32 %1, %9, %10, %1;\n\t"
+                "madc.lo.cc.u32 %2, %9, %11, %2;\n\t"
+                "madc.hi.cc.u32 %3, %9, %11, %3;\n\t"
+                "madc.lo.cc.u32 %4, %9, %12, %4;\n\t"
+                "madc.hi.cc.u32 %5, %9, %12, %5;\n\t"
+                "madc.lo.cc.u32 %6, %9, %13, %6;\n\t"
+                "madc.hi.cc.u32 %7, %9, %13, %7;\n\t"
+                "addc.u32 %8, %8, 0;"
+                : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)
+                : "r"(m), "n"(C::P0), "n"(C::P2), "n"(C::P4), "n"(C::P6));
+            asm("mad.lo.cc.u32 %0, %8, %9, %0;\n\t"
+                "madc.hi.cc.u32 %1, %8, %9, %1;\n\t"
+                "madc.lo.cc.u32 %2, %8, %10, %2;\n\t"
+                "madc.hi.cc.u32 %3, %8, %10, %3;\n\t"
+                "madc.lo.cc.u32 %4, %8, %11, %4;\n\t"
+                "madc.hi.cc.u32 %5, %8, %11, %5;\n\t"
+                "madc.lo.cc.u32 %6, %8, %12, %6;\n\t"
+                "madc.hi.u32 %7, %8, %12, %7;"
+                : "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)
+                : "r"(m), "n"(C::P1), "n"(C::P3), "n"(C::P5), "n"(C::P7));
+            // t0 is now 0 (mod 2^32): shift one limb down.
+            t0 = t1; t1 = t2; t2 = t3; t3 = t4; t4 = t5; t5 = t6; t6 = t7; t7 = t8; t8 = 0;
+        }
+        Fp r;
+        r.v[0] = t0; r.v[1] = t1; r.v[2] = t2; r.v[3] = t3;
+        r.v[4] = t4; r.v[5] = t5; r.v[6] = t6; r.v[7] = t7;
+        reduce_once(r.v);
+        return r;
+    }
+
+    DV_INL static Fp sqr(const Fp& a) { return mul(a, a); }
+
+    // Canonical little-endian limbs <-> Montgomery form.
+    DV_INL static Fp from_canonical(const uint32_t* c) {
+        Fp a;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a.v[i] = c[i];
+        return mul(a, r2());
+    }
+    DV_INL void to_canonical(uint32_t* c) const {
+        Fp one_raw = zero();
+        one_raw.v[0] = 1;
+        Fp r = mul(*this, one_raw);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) c[i] = r.v[i];
+    }
+    // Canonical check: c < p.
+    DV_INL static bool is_canonical(const uint32_t* c) {
+        const uint32_t p[8] = {C::P0, C::P1, C::P2, C::P3, C::P4, C::P5, C::P6, C::P7};
+#pragma unroll
+        for (int i = 7; i >= 0; --i) {
+            if (c[i] < p[i]) return true;
+            if (c[i] > p[i]) return false;
+        }
+        return false;
+    }
+
+    // a^e for a 256-bit exponent given as 8 little-endian limbs.
+    DV_INL static Fp pow(const Fp& a, const uint32_t* e) {
+        Fp r = one();
+        for (int i = 255; i >= 0; --i) {
+            r = sqr(r);
+            if ((e[i >> 5] >> (i & 31)) & 1) r = mul(r, a);
+        }
+        return r;
+    }
+    DV_INL static Fp inv(const Fp& a) {
+        const uint32_t e[8] = {C::P0 - 2, C::P1, C::P2, C::P3, C::P4, C::P5, C::P6, C::P7};
+        return pow(a, e);
+    }
+};
+
+typedef Fp<FqCfg> Fq;
+typedef Fp<FrCfg> Fr;
+
+// Fq2 = Fq[u] / (u^2 + 1)
+struct Fq2 {
+    Fq c0, c1;
+    DV_INL static Fq2 zero() { return {Fq::zero(), Fq::zero()}; }
+    DV_INL static Fq2 one() { return {Fq::one(), Fq::zero()}; }
+    DV_INL bool is_zero() const { return c0.is_zero() && c1.is_zero(); }
+    DV_INL bool operator==(const Fq2& o) const { return c0 == o.c0 && c1 == o.c1; }
+    DV_INL static Fq2 add(const Fq2& a, const Fq2& b) { return {Fq::add(a.c0, b.c0), Fq::add(a.c1, b.c1)}; }
+    DV_INL static Fq2 sub(const Fq2& a, const Fq2& b) { return {Fq::sub(a.c0, b.c0), Fq::sub(a.c1, b.c1)}; }
+    DV_INL static Fq2 dbl(const Fq2& a) { return {Fq::dbl(a.c0), Fq::dbl(a.c1)}; }
+    DV_INL static Fq2 neg(const Fq2& a) { return {Fq::neg(a.c0), Fq::neg(a.c1)}; }
+    DV_INL static Fq2 conj(const Fq2& a) { return {a.c0, Fq::neg(a.c1)}; }
+    DV_INL static Fq2 mul(const Fq2& a, const Fq2& b) {
+        // Karatsuba: 3 base multiplications.
+        const Fq t0 = Fq::mul(a.c0, b.c0);
+        const Fq t1 = Fq::mul(a.c1, b.c1);
+        const Fq t2 = Fq::mul(Fq::add(a.c0, a.c1), Fq::add(b.c0, b.c1));
+        return {Fq::sub(t0, t1), Fq::sub(Fq::sub(t2, t0), t1)};
+    }
+    DV_INL static Fq2 sqr(const Fq2& a) {
+        // (c0 + c1 u)^2 = (c0+c1)(c0-c1) + 2 c0 c1 u
+        const Fq m = Fq::mul(Fq::add(a.c0, a.c1), Fq::sub(a.c0, a.c1));
+        const Fq c = Fq::mul(a.c0, a.c1);
+        return {m, Fq::dbl(c)};
+    }
+    DV_INL static Fq2 mul_fq(const Fq2& a, const Fq& s) { return {Fq::mul(a.c0, s), Fq::mul(a.c1, s)}; }
+    DV_INL static Fq2 inv(const Fq2& a) {
+        const Fq n = Fq::add(Fq::sqr(a.c0), Fq::sqr(a.c1));
+        const Fq ni = Fq::inv(n);
+        return {Fq::mul(a.c0, ni), Fq::neg(Fq::mul(a.c1, ni))};
+    }
+};
+
+}  // namespace dv

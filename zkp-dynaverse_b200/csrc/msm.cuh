@@ -1,0 +1,83 @@
+// Pippenger multi-scalar multiplication on sm_100a for BN254 G1 and G2.
+//
+// One engine serves the plain MSM (OperatorBackend::msm / msm_g2_host,
+// crates/protocol/src/types.rs:295-356), the padded batch
+// (dvgpu_bn254_msm_batch, native/src/icicle_msm.cu:810-880), uneven batches
+// and the sparse-index MSM (types.rs:262-345): every input is a list of
+// "sets" (independent MSMs) over concatenated point/scalar arrays, and the
+// set index is folded into the bucket key, so all sets run in the same
+// launches.
+//
+// Pipeline (all on one stream):
+//   1. hist     signed c-bit digits of every scalar, count per (set, window, bucket)
+//   2. scan     exclusive prefix sum -> bucket offsets in the sorted list
+//   3. scatter  counting-sort placement of (point index | sign) per digit
+//   4. accum    persistent, perfectly balanced bucket accumulation: each thread
+//               sums a fixed-length slice of the sorted list with XYZZ mixed
+//               additions; buckets cut by a slice boundary leave partials
+//   5. fixup    partial sums of buckets that span slices are merged
+//   6. segments per (set, window): running sums over segments of 2^seg_log
+//               buckets, each segment weighted by its offset (small scalar mul)
+//   7. wsum     per (set, window) block reduction of the segment values
+//   8. host     Horner over the windows and normalisation to affine
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "curve.cuh"
+#include "engine.hpp"
+
+namespace dv {
+
+struct MsmPlan {
+    int c;            // window width in bits
+    int windows;      // ceil(255 / c): top window never carries out
+    uint32_t buckets; // 2^(c-1) signed-digit buckets per window
+    int seg_log;      // bucket-reduction segment length = 2^seg_log
+};
+
+// Cost model: windows * (10 * n + 28 * buckets) base-field multiplications
+// (XYZZ mixed add = 10, two full adds per bucket in the reduction = 28).
+MsmPlan msm_plan(uint64_t points_per_set, int force_c);
+
+// Optional per-phase device timing (CUDA events on the launching stream).
+enum { MSM_PHASES = 8 };  // hist, scan, scatter, accum, fixup, segments, wsum, tail(D2H + host Horner)
+struct MsmTimeline {
+    bool enabled = false;
+    cudaEvent_t ev[MSM_PHASES + 1] = {};
+    double ms[MSM_PHASES] = {};
+    uint64_t calls = 0;
+    uint64_t accum_mixed_adds = 0;  // N * windows summed over timed calls (for the roofline)
+};
+
+struct MsmWorkspace {
+    DevBuf set_off, counts, offsets, cursor, sorted, buckets, pgid, ppt, segs, windows, err;
+    PinnedBuf host_windows, host_err;
+    MsmTimeline timeline;
+};
+
+struct MsmStats {
+    uint64_t calls = 0, sets = 0, points = 0, last_c = 0;
+};
+
+// d_points: Montgomery-form affine points, d_scalars: canonical 8-word
+// little-endian scalars (checked < r), both concatenated over sets.
+// set_offsets (host, count + 1 entries) delimit the sets.  host_out receives
+// count canonical affine points (2 * sizeof(F) bytes each, all-zero for
+// infinity).  Throws InvalidArgument for non-canonical scalars.
+template <class F>
+void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const uint32_t* set_offsets,
+             uint32_t count, int force_c, cudaStream_t stream, uint8_t* host_out, MsmStats* stats);
+
+// Canonical bytes -> Montgomery affine, with canonical and on-curve checks.
+// Sets *first_bad (device) to the lowest failing index, or leaves it.
+template <class F>
+void convert_points(const uint8_t* d_canon, Affine<F>* d_out, uint64_t n, uint32_t* d_first_bad, cudaStream_t stream);
+
+// Gather (sparse MSM): out[j] = bases[idx[j]], with idx checked against nbases.
+template <class F>
+void gather_points(const Affine<F>* d_bases, uint64_t nbases, const uint64_t* d_idx, uint64_t k, Affine<F>* d_out,
+                   uint32_t* d_first_bad, cudaStream_t stream);
+
+}  // namespace dv

@@ -1,0 +1,269 @@
+// Fr NTT kernels and launch sequence (see ntt.cuh).
+#include <algorithm>
+#include <string>
+
+#include "curve.cuh"
+#include "ntt.cuh"
+
+namespace dv {
+
+namespace {
+
+// TWO_ADIC_ROOT_OF_UNITY of BN254 Fr: 5^((r-1)/2^28), canonical limbs.
+__device__ __constant__ uint32_t ROOT28[8] = {0x725b19f0u, 0x9bd61b6eu, 0x41112ed4u, 0x402d111eu,
+                                              0x8ef62abcu, 0x00e0a7ebu, 0xa58a7e85u, 0x2a3c09f0u};
+
+// consts layout (Fr, Montgomery unless noted):
+//  0: w (order n; inverted for inverse kinds)   1: n^-1   2: n^-1 (canonical)
+//  3: g = 5   4: g^-1   5: g^(2^split)   6: g^-(2^split)   7: R (= R2 as Montgomery)
+//  8: one (canonical 1)
+enum { C_W = 0, C_NINV, C_NINV_CANON, C_G, C_GINV, C_G_SPLIT, C_GINV_SPLIT, C_R, C_ONE_RAW, C_COUNT };
+
+__global__ void k_setup_consts(int logn, int inverse, int split, Fr* out) {
+    if (threadIdx.x || blockIdx.x) return;
+    uint32_t rc[8];
+    for (int i = 0; i < 8; ++i) rc[i] = ROOT28[i];
+    Fr w = Fr::from_canonical(rc);
+    for (int k = logn; k < 28; ++k) w = Fr::sqr(w);
+    if (inverse) w = Fr::inv(w);
+    uint32_t nc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    nc[logn / 32] = 1u << (logn % 32);
+    const Fr nm = Fr::from_canonical(nc);
+    const Fr ninv = Fr::inv(nm);
+    uint32_t gc[8] = {5, 0, 0, 0, 0, 0, 0, 0};
+    const Fr g = Fr::from_canonical(gc);
+    const Fr ginv = Fr::inv(g);
+    Fr gs = g, gis = ginv;
+    for (int k = 0; k < split; ++k) { gs = Fr::sqr(gs); gis = Fr::sqr(gis); }
+    const Fr r2 = Fr::r2();
+    uint32_t canon[8];
+    ninv.to_canonical(canon);
+    Fr ninv_c;
+    for (int i = 0; i < 8; ++i) ninv_c.v[i] = canon[i];
+    Fr one_raw = Fr::zero();
+    one_raw.v[0] = 1;
+    out[C_W] = w;
+    out[C_NINV] = ninv;
+    out[C_NINV_CANON] = ninv_c;
+    out[C_G] = g;
+    out[C_GINV] = ginv;
+    out[C_G_SPLIT] = gs;
+    out[C_GINV_SPLIT] = gis;
+    out[C_R] = r2;
+    out[C_ONE_RAW] = one_raw;
+}
+
+// out[i] = base^i * mul for i < count (Montgomery), computed in chunks of
+// `chunk` consecutive powers per thread.  canonical_out converts to canonical.
+__global__ void k_pow_table(const Fr* __restrict__ base_p, const Fr* __restrict__ mul_p, uint64_t count,
+                            uint32_t chunk, int canonical_out, Fr* __restrict__ out) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t start = t * chunk;
+    if (start >= count) return;
+    const Fr base = *base_p;
+    // x = base^start
+    Fr x = Fr::one();
+    for (int bit = 63 - __clzll(start | 1); bit >= 0; --bit) {
+        x = Fr::sqr(x);
+        if ((start >> bit) & 1) x = Fr::mul(x, base);
+    }
+    const uint64_t end = min(count, start + chunk);
+    for (uint64_t i = start; i < end; ++i) {
+        Fr v = mul_p ? Fr::mul(x, *mul_p) : x;
+        if (canonical_out) {
+            uint32_t c[8];
+            v.to_canonical(c);
+            for (int j = 0; j < 8; ++j) v.v[j] = c[j];
+        }
+        out[i] = v;
+        x = Fr::mul(x, base);
+    }
+}
+
+DV_INL void load_plane(const uint32_t* sm, uint32_t n, uint32_t t, Fr& a) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a.v[j] = sm[j * n + t];
+}
+DV_INL void store_plane(uint32_t* sm, uint32_t n, uint32_t t, const Fr& a) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sm[j * n + t] = a.v[j];
+}
+
+// One DIF pass over stages [s0, s0 + k).  first: convert canonical input
+// (with coset pre-scale if pre_hi != null) and check canonical form.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_dif_pass(const uint8_t* __restrict__ in, Fr* __restrict__ work, int logn,
+                                                      int s0, int k, const Fr* __restrict__ tw, int first,
+                                                      const Fr* __restrict__ pre_hi, const Fr* __restrict__ pre_lo,
+                                                      int split, const Fr* __restrict__ consts,
+                                                      uint32_t* __restrict__ first_bad) {
+    extern __shared__ uint32_t sm[];
+    const uint32_t G = 1u << k;
+    const int lb = logn - s0 - k;
+    const uint64_t g = blockIdx.x;
+    const uint64_t low = g & ((1ull << lb) - 1), high = g >> lb;
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t t = tid; t < G; t += THREADS) {
+        const uint64_t idx = (high << (lb + k)) | ((uint64_t)t << lb) | low;
+        Fr a;
+        if (first) {
+            uint32_t c[8];
+            load_words(in + 32 * idx, c);
+            if (!Fr::is_canonical(c)) {
+                atomicMin(first_bad, (uint32_t)idx);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) c[j] = 0;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) a.v[j] = c[j];
+            if (pre_hi) {
+                const uint64_t lo_mask = (1ull << split) - 1;
+                a = Fr::mul(Fr::mul(a, pre_hi[idx >> split]), pre_lo[idx & lo_mask]);
+            } else {
+                a = Fr::mul(a, consts[C_R]);
+            }
+        } else {
+            a = work[idx];
+        }
+        store_plane(sm, G, t, a);
+    }
+    __syncthreads();
+    for (int l = 0; l < k; ++l) {
+        const int s = s0 + l;
+        const uint32_t half = 1u << (k - 1 - l);
+        for (uint32_t b = tid; b < G / 2; b += THREADS) {
+            const uint32_t t0 = ((b >> (k - 1 - l)) << (k - l)) | (b & (half - 1));
+            const uint32_t t1 = t0 + half;
+            Fr u, v;
+            load_plane(sm, G, t0, u);
+            load_plane(sm, G, t1, v);
+            const uint64_t jp = ((uint64_t)(t0 & (half - 1)) << lb) | low;
+            const Fr x = Fr::add(u, v);
+            const Fr y = Fr::mul(Fr::sub(u, v), tw[jp << s]);
+            store_plane(sm, G, t0, x);
+            store_plane(sm, G, t1, y);
+        }
+        __syncthreads();
+    }
+    for (uint32_t t = tid; t < G; t += THREADS) {
+        const uint64_t idx = (high << (lb + k)) | ((uint64_t)t << lb) | low;
+        Fr a;
+        load_plane(sm, G, t, a);
+        work[idx] = a;
+    }
+}
+
+// Bit-reversal permutation + post scaling + conversion to canonical form.
+__global__ void k_permute(const Fr* __restrict__ work, uint8_t* __restrict__ out, int logn,
+                          const Fr* __restrict__ post_hi, const Fr* __restrict__ post_lo, int split,
+                          const Fr* __restrict__ post_const) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >> logn) return;
+    const uint64_t r = logn ? (__brevll(i) >> (64 - logn)) : 0;
+    Fr a = work[r];
+    if (post_hi) {
+        const uint64_t lo_mask = (1ull << split) - 1;
+        a = Fr::mul(Fr::mul(a, post_hi[i >> split]), post_lo[i & lo_mask]);
+    } else {
+        a = Fr::mul(a, *post_const);
+    }
+    store_words(out + 32 * i, a.v);
+}
+
+template <int THREADS>
+void launch_pass(const uint8_t* in, Fr* work, int logn, int s0, int k, const Fr* tw, int first, const Fr* pre_hi,
+                 const Fr* pre_lo, int split, const Fr* consts, uint32_t* bad, cudaStream_t st) {
+    const size_t smem = (size_t)8 * sizeof(uint32_t) << k;
+    static bool configured = false;
+    if (!configured) {
+        DV_CUDA(cudaFuncSetAttribute(k_dif_pass<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        configured = true;
+    }
+    const unsigned groups = 1u << (logn - k);
+    k_dif_pass<THREADS><<<groups, THREADS, smem, st>>>(in, work, logn, s0, k, tw, first, pre_hi, pre_lo, split,
+                                                       consts, bad);
+    DV_LAUNCH();
+}
+
+}  // namespace
+
+void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, int kind, cudaStream_t st) {
+    if (logn < 0 || logn > NTT_MAX_LOG || kind < 0 || kind > 3) throw InvalidArgument("invalid NTT size or kind");
+    const uint64_t n = 1ull << logn;
+    const bool inverse = kind & 1, coset = kind >= 2;
+    const int split = (logn + 1) / 2;
+    const int key = logn * 4 + kind;
+    auto it = ws.tables.find(key);
+    NttTables* tab;
+    Fr* kc;
+    if (it == ws.tables.end()) {
+        auto t = std::make_unique<NttTables>();
+        t->split = split;
+        kc = t->consts.as<Fr>(C_COUNT);
+        k_setup_consts<<<1, 1, 0, st>>>(logn, inverse ? 1 : 0, split, kc);
+        DV_LAUNCH();
+        const uint64_t half = std::max<uint64_t>(1, n / 2);
+        Fr* tw = t->tw.as<Fr>(half);
+        const uint32_t chunk = 64;
+        const uint64_t threads = (half + chunk - 1) / chunk;
+        k_pow_table<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(kc + C_W, nullptr, half, chunk, 0, tw);
+        DV_LAUNCH();
+        if (coset) {
+            const uint64_t nlo = 1ull << split, nhi = (n + nlo - 1) >> split;
+            if (!inverse) {
+                Fr* hi = t->pre_hi.as<Fr>(nhi);
+                Fr* lo = t->pre_lo.as<Fr>(nlo);
+                k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(kc + C_G_SPLIT, kc + C_R, nhi, 1, 0, hi);
+                DV_LAUNCH();
+                k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(kc + C_G, nullptr, nlo, 1, 0, lo);
+                DV_LAUNCH();
+            } else {
+                Fr* hi = t->post_hi.as<Fr>(nhi);
+                Fr* lo = t->post_lo.as<Fr>(nlo);
+                k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(kc + C_GINV_SPLIT, kc + C_NINV, nhi, 1, 0,
+                                                                          hi);
+                DV_LAUNCH();
+                k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(kc + C_GINV, nullptr, nlo, 1, 1, lo);
+                DV_LAUNCH();
+            }
+        }
+        tab = t.get();
+        ws.tables[key] = std::move(t);
+    } else {
+        tab = it->second.get();
+        kc = tab->consts.as<Fr>(C_COUNT);
+    }
+    Fr* work = ws.work.as<Fr>(n);
+    uint32_t* bad = ws.err.as<uint32_t>(1);
+    DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
+
+    const Fr* tw = tab->tw.as<Fr>(1);
+    if (logn == 0) {
+        // single element: conversion round trip checks canonical form
+        launch_pass<32>(d_in, work, 0, 0, 0, tw, 1, nullptr, nullptr, split, kc, bad, st);
+    } else {
+        const int passes = (logn + 10) / 11;
+        int s0 = 0;
+        for (int p = 0; p < passes; ++p) {
+            const int k = logn / passes + (p < logn % passes ? 1 : 0);
+            const Fr* pre_hi = (coset && !inverse) ? tab->pre_hi.as<Fr>(1) : nullptr;
+            const Fr* pre_lo = (coset && !inverse) ? tab->pre_lo.as<Fr>(1) : nullptr;
+            if (k >= 9) launch_pass<256>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, kc, bad, st);
+            else launch_pass<64>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, kc, bad, st);
+            s0 += k;
+        }
+    }
+    const Fr* post_hi = (coset && inverse) ? tab->post_hi.as<Fr>(1) : nullptr;
+    const Fr* post_lo = (coset && inverse) ? tab->post_lo.as<Fr>(1) : nullptr;
+    const Fr* post_const = inverse ? kc + C_NINV_CANON : kc + C_ONE_RAW;
+    k_permute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(work, d_out, logn, post_hi, post_lo, split, post_const);
+    DV_LAUNCH();
+    uint32_t host_bad = 0;
+    DV_CUDA(cudaMemcpyAsync(&host_bad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaStreamSynchronize(st));
+    if (host_bad != 0xffffffffu) throw InvalidArgument("non-canonical NTT input at index " + std::to_string(host_bad));
+    ws.calls++;
+    ws.elements += n;
+}
+
+}  // namespace dv

@@ -1,0 +1,53 @@
+// BN254 Fr number-theoretic transform on sm_100a.
+//
+// Semantics follow ark-poly 0.4 Radix2EvaluationDomain as used by the
+// reference CPU path (crates/gpu/src/lib.rs:99-118,
+// crates/protocol/src/dynaverse.rs:1157-1164) and the ICICLE wrapper
+// (crates/gpu/src/icicle.rs:429-456): natural order in and out, forward =
+// evaluations at w^i, inverse = coefficients scaled by 1/n, w = the 2^28-th
+// root GENERATOR^((r-1)/2^28) (GENERATOR = 5) squared down to order n.
+// Coset forms use the offset g = 5: forward scales coefficient j by g^j
+// before the transform, inverse scales output i by g^-i after it.
+//
+// Layout: canonical little-endian 32-byte elements in HBM (the wire format),
+// converted to Montgomery form on load and back on store.  The transform is
+// decimation-in-frequency radix-2, grouped into passes of up to 11 stages;
+// each pass stages one group of 2^k elements (stride 2^low) in shared memory
+// as 8 word planes (bank-conflict free), runs its k butterfly stages there
+// with twiddles from a resident table w^i (i < n/2), and writes back.  A
+// final pass applies the bit-reversal permutation fused with the inverse
+// scaling and the conversion to canonical form.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+
+#include "engine.hpp"
+
+namespace dv {
+
+enum NttKind { NTT_FORWARD = 0, NTT_INVERSE = 1, NTT_COSET_FORWARD = 2, NTT_COSET_INVERSE = 3 };
+
+struct NttTables {
+    DevBuf tw;         // w^i, i < n/2 (Montgomery), w of order n (or w^-1 for inverse)
+    DevBuf pre_hi, pre_lo, post_hi, post_lo;  // two-level scaling tables
+    DevBuf consts;     // per-(size, kind) field constants
+    int split = 0;     // bits in the low table index
+};
+
+struct NttWorkspace {
+    DevBuf work;
+    DevBuf err;
+    std::map<int, std::unique_ptr<NttTables>> tables;  // key: logn * 4 + kind
+    uint64_t calls = 0, elements = 0;
+};
+
+constexpr int NTT_MAX_LOG = 26;
+
+// d_in, d_out: canonical elements (may alias).  Throws InvalidArgument for
+// non-canonical input (checked on device, reported after the transform).
+void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, int kind, cudaStream_t stream);
+
+}  // namespace dv
