@@ -214,6 +214,9 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
 
+    # window width for this size, measured (setup, not timed)
+    tuned_c, tune_log = b.autotune_msm(n)
+    torch.cuda.synchronize()
     for _ in range(args.warmup):
         result = b.msm_device(points.data_ptr(), scalars.data_ptr(), n, stream=s)
 
@@ -313,6 +316,7 @@ def main():
         "msm_roofline": {"algorithmic_macs": msm_macs, "achieved_tmacs": msm_macs / (ms_per_msm * 1e-3) / 1e12,
                          "frac": msm_macs / (ms_per_msm * 1e-3) / imad_peak},
         "phases_ms": phases,
+        "autotune": tune_log,
         "gpu_launches": launches,
         "clocks": clocks,
     }

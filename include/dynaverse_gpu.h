@@ -173,7 +173,13 @@ int dvgpu_bn254_g2_check_device(void* backend, const uint8_t* d_wire, size_t n, 
                                 uint32_t* d_masks, DvgpuG2ValidationReport* report_host, void* stream, char* error,
                                 size_t error_capacity);
 
-/* Tuning: force the Pippenger window width c (0 = cost-model choice). */
+/* Autotuner: times candidate window widths on seeded synthetic data of n
+ * points (G1 or G2) on this owner, stores the fastest for n's size class
+ * (ceil(log2 n)) and returns it; later MSMs of that class use it.  log_json
+ * receives the measured candidates as one JSON object. */
+int dvgpu_msm_autotune(void* backend, size_t n, int g2, int* best_c, char* log_json, size_t log_capacity,
+                       char* error, size_t error_capacity);
+/* Tuning: force the Pippenger window width c (0 = autotuned / cost-model choice). */
 int dvgpu_msm_set_window(void* backend, int c);
 int dvgpu_msm_get_window(void* backend, size_t points_per_set, int* c);
 
@@ -186,8 +192,10 @@ int dvgpu_probe_imad_rate(void* backend, double* macs_per_second, char* error, s
 uint64_t dvgpu_launch_count(void);
 /* Per-phase MSM device time, accumulated over calls while enabled (CUDA
  * events on the launching stream).  ms[]: 0 digit histogram, 1 offsets scan,
- * 2 scatter, 3 bucket accumulation, 4 split-bucket merge, 5 segment
- * reduction, 6 window sums, 7 tail (window D2H + host Horner).  enable = 1
+ * 2 scatter, 3 bucket accumulation (sum of its launches), 4 split-bucket
+ * merges plus the part of the first window group's reduction that overlaps
+ * the accumulation, 5 reduction tail of the last group, 6 unused, 7 tail
+ * (window D2H + host Horner).  enable = 1
  * resets and starts, 0 stops; out (may be NULL) receives the totals so far. */
 typedef struct DvgpuMsmPhaseTimes {
     double ms[8];

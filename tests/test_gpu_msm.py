@@ -160,3 +160,35 @@ def test_sparse_resident_matches_oracle(backend, oracle):
             backend.sparse_msm_resident(h, np.array([n], dtype=np.uint64), bytes(32), [0, 1])
     finally:
         backend.release_bases(h)
+
+
+def test_autotune_picks_a_window_and_results_stay_exact(dv, oracle):
+    with dv.DvgpuBackend() as b:
+        c, log = b.autotune_msm(4096)
+        assert 4 <= c <= 20 and log["best_c"] == c and len(log["candidates"]) >= 3
+        assert b.window_for(4096) == c
+        pts, scs = _case_inputs(oracle, 4242, 4000)
+        assert b.msm(pts, scs) == oracle.msm_g1(pts, scs)
+        c2, _ = b.autotune_msm(1000, g2=True)
+        pts2, scs2 = _case_inputs(oracle, 4343, 1000, g2=True)
+        assert b.msm_g2_host(pts2, scs2) == oracle.msm_g2(pts2, scs2)
+
+
+def test_skewed_digits_long_bucket_chains(backend, oracle):
+    """Buckets that span thousands of accumulation slices (every scalar equal)
+    and tiny top windows (c = 14 and 18 leave 2 bits in the top window)."""
+    n = 1 << 17
+    pts, _ = oracle.srs_g1(1717, n)
+    same = oracle.uniform_fr(1718, 1) * n
+    assert backend.msm(pts, same) == oracle.msm_g1(pts, same)
+    top = b"".join((((1 << 253) + (i % 3)) % (1 << 254)).to_bytes(32, "little") for i in range(n))
+    expect = oracle.msm_g1(pts, top)
+    rnd = oracle.uniform_fr(1719, n)
+    expect_rnd = oracle.msm_g1(pts, rnd)
+    for c in (14, 18):
+        backend.set_window(c)
+        try:
+            assert backend.msm(pts, top) == expect, f"c={c}"
+            assert backend.msm(pts, rnd) == expect_rnd, f"c={c}"
+        finally:
+            backend.set_window(0)

@@ -20,7 +20,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libdvgpu.so")
+LIB_PATH = os.environ.get("DVGPU_LIB_PATH", os.path.join(HERE, "lib", "libdvgpu.so"))
 
 FR_BYTES = 32
 G1_BYTES = 64
@@ -59,7 +59,7 @@ class MsmPhaseTimes(ctypes.Structure):
     _fields_ = [("ms", ctypes.c_double * 8), ("calls", ctypes.c_uint64), ("accum_mixed_adds", ctypes.c_uint64)]
 
 
-MSM_PHASE_NAMES = ["hist", "scan", "scatter", "accum", "fixup", "segments", "wsum", "tail"]
+MSM_PHASE_NAMES = ["hist", "scan", "scatter", "accum", "merge_and_overlapped_reduce", "reduce_tail", "unused", "tail"]
 
 
 class SetupStats(ctypes.Structure):
@@ -110,6 +110,7 @@ SIGNATURES = [
     ("dvgpu_msm_get_window", ctypes.c_int, [_P, _SZ, ctypes.POINTER(ctypes.c_int)]),
     ("dvgpu_probe_imad_rate", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)] + _E),
     ("dvgpu_launch_count", ctypes.c_uint64, []),
+    ("dvgpu_msm_autotune", ctypes.c_int, [_P, _SZ, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _B, _SZ] + _E),
     ("dvgpu_msm_timeline", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(MsmPhaseTimes)]),
     ("dvgpu_random_fr_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
     ("dvgpu_fr_powers_device", ctypes.c_int, [_P, _P, _SZ, _P, _P] + _E),
@@ -332,6 +333,14 @@ class DvgpuBackend:
     def set_window(self, c: int):
         if self._L.dvgpu_msm_set_window(self.handle, c) != 0:
             raise DvgpuError(-1, "invalid window width")
+
+    def autotune_msm(self, n: int, g2=False):
+        """Time candidate window widths for n points; returns (best_c, log dict)."""
+        import json
+        c = ctypes.c_int()
+        log = ctypes.create_string_buffer(8192)
+        self._call("dvgpu_msm_autotune", n, int(g2), ctypes.byref(c), log, len(log))
+        return c.value, json.loads(log.value.decode())
 
     def window_for(self, points_per_set: int) -> int:
         c = ctypes.c_int()

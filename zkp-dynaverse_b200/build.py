@@ -13,9 +13,10 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-BUILD = os.path.join(HERE, "_build")
-LIB_DIR = os.path.join(HERE, "lib")
-LIB = os.path.join(LIB_DIR, "libdvgpu.so")
+BUILD = os.environ.get("DVGPU_BUILD_DIR", os.path.join(HERE, "_build"))
+LIB = os.environ.get("DVGPU_LIB_OUT", os.path.join(HERE, "lib", "libdvgpu.so"))
+LIB_DIR = os.path.dirname(LIB)
+EXTRA = os.environ.get("DVGPU_EXTRA_FLAGS", "").split()
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -41,7 +42,7 @@ def build(verbose_ptxas=False, force=False):
         objs.append(obj)
         if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_time):
             continue
-        cmd = [NVCC] + ARCH + FLAGS + (["-Xptxas", "-v"] if verbose_ptxas else []) + ["-c", src, "-o", obj]
+        cmd = [NVCC] + ARCH + FLAGS + EXTRA + (["-Xptxas", "-v"] if verbose_ptxas else []) + ["-c", src, "-o", obj]
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
     failed = False
     for src, p in procs:

@@ -62,6 +62,18 @@ uint32_t read_err_word(Backend& b, uint32_t* d_word, cudaStream_t st) {
     return *h;
 }
 
+// Window width: an explicit dvgpu_msm_set_window wins, then the autotuned
+// width for the size class of the largest set, then the cost model (0).
+template <class F>
+int window_for(const Backend& b, const std::vector<uint32_t>& offs) {
+    if (b.force_c) return b.force_c;
+    uint32_t m = 0;
+    for (size_t k = 0; k + 1 < offs.size(); ++k) m = std::max(m, offs[k + 1] - offs[k]);
+    int cls = 0;
+    while ((1u << cls) < m && cls < 39) ++cls;
+    return (sizeof(F) == sizeof(Fq) ? b.tuned_c_g1 : b.tuned_c_g2)[cls];
+}
+
 // MSM over canonical device points/scalars, count sets (offsets host u32).
 template <class F>
 void msm_sets_device(Backend& b, const uint8_t* d_points, const uint8_t* d_scalars, const std::vector<uint32_t>& offs,
@@ -78,8 +90,8 @@ void msm_sets_device(Backend& b, const uint8_t* d_points, const uint8_t* d_scala
     uint32_t* bad = b.err.as<uint32_t>(1);
     DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
     convert_points<F>(d_points, conv, n, bad, st);
-    msm_run<F>(b.msm, conv, reinterpret_cast<const uint32_t*>(d_scalars), offs.data(), count, b.force_c, st,
-               tmp.data(), &b.msm_stats);
+    msm_run<F>(b.msm, conv, reinterpret_cast<const uint32_t*>(d_scalars), offs.data(), count, window_for<F>(b, offs),
+               st, tmp.data(), &b.msm_stats);
     const uint32_t first_bad = read_err_word(b, bad, st);
     if (first_bad != 0xffffffffu) throw InvalidArgument("invalid point at index " + std::to_string(first_bad));
     memcpy(result, tmp.data(), tmp.size());
@@ -218,6 +230,19 @@ __global__ void k_probe_madc(uint32_t seed, uint32_t iters, uint32_t* sink) {
 
 void Backend::release_all() noexcept {
     bases.clear();
+    MsmTimeline& tl = msm.timeline;
+    for (auto& e : tl.ev)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    for (auto& e : tl.acc_ev)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    tl.enabled = false;
+    if (msm.side) {
+        cudaStreamSynchronize(msm.side);
+        cudaStreamDestroy(msm.side);
+        msm.side = nullptr;
+        for (auto& e : msm.sync_ev)
+            if (e) { cudaEventDestroy(e); e = nullptr; }
+    }
     if (stream) {
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
@@ -438,7 +463,7 @@ extern "C" int dvgpu_bn254_msm_sparse_batch(void* opaque, uint64_t bases_handle,
         gather_points<Fq>(rb.points.view<G1A>(), rb.n, d_idx, k_total, gathered, bad, b.stream);
         std::vector<uint8_t> tmp(count * 64);
         msm_run<Fq>(b.msm, gathered, reinterpret_cast<const uint32_t*>(d_vals), offs.data(), (uint32_t)count,
-                    b.force_c, b.stream, tmp.data(), &b.msm_stats);
+                    window_for<Fq>(b, offs), b.stream, tmp.data(), &b.msm_stats);
         require(read_err_word(b, bad, b.stream) == 0xffffffffu, "sparse MSM index out of range");
         b.batch_stats.icicle_calls++;
         b.batch_stats.max_batch_size = std::max<uint64_t>(b.batch_stats.max_batch_size, count);
@@ -473,12 +498,12 @@ extern "C" int dvgpu_bn254_msm_resident(void* opaque, uint64_t bases_handle, con
         if (rb.g2) {
             uint8_t tmp[128];
             msm_run<Fq2>(b.msm, rb.points.view<G2A>(), reinterpret_cast<const uint32_t*>(d_scalars), offs.data(), 1,
-                         b.force_c, st, tmp, &b.msm_stats);
+                         window_for<Fq2>(b, offs), st, tmp, &b.msm_stats);
             memcpy(result_host, tmp, 128);
         } else {
             uint8_t tmp[64];
             msm_run<Fq>(b.msm, rb.points.view<G1A>(), reinterpret_cast<const uint32_t*>(d_scalars), offs.data(), 1,
-                        b.force_c, st, tmp, &b.msm_stats);
+                        window_for<Fq>(b, offs), st, tmp, &b.msm_stats);
             memcpy(result_host, tmp, 64);
         }
     });
@@ -494,7 +519,9 @@ extern "C" int dvgpu_msm_set_window(void* opaque, int c) {
 extern "C" int dvgpu_msm_get_window(void* opaque, size_t points, int* c) {
     auto* b = static_cast<Backend*>(opaque);
     if (!b || !c) return -1;
-    *c = msm_plan(points, b->force_c).c;
+    int cls = 0;
+    while ((1ull << cls) < points && cls < 39) ++cls;
+    *c = msm_plan(points, b->force_c ? b->force_c : b->tuned_c_g1[cls]).c;
     return 0;
 }
 
@@ -786,8 +813,10 @@ extern "C" int dvgpu_msm_timeline(void* opaque, int enable, DvgpuMsmPhaseTimes* 
             out->accum_mixed_adds = tl.accum_mixed_adds;
         }
         if (enable) {
-            if (!tl.ev[0])
+            if (!tl.ev[0]) {
                 for (auto& e : tl.ev) DV_CUDA(cudaEventCreate(&e));
+                for (auto& e : tl.acc_ev) DV_CUDA(cudaEventCreate(&e));
+            }
             for (auto& m : tl.ms) m = 0;
             tl.calls = 0;
             tl.accum_mixed_adds = 0;
@@ -814,5 +843,81 @@ extern "C" int dvgpu_fr_powers_device(void* opaque, const uint8_t* d_tau, size_t
     return guarded(opaque, error, cap, [&](Backend& b) {
         require(d_tau && (!n || d_out), "null buffers");
         dv::powers_launch(d_tau, n, d_out, pick(b, stream));
+    });
+}
+
+// ============================================================ autotuner
+namespace {
+int size_class(uint64_t n) {
+    int k = 0;
+    while ((1ull << k) < n) ++k;
+    return k;
+}
+
+template <class F>
+double time_msm(Backend& b, const Affine<F>* pts, const uint32_t* sc, uint32_t n, int c, int reps) {
+    const std::vector<uint32_t> offs = {0u, n};
+    std::vector<uint8_t> out(2 * sizeof(F));
+    cudaEvent_t e0, e1;
+    DV_CUDA(cudaEventCreate(&e0));
+    DV_CUDA(cudaEventCreate(&e1));
+    msm_run<F>(b.msm, pts, sc, offs.data(), 1, c, b.stream, out.data(), nullptr);  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < reps; ++r) {
+        DV_CUDA(cudaEventRecord(e0, b.stream));
+        msm_run<F>(b.msm, pts, sc, offs.data(), 1, c, b.stream, out.data(), nullptr);
+        DV_CUDA(cudaEventRecord(e1, b.stream));
+        DV_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        DV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+template <class F>
+int autotune(Backend& b, uint64_t n, std::string& log) {
+    const int g2 = sizeof(F) == sizeof(Fq) ? 0 : 1;
+    uint8_t* d_sc = b.in_scalars.as<uint8_t>(n * 32);
+    uint8_t* d_pts = b.in_points.as<uint8_t>(n * 2 * sizeof(F));
+    dv::random_fr_launch(0x5eed0000ull + n, n, d_sc, b.stream);
+    uint32_t* bad = b.err.as<uint32_t>(1);
+    DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), b.stream));
+    fixed_base_launch(b.fixed_base, d_sc, n, g2, d_pts, bad, b.stream);
+    dv::random_fr_launch(0x5eed1111ull + n, n, d_sc, b.stream);
+    Affine<F>* conv = b.conv_points.as<Affine<F>>(n);
+    convert_points<F>(d_pts, conv, n, bad, b.stream);
+    const int model = msm_plan(n, 0).c;
+    int best_c = model;
+    double best_ms = 1e300;
+    log += "{\"points\":" + std::to_string(n) + ",\"curve\":\"" + (g2 ? "G2" : "G1") +
+           "\",\"model_c\":" + std::to_string(model) + ",\"candidates\":[";
+    bool first = true;
+    for (int c = std::max(4, model - 3); c <= std::min(20, model + 2); ++c) {
+        const double ms = time_msm<F>(b, conv, reinterpret_cast<const uint32_t*>(d_sc), (uint32_t)n, c, 2);
+        log += std::string(first ? "" : ",") + "{\"c\":" + std::to_string(c) + ",\"ms\":" + std::to_string(ms) + "}";
+        first = false;
+        if (ms < best_ms) { best_ms = ms; best_c = c; }
+    }
+    log += "],\"best_c\":" + std::to_string(best_c) + "}";
+    return best_c;
+}
+}  // namespace
+
+extern "C" int dvgpu_msm_autotune(void* opaque, size_t n, int g2, int* best_c, char* log_json, size_t log_capacity,
+                                  char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(n >= 2 && n <= DVGPU_MAX_MSM_SIZE && (g2 == 0 || g2 == 1) && best_c, "invalid autotune arguments");
+        std::string log;
+        const int c = g2 ? autotune<Fq2>(b, n, log) : autotune<Fq>(b, n, log);
+        (g2 ? b.tuned_c_g2 : b.tuned_c_g1)[size_class(n)] = c;
+        *best_c = c;
+        if (log_json && log_capacity) {
+            const size_t k = std::min(log_capacity - 1, log.size());
+            memcpy(log_json, log.data(), k);
+            log_json[k] = '\0';
+        }
     });
 }

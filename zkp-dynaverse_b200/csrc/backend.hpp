@@ -48,6 +48,8 @@ struct Backend {
     DvgpuG2ValidationTraffic g2_traffic{};
     int setup_mode = 2;
     int force_c = 0;
+    int tuned_c_g1[40] = {};  // autotuned window width per ceil(log2(points per set))
+    int tuned_c_g2[40] = {};
 
     std::map<uint64_t, std::unique_ptr<ResidentBases>> bases;
     uint64_t next_handle = 1;

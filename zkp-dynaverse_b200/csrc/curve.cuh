@@ -57,6 +57,13 @@ struct XYZZ {
         return {x3, y3, F::mul(v, p.zz), F::mul(w, p.zzz)};
     }
 
+    // Rare case of add_affine: same x coordinate (doubling or P + (-P)), kept
+    // out of line so the hot accumulation loop stays small.
+    __device__ __noinline__ static XYZZ add_affine_equal_x(Affine<F> a, F r) {
+        if (r.is_zero()) return dbl_affine(a);
+        return inf();
+    }
+
     // p + a with a affine (madd-2008-s).
     DV_INL static XYZZ add_affine(const XYZZ& p, const Affine<F>& a) {
         if (a.is_inf()) return p;
@@ -65,10 +72,7 @@ struct XYZZ {
         const F s2 = F::mul(a.y, p.zzz);
         const F pp_ = F::sub(u2, p.x);
         const F r = F::sub(s2, p.y);
-        if (pp_.is_zero()) {
-            if (r.is_zero()) return dbl_affine(a);
-            return inf();
-        }
+        if (pp_.is_zero()) return add_affine_equal_x(a, r);
         const F pp = F::sqr(pp_);
         const F ppp = F::mul(pp_, pp);
         const F q = F::mul(p.x, pp);

@@ -50,41 +50,104 @@ __global__ void k_hist(const uint32_t* __restrict__ scalars, uint32_t n, const u
     }
     const uint32_t set = count > 1 ? set_of(set_off, count, i) : 0;
     const uint32_t B = 1u << (c - 1), full = 1u << c;
-    uint32_t* base = counts + (size_t)set * W * B;
+    const uint32_t base = set * (uint32_t)W * B;
+    const uint32_t active = __activemask();
+    const uint32_t lane = threadIdx.x & 31;
     uint32_t carry = 0;
     for (int w = 0; w < W; ++w) {
         const uint32_t d = window_raw(s, w * c, c) + carry;
         const bool neg = d > B;
         const uint32_t mag = neg ? full - d : d;
         carry = neg ? 1u : 0u;
-        if (mag) atomicAdd(base + (size_t)w * B + mag - 1, 1u);
+        // Warp-aggregated increment: lanes hitting the same bucket (skewed
+        // digits, e.g. a top window with few bits) issue one atomic.
+        const uint32_t key = mag ? base + (uint32_t)w * B + mag - 1 : NO_INDEX;
+        const uint32_t peers = __match_any_sync(active, key);
+        if (key != NO_INDEX && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(counts + key, (uint32_t)__popc(peers));
     }
 }
 
-// 2. Exclusive scan of counts (one block of 1024 threads).
-__global__ void __launch_bounds__(1024) k_scan(const uint32_t* __restrict__ counts, uint32_t nb,
-                                               uint32_t* __restrict__ offsets, uint32_t* __restrict__ cursor) {
-    __shared__ uint32_t part[1024];
-    const uint32_t t = threadIdx.x;
-    const uint32_t per = (nb + 1023) / 1024;
-    const uint32_t lo = min(nb, t * per), hi = min(nb, lo + per);
-    uint32_t local = 0;
-    for (uint32_t i = lo; i < hi; ++i) local += counts[i];
-    part[t] = local;
+// 2. Exclusive scan of the counts: tiles of 4096 (1024 threads x 4), three
+// passes -- tile sums, scan of the tile sums, per-tile scan with its prefix.
+constexpr uint32_t SCAN_TILE = 4096;
+
+// Exclusive scan of one value per thread over a 1024-thread block.
+DV_INL uint32_t block_exclusive_scan(uint32_t v, uint32_t* block_total) {
+    __shared__ uint32_t warp_sums[32];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= (uint32_t)d) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
     __syncthreads();
-    for (uint32_t d = 1; d < 1024; d <<= 1) {
-        const uint32_t v = t >= d ? part[t - d] : 0;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
+    if (wid == 0) {
+        uint32_t s = warp_sums[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, s, d);
+            if (lane >= (uint32_t)d) s += y;
+        }
+        warp_sums[lane] = s;
     }
-    uint32_t run = part[t] - local;  // exclusive prefix
+    __syncthreads();
+    const uint32_t prefix = (wid ? warp_sums[wid - 1] : 0u) + x - v;
+    if (block_total) *block_total = warp_sums[31];
+    __syncthreads();
+    return prefix;
+}
+
+DV_INL void load4(const uint32_t* counts, uint32_t nb, uint32_t i, uint32_t* v) {
+    if (i + 3 < nb) {
+        const uint4 q = *reinterpret_cast<const uint4*>(counts + i);
+        v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    } else {
+        for (int k = 0; k < 4; ++k) v[k] = i + k < nb ? counts[i + k] : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tiles(const uint32_t* __restrict__ counts, uint32_t nb,
+                                                     uint32_t* __restrict__ tile_sums) {
+    const uint32_t i = blockIdx.x * SCAN_TILE + threadIdx.x * 4;
+    uint32_t v[4];
+    load4(counts, nb, i, v);
+    uint32_t total;
+    block_exclusive_scan(v[0] + v[1] + v[2] + v[3], &total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_top(uint32_t* __restrict__ tile_sums, uint32_t ntiles,
+                                                   uint32_t* __restrict__ grand_total) {
+    const uint32_t per = (ntiles + 1023) / 1024;
+    const uint32_t lo = min(ntiles, threadIdx.x * per), hi = min(ntiles, lo + per);
+    uint32_t local = 0;
+    for (uint32_t i = lo; i < hi; ++i) local += tile_sums[i];
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(local, &total);
     for (uint32_t i = lo; i < hi; ++i) {
-        offsets[i] = run;
-        cursor[i] = run;
-        run += counts[i];
+        const uint32_t v = tile_sums[i];
+        tile_sums[i] = run;
+        run += v;
     }
-    if (t == 1023) offsets[nb] = part[1023];
+    if (threadIdx.x == 0) *grand_total = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict__ counts, uint32_t nb,
+                                                     const uint32_t* __restrict__ tile_prefix,
+                                                     uint32_t* __restrict__ offsets, uint32_t* __restrict__ cursor) {
+    const uint32_t i = blockIdx.x * SCAN_TILE + threadIdx.x * 4;
+    uint32_t v[4];
+    load4(counts, nb, i, v);
+    uint32_t run = tile_prefix[blockIdx.x] + block_exclusive_scan(v[0] + v[1] + v[2] + v[3], nullptr);
+    for (int k = 0; k < 4; ++k) {
+        if (i + k < nb) {
+            offsets[i + k] = run;
+            cursor[i + k] = run;
+        }
+        run += v[k];
+    }
 }
 
 // 3. Scatter (point index | sign << 31) into bucket order.
@@ -97,36 +160,50 @@ __global__ void k_scatter(const uint32_t* __restrict__ scalars, uint32_t n, cons
     if (!Fr::is_canonical(s)) return;
     const uint32_t set = count > 1 ? set_of(set_off, count, i) : 0;
     const uint32_t B = 1u << (c - 1), full = 1u << c;
-    uint32_t* base = cursor + (size_t)set * W * B;
+    const uint32_t base = set * (uint32_t)W * B;
+    const uint32_t active = __activemask();
+    const uint32_t lane = threadIdx.x & 31;
     uint32_t carry = 0;
     for (int w = 0; w < W; ++w) {
         const uint32_t d = window_raw(s, w * c, c) + carry;
         const bool neg = d > B;
         const uint32_t mag = neg ? full - d : d;
         carry = neg ? 1u : 0u;
-        if (mag) {
-            const uint32_t pos = atomicAdd(base + (size_t)w * B + mag - 1, 1u);
+        const uint32_t key = mag ? base + (uint32_t)w * B + mag - 1 : NO_INDEX;
+        const uint32_t peers = __match_any_sync(active, key);
+        if (key != NO_INDEX) {
+            // one atomic per group of lanes with the same bucket; each lane
+            // takes its rank within the group
+            const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+            uint32_t pos = 0;
+            if (lane == leader) pos = atomicAdd(cursor + key, (uint32_t)__popc(peers));
+            pos = __shfl_sync(peers, pos, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
             sorted[pos] = i | (neg ? 0x80000000u : 0u);
         }
     }
 }
 
 // 4. Balanced accumulation over the sorted list.
+#ifndef DV_ACCUM_MINB
+#define DV_ACCUM_MINB 4
+#endif
 template <class F>
-__global__ void __launch_bounds__(128) k_accum(const Affine<F>* __restrict__ pts, const uint32_t* __restrict__ sorted,
+__global__ void __launch_bounds__(128, DV_ACCUM_MINB) k_accum(const Affine<F>* __restrict__ pts, const uint32_t* __restrict__ sorted,
                                                const uint32_t* __restrict__ offsets, uint32_t nb,
                                                XYZZ<F>* __restrict__ buckets, int* __restrict__ pgid,
                                                XYZZ<F>* __restrict__ ppt) {
+    // buckets [0, nb) of this launch cover sorted positions [offsets[0], offsets[nb])
     const uint32_t T = gridDim.x * blockDim.x;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t M = offsets[nb];
+    const uint32_t M0 = offsets[0];
+    const uint32_t M = offsets[nb] - M0;
     const uint32_t L = (M + T - 1) / T;
     int head_gid = -1, tail_gid = -1;
     XYZZ<F> head = XYZZ<F>::inf(), tail = XYZZ<F>::inf();
-    const uint64_t start64 = (uint64_t)t * L;
-    if (L && start64 < M) {
-        const uint32_t start = (uint32_t)start64;
-        const uint32_t end = min(M, start + L);
+    const uint64_t rel64 = (uint64_t)t * L;
+    if (L && rel64 < M) {
+        const uint32_t start = M0 + (uint32_t)rel64;
+        const uint32_t end = M0 + min(M, (uint32_t)rel64 + L);
         uint32_t lo = 0, hi = nb;  // offsets[lo] <= start < offsets[hi]
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;
@@ -164,64 +241,118 @@ __global__ void __launch_bounds__(128) k_accum(const Affine<F>* __restrict__ pts
 
 // 5. Merge partials of buckets that span slices.  The owner of bucket g is
 // the slice whose tail holds g; the following slices hold g in their heads.
+// Chains of more than FIX_SHORT heads (a bucket spanning many slices: skewed
+// digits) are queued for k_fixup_long, which merges them with a block-wide
+// tree instead of one serial walk.
+constexpr uint32_t FIX_SHORT = 32;
+
 template <class F>
 __global__ void k_fixup(const int* __restrict__ pgid, const XYZZ<F>* __restrict__ ppt, uint32_t T,
-                        XYZZ<F>* __restrict__ buckets) {
+                        XYZZ<F>* __restrict__ buckets, uint32_t* __restrict__ long_list,
+                        uint32_t* __restrict__ long_count) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     const int g = pgid[2 * t + 1];
     if (g < 0) return;
+    uint32_t end = t + 1;
+    while (end < T && pgid[2 * end] == g && end - t <= FIX_SHORT) ++end;
+    if (end < T && pgid[2 * end] == g) {
+        long_list[atomicAdd(long_count, 1u)] = t;
+        return;
+    }
     XYZZ<F> acc = ppt[2 * t + 1];
-    for (uint32_t k = t + 1; k < T && pgid[2 * k] == g; ++k) acc = XYZZ<F>::add(acc, ppt[2 * k]);
+    for (uint32_t k = t + 1; k < end; ++k) acc = XYZZ<F>::add(acc, ppt[2 * k]);
     buckets[g] = acc;
 }
 
-// 6. Segment values: for segment j of window (set, w), with buckets
-// b in [j s, (j+1) s) weighted by (b + 1):
-//   V_j = sum_b (b - j s + 1) B_b  +  (j s) * sum_b B_b
+template <class F, int TH>
+__global__ void __launch_bounds__(TH) k_fixup_long(const int* __restrict__ pgid, const XYZZ<F>* __restrict__ ppt,
+                                                   uint32_t T, XYZZ<F>* __restrict__ buckets,
+                                                   const uint32_t* __restrict__ long_list,
+                                                   const uint32_t* __restrict__ long_count) {
+    __shared__ XYZZ<F> sh[TH];
+    if (blockIdx.x >= *long_count) return;
+    const uint32_t t0 = long_list[blockIdx.x];
+    const int g = pgid[2 * t0 + 1];
+    XYZZ<F> acc = threadIdx.x == 0 ? ppt[2 * t0 + 1] : XYZZ<F>::inf();
+    // the heads of g are contiguous from t0 + 1: stop at the first other key
+    for (uint32_t k = t0 + 1 + threadIdx.x; k < T && pgid[2 * k] == g; k += TH) acc = XYZZ<F>::add(acc, ppt[2 * k]);
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int d = TH / 2; d > 0; d >>= 1) {
+        if ((int)threadIdx.x < d) sh[threadIdx.x] = XYZZ<F>::add(sh[threadIdx.x], sh[threadIdx.x + d]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) buckets[g] = sh[0];
+}
+
+// 6. Bucket reduction, level 1.  Window (set, w) needs
+//      S_w = sum_b (b + 1) B_b,   b < 2^(c-1).
+// Segment j holds buckets [j s, (j+1) s); a running sum from the top gives
+//      U_j = sum_i (i + 1) B_{js+i},   R_j = sum_i B_{js+i},
+// and S_w = sum_j U_j + s * sum_j j R_j   (combined by k_wlevel).
 template <class F>
 __global__ void __launch_bounds__(128) k_segments(const XYZZ<F>* __restrict__ buckets, const uint32_t* __restrict__ offsets,
-                                                  uint32_t B, uint32_t NW, int seg_log, XYZZ<F>* __restrict__ segs) {
+                                                  uint32_t B, uint32_t NW, int seg_log, XYZZ<F>* __restrict__ seg_u,
+                                                  XYZZ<F>* __restrict__ seg_r) {
     const uint32_t S = B >> seg_log;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= NW * S) return;
     const uint32_t w = tid / S, j = tid % S;
     const uint32_t s = 1u << seg_log;
-    XYZZ<F> R = XYZZ<F>::inf(), Tsum = XYZZ<F>::inf();
+    XYZZ<F> R = XYZZ<F>::inf(), U = XYZZ<F>::inf();
     const size_t base = (size_t)w * B + (size_t)j * s;
     for (int b = (int)s - 1; b >= 0; --b) {
         const size_t g = base + b;
         if (offsets[g + 1] != offsets[g]) R = XYZZ<F>::add(R, buckets[g]);
-        Tsum = XYZZ<F>::add(Tsum, R);
+        U = XYZZ<F>::add(U, R);
     }
-    // (j s) * R = (j * R) doubled seg_log times
-    XYZZ<F> jr = XYZZ<F>::inf();
-    if (j && !R.is_inf()) {
-        const int top = 31 - __clz(j);
-        for (int bit = top; bit >= 0; --bit) {
-            jr = XYZZ<F>::dbl(jr);
-            if ((j >> bit) & 1) jr = XYZZ<F>::add(jr, R);
-        }
-        for (int k = 0; k < seg_log; ++k) jr = XYZZ<F>::dbl(jr);
-    }
-    segs[tid] = XYZZ<F>::add(Tsum, jr);
+    seg_u[tid] = U;
+    seg_r[tid] = R;
 }
 
-// 7. Sum of the S segment values of each (set, window): one block each.
-template <class F, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_wsum(const XYZZ<F>* __restrict__ segs, uint32_t S,
-                                                  XYZZ<F>* __restrict__ out) {
-    __shared__ XYZZ<F> sh[THREADS];
-    const uint32_t w = blockIdx.x, t = threadIdx.x;
-    XYZZ<F> acc = XYZZ<F>::inf();
-    for (uint32_t j = t; j < S; j += THREADS) acc = XYZZ<F>::add(acc, segs[(size_t)w * S + j]);
-    sh[t] = acc;
+// 7. Bucket reduction, upper levels.  Each window is carried as a pair of
+// vectors (U, R) of length S with a power-of-two multiplier m:
+//      S_w = sum_j U_j + m * sum_j j R_j .
+// A level splits each window into blocks of P entries; block k (entries
+// j = k P + t) replaces its P pairs by one pair
+//      U'_k = sum_t ( U_t + m Suf_{t+1} ),   R'_k = sum_t R_t ,
+// where Suf is the block's suffix sum of R (so sum_t t R_t = sum_t Suf_{t+1}),
+// and the multiplier becomes m P.  Levels repeat until one entry per window
+// remains, which is S_w.  Depth per level: log2 P (scan) + log2 m
+// (doublings) + log2 P (tree).
+template <class F, int P>
+__global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, const XYZZ<F>* __restrict__ r_in,
+                                              uint32_t S, int log_m, XYZZ<F>* __restrict__ u_out,
+                                              XYZZ<F>* __restrict__ r_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    XYZZ<F>* sh = reinterpret_cast<XYZZ<F>*>(smem_raw);
+    const uint32_t nblk = S > (uint32_t)P ? S / P : 1u;
+    const uint32_t w = blockIdx.x / nblk, k = blockIdx.x % nblk;
+    const uint32_t width = S < (uint32_t)P ? S : (uint32_t)P;
+    const uint32_t t = threadIdx.x;
+    const size_t idx = (size_t)w * S + (size_t)k * P + t;
+    const bool live = t < width;
+    sh[t] = live ? r_in[idx] : XYZZ<F>::inf();
     __syncthreads();
-    for (int d = THREADS / 2; d > 0; d >>= 1) {
-        if ((int)t < d) sh[t] = XYZZ<F>::add(sh[t], sh[t + d]);
+    for (uint32_t d = 1; d < width; d <<= 1) {
+        const XYZZ<F> o = t + d < width ? sh[t + d] : XYZZ<F>::inf();
+        __syncthreads();
+        if (t + d < width) sh[t] = XYZZ<F>::add(sh[t], o);
         __syncthreads();
     }
-    if (t == 0) out[w] = sh[0];
+    XYZZ<F> x = t + 1 < width ? sh[t + 1] : XYZZ<F>::inf();  // Suf_{t+1}
+    if (t == 0) r_out[blockIdx.x] = sh[0];                     // sum of the block's R
+    __syncthreads();
+    for (int i = 0; i < log_m; ++i) x = XYZZ<F>::dbl(x);
+    if (live) x = XYZZ<F>::add(x, u_in[idx]);
+    sh[t] = x;
+    __syncthreads();
+    for (uint32_t d = (uint32_t)P / 2; d > 0; d >>= 1) {
+        if (t < d) sh[t] = XYZZ<F>::add(sh[t], sh[t + d]);
+        __syncthreads();
+    }
+    if (t == 0) u_out[blockIdx.x] = sh[0];
 }
 
 // Canonical -> Montgomery conversion with validation.
@@ -317,7 +448,7 @@ MsmPlan msm_plan(uint64_t n, int force_c) {
     p.c = force_c ? force_c : best_c;
     p.windows = (255 + p.c - 1) / p.c;
     p.buckets = 1u << (p.c - 1);
-    p.seg_log = std::min(4, p.c - 1);
+    p.seg_log = std::min(3, p.c - 1);
     return p;
 }
 
@@ -356,7 +487,7 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         plan.c--;
         plan.windows = (255 + plan.c - 1) / plan.c;
         plan.buckets = 1u << (plan.c - 1);
-        plan.seg_log = std::min(4, plan.c - 1);
+        plan.seg_log = std::min(3, plan.c - 1);
     }
     if ((uint64_t)count * plan.windows * plan.buckets > (1ull << 31) || (uint64_t)n * plan.windows > 0xffffffffull)
         throw InvalidArgument("MSM batch too large for one launch sequence");
@@ -386,8 +517,16 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
     k_hist<<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_counts, d_err);
     DV_LAUNCH();
     mark(1);
-    k_scan<<<1, 1024, 0, st>>>(d_counts, NB, d_offsets, d_cursor);
-    DV_LAUNCH();
+    {
+        const uint32_t ntiles = (NB + SCAN_TILE - 1) / SCAN_TILE;
+        uint32_t* d_tiles = ws.scan_tiles.as<uint32_t>(ntiles);
+        k_scan_tiles<<<ntiles, 1024, 0, st>>>(d_counts, NB, d_tiles);
+        DV_LAUNCH();
+        k_scan_top<<<1, 1024, 0, st>>>(d_tiles, ntiles, d_offsets + NB);
+        DV_LAUNCH();
+        k_scan_apply<<<ntiles, 1024, 0, st>>>(d_counts, NB, d_tiles, d_offsets, d_cursor);
+        DV_LAUNCH();
+    }
     mark(2);
     k_scatter<<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_cursor, d_sorted);
     DV_LAUNCH();
@@ -403,23 +542,76 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
     const uint32_t T = grid * 128;
     int* d_pgid = ws.pgid.as<int>(2ull * T);
     XYZZ<F>* d_ppt = ws.ppt.as<XYZZ<F>>(2ull * T);
-    k_accum<F><<<grid, 128, 0, st>>>(d_points, d_sorted, d_offsets, NB, d_buckets, d_pgid, d_ppt);
-    DV_LAUNCH();
-    mark(4);
-    k_fixup<F><<<blocks_for(T, 128), 128, 0, st>>>(d_pgid, d_ppt, T, d_buckets);
-    DV_LAUNCH();
-    mark(5);
 
     const int seg_log = plan.seg_log;
     const uint32_t S = B >> seg_log;
-    XYZZ<F>* d_segs = ws.segs.as<XYZZ<F>>((size_t)NW * S);
+    XYZZ<F>* d_seg_u = ws.segs.as<XYZZ<F>>(4ull * NW * S);
+    XYZZ<F>* d_seg_r = d_seg_u + (size_t)NW * S;
+    XYZZ<F>* d_lvl_u = d_seg_r + (size_t)NW * S;  // ping-pong buffers of the upper levels
+    XYZZ<F>* d_lvl_r = d_lvl_u + (size_t)NW * S;
     XYZZ<F>* d_win = ws.windows.as<XYZZ<F>>(NW);
-    k_segments<F><<<blocks_for((uint64_t)NW * S, 128), 128, 0, st>>>(d_buckets, d_offsets, B, NW, seg_log, d_segs);
-    DV_LAUNCH();
-    mark(6);
-    k_wsum<F, 128><<<NW, 128, 0, st>>>(d_segs, S, d_win);
-    DV_LAUNCH();
-    mark(7);
+    constexpr int P = sizeof(F) == sizeof(Fq) ? 256 : 128;
+    const size_t smem = (size_t)P * sizeof(XYZZ<F>);
+    static bool smem_set = false;
+    if (!smem_set) {
+        DV_CUDA(cudaFuncSetAttribute(k_wlevel<F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_set = true;
+    }
+    if (!ws.side) {
+        DV_CUDA(cudaStreamCreateWithFlags(&ws.side, cudaStreamNonBlocking));
+        for (auto& e : ws.sync_ev) DV_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+
+    // Windows may be processed in groups, each group's reduction on the side
+    // stream.  Measured: the accumulation kernel occupies every SM, so a
+    // second group does not overlap and only lengthens the critical path;
+    // one group is used.
+    const uint32_t split = NW;
+    const uint32_t bounds[3] = {0, split, NW};
+    const int groups = split < NW ? 2 : 1;
+    for (int gi = 0; gi < groups; ++gi) {
+        const uint32_t w0 = bounds[gi], w1 = bounds[gi + 1];
+        const uint32_t gb0 = w0 * B, nbg = (w1 - w0) * B;
+        if (tl.enabled) DV_CUDA(cudaEventRecord(tl.acc_ev[2 * gi], st));
+        k_accum<F><<<grid, 128, 0, st>>>(d_points, d_sorted, d_offsets + gb0, nbg, d_buckets + gb0, d_pgid, d_ppt);
+        DV_LAUNCH();
+        if (tl.enabled) DV_CUDA(cudaEventRecord(tl.acc_ev[2 * gi + 1], st));
+        uint32_t* d_fix_count = ws.fix_count.as<uint32_t>(1);
+        uint32_t* d_fix_list = ws.fix_list.as<uint32_t>(T / FIX_SHORT + 1);
+        DV_CUDA(cudaMemsetAsync(d_fix_count, 0, sizeof(uint32_t), st));
+        k_fixup<F><<<blocks_for(T, 128), 128, 0, st>>>(d_pgid, d_ppt, T, d_buckets + gb0, d_fix_list, d_fix_count);
+        DV_LAUNCH();
+        k_fixup_long<F, 128><<<T / FIX_SHORT + 1, 128, 0, st>>>(d_pgid, d_ppt, T, d_buckets + gb0, d_fix_list,
+                                                                d_fix_count);
+        DV_LAUNCH();
+        DV_CUDA(cudaEventRecord(ws.sync_ev[gi], st));
+        DV_CUDA(cudaStreamWaitEvent(ws.side, ws.sync_ev[gi], 0));
+        k_segments<F><<<blocks_for((uint64_t)(w1 - w0) * S, 128), 128, 0, ws.side>>>(
+            d_buckets + gb0, d_offsets + gb0, B, w1 - w0, seg_log, d_seg_u + (size_t)w0 * S, d_seg_r + (size_t)w0 * S);
+        DV_LAUNCH();
+        // upper levels: (U, R) pairs with multiplier m = 2^log_m
+        XYZZ<F>* u = d_seg_u + (size_t)w0 * S;
+        XYZZ<F>* r = d_seg_r + (size_t)w0 * S;
+        XYZZ<F>* u2 = d_lvl_u + (size_t)w0 * S;
+        XYZZ<F>* r2 = d_lvl_r + (size_t)w0 * S;
+        uint32_t len = S;
+        int log_m = seg_log;
+        for (;;) {
+            const uint32_t nblk = len > (uint32_t)P ? len / P : 1u;
+            XYZZ<F>* u_dst = nblk == 1 ? d_win + w0 : u2;
+            k_wlevel<F, P><<<(w1 - w0) * nblk, P, smem, ws.side>>>(u, r, len, log_m, u_dst, r2);
+            DV_LAUNCH();
+            if (nblk == 1) break;
+            log_m += __builtin_ctz((unsigned)P);
+            len = nblk;
+            std::swap(u, u2);
+            std::swap(r, r2);
+        }
+    }
+    mark(4);  // main stream done with accumulation
+    DV_CUDA(cudaEventRecord(ws.sync_ev[2], ws.side));
+    DV_CUDA(cudaStreamWaitEvent(st, ws.sync_ev[2], 0));
+    mark(5);  // reduction joined
 
     XYZZ<F>* h_win = ws.host_windows.as<XYZZ<F>>(NW);
     DV_CUDA(cudaMemcpyAsync(h_win, d_win, (size_t)NW * sizeof(XYZZ<F>), cudaMemcpyDeviceToHost, st));
@@ -431,13 +623,22 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
     const auto* hw = reinterpret_cast<const dvh::XYZZ<HF>*>(h_win);
     for (uint32_t k = 0; k < count; ++k) horner(hw + (size_t)k * W, W, c, host_out + (size_t)k * out_bytes);
     if (tl.enabled) {
-        DV_CUDA(cudaEventRecord(tl.ev[8], st));
-        DV_CUDA(cudaEventSynchronize(tl.ev[8]));
-        for (int k = 0; k < MSM_PHASES; ++k) {
+        DV_CUDA(cudaEventRecord(tl.ev[6], st));
+        DV_CUDA(cudaEventSynchronize(tl.ev[6]));
+        auto span = [&](cudaEvent_t a, cudaEvent_t b) {
             float ms = 0;
-            DV_CUDA(cudaEventElapsedTime(&ms, tl.ev[k], tl.ev[k + 1]));
-            tl.ms[k] += ms;
-        }
+            DV_CUDA(cudaEventElapsedTime(&ms, a, b));
+            return (double)ms;
+        };
+        double acc = 0;
+        for (int gi = 0; gi < groups; ++gi) acc += span(tl.acc_ev[2 * gi], tl.acc_ev[2 * gi + 1]);
+        tl.ms[0] += span(tl.ev[0], tl.ev[1]);           // digit histogram
+        tl.ms[1] += span(tl.ev[1], tl.ev[2]);           // offsets scan
+        tl.ms[2] += span(tl.ev[2], tl.ev[3]);           // scatter
+        tl.ms[3] += acc;                                // bucket accumulation (all groups)
+        tl.ms[4] += span(tl.ev[3], tl.ev[4]) - acc;     // merges + overlapped reduction of group 0
+        tl.ms[5] += span(tl.ev[4], tl.ev[5]);           // reduction tail (last group)
+        tl.ms[7] += span(tl.ev[5], tl.ev[6]);           // window D2H + host Horner
         tl.calls++;
         tl.accum_mixed_adds += (uint64_t)n * W;
     }

@@ -42,19 +42,26 @@ struct MsmPlan {
 MsmPlan msm_plan(uint64_t points_per_set, int force_c);
 
 // Optional per-phase device timing (CUDA events on the launching stream).
-enum { MSM_PHASES = 8 };  // hist, scan, scatter, accum, fixup, segments, wsum, tail(D2H + host Horner)
+// Phases: 0 hist, 1 scan, 2 scatter, 3 accumulation, 4 split-bucket merges
+// plus the overlapped reduction of the first window group, 5 reduction tail
+// (last group), 6 unused, 7 window D2H + host Horner.
+enum { MSM_PHASES = 8 };
 struct MsmTimeline {
     bool enabled = false;
-    cudaEvent_t ev[MSM_PHASES + 1] = {};
+    cudaEvent_t ev[7] = {};
+    cudaEvent_t acc_ev[4] = {};
     double ms[MSM_PHASES] = {};
     uint64_t calls = 0;
     uint64_t accum_mixed_adds = 0;  // N * windows summed over timed calls (for the roofline)
 };
 
 struct MsmWorkspace {
-    DevBuf set_off, counts, offsets, cursor, sorted, buckets, pgid, ppt, segs, windows, err;
+    DevBuf set_off, counts, offsets, cursor, scan_tiles, sorted, buckets, pgid, ppt, fix_list, fix_count, segs, windows,
+        err;
     PinnedBuf host_windows, host_err;
     MsmTimeline timeline;
+    cudaStream_t side = nullptr;       // bucket-reduction stream (created on first use)
+    cudaEvent_t sync_ev[3] = {};
 };
 
 struct MsmStats {

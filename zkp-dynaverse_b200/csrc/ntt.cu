@@ -118,9 +118,9 @@ __global__ void __launch_bounds__(THREADS) k_dif_pass(const uint8_t* __restrict_
             for (int j = 0; j < 8; ++j) a.v[j] = c[j];
             if (pre_hi) {
                 const uint64_t lo_mask = (1ull << split) - 1;
-                a = Fr::mul(Fr::mul(a, pre_hi[idx >> split]), pre_lo[idx & lo_mask]);
+                a = Fr::mul_inl(Fr::mul_inl(a, pre_hi[idx >> split]), pre_lo[idx & lo_mask]);
             } else {
-                a = Fr::mul(a, consts[C_R]);
+                a = Fr::mul_inl(a, consts[C_R]);
             }
         } else {
             a = work[idx];
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(THREADS) k_dif_pass(const uint8_t* __restrict_
             load_plane(sm, G, t1, v);
             const uint64_t jp = ((uint64_t)(t0 & (half - 1)) << lb) | low;
             const Fr x = Fr::add(u, v);
-            const Fr y = Fr::mul(Fr::sub(u, v), tw[jp << s]);
+            const Fr y = Fr::mul_inl(Fr::sub(u, v), tw[jp << s]);
             store_plane(sm, G, t0, x);
             store_plane(sm, G, t1, y);
         }
@@ -163,9 +163,9 @@ __global__ void k_permute(const Fr* __restrict__ work, uint8_t* __restrict__ out
     Fr a = work[r];
     if (post_hi) {
         const uint64_t lo_mask = (1ull << split) - 1;
-        a = Fr::mul(Fr::mul(a, post_hi[i >> split]), post_lo[i & lo_mask]);
+        a = Fr::mul_inl(Fr::mul_inl(a, post_hi[i >> split]), post_lo[i & lo_mask]);
     } else {
-        a = Fr::mul(a, *post_const);
+        a = Fr::mul_inl(a, *post_const);
     }
     store_words(out + 32 * i, a.v);
 }
