@@ -80,80 +80,159 @@ __global__ void k_pow_table(const Fr* __restrict__ base_p, const Fr* __restrict_
     }
 }
 
+// Shared-memory word planes: plane j holds word j of every element, padded
+// by one word per 32 elements so strided element access stays bank-free.
+DV_INL uint32_t plane_stride(uint32_t n) { return n + (n >> 5); }
 DV_INL void load_plane(const uint32_t* sm, uint32_t n, uint32_t t, Fr& a) {
+    const uint32_t ps = plane_stride(n), o = t + (t >> 5);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) a.v[j] = sm[j * n + t];
+    for (int j = 0; j < 8; ++j) a.v[j] = sm[j * ps + o];
 }
 DV_INL void store_plane(uint32_t* sm, uint32_t n, uint32_t t, const Fr& a) {
+    const uint32_t ps = plane_stride(n), o = t + (t >> 5);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) sm[j * n + t] = a.v[j];
+    for (int j = 0; j < 8; ++j) sm[j * ps + o] = a.v[j];
 }
 
-// One DIF pass over stages [s0, s0 + k).  first: convert canonical input
-// (with coset pre-scale if pre_hi != null) and check canonical form.
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS) k_dif_pass(const uint8_t* __restrict__ in, Fr* __restrict__ work, int logn,
+// One DIF pass over stages [s0, s0 + k) for one group of G = 2^k elements
+// (stride 2^lb in the vector).  Register-blocked: the k stages are processed
+// in rounds of up to R = 2^R_LOG elements per thread; a round loads R
+// elements that differ only in its bits, runs its radix-2 stages in
+// registers and writes them back, so shared memory (8 word planes, bank-
+// conflict free) is touched once per round rather than once per stage.  The
+// first round reads global memory directly (first pass: canonical check and
+// coset pre-scale), the last round writes global memory directly.
+// One round of RR stages: thread-group tau owns the 2^RR elements that differ
+// only in local bits [bit_hi - RR, bit_hi).  RR is a compile-time constant so
+// the element array stays in registers.
+template <int RR, int THREADS>
+DV_INL void dif_round(const uint8_t* __restrict__ in, Fr* __restrict__ work, uint32_t* sm, int logn, int s0, int k,
+                      int lb, uint64_t low, uint64_t high, int bit_hi, bool first_round, bool first,
+                      const Fr* __restrict__ tw, const Fr* __restrict__ pre_hi, const Fr* __restrict__ pre_lo,
+                      int split, uint32_t* __restrict__ first_bad) {
+    constexpr int R = 1 << RR;
+    const uint32_t G = 1u << k;
+    const int b_lo = bit_hi - RR;
+    const bool last_round = b_lo == 0;
+    const uint32_t lanes = G >> RR;
+    for (uint32_t tau = threadIdx.x; tau < lanes; tau += THREADS) {
+        const uint32_t base_e = ((tau >> b_lo) << bit_hi) | (tau & ((1u << b_lo) - 1));
+        Fr x[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const uint32_t e = base_e | ((uint32_t)m << b_lo);
+            const uint64_t idx = (high << (lb + k)) | ((uint64_t)e << lb) | low;
+            if (first_round) {
+                if (first) {
+                    uint32_t c[8];
+                    load_words(in + 32 * idx, c);
+                    if (!Fr::is_canonical(c)) {
+                        atomicMin(first_bad, (uint32_t)idx);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) c[j] = 0;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) x[m].v[j] = c[j];
+                    // values stay canonical: multipliers are held in
+                    // Montgomery form and mont_mul(a, x R) = a x
+                    if (pre_hi) {
+                        const uint64_t lo_mask = (1ull << split) - 1;
+                        x[m] = Fr::mul_inl(Fr::mul_inl(x[m], pre_hi[idx >> split]), pre_lo[idx & lo_mask]);
+                    }
+                } else {
+                    x[m] = work[idx];
+                }
+            } else {
+                load_plane(sm, G, e, x[m]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < RR; ++j) {
+            const int s = s0 + (k - bit_hi) + j;  // global stage
+            const int pb = bit_hi - 1 - j;        // local bit of this stage
+            const int hs = 1 << (RR - 1 - j);    // pair distance in m
+            // issue this stage's twiddle loads before its butterflies
+            Fr w[R / 2];
+#pragma unroll
+            for (int m = 0, q = 0; m < R; ++m) {
+                if (m & hs) continue;
+                const uint32_t e = base_e | ((uint32_t)m << b_lo);
+                const uint64_t jp = ((uint64_t)(e & ((1u << pb) - 1)) << lb) | low;
+                w[q++] = tw[jp << s];
+            }
+#pragma unroll
+            for (int m = 0, q = 0; m < R; ++m) {
+                if (m & hs) continue;
+                const Fr u = x[m], v = x[m + hs];
+                x[m] = Fr::add(u, v);
+                x[m + hs] = Fr::mul_inl(Fr::sub(u, v), w[q++]);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const uint32_t e = base_e | ((uint32_t)m << b_lo);
+            if (last_round) {
+                const uint64_t idx = (high << (lb + k)) | ((uint64_t)e << lb) | low;
+                work[idx] = x[m];
+            } else {
+                store_plane(sm, G, e, x[m]);
+            }
+        }
+    }
+}
+
+template <int THREADS, int R_LOG>
+#ifndef DV_NTT_MINB
+#define DV_NTT_MINB 3
+#endif
+#ifndef DV_NTT_RADIX_LOG
+#define DV_NTT_RADIX_LOG 2
+#endif
+__global__ void __launch_bounds__(THREADS, (THREADS >= 256 ? DV_NTT_MINB : 8)) k_dif_pass(const uint8_t* __restrict__ in, Fr* __restrict__ work, int logn,
                                                       int s0, int k, const Fr* __restrict__ tw, int first,
                                                       const Fr* __restrict__ pre_hi, const Fr* __restrict__ pre_lo,
-                                                      int split, const Fr* __restrict__ consts,
-                                                      uint32_t* __restrict__ first_bad) {
+                                                      int split, uint32_t* __restrict__ first_bad) {
     extern __shared__ uint32_t sm[];
-    const uint32_t G = 1u << k;
     const int lb = logn - s0 - k;
     const uint64_t g = blockIdx.x;
     const uint64_t low = g & ((1ull << lb) - 1), high = g >> lb;
     const uint32_t tid = threadIdx.x;
-    for (uint32_t t = tid; t < G; t += THREADS) {
-        const uint64_t idx = (high << (lb + k)) | ((uint64_t)t << lb) | low;
-        Fr a;
-        if (first) {
-            uint32_t c[8];
-            load_words(in + 32 * idx, c);
-            if (!Fr::is_canonical(c)) {
-                atomicMin(first_bad, (uint32_t)idx);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) c[j] = 0;
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) a.v[j] = c[j];
-            if (pre_hi) {
-                const uint64_t lo_mask = (1ull << split) - 1;
-                a = Fr::mul_inl(Fr::mul_inl(a, pre_hi[idx >> split]), pre_lo[idx & lo_mask]);
-            } else {
-                a = Fr::mul_inl(a, consts[C_R]);
-            }
-        } else {
-            a = work[idx];
-        }
-        store_plane(sm, G, t, a);
-    }
-    __syncthreads();
-    for (int l = 0; l < k; ++l) {
-        const int s = s0 + l;
-        const uint32_t half = 1u << (k - 1 - l);
-        for (uint32_t b = tid; b < G / 2; b += THREADS) {
-            const uint32_t t0 = ((b >> (k - 1 - l)) << (k - l)) | (b & (half - 1));
-            const uint32_t t1 = t0 + half;
-            Fr u, v;
-            load_plane(sm, G, t0, u);
-            load_plane(sm, G, t1, v);
-            const uint64_t jp = ((uint64_t)(t0 & (half - 1)) << lb) | low;
-            const Fr x = Fr::add(u, v);
-            const Fr y = Fr::mul_inl(Fr::sub(u, v), tw[jp << s]);
-            store_plane(sm, G, t0, x);
-            store_plane(sm, G, t1, y);
-        }
+    int bit_hi = k;
+    bool first_round = true;
+    while (bit_hi > 0) {
+        const int rr = bit_hi < R_LOG ? bit_hi : R_LOG;
+        if (rr == 3 && R_LOG >= 3) dif_round<(R_LOG >= 3 ? 3 : 1), THREADS>(in, work, sm, logn, s0, k, lb, low, high, bit_hi, first_round, first, tw,
+                                           pre_hi, pre_lo, split, first_bad);
+        else if (rr == 2) dif_round<2, THREADS>(in, work, sm, logn, s0, k, lb, low, high, bit_hi, first_round, first,
+                                                tw, pre_hi, pre_lo, split, first_bad);
+        else dif_round<1, THREADS>(in, work, sm, logn, s0, k, lb, low, high, bit_hi, first_round, first, tw, pre_hi,
+                                   pre_lo, split, first_bad);
         __syncthreads();
+        bit_hi -= rr;
+        first_round = false;
     }
-    for (uint32_t t = tid; t < G; t += THREADS) {
-        const uint64_t idx = (high << (lb + k)) | ((uint64_t)t << lb) | low;
-        Fr a;
-        load_plane(sm, G, t, a);
-        work[idx] = a;
+    if (k == 0) {  // single element: copy (with the first pass's check)
+        if (tid == 0) {
+            const uint64_t idx = (high << lb) | low;
+            Fr a;
+            if (first) {
+                uint32_t c[8];
+                load_words(in + 32 * idx, c);
+                if (!Fr::is_canonical(c)) {
+                    atomicMin(first_bad, (uint32_t)idx);
+                    for (int j = 0; j < 8; ++j) c[j] = 0;
+                }
+                for (int j = 0; j < 8; ++j) a.v[j] = c[j];
+                if (pre_hi) a = Fr::mul_inl(Fr::mul_inl(a, pre_hi[0]), pre_lo[0]);
+            } else {
+                a = work[idx];
+            }
+            work[idx] = a;
+        }
     }
 }
 
-// Bit-reversal permutation + post scaling + conversion to canonical form.
+// Bit-reversal permutation + post scaling (values are already canonical).
 __global__ void k_permute(const Fr* __restrict__ work, uint8_t* __restrict__ out, int logn,
                           const Fr* __restrict__ post_hi, const Fr* __restrict__ post_lo, int split,
                           const Fr* __restrict__ post_const) {
@@ -164,7 +243,7 @@ __global__ void k_permute(const Fr* __restrict__ work, uint8_t* __restrict__ out
     if (post_hi) {
         const uint64_t lo_mask = (1ull << split) - 1;
         a = Fr::mul_inl(Fr::mul_inl(a, post_hi[i >> split]), post_lo[i & lo_mask]);
-    } else {
+    } else if (post_const) {
         a = Fr::mul_inl(a, *post_const);
     }
     store_words(out + 32 * i, a.v);
@@ -172,16 +251,15 @@ __global__ void k_permute(const Fr* __restrict__ work, uint8_t* __restrict__ out
 
 template <int THREADS>
 void launch_pass(const uint8_t* in, Fr* work, int logn, int s0, int k, const Fr* tw, int first, const Fr* pre_hi,
-                 const Fr* pre_lo, int split, const Fr* consts, uint32_t* bad, cudaStream_t st) {
-    const size_t smem = (size_t)8 * sizeof(uint32_t) << k;
+                 const Fr* pre_lo, int split, uint32_t* bad, cudaStream_t st) {
+    const size_t smem = (size_t)8 * sizeof(uint32_t) * ((1u << k) + ((1u << k) >> 5));
     static bool configured = false;
     if (!configured) {
-        DV_CUDA(cudaFuncSetAttribute(k_dif_pass<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        DV_CUDA(cudaFuncSetAttribute(k_dif_pass<THREADS, DV_NTT_RADIX_LOG>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
         configured = true;
     }
     const unsigned groups = 1u << (logn - k);
-    k_dif_pass<THREADS><<<groups, THREADS, smem, st>>>(in, work, logn, s0, k, tw, first, pre_hi, pre_lo, split,
-                                                       consts, bad);
+    k_dif_pass<THREADS, DV_NTT_RADIX_LOG><<<groups, THREADS, smem, st>>>(in, work, logn, s0, k, tw, first, pre_hi, pre_lo, split, bad);
     DV_LAUNCH();
 }
 
@@ -213,7 +291,7 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
             if (!inverse) {
                 Fr* hi = t->pre_hi.as<Fr>(nhi);
                 Fr* lo = t->pre_lo.as<Fr>(nlo);
-                k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(kc + C_G_SPLIT, kc + C_R, nhi, 1, 0, hi);
+                k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(kc + C_G_SPLIT, nullptr, nhi, 1, 0, hi);
                 DV_LAUNCH();
                 k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(kc + C_G, nullptr, nlo, 1, 0, lo);
                 DV_LAUNCH();
@@ -223,7 +301,7 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
                 k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(kc + C_GINV_SPLIT, kc + C_NINV, nhi, 1, 0,
                                                                           hi);
                 DV_LAUNCH();
-                k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(kc + C_GINV, nullptr, nlo, 1, 1, lo);
+                k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(kc + C_GINV, nullptr, nlo, 1, 0, lo);
                 DV_LAUNCH();
             }
         }
@@ -238,9 +316,11 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
     DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
 
     const Fr* tw = tab->tw.as<Fr>(1);
+    const Fr* pre_hi0 = (coset && !inverse) ? tab->pre_hi.as<Fr>(1) : nullptr;
+    const Fr* pre_lo0 = (coset && !inverse) ? tab->pre_lo.as<Fr>(1) : nullptr;
     if (logn == 0) {
         // single element: conversion round trip checks canonical form
-        launch_pass<32>(d_in, work, 0, 0, 0, tw, 1, nullptr, nullptr, split, kc, bad, st);
+        launch_pass<32>(d_in, work, 0, 0, 0, tw, 1, pre_hi0, pre_lo0, split, bad, st);
     } else {
         const int passes = (logn + 10) / 11;
         int s0 = 0;
@@ -248,14 +328,14 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
             const int k = logn / passes + (p < logn % passes ? 1 : 0);
             const Fr* pre_hi = (coset && !inverse) ? tab->pre_hi.as<Fr>(1) : nullptr;
             const Fr* pre_lo = (coset && !inverse) ? tab->pre_lo.as<Fr>(1) : nullptr;
-            if (k >= 9) launch_pass<256>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, kc, bad, st);
-            else launch_pass<64>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, kc, bad, st);
+            if (k >= 9) launch_pass<256>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, bad, st);
+            else launch_pass<64>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, bad, st);
             s0 += k;
         }
     }
     const Fr* post_hi = (coset && inverse) ? tab->post_hi.as<Fr>(1) : nullptr;
     const Fr* post_lo = (coset && inverse) ? tab->post_lo.as<Fr>(1) : nullptr;
-    const Fr* post_const = inverse ? kc + C_NINV_CANON : kc + C_ONE_RAW;
+    const Fr* post_const = inverse ? kc + C_NINV : nullptr;
     k_permute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(work, d_out, logn, post_hi, post_lo, split, post_const);
     DV_LAUNCH();
     uint32_t host_bad = 0;
