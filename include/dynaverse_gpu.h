@@ -179,6 +179,24 @@ int dvgpu_bn254_g2_check_device(void* backend, const uint8_t* d_wire, size_t n, 
  * receives the measured candidates as one JSON object. */
 int dvgpu_msm_autotune(void* backend, size_t n, int g2, int* best_c, char* log_json, size_t log_capacity,
                        char* error, size_t error_capacity);
+/* Allocation-free NTT (no counterpart in the reference).  For callers that
+ * must not allocate device memory when they need a transform -- code that
+ * runs while a caching allocator or memory pool owns device memory, a
+ * latency-critical path that cannot afford the device synchronisation
+ * cudaMalloc/cudaFree may cause, or a host with a device-memory budget fixed
+ * at start-up.  The caller passes canonical input and output device buffers
+ * and a stream (NULL = legacy default stream); no owner is needed, and the
+ * call allocates nothing: its working memory is a static device array of
+ * about 3.1 MB reserved on each device that loads the library, held until
+ * process exit.  length is a power of two up to 65536 (larger is rejected
+ * with -1); kind as in dvgpu_bn254_ntt_ex.  Calls share that array: calls
+ * whose device work overlaps (unordered streams) race and must be
+ * serialised by the caller.  The first call on a device looks up the
+ * array's address and should come before any stream capture.  Returns after
+ * the transform on `stream` has completed. */
+int dvgpu_bn254_ntt_noalloc(const uint8_t* d_values, size_t length, int kind, uint8_t* d_result, void* stream,
+                            char* error, size_t error_capacity);
+
 /* Tuning: force the Pippenger window width c (0 = autotuned / cost-model choice). */
 int dvgpu_msm_set_window(void* backend, int c);
 int dvgpu_msm_get_window(void* backend, size_t points_per_set, int* c);

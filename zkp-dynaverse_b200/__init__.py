@@ -110,6 +110,7 @@ SIGNATURES = [
     ("dvgpu_msm_get_window", ctypes.c_int, [_P, _SZ, ctypes.POINTER(ctypes.c_int)]),
     ("dvgpu_probe_imad_rate", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)] + _E),
     ("dvgpu_launch_count", ctypes.c_uint64, []),
+    ("dvgpu_bn254_ntt_noalloc", ctypes.c_int, [_P, _SZ, ctypes.c_int, _P, _P] + _E),
     ("dvgpu_msm_autotune", ctypes.c_int, [_P, _SZ, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _B, _SZ] + _E),
     ("dvgpu_msm_timeline", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(MsmPhaseTimes)]),
     ("dvgpu_random_fr_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
@@ -166,6 +167,17 @@ def decode_fr(b: bytes) -> int:
     if v >= R_MODULUS:
         raise ValueError("non-canonical or invalid scalar bytes")
     return v
+
+
+def ntt_noalloc(d_values: int, n: int, kind: int, d_result: int, stream=None):
+    """Allocation-free NTT on device buffers (dvgpu_bn254_ntt_noalloc): for
+    callers that cannot allocate device memory at call time; n <= 65536.
+    Its working memory is a static device array shared by all calls, so
+    calls must not overlap on the GPU."""
+    err = ctypes.create_string_buffer(256)
+    rc = lib().dvgpu_bn254_ntt_noalloc(d_values, n, kind, d_result, stream, err, len(err))
+    if rc != 0:
+        raise DvgpuError(rc, err.value.decode(errors="replace"))
 
 
 class DvgpuBackend:

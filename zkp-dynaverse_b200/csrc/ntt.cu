@@ -1,5 +1,6 @@
 // Fr NTT kernels and launch sequence (see ntt.cuh).
 #include <algorithm>
+#include <cstring>
 #include <string>
 
 #include "curve.cuh"
@@ -347,3 +348,142 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
 }
 
 }  // namespace dv
+
+// =====================================================================
+// Allocation-free NTT entry point.
+//
+// Some callers cannot allocate device memory at the moment they need a
+// transform: code that runs while another component owns the allocator
+// (a caching allocator or memory pool that must not be bypassed), code
+// on a latency-critical path that must never block on cudaMalloc/cudaFree
+// (both can synchronise the device), and hosts with a hard device-memory
+// budget fixed at start-up.  dvgpu_bn254_ntt_noalloc serves them: the
+// caller passes the input and output device buffers and a stream; every
+// other buffer the transform needs (the working vector, twiddle and coset
+// tables, constants and the error word) lives in the file-scope array
+// below, reserved when the library is loaded on a device and kept until
+// the process exits.  The array bounds the size: at most 2^16 elements.
+//
+// The array is shared by all calls on a device and keeps the last call's
+// contents; each call rebuilds its tables and resets its error word.  Two
+// calls whose work overlaps on the GPU (different streams, no ordering
+// between them) race on the array and may both produce wrong results.
+// The first call on a device looks up the array's device address; make
+// that first call before starting any stream capture.
+// =====================================================================
+namespace dv {
+namespace {
+
+constexpr int NOALLOC_MAX_LOG = 16;
+constexpr uint64_t NOALLOC_MAX_N = 1ull << NOALLOC_MAX_LOG;
+constexpr uint64_t NOALLOC_TAB = 1ull << ((NOALLOC_MAX_LOG + 1) / 2);
+// layout in Fr elements: work | twiddles | coset hi | coset lo | constants | error word
+constexpr uint64_t NA_WORK = 0;
+constexpr uint64_t NA_TW = NA_WORK + NOALLOC_MAX_N;
+constexpr uint64_t NA_HI = NA_TW + NOALLOC_MAX_N / 2;
+constexpr uint64_t NA_LO = NA_HI + NOALLOC_TAB;
+constexpr uint64_t NA_CONST = NA_LO + NOALLOC_TAB;
+constexpr uint64_t NA_ERR = NA_CONST + C_COUNT;
+constexpr uint64_t NA_TOTAL = NA_ERR + 1;
+
+static __device__ __align__(256) Fr noalloc_scratch[NA_TOTAL];  // about 3.1 MB per device
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+Fr* noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of the scratch array on the current device (looked up once
+// per device; host code must not use the symbol itself as a pointer).
+Fr* noalloc_scratch_on(int dev) {
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) throw InvalidArgument("device ordinal out of range");
+    if (!noalloc_ptr[dev]) {
+        void* p = nullptr;
+        DV_CUDA(cudaGetSymbolAddress(&p, noalloc_scratch));
+        noalloc_ptr[dev] = static_cast<Fr*>(p);
+    }
+    return noalloc_ptr[dev];
+}
+
+void ntt_noalloc(const uint8_t* d_in, uint8_t* d_out, int logn, int kind, cudaStream_t st) {
+    const uint64_t n = 1ull << logn;
+    const bool inverse = kind & 1, coset = kind >= 2;
+    const int split = (logn + 1) / 2;
+    int dev = 0;
+    DV_CUDA(cudaGetDevice(&dev));
+    Fr* base = noalloc_scratch_on(dev);
+    Fr* work = base + NA_WORK;
+    Fr* tw = base + NA_TW;
+    Fr* hi = base + NA_HI;
+    Fr* lo = base + NA_LO;
+    Fr* kc = base + NA_CONST;
+    uint32_t* bad = reinterpret_cast<uint32_t*>(base + NA_ERR);
+    DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
+    k_setup_consts<<<1, 1, 0, st>>>(logn, inverse ? 1 : 0, split, kc);
+    DV_LAUNCH();
+    const uint64_t half = std::max<uint64_t>(1, n / 2);
+    const uint32_t chunk = 64;
+    const uint64_t threads = (half + chunk - 1) / chunk;
+    k_pow_table<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(kc + C_W, nullptr, half, chunk, 0, tw);
+    DV_LAUNCH();
+    const uint64_t nlo = 1ull << split, nhi = (n + nlo - 1) >> split;
+    if (coset) {
+        k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(inverse ? kc + C_GINV_SPLIT : kc + C_G_SPLIT,
+                                                                  inverse ? kc + C_NINV : nullptr, nhi, 1, 0, hi);
+        DV_LAUNCH();
+        k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(inverse ? kc + C_GINV : kc + C_G, nullptr, nlo, 1,
+                                                                  0, lo);
+        DV_LAUNCH();
+    }
+    const Fr* pre_hi = (coset && !inverse) ? hi : nullptr;
+    const Fr* pre_lo = (coset && !inverse) ? lo : nullptr;
+    if (logn == 0) {
+        launch_pass<32>(d_in, work, 0, 0, 0, tw, 1, pre_hi, pre_lo, split, bad, st);
+    } else {
+        const int passes = (logn + 10) / 11;
+        int s0 = 0;
+        for (int p = 0; p < passes; ++p) {
+            const int k = logn / passes + (p < logn % passes ? 1 : 0);
+            if (k >= 9) launch_pass<256>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, bad, st);
+            else launch_pass<64>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, bad, st);
+            s0 += k;
+        }
+    }
+    k_permute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(work, d_out, logn, (coset && inverse) ? hi : nullptr,
+                                                          (coset && inverse) ? lo : nullptr, split,
+                                                          inverse ? kc + C_NINV : nullptr);
+    DV_LAUNCH();
+    uint32_t host_bad = 0;
+    DV_CUDA(cudaMemcpyAsync(&host_bad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaStreamSynchronize(st));
+    if (host_bad != 0xffffffffu) throw InvalidArgument("non-canonical NTT input at index " + std::to_string(host_bad));
+}
+
+}  // namespace
+}  // namespace dv
+
+extern "C" int dvgpu_bn254_ntt_noalloc(const uint8_t* d_values, size_t length, int kind, uint8_t* d_result,
+                                       void* stream, char* error, size_t error_capacity) {
+    auto fail = [&](int status, const std::string& msg) {
+        if (error && error_capacity) {
+            const size_t k = std::min(error_capacity - 1, msg.size());
+            memcpy(error, msg.data(), k);
+            error[k] = '\0';
+        }
+        return status;
+    };
+    if (!d_values || !d_result || kind < 0 || kind > 3 || !length || (length & (length - 1)))
+        return fail(-1, "invalid allocation-free NTT arguments");
+    if (length > dv::NOALLOC_MAX_N)
+        return fail(-1, "NTT length exceeds the allocation-free maximum of 65536 elements");
+    int logn = 0;
+    while ((1ull << logn) < length) ++logn;
+    try {
+        dv::ntt_noalloc(d_values, d_result, logn, kind, static_cast<cudaStream_t>(stream));
+        return 0;
+    } catch (const dv::InvalidArgument& e) {
+        return fail(-1, e.what());
+    } catch (const std::exception& e) {
+        return fail(-2, e.what());
+    } catch (...) {
+        return fail(-3, "unknown native exception");
+    }
+}
