@@ -1,35 +1,40 @@
 #!/usr/bin/env python
-"""Benchmark: BN254 G1 MSM over 2^20 points (SRS bases [tau^i]G1, uniform Fr
-scalars), the operator-level headline of the reference's prover hot path.
+"""Benchmark of the BN254 prover hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--log-n 20] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--op msm] [--log-n 20] [--impl ours|reference]
 
-One JSON line on stdout (rank 0).  A step is one complete MSM: device
-conversion and validation of the bases, signed-digit bucket sort, bucket
-accumulation and reduction, window combination and normalisation to a
-canonical affine point in host memory.
+Default (the headline): G1 MSM over 2^20 points, bases [tau^i]G1 (seeded
+tau), uniform Fr scalars.  Other operators of the same path: --op g2msm,
+ntt (--kind forward|inverse|coset_forward|coset_inverse), sparse (--k, over
+2^16 resident bases), fixedbase.  One JSON line on stdout (rank 0).
 
-  value / ms_per_step : device time per MSM (CUDA events on the launching
-                        stream), inputs resident in HBM, L2 flushed (256 MB
-                        write) between steps; the sum over K steps / K.
-                        With N GPUs the ranks run independent replicas;
-                        value = max-over-ranks time / (N * K) (ms per MSM
-                        of the whole job).
-  e2e                 : the same MSM through the reference-facing C-ABI
-                        call dvgpu_bn254_msm with pinned HOST buffers
-                        (H2D of 96 bytes/point inside the timed region).
-  roofline            : the bucket-accumulation kernel (the dominant one):
-                        N * windows XYZZ mixed additions x 10 Fq
-                        multiplications x 136 32x32->64 multiply-accumulates
-                        per launch, over its CUDA-event duration, against
-                        the IMAD rate measured in this run.
+A step is one complete operator call on device-resident inputs; its result
+is a canonical value in host memory (MSM: affine point; NTT: the device
+output vector).
+
+  value / ms_per_step : device time per step (CUDA events on the launching
+                        stream), L2 flushed (256 MB write) between steps, the
+                        sum over K steps / K.  With N GPUs the ranks run
+                        independent replicas (nothing is sharded);
+                        value = max-over-ranks time / (N * K).
+  e2e                 : the same operator through the reference-facing C-ABI
+                        call with pinned HOST buffers (host->device input
+                        copies and the result copy inside the timed region).
+  roofline            : integer-multiply bound.  MSM: the bucket-accumulation
+                        kernel, (points x windows) XYZZ mixed additions x 10
+                        Fq multiplications x 136 32x32->64-bit
+                        multiply-accumulates per launch, over its CUDA-event
+                        duration.  Other operators: the whole call, with the
+                        algorithmic multiplication count stated in the line.
+                        Peak = IMAD rate measured in this run.
   cpu_baseline        : the CPU oracle (C++ restatement of arkworks
-                        semantics, window-parallel Pippenger) on the same
-                        inputs, one full MSM, all host threads.
-  --impl reference    : times that CPU implementation alone (the reference
-                        itself, Rust + arkworks + ICICLE, cannot be built here).
+                        semantics) on the same inputs, all host threads.
+  --impl reference    : that CPU implementation alone, on the same workload
+                        (the reference's Rust + arkworks + ICICLE code cannot
+                        be built in this image).
 """
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -41,26 +46,36 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "G1 MSM 2^20 ms"
-UNIT = "ms"
+NTT_KINDS = {"forward": 0, "inverse": 1, "coset_forward": 2, "coset_inverse": 3}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--log-n", type=int, default=20)
+    ap.add_argument("--op", default="msm", choices=["msm", "g2msm", "ntt", "sparse", "fixedbase"])
+    ap.add_argument("--log-n", type=int, default=None)
+    ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
+    ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.log_n is None:
+        a.log_n = {"msm": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20}[a.op]
+    if a.steps is None:
+        a.steps = {"msm": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100}[a.op]
+    return a
 
 
-def msm_fme(n):
-    """Algorithmic work of a G1 MSM in Fq multiplications:
-    min over c of ceil(254/c) * (10 n + 14 * 2^c)."""
-    return min(math.ceil(254 / c) * (10 * n + 14 * (1 << c)) for c in range(2, 24))
+def msm_fme(n, g2=False):
+    """Algorithmic work of an MSM in Fq multiplications (Fq2 multiplication
+    = 3): min over c of ceil(254/c) * (10 n + 14 * 2^c), times 3 for G2."""
+    if n <= 0:
+        return 0
+    w = min(math.ceil(254 / c) * (10 * n + 14 * (1 << c)) for c in range(2, 24))
+    return 3 * w if g2 else w
 
 
 class ClockSampler:
@@ -121,10 +136,10 @@ class ClockSampler:
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
 
 
-def load_traffic():
-    """DRAM bytes per launch of the accumulation kernel from the committed
-    ncu summary (profiles/msm_g1_accum_2p20.txt), or None."""
-    path = os.path.join(ROOT, "profiles", "msm_g1_accum_2p20.txt")
+def load_traffic(name):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary profiles/<name>.txt (line 'traffic_bytes_per_launch: X')."""
+    path = os.path.join(ROOT, "profiles", name + ".txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -136,47 +151,306 @@ def load_traffic():
     return None
 
 
-def cpu_reference_msm(points: bytes, scalars: bytes, threads: int):
-    from oracle import oracle
-    t0 = time.perf_counter()
-    out = oracle.msm_g1(points, scalars, threads=threads)
-    return out, (time.perf_counter() - t0) * 1e3
+# ----------------------------------------------------------------- operators
+class MsmOp:
+    def __init__(self, args, g2=False):
+        self.g2 = g2
+        self.n = 1 << args.log_n
+        self.size = 128 if g2 else 64
+        self.metric = f"{'G2' if g2 else 'G1'} MSM 2^{args.log_n} ms"
+        self.workload = (f"{'G2' if g2 else 'G1'} MSM 2^{args.log_n}: bases [tau^i]{'G2' if g2 else 'G1'} affine "
+                         f"(seeded tau), uniform Fr scalars")
+        self.profile = f"msm_{'g2' if g2 else 'g1'}_accum_2p{args.log_n}"
+
+    def setup(self, torch, b, s, rank):
+        n = self.n
+        tau = torch.empty(32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(2812, 1, tau.data_ptr(), s)
+        powers = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+        b.fr_powers_device(tau.data_ptr(), n, powers.data_ptr(), s)
+        self.points = torch.empty(n * self.size, dtype=torch.uint8, device="cuda")
+        b.fixed_base_device(powers.data_ptr(), n, self.g2, self.points.data_ptr(), s)
+        self.scalars = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(2813 + rank, n, self.scalars.data_ptr(), s)
+        torch.cuda.synchronize()
+        self.tuned_c, self.tune_log = b.autotune_msm(n, g2=self.g2)
+        self.config = {"points": n, "window_bits": self.tuned_c, "windows": math.ceil(255 / self.tuned_c)}
+
+    def step(self, b, s):
+        return b.msm_device(self.points.data_ptr(), self.scalars.data_ptr(), self.n, g2=self.g2, stream=s)
+
+    def host_inputs(self, torch):
+        self.h_points = torch.empty(self.n * self.size, dtype=torch.uint8, pin_memory=True)
+        self.h_scalars = torch.empty(self.n * 32, dtype=torch.uint8, pin_memory=True)
+        self.h_points.copy_(self.points)
+        self.h_scalars.copy_(self.scalars)
+        self.out = ctypes.create_string_buffer(self.size)
+
+    def e2e_step(self, dv, b):
+        fn = dv.lib().dvgpu_bn254_g2_msm if self.g2 else dv.lib().dvgpu_bn254_msm
+        err = ctypes.create_string_buffer(256)
+        rc = fn(b.handle, self.h_points.data_ptr(), self.h_scalars.data_ptr(), self.n, self.out, err, 256)
+        if rc != 0:
+            raise RuntimeError(err.value)
+        return self.out.raw
+
+    def e2e_bytes(self):
+        return self.n * (self.size + 32), self.size + self.config["windows"] * 2 * self.size
+
+    def roofline(self, tl, imad_peak, step_ms):
+        macs_total = msm_fme(self.n, self.g2) * 136
+        accum_ms = tl.ms[3] / max(1, tl.calls)
+        adds = tl.accum_mixed_adds / max(1, tl.calls)
+        macs = adds * 10 * 136 * (3 if self.g2 else 1)
+        ach = macs / (accum_ms * 1e-3) / 1e12
+        return ({"bound": "imad", "kernel": "k_accum (bucket accumulation)", "achieved": ach,
+                 "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
+                 "algorithmic_macs_per_launch": macs, "launch_ms": accum_ms},
+                {"algorithmic_macs": macs_total, "achieved_tmacs": macs_total / (step_ms * 1e-3) / 1e12,
+                 "frac": macs_total / (step_ms * 1e-3) / imad_peak})
+
+    def cpu(self, oracle, threads):
+        pts = bytes(self.h_points.numpy().tobytes())
+        sc = bytes(self.h_scalars.numpy().tobytes())
+        t0 = time.perf_counter()
+        out = (oracle.msm_g2 if self.g2 else oracle.msm_g1)(pts, sc, threads=threads)
+        return out, (time.perf_counter() - t0) * 1e3, f"one full 2^{int(math.log2(self.n))}-point MSM on the same inputs"
 
 
+class NttOp:
+    def __init__(self, args):
+        self.n = 1 << args.log_n
+        self.logn = args.log_n
+        self.kind = NTT_KINDS[args.kind]
+        self.kind_name = args.kind
+        self.metric = f"Fr NTT 2^{args.log_n} ms ({args.kind})"
+        self.workload = f"Fr radix-2 NTT 2^{args.log_n} {args.kind} (arkworks domain, coset g=5) on uniform Fr"
+        self.profile = f"ntt_pass_2p{args.log_n}"
+
+    def setup(self, torch, b, s, rank):
+        self.src = torch.empty(self.n * 32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(3000 + rank, self.n, self.src.data_ptr(), s)
+        self.dst = torch.empty_like(self.src)
+        torch.cuda.synchronize()
+        self.tune_log = None
+        self.config = {"elements": self.n, "kind": self.kind_name, "passes": (self.logn + 10) // 11}
+
+    def step(self, b, s):
+        b.ntt_device(self.src.data_ptr(), self.n, self.kind, self.dst.data_ptr(), s)
+        return None
+
+    def host_inputs(self, torch):
+        self.h_src = torch.empty(self.n * 32, dtype=torch.uint8, pin_memory=True)
+        self.h_src.copy_(self.src)
+        self.h_dst = torch.empty(self.n * 32, dtype=torch.uint8, pin_memory=True)
+
+    def e2e_step(self, dv, b):
+        err = ctypes.create_string_buffer(256)
+        dst = ctypes.cast(ctypes.c_void_p(self.h_dst.data_ptr()), ctypes.c_char_p)
+        rc = dv.lib().dvgpu_bn254_ntt_ex(b.handle, self.h_src.data_ptr(), self.n, self.kind, dst, err, 256)
+        if rc != 0:
+            raise RuntimeError(err.value)
+        return None
+
+    def e2e_bytes(self):
+        return self.n * 32, self.n * 32
+
+    def fme(self):
+        extra = self.n if self.kind in (1, 2) else (2 * self.n if self.kind == 3 else 0)
+        return self.n // 2 * self.logn + extra
+
+    def roofline(self, tl, imad_peak, step_ms):
+        macs = self.fme() * 136
+        ach = macs / (step_ms * 1e-3) / 1e12
+        hbm = 64 * self.n / (step_ms * 1e-3) / 1e9
+        r = {"bound": "imad", "kernel": "whole NTT (k_dif_pass passes + k_permute)", "achieved": ach,
+             "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
+             "algorithmic_macs_per_launch": macs, "launch_ms": step_ms,
+             "hbm_achieved_gbs": hbm, "hbm_algorithmic_bytes": 64 * self.n}
+        return r, None
+
+    def cpu(self, oracle, threads):
+        sample = min(self.n, 1 << 20)
+        vals = bytes(self.h_src.numpy().tobytes()[:sample * 32])
+        t0 = time.perf_counter()
+        oracle.ntt(vals, self.kind_name)
+        ms = (time.perf_counter() - t0) * 1e3
+        scale = (self.n * self.logn) / (sample * math.log2(sample))
+        return None, ms * scale, (f"one 2^{int(math.log2(sample))} transform on 1 thread, scaled by n log n to "
+                                  f"2^{self.logn}")
+
+
+class SparseOp:
+    def __init__(self, args):
+        self.nb = 1 << args.log_n
+        self.k = args.k
+        self.metric = f"sparse G1 MSM k={args.k} over 2^{args.log_n} bases us"
+        self.workload = (f"sparse-index G1 MSM: {args.k} indices without replacement from [0, 2^{args.log_n}) "
+                         f"over resident [tau^i]G1, uniform Fr values")
+        self.profile = "msm_g1_sparse"
+
+    def setup(self, torch, b, s, rank):
+        import numpy as np
+        tau = torch.empty(32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(2812, 1, tau.data_ptr(), s)
+        powers = torch.empty(self.nb * 32, dtype=torch.uint8, device="cuda")
+        b.fr_powers_device(tau.data_ptr(), self.nb, powers.data_ptr(), s)
+        pts = torch.empty(self.nb * 64, dtype=torch.uint8, device="cuda")
+        b.fixed_base_device(powers.data_ptr(), self.nb, False, pts.data_ptr(), s)
+        torch.cuda.synchronize()
+        self.h_bases = pts.cpu().numpy().tobytes()
+        self.handle = b.register_bases(self.h_bases)
+        rng = np.random.default_rng(5150 + rank)
+        self.idx = rng.choice(self.nb, size=self.k, replace=False).astype(np.uint64)
+        self.d_idx = torch.from_numpy(self.idx.view(np.int64)).cuda()
+        self.d_vals = torch.empty(self.k * 32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(5151 + rank, self.k, self.d_vals.data_ptr(), s)
+        torch.cuda.synchronize()
+        self.tune_log = None
+        self.config = {"bases": self.nb, "k": self.k}
+
+    def step(self, b, s):
+        return b.sparse_msm_device(self.handle, self.d_idx.data_ptr(), self.d_vals.data_ptr(), [0, self.k], stream=s)[0]
+
+    def host_inputs(self, torch):
+        self.h_vals = self.d_vals.cpu().numpy().tobytes()
+
+    def e2e_step(self, dv, b):
+        return b.sparse_msm_resident(self.handle, self.idx, self.h_vals, [0, self.k])[0]
+
+    def e2e_bytes(self):
+        return self.k * 40, 64
+
+    def roofline(self, tl, imad_peak, step_ms):
+        macs = msm_fme(self.k) * 136
+        ach = macs / (step_ms * 1e-3) / 1e12
+        return ({"bound": "imad", "kernel": "whole sparse MSM (gather + Pippenger)", "achieved": ach,
+                 "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
+                 "algorithmic_macs_per_launch": macs, "launch_ms": step_ms}, None)
+
+    def cpu(self, oracle, threads):
+        vals = self.h_vals
+        t0 = time.perf_counter()
+        out = oracle.sparse_msm_g1(self.h_bases, self.idx, vals, threads=threads)
+        return out, (time.perf_counter() - t0) * 1e3, f"one k={self.k} sparse MSM on the same inputs"
+
+
+class FixedBaseOp:
+    def __init__(self, args):
+        self.n = 1 << args.log_n
+        self.metric = f"fixed-base G1 2^{args.log_n} ms"
+        self.workload = f"fixed-base [s_i]G1 for 2^{args.log_n} SRS exponents tau^i"
+        self.profile = "fixed_base_g1"
+
+    def setup(self, torch, b, s, rank):
+        tau = torch.empty(32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(2812 + rank, 1, tau.data_ptr(), s)
+        self.sc = torch.empty(self.n * 32, dtype=torch.uint8, device="cuda")
+        b.fr_powers_device(tau.data_ptr(), self.n, self.sc.data_ptr(), s)
+        self.out = torch.empty(self.n * 64, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        self.tune_log = None
+        self.config = {"points": self.n}
+
+    def step(self, b, s):
+        b.fixed_base_device(self.sc.data_ptr(), self.n, False, self.out.data_ptr(), s)
+        return None
+
+    def host_inputs(self, torch):
+        self.h_sc = self.sc.cpu().numpy().tobytes()
+
+    def e2e_step(self, dv, b):
+        b.fixed_base_g1(self.h_sc)
+        return None
+
+    def e2e_bytes(self):
+        return self.n * 32, self.n * 64
+
+    def roofline(self, tl, imad_peak, step_ms):
+        macs = self.n * (64 * 10 + 10) * 136  # 64 mixed adds + warp-shared normalisation per point
+        ach = macs / (step_ms * 1e-3) / 1e12
+        return ({"bound": "imad", "kernel": "k_fb_generate", "achieved": ach, "peak": imad_peak / 1e12,
+                 "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12), "algorithmic_macs_per_launch": macs,
+                 "launch_ms": step_ms}, None)
+
+    def cpu(self, oracle, threads):
+        sample = min(self.n, 1 << 16)
+        t0 = time.perf_counter()
+        oracle.fixed_base_g1(self.h_sc[:sample * 32], threads=threads)
+        ms = (time.perf_counter() - t0) * 1e3
+        return None, ms * self.n / sample, f"2^{int(math.log2(sample))} points, scaled linearly to the workload"
+
+
+def make_op(args):
+    return {"msm": lambda: MsmOp(args), "g2msm": lambda: MsmOp(args, g2=True), "ntt": lambda: NttOp(args),
+            "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args)}[args.op]()
+
+
+# ----------------------------------------------------------------- reference arm
 def run_reference(args, rank, world):
     """--impl reference: the CPU implementation of the path on host cores."""
     if rank != 0:
         return
     from oracle import oracle
-    n = 1 << args.log_n
     threads = os.cpu_count() or 1
-    tau = oracle.uniform_fr(2812, 1)
-    points = oracle.fixed_base_g1(oracle.fr_powers(tau, n), threads=threads)
-    scalars = oracle.uniform_fr(2813, n)
-    # warm-up (bounded) then timed steps, bounded to ~90 s of wall time
-    _, first = cpu_reference_msm(points, scalars, threads)
-    budget_ms = 90e3
-    steps = max(1, min(args.steps, int(budget_ms // max(first, 1.0))))
+    op = args.op
+    n = 1 << args.log_n
+    if op in ("msm", "g2msm"):
+        g2 = op == "g2msm"
+        tau = oracle.uniform_fr(2812, 1)
+        fb = oracle.fixed_base_g2 if g2 else oracle.fixed_base_g1
+        points = fb(oracle.fr_powers(tau, n), threads=threads)
+        scalars = oracle.uniform_fr(2813, n)
+        fn = (lambda: (oracle.msm_g2 if g2 else oracle.msm_g1)(points, scalars, threads=threads))
+        metric = f"{'G2' if g2 else 'G1'} MSM 2^{args.log_n} ms"
+        sample = f"full 2^{args.log_n}-point MSMs, window-parallel Pippenger"
+    elif op == "ntt":
+        vals = oracle.uniform_fr(3000, n)
+        fn = lambda: oracle.ntt(vals, args.kind)
+        metric = f"Fr NTT 2^{args.log_n} ms ({args.kind})"
+        sample = f"full 2^{args.log_n} transforms, 1 thread (radix-2)"
+        threads = 1
+    elif op == "sparse":
+        import numpy as np
+        bases = oracle.fixed_base_g1(oracle.fr_powers(oracle.uniform_fr(2812, 1), n), threads=threads)
+        idx = np.random.default_rng(5150).choice(n, size=args.k, replace=False).astype(np.uint64)
+        vals = oracle.uniform_fr(5151, args.k)
+        fn = lambda: oracle.sparse_msm_g1(bases, idx, vals, threads=threads)
+        metric = f"sparse G1 MSM k={args.k} over 2^{args.log_n} bases us"
+        sample = f"k={args.k} sparse MSMs"
+    else:
+        sc = oracle.fr_powers(oracle.uniform_fr(2812, 1), n)
+        fn = lambda: oracle.fixed_base_g1(sc, threads=threads)
+        metric = f"fixed-base G1 2^{args.log_n} ms"
+        sample = f"full 2^{args.log_n}-point fixed-base generations"
+    t0 = time.perf_counter()
+    fn()
+    first = (time.perf_counter() - t0) * 1e3
+    steps = max(1, min(args.steps, int(90e3 // max(first, 1.0))))
     times = []
     for _ in range(steps):
-        _, ms = cpu_reference_msm(points, scalars, threads)
-        times.append(ms)
+        t0 = time.perf_counter()
+        fn()
+        times.append((time.perf_counter() - t0) * 1e3)
     value = sum(times) / len(times)
-    sample = f"{steps} full 2^{args.log_n}-point MSMs (after 1 warm-up), window-parallel Pippenger"
+    if op == "sparse":
+        value *= 1e3  # us
+    unit = "us" if op == "sparse" else "ms"
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32 limbs (Fq/Fr, exact)", "data": "synthetic",
-        "config": {"workload": f"G1 MSM 2^{args.log_n}: bases [tau^i]G1 affine (seeded tau), uniform Fr scalars",
-                   "parallelism": "host threads"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value / (1e3 if op == "sparse" else 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 limbs (Fq/Fr, exact)", "data": "synthetic",
+        "config": {"workload": metric, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
+                         "sample": f"{steps} {sample} (after 1 warm-up)"},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": ("reference = C++ restatement of arkworks 0.4 semantics (oracle/); the reference's own "
                  "Rust/arkworks/ICICLE code cannot be built in this image"),
     }
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------- our arm
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -197,28 +471,15 @@ def main():
     from __graft_entry__ import load_package
     dv = load_package()
     b = dv.DvgpuBackend()
-    n = 1 << args.log_n
     stream = torch.cuda.current_stream()
     s = stream.cuda_stream
-
-    # ---- inputs, generated on the device (seeded): SRS bases and scalars
-    tau = torch.empty(32, dtype=torch.uint8, device="cuda")
-    b.random_fr_device(2812, 1, tau.data_ptr(), s)
-    powers = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
-    b.fr_powers_device(tau.data_ptr(), n, powers.data_ptr(), s)
-    points = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
-    b.fixed_base_device(powers.data_ptr(), n, False, points.data_ptr(), s)
-    scalars = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
-    b.random_fr_device(2813 + rank, n, scalars.data_ptr(), s)
-    del powers
+    op = make_op(args)
+    op.setup(torch, b, s, rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    torch.cuda.synchronize()
-
-    # window width for this size, measured (setup, not timed)
-    tuned_c, tune_log = b.autotune_msm(n)
-    torch.cuda.synchronize()
+    result = None
     for _ in range(args.warmup):
-        result = b.msm_device(points.data_ptr(), scalars.data_ptr(), n, stream=s)
+        result = op.step(b, s)
+    torch.cuda.synchronize()
 
     try:
         bus = torch.cuda.get_device_properties(dev).pci_bus_id
@@ -238,12 +499,12 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        r = b.msm_device(points.data_ptr(), scalars.data_ptr(), n, stream=s)
+        r = op.step(b, s)
         e1.record(stream)
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
         if r != result:
-            raise RuntimeError("MSM result changed between steps")
+            raise RuntimeError("result changed between steps")
     torch.cuda.synchronize()
     tl = b.msm_timeline(False)
     launches = b.launch_count() - launches0
@@ -255,79 +516,63 @@ def main():
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    ms_per_msm = total_ms / args.steps
+    ms_per_step = total_ms / args.steps
     value = total_ms / (args.steps * world)
 
     # ---- end to end through the C-ABI with pinned host buffers
-    h_points = torch.empty(n * 64, dtype=torch.uint8, pin_memory=True)
-    h_scalars = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
-    h_points.copy_(points)
-    h_scalars.copy_(scalars)
+    op.host_inputs(torch)
     torch.cuda.synchronize()
-    L = dv.lib()
-    out = bytearray(64)
-    import ctypes
-    outbuf = (ctypes.c_char * 64).from_buffer(out)
-    err = ctypes.create_string_buffer(256)
-    rc = L.dvgpu_bn254_msm(b.handle, h_points.data_ptr(), h_scalars.data_ptr(), n, outbuf, err, 256)
-    if rc != 0 or bytes(out) != result:
-        raise RuntimeError(f"e2e MSM failed or differs: {rc} {err.value}")
+    r0 = op.e2e_step(dv, b)
+    if result is not None and r0 != result:
+        raise RuntimeError("host-buffer call differs from the device-resident call")
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        L.dvgpu_bn254_msm(b.handle, h_points.data_ptr(), h_scalars.data_ptr(), n, outbuf, err, 256)
+        op.e2e_step(dv, b)
     e2e_total = (time.perf_counter() - t0) * 1e3
     if world > 1:
         t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
     e2e_ms = e2e_total / (args.e2e_steps * world)
-    c = b.window_for(n)
-    windows = math.ceil(255 / c)
 
-    # ---- roofline of the dominant kernel (bucket accumulation)
-    imad_peak = b.probe_imad_rate()  # MAC/s
-    accum_ms = tl.ms[3] / max(1, tl.calls)
-    adds_per_launch = tl.accum_mixed_adds / max(1, tl.calls)
-    accum_macs = adds_per_launch * 10 * 136
-    achieved = accum_macs / (accum_ms * 1e-3) / 1e12
-    peak = imad_peak / 1e12
-    traffic = load_traffic()
-    phases = {name: tl.ms[k] / max(1, tl.calls) for k, name in enumerate(dv.MSM_PHASE_NAMES)}
-    msm_macs = msm_fme(n) * 136
-
+    imad_peak = b.probe_imad_rate()
+    roof, whole = op.roofline(tl, imad_peak, ms_per_step)
+    roof["traffic"] = load_traffic(op.profile)
+    roof["peak_source"] = "dvgpu_probe_imad_rate in this run (madc.lo/hi chains on all SMs)"
+    scale = 1e3 if args.op == "sparse" else 1.0  # sparse reported in microseconds
+    unit = "us" if args.op == "sparse" else "ms"
+    h2d, d2h = op.e2e_bytes()
+    config = {"workload": op.workload, "op": args.op,
+              "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+              "l2": "flushed between steps (256 MB write)"}
+    config.update(op.config)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_msm, "higher_is_better": False, "scaling": "weak",
+        "metric": op.metric, "value": value * scale, "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 limbs (Fq/Fr Montgomery, exact)", "data": "synthetic",
-        "config": {"workload": f"G1 MSM 2^{args.log_n}: bases [tau^i]G1 affine (seeded tau), uniform Fr scalars",
-                   "points": n, "window_bits": c, "windows": windows,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "flushed between steps (256 MB write)"},
-        "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": n * 96,
-                "d2h_bytes_per_step": 64 + windows * 128,
-                "call": "dvgpu_bn254_msm (pinned host buffers)"},
-        "roofline": {"bound": "imad", "kernel": "k_accum (bucket accumulation)",
-                     "achieved": achieved, "peak": peak, "unit": "TMAC/s", "frac": achieved / peak,
-                     "traffic": traffic, "algorithmic_macs_per_launch": accum_macs,
-                     "peak_source": "dvgpu_probe_imad_rate in this run (madc.lo/hi chains on all SMs)",
-                     "launch_ms": accum_ms},
-        "msm_roofline": {"algorithmic_macs": msm_macs, "achieved_tmacs": msm_macs / (ms_per_msm * 1e-3) / 1e12,
-                         "frac": msm_macs / (ms_per_msm * 1e-3) / imad_peak},
-        "phases_ms": phases,
-        "autotune": tune_log,
+        "config": config,
+        "e2e": {"value": e2e_ms * scale, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "call": "reference-facing C-ABI entry point with pinned host buffers"},
+        "roofline": roof,
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if whole:
+        line["msm_roofline"] = whole
+    if tl.calls:
+        line["phases_ms"] = {name: tl.ms[k] / tl.calls for k, name in enumerate(dv.MSM_PHASE_NAMES)}
+    if op.tune_log:
+        line["autotune"] = op.tune_log
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        host_pts = bytes(h_points.numpy().tobytes())
-        host_sc = bytes(h_scalars.numpy().tobytes())
+        from oracle import oracle
         threads = os.cpu_count() or 1
-        cpu_out, cpu_ms = cpu_reference_msm(host_pts, host_sc, threads)
-        line["cpu_baseline"] = {"value": cpu_ms, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"one full 2^{args.log_n}-point MSM on the same inputs",
-                                "matches_gpu": cpu_out == result}
+        cpu_out, cpu_ms, sample = op.cpu(oracle, threads)
+        line["cpu_baseline"] = {"value": cpu_ms * scale, "unit": unit,
+                                "cores": 1 if args.op == "ntt" else threads, "kind": "port", "sample": sample}
+        if cpu_out is not None:
+            line["cpu_baseline"]["matches_gpu"] = cpu_out == result
     if rank == 0:
         print(json.dumps(line), flush=True)
     b.close()

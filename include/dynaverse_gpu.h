@@ -157,6 +157,13 @@ int dvgpu_bn254_msm_sparse_batch(void* backend, uint64_t bases_handle, const uin
                                  const uint64_t* request_offsets, size_t count, uint8_t* results, char* error,
                                  size_t error_capacity);
 
+/* The same over device-resident indices and values (request_offsets and the
+ * results stay in host memory).  Indices are checked on the device; an index
+ * out of range returns -1 and writes no result. */
+int dvgpu_bn254_msm_sparse_device(void* backend, uint64_t bases_handle, const uint64_t* d_indices,
+                                  const uint8_t* d_values, const uint64_t* request_offsets, size_t count,
+                                  uint8_t* results_host, void* stream, char* error, size_t error_capacity);
+
 /* Device-pointer forms (inputs already in HBM, canonical wire layout).
  * stream: a cudaStream_t, or NULL for the owner's stream.  The call returns
  * after the device work on `stream` completed.  result_host: host memory. */

@@ -101,6 +101,7 @@ SIGNATURES = [
     ("dvgpu_bases_release", ctypes.c_int, [_P, ctypes.c_uint64]),
     ("dvgpu_bn254_msm_sparse_batch", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _P, _SZ, _B] + _E),
     ("dvgpu_bn254_msm_device", ctypes.c_int, [_P, _P, _P, _SZ, ctypes.c_int, _B, _P] + _E),
+    ("dvgpu_bn254_msm_sparse_device", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _P, _SZ, _B, _P] + _E),
     ("dvgpu_bn254_msm_resident", ctypes.c_int, [_P, ctypes.c_uint64, _P, _SZ, _B, _P] + _E),
     ("dvgpu_bn254_ntt_device", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _P, _P] + _E),
     ("dvgpu_bn254_fixed_base_device", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _P, _P] + _E),
@@ -426,6 +427,14 @@ class DvgpuBackend:
         out = ctypes.create_string_buffer(G2_BYTES if g2 else G1_BYTES)
         self._call("dvgpu_bn254_msm_device", d_points, d_scalars, n, int(g2), out, stream)
         return out.raw
+
+    def sparse_msm_device(self, handle: int, d_indices: int, d_values: int, request_offsets, stream=None):
+        offs = np.ascontiguousarray(np.asarray(request_offsets, dtype=np.uint64))
+        count = len(offs) - 1
+        out = ctypes.create_string_buffer(max(1, count) * G1_BYTES)
+        self._call("dvgpu_bn254_msm_sparse_device", handle, d_indices, d_values, offs.ctypes.data, count, out, stream)
+        raw = out.raw
+        return [raw[i * G1_BYTES:(i + 1) * G1_BYTES] for i in range(count)]
 
     def msm_resident(self, handle: int, d_scalars: int, n: int, stream=None, g2=False) -> bytes:
         out = ctypes.create_string_buffer(G2_BYTES if g2 else G1_BYTES)

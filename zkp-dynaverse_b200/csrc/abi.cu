@@ -471,6 +471,41 @@ extern "C" int dvgpu_bn254_msm_sparse_batch(void* opaque, uint64_t bases_handle,
     });
 }
 
+extern "C" int dvgpu_bn254_msm_sparse_device(void* opaque, uint64_t bases_handle, const uint64_t* d_indices,
+                                             const uint8_t* d_values, const uint64_t* request_offsets, size_t count,
+                                             uint8_t* results_host, void* stream, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        auto it = b.bases.find(bases_handle);
+        require(it != b.bases.end() && !it->second->g2, "unknown G1 base handle");
+        require(request_offsets && results_host && count <= DVGPU_MAX_MSM_BATCH_SIZE && request_offsets[0] == 0,
+                "invalid sparse request arguments");
+        std::vector<uint32_t> offs(count + 1);
+        for (size_t k = 0; k <= count; ++k) {
+            require(k == 0 || request_offsets[k] >= request_offsets[k - 1], "request offsets must be non-decreasing");
+            require(request_offsets[k] <= DVGPU_MAX_MSM_SIZE, "sparse batch exceeds the MSM size bound");
+            offs[k] = (uint32_t)request_offsets[k];
+        }
+        const uint64_t k_total = offs[count];
+        require(!k_total || (d_indices && d_values), "null index or value buffer");
+        if (!count) return;
+        if (!k_total) {
+            memset(results_host, 0, count * 64);
+            return;
+        }
+        const cudaStream_t st = pick(b, stream);
+        const ResidentBases& rb = *it->second;
+        G1A* gathered = b.conv_points.as<G1A>(k_total);
+        uint32_t* bad = b.err.as<uint32_t>(1);
+        DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
+        gather_points<Fq>(rb.points.view<G1A>(), rb.n, d_indices, k_total, gathered, bad, st);
+        std::vector<uint8_t> tmp(count * 64);
+        msm_run<Fq>(b.msm, gathered, reinterpret_cast<const uint32_t*>(d_values), offs.data(), (uint32_t)count,
+                    window_for<Fq>(b, offs), st, tmp.data(), &b.msm_stats);
+        require(read_err_word(b, bad, st) == 0xffffffffu, "sparse MSM index out of range");
+        memcpy(results_host, tmp.data(), tmp.size());
+    });
+}
+
 extern "C" int dvgpu_bn254_msm_device(void* opaque, const uint8_t* d_points, const uint8_t* d_scalars, size_t length,
                                       int g2, uint8_t* result_host, void* stream, char* error, size_t cap) {
     return guarded(opaque, error, cap, [&](Backend& b) {
@@ -535,11 +570,10 @@ void ntt_host(Backend& b, const uint8_t* values, size_t length, int kind, uint8_
     uint8_t* d = b.in_scalars.as<uint8_t>(length * 32);
     DV_CUDA(cudaMemcpyAsync(d, values, length * 32, cudaMemcpyHostToDevice, b.stream));
     uint8_t* d_out = b.out_buf.as<uint8_t>(length * 32);
-    ntt_run(b.ntt, d, d_out, logn, kind, b.stream);  // synchronises and checks
-    uint8_t* h = b.pin_out.as<uint8_t>(length * 32);
-    DV_CUDA(cudaMemcpyAsync(h, d_out, length * 32, cudaMemcpyDeviceToHost, b.stream));
+    ntt_run(b.ntt, d, d_out, logn, kind, b.stream);  // synchronises and checks the input
+    // validated: the result goes straight to the caller's buffer
+    DV_CUDA(cudaMemcpyAsync(result, d_out, length * 32, cudaMemcpyDeviceToHost, b.stream));
     DV_CUDA(cudaStreamSynchronize(b.stream));
-    memcpy(result, h, length * 32);
 }
 }  // namespace
 
@@ -607,11 +641,9 @@ extern "C" int dvgpu_bn254_fixed_base(void* opaque, const uint8_t* scalars, size
         uint8_t* d_sc = b.in_scalars.as<uint8_t>(length * 32);
         uint8_t* d_out = b.out_buf.as<uint8_t>(length * psize);
         DV_CUDA(cudaMemcpyAsync(d_sc, scalars, length * 32, cudaMemcpyHostToDevice, b.stream));
-        fixed_base_device(b, d_sc, length, g2, d_out, b.stream);
-        uint8_t* h = b.pin_out.as<uint8_t>(length * psize);
-        DV_CUDA(cudaMemcpyAsync(h, d_out, length * psize, cudaMemcpyDeviceToHost, b.stream));
+        fixed_base_device(b, d_sc, length, g2, d_out, b.stream);  // synchronises and checks the scalars
+        DV_CUDA(cudaMemcpyAsync(output, d_out, length * psize, cudaMemcpyDeviceToHost, b.stream));
         DV_CUDA(cudaStreamSynchronize(b.stream));
-        memcpy(output, h, length * psize);
         b.setup_stats.native_wall_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
                                             std::chrono::steady_clock::now() - t0)
                                             .count();

@@ -271,19 +271,23 @@ __global__ void __launch_bounds__(TH) k_fixup_long(const int* __restrict__ pgid,
                                                    const uint32_t* __restrict__ long_list,
                                                    const uint32_t* __restrict__ long_count) {
     __shared__ XYZZ<F> sh[TH];
-    if (blockIdx.x >= *long_count) return;
-    const uint32_t t0 = long_list[blockIdx.x];
-    const int g = pgid[2 * t0 + 1];
-    XYZZ<F> acc = threadIdx.x == 0 ? ppt[2 * t0 + 1] : XYZZ<F>::inf();
-    // the heads of g are contiguous from t0 + 1: stop at the first other key
-    for (uint32_t k = t0 + 1 + threadIdx.x; k < T && pgid[2 * k] == g; k += TH) acc = XYZZ<F>::add(acc, ppt[2 * k]);
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int d = TH / 2; d > 0; d >>= 1) {
-        if ((int)threadIdx.x < d) sh[threadIdx.x] = XYZZ<F>::add(sh[threadIdx.x], sh[threadIdx.x + d]);
+    const uint32_t nlong = *long_count;
+    for (uint32_t item = blockIdx.x; item < nlong; item += gridDim.x) {
+        const uint32_t t0 = long_list[item];
+        const int g = pgid[2 * t0 + 1];
+        XYZZ<F> acc = threadIdx.x == 0 ? ppt[2 * t0 + 1] : XYZZ<F>::inf();
+        // the heads of g are contiguous from t0 + 1: stop at the first other key
+        for (uint32_t k = t0 + 1 + threadIdx.x; k < T && pgid[2 * k] == g; k += TH)
+            acc = XYZZ<F>::add(acc, ppt[2 * k]);
+        sh[threadIdx.x] = acc;
+        __syncthreads();
+        for (int d = TH / 2; d > 0; d >>= 1) {
+            if ((int)threadIdx.x < d) sh[threadIdx.x] = XYZZ<F>::add(sh[threadIdx.x], sh[threadIdx.x + d]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) buckets[g] = sh[0];
         __syncthreads();
     }
-    if (threadIdx.x == 0) buckets[g] = sh[0];
 }
 
 // 6. Bucket reduction, level 1.  Window (set, w) needs
@@ -581,8 +585,9 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         DV_CUDA(cudaMemsetAsync(d_fix_count, 0, sizeof(uint32_t), st));
         k_fixup<F><<<blocks_for(T, 128), 128, 0, st>>>(d_pgid, d_ppt, T, d_buckets + gb0, d_fix_list, d_fix_count);
         DV_LAUNCH();
-        k_fixup_long<F, 128><<<T / FIX_SHORT + 1, 128, 0, st>>>(d_pgid, d_ppt, T, d_buckets + gb0, d_fix_list,
-                                                                d_fix_count);
+        // long chains are rare: a small grid loops over the queue
+        k_fixup_long<F, 128><<<std::min<uint32_t>(T / FIX_SHORT + 1, (uint32_t)sm_count()), 128, 0, st>>>(
+            d_pgid, d_ppt, T, d_buckets + gb0, d_fix_list, d_fix_count);
         DV_LAUNCH();
         DV_CUDA(cudaEventRecord(ws.sync_ev[gi], st));
         DV_CUDA(cudaStreamWaitEvent(ws.side, ws.sync_ev[gi], 0));

@@ -9,14 +9,15 @@
 // Coset forms use the offset g = 5: forward scales coefficient j by g^j
 // before the transform, inverse scales output i by g^-i after it.
 //
-// Layout: canonical little-endian 32-byte elements in HBM (the wire format),
-// converted to Montgomery form on load and back on store.  The transform is
-// decimation-in-frequency radix-2, grouped into passes of up to 11 stages;
-// each pass stages one group of 2^k elements (stride 2^low) in shared memory
-// as 8 word planes (bank-conflict free), runs its k butterfly stages there
-// with twiddles from a resident table w^i (i < n/2), and writes back.  A
-// final pass applies the bit-reversal permutation fused with the inverse
-// scaling and the conversion to canonical form.
+// Layout: canonical little-endian 32-byte elements in HBM (the wire format).
+// Values stay canonical throughout: every multiplier (twiddles, coset and
+// scale factors) is held in Montgomery form, and mont_mul(a, x R) = a x.
+// The transform is decimation-in-frequency radix-2, grouped into passes of
+// up to 11 stages; each pass stages one group of 2^k elements (stride 2^lb)
+// in shared memory as 8 padded word planes and runs its stages in
+// register rounds of two (each thread owns 4 elements per round), with
+// twiddles from a resident table w^i (i < n/2).  A final pass applies the
+// bit-reversal permutation fused with the inverse and coset scaling.
 #pragma once
 #include <cuda_runtime.h>
 
