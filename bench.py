@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--op", default="msm", choices=["msm", "g2msm", "ntt", "sparse", "fixedbase"])
+    ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase"])
     ap.add_argument("--log-n", type=int, default=None)
     ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
     ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
@@ -63,9 +63,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
     if a.log_n is None:
-        a.log_n = {"msm": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20}[a.op]
+        a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20}[a.op]
     if a.steps is None:
-        a.steps = {"msm": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100}[a.op]
+        a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100}[a.op]
     return a
 
 
@@ -215,6 +215,43 @@ class MsmOp:
         t0 = time.perf_counter()
         out = (oracle.msm_g2 if self.g2 else oracle.msm_g1)(pts, sc, threads=threads)
         return out, (time.perf_counter() - t0) * 1e3, f"one full 2^{int(math.log2(self.n))}-point MSM on the same inputs"
+
+
+class ResidentMsmOp(MsmOp):
+    """G1 MSM over a registered (HBM-resident) SRS with precomputed window
+    multiples (dvgpu_bases_precompute, setup, not timed): every window adds
+    into one shared bucket set.  e2e stays the reference-facing per-call
+    dvgpu_bn254_msm with host buffers."""
+
+    def __init__(self, args):
+        super().__init__(args, g2=False)
+        self.workload = (self.workload + "; SRS resident in HBM with precomputed window multiples "
+                         "(registration and precomputation are setup, not timed)")
+        self.profile = f"msm_g1_resident_accum_2p{args.log_n}"
+
+    def setup(self, torch, b, s, rank):
+        super().setup(torch, b, s, rank)
+        torch.cuda.synchronize()
+        self.handle = b.register_bases(self.points.cpu().numpy().tobytes())
+        self.pre_c = b.precompute_bases(self.handle, 0)
+        self.config = {"points": self.n, "window_bits": self.pre_c, "windows": math.ceil(255 / self.pre_c),
+                       "precomputed_table_bytes": self.n * math.ceil(255 / self.pre_c) * 64}
+        self.tune_log = None
+
+    def step(self, b, s):
+        return b.msm_resident(self.handle, self.scalars.data_ptr(), self.n, stream=s)
+
+    def e2e_step(self, dv, b):
+        # the per-request call of a resident prover: scalars from host memory
+        err = ctypes.create_string_buffer(256)
+        rc = dv.lib().dvgpu_bn254_msm_resident_host(b.handle, self.handle, self.h_scalars.data_ptr(), self.n,
+                                                    self.out, err, 256)
+        if rc != 0:
+            raise RuntimeError(err.value)
+        return self.out.raw
+
+    def e2e_bytes(self):
+        return self.n * 32, 64
 
 
 class NttOp:
@@ -382,7 +419,7 @@ class FixedBaseOp:
 
 
 def make_op(args):
-    return {"msm": lambda: MsmOp(args), "g2msm": lambda: MsmOp(args, g2=True), "ntt": lambda: NttOp(args),
+    return {"msm": lambda: MsmOp(args), "msmres": lambda: ResidentMsmOp(args), "g2msm": lambda: MsmOp(args, g2=True), "ntt": lambda: NttOp(args),
             "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args)}[args.op]()
 
 
@@ -395,7 +432,7 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     op = args.op
     n = 1 << args.log_n
-    if op in ("msm", "g2msm"):
+    if op in ("msm", "msmres", "g2msm"):
         g2 = op == "g2msm"
         tau = oracle.uniform_fr(2812, 1)
         fb = oracle.fixed_base_g2 if g2 else oracle.fixed_base_g1

@@ -147,6 +147,12 @@ int dvgpu_bn254_msm_batch_uneven(void* backend, const uint8_t* points, const uin
 int dvgpu_bases_register(void* backend, const uint8_t* points, size_t n, int g2, uint64_t* handle, char* error,
                          size_t error_capacity);
 int dvgpu_bases_release(void* backend, uint64_t handle);
+/* Precomputed window multiples for registered bases: stores 2^(c w) P_i for
+ * every base and window (windows = ceil(255 / c) entries per base, e.g. 13 x
+ * 64 B per G1 base at c = 20).  dvgpu_bn254_msm_resident then adds every
+ * window into one shared bucket set and skips the window combination.
+ * c = 0 picks the width by cost model; c_used (may be NULL) receives it. */
+int dvgpu_bases_precompute(void* backend, uint64_t handle, int c, int* c_used, char* error, size_t error_capacity);
 
 /* Sparse-index G1 MSM over resident bases (OperatorBackend::msm_sparse_batch,
  * crates/protocol/src/types.rs:262-345): request k sums
@@ -172,6 +178,10 @@ int dvgpu_bn254_msm_device(void* backend, const uint8_t* d_points, const uint8_t
 /* MSM over a registered base table (first `length` bases) with device scalars. */
 int dvgpu_bn254_msm_resident(void* backend, uint64_t bases_handle, const uint8_t* d_scalars, size_t length,
                              uint8_t* result_host, void* stream, char* error, size_t error_capacity);
+/* The resident-bases MSM with scalars in host memory (synchronous, like
+ * dvgpu_bn254_msm): the per-request call of a prover whose SRS is resident. */
+int dvgpu_bn254_msm_resident_host(void* backend, uint64_t bases_handle, const uint8_t* scalars, size_t length,
+                                  uint8_t* result, char* error, size_t error_capacity);
 int dvgpu_bn254_ntt_device(void* backend, const uint8_t* d_values, size_t length, int kind, uint8_t* d_result,
                            void* stream, char* error, size_t error_capacity);
 int dvgpu_bn254_fixed_base_device(void* backend, const uint8_t* d_scalars, size_t length, int g2, uint8_t* d_output,

@@ -192,3 +192,32 @@ def test_skewed_digits_long_bucket_chains(backend, oracle):
             assert backend.msm(pts, rnd) == expect_rnd, f"c={c}"
         finally:
             backend.set_window(0)
+
+
+def test_precomputed_resident_msm_matches_oracle(backend, oracle):
+    import torch
+    n = 1 << 14
+    pts, _ = oracle.srs_g1(777, n)
+    scs = oracle.uniform_fr(778, n)
+    expect = oracle.msm_g1(pts, scs)
+    expect_prefix = oracle.msm_g1(pts[:1000 * 64], scs[:1000 * 32])
+    d_sc = torch.frombuffer(bytearray(scs), dtype=torch.uint8).cuda()
+    torch.cuda.synchronize()
+    h = backend.register_bases(pts)
+    try:
+        assert backend.msm_resident(h, d_sc.data_ptr(), n) == expect
+        for c in (0, 8, 13, 16):
+            backend.precompute_bases(h, c)
+            assert backend.msm_resident(h, d_sc.data_ptr(), n) == expect, f"c={c}"
+            assert backend.msm_resident(h, d_sc.data_ptr(), 1000) == expect_prefix, f"c={c} prefix"
+    finally:
+        backend.release_bases(h)
+    pts2, scs2 = _case_inputs(oracle, 779, 2000, g2=True)
+    d_sc2 = torch.frombuffer(bytearray(scs2), dtype=torch.uint8).cuda()
+    torch.cuda.synchronize()
+    h2 = backend.register_bases(pts2, g2=True)
+    try:
+        backend.precompute_bases(h2, 0)
+        assert backend.msm_resident(h2, d_sc2.data_ptr(), 2000, g2=True) == oracle.msm_g2(pts2, scs2)
+    finally:
+        backend.release_bases(h2)

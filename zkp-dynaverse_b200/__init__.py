@@ -99,10 +99,12 @@ SIGNATURES = [
     ("dvgpu_bn254_msm_batch_uneven", ctypes.c_int, [_P, _P, _P, _P, _SZ, _B] + _E),
     ("dvgpu_bases_register", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)] + _E),
     ("dvgpu_bases_release", ctypes.c_int, [_P, ctypes.c_uint64]),
+    ("dvgpu_bases_precompute", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_int)] + _E),
     ("dvgpu_bn254_msm_sparse_batch", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _P, _SZ, _B] + _E),
     ("dvgpu_bn254_msm_device", ctypes.c_int, [_P, _P, _P, _SZ, ctypes.c_int, _B, _P] + _E),
     ("dvgpu_bn254_msm_sparse_device", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _P, _SZ, _B, _P] + _E),
     ("dvgpu_bn254_msm_resident", ctypes.c_int, [_P, ctypes.c_uint64, _P, _SZ, _B, _P] + _E),
+    ("dvgpu_bn254_msm_resident_host", ctypes.c_int, [_P, ctypes.c_uint64, _P, _SZ, _B] + _E),
     ("dvgpu_bn254_ntt_device", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _P, _P] + _E),
     ("dvgpu_bn254_fixed_base_device", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _P, _P] + _E),
     ("dvgpu_bn254_g2_check_device", ctypes.c_int,
@@ -329,6 +331,12 @@ class DvgpuBackend:
         h = ctypes.c_uint64()
         self._call("dvgpu_bases_register", _ptr(points), len(points) // size, int(g2), ctypes.byref(h))
         return h.value
+
+    def precompute_bases(self, handle: int, c: int = 0) -> int:
+        """Attach precomputed window multiples to registered bases; returns c."""
+        used = ctypes.c_int()
+        self._call("dvgpu_bases_precompute", handle, c, ctypes.byref(used))
+        return used.value
 
     def release_bases(self, handle: int):
         self._L.dvgpu_bases_release(self.handle, handle)

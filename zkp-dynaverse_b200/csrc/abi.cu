@@ -530,17 +530,33 @@ extern "C" int dvgpu_bn254_msm_resident(void* opaque, uint64_t bases_handle, con
             memset(result_host, 0, rb.g2 ? 128 : 64);
             return;
         }
+        // a table of precomputed window multiples, when registered, is used
         if (rb.g2) {
             uint8_t tmp[128];
+            const MsmPrecomp<Fq2> pre{rb.pre_table.view<G2A>(), rb.pre_c, rb.pre_windows};
             msm_run<Fq2>(b.msm, rb.points.view<G2A>(), reinterpret_cast<const uint32_t*>(d_scalars), offs.data(), 1,
-                         window_for<Fq2>(b, offs), st, tmp, &b.msm_stats);
+                         window_for<Fq2>(b, offs), st, tmp, &b.msm_stats, rb.pre_c ? &pre : nullptr);
             memcpy(result_host, tmp, 128);
         } else {
             uint8_t tmp[64];
+            const MsmPrecomp<Fq> pre{rb.pre_table.view<G1A>(), rb.pre_c, rb.pre_windows};
             msm_run<Fq>(b.msm, rb.points.view<G1A>(), reinterpret_cast<const uint32_t*>(d_scalars), offs.data(), 1,
-                        window_for<Fq>(b, offs), st, tmp, &b.msm_stats);
+                        window_for<Fq>(b, offs), st, tmp, &b.msm_stats, rb.pre_c ? &pre : nullptr);
             memcpy(result_host, tmp, 64);
         }
+    });
+}
+
+extern "C" int dvgpu_bn254_msm_resident_host(void* opaque, uint64_t bases_handle, const uint8_t* scalars,
+                                             size_t length, uint8_t* result, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(result && (!length || scalars), "invalid resident MSM arguments");
+        uint8_t* d_sc = b.in_scalars.as<uint8_t>(std::max<size_t>(1, length) * 32);
+        if (length) DV_CUDA(cudaMemcpyAsync(d_sc, scalars, length * 32, cudaMemcpyHostToDevice, b.stream));
+        char err2[256];
+        const int rc = dvgpu_bn254_msm_resident(opaque, bases_handle, d_sc, length, result, nullptr, err2, sizeof err2);
+        if (rc == -1) throw InvalidArgument(err2);
+        if (rc != 0) throw CudaFailure(err2);
     });
 }
 
@@ -951,5 +967,31 @@ extern "C" int dvgpu_msm_autotune(void* opaque, size_t n, int g2, int* best_c, c
             memcpy(log_json, log.data(), k);
             log_json[k] = '\0';
         }
+    });
+}
+
+// ============================================================ precomputed resident bases
+extern "C" int dvgpu_bases_precompute(void* opaque, uint64_t handle, int c, int* c_used, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        auto it = b.bases.find(handle);
+        require(it != b.bases.end(), "unknown base handle");
+        require(c == 0 || (c >= 8 && c <= 22), "window width must be 0 (automatic) or within 8..22");
+        ResidentBases& rb = *it->second;
+        const MsmPlan plan = c ? MsmPlan{c, (255 + c - 1) / c, 1u << (c - 1), std::min(3, c - 1)}
+                               : msm_plan_precomputed(rb.n);
+        rb.pre_table.release();
+        rb.pre_c = rb.pre_windows = 0;
+        if (rb.n) {
+            if (rb.g2)
+                msm_precompute<Fq2>(rb.points.view<G2A>(), rb.n, plan.c, plan.windows,
+                                    rb.pre_table.as<G2A>(rb.n * (uint64_t)plan.windows), b.stream);
+            else
+                msm_precompute<Fq>(rb.points.view<G1A>(), rb.n, plan.c, plan.windows,
+                                   rb.pre_table.as<G1A>(rb.n * (uint64_t)plan.windows), b.stream);
+            DV_CUDA(cudaStreamSynchronize(b.stream));
+        }
+        rb.pre_c = plan.c;
+        rb.pre_windows = plan.windows;
+        if (c_used) *c_used = plan.c;
     });
 }

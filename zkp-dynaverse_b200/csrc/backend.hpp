@@ -27,6 +27,8 @@ struct ResidentBases {
     DevBuf points;  // Montgomery affine
     uint64_t n = 0;
     int g2 = 0;
+    DevBuf pre_table;  // optional precomputed window multiples (n * pre_windows entries)
+    int pre_c = 0, pre_windows = 0;
 };
 
 struct Backend {

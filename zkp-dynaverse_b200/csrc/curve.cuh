@@ -119,6 +119,53 @@ struct XYZZ {
     }
 };
 
+// ------------------------------------------------------------- warp helpers
+DV_INL Fq shfl_up(const Fq& a, int d) {
+    Fq r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r.v[i] = __shfl_up_sync(0xffffffffu, a.v[i], d);
+    return r;
+}
+DV_INL Fq shfl_down(const Fq& a, int d) {
+    Fq r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r.v[i] = __shfl_down_sync(0xffffffffu, a.v[i], d);
+    return r;
+}
+DV_INL Fq shfl_idx(const Fq& a, int l) {
+    Fq r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r.v[i] = __shfl_sync(0xffffffffu, a.v[i], l);
+    return r;
+}
+DV_INL Fq2 shfl_up(const Fq2& a, int d) { return {shfl_up(a.c0, d), shfl_up(a.c1, d)}; }
+DV_INL Fq2 shfl_down(const Fq2& a, int d) { return {shfl_down(a.c0, d), shfl_down(a.c1, d)}; }
+DV_INL Fq2 shfl_idx(const Fq2& a, int l) { return {shfl_idx(a.c0, l), shfl_idx(a.c1, l)}; }
+
+// Warp-wide simultaneous inversion: returns 1/x for every lane (x != 0).
+template <class F>
+DV_INL F warp_batch_inverse(const F& x) {
+    const int lane = threadIdx.x & 31;
+    F pre = x;  // inclusive prefix product
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const F o = shfl_up(pre, d);
+        if (lane >= d) pre = F::mul(pre, o);
+    }
+    F suf = x;  // inclusive suffix product
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const F o = shfl_down(suf, d);
+        if (lane + d < 32) suf = F::mul(suf, o);
+    }
+    F total_inv = F::inv(shfl_idx(pre, 31));
+    F excl_pre = shfl_up(pre, 1);
+    F excl_suf = shfl_down(suf, 1);
+    if (lane == 0) excl_pre = F::one();
+    if (lane == 31) excl_suf = F::one();
+    return F::mul(total_inv, F::mul(excl_pre, excl_suf));
+}
+
 typedef Affine<Fq> G1A;
 typedef XYZZ<Fq> G1X;
 typedef Affine<Fq2> G2A;

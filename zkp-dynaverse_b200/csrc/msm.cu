@@ -38,6 +38,7 @@ DV_INL uint32_t set_of(const uint32_t* set_off, uint32_t count, uint32_t i) {
 }
 
 // 1. Histogram of signed digits.
+template <bool PRE>
 __global__ void k_hist(const uint32_t* __restrict__ scalars, uint32_t n, const uint32_t* __restrict__ set_off,
                        uint32_t count, int c, int W, uint32_t* __restrict__ counts, uint32_t* __restrict__ first_bad) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -50,7 +51,8 @@ __global__ void k_hist(const uint32_t* __restrict__ scalars, uint32_t n, const u
     }
     const uint32_t set = count > 1 ? set_of(set_off, count, i) : 0;
     const uint32_t B = 1u << (c - 1), full = 1u << c;
-    const uint32_t base = set * (uint32_t)W * B;
+    // PRE: precomputed window multiples share one bucket set per MSM
+    const uint32_t base = PRE ? set * B : set * (uint32_t)W * B;
     const uint32_t active = __activemask();
     const uint32_t lane = threadIdx.x & 31;
     uint32_t carry = 0;
@@ -61,7 +63,7 @@ __global__ void k_hist(const uint32_t* __restrict__ scalars, uint32_t n, const u
         carry = neg ? 1u : 0u;
         // Warp-aggregated increment: lanes hitting the same bucket (skewed
         // digits, e.g. a top window with few bits) issue one atomic.
-        const uint32_t key = mag ? base + (uint32_t)w * B + mag - 1 : NO_INDEX;
+        const uint32_t key = mag ? base + (PRE ? 0u : (uint32_t)w * B) + mag - 1 : NO_INDEX;
         const uint32_t peers = __match_any_sync(active, key);
         if (key != NO_INDEX && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(counts + key, (uint32_t)__popc(peers));
     }
@@ -151,6 +153,7 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
 }
 
 // 3. Scatter (point index | sign << 31) into bucket order.
+template <bool PRE>
 __global__ void k_scatter(const uint32_t* __restrict__ scalars, uint32_t n, const uint32_t* __restrict__ set_off,
                           uint32_t count, int c, int W, uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -160,7 +163,8 @@ __global__ void k_scatter(const uint32_t* __restrict__ scalars, uint32_t n, cons
     if (!Fr::is_canonical(s)) return;
     const uint32_t set = count > 1 ? set_of(set_off, count, i) : 0;
     const uint32_t B = 1u << (c - 1), full = 1u << c;
-    const uint32_t base = set * (uint32_t)W * B;
+    // PRE: precomputed window multiples share one bucket set per MSM
+    const uint32_t base = PRE ? set * B : set * (uint32_t)W * B;
     const uint32_t active = __activemask();
     const uint32_t lane = threadIdx.x & 31;
     uint32_t carry = 0;
@@ -169,7 +173,7 @@ __global__ void k_scatter(const uint32_t* __restrict__ scalars, uint32_t n, cons
         const bool neg = d > B;
         const uint32_t mag = neg ? full - d : d;
         carry = neg ? 1u : 0u;
-        const uint32_t key = mag ? base + (uint32_t)w * B + mag - 1 : NO_INDEX;
+        const uint32_t key = mag ? base + (PRE ? 0u : (uint32_t)w * B) + mag - 1 : NO_INDEX;
         const uint32_t peers = __match_any_sync(active, key);
         if (key != NO_INDEX) {
             // one atomic per group of lanes with the same bucket; each lane
@@ -178,7 +182,8 @@ __global__ void k_scatter(const uint32_t* __restrict__ scalars, uint32_t n, cons
             uint32_t pos = 0;
             if (lane == leader) pos = atomicAdd(cursor + key, (uint32_t)__popc(peers));
             pos = __shfl_sync(peers, pos, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
-            sorted[pos] = i | (neg ? 0x80000000u : 0u);
+            const uint32_t idx = PRE ? i * (uint32_t)W + (uint32_t)w : i;  // PRE: table entry 2^(c w) P_i
+            sorted[pos] = idx | (neg ? 0x80000000u : 0u);
         }
     }
 }
@@ -359,6 +364,29 @@ __global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, 
     if (t == 0) u_out[blockIdx.x] = sh[0];
 }
 
+// Window multiples of resident bases: table[i W + w] = 2^(c w) P_i (affine,
+// Montgomery).  One thread per base, c doublings per window, normalised with
+// one inversion per warp per window (warp_batch_inverse: every lane takes
+// part, so lanes past n carry infinity).
+template <class F>
+__global__ void __launch_bounds__(128) k_precompute(const Affine<F>* __restrict__ bases, uint64_t n, int W, int c,
+                                                    Affine<F>* __restrict__ table) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < n;
+    XYZZ<F> acc = active ? XYZZ<F>::from_affine(bases[i]) : XYZZ<F>::inf();
+    for (int w = 0; w < W; ++w) {
+        const bool inf = acc.is_inf();
+        const F d = warp_batch_inverse<F>(inf ? F::one() : F::mul(acc.zz, acc.zzz));
+        if (active) {
+            table[i * (uint64_t)W + w] =
+                inf ? Affine<F>::inf()
+                    : Affine<F>{F::mul(acc.x, F::mul(d, acc.zzz)), F::mul(acc.y, F::mul(d, acc.zz))};
+        }
+        if (w + 1 < W)
+            for (int k = 0; k < c; ++k) acc = XYZZ<F>::dbl(acc);
+    }
+}
+
 // Canonical -> Montgomery conversion with validation.
 DV_INL bool all_zero_words(const uint32_t* w, int n) {
     uint32_t x = 0;
@@ -474,7 +502,8 @@ void gather_points(const Affine<F>* d_bases, uint64_t nbases, const uint64_t* d_
 
 template <class F>
 void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const uint32_t* set_offsets,
-             uint32_t count, int force_c, cudaStream_t st, uint8_t* host_out, MsmStats* stats) {
+             uint32_t count, int force_c, cudaStream_t st, uint8_t* host_out, MsmStats* stats,
+             const MsmPrecomp<F>* pre) {
     typedef typename HostOf<F>::T HF;
     const size_t out_bytes = 2 * sizeof(F);
     const uint32_t n = set_offsets[count];
@@ -493,11 +522,20 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         plan.buckets = 1u << (plan.c - 1);
         plan.seg_log = std::min(3, plan.c - 1);
     }
+    if (pre) {
+        // precomputed window multiples: the table fixes c and the window count
+        plan.c = pre->c;
+        plan.windows = pre->windows;
+        plan.buckets = 1u << (plan.c - 1);
+        plan.seg_log = std::min(3, plan.c - 1);
+        if ((uint64_t)n * plan.windows >= (1ull << 31)) throw InvalidArgument("precomputed MSM too large");
+    }
     if ((uint64_t)count * plan.windows * plan.buckets > (1ull << 31) || (uint64_t)n * plan.windows > 0xffffffffull)
         throw InvalidArgument("MSM batch too large for one launch sequence");
     const int c = plan.c, W = plan.windows;
     const uint32_t B = plan.buckets;
-    const uint32_t NW = count * (uint32_t)W;
+    const uint32_t Wr = pre ? 1u : (uint32_t)W;  // bucket sets (reduction windows) per MSM
+    const uint32_t NW = count * Wr;
     const uint32_t NB = NW * B;
 
     uint32_t* d_set = ws.set_off.as<uint32_t>(count + 1);
@@ -518,7 +556,8 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         if (tl.enabled) DV_CUDA(cudaEventRecord(tl.ev[k], st));
     };
     mark(0);
-    k_hist<<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_counts, d_err);
+    if (pre) k_hist<true><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_counts, d_err);
+    else k_hist<false><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_counts, d_err);
     DV_LAUNCH();
     mark(1);
     {
@@ -532,7 +571,8 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         DV_LAUNCH();
     }
     mark(2);
-    k_scatter<<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_cursor, d_sorted);
+    if (pre) k_scatter<true><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_cursor, d_sorted);
+    else k_scatter<false><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_cursor, d_sorted);
     DV_LAUNCH();
     mark(3);
 
@@ -577,7 +617,8 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         const uint32_t w0 = bounds[gi], w1 = bounds[gi + 1];
         const uint32_t gb0 = w0 * B, nbg = (w1 - w0) * B;
         if (tl.enabled) DV_CUDA(cudaEventRecord(tl.acc_ev[2 * gi], st));
-        k_accum<F><<<grid, 128, 0, st>>>(d_points, d_sorted, d_offsets + gb0, nbg, d_buckets + gb0, d_pgid, d_ppt);
+        k_accum<F><<<grid, 128, 0, st>>>(pre ? pre->table : d_points, d_sorted, d_offsets + gb0, nbg, d_buckets + gb0,
+                                         d_pgid, d_ppt);
         DV_LAUNCH();
         if (tl.enabled) DV_CUDA(cudaEventRecord(tl.acc_ev[2 * gi + 1], st));
         uint32_t* d_fix_count = ws.fix_count.as<uint32_t>(1);
@@ -626,7 +667,7 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         throw InvalidArgument("non-canonical scalar at index " + std::to_string(*h_err));
     static_assert(sizeof(XYZZ<F>) == sizeof(dvh::XYZZ<HF>), "host/device XYZZ layout");
     const auto* hw = reinterpret_cast<const dvh::XYZZ<HF>*>(h_win);
-    for (uint32_t k = 0; k < count; ++k) horner(hw + (size_t)k * W, W, c, host_out + (size_t)k * out_bytes);
+    for (uint32_t k = 0; k < count; ++k) horner(hw + (size_t)k * Wr, (int)Wr, c, host_out + (size_t)k * out_bytes);
     if (tl.enabled) {
         DV_CUDA(cudaEventRecord(tl.ev[6], st));
         DV_CUDA(cudaEventSynchronize(tl.ev[6]));
@@ -656,9 +697,33 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
 }
 
 template void msm_run<Fq>(MsmWorkspace&, const Affine<Fq>*, const uint32_t*, const uint32_t*, uint32_t, int,
-                          cudaStream_t, uint8_t*, MsmStats*);
+                          cudaStream_t, uint8_t*, MsmStats*, const MsmPrecomp<Fq>*);
 template void msm_run<Fq2>(MsmWorkspace&, const Affine<Fq2>*, const uint32_t*, const uint32_t*, uint32_t, int,
-                           cudaStream_t, uint8_t*, MsmStats*);
+                           cudaStream_t, uint8_t*, MsmStats*, const MsmPrecomp<Fq2>*);
+
+template <class F>
+void msm_precompute(const Affine<F>* d_bases, uint64_t n, int c, int windows, Affine<F>* d_table, cudaStream_t st) {
+    if (!n) return;
+    k_precompute<F><<<blocks_for(n, 128), 128, 0, st>>>(d_bases, n, windows, c, d_table);
+    DV_LAUNCH();
+}
+template void msm_precompute<Fq>(const Affine<Fq>*, uint64_t, int, int, Affine<Fq>*, cudaStream_t);
+template void msm_precompute<Fq2>(const Affine<Fq2>*, uint64_t, int, int, Affine<Fq2>*, cudaStream_t);
+
+MsmPlan msm_plan_precomputed(uint64_t n) {
+    // one shared bucket set: windows * 10 n additions + 28 * 2^(c-1) for the reduction
+    MsmPlan p{};
+    double best = 1e300;
+    for (int c = 8; c <= 22; ++c) {
+        const double W = (255 + c - 1) / c;
+        const double cost = W * 10.0 * (double)n + 28.0 * (double)(1u << (c - 1));
+        if (cost < best) { best = cost; p.c = c; }
+    }
+    p.windows = (255 + p.c - 1) / p.c;
+    p.buckets = 1u << (p.c - 1);
+    p.seg_log = std::min(3, p.c - 1);
+    return p;
+}
 template void convert_points<Fq>(const uint8_t*, Affine<Fq>*, uint64_t, uint32_t*, cudaStream_t);
 template void convert_points<Fq2>(const uint8_t*, Affine<Fq2>*, uint64_t, uint32_t*, cudaStream_t);
 template void gather_points<Fq>(const Affine<Fq>*, uint64_t, const uint64_t*, uint64_t, Affine<Fq>*, uint32_t*,

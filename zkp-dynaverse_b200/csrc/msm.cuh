@@ -16,10 +16,12 @@
 //               sums a fixed-length slice of the sorted list with XYZZ mixed
 //               additions; buckets cut by a slice boundary leave partials
 //   5. fixup    partial sums of buckets that span slices are merged
-//   6. segments per (set, window): running sums over segments of 2^seg_log
-//               buckets, each segment weighted by its offset (small scalar mul)
-//   7. wsum     per (set, window) block reduction of the segment values
+//   6. segments per (set, window): running sums over segments of 2^seg_log buckets
+//   7. wlevel   logarithmic-depth levels of the weighted bucket sum (suffix
+//               scan + tree per block), down to one value per (set, window)
 //   8. host     Horner over the windows and normalisation to affine
+// With a table of precomputed window multiples (resident bases), steps 1-7
+// use one bucket set per MSM and step 8 only normalises.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -68,6 +70,16 @@ struct MsmStats {
     uint64_t calls = 0, sets = 0, points = 0, last_c = 0;
 };
 
+// Precomputed window multiples of a fixed base set (a resident SRS):
+// table[i * windows + w] = 2^(c w) P_i.  With a table, every window of an MSM
+// adds into one shared bucket set and no window combination is needed.
+template <class F>
+struct MsmPrecomp {
+    const Affine<F>* table;
+    int c;
+    int windows;
+};
+
 // d_points: Montgomery-form affine points, d_scalars: canonical 8-word
 // little-endian scalars (checked < r), both concatenated over sets.
 // set_offsets (host, count + 1 entries) delimit the sets.  host_out receives
@@ -75,7 +87,14 @@ struct MsmStats {
 // infinity).  Throws InvalidArgument for non-canonical scalars.
 template <class F>
 void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const uint32_t* set_offsets,
-             uint32_t count, int force_c, cudaStream_t stream, uint8_t* host_out, MsmStats* stats);
+             uint32_t count, int force_c, cudaStream_t stream, uint8_t* host_out, MsmStats* stats,
+             const MsmPrecomp<F>* pre = nullptr);
+
+// Builds the table of precomputed window multiples (windows * n entries).
+template <class F>
+void msm_precompute(const Affine<F>* d_bases, uint64_t n, int c, int windows, Affine<F>* d_table, cudaStream_t stream);
+// Window width for a precomputed table of n bases (cost model).
+MsmPlan msm_plan_precomputed(uint64_t n);
 
 // Canonical bytes -> Montgomery affine, with canonical and on-curve checks.
 // Sets *first_bad (device) to the lowest failing index, or leaves it.
