@@ -32,7 +32,7 @@ struct FrCfg {
 #define DV_INL __device__ __forceinline__
 
 template <class C>
-struct Fp {
+struct __align__(16) Fp {  // 16-byte aligned: global copies move as 128-bit accesses
     uint32_t v[8];
 
     DV_INL static Fp zero() {

@@ -81,37 +81,65 @@ __global__ void k_pow_table(const Fr* __restrict__ base_p, const Fr* __restrict_
     }
 }
 
-// Shared-memory word planes: plane j holds word j of every element, padded
-// by one word per 32 elements so strided element access stays bank-free.
-DV_INL uint32_t plane_stride(uint32_t n) { return n + (n >> 5); }
-DV_INL void load_plane(const uint32_t* sm, uint32_t n, uint32_t t, Fr& a) {
-    const uint32_t ps = plane_stride(n), o = t + (t >> 5);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) a.v[j] = sm[j * ps + o];
+// Shared-memory staging: two planes of 16-byte halves (plane 0: words 0-3 of
+// every element, plane 1: words 4-7), so an element moves with two 128-bit
+// accesses.  A 128-bit access is served eight threads at a time, one
+// 128-byte row of 8 slots, so eight threads must hit eight distinct slots
+// (index mod 8).  Within a round, the eight threads' element indices differ
+// in three bits taken from {0..5} (the low tau bits land on element bits
+// [0, b_lo) and [b_lo + RR, ...)).  The slot is e XOR S(e[3..5]) with
+// S linear over GF(2): e3 -> 7, e4 -> 5, e5 -> 6; for every (b_lo, RR) with
+// RR <= 3 the three varying bits map to independent slot vectors, so the
+// rows are conflict-free.  SWZ packs S(b) for b = 0..7 in nibbles.
+constexpr uint32_t SWZ = 0x43162570u;
+DV_INL uint32_t slot(uint32_t e) { return e ^ ((SWZ >> (((e >> 3) & 7u) << 2)) & 7u); }
+DV_INL void load_plane(const uint32_t* sm, uint32_t n, uint32_t e, Fr& a) {
+    const uint4* s4 = reinterpret_cast<const uint4*>(sm);
+    const uint32_t o = slot(e);
+    const uint4 lo = s4[o], hi = s4[n + o];
+    a.v[0] = lo.x; a.v[1] = lo.y; a.v[2] = lo.z; a.v[3] = lo.w;
+    a.v[4] = hi.x; a.v[5] = hi.y; a.v[6] = hi.z; a.v[7] = hi.w;
 }
-DV_INL void store_plane(uint32_t* sm, uint32_t n, uint32_t t, const Fr& a) {
-    const uint32_t ps = plane_stride(n), o = t + (t >> 5);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) sm[j * ps + o] = a.v[j];
+DV_INL void store_plane(uint32_t* sm, uint32_t n, uint32_t e, const Fr& a) {
+    uint4* s4 = reinterpret_cast<uint4*>(sm);
+    const uint32_t o = slot(e);
+    s4[o] = make_uint4(a.v[0], a.v[1], a.v[2], a.v[3]);
+    s4[n + o] = make_uint4(a.v[4], a.v[5], a.v[6], a.v[7]);
 }
+
+// Arguments of one DIF pass (kernel parameters, passed by value).
+struct PassArgs {
+    const uint8_t* in;        // first pass: canonical input bytes
+    Fr* work;                 // working vector (bit-reversed order after the last pass)
+    uint8_t* out;             // non-null on a fused last pass: natural-order output bytes
+    const Fr* tw;             // w^i, i < n/2
+    const Fr* pre_hi;         // coset pre-scale g^i (two-level table), first pass only
+    const Fr* pre_lo;
+    const Fr* post_hi;        // fused last pass: coset post-scale g^-i n^-1
+    const Fr* post_lo;
+    const Fr* post_const;     // fused last pass: n^-1 (plain inverse)
+    uint32_t* first_bad;      // lowest non-canonical input index
+    int logn, s0, k, first, split;
+};
 
 // One DIF pass over stages [s0, s0 + k) for one group of G = 2^k elements
 // (stride 2^lb in the vector).  Register-blocked: the k stages are processed
 // in rounds of up to R = 2^R_LOG elements per thread; a round loads R
 // elements that differ only in its bits, runs its radix-2 stages in
-// registers and writes them back, so shared memory (8 word planes, bank-
-// conflict free) is touched once per round rather than once per stage.  The
-// first round reads global memory directly (first pass: canonical check and
-// coset pre-scale), the last round writes global memory directly.
+// registers and writes them back, so shared memory is touched once per
+// round rather than once per stage.  The first round reads global memory
+// directly (first pass: canonical check and coset pre-scale); the last round
+// writes global memory directly: the working vector, or, on a fused last
+// pass, the output bytes at the bit-reversed position with the inverse or
+// coset post-scale applied.
 // One round of RR stages: thread-group tau owns the 2^RR elements that differ
 // only in local bits [bit_hi - RR, bit_hi).  RR is a compile-time constant so
 // the element array stays in registers.
 template <int RR, int THREADS>
-DV_INL void dif_round(const uint8_t* __restrict__ in, Fr* __restrict__ work, uint32_t* sm, int logn, int s0, int k,
-                      int lb, uint64_t low, uint64_t high, int bit_hi, bool first_round, bool first,
-                      const Fr* __restrict__ tw, const Fr* __restrict__ pre_hi, const Fr* __restrict__ pre_lo,
-                      int split, uint32_t* __restrict__ first_bad) {
+DV_INL void dif_round(const PassArgs& a, uint32_t* sm, int lb, uint64_t low, uint64_t high, int bit_hi,
+                      bool first_round) {
     constexpr int R = 1 << RR;
+    const int k = a.k;
     const uint32_t G = 1u << k;
     const int b_lo = bit_hi - RR;
     const bool last_round = b_lo == 0;
@@ -124,11 +152,11 @@ DV_INL void dif_round(const uint8_t* __restrict__ in, Fr* __restrict__ work, uin
             const uint32_t e = base_e | ((uint32_t)m << b_lo);
             const uint64_t idx = (high << (lb + k)) | ((uint64_t)e << lb) | low;
             if (first_round) {
-                if (first) {
+                if (a.first) {
                     uint32_t c[8];
-                    load_words(in + 32 * idx, c);
+                    load_words(a.in + 32 * idx, c);
                     if (!Fr::is_canonical(c)) {
-                        atomicMin(first_bad, (uint32_t)idx);
+                        atomicMin(a.first_bad, (uint32_t)idx);
 #pragma unroll
                         for (int j = 0; j < 8; ++j) c[j] = 0;
                     }
@@ -136,12 +164,12 @@ DV_INL void dif_round(const uint8_t* __restrict__ in, Fr* __restrict__ work, uin
                     for (int j = 0; j < 8; ++j) x[m].v[j] = c[j];
                     // values stay canonical: multipliers are held in
                     // Montgomery form and mont_mul(a, x R) = a x
-                    if (pre_hi) {
-                        const uint64_t lo_mask = (1ull << split) - 1;
-                        x[m] = Fr::mul_inl(Fr::mul_inl(x[m], pre_hi[idx >> split]), pre_lo[idx & lo_mask]);
+                    if (a.pre_hi) {
+                        const uint64_t lo_mask = (1ull << a.split) - 1;
+                        x[m] = Fr::mul_inl(Fr::mul_inl(x[m], a.pre_hi[idx >> a.split]), a.pre_lo[idx & lo_mask]);
                     }
                 } else {
-                    x[m] = work[idx];
+                    x[m] = a.work[idx];
                 }
             } else {
                 load_plane(sm, G, e, x[m]);
@@ -149,9 +177,9 @@ DV_INL void dif_round(const uint8_t* __restrict__ in, Fr* __restrict__ work, uin
         }
 #pragma unroll
         for (int j = 0; j < RR; ++j) {
-            const int s = s0 + (k - bit_hi) + j;  // global stage
-            const int pb = bit_hi - 1 - j;        // local bit of this stage
-            const int hs = 1 << (RR - 1 - j);    // pair distance in m
+            const int s = a.s0 + (k - bit_hi) + j;  // global stage
+            const int pb = bit_hi - 1 - j;          // local bit of this stage
+            const int hs = 1 << (RR - 1 - j);      // pair distance in m
             // issue this stage's twiddle loads before its butterflies
             Fr w[R / 2];
 #pragma unroll
@@ -159,7 +187,7 @@ DV_INL void dif_round(const uint8_t* __restrict__ in, Fr* __restrict__ work, uin
                 if (m & hs) continue;
                 const uint32_t e = base_e | ((uint32_t)m << b_lo);
                 const uint64_t jp = ((uint64_t)(e & ((1u << pb) - 1)) << lb) | low;
-                w[q++] = tw[jp << s];
+                w[q++] = a.tw[jp << s];
             }
 #pragma unroll
             for (int m = 0, q = 0; m < R; ++m) {
@@ -174,7 +202,19 @@ DV_INL void dif_round(const uint8_t* __restrict__ in, Fr* __restrict__ work, uin
             const uint32_t e = base_e | ((uint32_t)m << b_lo);
             if (last_round) {
                 const uint64_t idx = (high << (lb + k)) | ((uint64_t)e << lb) | low;
-                work[idx] = x[m];
+                if (a.out) {
+                    const uint64_t i = __brevll(idx) >> (64 - a.logn);
+                    Fr y = x[m];
+                    if (a.post_hi) {
+                        const uint64_t lo_mask = (1ull << a.split) - 1;
+                        y = Fr::mul_inl(Fr::mul_inl(y, a.post_hi[i >> a.split]), a.post_lo[i & lo_mask]);
+                    } else if (a.post_const) {
+                        y = Fr::mul_inl(y, *a.post_const);
+                    }
+                    store_words(a.out + 32 * i, y.v);
+                } else {
+                    a.work[idx] = x[m];
+                }
             } else {
                 store_plane(sm, G, e, x[m]);
             }
@@ -182,53 +222,47 @@ DV_INL void dif_round(const uint8_t* __restrict__ in, Fr* __restrict__ work, uin
     }
 }
 
-template <int THREADS, int R_LOG>
 #ifndef DV_NTT_MINB
 #define DV_NTT_MINB 3
 #endif
 #ifndef DV_NTT_RADIX_LOG
 #define DV_NTT_RADIX_LOG 2
 #endif
-__global__ void __launch_bounds__(THREADS, (THREADS >= 256 ? DV_NTT_MINB : 8)) k_dif_pass(const uint8_t* __restrict__ in, Fr* __restrict__ work, int logn,
-                                                      int s0, int k, const Fr* __restrict__ tw, int first,
-                                                      const Fr* __restrict__ pre_hi, const Fr* __restrict__ pre_lo,
-                                                      int split, uint32_t* __restrict__ first_bad) {
-    extern __shared__ uint32_t sm[];
-    const int lb = logn - s0 - k;
+template <int THREADS, int R_LOG>
+__global__ void __launch_bounds__(THREADS, (THREADS >= 256 ? DV_NTT_MINB : 8)) k_dif_pass(const PassArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    const int k = a.k;
+    const int lb = a.logn - a.s0 - k;
     const uint64_t g = blockIdx.x;
     const uint64_t low = g & ((1ull << lb) - 1), high = g >> lb;
-    const uint32_t tid = threadIdx.x;
     int bit_hi = k;
     bool first_round = true;
     while (bit_hi > 0) {
         const int rr = bit_hi < R_LOG ? bit_hi : R_LOG;
-        if (rr == 3 && R_LOG >= 3) dif_round<(R_LOG >= 3 ? 3 : 1), THREADS>(in, work, sm, logn, s0, k, lb, low, high, bit_hi, first_round, first, tw,
-                                           pre_hi, pre_lo, split, first_bad);
-        else if (rr == 2) dif_round<2, THREADS>(in, work, sm, logn, s0, k, lb, low, high, bit_hi, first_round, first,
-                                                tw, pre_hi, pre_lo, split, first_bad);
-        else dif_round<1, THREADS>(in, work, sm, logn, s0, k, lb, low, high, bit_hi, first_round, first, tw, pre_hi,
-                                   pre_lo, split, first_bad);
+        if (rr == 3 && R_LOG >= 3) dif_round<(R_LOG >= 3 ? 3 : 1), THREADS>(a, sm, lb, low, high, bit_hi, first_round);
+        else if (rr == 2) dif_round<2, THREADS>(a, sm, lb, low, high, bit_hi, first_round);
+        else dif_round<1, THREADS>(a, sm, lb, low, high, bit_hi, first_round);
         __syncthreads();
         bit_hi -= rr;
         first_round = false;
     }
     if (k == 0) {  // single element: copy (with the first pass's check)
-        if (tid == 0) {
+        if (threadIdx.x == 0) {
             const uint64_t idx = (high << lb) | low;
-            Fr a;
-            if (first) {
+            Fr v;
+            if (a.first) {
                 uint32_t c[8];
-                load_words(in + 32 * idx, c);
+                load_words(a.in + 32 * idx, c);
                 if (!Fr::is_canonical(c)) {
-                    atomicMin(first_bad, (uint32_t)idx);
+                    atomicMin(a.first_bad, (uint32_t)idx);
                     for (int j = 0; j < 8; ++j) c[j] = 0;
                 }
-                for (int j = 0; j < 8; ++j) a.v[j] = c[j];
-                if (pre_hi) a = Fr::mul_inl(Fr::mul_inl(a, pre_hi[0]), pre_lo[0]);
+                for (int j = 0; j < 8; ++j) v.v[j] = c[j];
+                if (a.pre_hi) v = Fr::mul_inl(Fr::mul_inl(v, a.pre_hi[0]), a.pre_lo[0]);
             } else {
-                a = work[idx];
+                v = a.work[idx];
             }
-            work[idx] = a;
+            a.work[idx] = v;
         }
     }
 }
@@ -250,18 +284,52 @@ __global__ void k_permute(const Fr* __restrict__ work, uint8_t* __restrict__ out
     store_words(out + 32 * i, a.v);
 }
 
+constexpr int MAX_DEVICES = 64;
+
 template <int THREADS>
-void launch_pass(const uint8_t* in, Fr* work, int logn, int s0, int k, const Fr* tw, int first, const Fr* pre_hi,
-                 const Fr* pre_lo, int split, uint32_t* bad, cudaStream_t st) {
-    const size_t smem = (size_t)8 * sizeof(uint32_t) * ((1u << k) + ((1u << k) >> 5));
-    static bool configured = false;
-    if (!configured) {
-        DV_CUDA(cudaFuncSetAttribute(k_dif_pass<THREADS, DV_NTT_RADIX_LOG>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-        configured = true;
+void launch_pass(const PassArgs& a, cudaStream_t st) {
+    const size_t smem = (size_t)32 << a.k;  // two planes of 16 bytes per element
+    static bool configured[MAX_DEVICES] = {};
+    int dev = 0;
+    DV_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= MAX_DEVICES) throw InvalidArgument("device ordinal out of range");
+    if (!configured[dev]) {
+        DV_CUDA(cudaFuncSetAttribute(k_dif_pass<THREADS, DV_NTT_RADIX_LOG>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        configured[dev] = true;
     }
-    const unsigned groups = 1u << (logn - k);
-    k_dif_pass<THREADS, DV_NTT_RADIX_LOG><<<groups, THREADS, smem, st>>>(in, work, logn, s0, k, tw, first, pre_hi, pre_lo, split, bad);
+    const unsigned groups = 1u << (a.logn - a.k);
+    k_dif_pass<THREADS, DV_NTT_RADIX_LOG><<<groups, THREADS, smem, st>>>(a);
     DV_LAUNCH();
+}
+
+// Runs the DIF passes of a transform of 2^logn elements.  With fuse_out the
+// last pass (of two or more) writes the natural-order output bytes itself;
+// a single pass never does, since its one block may read and write the same
+// positions of an in-place vector within one round.  Returns whether the
+// output was written (otherwise k_permute must run).
+bool run_passes(const uint8_t* d_in, Fr* work, uint8_t* d_out, int logn, const Fr* tw, const Fr* pre_hi,
+                const Fr* pre_lo, const Fr* post_hi, const Fr* post_lo, const Fr* post_const, int split,
+                uint32_t* bad, bool fuse_out, cudaStream_t st) {
+    PassArgs a{d_in, work, nullptr, tw, pre_hi, pre_lo, post_hi, post_lo, post_const, bad, logn, 0, 0, 1, split};
+    if (logn == 0) {
+        // single element: conversion round trip checks canonical form
+        launch_pass<32>(a, st);
+        return false;
+    }
+    const int passes = (logn + 10) / 11;
+    const bool fused = fuse_out && passes >= 2;
+    int s0 = 0;
+    for (int p = 0; p < passes; ++p) {
+        a.k = logn / passes + (p < logn % passes ? 1 : 0);
+        a.s0 = s0;
+        a.first = p == 0;
+        a.out = (fused && p == passes - 1) ? d_out : nullptr;
+        if (a.k >= 9) launch_pass<256>(a, st);
+        else launch_pass<64>(a, st);
+        s0 += a.k;
+    }
+    return fused;
 }
 
 }  // namespace
@@ -317,28 +385,15 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
     DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
 
     const Fr* tw = tab->tw.as<Fr>(1);
-    const Fr* pre_hi0 = (coset && !inverse) ? tab->pre_hi.as<Fr>(1) : nullptr;
-    const Fr* pre_lo0 = (coset && !inverse) ? tab->pre_lo.as<Fr>(1) : nullptr;
-    if (logn == 0) {
-        // single element: conversion round trip checks canonical form
-        launch_pass<32>(d_in, work, 0, 0, 0, tw, 1, pre_hi0, pre_lo0, split, bad, st);
-    } else {
-        const int passes = (logn + 10) / 11;
-        int s0 = 0;
-        for (int p = 0; p < passes; ++p) {
-            const int k = logn / passes + (p < logn % passes ? 1 : 0);
-            const Fr* pre_hi = (coset && !inverse) ? tab->pre_hi.as<Fr>(1) : nullptr;
-            const Fr* pre_lo = (coset && !inverse) ? tab->pre_lo.as<Fr>(1) : nullptr;
-            if (k >= 9) launch_pass<256>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, bad, st);
-            else launch_pass<64>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, bad, st);
-            s0 += k;
-        }
-    }
+    const Fr* pre_hi = (coset && !inverse) ? tab->pre_hi.as<Fr>(1) : nullptr;
+    const Fr* pre_lo = (coset && !inverse) ? tab->pre_lo.as<Fr>(1) : nullptr;
     const Fr* post_hi = (coset && inverse) ? tab->post_hi.as<Fr>(1) : nullptr;
     const Fr* post_lo = (coset && inverse) ? tab->post_lo.as<Fr>(1) : nullptr;
     const Fr* post_const = inverse ? kc + C_NINV : nullptr;
-    k_permute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(work, d_out, logn, post_hi, post_lo, split, post_const);
-    DV_LAUNCH();
+    if (!run_passes(d_in, work, d_out, logn, tw, pre_hi, pre_lo, post_hi, post_lo, post_const, split, bad, true, st)) {
+        k_permute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(work, d_out, logn, post_hi, post_lo, split, post_const);
+        DV_LAUNCH();
+    }
     uint32_t host_bad = 0;
     DV_CUDA(cudaMemcpyAsync(&host_bad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaStreamSynchronize(st));
@@ -435,18 +490,7 @@ void ntt_noalloc(const uint8_t* d_in, uint8_t* d_out, int logn, int kind, cudaSt
     }
     const Fr* pre_hi = (coset && !inverse) ? hi : nullptr;
     const Fr* pre_lo = (coset && !inverse) ? lo : nullptr;
-    if (logn == 0) {
-        launch_pass<32>(d_in, work, 0, 0, 0, tw, 1, pre_hi, pre_lo, split, bad, st);
-    } else {
-        const int passes = (logn + 10) / 11;
-        int s0 = 0;
-        for (int p = 0; p < passes; ++p) {
-            const int k = logn / passes + (p < logn % passes ? 1 : 0);
-            if (k >= 9) launch_pass<256>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, bad, st);
-            else launch_pass<64>(d_in, work, logn, s0, k, tw, p == 0, pre_hi, pre_lo, split, bad, st);
-            s0 += k;
-        }
-    }
+    run_passes(d_in, work, d_out, logn, tw, pre_hi, pre_lo, nullptr, nullptr, nullptr, split, bad, false, st);
     k_permute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(work, d_out, logn, (coset && inverse) ? hi : nullptr,
                                                           (coset && inverse) ? lo : nullptr, split,
                                                           inverse ? kc + C_NINV : nullptr);
