@@ -227,10 +227,8 @@ int dvgpu_probe_imad_rate(void* backend, double* macs_per_second, char* error, s
 uint64_t dvgpu_launch_count(void);
 /* Per-phase MSM device time, accumulated over calls while enabled (CUDA
  * events on the launching stream).  ms[]: 0 digit histogram, 1 offsets scan,
- * 2 scatter, 3 bucket accumulation (sum of its launches), 4 split-bucket
- * merges plus the part of the first window group's reduction that overlaps
- * the accumulation, 5 reduction tail of the last group, 6 unused, 7 tail
- * (window D2H + host Horner).  enable = 1
+ * 2 scatter, 3 bucket accumulation, 4 split-bucket merges, 5 bucket
+ * reduction, 6 unused, 7 tail (window D2H + host Horner).  enable = 1
  * resets and starts, 0 stops; out (may be NULL) receives the totals so far. */
 typedef struct DvgpuMsmPhaseTimes {
     double ms[8];
@@ -245,6 +243,57 @@ int dvgpu_random_fr_device(void* backend, uint64_t seed, size_t n, uint8_t* d_ou
                            size_t error_capacity);
 int dvgpu_fr_powers_device(void* backend, const uint8_t* d_tau, size_t n, uint8_t* d_out, void* stream, char* error,
                            size_t error_capacity);
+
+/* ---------------------------------------------------------------- batching
+ * No counterpart in the reference ABI (its batch path is
+ * dvgpu_bn254_msm_batch with next-pow2 padding, icicle_msm.cu:810-880, and
+ * one dvgpu_bn254_ntt call per vector, icicle.rs:429-456).
+ *
+ * dvgpu_bn254_ntt_batch: count transforms of sizes 2^log_sizes[i]
+ * (1 <= log <= 24) in ONE persistent launch.  values / results: the
+ * transforms' canonical elements concatenated in order (may alias);
+ * kinds[i] as in dvgpu_bn254_ntt_ex (NULL = all forward).  The _device form
+ * takes device buffers and returns after `stream` has completed. */
+int dvgpu_bn254_ntt_batch(void* backend, const uint8_t* values, const uint32_t* log_sizes, const int32_t* kinds,
+                          size_t count, uint8_t* results, char* error, size_t error_capacity);
+int dvgpu_bn254_ntt_batch_device(void* backend, const uint8_t* d_values, const uint32_t* log_sizes,
+                                 const int32_t* kinds, size_t count, uint8_t* d_results, void* stream, char* error,
+                                 size_t error_capacity);
+
+/* Batch plans: a fixed workload of G1 MSMs over prefixes of one registered
+ * G1 base set (MSM i uses bases [0, msm_sizes[i]) and scalars
+ * msm_sizes[0] + ... + msm_sizes[i-1] onwards) plus NTTs of fixed sizes and
+ * kinds, captured once into a CUDA graph and replayed per run.  At creation
+ * the MSMs are grouped into size classes; the autotuner times candidate
+ * window widths per class on random scalars, keeps a table of precomputed
+ * window multiples for the best one and writes its log (JSON) to log_json.
+ * Each class is one launch sequence over all its MSMs; the NTTs are one
+ * persistent launch on a parallel branch of the graph.
+ *
+ * dvgpu_batch_plan_buffers: the plan's device buffers (inputs in request
+ * order, outputs in request order: 64-byte affine G1 results, canonical NTT
+ * elements).  dvgpu_batch_plan_launch: enqueue one replay on `stream` (NULL:
+ * the plan's own stream) and return; dvgpu_batch_plan_check: wait for it and
+ * report invalid inputs (-1) of the last replay.  dvgpu_batch_plan_run: host
+ * inputs and outputs, copies included, synchronous. */
+typedef struct DvgpuBatchPlanBuffers {
+    uint8_t* scalars;      /* sum(msm_sizes) x 32 bytes */
+    uint8_t* ntt_values;   /* sum(2^ntt_log_sizes) x 32 bytes */
+    uint8_t* msm_results;  /* msm_count x 64 bytes */
+    uint8_t* ntt_results;  /* sum(2^ntt_log_sizes) x 32 bytes */
+    uint64_t scalar_bytes, ntt_bytes, msm_result_bytes;
+    uint32_t msm_classes, graph_nodes;
+} DvgpuBatchPlanBuffers;
+int dvgpu_batch_plan_create(void* backend, uint64_t bases_handle, const uint64_t* msm_sizes, size_t msm_count,
+                            const uint32_t* ntt_log_sizes, const int32_t* ntt_kinds, size_t ntt_count,
+                            uint64_t* plan, char* log_json, size_t log_capacity, char* error, size_t error_capacity);
+int dvgpu_batch_plan_buffers(void* backend, uint64_t plan, DvgpuBatchPlanBuffers* out, char* error,
+                             size_t error_capacity);
+int dvgpu_batch_plan_launch(void* backend, uint64_t plan, void* stream, char* error, size_t error_capacity);
+int dvgpu_batch_plan_check(void* backend, uint64_t plan, char* error, size_t error_capacity);
+int dvgpu_batch_plan_run(void* backend, uint64_t plan, const uint8_t* scalars, const uint8_t* ntt_values,
+                         uint8_t* msm_results, uint8_t* ntt_results, char* error, size_t error_capacity);
+int dvgpu_batch_plan_destroy(void* backend, uint64_t plan, char* error, size_t error_capacity);
 
 #ifdef __cplusplus
 }

@@ -59,7 +59,14 @@ class MsmPhaseTimes(ctypes.Structure):
     _fields_ = [("ms", ctypes.c_double * 8), ("calls", ctypes.c_uint64), ("accum_mixed_adds", ctypes.c_uint64)]
 
 
-MSM_PHASE_NAMES = ["hist", "scan", "scatter", "accum", "merge_and_overlapped_reduce", "reduce_tail", "unused", "tail"]
+MSM_PHASE_NAMES = ["hist", "scan", "scatter", "accum", "merge", "reduce", "unused", "tail"]
+
+
+class BatchPlanBuffers(ctypes.Structure):
+    _fields_ = [("scalars", ctypes.c_void_p), ("ntt_values", ctypes.c_void_p), ("msm_results", ctypes.c_void_p),
+                ("ntt_results", ctypes.c_void_p), ("scalar_bytes", ctypes.c_uint64), ("ntt_bytes", ctypes.c_uint64),
+                ("msm_result_bytes", ctypes.c_uint64), ("msm_classes", ctypes.c_uint32),
+                ("graph_nodes", ctypes.c_uint32)]
 
 
 class SetupStats(ctypes.Structure):
@@ -118,6 +125,15 @@ SIGNATURES = [
     ("dvgpu_msm_timeline", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(MsmPhaseTimes)]),
     ("dvgpu_random_fr_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
     ("dvgpu_fr_powers_device", ctypes.c_int, [_P, _P, _SZ, _P, _P] + _E),
+    ("dvgpu_bn254_ntt_batch", ctypes.c_int, [_P, _P, _P, _P, _SZ, _B] + _E),
+    ("dvgpu_bn254_ntt_batch_device", ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P] + _E),
+    ("dvgpu_batch_plan_create", ctypes.c_int,
+     [_P, ctypes.c_uint64, _P, _SZ, _P, _P, _SZ, ctypes.POINTER(ctypes.c_uint64), _B, _SZ] + _E),
+    ("dvgpu_batch_plan_buffers", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.POINTER(BatchPlanBuffers)] + _E),
+    ("dvgpu_batch_plan_launch", ctypes.c_int, [_P, ctypes.c_uint64, _P] + _E),
+    ("dvgpu_batch_plan_check", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
+    ("dvgpu_batch_plan_run", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _B, _B] + _E),
+    ("dvgpu_batch_plan_destroy", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
 ]
 
 
@@ -474,6 +490,62 @@ class DvgpuBackend:
 
     def fr_powers_device(self, d_tau: int, n: int, d_out: int, stream=None):
         self._call("dvgpu_fr_powers_device", d_tau, n, d_out, stream)
+
+    # ------------------------------------------------------------------ batching
+    def ntt_batch(self, values: bytes, log_sizes, kinds=None) -> bytes:
+        """Transforms of sizes 2^log_sizes[i] (concatenated canonical
+        elements) in one persistent launch; kinds as in ntt_ex (None =
+        forward)."""
+        logs = np.ascontiguousarray(np.asarray(log_sizes, dtype=np.uint32))
+        kd = None if kinds is None else np.ascontiguousarray(np.asarray(kinds, dtype=np.int32))
+        out = ctypes.create_string_buffer(max(1, len(values)))
+        self._call("dvgpu_bn254_ntt_batch", _ptr(values), logs.ctypes.data if logs.size else None,
+                   None if kd is None else kd.ctypes.data, len(logs), out)
+        return out.raw[:len(values)]
+
+    def ntt_batch_device(self, d_values: int, log_sizes, d_out: int, kinds=None, stream=None):
+        logs = np.ascontiguousarray(np.asarray(log_sizes, dtype=np.uint32))
+        kd = None if kinds is None else np.ascontiguousarray(np.asarray(kinds, dtype=np.int32))
+        self._call("dvgpu_bn254_ntt_batch_device", d_values, logs.ctypes.data if logs.size else None,
+                   None if kd is None else kd.ctypes.data, len(logs), d_out, stream)
+
+    def batch_plan_create(self, bases_handle: int, msm_sizes, ntt_log_sizes=(), ntt_kinds=None):
+        """CUDA-graph plan of G1 MSMs over prefixes of registered bases plus
+        NTTs; returns (plan handle, autotuner log dict)."""
+        import json
+        sizes = np.ascontiguousarray(np.asarray(msm_sizes, dtype=np.uint64))
+        logs = np.ascontiguousarray(np.asarray(ntt_log_sizes, dtype=np.uint32))
+        kd = None if ntt_kinds is None else np.ascontiguousarray(np.asarray(ntt_kinds, dtype=np.int32))
+        h = ctypes.c_uint64()
+        log = ctypes.create_string_buffer(1 << 16)
+        self._call("dvgpu_batch_plan_create", bases_handle, sizes.ctypes.data if sizes.size else None, len(sizes),
+                   logs.ctypes.data if logs.size else None, None if kd is None else kd.ctypes.data, len(logs),
+                   ctypes.byref(h), log, len(log))
+        return h.value, json.loads(log.value.decode())
+
+    def batch_plan_buffers(self, plan: int) -> BatchPlanBuffers:
+        b = BatchPlanBuffers()
+        self._call("dvgpu_batch_plan_buffers", plan, ctypes.byref(b))
+        return b
+
+    def batch_plan_launch(self, plan: int, stream=None):
+        self._call("dvgpu_batch_plan_launch", plan, stream)
+
+    def batch_plan_check(self, plan: int):
+        self._call("dvgpu_batch_plan_check", plan)
+
+    def batch_plan_run(self, plan: int, scalars, ntt_values, msm_count: int):
+        """Host inputs (concatenated, request order) -> (list of 64-byte MSM
+        results, concatenated NTT outputs)."""
+        msm_out = ctypes.create_string_buffer(max(1, msm_count) * G1_BYTES)
+        nbytes = 0 if ntt_values is None else len(ntt_values)
+        ntt_out = ctypes.create_string_buffer(max(1, nbytes))
+        self._call("dvgpu_batch_plan_run", plan, _ptr(scalars), _ptr(ntt_values), msm_out, ntt_out)
+        raw = msm_out.raw
+        return [raw[i * G1_BYTES:(i + 1) * G1_BYTES] for i in range(msm_count)], ntt_out.raw[:nbytes]
+
+    def batch_plan_destroy(self, plan: int):
+        self._call("dvgpu_batch_plan_destroy", plan)
 
     def probe_imad_rate(self) -> float:
         v = ctypes.c_double()

@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "abi_util.hpp"
 #include "backend.hpp"
 #include "g2.cuh"
 #include "host_curve.hpp"
@@ -17,50 +18,6 @@
 using namespace dv;
 
 namespace {
-
-int fail(int status, const std::string& msg, char* error, size_t cap) {
-    if (error && cap) {
-        const size_t n = std::min(cap - 1, msg.size());
-        memcpy(error, msg.data(), n);
-        error[n] = '\0';
-    }
-    return status;
-}
-
-template <class Fn>
-int guarded(void* opaque, char* error, size_t cap, Fn&& fn) {
-    auto* b = static_cast<Backend*>(opaque);
-    if (!b) return fail(-1, "null backend", error, cap);
-    if (b->retired) return fail(-4, "backend retired after an error; create a new backend", error, cap);
-    try {
-        DV_CUDA(cudaSetDevice(b->device));
-        fn(*b);
-        return 0;
-    } catch (const InvalidArgument& e) {
-        return fail(-1, e.what(), error, cap);
-    } catch (const std::exception& e) {
-        b->retired = true;
-        b->release_all();
-        return fail(-2, e.what(), error, cap);
-    } catch (...) {
-        b->retired = true;
-        b->release_all();
-        return fail(-3, "unknown native exception", error, cap);
-    }
-}
-
-inline cudaStream_t pick(Backend& b, void* s) { return s ? static_cast<cudaStream_t>(s) : b.stream; }
-
-void require(bool ok, const char* msg) {
-    if (!ok) throw InvalidArgument(msg);
-}
-
-uint32_t read_err_word(Backend& b, uint32_t* d_word, cudaStream_t st) {
-    uint32_t* h = b.pin_err.as<uint32_t>(1);
-    DV_CUDA(cudaMemcpyAsync(h, d_word, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    DV_CUDA(cudaStreamSynchronize(st));
-    return *h;
-}
 
 // Window width: an explicit dvgpu_msm_set_window wins, then the autotuned
 // width for the size class of the largest set, then the cost model (0).
@@ -229,6 +186,7 @@ __global__ void k_probe_madc(uint32_t seed, uint32_t iters, uint32_t* sink) {
 }  // namespace
 
 void Backend::release_all() noexcept {
+    plans.clear();
     bases.clear();
     MsmTimeline& tl = msm.timeline;
     for (auto& e : tl.ev)
@@ -236,13 +194,6 @@ void Backend::release_all() noexcept {
     for (auto& e : tl.acc_ev)
         if (e) { cudaEventDestroy(e); e = nullptr; }
     tl.enabled = false;
-    if (msm.side) {
-        cudaStreamSynchronize(msm.side);
-        cudaStreamDestroy(msm.side);
-        msm.side = nullptr;
-        for (auto& e : msm.sync_ev)
-            if (e) { cudaEventDestroy(e); e = nullptr; }
-    }
     if (stream) {
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);

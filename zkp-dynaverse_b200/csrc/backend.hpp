@@ -16,6 +16,7 @@
 #include <string>
 
 #include "../../include/dynaverse_gpu.h"
+#include "batch.hpp"
 #include "engine.hpp"
 #include "g2.cuh"
 #include "msm.cuh"
@@ -54,6 +55,7 @@ struct Backend {
     int tuned_c_g2[40] = {};
 
     std::map<uint64_t, std::unique_ptr<ResidentBases>> bases;
+    std::map<uint64_t, std::unique_ptr<BatchPlan>> plans;  // CUDA-graph batch plans
     uint64_t next_handle = 1;
 
     void release_all() noexcept;

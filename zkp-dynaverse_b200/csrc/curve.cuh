@@ -186,6 +186,17 @@ DV_INL void store_words(uint8_t* p, const uint32_t* w) {
     q[1] = make_uint4(w[4], w[5], w[6], w[7]);
 }
 
+// Montgomery field element -> canonical little-endian bytes (Fq2: c0, c1).
+DV_INL void store_canonical(uint8_t* out, const Fq& a) {
+    uint32_t c[8];
+    a.to_canonical(c);
+    store_words(out, c);
+}
+DV_INL void store_canonical(uint8_t* out, const Fq2& a) {
+    store_canonical(out, a.c0);
+    store_canonical(out + 32, a.c1);
+}
+
 // Curve equations (Montgomery constants).
 DV_INL Fq g1_b() {
     uint32_t c[8] = {3, 0, 0, 0, 0, 0, 0, 0};

@@ -140,16 +140,6 @@ __global__ void k_fb_table(Affine<F>* __restrict__ table) {
 }
 
 
-DV_INL void store_canonical(uint8_t* out, const Fq& a) {
-    uint32_t c[8];
-    a.to_canonical(c);
-    store_words(out, c);
-}
-DV_INL void store_canonical(uint8_t* out, const Fq2& a) {
-    store_canonical(out, a.c0);
-    store_canonical(out + 32, a.c1);
-}
-
 template <class F>
 __global__ void __launch_bounds__(128) k_fb_generate(const uint8_t* __restrict__ scalars, uint64_t n,
                                                      const Affine<F>* __restrict__ table, uint8_t* __restrict__ out,

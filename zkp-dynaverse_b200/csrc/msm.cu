@@ -37,19 +37,28 @@ DV_INL uint32_t set_of(const uint32_t* set_off, uint32_t count, uint32_t i) {
     return lo;
 }
 
+// Where digit i of a launch comes from: its set, its scalar and its point.
+DV_INL void locate(const SetMap& m, uint32_t i, uint32_t& set, uint32_t& sidx, uint32_t& pidx) {
+    set = m.count > 1 ? set_of(m.off, m.count, i) : 0;
+    const uint32_t rel = i - (m.count > 1 ? m.off[set] : 0u);
+    sidx = m.src ? m.src[set] + rel : i;
+    pidx = m.prefix ? rel : sidx;
+}
+
 // 1. Histogram of signed digits.
 template <bool PRE>
-__global__ void k_hist(const uint32_t* __restrict__ scalars, uint32_t n, const uint32_t* __restrict__ set_off,
-                       uint32_t count, int c, int W, uint32_t* __restrict__ counts, uint32_t* __restrict__ first_bad) {
+__global__ void k_hist(const uint32_t* __restrict__ scalars, uint32_t n, const SetMap m, int c, int W,
+                       uint32_t* __restrict__ counts, uint32_t* __restrict__ first_bad) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    uint32_t set, sidx, pidx;
+    locate(m, i, set, sidx, pidx);
     uint32_t s[8];
-    load_scalar(scalars, i, s);
+    load_scalar(scalars, sidx, s);
     if (!Fr::is_canonical(s)) {
-        atomicMin(first_bad, i);
+        atomicMin(first_bad, sidx);
         return;
     }
-    const uint32_t set = count > 1 ? set_of(set_off, count, i) : 0;
     const uint32_t B = 1u << (c - 1), full = 1u << c;
     // PRE: precomputed window multiples share one bucket set per MSM
     const uint32_t base = PRE ? set * B : set * (uint32_t)W * B;
@@ -154,14 +163,15 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
 
 // 3. Scatter (point index | sign << 31) into bucket order.
 template <bool PRE>
-__global__ void k_scatter(const uint32_t* __restrict__ scalars, uint32_t n, const uint32_t* __restrict__ set_off,
-                          uint32_t count, int c, int W, uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
+__global__ void k_scatter(const uint32_t* __restrict__ scalars, uint32_t n, const SetMap m, int c, int W,
+                          uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    uint32_t set, sidx, pidx;
+    locate(m, i, set, sidx, pidx);
     uint32_t s[8];
-    load_scalar(scalars, i, s);
+    load_scalar(scalars, sidx, s);
     if (!Fr::is_canonical(s)) return;
-    const uint32_t set = count > 1 ? set_of(set_off, count, i) : 0;
     const uint32_t B = 1u << (c - 1), full = 1u << c;
     // PRE: precomputed window multiples share one bucket set per MSM
     const uint32_t base = PRE ? set * B : set * (uint32_t)W * B;
@@ -182,7 +192,7 @@ __global__ void k_scatter(const uint32_t* __restrict__ scalars, uint32_t n, cons
             uint32_t pos = 0;
             if (lane == leader) pos = atomicAdd(cursor + key, (uint32_t)__popc(peers));
             pos = __shfl_sync(peers, pos, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
-            const uint32_t idx = PRE ? i * (uint32_t)W + (uint32_t)w : i;  // PRE: table entry 2^(c w) P_i
+            const uint32_t idx = PRE ? pidx * (uint32_t)W + (uint32_t)w : pidx;  // PRE: table entry 2^(c w) P_i
             sorted[pos] = idx | (neg ? 0x80000000u : 0u);
         }
     }
@@ -459,6 +469,31 @@ void horner(const dvh::XYZZ<HF>* win, int W, int c, uint8_t* out) {
     dvh::xyzz_to_affine_bytes(acc, out);
 }
 
+// Device tail of one MSM per thread: Horner over the set's window sums, then
+// affine normalisation (infinity stays all-zero bytes).
+template <class F>
+__global__ void __launch_bounds__(64) k_msm_finish(const XYZZ<F>* __restrict__ win, uint32_t count, int W, int c,
+                                                   const uint32_t* __restrict__ out_idx, uint8_t* __restrict__ out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const XYZZ<F>* w = win + (size_t)k * W;
+    XYZZ<F> acc = w[W - 1];
+    for (int j = W - 2; j >= 0; --j) {
+        if (!acc.is_inf())
+            for (int d = 0; d < c; ++d) acc = XYZZ<F>::dbl(acc);
+        acc = XYZZ<F>::add(acc, w[j]);
+    }
+    uint8_t* o = out + (size_t)(out_idx ? out_idx[k] : k) * 2 * sizeof(F);
+    if (acc.is_inf()) {
+        const uint4 z = make_uint4(0, 0, 0, 0);
+        for (size_t b = 0; b < 2 * sizeof(F); b += 16) *reinterpret_cast<uint4*>(o + b) = z;
+        return;
+    }
+    const Affine<F> a = acc.to_affine();
+    store_canonical(o, a.x);
+    store_canonical(o + sizeof(F), a.y);
+}
+
 template <class F>
 struct HostOf;
 template <>
@@ -501,18 +536,7 @@ void gather_points(const Affine<F>* d_bases, uint64_t nbases, const uint64_t* d_
 }
 
 template <class F>
-void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const uint32_t* set_offsets,
-             uint32_t count, int force_c, cudaStream_t st, uint8_t* host_out, MsmStats* stats,
-             const MsmPrecomp<F>* pre) {
-    typedef typename HostOf<F>::T HF;
-    const size_t out_bytes = 2 * sizeof(F);
-    const uint32_t n = set_offsets[count];
-    uint32_t max_set = 0;
-    for (uint32_t k = 0; k < count; ++k) max_set = std::max(max_set, set_offsets[k + 1] - set_offsets[k]);
-    if (n == 0 || count == 0) {
-        memset(host_out, 0, (size_t)count * out_bytes);
-        return;
-    }
+MsmPlan msm_plan_batch(uint32_t count, uint32_t max_set, int force_c, const MsmPrecomp<F>* pre) {
     MsmPlan plan = msm_plan(max_set, force_c);
     // Bound the bucket table of a batch: count * windows * buckets <= 2^26
     // (8 GB of G1 XYZZ buckets); smaller windows trade buckets for windows.
@@ -528,36 +552,37 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         plan.windows = pre->windows;
         plan.buckets = 1u << (plan.c - 1);
         plan.seg_log = std::min(3, plan.c - 1);
-        if ((uint64_t)n * plan.windows >= (1ull << 31)) throw InvalidArgument("precomputed MSM too large");
     }
-    if ((uint64_t)count * plan.windows * plan.buckets > (1ull << 31) || (uint64_t)n * plan.windows > 0xffffffffull)
-        throw InvalidArgument("MSM batch too large for one launch sequence");
+    return plan;
+}
+
+template <class F>
+void msm_enqueue(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const SetMap& map,
+                 uint32_t n, const MsmPlan& plan, const MsmPrecomp<F>* pre, uint32_t* d_err, cudaStream_t st) {
+    const uint32_t count = map.count;
     const int c = plan.c, W = plan.windows;
     const uint32_t B = plan.buckets;
     const uint32_t Wr = pre ? 1u : (uint32_t)W;  // bucket sets (reduction windows) per MSM
+    if (pre && (uint64_t)n * plan.windows >= (1ull << 31)) throw InvalidArgument("precomputed MSM too large");
+    if ((uint64_t)count * Wr * plan.buckets > (1ull << 31) || (uint64_t)n * plan.windows > 0xffffffffull)
+        throw InvalidArgument("MSM batch too large for one launch sequence");
     const uint32_t NW = count * Wr;
     const uint32_t NB = NW * B;
 
-    uint32_t* d_set = ws.set_off.as<uint32_t>(count + 1);
     uint32_t* d_counts = ws.counts.as<uint32_t>(NB);
     uint32_t* d_offsets = ws.offsets.as<uint32_t>(NB + 1);
     uint32_t* d_cursor = ws.cursor.as<uint32_t>(NB);
     uint32_t* d_sorted = ws.sorted.as<uint32_t>((size_t)n * W);
     XYZZ<F>* d_buckets = ws.buckets.as<XYZZ<F>>(NB);
-    uint32_t* d_err = ws.err.as<uint32_t>(1);
-    uint32_t* h_err = ws.host_err.as<uint32_t>(1);
-
-    DV_CUDA(cudaMemcpyAsync(d_set, set_offsets, (count + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     DV_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)NB * sizeof(uint32_t), st));
-    DV_CUDA(cudaMemsetAsync(d_err, 0xff, sizeof(uint32_t), st));
 
     MsmTimeline& tl = ws.timeline;
     auto mark = [&](int k) {
         if (tl.enabled) DV_CUDA(cudaEventRecord(tl.ev[k], st));
     };
     mark(0);
-    if (pre) k_hist<true><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_counts, d_err);
-    else k_hist<false><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_counts, d_err);
+    if (pre) k_hist<true><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, map, c, W, d_counts, d_err);
+    else k_hist<false><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, map, c, W, d_counts, d_err);
     DV_LAUNCH();
     mark(1);
     {
@@ -571,8 +596,8 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         DV_LAUNCH();
     }
     mark(2);
-    if (pre) k_scatter<true><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_cursor, d_sorted);
-    else k_scatter<false><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_set, count, c, W, d_cursor, d_sorted);
+    if (pre) k_scatter<true><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, map, c, W, d_cursor, d_sorted);
+    else k_scatter<false><<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, map, c, W, d_cursor, d_sorted);
     DV_LAUNCH();
     mark(3);
 
@@ -596,71 +621,81 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
     XYZZ<F>* d_win = ws.windows.as<XYZZ<F>>(NW);
     constexpr int P = sizeof(F) == sizeof(Fq) ? 256 : 128;
     const size_t smem = (size_t)P * sizeof(XYZZ<F>);
-    static bool smem_set = false;
-    if (!smem_set) {
+    static bool smem_set[64] = {};
+    int dev = 0;
+    DV_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw InvalidArgument("device ordinal out of range");
+    if (!smem_set[dev]) {
         DV_CUDA(cudaFuncSetAttribute(k_wlevel<F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        smem_set = true;
-    }
-    if (!ws.side) {
-        DV_CUDA(cudaStreamCreateWithFlags(&ws.side, cudaStreamNonBlocking));
-        for (auto& e : ws.sync_ev) DV_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        smem_set[dev] = true;
     }
 
-    // Windows may be processed in groups, each group's reduction on the side
-    // stream.  Measured: the accumulation kernel occupies every SM, so a
-    // second group does not overlap and only lengthens the critical path;
-    // one group is used.
-    const uint32_t split = NW;
-    const uint32_t bounds[3] = {0, split, NW};
-    const int groups = split < NW ? 2 : 1;
-    for (int gi = 0; gi < groups; ++gi) {
-        const uint32_t w0 = bounds[gi], w1 = bounds[gi + 1];
-        const uint32_t gb0 = w0 * B, nbg = (w1 - w0) * B;
-        if (tl.enabled) DV_CUDA(cudaEventRecord(tl.acc_ev[2 * gi], st));
-        k_accum<F><<<grid, 128, 0, st>>>(pre ? pre->table : d_points, d_sorted, d_offsets + gb0, nbg, d_buckets + gb0,
-                                         d_pgid, d_ppt);
+    if (tl.enabled) DV_CUDA(cudaEventRecord(tl.acc_ev[0], st));
+    k_accum<F><<<grid, 128, 0, st>>>(pre ? pre->table : d_points, d_sorted, d_offsets, NB, d_buckets, d_pgid, d_ppt);
+    DV_LAUNCH();
+    if (tl.enabled) DV_CUDA(cudaEventRecord(tl.acc_ev[1], st));
+    uint32_t* d_fix_count = ws.fix_count.as<uint32_t>(1);
+    uint32_t* d_fix_list = ws.fix_list.as<uint32_t>(T / FIX_SHORT + 1);
+    DV_CUDA(cudaMemsetAsync(d_fix_count, 0, sizeof(uint32_t), st));
+    k_fixup<F><<<blocks_for(T, 128), 128, 0, st>>>(d_pgid, d_ppt, T, d_buckets, d_fix_list, d_fix_count);
+    DV_LAUNCH();
+    // long chains are rare: a small grid loops over the queue
+    k_fixup_long<F, 128><<<std::min<uint32_t>(T / FIX_SHORT + 1, (uint32_t)sm_count()), 128, 0, st>>>(
+        d_pgid, d_ppt, T, d_buckets, d_fix_list, d_fix_count);
+    DV_LAUNCH();
+    mark(4);
+    k_segments<F><<<blocks_for((uint64_t)NW * S, 128), 128, 0, st>>>(d_buckets, d_offsets, B, NW, seg_log, d_seg_u,
+                                                                     d_seg_r);
+    DV_LAUNCH();
+    // upper levels: (U, R) pairs with multiplier m = 2^log_m
+    XYZZ<F>* u = d_seg_u;
+    XYZZ<F>* r = d_seg_r;
+    XYZZ<F>* u2 = d_lvl_u;
+    XYZZ<F>* r2 = d_lvl_r;
+    uint32_t len = S;
+    int log_m = seg_log;
+    for (;;) {
+        const uint32_t nblk = len > (uint32_t)P ? len / P : 1u;
+        XYZZ<F>* u_dst = nblk == 1 ? d_win : u2;
+        k_wlevel<F, P><<<NW * nblk, P, smem, st>>>(u, r, len, log_m, u_dst, r2);
         DV_LAUNCH();
-        if (tl.enabled) DV_CUDA(cudaEventRecord(tl.acc_ev[2 * gi + 1], st));
-        uint32_t* d_fix_count = ws.fix_count.as<uint32_t>(1);
-        uint32_t* d_fix_list = ws.fix_list.as<uint32_t>(T / FIX_SHORT + 1);
-        DV_CUDA(cudaMemsetAsync(d_fix_count, 0, sizeof(uint32_t), st));
-        k_fixup<F><<<blocks_for(T, 128), 128, 0, st>>>(d_pgid, d_ppt, T, d_buckets + gb0, d_fix_list, d_fix_count);
-        DV_LAUNCH();
-        // long chains are rare: a small grid loops over the queue
-        k_fixup_long<F, 128><<<std::min<uint32_t>(T / FIX_SHORT + 1, (uint32_t)sm_count()), 128, 0, st>>>(
-            d_pgid, d_ppt, T, d_buckets + gb0, d_fix_list, d_fix_count);
-        DV_LAUNCH();
-        DV_CUDA(cudaEventRecord(ws.sync_ev[gi], st));
-        DV_CUDA(cudaStreamWaitEvent(ws.side, ws.sync_ev[gi], 0));
-        k_segments<F><<<blocks_for((uint64_t)(w1 - w0) * S, 128), 128, 0, ws.side>>>(
-            d_buckets + gb0, d_offsets + gb0, B, w1 - w0, seg_log, d_seg_u + (size_t)w0 * S, d_seg_r + (size_t)w0 * S);
-        DV_LAUNCH();
-        // upper levels: (U, R) pairs with multiplier m = 2^log_m
-        XYZZ<F>* u = d_seg_u + (size_t)w0 * S;
-        XYZZ<F>* r = d_seg_r + (size_t)w0 * S;
-        XYZZ<F>* u2 = d_lvl_u + (size_t)w0 * S;
-        XYZZ<F>* r2 = d_lvl_r + (size_t)w0 * S;
-        uint32_t len = S;
-        int log_m = seg_log;
-        for (;;) {
-            const uint32_t nblk = len > (uint32_t)P ? len / P : 1u;
-            XYZZ<F>* u_dst = nblk == 1 ? d_win + w0 : u2;
-            k_wlevel<F, P><<<(w1 - w0) * nblk, P, smem, ws.side>>>(u, r, len, log_m, u_dst, r2);
-            DV_LAUNCH();
-            if (nblk == 1) break;
-            log_m += __builtin_ctz((unsigned)P);
-            len = nblk;
-            std::swap(u, u2);
-            std::swap(r, r2);
-        }
+        if (nblk == 1) break;
+        log_m += __builtin_ctz((unsigned)P);
+        len = nblk;
+        std::swap(u, u2);
+        std::swap(r, r2);
     }
-    mark(4);  // main stream done with accumulation
-    DV_CUDA(cudaEventRecord(ws.sync_ev[2], ws.side));
-    DV_CUDA(cudaStreamWaitEvent(st, ws.sync_ev[2], 0));
-    mark(5);  // reduction joined
+    mark(5);
+}
+
+template <class F>
+void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const uint32_t* set_offsets,
+             uint32_t count, int force_c, cudaStream_t st, uint8_t* host_out, MsmStats* stats,
+             const MsmPrecomp<F>* pre) {
+    typedef typename HostOf<F>::T HF;
+    const size_t out_bytes = 2 * sizeof(F);
+    const uint32_t n = set_offsets[count];
+    uint32_t max_set = 0;
+    for (uint32_t k = 0; k < count; ++k) max_set = std::max(max_set, set_offsets[k + 1] - set_offsets[k]);
+    if (n == 0 || count == 0) {
+        memset(host_out, 0, (size_t)count * out_bytes);
+        return;
+    }
+    const MsmPlan plan = msm_plan_batch<F>(count, max_set, force_c, pre);
+    const int c = plan.c, W = plan.windows;
+    const uint32_t Wr = pre ? 1u : (uint32_t)W;
+    const uint32_t NW = count * Wr;
+
+    uint32_t* d_set = ws.set_off.as<uint32_t>(count + 1);
+    uint32_t* d_err = ws.err.as<uint32_t>(1);
+    uint32_t* h_err = ws.host_err.as<uint32_t>(1);
+    DV_CUDA(cudaMemcpyAsync(d_set, set_offsets, (count + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    DV_CUDA(cudaMemsetAsync(d_err, 0xff, sizeof(uint32_t), st));
+    msm_enqueue<F>(ws, d_points, d_scalars, SetMap{d_set, nullptr, count, 0}, n, plan, pre, d_err, st);
 
     XYZZ<F>* h_win = ws.host_windows.as<XYZZ<F>>(NW);
-    DV_CUDA(cudaMemcpyAsync(h_win, d_win, (size_t)NW * sizeof(XYZZ<F>), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaMemcpyAsync(h_win, ws.windows.as<XYZZ<F>>(NW), (size_t)NW * sizeof(XYZZ<F>), cudaMemcpyDeviceToHost,
+                            st));
     DV_CUDA(cudaMemcpyAsync(h_err, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaStreamSynchronize(st));
     if (*h_err != NO_INDEX)
@@ -668,6 +703,7 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
     static_assert(sizeof(XYZZ<F>) == sizeof(dvh::XYZZ<HF>), "host/device XYZZ layout");
     const auto* hw = reinterpret_cast<const dvh::XYZZ<HF>*>(h_win);
     for (uint32_t k = 0; k < count; ++k) horner(hw + (size_t)k * Wr, (int)Wr, c, host_out + (size_t)k * out_bytes);
+    MsmTimeline& tl = ws.timeline;
     if (tl.enabled) {
         DV_CUDA(cudaEventRecord(tl.ev[6], st));
         DV_CUDA(cudaEventSynchronize(tl.ev[6]));
@@ -676,15 +712,14 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
             DV_CUDA(cudaEventElapsedTime(&ms, a, b));
             return (double)ms;
         };
-        double acc = 0;
-        for (int gi = 0; gi < groups; ++gi) acc += span(tl.acc_ev[2 * gi], tl.acc_ev[2 * gi + 1]);
-        tl.ms[0] += span(tl.ev[0], tl.ev[1]);           // digit histogram
-        tl.ms[1] += span(tl.ev[1], tl.ev[2]);           // offsets scan
-        tl.ms[2] += span(tl.ev[2], tl.ev[3]);           // scatter
-        tl.ms[3] += acc;                                // bucket accumulation (all groups)
-        tl.ms[4] += span(tl.ev[3], tl.ev[4]) - acc;     // merges + overlapped reduction of group 0
-        tl.ms[5] += span(tl.ev[4], tl.ev[5]);           // reduction tail (last group)
-        tl.ms[7] += span(tl.ev[5], tl.ev[6]);           // window D2H + host Horner
+        const double acc = span(tl.acc_ev[0], tl.acc_ev[1]);
+        tl.ms[0] += span(tl.ev[0], tl.ev[1]);        // digit histogram
+        tl.ms[1] += span(tl.ev[1], tl.ev[2]);        // offsets scan
+        tl.ms[2] += span(tl.ev[2], tl.ev[3]);        // scatter
+        tl.ms[3] += acc;                             // bucket accumulation
+        tl.ms[4] += span(tl.ev[3], tl.ev[4]) - acc;  // split-bucket merges
+        tl.ms[5] += span(tl.ev[4], tl.ev[5]);        // bucket reduction
+        tl.ms[7] += span(tl.ev[5], tl.ev[6]);        // window D2H + host Horner
         tl.calls++;
         tl.accum_mixed_adds += (uint64_t)n * W;
     }
@@ -700,6 +735,22 @@ template void msm_run<Fq>(MsmWorkspace&, const Affine<Fq>*, const uint32_t*, con
                           cudaStream_t, uint8_t*, MsmStats*, const MsmPrecomp<Fq>*);
 template void msm_run<Fq2>(MsmWorkspace&, const Affine<Fq2>*, const uint32_t*, const uint32_t*, uint32_t, int,
                            cudaStream_t, uint8_t*, MsmStats*, const MsmPrecomp<Fq2>*);
+template MsmPlan msm_plan_batch<Fq>(uint32_t, uint32_t, int, const MsmPrecomp<Fq>*);
+template MsmPlan msm_plan_batch<Fq2>(uint32_t, uint32_t, int, const MsmPrecomp<Fq2>*);
+template void msm_enqueue<Fq>(MsmWorkspace&, const Affine<Fq>*, const uint32_t*, const SetMap&, uint32_t,
+                              const MsmPlan&, const MsmPrecomp<Fq>*, uint32_t*, cudaStream_t);
+template void msm_enqueue<Fq2>(MsmWorkspace&, const Affine<Fq2>*, const uint32_t*, const SetMap&, uint32_t,
+                               const MsmPlan&, const MsmPrecomp<Fq2>*, uint32_t*, cudaStream_t);
+
+template <class F>
+void msm_finish_device(const XYZZ<F>* d_windows, uint32_t count, int windows_per_set, int c, const uint32_t* d_out_idx,
+                       uint8_t* d_out, cudaStream_t st) {
+    if (!count) return;
+    k_msm_finish<F><<<blocks_for(count, 64), 64, 0, st>>>(d_windows, count, windows_per_set, c, d_out_idx, d_out);
+    DV_LAUNCH();
+}
+template void msm_finish_device<Fq>(const XYZZ<Fq>*, uint32_t, int, int, const uint32_t*, uint8_t*, cudaStream_t);
+template void msm_finish_device<Fq2>(const XYZZ<Fq2>*, uint32_t, int, int, const uint32_t*, uint8_t*, cudaStream_t);
 
 template <class F>
 void msm_precompute(const Affine<F>* d_bases, uint64_t n, int c, int windows, Affine<F>* d_table, cudaStream_t st) {

@@ -44,9 +44,8 @@ struct MsmPlan {
 MsmPlan msm_plan(uint64_t points_per_set, int force_c);
 
 // Optional per-phase device timing (CUDA events on the launching stream).
-// Phases: 0 hist, 1 scan, 2 scatter, 3 accumulation, 4 split-bucket merges
-// plus the overlapped reduction of the first window group, 5 reduction tail
-// (last group), 6 unused, 7 window D2H + host Horner.
+// Phases: 0 hist, 1 scan, 2 scatter, 3 accumulation, 4 split-bucket merges,
+// 5 bucket reduction, 6 unused, 7 window D2H + host Horner.
 enum { MSM_PHASES = 8 };
 struct MsmTimeline {
     bool enabled = false;
@@ -62,8 +61,6 @@ struct MsmWorkspace {
         err;
     PinnedBuf host_windows, host_err;
     MsmTimeline timeline;
-    cudaStream_t side = nullptr;       // bucket-reduction stream (created on first use)
-    cudaEvent_t sync_ev[3] = {};
 };
 
 struct MsmStats {
@@ -89,6 +86,43 @@ template <class F>
 void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const uint32_t* set_offsets,
              uint32_t count, int force_c, cudaStream_t stream, uint8_t* host_out, MsmStats* stats,
              const MsmPrecomp<F>* pre = nullptr);
+
+// How the digits of one launch sequence map to sets, scalars and points.
+// Digit i (0 <= i < off[count]) belongs to the set k with
+// off[k] <= i < off[k + 1]; its scalar is src[k] + (i - off[k]) (i itself
+// when src is null); its point is i - off[k] with prefix (every set uses a
+// prefix of one base array), else the scalar's index.
+struct SetMap {
+    const uint32_t* off;  // device, count + 1 entries
+    const uint32_t* src;  // device or null
+    uint32_t count;
+    int prefix;
+};
+
+// Window plan of a launch sequence: the cost model (or force_c), bounded so
+// that count * windows * buckets stays launchable; a precomputed table fixes
+// c and uses one bucket set per MSM.
+template <class F>
+MsmPlan msm_plan_batch(uint32_t count, uint32_t max_set, int force_c, const MsmPrecomp<F>* pre);
+
+// The device part of an MSM launch sequence: digit sort, accumulation,
+// merges and bucket reduction, all on `stream`, without host
+// synchronisation.  Leaves count * (pre ? 1 : windows) XYZZ window sums in
+// ws.windows and the lowest non-canonical scalar index (or 0xffffffff) in
+// *d_err, which the caller initialises.  Allocates only when a workspace
+// buffer must grow, so a second call with the same shapes allocates nothing
+// (and can be captured in a CUDA graph).
+template <class F>
+void msm_enqueue(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const SetMap& map,
+                 uint32_t n, const MsmPlan& plan, const MsmPrecomp<F>* pre, uint32_t* d_err, cudaStream_t stream);
+
+// Device tail: Horner over each set's window sums (weights 2^(c w)) and
+// normalisation to canonical affine bytes (2 * sizeof(F) per set, all-zero
+// for infinity), one thread per set.  Set k is written at result position
+// d_out_idx[k] (k when null).
+template <class F>
+void msm_finish_device(const XYZZ<F>* d_windows, uint32_t count, int windows_per_set, int c, const uint32_t* d_out_idx,
+                       uint8_t* d_out, cudaStream_t stream);
 
 // Builds the table of precomputed window multiples (windows * n entries).
 template <class F>

@@ -135,17 +135,36 @@ struct PassArgs {
 // One round of RR stages: thread-group tau owns the 2^RR elements that differ
 // only in local bits [bit_hi - RR, bit_hi).  RR is a compile-time constant so
 // the element array stays in registers.
-template <int RR, int THREADS>
-DV_INL void dif_round(const PassArgs& a, uint32_t* sm, int lb, uint64_t low, uint64_t high, int bit_hi,
+// Working-vector load that bypasses L1: in a batch, a later pass reads
+// elements that other blocks of the same launch wrote.
+DV_INL Fr load_cg(const Fr* p) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    const uint4 lo = __ldcg(q), hi = __ldcg(q + 1);
+    Fr a;
+    a.v[0] = lo.x; a.v[1] = lo.y; a.v[2] = lo.z; a.v[3] = lo.w;
+    a.v[4] = hi.x; a.v[5] = hi.y; a.v[6] = hi.z; a.v[7] = hi.w;
+    return a;
+}
+
+// The tile holds 2^tile_log elements: groups first_group, first_group + 1, ...
+// of 2^k elements each.  Tile index t = (group in tile) << k | element in
+// group, so the round's lane -> element formula covers every group at once.
+template <int RR, int THREADS, bool CG>
+DV_INL void dif_round(const PassArgs& a, uint32_t* sm, int tile_log, uint64_t first_group, int bit_hi,
                       bool first_round) {
     constexpr int R = 1 << RR;
     const int k = a.k;
+    const int lb = a.logn - a.s0 - k;
     const uint32_t G = 1u << k;
+    const uint32_t TE = 1u << tile_log;
     const int b_lo = bit_hi - RR;
     const bool last_round = b_lo == 0;
-    const uint32_t lanes = G >> RR;
+    const uint32_t lanes = TE >> RR;
     for (uint32_t tau = threadIdx.x; tau < lanes; tau += THREADS) {
-        const uint32_t base_e = ((tau >> b_lo) << bit_hi) | (tau & ((1u << b_lo) - 1));
+        const uint32_t base_t = ((tau >> b_lo) << bit_hi) | (tau & ((1u << b_lo) - 1));
+        const uint64_t g = first_group + (base_t >> k);
+        const uint64_t low = g & ((1ull << lb) - 1), high = g >> lb;
+        const uint32_t base_e = base_t & (G - 1);
         Fr x[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) {
@@ -169,10 +188,10 @@ DV_INL void dif_round(const PassArgs& a, uint32_t* sm, int lb, uint64_t low, uin
                         x[m] = Fr::mul_inl(Fr::mul_inl(x[m], a.pre_hi[idx >> a.split]), a.pre_lo[idx & lo_mask]);
                     }
                 } else {
-                    x[m] = a.work[idx];
+                    x[m] = CG ? load_cg(a.work + idx) : a.work[idx];
                 }
             } else {
-                load_plane(sm, G, e, x[m]);
+                load_plane(sm, TE, base_t | ((uint32_t)m << b_lo), x[m]);
             }
         }
 #pragma unroll
@@ -216,9 +235,27 @@ DV_INL void dif_round(const PassArgs& a, uint32_t* sm, int lb, uint64_t low, uin
                     a.work[idx] = x[m];
                 }
             } else {
-                store_plane(sm, G, e, x[m]);
+                store_plane(sm, TE, base_t | ((uint32_t)m << b_lo), x[m]);
             }
         }
+    }
+}
+
+// Runs the rounds of one tile (all stages of the pass), ending with a
+// barrier.
+template <int THREADS, int R_LOG, bool CG>
+DV_INL void dif_tile(const PassArgs& a, uint32_t* sm, int tile_log, uint64_t first_group) {
+    int bit_hi = a.k;
+    bool first_round = true;
+    while (bit_hi > 0) {
+        const int rr = bit_hi < R_LOG ? bit_hi : R_LOG;
+        if (rr == 3 && R_LOG >= 3)
+            dif_round<(R_LOG >= 3 ? 3 : 1), THREADS, CG>(a, sm, tile_log, first_group, bit_hi, first_round);
+        else if (rr == 2) dif_round<2, THREADS, CG>(a, sm, tile_log, first_group, bit_hi, first_round);
+        else dif_round<1, THREADS, CG>(a, sm, tile_log, first_group, bit_hi, first_round);
+        __syncthreads();
+        bit_hi -= rr;
+        first_round = false;
     }
 }
 
@@ -235,17 +272,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 256 ? DV_NTT_MINB : 8)) k
     const int lb = a.logn - a.s0 - k;
     const uint64_t g = blockIdx.x;
     const uint64_t low = g & ((1ull << lb) - 1), high = g >> lb;
-    int bit_hi = k;
-    bool first_round = true;
-    while (bit_hi > 0) {
-        const int rr = bit_hi < R_LOG ? bit_hi : R_LOG;
-        if (rr == 3 && R_LOG >= 3) dif_round<(R_LOG >= 3 ? 3 : 1), THREADS>(a, sm, lb, low, high, bit_hi, first_round);
-        else if (rr == 2) dif_round<2, THREADS>(a, sm, lb, low, high, bit_hi, first_round);
-        else dif_round<1, THREADS>(a, sm, lb, low, high, bit_hi, first_round);
-        __syncthreads();
-        bit_hi -= rr;
-        first_round = false;
-    }
+    dif_tile<THREADS, R_LOG, false>(a, sm, k, g);
     if (k == 0) {  // single element: copy (with the first pass's check)
         if (threadIdx.x == 0) {
             const uint64_t idx = (high << lb) | low;
@@ -304,10 +331,12 @@ void launch_pass(const PassArgs& a, cudaStream_t st) {
 }
 
 // Runs the DIF passes of a transform of 2^logn elements.  With fuse_out the
-// last pass (of two or more) writes the natural-order output bytes itself;
-// a single pass never does, since its one block may read and write the same
-// positions of an in-place vector within one round.  Returns whether the
-// output was written (otherwise k_permute must run).
+// last pass writes the natural-order output bytes itself.  In-place use is
+// safe: the first pass reads the input and a later pass writes the output;
+// a single pass is one block whose first round reads every element before
+// a barrier (or, with one round, one thread reading all before writing) and
+// whose last round writes.  Returns whether the output was written
+// (otherwise k_permute must run).
 bool run_passes(const uint8_t* d_in, Fr* work, uint8_t* d_out, int logn, const Fr* tw, const Fr* pre_hi,
                 const Fr* pre_lo, const Fr* post_hi, const Fr* post_lo, const Fr* post_const, int split,
                 uint32_t* bad, bool fuse_out, cudaStream_t st) {
@@ -318,7 +347,7 @@ bool run_passes(const uint8_t* d_in, Fr* work, uint8_t* d_out, int logn, const F
         return false;
     }
     const int passes = (logn + 10) / 11;
-    const bool fused = fuse_out && passes >= 2;
+    const bool fused = fuse_out;
     int s0 = 0;
     for (int p = 0; p < passes; ++p) {
         a.k = logn / passes + (p < logn % passes ? 1 : 0);
@@ -334,64 +363,79 @@ bool run_passes(const uint8_t* d_in, Fr* work, uint8_t* d_out, int logn, const F
 
 }  // namespace
 
-void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, int kind, cudaStream_t st) {
+NttTables& ntt_tables(NttWorkspace& ws, int logn, int kind, cudaStream_t st) {
     if (logn < 0 || logn > NTT_MAX_LOG || kind < 0 || kind > 3) throw InvalidArgument("invalid NTT size or kind");
     const uint64_t n = 1ull << logn;
     const bool inverse = kind & 1, coset = kind >= 2;
     const int split = (logn + 1) / 2;
     const int key = logn * 4 + kind;
     auto it = ws.tables.find(key);
-    NttTables* tab;
-    Fr* kc;
-    if (it == ws.tables.end()) {
-        auto t = std::make_unique<NttTables>();
-        t->split = split;
-        kc = t->consts.as<Fr>(C_COUNT);
-        k_setup_consts<<<1, 1, 0, st>>>(logn, inverse ? 1 : 0, split, kc);
-        DV_LAUNCH();
-        const uint64_t half = std::max<uint64_t>(1, n / 2);
-        Fr* tw = t->tw.as<Fr>(half);
-        const uint32_t chunk = 64;
-        const uint64_t threads = (half + chunk - 1) / chunk;
-        k_pow_table<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(kc + C_W, nullptr, half, chunk, 0, tw);
-        DV_LAUNCH();
-        if (coset) {
-            const uint64_t nlo = 1ull << split, nhi = (n + nlo - 1) >> split;
-            if (!inverse) {
-                Fr* hi = t->pre_hi.as<Fr>(nhi);
-                Fr* lo = t->pre_lo.as<Fr>(nlo);
-                k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(kc + C_G_SPLIT, nullptr, nhi, 1, 0, hi);
-                DV_LAUNCH();
-                k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(kc + C_G, nullptr, nlo, 1, 0, lo);
-                DV_LAUNCH();
-            } else {
-                Fr* hi = t->post_hi.as<Fr>(nhi);
-                Fr* lo = t->post_lo.as<Fr>(nlo);
-                k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(kc + C_GINV_SPLIT, kc + C_NINV, nhi, 1, 0,
-                                                                          hi);
-                DV_LAUNCH();
-                k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(kc + C_GINV, nullptr, nlo, 1, 0, lo);
-                DV_LAUNCH();
-            }
+    if (it != ws.tables.end()) return *it->second;
+    auto t = std::make_unique<NttTables>();
+    t->split = split;
+    Fr* kc = t->consts.as<Fr>(C_COUNT);
+    k_setup_consts<<<1, 1, 0, st>>>(logn, inverse ? 1 : 0, split, kc);
+    DV_LAUNCH();
+    const uint64_t half = std::max<uint64_t>(1, n / 2);
+    Fr* tw = t->tw.as<Fr>(half);
+    const uint32_t chunk = 64;
+    const uint64_t threads = (half + chunk - 1) / chunk;
+    k_pow_table<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(kc + C_W, nullptr, half, chunk, 0, tw);
+    DV_LAUNCH();
+    if (coset) {
+        const uint64_t nlo = 1ull << split, nhi = (n + nlo - 1) >> split;
+        if (!inverse) {
+            Fr* hi = t->pre_hi.as<Fr>(nhi);
+            Fr* lo = t->pre_lo.as<Fr>(nlo);
+            k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(kc + C_G_SPLIT, nullptr, nhi, 1, 0, hi);
+            DV_LAUNCH();
+            k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(kc + C_G, nullptr, nlo, 1, 0, lo);
+            DV_LAUNCH();
+        } else {
+            Fr* hi = t->post_hi.as<Fr>(nhi);
+            Fr* lo = t->post_lo.as<Fr>(nlo);
+            k_pow_table<<<(unsigned)((nhi + 127) / 128), 128, 0, st>>>(kc + C_GINV_SPLIT, kc + C_NINV, nhi, 1, 0, hi);
+            DV_LAUNCH();
+            k_pow_table<<<(unsigned)((nlo + 127) / 128), 128, 0, st>>>(kc + C_GINV, nullptr, nlo, 1, 0, lo);
+            DV_LAUNCH();
         }
-        tab = t.get();
-        ws.tables[key] = std::move(t);
-    } else {
-        tab = it->second.get();
-        kc = tab->consts.as<Fr>(C_COUNT);
     }
+    NttTables& ref = *t;
+    ws.tables[key] = std::move(t);
+    return ref;
+}
+
+namespace {
+// Multipliers of one transform, taken from its tables.
+struct Scaling {
+    const Fr *tw, *pre_hi, *pre_lo, *post_hi, *post_lo, *post_const;
+    int split;
+};
+Scaling scaling_of(NttTables& tab, int kind) {
+    const bool inverse = kind & 1, coset = kind >= 2;
+    Fr* kc = tab.consts.as<Fr>(C_COUNT);
+    return Scaling{tab.tw.as<Fr>(1),
+                   (coset && !inverse) ? tab.pre_hi.as<Fr>(1) : nullptr,
+                   (coset && !inverse) ? tab.pre_lo.as<Fr>(1) : nullptr,
+                   (coset && inverse) ? tab.post_hi.as<Fr>(1) : nullptr,
+                   (coset && inverse) ? tab.post_lo.as<Fr>(1) : nullptr,
+                   inverse ? kc + C_NINV : nullptr,
+                   tab.split};
+}
+}  // namespace
+
+void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, int kind, cudaStream_t st) {
+    NttTables& tab = ntt_tables(ws, logn, kind, st);
+    const uint64_t n = 1ull << logn;
+    const Scaling sc = scaling_of(tab, kind);
     Fr* work = ws.work.as<Fr>(n);
     uint32_t* bad = ws.err.as<uint32_t>(1);
     DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
 
-    const Fr* tw = tab->tw.as<Fr>(1);
-    const Fr* pre_hi = (coset && !inverse) ? tab->pre_hi.as<Fr>(1) : nullptr;
-    const Fr* pre_lo = (coset && !inverse) ? tab->pre_lo.as<Fr>(1) : nullptr;
-    const Fr* post_hi = (coset && inverse) ? tab->post_hi.as<Fr>(1) : nullptr;
-    const Fr* post_lo = (coset && inverse) ? tab->post_lo.as<Fr>(1) : nullptr;
-    const Fr* post_const = inverse ? kc + C_NINV : nullptr;
-    if (!run_passes(d_in, work, d_out, logn, tw, pre_hi, pre_lo, post_hi, post_lo, post_const, split, bad, true, st)) {
-        k_permute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(work, d_out, logn, post_hi, post_lo, split, post_const);
+    if (!run_passes(d_in, work, d_out, logn, sc.tw, sc.pre_hi, sc.pre_lo, sc.post_hi, sc.post_lo, sc.post_const,
+                    sc.split, bad, true, st)) {
+        k_permute<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(work, d_out, logn, sc.post_hi, sc.post_lo, sc.split,
+                                                              sc.post_const);
         DV_LAUNCH();
     }
     uint32_t host_bad = 0;
@@ -400,6 +444,161 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
     if (host_bad != 0xffffffffu) throw InvalidArgument("non-canonical NTT input at index " + std::to_string(host_bad));
     ws.calls++;
     ws.elements += n;
+}
+
+// ===================================================================== batches
+namespace {
+
+constexpr int BATCH_TILE_LOG = 11;               // elements per tile: 2^11 (64 KB of shared memory)
+constexpr uint32_t BATCH_SPIN_LIMIT = 1u << 24;  // dependency wait: ~2 s of 128 ns sleeps
+
+struct BatchDesc {
+    PassArgs a;         // k, s0, first and out are set per pass
+    int passes;
+    int k[3], s0[3], tile_log[3];
+    uint32_t tiles[3];  // tiles of each pass
+};
+struct BatchTile {
+    uint32_t desc;
+    uint32_t pass;
+    uint64_t first_group;
+};
+
+// Persistent batch kernel.  ctl[0]: next tile, ctl[1]: status (bit 0: a
+// dependency wait gave up), ctl[2 + 3 d + p]: finished tiles of pass p of
+// transform d.  Tiles are listed pass by pass, so a tile only waits for
+// tiles that running blocks took earlier.
+template <int R_LOG>
+__global__ void __launch_bounds__(256, DV_NTT_MINB) k_ntt_batch(const BatchDesc* __restrict__ descs,
+                                                                const BatchTile* __restrict__ tiles, uint32_t ntiles,
+                                                                uint32_t* __restrict__ ctl) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t cur;
+    for (;;) {
+        if (threadIdx.x == 0) cur = atomicAdd(ctl, 1u);
+        __syncthreads();
+        const uint32_t t = cur;
+        if (t >= ntiles) return;
+        const BatchTile tile = tiles[t];
+        const BatchDesc& d = descs[tile.desc];
+        const int p = (int)tile.pass;
+        if (p > 0) {
+            if (threadIdx.x == 0) {
+                const volatile uint32_t* dep = ctl + 2 + 3 * tile.desc + (p - 1);
+                const uint32_t need = d.tiles[p - 1];
+                uint32_t spins = 0;
+                while (*dep < need) {
+                    if (++spins > BATCH_SPIN_LIMIT) {
+                        atomicOr(ctl + 1, 1u);
+                        break;
+                    }
+                    __nanosleep(128);
+                }
+                __threadfence();
+            }
+            __syncthreads();
+        }
+        PassArgs a = d.a;
+        a.k = d.k[p];
+        a.s0 = d.s0[p];
+        a.first = p == 0;
+        a.out = p == d.passes - 1 ? d.a.out : nullptr;
+        dif_tile<256, R_LOG, true>(a, sm, d.tile_log[p], tile.first_group);  // ends with a barrier
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(ctl + 2 + 3 * tile.desc + p, 1u);
+        }
+    }
+}
+
+}  // namespace
+
+void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttBatchItem>& items, cudaStream_t st) {
+    const uint32_t count = (uint32_t)items.size();
+    std::vector<BatchDesc> descs(count);
+    std::vector<BatchTile> tiles[3];
+    batch.work_off.assign(count, 0);
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const NttBatchItem& it = items[i];
+        if (it.logn < 1 || it.logn > 24 || it.kind < 0 || it.kind > 3 || !it.in || !it.out)
+            throw InvalidArgument("invalid batch NTT item " + std::to_string(i));
+        batch.work_off[i] = total;
+        total += 1ull << it.logn;
+    }
+    if (total > (1ull << 30)) throw InvalidArgument("NTT batch too large");
+    Fr* work = batch.work.as<Fr>(std::max<uint64_t>(1, total));
+    uint32_t* errs = batch.errs.as<uint32_t>(std::max<uint32_t>(1, count));
+    for (uint32_t i = 0; i < count; ++i) {
+        const NttBatchItem& it = items[i];
+        const Scaling sc = scaling_of(ntt_tables(ws, it.logn, it.kind, st), it.kind);
+        BatchDesc& d = descs[i];
+        d.a = PassArgs{it.in,       work + batch.work_off[i], it.out, sc.tw,    sc.pre_hi, sc.pre_lo,
+                       sc.post_hi, sc.post_lo,               sc.post_const,    errs + i, it.logn,  0,
+                       0,          1,                        sc.split};
+        d.passes = (it.logn + BATCH_TILE_LOG - 1) / BATCH_TILE_LOG;
+        for (int p = 0; p < 3; ++p) {
+            d.k[p] = d.s0[p] = d.tile_log[p] = 0;
+            d.tiles[p] = 0;
+        }
+        int s0 = 0;
+        for (int p = 0; p < d.passes; ++p) {
+            const int k = it.logn / d.passes + (p < it.logn % d.passes ? 1 : 0);
+            const int tile_log = std::min(it.logn, BATCH_TILE_LOG);  // 2^(tile_log - k) groups of 2^k per tile
+            const uint64_t groups = 1ull << (it.logn - k);
+            const uint64_t per_tile = 1ull << (tile_log - k);
+            d.k[p] = k;
+            d.s0[p] = s0;
+            d.tile_log[p] = tile_log;
+            d.tiles[p] = (uint32_t)(groups / per_tile);
+            for (uint64_t g = 0; g < groups; g += per_tile) tiles[p].push_back(BatchTile{i, (uint32_t)p, g});
+            s0 += k;
+        }
+    }
+    std::vector<BatchTile> all;
+    for (auto& v : tiles) all.insert(all.end(), v.begin(), v.end());
+    batch.count = count;
+    batch.ntiles = (uint32_t)all.size();
+    batch.elements = total;
+    BatchDesc* d_descs = batch.descs.as<BatchDesc>(std::max<uint32_t>(1, count));
+    BatchTile* d_tiles = batch.tiles.as<BatchTile>(std::max<size_t>(1, all.size()));
+    batch.ctl.as<uint32_t>(2 + 3ull * count);
+    if (count) DV_CUDA(cudaMemcpyAsync(d_descs, descs.data(), count * sizeof(BatchDesc), cudaMemcpyHostToDevice, st));
+    if (!all.empty())
+        DV_CUDA(cudaMemcpyAsync(d_tiles, all.data(), all.size() * sizeof(BatchTile), cudaMemcpyHostToDevice, st));
+    const int smem = 32 << BATCH_TILE_LOG;
+    DV_CUDA(cudaFuncSetAttribute(k_ntt_batch<DV_NTT_RADIX_LOG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ntt_batch<DV_NTT_RADIX_LOG>, 256, smem));
+    batch.grid = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>((uint64_t)sm_count() * (uint32_t)std::max(1, per_sm), batch.ntiles));
+    // the host descriptor vectors must outlive the copies above
+    DV_CUDA(cudaStreamSynchronize(st));
+}
+
+void ntt_batch_enqueue(NttBatch& batch, cudaStream_t st) {
+    if (!batch.count) return;
+    uint32_t* ctl = batch.ctl.as<uint32_t>(2 + 3ull * batch.count);
+    DV_CUDA(cudaMemsetAsync(ctl, 0, (2 + 3ull * batch.count) * sizeof(uint32_t), st));
+    DV_CUDA(cudaMemsetAsync(batch.errs.as<uint32_t>(batch.count), 0xff, batch.count * sizeof(uint32_t), st));
+    k_ntt_batch<DV_NTT_RADIX_LOG><<<batch.grid, 256, 32 << BATCH_TILE_LOG, st>>>(
+        batch.descs.as<BatchDesc>(batch.count), batch.tiles.as<BatchTile>(batch.ntiles), batch.ntiles, ctl);
+    DV_LAUNCH();
+}
+
+void ntt_batch_check(NttBatch& batch, cudaStream_t st) {
+    if (!batch.count) return;
+    std::vector<uint32_t> errs(batch.count);
+    uint32_t status = 0;
+    DV_CUDA(cudaMemcpyAsync(errs.data(), batch.errs.as<uint32_t>(batch.count), batch.count * sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaMemcpyAsync(&status, batch.ctl.as<uint32_t>(2) + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaStreamSynchronize(st));
+    if (status) throw CudaFailure("NTT batch: a pass dependency wait timed out");
+    for (uint32_t i = 0; i < batch.count; ++i)
+        if (errs[i] != 0xffffffffu)
+            throw InvalidArgument("non-canonical NTT input in transform " + std::to_string(i) + " at index " +
+                                  std::to_string(errs[i]));
 }
 
 }  // namespace dv

@@ -13,17 +13,24 @@
 // Values stay canonical throughout: every multiplier (twiddles, coset and
 // scale factors) is held in Montgomery form, and mont_mul(a, x R) = a x.
 // The transform is decimation-in-frequency radix-2, grouped into passes of
-// up to 11 stages; each pass stages one group of 2^k elements (stride 2^lb)
-// in shared memory as 8 padded word planes and runs its stages in
-// register rounds of two (each thread owns 4 elements per round), with
-// twiddles from a resident table w^i (i < n/2).  A final pass applies the
-// bit-reversal permutation fused with the inverse and coset scaling.
+// up to 11 stages; each pass stages a tile of 2^11 elements (one group of
+// 2^k elements with stride 2^lb, or several consecutive groups when k < 11)
+// in shared memory as two swizzled planes of 16-byte halves and runs its
+// stages in register rounds of two (each thread owns 4 elements per round),
+// with twiddles from a resident table w^i (i < n/2).  The last pass writes
+// the output in natural order (bit reversal fused with the inverse and
+// coset scaling).
+//
+// Batches of transforms of any sizes run as ONE persistent launch: blocks
+// take tiles from an atomic counter in pass order; a tile of pass p of a
+// transform waits (bounded) until every tile of its pass p - 1 is done.
 #pragma once
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <map>
 #include <memory>
+#include <vector>
 
 #include "engine.hpp"
 
@@ -50,5 +57,35 @@ constexpr int NTT_MAX_LOG = 26;
 // d_in, d_out: canonical elements (may alias).  Throws InvalidArgument for
 // non-canonical input (checked on device, reported after the transform).
 void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, int kind, cudaStream_t stream);
+
+// Twiddle and scaling tables of one (size, kind), built on first use and
+// kept in the workspace.
+NttTables& ntt_tables(NttWorkspace& ws, int logn, int kind, cudaStream_t stream);
+
+// ---------------------------------------------------------------- batches
+struct NttBatchItem {
+    const uint8_t* in;  // canonical elements on the device
+    uint8_t* out;       // may alias in
+    int logn;           // 1..24
+    int kind;           // NttKind
+};
+
+// A prepared batch: descriptors, the tile list and per-transform working
+// vectors on the device.  Prepare once, enqueue any number of times (each
+// enqueue = two memsets and one kernel launch, no allocation, no host
+// synchronisation: capturable in a CUDA graph).
+struct NttBatch {
+    DevBuf descs, tiles, ctl, work, errs;
+    uint32_t count = 0, ntiles = 0, grid = 0;
+    uint64_t elements = 0;
+    std::vector<uint64_t> work_off;
+};
+void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttBatchItem>& items,
+                       cudaStream_t stream);
+void ntt_batch_enqueue(NttBatch& batch, cudaStream_t stream);
+// After the stream has completed: throws InvalidArgument naming the first
+// transform with a non-canonical input, or CudaFailure if a dependency wait
+// gave up.
+void ntt_batch_check(NttBatch& batch, cudaStream_t stream);
 
 }  // namespace dv
