@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase"])
+    ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch"])
     ap.add_argument("--log-n", type=int, default=None)
     ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
     ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
@@ -63,9 +63,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
     if a.log_n is None:
-        a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20}[a.op]
+        a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20, "batch": 18}[a.op]
     if a.steps is None:
-        a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100}[a.op]
+        a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100,
+                   "batch": 20}[a.op]
     return a
 
 
@@ -134,6 +135,18 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower() == "active"})
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+class _DeviceBytes:
+    """A raw device pointer as a CUDA array (for torch.as_tensor)."""
+
+    def __init__(self, ptr, nbytes):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False),
+                                         "version": 3}
+
+
+def device_view(torch, ptr, nbytes):
+    return torch.as_tensor(_DeviceBytes(ptr, nbytes), device="cuda")
 
 
 def load_traffic(name):
@@ -418,9 +431,200 @@ class FixedBaseOp:
         return None, ms * self.n / sample, f"2^{int(math.log2(sample))} points, scaled linearly to the workload"
 
 
+def batch_workload(log_bases):
+    """The batching workload: 512 G1 MSMs of floor(2^U) points, U ~ U[8, 18],
+    over prefixes of the SRS, and 256 forward NTTs of 2^floor(U) elements,
+    U ~ U[10, 20] (seeded)."""
+    import numpy as np
+    rng = np.random.default_rng(4004)
+    sizes = [min(1 << log_bases, int(2 ** u)) for u in rng.uniform(8, 18, 512)]
+    logs = [int(u) for u in rng.uniform(10, 20, 256)]
+    return sizes, logs
+
+
+def batch_macs(sizes, logs):
+    return (sum(msm_fme(n) for n in sizes) + sum((1 << L) // 2 * L for L in logs)) * 136
+
+
+def batch_cpu(oracle, threads, bases, sizes, logs, scalars, ntt_vals):
+    """CPU oracle on a bounded sample of the batch (MSMs in order until 2^20
+    points, on all threads; the first 8 NTTs on 1 thread), scaled to the
+    whole batch by algorithmic multiply-accumulates."""
+    msm_t, msm_macs, off, k = 0.0, 0, 0, 0
+    while k < len(sizes) and (k == 0 or sum(sizes[:k]) < (1 << 20)):
+        n = sizes[k]
+        t0 = time.perf_counter()
+        oracle.msm_g1(bases[:64 * n], scalars[32 * off:32 * (off + n)], threads=threads)
+        msm_t += time.perf_counter() - t0
+        msm_macs += msm_fme(n) * 136
+        off += n
+        k += 1
+    ntt_t, ntt_macs, noff = 0.0, 0, 0
+    for L in logs[:8]:
+        n = 1 << L
+        t0 = time.perf_counter()
+        oracle.ntt(ntt_vals[32 * noff:32 * (noff + n)], "forward")
+        ntt_t += time.perf_counter() - t0
+        ntt_macs += n // 2 * L * 136
+        noff += n
+    all_msm = sum(msm_fme(n) for n in sizes) * 136
+    all_ntt = sum((1 << L) // 2 * L for L in logs) * 136
+    ms = (msm_t * all_msm / msm_macs + ntt_t * all_ntt / ntt_macs) * 1e3
+    return ms, (f"{k} MSMs ({sum(sizes[:k])} points, {threads} threads) and 8 NTTs (1 thread), scaled to the "
+                f"whole batch by algorithmic multiply-accumulates")
+
+
+class BatchOp:
+    """Batching: 512 uneven G1 MSMs over a resident SRS plus 256 uneven NTTs
+    per step, as one replay of a CUDA-graph batch plan (per-class launch
+    sequences over precomputed tables, NTTs in one persistent launch),
+    compared with the plain per-call loop on the same GPU and inputs."""
+
+    LOG_BASES = 18
+
+    def __init__(self, args):
+        self.sizes, self.logs = batch_workload(self.LOG_BASES)
+        self.metric = "batch of 512 G1 MSMs (2^8..2^18) + 256 NTTs (2^10..2^20) ms"
+        self.workload = ("512 G1 MSMs of floor(2^U) points, U~U[8,18], over prefixes of a resident 2^18 SRS "
+                         "[tau^i]G1, uniform Fr scalars; 256 forward Fr NTTs of 2^floor(U), U~U[10,20]; one "
+                         "replay of a CUDA-graph batch plan (plan creation, autotuning and tables are setup)")
+        self.profile = "batch_plan"
+
+    def setup(self, torch, b, s, rank):
+        nb = 1 << self.LOG_BASES
+        tau = torch.empty(32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(2812, 1, tau.data_ptr(), s)
+        powers = torch.empty(nb * 32, dtype=torch.uint8, device="cuda")
+        b.fr_powers_device(tau.data_ptr(), nb, powers.data_ptr(), s)
+        pts = torch.empty(nb * 64, dtype=torch.uint8, device="cuda")
+        b.fixed_base_device(powers.data_ptr(), nb, False, pts.data_ptr(), s)
+        torch.cuda.synchronize()
+        self.h_points = torch.empty(nb * 64, dtype=torch.uint8, pin_memory=True)
+        self.h_points.copy_(pts)
+        self.handle = b.register_bases(self.h_points.numpy().tobytes())
+        self.plan, self.tune_log = b.batch_plan_create(self.handle, self.sizes, self.logs)
+        self.buf = b.batch_plan_buffers(self.plan)
+        self.total = sum(self.sizes)
+        self.ntt_elems = sum(1 << L for L in self.logs)
+        b.random_fr_device(2813 + rank, self.total, self.buf.scalars, s)
+        b.random_fr_device(3000 + rank, self.ntt_elems, self.buf.ntt_values, s)
+        torch.cuda.synchronize()
+        self.config = {"msms": len(self.sizes), "msm_points_total": self.total,
+                       "msm_sizes": [min(self.sizes), max(self.sizes)], "ntts": len(self.logs),
+                       "ntt_elements_total": self.ntt_elems, "ntt_logs": [min(self.logs), max(self.logs)],
+                       "msm_classes": [{"sets": c["sets"], "c": c["best_c"]} for c in self.tune_log["classes"]],
+                       "graph_nodes": self.buf.graph_nodes, "graph_kernels": self.buf.graph_kernels}
+        self.launches_per_step = self.buf.graph_kernels
+
+    def step(self, b, s):
+        b.batch_plan_launch(self.plan, s)
+        return None
+
+    def host_inputs(self, torch):
+        import ctypes as C
+        self._b.batch_plan_check(self.plan)  # the timed replays had valid inputs
+        self.h_scalars = torch.empty(self.total * 32, dtype=torch.uint8, pin_memory=True)
+        self.h_ntt = torch.empty(self.ntt_elems * 32, dtype=torch.uint8, pin_memory=True)
+        self.h_scalars.copy_(device_view(torch, self.buf.scalars, self.buf.scalar_bytes))
+        self.h_ntt.copy_(device_view(torch, self.buf.ntt_values, self.buf.ntt_bytes))
+        self.h_msm_out = torch.empty(64 * len(self.sizes), dtype=torch.uint8, pin_memory=True)
+        self.h_ntt_out = torch.empty(self.ntt_elems * 32, dtype=torch.uint8, pin_memory=True)
+        self.graph_msm = device_view(torch, self.buf.msm_results, self.buf.msm_result_bytes).cpu().numpy().tobytes()
+        self.graph_ntt = device_view(torch, self.buf.ntt_results, self.buf.ntt_bytes).clone()
+
+    def extra(self, torch, dv, b, s):
+        """The plain per-call loop on the same GPU and inputs: device-resident
+        (dvgpu_bn254_msm_resident without precomputed tables + ntt_device per
+        transform) and reference-facing with host buffers (dvgpu_bn254_msm,
+        dvgpu_bn254_ntt_ex per call).  Both must reproduce the graph's
+        results bit for bit."""
+        err = ctypes.create_string_buffer(256)
+        d_sc = self.buf.scalars
+        d_in = self.buf.ntt_values
+        ref_ntt = torch.empty(self.ntt_elems * 32, dtype=torch.uint8, device="cuda")
+
+        def device_loop():
+            outs, off = [], 0
+            for n in self.sizes:
+                outs.append(b.msm_resident(self.handle, d_sc + 32 * off, n, stream=s))
+                off += n
+            off = 0
+            for L in self.logs:
+                b.ntt_device(d_in + 32 * off, 1 << L, 0, ref_ntt.data_ptr() + 32 * off, s)
+                off += 1 << L
+            torch.cuda.synchronize()
+            return outs
+
+        outs = device_loop()  # warm-up (window tables, NTT tables)
+        t0 = time.perf_counter()
+        outs = device_loop()
+        per_call_ms = (time.perf_counter() - t0) * 1e3
+        exact = b"".join(outs) == self.graph_msm and bool(torch.equal(ref_ntt, self.graph_ntt))
+        L = dv.lib()
+        cast = lambda p: ctypes.cast(ctypes.c_void_p(p), ctypes.c_char_p)
+        out = ctypes.create_string_buffer(64)
+        h_out = torch.empty(self.ntt_elems * 32, dtype=torch.uint8, pin_memory=True)
+
+        def host_loop():
+            res, off = [], 0
+            for n in self.sizes:
+                if L.dvgpu_bn254_msm(b.handle, self.h_points.data_ptr(), self.h_scalars.data_ptr() + 32 * off, n,
+                                     out, err, 256) != 0:
+                    raise RuntimeError(err.value)
+                res.append(out.raw)
+                off += n
+            off = 0
+            for Lg in self.logs:
+                if L.dvgpu_bn254_ntt_ex(b.handle, self.h_ntt.data_ptr() + 32 * off, 1 << Lg, 0,
+                                        cast(h_out.data_ptr() + 32 * off), err, 256) != 0:
+                    raise RuntimeError(err.value)
+                off += 1 << Lg
+            return res
+
+        t0 = time.perf_counter()
+        res = host_loop()
+        per_call_e2e_ms = (time.perf_counter() - t0) * 1e3
+        exact = exact and b"".join(res) == self.graph_msm and bool(torch.equal(h_out, self.graph_ntt.cpu()))
+        # the graph replay itself, host-timed the same way (launch + synchronize)
+        t0 = time.perf_counter()
+        b.batch_plan_launch(self.plan, s)
+        torch.cuda.synchronize()
+        graph_wall_ms = (time.perf_counter() - t0) * 1e3
+        return {"per_call": {"device_resident_loop_ms": per_call_ms, "host_buffer_loop_ms": per_call_e2e_ms,
+                             "graph_replay_wall_ms": graph_wall_ms, "bit_exact_with_graph": exact,
+                             "calls_per_batch": len(self.sizes) + len(self.logs),
+                             "note": "wall clock around each loop; every per-call form returns its result to "
+                                     "the host, the graph form waits once"}}
+
+    def e2e_step(self, dv, b):
+        err = ctypes.create_string_buffer(256)
+        cast = lambda t: ctypes.cast(ctypes.c_void_p(t.data_ptr()), ctypes.c_char_p)
+        rc = dv.lib().dvgpu_batch_plan_run(b.handle, self.plan, self.h_scalars.data_ptr(), self.h_ntt.data_ptr(),
+                                           cast(self.h_msm_out), cast(self.h_ntt_out), err, 256)
+        if rc != 0:
+            raise RuntimeError(err.value)
+        return None
+
+    def e2e_bytes(self):
+        return 32 * (self.total + self.ntt_elems), 64 * len(self.sizes) + 32 * self.ntt_elems
+
+    def roofline(self, tl, imad_peak, step_ms):
+        macs = batch_macs(self.sizes, self.logs)
+        ach = macs / (step_ms * 1e-3) / 1e12
+        return ({"bound": "imad", "kernel": "whole batch graph (MSM accumulation dominant)", "achieved": ach,
+                 "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
+                 "algorithmic_macs_per_launch": macs, "launch_ms": step_ms}, None)
+
+    def cpu(self, oracle, threads):
+        ms, sample = batch_cpu(oracle, threads, self.h_points.numpy().tobytes(), self.sizes, self.logs,
+                               self.h_scalars.numpy().tobytes(), self.h_ntt.numpy().tobytes())
+        return None, ms, sample
+
+
 def make_op(args):
-    return {"msm": lambda: MsmOp(args), "msmres": lambda: ResidentMsmOp(args), "g2msm": lambda: MsmOp(args, g2=True), "ntt": lambda: NttOp(args),
-            "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args)}[args.op]()
+    return {"msm": lambda: MsmOp(args), "msmres": lambda: ResidentMsmOp(args), "g2msm": lambda: MsmOp(args, g2=True),
+            "ntt": lambda: NttOp(args), "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args),
+            "batch": lambda: BatchOp(args)}[args.op]()
 
 
 # ----------------------------------------------------------------- reference arm
@@ -455,6 +659,20 @@ def run_reference(args, rank, world):
         fn = lambda: oracle.sparse_msm_g1(bases, idx, vals, threads=threads)
         metric = f"sparse G1 MSM k={args.k} over 2^{args.log_n} bases us"
         sample = f"k={args.k} sparse MSMs"
+    elif op == "batch":
+        sizes, logs = batch_workload(BatchOp.LOG_BASES)
+        nb = 1 << BatchOp.LOG_BASES
+        bases = oracle.fixed_base_g1(oracle.fr_powers(oracle.uniform_fr(2812, 1), nb), threads=threads)
+        scalars = oracle.uniform_fr(2813, min(sum(sizes), (1 << 20) + nb))
+        ntt_vals = oracle.uniform_fr(3000, sum(1 << L for L in logs[:8]))
+        est = []
+
+        def fn():
+            ms, smp = batch_cpu(oracle, threads, bases, sizes, logs, scalars, ntt_vals)
+            est.append((ms, smp))
+
+        metric = BatchOp(args).metric
+        sample = "batch estimates"
     else:
         sc = oracle.fr_powers(oracle.uniform_fr(2812, 1), n)
         fn = lambda: oracle.fixed_base_g1(sc, threads=threads)
@@ -470,6 +688,9 @@ def run_reference(args, rank, world):
         fn()
         times.append((time.perf_counter() - t0) * 1e3)
     value = sum(times) / len(times)
+    if op == "batch":
+        value = sum(e[0] for e in est[1:]) / len(est[1:])
+        sample = f"batch estimates, each from {est[-1][1]}"
     if op == "sparse":
         value *= 1e3  # us
     unit = "us" if op == "sparse" else "ms"
@@ -508,9 +729,14 @@ def main():
     from __graft_entry__ import load_package
     dv = load_package()
     b = dv.DvgpuBackend()
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: every entry point gets its handle (a null handle
+    # would select the owner's own stream), so the events below bracket the
+    # work itself, including graph replays that return before completion
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     s = stream.cuda_stream
     op = make_op(args)
+    op._b = b
     op.setup(torch, b, s, rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     result = None
@@ -544,7 +770,7 @@ def main():
             raise RuntimeError("result changed between steps")
     torch.cuda.synchronize()
     tl = b.msm_timeline(False)
-    launches = b.launch_count() - launches0
+    launches = b.launch_count() - launches0 + getattr(op, "launches_per_step", 0) * args.steps
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
@@ -574,6 +800,7 @@ def main():
         e2e_total = float(t.item())
     e2e_ms = e2e_total / (args.e2e_steps * world)
 
+    extra = op.extra(torch, dv, b, s) if hasattr(op, "extra") else {}
     imad_peak = b.probe_imad_rate()
     roof, whole = op.roofline(tl, imad_peak, ms_per_step)
     roof["traffic"] = load_traffic(op.profile)
@@ -598,6 +825,7 @@ def main():
     }
     if whole:
         line["msm_roofline"] = whole
+    line.update(extra)
     if tl.calls:
         line["phases_ms"] = {name: tl.ms[k] / tl.calls for k, name in enumerate(dv.MSM_PHASE_NAMES)}
     if op.tune_log:

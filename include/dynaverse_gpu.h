@@ -282,7 +282,7 @@ typedef struct DvgpuBatchPlanBuffers {
     uint8_t* msm_results;  /* msm_count x 64 bytes */
     uint8_t* ntt_results;  /* sum(2^ntt_log_sizes) x 32 bytes */
     uint64_t scalar_bytes, ntt_bytes, msm_result_bytes;
-    uint32_t msm_classes, graph_nodes;
+    uint32_t msm_classes, graph_nodes, graph_kernels, reserved;
 } DvgpuBatchPlanBuffers;
 int dvgpu_batch_plan_create(void* backend, uint64_t bases_handle, const uint64_t* msm_sizes, size_t msm_count,
                             const uint32_t* ntt_log_sizes, const int32_t* ntt_kinds, size_t ntt_count,

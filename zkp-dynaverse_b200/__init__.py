@@ -66,7 +66,7 @@ class BatchPlanBuffers(ctypes.Structure):
     _fields_ = [("scalars", ctypes.c_void_p), ("ntt_values", ctypes.c_void_p), ("msm_results", ctypes.c_void_p),
                 ("ntt_results", ctypes.c_void_p), ("scalar_bytes", ctypes.c_uint64), ("ntt_bytes", ctypes.c_uint64),
                 ("msm_result_bytes", ctypes.c_uint64), ("msm_classes", ctypes.c_uint32),
-                ("graph_nodes", ctypes.c_uint32)]
+                ("graph_nodes", ctypes.c_uint32), ("graph_kernels", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class SetupStats(ctypes.Structure):

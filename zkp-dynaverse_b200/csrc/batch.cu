@@ -223,7 +223,15 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
     DV_CUDA(cudaStreamEndCapture(p.stream, &p.graph));
     DV_CUDA(cudaGraphInstantiate(&p.exec, p.graph, 0));
     DV_CUDA(cudaGraphGetNodes(p.graph, nullptr, &p.graph_nodes));
-    log += ",\"graph_nodes\":" + std::to_string(p.graph_nodes) + "}";
+    std::vector<cudaGraphNode_t> nodes(p.graph_nodes);
+    DV_CUDA(cudaGraphGetNodes(p.graph, nodes.data(), &p.graph_nodes));
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        DV_CUDA(cudaGraphNodeGetType(node, &type));
+        if (type == cudaGraphNodeTypeKernel) ++p.graph_kernels;
+    }
+    log += ",\"graph_nodes\":" + std::to_string(p.graph_nodes) +
+           ",\"graph_kernels\":" + std::to_string(p.graph_kernels) + "}";
     p.last = p.stream;
     return plan;
 }
@@ -357,6 +365,8 @@ extern "C" int dvgpu_batch_plan_buffers(void* opaque, uint64_t handle, DvgpuBatc
         out->msm_result_bytes = p.msm_sizes.size() * 64;
         out->msm_classes = (uint32_t)p.classes.size();
         out->graph_nodes = (uint32_t)p.graph_nodes;
+        out->graph_kernels = (uint32_t)p.graph_kernels;
+        out->reserved = 0;
     });
 }
 

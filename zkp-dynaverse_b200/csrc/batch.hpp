@@ -43,7 +43,7 @@ struct BatchPlan {
     cudaEvent_t fork = nullptr, join = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    size_t graph_nodes = 0;
+    size_t graph_nodes = 0, graph_kernels = 0;
 
     std::vector<uint64_t> msm_sizes, scalar_off;
     std::vector<std::unique_ptr<BatchClass>> classes;
