@@ -515,6 +515,9 @@ class BatchOp:
                        "msm_classes": [{"sets": c["sets"], "c": c["best_c"]} for c in self.tune_log["classes"]],
                        "graph_nodes": self.buf.graph_nodes, "graph_kernels": self.buf.graph_kernels}
         self.launches_per_step = self.buf.graph_kernels
+        # library kernels run so far (captured launches did not run): a
+        # profiler skips these plus the warm-up replays to reach a replay
+        self.config["setup_launches"] = b.launch_count() - self.buf.graph_kernels
 
     def step(self, b, s):
         b.batch_plan_launch(self.plan, s)
