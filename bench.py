@@ -54,19 +54,21 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch"])
+    ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch", "g2check"])
     ap.add_argument("--log-n", type=int, default=None)
     ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
     ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
+    ap.add_argument("--alg", type=int, default=3, choices=[1, 2, 3], help="g2check: subgroup algorithm")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
     if a.log_n is None:
-        a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20, "batch": 18}[a.op]
+        a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20, "batch": 18,
+                   "g2check": 16}[a.op]
     if a.steps is None:
         a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100,
-                   "batch": 20}[a.op]
+                   "batch": 20, "g2check": 50}[a.op]
     return a
 
 
@@ -431,6 +433,93 @@ class FixedBaseOp:
         return None, ms * self.n / sample, f"2^{int(math.log2(sample))} points, scaled linearly to the workload"
 
 
+BN_R = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+BN_X = 4965661367192848881
+
+
+def g2_check_fme(alg):
+    """Fq multiplications per point of a subgroup check: G2 XYZZ doubling 27
+    (9 Fq2 products), mixed addition 30, full addition 42, psi 6.
+    Algorithm 1: [r]Q = 0; 2: psi(Q) = [6x^2]Q; 3: the seed-x Frobenius
+    relation ([x]Q + Q + psi([x]Q) + psi^2([x]Q) = psi^3([2x]Q))."""
+    if alg == 1:
+        return 254 * 27 + bin(BN_R).count("1") * 30
+    if alg == 2:
+        lam = 6 * BN_X * BN_X
+        return (lam.bit_length() - 1) * 27 + bin(lam).count("1") * 30 + 6 + 3 * 10
+    return (BN_X.bit_length() - 1) * 27 + bin(BN_X).count("1") * 30 + 3 * 6 + 30 + 2 * 42 + 27 + 2 * 3 * 10
+
+
+class G2CheckOp:
+    """Batched G2 subgroup check over a corpus of 2^n wire points: half
+    [s]G2 for uniform s (valid), half random twist points without cofactor
+    clearing (invalid), all in one launch."""
+
+    def __init__(self, args):
+        self.n = 1 << args.log_n
+        self.alg = args.alg
+        self.metric = f"G2 subgroup check 2^{args.log_n} points ms (algorithm {args.alg})"
+        self.workload = (f"2^{args.log_n} G2 wire points: half [s]G2 for uniform s, half random on-curve twist "
+                         f"points without cofactor clearing; subgroup algorithm {args.alg}")
+        self.profile = f"g2_check_2p{args.log_n}"
+
+    def setup(self, torch, b, s, rank):
+        half = self.n // 2
+        sc = torch.empty(half * 32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(4100 + rank, half, sc.data_ptr(), s)
+        self.wire = torch.empty(self.n * 128, dtype=torch.uint8, device="cuda")
+        b.fixed_base_device(sc.data_ptr(), half, True, self.wire.data_ptr(), s)
+        b.random_twist_device(4200 + rank, self.n - half, self.wire.data_ptr() + 128 * half, s)
+        self.masks = torch.empty(self.n, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        self.tune_log = None
+        self.config = {"points": self.n, "valid": half, "algorithm": self.alg}
+
+    def step(self, b, s):
+        rep = b.g2_check_device(self.wire.data_ptr(), self.n, self.alg, self.masks.data_ptr(), s)
+        return (rep.invalid_points, rep.first_invalid, rep.failure_mask)
+
+    def host_inputs(self, torch):
+        self.h_wire = torch.empty(self.n * 128, dtype=torch.uint8, pin_memory=True)
+        self.h_wire.copy_(self.wire)
+        self.h_masks = torch.empty(self.n, dtype=torch.int32, pin_memory=True)
+
+    def e2e_step(self, dv, b):
+        rep = dv.G2ValidationReport()
+        err = ctypes.create_string_buffer(256)
+        rc = dv.lib().dvgpu_bn254_g2_validation_inspect(b.handle, self.h_wire.data_ptr(), self.n, self.alg,
+                                                         self.h_masks.data_ptr(), ctypes.byref(rep), err, 256)
+        if rc not in (0, -5):  # -5: content rejected, report published (the reference's convention)
+            raise RuntimeError(err.value)
+        return (rep.invalid_points, rep.first_invalid, rep.failure_mask)
+
+    def e2e_bytes(self):
+        return self.n * 128, self.n * 4
+
+    def roofline(self, tl, imad_peak, step_ms):
+        macs = self.n * g2_check_fme(self.alg) * 136
+        ach = macs / (step_ms * 1e-3) / 1e12
+        return ({"bound": "imad", "kernel": "k_g2_check", "achieved": ach, "peak": imad_peak / 1e12,
+                 "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12), "algorithmic_macs_per_launch": macs,
+                 "fme_per_point": g2_check_fme(self.alg), "launch_ms": step_ms}, None)
+
+    def cpu(self, oracle, threads):
+        import numpy as np
+        sample = min(self.n, 1 << 13)
+        wire = self.h_wire.numpy().tobytes()
+        half = self.n // 2
+        sub = wire[:64 * sample] + wire[128 * half:128 * half + 64 * sample]  # half valid, half invalid
+        t0 = time.perf_counter()
+        masks = oracle.g2_check(sub, self.alg, threads=threads)
+        ms = (time.perf_counter() - t0) * 1e3
+        gpu = self.h_masks.numpy()
+        agree = bool(np.array_equal(masks[:sample // 2], gpu[:sample // 2]) and
+                     np.array_equal(masks[sample // 2:], gpu[half:half + sample // 2]))
+        self.cpu_agrees = agree
+        return None, ms * self.n / sample, (f"{sample} points (half valid, half invalid) on {threads} threads, "
+                                            f"scaled linearly; verdicts identical to the GPU's: {agree}")
+
+
 def batch_workload(log_bases):
     """The batching workload: 512 G1 MSMs of floor(2^U) points, U ~ U[8, 18],
     over prefixes of the SRS, and 256 forward NTTs of 2^floor(U) elements,
@@ -627,7 +716,7 @@ class BatchOp:
 def make_op(args):
     return {"msm": lambda: MsmOp(args), "msmres": lambda: ResidentMsmOp(args), "g2msm": lambda: MsmOp(args, g2=True),
             "ntt": lambda: NttOp(args), "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args),
-            "batch": lambda: BatchOp(args)}[args.op]()
+            "batch": lambda: BatchOp(args), "g2check": lambda: G2CheckOp(args)}[args.op]()
 
 
 # ----------------------------------------------------------------- reference arm

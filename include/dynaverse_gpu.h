@@ -243,6 +243,12 @@ int dvgpu_random_fr_device(void* backend, uint64_t seed, size_t n, uint8_t* d_ou
                            size_t error_capacity);
 int dvgpu_fr_powers_device(void* backend, const uint8_t* d_tau, size_t n, uint8_t* d_out, void* stream, char* error,
                            size_t error_capacity);
+/* n seeded random points of the G2 twist curve, 128-byte wire form, with no
+ * cofactor clearing: on the curve but (with overwhelming probability) not in
+ * the order-r subgroup -- the invalid half of a subgroup-check corpus, as
+ * built by crates/gpu/src/g2_validation/tests.rs:24-31. */
+int dvgpu_g2_random_twist_device(void* backend, uint64_t seed, size_t n, uint8_t* d_out, void* stream, char* error,
+                                 size_t error_capacity);
 
 /* ---------------------------------------------------------------- batching
  * No counterpart in the reference ABI (its batch path is

@@ -125,3 +125,21 @@ def test_fixed_base_g2_checked(backend, oracle, dv):
     out, rep = backend.fixed_base_g2_checked(sc, 3)
     assert out == oracle.fixed_base_g2(sc)
     assert rep.invalid_points == 0 and rep.first_invalid == 2**64 - 1 and rep.checked_points == 300
+
+
+def test_random_twist_points_are_off_subgroup(backend, oracle):
+    """The device corpus generator: every point parses, lies on the twist
+    curve and (no cofactor clearing) fails the subgroup check -- mask 4 in
+    the oracle and on the GPU, for every algorithm."""
+    import torch
+    n = 300
+    d = torch.empty(n * 128, dtype=torch.uint8, device="cuda")
+    backend.random_twist_device(99, n, d.data_ptr())
+    torch.cuda.synchronize()
+    wire = d.cpu().numpy().tobytes()
+    assert len(set(wire[128 * i:128 * (i + 1)] for i in range(n))) == n
+    for alg in (1, 2, 3):
+        expect = oracle.g2_check(wire, alg)
+        assert (expect == 4).all(), alg
+        masks, rep = backend.inspect_g2_validation(wire, alg)
+        assert (masks == expect).all() and rep.invalid_points == n, alg

@@ -125,6 +125,7 @@ SIGNATURES = [
     ("dvgpu_msm_timeline", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(MsmPhaseTimes)]),
     ("dvgpu_random_fr_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
     ("dvgpu_fr_powers_device", ctypes.c_int, [_P, _P, _SZ, _P, _P] + _E),
+    ("dvgpu_g2_random_twist_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
     ("dvgpu_bn254_ntt_batch", ctypes.c_int, [_P, _P, _P, _P, _SZ, _B] + _E),
     ("dvgpu_bn254_ntt_batch_device", ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P] + _E),
     ("dvgpu_batch_plan_create", ctypes.c_int,
@@ -487,6 +488,10 @@ class DvgpuBackend:
 
     def random_fr_device(self, seed: int, n: int, d_out: int, stream=None):
         self._call("dvgpu_random_fr_device", seed, n, d_out, stream)
+
+    def random_twist_device(self, seed: int, n: int, d_out: int, stream=None):
+        """n random on-curve G2 twist points (wire form) outside the subgroup."""
+        self._call("dvgpu_g2_random_twist_device", seed, n, d_out, stream)
 
     def fr_powers_device(self, d_tau: int, n: int, d_out: int, stream=None):
         self._call("dvgpu_fr_powers_device", d_tau, n, d_out, stream)

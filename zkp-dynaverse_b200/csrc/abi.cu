@@ -796,6 +796,7 @@ extern "C" int dvgpu_probe_imad_rate(void* opaque, double* macs_per_second, char
 namespace dv {
 void random_fr_launch(uint64_t seed, uint64_t n, uint8_t* d_out, cudaStream_t st);
 void powers_launch(const uint8_t* d_tau, uint64_t n, uint8_t* d_out, cudaStream_t st);
+void random_twist_launch(uint64_t seed, uint64_t n, uint8_t* d_out, cudaStream_t st);
 }  // namespace dv
 
 extern "C" uint64_t dvgpu_launch_count(void) { return __atomic_load_n(&dv::launch_counter(), __ATOMIC_RELAXED); }
@@ -834,6 +835,14 @@ extern "C" int dvgpu_random_fr_device(void* opaque, uint64_t seed, size_t n, uin
     return guarded(opaque, error, cap, [&](Backend& b) {
         require(!n || d_out, "null output");
         dv::random_fr_launch(seed, n, d_out, pick(b, stream));
+    });
+}
+
+extern "C" int dvgpu_g2_random_twist_device(void* opaque, uint64_t seed, size_t n, uint8_t* d_out, void* stream,
+                                            char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(!n || d_out, "null output");
+        dv::random_twist_launch(seed, n, d_out, pick(b, stream));
     });
 }
 
