@@ -31,6 +31,12 @@ struct FrCfg {
 
 #define DV_INL __device__ __forceinline__
 
+// Two results of a paired multiplication.
+template <class T>
+struct PairOf {
+    T r0, r1;
+};
+
 template <class C>
 struct __align__(16) Fp {  // 16-byte aligned: global copies move as 128-bit accesses
     uint32_t v[8];
@@ -212,6 +218,17 @@ struct __align__(16) Fp {  // 16-byte aligned: global copies move as 128-bit acc
 #else
     DV_INL static Fp mul(const Fp& a, const Fp& b) { return mul_inl(a, b); }
 #endif
+    // Two independent products in one out-of-line body: the compiler
+    // interleaves their carry chains, which hides the multiply latency that a
+    // lone chain exposes when few warps are resident.
+    typedef PairOf<Fp> Pair;
+#ifndef DV_MUL_INLINE
+    __device__ __noinline__ static Pair mul2(Fp a, Fp b, Fp c, Fp d) { return {mul_inl(a, b), mul_inl(c, d)}; }
+#else
+    DV_INL static Pair mul2(const Fp& a, const Fp& b, const Fp& c, const Fp& d) {
+        return {mul_inl(a, b), mul_inl(c, d)};
+    }
+#endif
     DV_INL static Fp sqr(const Fp& a) { return mul(a, a); }
 
     // Canonical little-endian limbs <-> Montgomery form.
@@ -275,6 +292,9 @@ struct Fq2 {
         const Fq t1 = Fq::mul(a.c1, b.c1);
         const Fq t2 = Fq::mul(Fq::add(a.c0, a.c1), Fq::add(b.c0, b.c1));
         return {Fq::sub(t0, t1), Fq::sub(Fq::sub(t2, t0), t1)};
+    }
+    DV_INL static PairOf<Fq2> mul2(const Fq2& a, const Fq2& b, const Fq2& c, const Fq2& d) {
+        return {mul(a, b), mul(c, d)};
     }
     DV_INL static Fq2 sqr(const Fq2& a) {
         // (c0 + c1 u)^2 = (c0+c1)(c0-c1) + 2 c0 c1 u
