@@ -311,15 +311,24 @@ __global__ void __launch_bounds__(TH) k_fixup_long(const int* __restrict__ pgid,
     }
 }
 
-// 6. Bucket reduction, level 1.  Window (set, w) needs
+// 6. Bucket reduction.  Window (set, w) needs
 //      S_w = sum_b (b + 1) B_b,   b < 2^(c-1).
-// Segment j holds buckets [j s, (j+1) s); a running sum from the top gives
-//      U_j = sum_i (i + 1) B_{js+i},   R_j = sum_i B_{js+i},
-// and S_w = sum_j U_j + s * sum_j j R_j   (combined by k_wlevel).
+// Every level carries a window as pairs (U_j, V_j) with
+//      S_w = sum_j U_j + sum_j j V_j ,
+// V_j already multiplied by the weight unit of its level.  Level 1:
+// segment j holds buckets [j s, (j+1) s); a running sum from the top gives
+//      U_j = sum_i (i + 1) B_{js+i},   V_j = s sum_i B_{js+i}.
+// Grouping G consecutive pairs (j = G q + l) gives the next level:
+//      U'_q = sum_l U_{Gq+l} + sum_l l V_{Gq+l} = sum_l (U_l + Suf_{l+1}),
+//      V'_q = G sum_l V_{Gq+l},
+// with Suf the group's suffix sums of V; the doublings for G apply to one
+// sum per group, so the critical path holds log2(total weight) of them.
+
+// Level 1: one segment of s buckets per thread.
 template <class F>
 __global__ void __launch_bounds__(128) k_segments(const XYZZ<F>* __restrict__ buckets, const uint32_t* __restrict__ offsets,
                                                   uint32_t B, uint32_t NW, int seg_log, XYZZ<F>* __restrict__ seg_u,
-                                                  XYZZ<F>* __restrict__ seg_r) {
+                                                  XYZZ<F>* __restrict__ seg_v) {
     const uint32_t S = B >> seg_log;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= NW * S) return;
@@ -332,24 +341,17 @@ __global__ void __launch_bounds__(128) k_segments(const XYZZ<F>* __restrict__ bu
         if (offsets[g + 1] != offsets[g]) R = XYZZ<F>::add(R, buckets[g]);
         U = XYZZ<F>::add(U, R);
     }
+    for (int i = 0; i < seg_log; ++i) R = XYZZ<F>::dbl(R);  // V = s R
     seg_u[tid] = U;
-    seg_r[tid] = R;
+    seg_v[tid] = R;
 }
 
-// 7. Bucket reduction, upper levels.  Each window is carried as a pair of
-// vectors (U, R) of length S with a power-of-two multiplier m:
-//      S_w = sum_j U_j + m * sum_j j R_j .
-// A level splits each window into blocks of P entries; block k (entries
-// j = k P + t) replaces its P pairs by one pair
-//      U'_k = sum_t ( U_t + m Suf_{t+1} ),   R'_k = sum_t R_t ,
-// where Suf is the block's suffix sum of R (so sum_t t R_t = sum_t Suf_{t+1}),
-// and the multiplier becomes m P.  Levels repeat until one entry per window
-// remains, which is S_w.  Depth per level: log2 P (scan) + log2 m
-// (doublings) + log2 P (tree).
+// Upper levels: blocks of P pairs (G = P), suffix scan and tree in shared
+// memory.  Windows of S pairs; S <= P is the last level (one block per
+// window, its U' is S_w).
 template <class F, int P>
-__global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, const XYZZ<F>* __restrict__ r_in,
-                                              uint32_t S, int log_m, XYZZ<F>* __restrict__ u_out,
-                                              XYZZ<F>* __restrict__ r_out) {
+__global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, const XYZZ<F>* __restrict__ v_in,
+                                              uint32_t S, XYZZ<F>* __restrict__ u_out, XYZZ<F>* __restrict__ v_out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     XYZZ<F>* sh = reinterpret_cast<XYZZ<F>*>(smem_raw);
     const uint32_t nblk = S > (uint32_t)P ? S / P : 1u;
@@ -358,7 +360,7 @@ __global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, 
     const uint32_t t = threadIdx.x;
     const size_t idx = (size_t)w * S + (size_t)k * P + t;
     const bool live = t < width;
-    sh[t] = live ? r_in[idx] : XYZZ<F>::inf();
+    sh[t] = live ? v_in[idx] : XYZZ<F>::inf();
     __syncthreads();
     for (uint32_t d = 1; d < width; d <<= 1) {
         const XYZZ<F> o = t + d < width ? sh[t + d] : XYZZ<F>::inf();
@@ -367,9 +369,8 @@ __global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, 
         __syncthreads();
     }
     XYZZ<F> x = t + 1 < width ? sh[t + 1] : XYZZ<F>::inf();  // Suf_{t+1}
-    if (t == 0) r_out[blockIdx.x] = sh[0];                     // sum of the block's R
+    XYZZ<F> vsum = sh[0];
     __syncthreads();
-    for (int i = 0; i < log_m; ++i) x = XYZZ<F>::dbl(x);
     if (live) x = XYZZ<F>::add(x, u_in[idx]);
     sh[t] = x;
     __syncthreads();
@@ -377,7 +378,13 @@ __global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, 
         if (t < d) sh[t] = XYZZ<F>::add(sh[t], sh[t + d]);
         __syncthreads();
     }
-    if (t == 0) u_out[blockIdx.x] = sh[0];
+    if (t == 0) {
+        u_out[blockIdx.x] = sh[0];
+        if (nblk > 1) {
+            for (int i = 0; i < __builtin_ctz((unsigned)P); ++i) vsum = XYZZ<F>::dbl(vsum);  // V' = P sum V
+            v_out[blockIdx.x] = vsum;
+        }
+    }
 }
 
 // Window multiples of resident bases: table[i W + w] = 2^(c w) P_i (affine,
@@ -659,20 +666,18 @@ void msm_enqueue(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_
     k_segments<F><<<blocks_for((uint64_t)NW * S, 128), 128, 0, st>>>(d_buckets, d_offsets, B, NW, seg_log, d_seg_u,
                                                                      d_seg_r);
     DV_LAUNCH();
-    // upper levels: (U, R) pairs with multiplier m = 2^log_m
+    // upper levels: (U, V) pairs
     XYZZ<F>* u = d_seg_u;
     XYZZ<F>* r = d_seg_r;
     XYZZ<F>* u2 = d_lvl_u;
     XYZZ<F>* r2 = d_lvl_r;
     uint32_t len = S;
-    int log_m = seg_log;
     for (;;) {
         const uint32_t nblk = len > (uint32_t)P ? len / P : 1u;
         XYZZ<F>* u_dst = nblk == 1 ? d_win : u2;
-        k_wlevel<F, P><<<NW * nblk, P, smem, st>>>(u, r, len, log_m, u_dst, r2);
+        k_wlevel<F, P><<<NW * nblk, P, smem, st>>>(u, r, len, u_dst, r2);
         DV_LAUNCH();
         if (nblk == 1) break;
-        log_m += __builtin_ctz((unsigned)P);
         len = nblk;
         std::swap(u, u2);
         std::swap(r, r2);
