@@ -301,6 +301,44 @@ int dvgpu_batch_plan_run(void* backend, uint64_t plan, const uint8_t* scalars, c
                          uint8_t* msm_results, uint8_t* ntt_results, char* error, size_t error_capacity);
 int dvgpu_batch_plan_destroy(void* backend, uint64_t plan, char* error, size_t error_capacity);
 
+/* ---------------------------------------------------------------- serving
+ * No counterpart in the reference ABI: the reference serves updates one
+ * call at a time per session (crates/protocol/src/session.rs:51-142).
+ *
+ * A server keeps sessions resident -- SRS bases (G1 wire form in), the
+ * committed vector of canonical Fr values, and its commitment
+ * C = sum v_i G_i -- and admits a session only while the resident bytes
+ * (n x 96 + 64 per session) stay within hbm_budget_bytes (-1 otherwise).
+ * dvgpu_serve_submit queues a commitment update of a session: the entries
+ * at `indices` (distinct, < n) take the new `values`; the result is the new
+ * commitment C' = C + sum (v'_i - v_i) G_i.  One engine thread merges the
+ * pending requests of up to max_batch sessions into shared launches (one
+ * per session per batch; a session's requests complete in order), and
+ * requests arriving meanwhile form the next batch.  max_batch = 1 is the
+ * per-call form.  dvgpu_serve_wait blocks until a ticket completes and
+ * returns its commitment and timings (steady-clock nanoseconds).  The
+ * server uses device 0 and its own stream and workspaces. */
+typedef struct DvgpuServeResult {
+    uint64_t submit_ns, start_ns, done_ns;
+    uint32_t batch_requests, batch_id;
+} DvgpuServeResult;
+typedef struct DvgpuServeStats {
+    uint64_t requests, batches, sessions, resident_bytes, budget_bytes;
+    uint64_t max_batch, largest_batch, busy_ns, pending;
+} DvgpuServeStats;
+int dvgpu_serve_create(uint64_t hbm_budget_bytes, uint32_t max_batch, void** server, char* error,
+                       size_t error_capacity);
+void dvgpu_serve_destroy(void* server);
+int dvgpu_serve_open_session(void* server, const uint8_t* srs_g1, const uint8_t* values, size_t n, uint64_t* session,
+                             uint8_t* commitment, char* error, size_t error_capacity);
+int dvgpu_serve_close_session(void* server, uint64_t session, char* error, size_t error_capacity);
+int dvgpu_serve_submit(void* server, uint64_t session, const uint64_t* indices, const uint8_t* values, size_t k,
+                       uint64_t* ticket, char* error, size_t error_capacity);
+int dvgpu_serve_wait(void* server, uint64_t ticket, uint8_t* commitment, DvgpuServeResult* result, char* error,
+                     size_t error_capacity);
+int dvgpu_serve_set_max_batch(void* server, uint32_t max_batch);
+int dvgpu_serve_stats(void* server, DvgpuServeStats* out);
+
 #ifdef __cplusplus
 }
 #endif

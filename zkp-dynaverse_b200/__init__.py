@@ -62,6 +62,17 @@ class MsmPhaseTimes(ctypes.Structure):
 MSM_PHASE_NAMES = ["hist", "scan", "scatter", "accum", "merge", "reduce", "unused", "tail"]
 
 
+class ServeResult(ctypes.Structure):
+    _fields_ = [("submit_ns", ctypes.c_uint64), ("start_ns", ctypes.c_uint64), ("done_ns", ctypes.c_uint64),
+                ("batch_requests", ctypes.c_uint32), ("batch_id", ctypes.c_uint32)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in ("requests", "batches", "sessions", "resident_bytes",
+                                                      "budget_bytes", "max_batch", "largest_batch", "busy_ns",
+                                                      "pending")]
+
+
 class BatchPlanBuffers(ctypes.Structure):
     _fields_ = [("scalars", ctypes.c_void_p), ("ntt_values", ctypes.c_void_p), ("msm_results", ctypes.c_void_p),
                 ("ntt_results", ctypes.c_void_p), ("scalar_bytes", ctypes.c_uint64), ("ntt_bytes", ctypes.c_uint64),
@@ -135,6 +146,14 @@ SIGNATURES = [
     ("dvgpu_batch_plan_check", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
     ("dvgpu_batch_plan_run", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _B, _B] + _E),
     ("dvgpu_batch_plan_destroy", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
+    ("dvgpu_serve_create", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(_P)] + _E),
+    ("dvgpu_serve_destroy", None, [_P]),
+    ("dvgpu_serve_open_session", ctypes.c_int, [_P, _P, _P, _SZ, ctypes.POINTER(ctypes.c_uint64), _B] + _E),
+    ("dvgpu_serve_close_session", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
+    ("dvgpu_serve_submit", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _SZ, ctypes.POINTER(ctypes.c_uint64)] + _E),
+    ("dvgpu_serve_wait", ctypes.c_int, [_P, ctypes.c_uint64, _B, ctypes.POINTER(ServeResult)] + _E),
+    ("dvgpu_serve_set_max_batch", ctypes.c_int, [_P, ctypes.c_uint32]),
+    ("dvgpu_serve_stats", ctypes.c_int, [_P, ctypes.POINTER(ServeStats)]),
 ]
 
 
@@ -198,6 +217,79 @@ def ntt_noalloc(d_values: int, n: int, kind: int, d_result: int, stream=None):
     rc = lib().dvgpu_bn254_ntt_noalloc(d_values, n, kind, d_result, stream, err, len(err))
     if rc != 0:
         raise DvgpuError(rc, err.value.decode(errors="replace"))
+
+
+class DvgpuServer:
+    """Serving engine for commitment updates (dvgpu_serve_*): resident
+    sessions, continuous batching across sessions; max_batch = 1 is the
+    per-call form.  submit() may be called from any thread."""
+
+    def __init__(self, hbm_budget_bytes: int, max_batch: int = 64):
+        self._L = lib()
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        rc = self._L.dvgpu_serve_create(hbm_budget_bytes, max_batch, ctypes.byref(h), err, len(err))
+        if rc != 0:
+            raise DvgpuError(rc, err.value.decode(errors="replace"))
+        self.handle = h
+
+    def _call(self, name, *args):
+        err = ctypes.create_string_buffer(512)
+        rc = getattr(self._L, name)(self.handle, *args, err, len(err))
+        if rc != 0:
+            raise DvgpuError(rc, err.value.decode(errors="replace"))
+
+    def open_session(self, srs_g1: bytes, values: bytes):
+        """Returns (session id, initial commitment: 64-byte affine G1)."""
+        n = len(values) // FR_BYTES
+        if len(srs_g1) != n * G1_BYTES:
+            raise ValueError("SRS and value vector lengths differ")
+        sid = ctypes.c_uint64()
+        out = ctypes.create_string_buffer(G1_BYTES)
+        self._call("dvgpu_serve_open_session", _ptr(srs_g1), _ptr(values), n, ctypes.byref(sid), out)
+        return sid.value, out.raw
+
+    def close_session(self, session: int):
+        self._call("dvgpu_serve_close_session", session)
+
+    def submit(self, session: int, indices, values: bytes) -> int:
+        idx = np.ascontiguousarray(np.asarray(indices, dtype=np.uint64))
+        t = ctypes.c_uint64()
+        self._call("dvgpu_serve_submit", session, idx.ctypes.data if idx.size else None, _ptr(values), len(idx),
+                   ctypes.byref(t))
+        return t.value
+
+    def wait(self, ticket: int):
+        """Returns (new commitment, ServeResult)."""
+        out = ctypes.create_string_buffer(G1_BYTES)
+        res = ServeResult()
+        self._call("dvgpu_serve_wait", ticket, out, ctypes.byref(res))
+        return out.raw, res
+
+    def set_max_batch(self, m: int):
+        self._L.dvgpu_serve_set_max_batch(self.handle, m)
+
+    def stats(self) -> ServeStats:
+        st = ServeStats()
+        self._L.dvgpu_serve_stats(self.handle, ctypes.byref(st))
+        return st
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._L.dvgpu_serve_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class DvgpuBackend:

@@ -24,6 +24,7 @@ namespace {
 template <class F>
 int window_for(const Backend& b, const std::vector<uint32_t>& offs) {
     if (b.force_c) return b.force_c;
+    if (offs.size() > 2) return 0;  // several sets: the batch cost model (tuned widths are per single MSM)
     uint32_t m = 0;
     for (size_t k = 0; k + 1 < offs.size(); ++k) m = std::max(m, offs[k + 1] - offs[k]);
     int cls = 0;

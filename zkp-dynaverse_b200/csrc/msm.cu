@@ -549,8 +549,22 @@ void gather_points(const Affine<F>* d_bases, uint64_t nbases, const uint64_t* d_
 }
 
 template <class F>
-MsmPlan msm_plan_batch(uint32_t count, uint32_t max_set, int force_c, const MsmPrecomp<F>* pre) {
+MsmPlan msm_plan_batch(uint32_t count, uint32_t max_set, uint64_t total, int force_c, const MsmPrecomp<F>* pre) {
     MsmPlan plan = msm_plan(max_set, force_c);
+    if (!force_c && !pre && count > 1) {
+        // every set carries windows * 2^(c-1) buckets: minimise
+        // windows * (10 total + 2 * 28 * count * 2^(c-1)) (the reduction
+        // runs at about half the accumulation's efficiency)
+        double best = 1e300;
+        for (int c = 4; c <= 20; ++c) {
+            const double W = (255 + c - 1) / c;
+            const double cost = W * (10.0 * (double)total + 56.0 * (double)count * (double)(1u << (c - 1)));
+            if (cost < best) { best = cost; plan.c = c; }
+        }
+        plan.windows = (255 + plan.c - 1) / plan.c;
+        plan.buckets = 1u << (plan.c - 1);
+        plan.seg_log = std::min(DV_SEG_LOG, plan.c - 1);
+    }
     // Bound the bucket table of a batch: count * windows * buckets <= 2^26
     // (8 GB of G1 XYZZ buckets); smaller windows trade buckets for windows.
     while (plan.c > 4 && (uint64_t)count * plan.windows * plan.buckets > (1ull << 26)) {
@@ -698,7 +712,7 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
         memset(host_out, 0, (size_t)count * out_bytes);
         return;
     }
-    const MsmPlan plan = msm_plan_batch<F>(count, max_set, force_c, pre);
+    const MsmPlan plan = msm_plan_batch<F>(count, max_set, n, force_c, pre);
     const int c = plan.c, W = plan.windows;
     const uint32_t Wr = pre ? 1u : (uint32_t)W;
     const uint32_t NW = count * Wr;
@@ -752,8 +766,8 @@ template void msm_run<Fq>(MsmWorkspace&, const Affine<Fq>*, const uint32_t*, con
                           cudaStream_t, uint8_t*, MsmStats*, const MsmPrecomp<Fq>*);
 template void msm_run<Fq2>(MsmWorkspace&, const Affine<Fq2>*, const uint32_t*, const uint32_t*, uint32_t, int,
                            cudaStream_t, uint8_t*, MsmStats*, const MsmPrecomp<Fq2>*);
-template MsmPlan msm_plan_batch<Fq>(uint32_t, uint32_t, int, const MsmPrecomp<Fq>*);
-template MsmPlan msm_plan_batch<Fq2>(uint32_t, uint32_t, int, const MsmPrecomp<Fq2>*);
+template MsmPlan msm_plan_batch<Fq>(uint32_t, uint32_t, uint64_t, int, const MsmPrecomp<Fq>*);
+template MsmPlan msm_plan_batch<Fq2>(uint32_t, uint32_t, uint64_t, int, const MsmPrecomp<Fq2>*);
 template void msm_enqueue<Fq>(MsmWorkspace&, const Affine<Fq>*, const uint32_t*, const SetMap&, uint32_t,
                               const MsmPlan&, const MsmPrecomp<Fq>*, uint32_t*, cudaStream_t);
 template void msm_enqueue<Fq2>(MsmWorkspace&, const Affine<Fq2>*, const uint32_t*, const SetMap&, uint32_t,

@@ -99,11 +99,12 @@ struct SetMap {
     int prefix;
 };
 
-// Window plan of a launch sequence: the cost model (or force_c), bounded so
-// that count * windows * buckets stays launchable; a precomputed table fixes
-// c and uses one bucket set per MSM.
+// Window plan of a launch sequence of count sets (largest max_set, total
+// points in all): force_c, else a cost model that charges every set its
+// windows * 2^(c-1) buckets, bounded so that count * windows * buckets stays
+// launchable; a precomputed table fixes c and uses one bucket set per MSM.
 template <class F>
-MsmPlan msm_plan_batch(uint32_t count, uint32_t max_set, int force_c, const MsmPrecomp<F>* pre);
+MsmPlan msm_plan_batch(uint32_t count, uint32_t max_set, uint64_t total, int force_c, const MsmPrecomp<F>* pre);
 
 // The device part of an MSM launch sequence: digit sort, accumulation,
 // merges and bucket reduction, all on `stream`, without host
