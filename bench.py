@@ -54,21 +54,23 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch", "g2check"])
+    ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch", "g2check",
+                                                         "serve"])
     ap.add_argument("--log-n", type=int, default=None)
     ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
     ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
     ap.add_argument("--alg", type=int, default=3, choices=[1, 2, 3], help="g2check: subgroup algorithm")
+    ap.add_argument("--requests", type=int, default=4000, help="serve: update requests per run")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
     if a.log_n is None:
         a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20, "batch": 18,
-                   "g2check": 16}[a.op]
+                   "g2check": 16, "serve": 16}[a.op]
     if a.steps is None:
         a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100,
-                   "batch": 20, "g2check": 50}[a.op]
+                   "batch": 20, "g2check": 50, "serve": 1}[a.op]
     return a
 
 
@@ -520,6 +522,158 @@ class G2CheckOp:
                                             f"scaled linearly; verdicts identical to the GPU's: {agree}")
 
 
+def serve_stream(sizes, count):
+    """The seeded update stream: (session, distinct indices) per request."""
+    import numpy as np
+    rng = np.random.default_rng(5000)
+    hot = [int(rng.integers(0, max(1, n - 64))) for n in sizes]
+    out = []
+    for t in range(count):
+        j = int(rng.integers(len(sizes)))
+        n = sizes[j]
+        k = min(n, int(2 ** rng.uniform(0, 10)))
+        if t % 2:
+            k = min(k, 64)
+            idx = hot[j] + rng.choice(64, size=k, replace=False)
+        else:
+            idx = rng.choice(n, size=k, replace=False)
+        out.append((j, idx.astype(np.uint64)))
+    return out
+
+
+class ServeOp:
+    """Serving: commitment updates from 64 resident sessions (n in
+    {256, 4096, 65536} in ratio 37:18:9), supports of floor(2^U) entries,
+    U ~ U[0, 10], capped at n, half in a 64-entry hotspot window per session,
+    half uniform; fresh uniform values.  The same request stream runs through
+    the served form (continuous batching, max_batch 64) and the per-call form
+    (max_batch 1): all requests at once (saturation throughput) and as a
+    Poisson stream at 80 % of the per-call capacity (latency)."""
+
+    SIZES = [256] * 37 + [4096] * 18 + [65536] * 9
+
+    def __init__(self, args):
+        self.requests = args.requests
+        self.metric = "served commitment updates/s (64 sessions, n 256/4096/65536)"
+        self.workload = ("commitment updates C' = C + sum (v'_i - v_i) G_i over 64 resident sessions, "
+                         f"{self.requests} requests, supports floor(2^U), U~U[0,10], half hotspot (64-entry window) "
+                         "half uniform, uniform Fr values")
+        self.profile = "serve"
+
+    def _inputs(self, torch, b, s):
+        self.sess = []
+        for j, n in enumerate(self.SIZES):
+            tau = torch.empty(32, dtype=torch.uint8, device="cuda")
+            b.random_fr_device(7000 + j, 1, tau.data_ptr(), s)
+            pw = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+            b.fr_powers_device(tau.data_ptr(), n, pw.data_ptr(), s)
+            pts = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
+            b.fixed_base_device(pw.data_ptr(), n, False, pts.data_ptr(), s)
+            vals = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+            b.random_fr_device(7100 + j, n, vals.data_ptr(), s)
+            torch.cuda.synchronize()
+            self.sess.append((pts.cpu().numpy().tobytes(), vals.cpu().numpy().tobytes()))
+        reqs, total = [], 0
+        for j, idx in serve_stream(self.SIZES, self.requests):
+            reqs.append((j, idx, total, len(idx)))
+            total += len(idx)
+        vals = torch.empty(total * 32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(7200, total, vals.data_ptr(), s)
+        torch.cuda.synchronize()
+        allv = vals.cpu().numpy().tobytes()
+        self.reqs = [(j, idx, allv[32 * o:32 * (o + k)]) for j, idx, o, k in reqs]
+        self.entries = total
+
+    def _run(self, srv, max_batch, arrivals):
+        """One pass of the request stream through a warm server: sessions
+        (re)opened from the initial vectors, then the stream submitted at its
+        arrival times (seconds from the start)."""
+        srv.set_max_batch(max_batch)
+        ids = [srv.open_session(p, v)[0] for p, v in self.sess]
+        before = srv.stats()
+        t0 = time.perf_counter()
+        tickets = []
+        for (j, idx, vals), at in zip(self.reqs, arrivals):
+            while time.perf_counter() - t0 < at:
+                pass
+            tickets.append(srv.submit(ids[j], idx, vals))
+        outs = [srv.wait(t) for t in tickets]
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        for sid in ids:
+            srv.close_session(sid)
+        lat = sorted((r.done_ns - r.submit_ns) / 1e6 for _, r in outs)
+        pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
+        return {"commitments": [c for c, _ in outs], "wall_s": wall, "per_s": len(outs) / wall,
+                "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1], "mean_ms": sum(lat) / len(lat),
+                "batches": st.batches - before.batches, "largest_batch": max(r.batch_requests for _, r in outs)}
+
+    def run_standalone(self, args, torch, dv, b, s, sampler, imad_peak_fn):
+        import numpy as np
+        self._inputs(torch, b, s)
+        zeros = [0.0] * self.requests
+        srv = dv.DvgpuServer(150 << 30, 64)
+        self._run(srv, 64, zeros)  # warm-up: workspaces reach their working size
+        self._run(srv, 1, zeros[:200])
+        sampler.start()
+        sat_served = self._run(srv, 64, zeros)
+        sat_plain = self._run(srv, 1, zeros)
+        rate = 0.8 * sat_plain["per_s"]
+        arrivals = np.cumsum(np.random.default_rng(5001).exponential(1.0 / rate, self.requests)).tolist()
+        poi_served = self._run(srv, 64, arrivals)
+        poi_plain = self._run(srv, 1, arrivals)
+        clocks = sampler.stop()
+        srv.close()
+        runs = (sat_served, sat_plain, poi_served, poi_plain)
+        exact = all(r["commitments"] == sat_served["commitments"] for r in runs)
+        # final commitment of every session = full recommitment of its final vector
+        vecs = [bytearray(v) for _, v in self.sess]
+        last = {}
+        for t, (j, idx, vals) in enumerate(self.reqs):
+            for q, i in enumerate(idx):
+                vecs[j][32 * int(i):32 * (int(i) + 1)] = vals[32 * q:32 * (q + 1)]
+            last[j] = sat_served["commitments"][t]
+        for j, c in last.items():
+            exact = exact and b.msm(self.sess[j][0], bytes(vecs[j])) == c
+        macs = sum(msm_fme(len(idx)) for _, idx, _ in self.reqs) * 136
+        ach = macs / sat_served["wall_s"] / 1e12
+        peak = imad_peak_fn() / 1e12
+        strip = lambda r: {k: v for k, v in r.items() if k != "commitments"}
+        line = {
+            "metric": self.metric, "value": sat_served["per_s"], "unit": "updates/s", "n_gpus": 1,
+            "steps": self.requests, "warmup": 1, "ms_per_step": 1e3 / sat_served["per_s"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Fq/Fr Montgomery, exact)",
+            "data": "synthetic",
+            "config": {"workload": self.workload, "op": "serve", "parallelism": "single GPU",
+                       "sessions": len(self.SIZES), "requests": self.requests, "entries": self.entries,
+                       "l2": "not flushed: a stream of small requests against resident sessions"},
+            "e2e": {"value": sat_served["per_s"], "unit": "updates/s",
+                    "h2d_bytes_per_step": 40 * self.entries / self.requests, "d2h_bytes_per_step": 64,
+                    "call": "dvgpu_serve_submit/wait from host memory (the serving API is host-to-host)"},
+            "serving": {"saturation": {"served": strip(sat_served), "per_call": strip(sat_plain),
+                                       "speedup": sat_served["per_s"] / sat_plain["per_s"]},
+                        "poisson": {"rate_per_s": rate, "served": strip(poi_served), "per_call": strip(poi_plain)},
+                        "bit_exact": exact,
+                        "note": "commitment updates only: the update proofs of the reference protocol are not "
+                                "built"},
+            "roofline": {"bound": "imad", "kernel": "all launches of the saturation run (sparse delta MSMs)",
+                         "achieved": ach, "peak": peak, "unit": "TMAC/s", "frac": ach / peak,
+                         "algorithmic_macs_per_launch": macs, "traffic": None},
+            "gpu_launches": None, "clocks": clocks,
+        }
+        if not args.no_cpu_baseline:
+            from oracle import oracle
+            threads = os.cpu_count() or 1
+            sample = self.reqs[:200]
+            t0 = time.perf_counter()
+            for j, idx, vals in sample:
+                oracle.sparse_msm_g1(self.sess[j][0], idx, vals, threads=threads)
+            cpu_s = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": len(sample) / cpu_s, "unit": "updates/s", "cores": threads,
+                                    "kind": "port", "sample": f"the first {len(sample)} requests' sparse MSMs"}
+        return line
+
+
 def batch_workload(log_bases):
     """The batching workload: 512 G1 MSMs of floor(2^U) points, U ~ U[8, 18],
     over prefixes of the SRS, and 256 forward NTTs of 2^floor(U) elements,
@@ -716,7 +870,7 @@ class BatchOp:
 def make_op(args):
     return {"msm": lambda: MsmOp(args), "msmres": lambda: ResidentMsmOp(args), "g2msm": lambda: MsmOp(args, g2=True),
             "ntt": lambda: NttOp(args), "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args),
-            "batch": lambda: BatchOp(args), "g2check": lambda: G2CheckOp(args)}[args.op]()
+            "batch": lambda: BatchOp(args), "g2check": lambda: G2CheckOp(args), "serve": lambda: ServeOp(args)}[args.op]()
 
 
 # ----------------------------------------------------------------- reference arm
@@ -751,6 +905,20 @@ def run_reference(args, rank, world):
         fn = lambda: oracle.sparse_msm_g1(bases, idx, vals, threads=threads)
         metric = f"sparse G1 MSM k={args.k} over 2^{args.log_n} bases us"
         sample = f"k={args.k} sparse MSMs"
+    elif op == "serve":
+        sizes = ServeOp.SIZES
+        stream = serve_stream(sizes, 400)
+        used = sorted(set(j for j, _ in stream))
+        bases = {j: oracle.fixed_base_g1(oracle.fr_powers(oracle.uniform_fr(7000 + j, 1), sizes[j]), threads=threads)
+                 for j in used}
+        vals = [oracle.uniform_fr(7300 + t, len(idx)) for t, (_, idx) in enumerate(stream)]
+
+        def fn():
+            for (j, idx), v in zip(stream, vals):
+                oracle.sparse_msm_g1(bases[j], idx, v, threads=threads)
+
+        metric = ServeOp(args).metric
+        sample = "passes over the first 400 requests of the update stream (sparse delta MSMs)"
     elif op == "batch":
         sizes, logs = batch_workload(BatchOp.LOG_BASES)
         nb = 1 << BatchOp.LOG_BASES
@@ -783,12 +951,17 @@ def run_reference(args, rank, world):
     if op == "batch":
         value = sum(e[0] for e in est[1:]) / len(est[1:])
         sample = f"batch estimates, each from {est[-1][1]}"
+    higher = False
+    ms_step = value
+    if op == "serve":
+        value = len(stream) / (value / 1e3)  # updates per second
+        higher = True
     if op == "sparse":
         value *= 1e3  # us
-    unit = "us" if op == "sparse" else "ms"
+    unit = "us" if op == "sparse" else ("updates/s" if op == "serve" else "ms")
     line = {
         "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": value / (1e3 if op == "sparse" else 1), "higher_is_better": False,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": higher,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 limbs (Fq/Fr, exact)", "data": "synthetic",
         "config": {"workload": metric, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
@@ -829,6 +1002,17 @@ def main():
     s = stream.cuda_stream
     op = make_op(args)
     op._b = b
+    if hasattr(op, "run_standalone"):
+        try:
+            bus = torch.cuda.get_device_properties(dev).pci_bus_id
+        except AttributeError:
+            bus = None
+        sampler = ClockSampler(bus if isinstance(bus, str) else None)
+        line = op.run_standalone(args, torch, dv, b, s, sampler, b.probe_imad_rate)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        b.close()
+        return
     op.setup(torch, b, s, rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     result = None

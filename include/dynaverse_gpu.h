@@ -306,9 +306,10 @@ int dvgpu_batch_plan_destroy(void* backend, uint64_t plan, char* error, size_t e
  * call at a time per session (crates/protocol/src/session.rs:51-142).
  *
  * A server keeps sessions resident -- SRS bases (G1 wire form in), the
- * committed vector of canonical Fr values, and its commitment
- * C = sum v_i G_i -- and admits a session only while the resident bytes
- * (n x 96 + 64 per session) stay within hbm_budget_bytes (-1 otherwise).
+ * committed vector of canonical Fr values, its commitment C = sum v_i G_i
+ * and a table of 32 precomputed window multiples per base -- and admits a
+ * session only while the resident bytes (n x (64 x 33 + 32) + 64 per
+ * session) stay within hbm_budget_bytes (-1 otherwise).
  * dvgpu_serve_submit queues a commitment update of a session: the entries
  * at `indices` (distinct, < n) take the new `values`; the result is the new
  * commitment C' = C + sum (v'_i - v_i) G_i.  One engine thread merges the

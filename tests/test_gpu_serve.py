@@ -82,7 +82,7 @@ def test_served_commitments_match_oracle_and_per_call(oracle, dv):
 def test_serve_admission_and_invalid_updates(oracle, dv):
     pts, _ = oracle.srs_g1(620, 512)
     vals = oracle.uniform_fr(621, 512)
-    with dv.DvgpuServer(512 * 96 + 64, 8) as srv:  # room for exactly one session of 512
+    with dv.DvgpuServer(512 * (64 * 33 + 32) + 64, 8) as srv:  # room for exactly one session of 512
         sid, c0 = srv.open_session(pts, vals)
         with pytest.raises(dv.DvgpuError) as e:
             srv.open_session(pts, vals)

@@ -30,14 +30,18 @@ inline void launched() {
 #define DV_CUDA(call) ::dv::cuda_check((call), #call)
 #define DV_LAUNCH() ::dv::launched()
 
-// Grow-only device buffer.  Contents are scratch between calls.
+// Grow-only device buffer.  Contents are scratch between calls.  A buffer
+// that has to grow again takes 1.5x headroom, so a stream of slowly
+// growing requests does not reallocate (and synchronise) every time.
 struct DevBuf {
     void* ptr = nullptr;
     size_t cap = 0;
     void* get(size_t bytes) {
         if (bytes <= cap && ptr) return ptr;
+        const size_t regrow = cap ? cap + cap / 2 : 0;
         release();
         size_t want = bytes < 256 ? 256 : bytes;
+        if (regrow > want) want = regrow;
         DV_CUDA(cudaMalloc(&ptr, want));
         cap = want;
         return ptr;

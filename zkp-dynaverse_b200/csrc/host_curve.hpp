@@ -198,4 +198,26 @@ inline void xyzz_to_affine_bytes(const XYZZ<F>& p, uint8_t* out) {
     to_canonical(y, out + sizeof(F));
 }
 
+// Canonical affine bytes of n points with one inversion (Montgomery's
+// simultaneous-inversion trick over the non-infinite points).
+template <class F>
+inline void xyzz_batch_to_affine_bytes(const XYZZ<F>* p, size_t n, uint8_t* out) {
+    F* pre = new F[n + 1];
+    pre[0] = one();
+    for (size_t i = 0; i < n; ++i) pre[i + 1] = is_zero(p[i].zz) ? pre[i] : mul(pre[i], mul(p[i].zz, p[i].zzz));
+    F acc = inv(pre[n]);  // 1 / prod (zz zzz)
+    for (size_t i = n; i-- > 0;) {
+        uint8_t* o = out + 2 * sizeof(F) * i;
+        if (is_zero(p[i].zz)) {
+            memset(o, 0, 2 * sizeof(F));
+            continue;
+        }
+        const F d = mul(acc, pre[i]);  // 1 / (zz zzz) of point i
+        acc = mul(acc, mul(p[i].zz, p[i].zzz));
+        to_canonical(mul(p[i].x, mul(d, p[i].zzz)), o);
+        to_canonical(mul(p[i].y, mul(d, p[i].zz)), o + sizeof(F));
+    }
+    delete[] pre;
+}
+
 }  // namespace dvh

@@ -16,6 +16,11 @@
 // batch is on the GPU form the next batch (continuous batching).  The same
 // engine with batches of one request is the per-call form.
 //
+// Each session also keeps a table of precomputed window multiples of its
+// bases (c = 8, 32 windows: 2 KB per base), so a request's MSM adds every
+// window into one set of 128 buckets and needs no window combination; the
+// batch's sets are finished (normalised) on the device.
+//
 // Within a batch a session has at most one request (later requests of a
 // session wait for the next batch), so each request's deltas are taken
 // against the vector its predecessors left and every result equals the one
@@ -72,22 +77,28 @@ dvh::XYZZ<dvh::Fq> xyzz_of(const uint8_t* p) {
     return {dvh::from_canonical(x), dvh::from_canonical(y), dvh::one(), dvh::one()};
 }
 
-// One thread per update entry: find the entry's request, gather its base
-// from the session's resident bases, replace the resident value by the new
-// one and emit the delta new - old (mod r) as the MSM scalar.
+constexpr int SERVE_C = 8;
+constexpr int SERVE_W = (255 + SERVE_C - 1) / SERVE_C;  // 32 windows
+
+// One thread per (update entry, window): find the entry's request, gather
+// the window multiple 2^(c w) G_i from the session's table; the window-0
+// thread also replaces the resident value by the new one and emits the
+// delta new - old (mod r) as the MSM scalar.
 __global__ void k_serve_prepare(uint32_t total, const uint32_t* __restrict__ req_off, uint32_t count,
-                                const G1A* const* __restrict__ srs, uint8_t* const* __restrict__ values,
+                                const G1A* const* __restrict__ tables, uint8_t* const* __restrict__ values,
                                 const uint32_t* __restrict__ idx, const uint8_t* __restrict__ new_vals,
                                 G1A* __restrict__ gathered, uint8_t* __restrict__ deltas) {
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= total) return;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)total * SERVE_W) return;
+    const uint32_t e = (uint32_t)(t / SERVE_W), w = (uint32_t)(t % SERVE_W);
     uint32_t lo = 0, hi = count;  // largest r with req_off[r] <= e
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
         if (req_off[mid] <= e) lo = mid; else hi = mid;
     }
     const uint32_t i = idx[e];
-    gathered[e] = srs[lo][i];
+    gathered[t] = tables[lo][(uint64_t)i * SERVE_W + w];
+    if (w) return;
     uint8_t* slot = values[lo] + 32ull * i;
     Fr oldv, newv;
     load_words(slot, oldv.v);
@@ -99,7 +110,7 @@ __global__ void k_serve_prepare(uint32_t total, const uint32_t* __restrict__ req
 
 struct Session {
     uint64_t id = 0, n = 0, footprint = 0;
-    DevBuf srs, values;
+    DevBuf srs, table, values;
     uint8_t commitment[64] = {};
 };
 
@@ -136,7 +147,7 @@ public:
     uint64_t open_session(const uint8_t* srs_wire, const uint8_t* values, uint64_t n, uint8_t* commitment) {
         uint64_t id = 0;
         run([&] {
-            const uint64_t footprint = n * (sizeof(G1A) + 32) + 64;
+            const uint64_t footprint = n * (sizeof(G1A) * (1 + SERVE_W) + 32) + 64;
             if (resident_ + footprint > budget_)
                 throw InvalidArgument("session does not fit the HBM budget (" + std::to_string(resident_) + " + " +
                                       std::to_string(footprint) + " > " + std::to_string(budget_) + " bytes)");
@@ -154,6 +165,7 @@ public:
             DV_CUDA(cudaMemcpyAsync(&h_bad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
             DV_CUDA(cudaStreamSynchronize(stream_));
             if (h_bad != 0xffffffffu) throw InvalidArgument("invalid SRS point at index " + std::to_string(h_bad));
+            msm_precompute<Fq>(s->srs.view<G1A>(), n, SERVE_C, SERVE_W, s->table.as<G1A>(n * SERVE_W), stream_);
             const uint32_t offs[2] = {0u, (uint32_t)n};
             msm_run<Fq>(ws_, s->srs.view<G1A>(), s->values.view<uint32_t>(), offs, 1, 0, stream_, s->commitment,
                         nullptr);
@@ -289,10 +301,17 @@ private:
             lk.unlock();
             int status = 0;
             std::string error;
+            affine_.assign(64 * batch.size(), 0);
             const uint64_t t0 = now_ns();
-            std::vector<uint8_t> deltas_out(batch.size() * 64);
+            dvh::XYZZ<dvh::Fq>* deltas_out = hwin_.as<dvh::XYZZ<dvh::Fq>>(batch.size());
             try {
-                process(batch, sess, deltas_out.data());
+                static_assert(sizeof(XYZZ<Fq>) == sizeof(dvh::XYZZ<dvh::Fq>), "host/device XYZZ layout");
+                process(batch, sess, reinterpret_cast<uint8_t*>(deltas_out));
+                // C' = C + delta C, then affine for the whole batch at once
+                std::vector<dvh::XYZZ<dvh::Fq>> sums(batch.size());
+                for (size_t r = 0; r < batch.size(); ++r)
+                    sums[r] = dvh::xyzz_add(xyzz_of(sess[r]->commitment), deltas_out[r]);
+                dvh::xyzz_batch_to_affine_bytes(sums.data(), sums.size(), affine_.data());
             } catch (const InvalidArgument& e) {
                 status = -1;
                 error = e.what();
@@ -307,9 +326,7 @@ private:
                 o.status = status;
                 o.error = error;
                 if (!status) {
-                    // C' = C + delta C (host normalisation of one point)
-                    const auto sum = dvh::xyzz_add(xyzz_of(sess[r]->commitment), xyzz_of(&deltas_out[64 * r]));
-                    dvh::xyzz_to_affine_bytes(sum, sess[r]->commitment);
+                    memcpy(sess[r]->commitment, &affine_[64 * r], 64);
                     memcpy(o.commitment, sess[r]->commitment, 64);
                 }
                 o.res.submit_ns = batch[r].submit_ns;
@@ -350,7 +367,7 @@ private:
         for (uint32_t r = 0; r < count; ++r) {
             memcpy(h_idx + offs[r], batch[r].idx.data(), 4ull * batch[r].idx.size());
             memcpy(h_val + 32ull * offs[r], batch[r].vals.data(), batch[r].vals.size());
-            h_srs[r] = sess[r]->srs.view<G1A>();
+            h_srs[r] = sess[r]->table.view<G1A>();
             h_vals[r] = sess[r]->values.view<uint8_t>();
         }
         memcpy(h_off, offs.data(), 4ull * (count + 1));
@@ -361,13 +378,24 @@ private:
         const uint32_t* d_off = reinterpret_cast<const uint32_t*>(d + off_req);
         const G1A* const* d_srs = reinterpret_cast<const G1A* const*>(d + off_ptr);
         uint8_t* const* d_vals = reinterpret_cast<uint8_t* const*>(d + off_ptr + sizeof(void*) * count);
-        G1A* gathered = gathered_.as<G1A>(total);
+        G1A* gathered = gathered_.as<G1A>((uint64_t)total * SERVE_W);
         uint8_t* deltas = deltas_.as<uint8_t>(32ull * total);
-        k_serve_prepare<<<(total + 127) / 128, 128, 0, stream_>>>(total, d_off, count, d_srs, d_vals, d_idx, d_val,
-                                                                 gathered, deltas);
+        const uint64_t threads = (uint64_t)total * SERVE_W;
+        k_serve_prepare<<<(unsigned)((threads + 127) / 128), 128, 0, stream_>>>(total, d_off, count, d_srs, d_vals,
+                                                                              d_idx, d_val, gathered, deltas);
         DV_LAUNCH();
-        msm_run<Fq>(ws_, gathered, reinterpret_cast<const uint32_t*>(deltas), offs.data(), count, 0, stream_,
-                    deltas_out, nullptr);
+        // one bucket set per request over the gathered window multiples
+        const MsmPrecomp<Fq> pre{gathered, SERVE_C, SERVE_W};
+        const MsmPlan plan = msm_plan_batch<Fq>(count, 0, total, 0, &pre);
+        uint32_t* bad = err_.as<uint32_t>(1);
+        DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), stream_));
+        msm_enqueue<Fq>(ws_, nullptr, reinterpret_cast<const uint32_t*>(deltas), SetMap{d_off, nullptr, count, 0},
+                        total, plan, &pre, bad, stream_);
+        // the per-request sums go to the host; the engine adds them to the
+        // commitments and normalises the batch with one inversion
+        DV_CUDA(cudaMemcpyAsync(deltas_out, ws_.windows.view<XYZZ<Fq>>(), sizeof(XYZZ<Fq>) * count,
+                                cudaMemcpyDeviceToHost, stream_));
+        DV_CUDA(cudaStreamSynchronize(stream_));
     }
 
     int device_ = 0;
@@ -376,7 +404,8 @@ private:
     uint32_t max_batch_;
     MsmWorkspace ws_;
     DevBuf stage_, err_, dstage_, gathered_, deltas_;
-    PinnedBuf pinned_;
+    PinnedBuf pinned_, hwin_;
+    std::vector<uint8_t> affine_;
 
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;
