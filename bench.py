@@ -55,22 +55,24 @@ def parse():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch", "g2check",
-                                                         "serve"])
+                                                         "serve", "ecntt"])
     ap.add_argument("--log-n", type=int, default=None)
     ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
     ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
     ap.add_argument("--alg", type=int, default=3, choices=[1, 2, 3], help="g2check: subgroup algorithm")
     ap.add_argument("--requests", type=int, default=4000, help="serve: update requests per run")
+    ap.add_argument("--rows", type=int, default=16, help="ecntt: rows per transform call")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
     if a.log_n is None:
         a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20, "batch": 18,
-                   "g2check": 16, "serve": 16}[a.op]
+                   "g2check": 16, "serve": 16, "ecntt": 12}[a.op]
     if a.steps is None:
         a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100,
-                   "batch": 20, "g2check": 50, "serve": 1}[a.op]
+                   "batch": 20, "g2check": 50, "serve": 1,
+                   "ecntt": 10}[a.op]
     return a
 
 
@@ -522,6 +524,79 @@ class G2CheckOp:
                                             f"scaled linearly; verdicts identical to the GPU's: {agree}")
 
 
+def ecntt_fme(logn, rows):
+    """Fq multiplications of a G1 transform: per stage, every butterfly costs
+    two XYZZ additions (2 x 14) and every butterfly with a twiddle other than
+    1 a double-and-add scalar multiplication (254 doublings x 9 + 127
+    additions x 14)."""
+    n = 1 << logn
+    smul = 254 * 9 + 127 * 14
+    nontrivial = sum(rows * (n // 2 - (1 << s)) for s in range(logn))
+    return rows * (n // 2) * logn * 28 + nontrivial * smul
+
+
+class EcNttOp:
+    """G1 transform (EC-NTT) of rows of 2^12 points, the four-step packet
+    length of the reference's rebuild (MAX_TRANSFORM_PACKET_LEN 4096)."""
+
+    def __init__(self, args):
+        self.logn = args.log_n
+        self.rows = args.rows
+        self.n = (1 << self.logn) * self.rows
+        self.metric = f"G1 EC-NTT {self.rows} x 2^{self.logn} ms"
+        self.workload = (f"G1 transform (arkworks radix-2 FFT over G1, rows normalised to affine) of {self.rows} "
+                         f"rows of 2^{self.logn} points [s_i]G1, forward")
+        self.profile = f"g1_ntt_{self.rows}x2p{self.logn}"
+
+    def setup(self, torch, b, s, rank):
+        sc = torch.empty(self.n * 32, dtype=torch.uint8, device="cuda")
+        b.random_fr_device(8100 + rank, self.n, sc.data_ptr(), s)
+        self.pts = torch.empty(self.n * 64, dtype=torch.uint8, device="cuda")
+        b.fixed_base_device(sc.data_ptr(), self.n, False, self.pts.data_ptr(), s)
+        self.out = torch.empty_like(self.pts)
+        torch.cuda.synchronize()
+        self.tune_log = None
+        self.config = {"rows": self.rows, "row_len": 1 << self.logn, "points": self.n}
+
+    def step(self, b, s):
+        b.g1_ntt_rows_device(self.pts.data_ptr(), 1 << self.logn, self.rows, False, self.out.data_ptr(), s)
+        return None
+
+    def host_inputs(self, torch):
+        self.h_pts = torch.empty(self.n * 64, dtype=torch.uint8, pin_memory=True)
+        self.h_pts.copy_(self.pts)
+        self.h_out = torch.empty(self.n * 64, dtype=torch.uint8, pin_memory=True)
+
+    def e2e_step(self, dv, b):
+        err = ctypes.create_string_buffer(256)
+        dst = ctypes.cast(ctypes.c_void_p(self.h_out.data_ptr()), ctypes.c_char_p)
+        rc = dv.lib().dvgpu_bn254_g1_ntt_rows(b.handle, self.h_pts.data_ptr(), 1 << self.logn, self.rows, 0, dst,
+                                               err, 256)
+        if rc != 0:
+            raise RuntimeError(err.value)
+        return None
+
+    def e2e_bytes(self):
+        return self.n * 64, self.n * 64
+
+    def roofline(self, tl, imad_peak, step_ms):
+        macs = ecntt_fme(self.logn, self.rows) * 136
+        ach = macs / (step_ms * 1e-3) / 1e12
+        return ({"bound": "imad", "kernel": "k_ec_stage (all stages) + k_ec_store", "achieved": ach,
+                 "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
+                 "algorithmic_macs_per_launch": macs, "launch_ms": step_ms}, None)
+
+    def cpu(self, oracle, threads):
+        rows = min(self.rows, threads)
+        pts = self.h_pts.numpy().tobytes()[:64 * rows << self.logn]
+        t0 = time.perf_counter()
+        out = oracle.g1_fft(pts, 1 << self.logn, False, threads=threads)
+        ms = (time.perf_counter() - t0) * 1e3
+        agree = out == self.h_out.numpy().tobytes()[:len(out)] if hasattr(self, "h_out") else None
+        return None, ms * self.rows / rows, (f"{rows} rows on {rows} threads, scaled to {self.rows} rows; "
+                                              f"identical to the GPU's: {agree}")
+
+
 def serve_stream(sizes, count):
     """The seeded update stream: (session, distinct indices) per request."""
     import numpy as np
@@ -870,7 +945,8 @@ class BatchOp:
 def make_op(args):
     return {"msm": lambda: MsmOp(args), "msmres": lambda: ResidentMsmOp(args), "g2msm": lambda: MsmOp(args, g2=True),
             "ntt": lambda: NttOp(args), "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args),
-            "batch": lambda: BatchOp(args), "g2check": lambda: G2CheckOp(args), "serve": lambda: ServeOp(args)}[args.op]()
+            "batch": lambda: BatchOp(args), "g2check": lambda: G2CheckOp(args), "serve": lambda: ServeOp(args),
+            "ecntt": lambda: EcNttOp(args)}[args.op]()
 
 
 # ----------------------------------------------------------------- reference arm
@@ -905,6 +981,13 @@ def run_reference(args, rank, world):
         fn = lambda: oracle.sparse_msm_g1(bases, idx, vals, threads=threads)
         metric = f"sparse G1 MSM k={args.k} over 2^{args.log_n} bases us"
         sample = f"k={args.k} sparse MSMs"
+    elif op == "ecntt":
+        rows = min(args.rows, threads)
+        pts = oracle.fixed_base_g1(oracle.uniform_fr(8100, rows << args.log_n), threads=threads)
+        fn = lambda: oracle.g1_fft(pts, 1 << args.log_n, False, threads=threads)
+        metric = EcNttOp(args).metric
+        sample = f"{rows}-row G1 transforms of 2^{args.log_n} points on {rows} threads, scaled to {args.rows} rows"
+        ecntt_scale = args.rows / rows
     elif op == "serve":
         sizes = ServeOp.SIZES
         stream = serve_stream(sizes, 400)
@@ -951,6 +1034,8 @@ def run_reference(args, rank, world):
     if op == "batch":
         value = sum(e[0] for e in est[1:]) / len(est[1:])
         sample = f"batch estimates, each from {est[-1][1]}"
+    if op == "ecntt":
+        value *= ecntt_scale
     higher = False
     ms_step = value
     if op == "serve":

@@ -250,6 +250,18 @@ int dvgpu_fr_powers_device(void* backend, const uint8_t* d_tau, size_t n, uint8_
 int dvgpu_g2_random_twist_device(void* backend, uint64_t seed, size_t n, uint8_t* d_out, void* stream, char* error,
                                  size_t error_capacity);
 
+/* G1 transform (EC-NTT) of `rows` rows of row_len = 2^k points (wire form,
+ * 64 bytes each, k <= 20, at most 2^24 points in all): per row
+ * out_i = sum_j w^(ij) P_j in natural order, w the arkworks root of order
+ * row_len; inverse = 1 uses w^-1 and scales by 1/row_len; results are
+ * canonical affine (RebuildBackend::transform_rows with kind G1,
+ * crates/protocol/src/incremental_rebuild/operators.rs:413-440; ICICLE's
+ * dvgpu_ecntt_rows, native/src/icicle_ntt.cu:90-95).  Invalid points: -1. */
+int dvgpu_bn254_g1_ntt_rows(void* backend, const uint8_t* points, size_t row_len, size_t rows, int inverse,
+                            uint8_t* results, char* error, size_t error_capacity);
+int dvgpu_bn254_g1_ntt_rows_device(void* backend, const uint8_t* d_points, size_t row_len, size_t rows, int inverse,
+                                   uint8_t* d_results, void* stream, char* error, size_t error_capacity);
+
 /* ---------------------------------------------------------------- batching
  * No counterpart in the reference ABI (its batch path is
  * dvgpu_bn254_msm_batch with next-pow2 padding, icicle_msm.cu:810-880, and

@@ -790,6 +790,40 @@ static Fe root_of_unity(size_t n) {
     return w;
 }
 
+// G1 FFT of one row (arkworks Radix2EvaluationDomain::fft_in_place over
+// G1Projective, as called by RebuildBackend::transform_rows,
+// crates/protocol/src/incremental_rebuild/operators.rs:413-440): the same
+// radix-2 butterflies as ntt_inplace with the twiddle acting on the point.
+static void g1_fft_inplace(std::vector<Jac<OpsFq>>& a, const Fe& omega) {
+    size_t n = a.size();
+    int logn = 0;
+    while (((size_t)1 << logn) < n) ++logn;
+    for (size_t i = 0; i < n; ++i) {
+        size_t j = 0;
+        for (int b = 0; b < logn; ++b) j |= ((i >> b) & 1) << (logn - 1 - b);
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (size_t len = 2; len <= n; len <<= 1) {
+        Fe wlen = omega;
+        for (size_t k = len; k < n; k <<= 1) fmul(FR, wlen, wlen, wlen);
+        std::vector<Fe> tw(len / 2);
+        tw[0] = FR.one;
+        for (size_t j = 1; j < len / 2; ++j) fmul(FR, tw[j], tw[j - 1], wlen);
+        for (size_t i = 0; i < n; i += len) {
+            for (size_t j = 0; j < len / 2; ++j) {
+                uint64_t k[4];
+                from_mont(FR, k, tw[j]);
+                const Jac<OpsFq> u = a[i + j];
+                const Jac<OpsFq> v = mul_bits_jac(a[i + j + len / 2], k, 256);
+                jac_add(a[i + j], u, v);
+                Jac<OpsFq> nv;
+                jac_neg(nv, v);
+                jac_add(a[i + j + len / 2], u, nv);
+            }
+        }
+    }
+}
+
 struct Init { Init() { init_psi(); } } init_once;
 
 // ------------------------------------------------------------------ ChaCha20
@@ -865,6 +899,40 @@ int oracle_sparse_msm_g1(const uint8_t* bases, size_t nbases, const uint64_t* in
 }
 
 // kind: 0 forward, 1 inverse, 2 coset forward, 3 coset inverse.
+// G1 transform of `rows` rows of n points each (wire form in and out;
+// inverse scales by 1/n; each row normalised to affine).
+int oracle_g1_fft(const uint8_t* points, size_t n, size_t rows, int inverse, uint8_t* out, int threads) {
+    if (n == 0 || (n & (n - 1)) || n > ((size_t)1 << 28)) return -1;
+    for (size_t i = 0; i < n * rows; ++i) {
+        Aff<OpsFq> p;
+        if (!g1_read(points + 64 * i, p)) return -1;
+    }
+    Fe w = root_of_unity(n);
+    if (inverse) finv(FR, w, w);
+    uint64_t nc[4] = {(uint64_t)n, 0, 0, 0}, ninv_c[4];
+    Fe nm, ni;
+    to_mont(FR, nm, nc);
+    finv(FR, ni, nm);
+    from_mont(FR, ninv_c, ni);
+    parallel_for(rows, num_threads(threads), [&](size_t lo, size_t hi) {
+      for (size_t r = lo; r < hi; ++r) {
+        std::vector<Jac<OpsFq>> a(n);
+        for (size_t i = 0; i < n; ++i) {
+            Aff<OpsFq> p;
+            g1_read(points + 64 * (r * n + i), p);
+            a[i] = p.inf ? jac_zero<OpsFq>() : Jac<OpsFq>{p.x, p.y, OpsFq::one()};
+        }
+        if (n > 1) g1_fft_inplace(a, w);
+        if (inverse)
+            for (auto& v : a) v = mul_bits_jac(v, ninv_c, 256);
+        std::vector<Aff<OpsFq>> aff(n);
+        batch_to_aff(a.data(), aff.data(), n);
+        for (size_t i = 0; i < n; ++i) g1_write(out + 64 * (r * n + i), aff[i]);
+      }
+    });
+    return 0;
+}
+
 int oracle_ntt(uint8_t* values, size_t n, int kind) {
     if (n == 0 || (n & (n - 1)) || n > ((size_t)1 << 28) || kind < 0 || kind > 3) return -1;
     std::vector<Fe> a(n);

@@ -35,6 +35,7 @@ def lib():
         L.oracle_msm_g2.argtypes = [u8p, u8p, sz, u8p, ctypes.c_int, ctypes.c_int]
         L.oracle_sparse_msm_g1.argtypes = [u8p, sz, ctypes.c_void_p, u8p, sz, u8p, ctypes.c_int]
         L.oracle_ntt.argtypes = [u8p, sz, ctypes.c_int]
+        L.oracle_g1_fft.argtypes = [u8p, sz, sz, ctypes.c_int, u8p, ctypes.c_int]
         L.oracle_fixed_base_g1.argtypes = [u8p, sz, u8p, ctypes.c_int]
         L.oracle_fixed_base_g2.argtypes = [u8p, sz, u8p, ctypes.c_int]
         L.oracle_g2_check.argtypes = [u8p, sz, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int]
@@ -83,6 +84,15 @@ def sparse_msm_g1(bases: bytes, indices, values: bytes, threads=0) -> bytes:
 
 
 NTT_KINDS = {"forward": 0, "inverse": 1, "coset_forward": 2, "coset_inverse": 3}
+
+
+def g1_fft(points: bytes, n: int, inverse=False, threads=0) -> bytes:
+    """G1 transform of len(points) / (64 n) rows of n points (arkworks
+    Radix2EvaluationDomain fft / ifft over G1, rows normalised to affine)."""
+    rows = len(points) // (64 * n)
+    out = _buf(64 * n * rows)
+    assert lib().oracle_g1_fft(points, n, rows, int(inverse), out, threads) == 0
+    return out.raw
 
 
 def ntt(values: bytes, kind="forward") -> bytes:

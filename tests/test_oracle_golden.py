@@ -123,3 +123,21 @@ def test_codec_rejections(golden, oracle):
             oracle.ntt(H(bad), "forward")
     for good in golden["codec"]["fr_accept"]:
         assert oracle.ntt(H(good), "forward") == H(good)
+
+
+def test_oracle_g1_fft_is_the_dft(oracle):
+    """The oracle's G1 transform (arkworks radix-2 FFT over G1, operators.rs:
+    413-440) equals the DFT definition out_i = sum_j w^(ij) P_j, one MSM per
+    output, with w the pinned arkworks root; inverse scales by 1/n."""
+    R = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+    root28 = 0x2A3C09F0A58A7E8500E0A7EB8EF62ABC402D111E41112ED49BD61B6E725B19F0
+    for n in (1, 2, 4, 8):
+        pts, _ = oracle.srs_g1(33 + n, n)
+        w = pow(root28, 2 ** (28 - (n.bit_length() - 1)), R)
+        for inverse in (False, True):
+            got = oracle.g1_fft(pts, n, inverse)
+            ww = pow(w, R - 2, R) if inverse else w
+            scale = pow(n, R - 2, R) if inverse else 1
+            for i in range(n):
+                sc = b"".join((pow(ww, i * j, R) * scale % R).to_bytes(32, "little") for j in range(n))
+                assert got[64 * i:64 * (i + 1)] == oracle.msm_g1(pts, sc), (n, inverse, i)

@@ -137,6 +137,8 @@ SIGNATURES = [
     ("dvgpu_random_fr_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
     ("dvgpu_fr_powers_device", ctypes.c_int, [_P, _P, _SZ, _P, _P] + _E),
     ("dvgpu_g2_random_twist_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
+    ("dvgpu_bn254_g1_ntt_rows", ctypes.c_int, [_P, _P, _SZ, _SZ, ctypes.c_int, _B] + _E),
+    ("dvgpu_bn254_g1_ntt_rows_device", ctypes.c_int, [_P, _P, _SZ, _SZ, ctypes.c_int, _P, _P] + _E),
     ("dvgpu_bn254_ntt_batch", ctypes.c_int, [_P, _P, _P, _P, _SZ, _B] + _E),
     ("dvgpu_bn254_ntt_batch_device", ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P] + _E),
     ("dvgpu_batch_plan_create", ctypes.c_int,
@@ -587,6 +589,20 @@ class DvgpuBackend:
 
     def fr_powers_device(self, d_tau: int, n: int, d_out: int, stream=None):
         self._call("dvgpu_fr_powers_device", d_tau, n, d_out, stream)
+
+    # ------------------------------------------------------------------ G1 transform
+    def g1_ntt_rows(self, points: bytes, row_len: int, inverse=False) -> bytes:
+        """Rows of row_len G1 points through the Fr-domain FFT (EC-NTT),
+        affine results (RebuildBackend::transform_rows, kind G1)."""
+        if row_len <= 0 or len(points) % (G1_BYTES * row_len):
+            raise ValueError("points must hold whole rows")
+        rows = len(points) // (G1_BYTES * row_len)
+        out = ctypes.create_string_buffer(max(1, len(points)))
+        self._call("dvgpu_bn254_g1_ntt_rows", _ptr(points), row_len, rows, int(inverse), out)
+        return out.raw[:len(points)]
+
+    def g1_ntt_rows_device(self, d_points: int, row_len: int, rows: int, inverse: bool, d_out: int, stream=None):
+        self._call("dvgpu_bn254_g1_ntt_rows_device", d_points, row_len, rows, int(inverse), d_out, stream)
 
     # ------------------------------------------------------------------ batching
     def ntt_batch(self, values: bytes, log_sizes, kinds=None) -> bytes:

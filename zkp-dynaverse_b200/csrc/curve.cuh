@@ -121,6 +121,45 @@ struct XYZZ {
         return {x3, y3, F::mul(F::mul(p.zz, q.zz), pp), F::mul(F::mul(p.zzz, q.zzz), ppp)};
     }
 
+    // Over Fq: doubling and full addition with their products issued as
+    // independent pairs (F::mul2), for the long dependent chains of a scalar
+    // multiplication run by few threads (the G1 transform's butterflies).
+    DV_INL static XYZZ dbl_paired(const XYZZ& p) {
+        if (p.is_inf()) return p;
+        const F u = F::dbl(p.y);
+        const auto vx = F::mul2(u, u, p.x, p.x);      // V = U^2, X^2
+        const F v = vx.r0;
+        const auto ws = F::mul2(u, v, p.x, v);         // W = U V, S = X V
+        const F w = ws.r0, s = ws.r1;
+        const F m = F::add(F::dbl(vx.r1), vx.r1);
+        const auto mz = F::mul2(m, m, v, p.zz);        // M^2, ZZ3
+        const F x3 = F::sub(mz.r0, F::dbl(s));
+        const auto wy = F::mul2(w, p.y, w, p.zzz);     // W Y, ZZZ3
+        const F y3 = F::sub(F::mul(m, F::sub(s, x3)), wy.r0);
+        return {x3, y3, mz.r1, wy.r1};
+    }
+    DV_INL static XYZZ add_paired(const XYZZ& p, const XYZZ& q) {
+        if (p.is_inf()) return q;
+        if (q.is_inf()) return p;
+        const auto u = F::mul2(p.x, q.zz, q.x, p.zz);  // U1, U2
+        const auto s = F::mul2(p.y, q.zzz, q.y, p.zzz);  // S1, S2
+        const F pp_ = F::sub(u.r1, u.r0);
+        const F r = F::sub(s.r1, s.r0);
+        if (pp_.is_zero()) {
+            if (r.is_zero()) return dbl_paired(p);
+            return inf();
+        }
+        const auto sq = F::mul2(pp_, pp_, r, r);        // PP, R^2
+        const F pp = sq.r0;
+        const auto pq = F::mul2(pp_, pp, u.r0, pp);     // PPP, Q
+        const F ppp = pq.r0, qq = pq.r1;
+        const F x3 = F::sub(F::sub(sq.r1, ppp), F::dbl(qq));
+        const auto zz = F::mul2(p.zz, q.zz, p.zzz, q.zzz);
+        const auto zs = F::mul2(zz.r0, pp, zz.r1, ppp);  // ZZ3, ZZZ3
+        const auto ys = F::mul2(r, F::sub(qq, x3), s.r0, ppp);
+        return {x3, F::sub(ys.r0, ys.r1), zs.r0, zs.r1};
+    }
+
     // Projective equality without normalisation.
     DV_INL static bool equal(const XYZZ& p, const XYZZ& q) {
         const bool pi = p.is_inf(), qi = q.is_inf();

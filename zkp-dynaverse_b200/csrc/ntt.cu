@@ -405,6 +405,10 @@ NttTables& ntt_tables(NttWorkspace& ws, int logn, int kind, cudaStream_t st) {
     return ref;
 }
 
+const uint32_t* ntt_ninv_canonical(NttTables& tables) {
+    return reinterpret_cast<const uint32_t*>(tables.consts.as<Fr>(C_COUNT) + C_NINV_CANON);
+}
+
 namespace {
 // Multipliers of one transform, taken from its tables.
 struct Scaling {

@@ -61,6 +61,8 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
 // Twiddle and scaling tables of one (size, kind), built on first use and
 // kept in the workspace.
 NttTables& ntt_tables(NttWorkspace& ws, int logn, int kind, cudaStream_t stream);
+// 1/n of a table set as a canonical scalar (8 little-endian words), on the device.
+const uint32_t* ntt_ninv_canonical(NttTables& tables);
 
 // ---------------------------------------------------------------- batches
 struct NttBatchItem {
