@@ -153,11 +153,25 @@ def test_sparse_resident_matches_oracle(backend, oracle):
         idx_all = np.concatenate([r[0] for r in reqs]) if reqs else np.zeros(0, np.uint64)
         vals_all = b"".join(r[1] for r in reqs)
         offs = np.concatenate([[0], np.cumsum([len(r[0]) for r in reqs])])
+        expect = [oracle.sparse_msm_g1(bases, idx, vals) for idx, vals in reqs]
         got = backend.sparse_msm_resident(h, idx_all, vals_all, offs)
-        for (idx, vals), g in zip(reqs, got):
-            assert g == oracle.sparse_msm_g1(bases, idx, vals)
+        assert got == expect
         with pytest.raises(Exception):
             backend.sparse_msm_resident(h, np.array([n], dtype=np.uint64), bytes(32), [0, 1])
+        # with a table of precomputed window multiples the same requests take
+        # the one-bucket-set path (host and device forms)
+        import torch
+        d_idx = torch.from_numpy(idx_all.view(np.int64)).cuda()
+        d_vals = torch.frombuffer(bytearray(vals_all), dtype=torch.uint8).cuda()
+        torch.cuda.synchronize()
+        for c in (8, 11, 0):
+            backend.precompute_bases(h, c)
+            assert backend.sparse_msm_resident(h, idx_all, vals_all, offs) == expect, c
+            assert backend.sparse_msm_device(h, d_idx.data_ptr(), d_vals.data_ptr(), offs) == expect, c
+        bad = torch.tensor([n], dtype=torch.int64, device="cuda")
+        with pytest.raises(Exception):
+            backend.sparse_msm_device(h, bad.data_ptr(), d_vals.data_ptr(), [0, 1])
+        assert backend.sparse_msm_resident(h, idx_all, vals_all, offs) == expect  # owner still healthy
     finally:
         backend.release_bases(h)
 

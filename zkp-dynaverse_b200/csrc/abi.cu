@@ -381,6 +381,33 @@ extern "C" int dvgpu_bases_release(void* opaque, uint64_t handle) {
     return b->bases.erase(handle) ? 0 : -1;
 }
 
+namespace {
+// Sparse MSMs over resident G1 bases: gather the selected bases (or, when
+// the bases carry a table of precomputed window multiples, each base's W
+// window multiples, so every request adds into one bucket set and needs
+// no window combination), then one launch sequence over all requests.
+void sparse_run(Backend& b, const ResidentBases& rb, const uint64_t* d_idx, const uint8_t* d_vals,
+                const std::vector<uint32_t>& offs, uint8_t* out, cudaStream_t st) {
+    const uint32_t count = (uint32_t)offs.size() - 1;
+    const uint64_t k_total = offs[count];
+    uint32_t* bad = b.err.as<uint32_t>(1);
+    DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
+    if (rb.pre_c) {
+        G1A* gathered = b.conv_points.as<G1A>(k_total * rb.pre_windows);
+        gather_table<Fq>(rb.pre_table.view<G1A>(), rb.n, rb.pre_windows, d_idx, k_total, gathered, bad, st);
+        const MsmPrecomp<Fq> pre{gathered, rb.pre_c, rb.pre_windows};
+        msm_run<Fq>(b.msm, nullptr, reinterpret_cast<const uint32_t*>(d_vals), offs.data(), count, 0, st, out,
+                    &b.msm_stats, &pre);
+    } else {
+        G1A* gathered = b.conv_points.as<G1A>(k_total);
+        gather_points<Fq>(rb.points.view<G1A>(), rb.n, d_idx, k_total, gathered, bad, st);
+        msm_run<Fq>(b.msm, gathered, reinterpret_cast<const uint32_t*>(d_vals), offs.data(), count,
+                    window_for<Fq>(b, offs), st, out, &b.msm_stats);
+    }
+    require(read_err_word(b, bad, st) == 0xffffffffu, "sparse MSM index out of range");
+}
+}  // namespace
+
 extern "C" int dvgpu_bn254_msm_sparse_batch(void* opaque, uint64_t bases_handle, const uint64_t* indices,
                                             const uint8_t* values, const uint64_t* request_offsets, size_t count,
                                             uint8_t* results, char* error, size_t cap) {
@@ -409,14 +436,8 @@ extern "C" int dvgpu_bn254_msm_sparse_batch(void* opaque, uint64_t bases_handle,
         uint8_t* d_vals = b.in_scalars.as<uint8_t>(k_total * 32);
         DV_CUDA(cudaMemcpyAsync(d_idx, indices, k_total * 8, cudaMemcpyHostToDevice, b.stream));
         DV_CUDA(cudaMemcpyAsync(d_vals, values, k_total * 32, cudaMemcpyHostToDevice, b.stream));
-        G1A* gathered = b.conv_points.as<G1A>(k_total);
-        uint32_t* bad = b.err.as<uint32_t>(1);
-        DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), b.stream));
-        gather_points<Fq>(rb.points.view<G1A>(), rb.n, d_idx, k_total, gathered, bad, b.stream);
         std::vector<uint8_t> tmp(count * 64);
-        msm_run<Fq>(b.msm, gathered, reinterpret_cast<const uint32_t*>(d_vals), offs.data(), (uint32_t)count,
-                    window_for<Fq>(b, offs), b.stream, tmp.data(), &b.msm_stats);
-        require(read_err_word(b, bad, b.stream) == 0xffffffffu, "sparse MSM index out of range");
+        sparse_run(b, rb, d_idx, d_vals, offs, tmp.data(), b.stream);
         b.batch_stats.icicle_calls++;
         b.batch_stats.max_batch_size = std::max<uint64_t>(b.batch_stats.max_batch_size, count);
         memcpy(results, tmp.data(), tmp.size());
@@ -446,14 +467,8 @@ extern "C" int dvgpu_bn254_msm_sparse_device(void* opaque, uint64_t bases_handle
         }
         const cudaStream_t st = pick(b, stream);
         const ResidentBases& rb = *it->second;
-        G1A* gathered = b.conv_points.as<G1A>(k_total);
-        uint32_t* bad = b.err.as<uint32_t>(1);
-        DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
-        gather_points<Fq>(rb.points.view<G1A>(), rb.n, d_indices, k_total, gathered, bad, st);
         std::vector<uint8_t> tmp(count * 64);
-        msm_run<Fq>(b.msm, gathered, reinterpret_cast<const uint32_t*>(d_values), offs.data(), (uint32_t)count,
-                    window_for<Fq>(b, offs), st, tmp.data(), &b.msm_stats);
-        require(read_err_word(b, bad, st) == 0xffffffffu, "sparse MSM index out of range");
+        sparse_run(b, rb, d_indices, d_values, offs, tmp.data(), st);
         memcpy(results_host, tmp.data(), tmp.size());
     });
 }

@@ -460,13 +460,15 @@ __global__ void k_convert_g2(const uint8_t* __restrict__ canon, G2A* __restrict_
 }
 
 template <class F>
-__global__ void k_gather(const Affine<F>* __restrict__ bases, uint64_t nbases, const uint64_t* __restrict__ idx,
+__global__ void k_gather(const Affine<F>* __restrict__ bases, uint64_t nbases, int W, const uint64_t* __restrict__ idx,
                          uint64_t k, Affine<F>* __restrict__ out, uint32_t* __restrict__ first_bad) {
-    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= k) return;
+    // W entries per index: a table of window multiples (W = 1: the bases)
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= k * (uint64_t)W) return;
+    const uint64_t j = t / (uint64_t)W, w = t % (uint64_t)W;
     const uint64_t i = idx[j];
     if (i >= nbases) { atomicMin(first_bad, (uint32_t)j); return; }
-    out[j] = bases[i];
+    out[t] = bases[i * W + w];
 }
 
 inline unsigned blocks_for(uint64_t n, unsigned threads) { return (unsigned)((n + threads - 1) / threads); }
@@ -544,9 +546,19 @@ template <class F>
 void gather_points(const Affine<F>* d_bases, uint64_t nbases, const uint64_t* d_idx, uint64_t k, Affine<F>* d_out,
                    uint32_t* d_first_bad, cudaStream_t st) {
     if (!k) return;
-    k_gather<F><<<blocks_for(k, 256), 256, 0, st>>>(d_bases, nbases, d_idx, k, d_out, d_first_bad);
+    k_gather<F><<<blocks_for(k, 256), 256, 0, st>>>(d_bases, nbases, 1, d_idx, k, d_out, d_first_bad);
     DV_LAUNCH();
 }
+
+template <class F>
+void gather_table(const Affine<F>* d_table, uint64_t nbases, int W, const uint64_t* d_idx, uint64_t k,
+                  Affine<F>* d_out, uint32_t* d_first_bad, cudaStream_t st) {
+    if (!k) return;
+    k_gather<F><<<blocks_for(k * (uint64_t)W, 256), 256, 0, st>>>(d_table, nbases, W, d_idx, k, d_out, d_first_bad);
+    DV_LAUNCH();
+}
+template void gather_table<Fq>(const Affine<Fq>*, uint64_t, int, const uint64_t*, uint64_t, Affine<Fq>*, uint32_t*,
+                               cudaStream_t);
 
 template <class F>
 MsmPlan msm_plan_batch(uint32_t count, uint32_t max_set, uint64_t total, int force_c, const MsmPrecomp<F>* pre) {
@@ -644,7 +656,14 @@ void msm_enqueue(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_
     // modest first level (measured 0.86 instead of 1.06 ms at 2^19 buckets);
     // shorter windows and G2, whose additions cost three times as much,
     // keep 8.
-    const int seg_want = (sizeof(F) == sizeof(Fq) && B >= (1u << 18)) ? DV_SEG_LOG + 1 : DV_SEG_LOG;
+    int seg_want = (sizeof(F) == sizeof(Fq) && B >= (1u << 18)) ? DV_SEG_LOG + 1 : DV_SEG_LOG;
+    // Few buckets in all (sparse updates over a precomputed table, small
+    // MSMs): the reduction is a latency chain, so keep about 2^15 first-level
+    // threads and shorten the segments (128 buckets: one bucket each).
+    const uint64_t all_buckets = (uint64_t)NW * B;
+    int room = 0;
+    while ((all_buckets >> (room + 1)) >= (1u << 15)) ++room;
+    seg_want = std::min(seg_want, room);
     const int seg_log = std::min(seg_want, c - 1);
     const uint32_t S = B >> seg_log;
     XYZZ<F>* d_seg_u = ws.segs.as<XYZZ<F>>(4ull * NW * S);

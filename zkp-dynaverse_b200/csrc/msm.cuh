@@ -136,6 +136,12 @@ MsmPlan msm_plan_precomputed(uint64_t n);
 template <class F>
 void convert_points(const uint8_t* d_canon, Affine<F>* d_out, uint64_t n, uint32_t* d_first_bad, cudaStream_t stream);
 
+// Gather of a table of window multiples (W entries per base):
+// out[j W + w] = table[idx[j] W + w], idx checked against nbases.
+template <class F>
+void gather_table(const Affine<F>* d_table, uint64_t nbases, int W, const uint64_t* d_idx, uint64_t k,
+                  Affine<F>* d_out, uint32_t* d_first_bad, cudaStream_t stream);
+
 // Gather (sparse MSM): out[j] = bases[idx[j]], with idx checked against nbases.
 template <class F>
 void gather_points(const Affine<F>* d_bases, uint64_t nbases, const uint64_t* d_idx, uint64_t k, Affine<F>* d_out,
