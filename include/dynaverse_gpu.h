@@ -262,6 +262,69 @@ int dvgpu_bn254_g1_ntt_rows(void* backend, const uint8_t* points, size_t row_len
 int dvgpu_bn254_g1_ntt_rows_device(void* backend, const uint8_t* d_points, size_t row_len, size_t rows, int inverse,
                                    uint8_t* d_results, void* stream, char* error, size_t error_capacity);
 
+/* ---------------------------------------------------------------- resident buffers
+ * The reference's resident ABI (native/include/dynaverse_gpu.h:100-160,
+ * bound by crates/gpu/src/resident.rs:81-92; semantics of
+ * CpuRebuildBackend, crates/protocol/src/incremental_rebuild/operators.rs):
+ * owner-local buffers of Fr (kind 0) or G1 (kind 1) elements, allocated
+ * zero / infinity before dvgpu_resident_seal; after sealing only writable
+ * buffers (ALLOC flags bit 0) accept writes.  ALLOC_BASES registers
+ * immutable affine MSM bases (kind 2), accepted only by READ and MSM_G1.
+ * BEGIN opens a transaction; the first write to an element saves its old
+ * value in the device journal (journal_bytes, 144 bytes per saved element);
+ * ROLLBACK restores every saved element; dvgpu_resident_commit publishes.
+ * Field use per opcode, as the reference binding sets them:
+ *   ALLOC kind,length,flags -> handle | LENGTH a | KIND a
+ *   WRITE/READ kind,a,a_offset,length,input/output (READ flags: 0 or 1)
+ *   COPY a,a_offset -> c,c_offset,length | REVERSE kind, same fields
+ *   TRANSPOSE kind,a -> c,rows,cols,a_offset = start,length,flags bit 0 with
+ *     input = root: element i -> (i % cols) rows + i / cols, times root^(row col)
+ *   TRANSFORM kind,a -> c,cols = row length,rows,a_offset = first row,
+ *     flags bit 0 = inverse (Fr NTT rows or G1 transform rows)
+ *   TRANSFORM_PACKET kind,a -> c (b scratch),length <= 4096,flags = inverse
+ *   ZIP flags 0 add / 1 sub / 2 mul, a,a_offset,b,b_offset -> c,c_offset,length
+ *   SCALE a points,a_offset x b scalars,b_offset -> c,c_offset,length
+ *   MSM_G1 a points,a_offset, b scalars,b_offset,length -> output 64 bytes
+ *   MSM_G2 input = length host G2 bases, b scalars,b_offset -> output 128 bytes
+ * Handles carry an owner tag; handles of other owners are rejected.
+ * configure: memory_limit_bytes caps device bytes (journal included); root
+ * must have multiplicative order exactly 2^20. */
+enum DvgpuResidentOpcode {
+    DVGPU_RESIDENT_ALLOC = 1, DVGPU_RESIDENT_LENGTH, DVGPU_RESIDENT_KIND,
+    DVGPU_RESIDENT_BEGIN, DVGPU_RESIDENT_ROLLBACK, DVGPU_RESIDENT_WRITE,
+    DVGPU_RESIDENT_READ, DVGPU_RESIDENT_COPY, DVGPU_RESIDENT_REVERSE,
+    DVGPU_RESIDENT_TRANSPOSE, DVGPU_RESIDENT_TRANSFORM, DVGPU_RESIDENT_ZIP,
+    DVGPU_RESIDENT_SCALE, DVGPU_RESIDENT_MSM_G1, DVGPU_RESIDENT_MSM_G2,
+    DVGPU_RESIDENT_ALLOC_BASES, DVGPU_RESIDENT_TRANSFORM_PACKET
+};
+typedef struct DvgpuResidentOp {
+    uint32_t opcode, kind, flags, reserved;
+    uint64_t a, b, c;
+    uint64_t a_offset, b_offset, c_offset, length, rows, cols;
+    const uint8_t* input;
+    uint8_t* output;
+} DvgpuResidentOp;
+typedef struct DvgpuResidentStats {
+    uint64_t h2d_bytes, d2h_bytes, bytes_allocated;
+    uint64_t fr_transform_elements, g1_transform_elements;
+    uint64_t msm_g1_points, msm_g2_points, calls;
+} DvgpuResidentStats;
+typedef struct DvgpuResidentDiagnostics {
+    uint64_t resident_allocations, temporary_allocations, temporary_peak_bytes;
+    uint64_t journal_saved_bytes, journal_saved_ranges, journal_peak_bytes;
+    uint64_t device_operation_ns, device_operations;
+    uint64_t physical_h2d_bytes, physical_d2h_bytes, explicit_d2d_bytes;
+    uint64_t journal_metadata_capacity_bytes;
+} DvgpuResidentDiagnostics;
+int dvgpu_resident_configure(void* backend, uint64_t memory_limit_bytes, uint64_t journal_bytes, const uint8_t* root,
+                             char* error, size_t error_capacity);
+int dvgpu_resident_call(void* backend, const DvgpuResidentOp* operation, uint64_t* result, char* error,
+                        size_t error_capacity);
+void dvgpu_resident_seal(void* backend);
+void dvgpu_resident_commit(void* backend);
+int dvgpu_resident_stats(void* backend, DvgpuResidentStats* stats);
+int dvgpu_resident_diagnostics(void* backend, DvgpuResidentDiagnostics* stats);
+
 /* ---------------------------------------------------------------- batching
  * No counterpart in the reference ABI (its batch path is
  * dvgpu_bn254_msm_batch with next-pow2 padding, icicle_msm.cu:810-880, and

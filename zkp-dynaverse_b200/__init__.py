@@ -73,6 +73,30 @@ class ServeStats(ctypes.Structure):
                                                       "pending")]
 
 
+class ResidentOp(ctypes.Structure):
+    _fields_ = [("opcode", ctypes.c_uint32), ("kind", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("a", ctypes.c_uint64), ("b", ctypes.c_uint64), ("c", ctypes.c_uint64),
+                ("a_offset", ctypes.c_uint64), ("b_offset", ctypes.c_uint64), ("c_offset", ctypes.c_uint64),
+                ("length", ctypes.c_uint64), ("rows", ctypes.c_uint64), ("cols", ctypes.c_uint64),
+                ("input", ctypes.c_void_p), ("output", ctypes.c_void_p)]
+
+
+class ResidentStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("h2d_bytes", "d2h_bytes", "bytes_allocated", "fr_transform_elements",
+                                               "g1_transform_elements", "msm_g1_points", "msm_g2_points", "calls")]
+
+
+class ResidentDiagnostics(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "resident_allocations", "temporary_allocations", "temporary_peak_bytes", "journal_saved_bytes",
+        "journal_saved_ranges", "journal_peak_bytes", "device_operation_ns", "device_operations",
+        "physical_h2d_bytes", "physical_d2h_bytes", "explicit_d2d_bytes", "journal_metadata_capacity_bytes")]
+
+
+RESIDENT_OPS = dict(ALLOC=1, LENGTH=2, KIND=3, BEGIN=4, ROLLBACK=5, WRITE=6, READ=7, COPY=8, REVERSE=9, TRANSPOSE=10,
+                    TRANSFORM=11, ZIP=12, SCALE=13, MSM_G1=14, MSM_G2=15, ALLOC_BASES=16, TRANSFORM_PACKET=17)
+
+
 class BatchPlanBuffers(ctypes.Structure):
     _fields_ = [("scalars", ctypes.c_void_p), ("ntt_values", ctypes.c_void_p), ("msm_results", ctypes.c_void_p),
                 ("ntt_results", ctypes.c_void_p), ("scalar_bytes", ctypes.c_uint64), ("ntt_bytes", ctypes.c_uint64),
@@ -148,6 +172,12 @@ SIGNATURES = [
     ("dvgpu_batch_plan_check", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
     ("dvgpu_batch_plan_run", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _B, _B] + _E),
     ("dvgpu_batch_plan_destroy", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
+    ("dvgpu_resident_configure", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint64, _P] + _E),
+    ("dvgpu_resident_call", ctypes.c_int, [_P, ctypes.POINTER(ResidentOp), ctypes.POINTER(ctypes.c_uint64)] + _E),
+    ("dvgpu_resident_seal", None, [_P]),
+    ("dvgpu_resident_commit", None, [_P]),
+    ("dvgpu_resident_stats", ctypes.c_int, [_P, ctypes.POINTER(ResidentStats)]),
+    ("dvgpu_resident_diagnostics", ctypes.c_int, [_P, ctypes.POINTER(ResidentDiagnostics)]),
     ("dvgpu_serve_create", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(_P)] + _E),
     ("dvgpu_serve_destroy", None, [_P]),
     ("dvgpu_serve_open_session", ctypes.c_int, [_P, _P, _P, _SZ, ctypes.POINTER(ctypes.c_uint64), _B] + _E),
@@ -603,6 +633,110 @@ class DvgpuBackend:
 
     def g1_ntt_rows_device(self, d_points: int, row_len: int, rows: int, inverse: bool, d_out: int, stream=None):
         self._call("dvgpu_bn254_g1_ntt_rows_device", d_points, row_len, rows, int(inverse), d_out, stream)
+
+    # ------------------------------------------------------------------ resident buffers
+    # RebuildBackend (crates/protocol/src/incremental_rebuild/operators.rs) over
+    # the resident ABI, with the reference binding's field encoding
+    # (crates/gpu/src/resident.rs:250-402).  Values: canonical bytes (Fr 32,
+    # G1 64 affine, G2 128).
+    def resident_configure(self, memory_limit: int, journal_bytes: int, root: bytes):
+        self._call("dvgpu_resident_configure", memory_limit, journal_bytes, _ptr(root))
+
+    def resident_call(self, opcode: str, keep=None, **fields) -> int:
+        op = ResidentOp()
+        op.opcode = RESIDENT_OPS[opcode]
+        for k, v in fields.items():
+            setattr(op, k, v)
+        r = ctypes.c_uint64()
+        self._call("dvgpu_resident_call", ctypes.byref(op), ctypes.byref(r))
+        return r.value
+
+    def rb_alloc(self, kind: int, length: int, writable: bool) -> int:
+        return self.resident_call("ALLOC", kind=kind, length=length, flags=int(writable))
+
+    def rb_register_bases(self, points: bytes) -> int:
+        buf = ctypes.create_string_buffer(points, max(1, len(points)))
+        return self.resident_call("ALLOC_BASES", length=len(points) // G1_BYTES, input=ctypes.addressof(buf))
+
+    def rb_seal(self):
+        self._L.dvgpu_resident_seal(self.handle)
+
+    def rb_commit(self):
+        self._L.dvgpu_resident_commit(self.handle)
+
+    def rb_len(self, h: int) -> int:
+        return self.resident_call("LENGTH", a=h)
+
+    def rb_kind(self, h: int) -> int:
+        return self.resident_call("KIND", a=h)
+
+    def rb_begin(self):
+        self.resident_call("BEGIN")
+
+    def rb_rollback(self):
+        self.resident_call("ROLLBACK")
+
+    def rb_write(self, h: int, offset: int, data: bytes, kind: int):
+        width = FR_BYTES if kind == 0 else G1_BYTES
+        buf = ctypes.create_string_buffer(data, max(1, len(data)))
+        self.resident_call("WRITE", kind=kind, a=h, a_offset=offset, length=len(data) // width,
+                           input=ctypes.addressof(buf))
+
+    def rb_read(self, h: int, offset: int, length: int, kind: int, flags: int = 0) -> bytes:
+        width = FR_BYTES if kind == 0 else G1_BYTES
+        out = ctypes.create_string_buffer(max(1, length * width))
+        self.resident_call("READ", kind=kind, a=h, a_offset=offset, length=length, flags=flags,
+                           output=ctypes.addressof(out))
+        return out.raw[:length * width]
+
+    def rb_copy(self, src, src_off, dst, dst_off, length):
+        self.resident_call("COPY", a=src, a_offset=src_off, c=dst, c_offset=dst_off, length=length)
+
+    def rb_reverse(self, kind, src, src_off, dst, dst_off, length):
+        self.resident_call("REVERSE", kind=kind, a=src, a_offset=src_off, c=dst, c_offset=dst_off, length=length)
+
+    def rb_transpose(self, kind, src, dst, rows, cols, start, length, root=None):
+        buf = ctypes.create_string_buffer(root if root else bytes(32), 32)
+        self.resident_call("TRANSPOSE", kind=kind, a=src, c=dst, rows=rows, cols=cols, a_offset=start, length=length,
+                           flags=int(root is not None), input=ctypes.addressof(buf))
+
+    def rb_transform_rows(self, kind, src, dst, row_len, first_row, row_count, inverse):
+        self.resident_call("TRANSFORM", kind=kind, a=src, c=dst, cols=row_len, rows=row_count, a_offset=first_row,
+                           flags=int(inverse))
+
+    def rb_transform_packet(self, kind, src, scratch, dst, length, inverse):
+        self.resident_call("TRANSFORM_PACKET", kind=kind, a=src, b=scratch, c=dst, length=length, flags=int(inverse))
+
+    def rb_zip(self, op: int, left, left_off, right, right_off, dst, dst_off, length):
+        self.resident_call("ZIP", flags=op, a=left, a_offset=left_off, b=right, b_offset=right_off, c=dst,
+                           c_offset=dst_off, length=length)
+
+    def rb_scale(self, pts, pts_off, sc, sc_off, dst, dst_off, length):
+        self.resident_call("SCALE", a=pts, a_offset=pts_off, b=sc, b_offset=sc_off, c=dst, c_offset=dst_off,
+                           length=length)
+
+    def rb_msm_g1(self, pts, pts_off, sc, sc_off, length) -> bytes:
+        out = ctypes.create_string_buffer(G1_BYTES)
+        self.resident_call("MSM_G1", a=pts, a_offset=pts_off, b=sc, b_offset=sc_off, length=length,
+                           output=ctypes.addressof(out))
+        return out.raw
+
+    def rb_msm_g2(self, points: bytes, sc, sc_off) -> bytes:
+        inp = ctypes.create_string_buffer(points, max(1, len(points)))
+        out = ctypes.create_string_buffer(G2_BYTES)
+        self.resident_call("MSM_G2", b=sc, b_offset=sc_off, length=len(points) // G2_BYTES,
+                           input=ctypes.addressof(inp), output=ctypes.addressof(out))
+        return out.raw
+
+    def rb_stats(self) -> ResidentStats:
+        st = ResidentStats()
+        self._L.dvgpu_resident_stats(self.handle, ctypes.byref(st))
+        return st
+
+    def rb_diagnostics(self) -> ResidentDiagnostics:
+        d = ResidentDiagnostics()
+        self._L.dvgpu_resident_diagnostics(self.handle, ctypes.byref(d))
+        return d
 
     # ------------------------------------------------------------------ batching
     def ntt_batch(self, values: bytes, log_sizes, kinds=None) -> bytes:

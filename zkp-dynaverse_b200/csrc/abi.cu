@@ -188,6 +188,7 @@ __global__ void k_probe_madc(uint32_t seed, uint32_t iters, uint32_t* sink) {
 
 void Backend::release_all() noexcept {
     plans.clear();
+    resident.reset();
     bases.clear();
     MsmTimeline& tl = msm.timeline;
     for (auto& e : tl.ev)
@@ -971,3 +972,9 @@ extern "C" int dvgpu_bases_precompute(void* opaque, uint64_t handle, int c, int*
         if (c_used) *c_used = plan.c;
     });
 }
+
+namespace dv {
+// The resident engine's configuration check (resident.cu): a root of
+// multiplicative order exactly 2^20.
+bool root_order_2_20(const uint8_t* root) { return root_has_order_2_20(root); }
+}  // namespace dv

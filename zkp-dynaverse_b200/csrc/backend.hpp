@@ -32,6 +32,8 @@ struct ResidentBases {
     int pre_c = 0, pre_windows = 0;
 };
 
+struct ResidentState;  // resident.cu
+
 struct Backend {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -56,6 +58,7 @@ struct Backend {
 
     std::map<uint64_t, std::unique_ptr<ResidentBases>> bases;
     std::map<uint64_t, std::unique_ptr<BatchPlan>> plans;  // CUDA-graph batch plans
+    std::shared_ptr<ResidentState> resident;                // resident transactional buffers
     uint64_t next_handle = 1;
 
     void release_all() noexcept;

@@ -116,6 +116,23 @@ void g1_ntt_rows(Backend& b, const uint8_t* d_in, int logn, uint64_t rows, bool 
     DV_LAUNCH();
 }
 
+// Bit-reversed XYZZ working rows -> natural-order XYZZ rows (x 1/n).
+__global__ void __launch_bounds__(128) k_ec_permute(const XYZZ<Fq>* __restrict__ work, int logn, uint64_t total,
+                                                    const uint32_t* __restrict__ ninv, XYZZ<Fq>* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const uint64_t r = i >> logn;
+    const uint32_t e = (uint32_t)(i & ((1ull << logn) - 1));
+    const uint32_t src = logn ? (__brev(e) >> (32 - logn)) : 0;
+    XYZZ<Fq> p = work[(r << logn) + src];
+    if (ninv) {
+        uint32_t k[8];
+        for (int w = 0; w < 8; ++w) k[w] = ninv[w];
+        p = scalar_mul(p, k);
+    }
+    out[i] = p;
+}
+
 int log2_exact(uint64_t n) {
     int k = 0;
     while ((1ull << k) < n) ++k;
@@ -123,6 +140,22 @@ int log2_exact(uint64_t n) {
 }
 
 }  // namespace
+
+void g1_ntt_rows_xyzz(NttWorkspace& ws, XYZZ<Fq>* work, int logn, uint64_t rows, bool inverse, XYZZ<Fq>* out,
+                      cudaStream_t st) {
+    const uint64_t total = rows << logn;
+    NttTables& tab = ntt_tables(ws, logn, inverse ? NTT_INVERSE : NTT_FORWARD, st);
+    const Fr* tw = tab.tw.as<Fr>(1);
+    const uint64_t butterflies = total / 2;
+    for (int s = 0; s < logn; ++s) {
+        k_ec_stage<<<(unsigned)((butterflies + 127) / 128), 128, 0, st>>>(work, logn, s, butterflies, tw);
+        DV_LAUNCH();
+    }
+    k_ec_permute<<<(unsigned)((total + 127) / 128), 128, 0, st>>>(work, logn, total,
+                                                                  inverse ? ntt_ninv_canonical(tab) : nullptr, out);
+    DV_LAUNCH();
+}
+
 }  // namespace dv
 
 using namespace dv;

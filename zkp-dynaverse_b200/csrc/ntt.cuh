@@ -32,6 +32,7 @@
 #include <memory>
 #include <vector>
 
+#include "curve.cuh"
 #include "engine.hpp"
 
 namespace dv {
@@ -63,6 +64,11 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
 NttTables& ntt_tables(NttWorkspace& ws, int logn, int kind, cudaStream_t stream);
 // 1/n of a table set as a canonical scalar (8 little-endian words), on the device.
 const uint32_t* ntt_ninv_canonical(NttTables& tables);
+
+// G1 transform of rows x 2^logn XYZZ points held in `work` (overwritten):
+// natural-order results (x 1/n for the inverse) in `out` (ecntt.cu).
+void g1_ntt_rows_xyzz(NttWorkspace& ws, XYZZ<Fq>* work, int logn, uint64_t rows, bool inverse, XYZZ<Fq>* out,
+                      cudaStream_t stream);
 
 // ---------------------------------------------------------------- batches
 struct NttBatchItem {
