@@ -262,6 +262,54 @@ int dvgpu_bn254_g1_ntt_rows(void* backend, const uint8_t* points, size_t row_len
 int dvgpu_bn254_g1_ntt_rows_device(void* backend, const uint8_t* d_points, size_t row_len, size_t rows, int inverse,
                                    uint8_t* d_results, void* stream, char* error, size_t error_capacity);
 
+/* ---------------------------------------------------------------- polynomial toolkit
+ * The field work of a sparse update (crates/protocol/src/domain/fast.rs,
+ * called from crates/protocol/src/dynaverse/sparse.rs:125-236), which the
+ * reference runs on the host with every product routed through
+ * OperatorBackend::ntt.  Polynomials are canonical Fr coefficient vectors,
+ * lowest degree first; results are trimmed as the reference's trim()
+ * (crates/protocol/src/domain.rs:339-346): no trailing zero coefficient,
+ * at least one entry.  Non-canonical inputs and the reference's error
+ * conditions return -1 with the reference's message. */
+
+/* fft_multiply_with_backend (domain/fast.rs:213-234): result_capacity >=
+ * max(1, left_len + right_len - 1) <= 2^24; an empty operand gives [0]. */
+int dvgpu_bn254_poly_multiply(void* backend, const uint8_t* left, size_t left_len, const uint8_t* right,
+                              size_t right_len, uint8_t* result, size_t result_capacity, size_t* result_len,
+                              char* error, size_t error_capacity);
+/* newton_divide_exact_with_backend (domain/fast.rs:236-240, div_rem_impl
+ * :163-202): the quotient of an exact division; quotient_capacity >=
+ * max(1, numerator_len).  Errors: "cannot divide by zero polynomial",
+ * "polynomial division has a nonzero remainder". */
+int dvgpu_bn254_poly_divide_exact(void* backend, const uint8_t* numerator, size_t numerator_len,
+                                  const uint8_t* denominator, size_t denominator_len, uint8_t* quotient,
+                                  size_t quotient_capacity, size_t* quotient_len, char* error, size_t error_capacity);
+/* SubproductTree::new_with_backend (domain/fast.rs:18-62) over `count`
+ * <= 2^20 distinct points, kept on the device under a handle.  A repeated
+ * point: -1 "duplicate interpolation point". */
+int dvgpu_bn254_tree_create(void* backend, const uint8_t* points, size_t count, uint64_t* tree, char* error,
+                            size_t error_capacity);
+int dvgpu_bn254_tree_destroy(void* backend, uint64_t tree, char* error, size_t error_capacity);
+/* vanishing() (fast.rs:64): prod (X - x_i), count + 1 coefficients. */
+int dvgpu_bn254_tree_vanishing(void* backend, uint64_t tree, uint8_t* coefficients, size_t capacity, size_t* length,
+                               char* error, size_t error_capacity);
+/* inverse_derivatives() (fast.rs:67): 1 / A'(x_i) in point order. */
+int dvgpu_bn254_tree_inverse_derivatives(void* backend, uint64_t tree, uint8_t* values, size_t capacity, char* error,
+                                         size_t error_capacity);
+/* multipoint_eval_with_backend (fast.rs:22-24, 73-84) of `rows` (<= 65535)
+ * polynomials of `length` coefficients each: rows x count values. */
+int dvgpu_bn254_tree_evaluate(void* backend, uint64_t tree, const uint8_t* polynomials, size_t length, size_t rows,
+                              uint8_t* values, char* error, size_t error_capacity);
+/* interpolate_with_backend (fast.rs:26-28, 90-116) of `rows` value vectors
+ * of `count` (= the tree's points) entries: row r's coefficients at
+ * coefficients + 32 * r * max(1, count), its trimmed length in lengths[r]. */
+int dvgpu_bn254_tree_interpolate(void* backend, uint64_t tree, const uint8_t* values, size_t count, size_t rows,
+                                 uint8_t* coefficients, size_t* lengths, char* error, size_t error_capacity);
+/* cauchy_sums_with_backend (fast.rs:30-32, 118-139): sum_{j != i}
+ * w_j / (x_i - x_j) for `rows` weight vectors of `count` entries. */
+int dvgpu_bn254_tree_cauchy_sums(void* backend, uint64_t tree, const uint8_t* weights, size_t count, size_t rows,
+                                 uint8_t* sums, char* error, size_t error_capacity);
+
 /* ---------------------------------------------------------------- resident buffers
  * The reference's resident ABI (native/include/dynaverse_gpu.h:100-160,
  * bound by crates/gpu/src/resident.rs:81-92; semantics of

@@ -23,6 +23,11 @@
 //    table in native/include/icicle_setup.cuh:44-65).
 //  * G2 wire parse + on-curve + subgroup predicates (masks 1/2/4):
 //    crates/gpu/src/g2_validation.rs:214-299, native/include/icicle_g2_wire.cuh.
+//  * Polynomial toolkit: crates/protocol/src/domain/fast.rs (subproduct
+//    tree, multipoint evaluation, interpolation, Cauchy sums, Newton exact
+//    division, FFT products) over the NTT above.  Outputs are fixed by
+//    exact arithmetic, so the restatement follows the reference's algorithm
+//    step by step and is pinned by the reference tests' direct definitions.
 //  * Codec: canonical little-endian, all-zero = infinity
 //    (crates/gpu/src/codec.rs:25-111, crates/gpu/src/resident.rs:419-431).
 //
@@ -824,6 +829,221 @@ static void g1_fft_inplace(std::vector<Jac<OpsFq>>& a, const Fe& omega) {
     }
 }
 
+// ------------------------------------------------------------------ polynomial toolkit
+// Restatement of crates/protocol/src/domain/fast.rs with the oracle's NTT as
+// the backend: fft_multiply_with_backend (:213-234), differentiate
+// (:141-150), div_rem_impl with the backend Newton reciprocal (:163-202),
+// SubproductTree new/eval/interpolate/cauchy (:38-139); trim and
+// subtract_polynomials from crates/protocol/src/domain.rs:169-179, 339-346.
+// Coefficients are Montgomery Fe, lowest degree first.
+typedef std::vector<Fe> Poly;
+
+static void poly_trim(Poly& p) {
+    while (p.size() > 1 && fzero(p.back())) p.pop_back();
+    if (p.empty()) p.push_back(Fe{});
+}
+static Fe fe_small(uint64_t v) {
+    uint64_t c[4] = {v, 0, 0, 0};
+    Fe r;
+    to_mont(FR, r, c);
+    return r;
+}
+static Poly poly_mul(const Poly& l, const Poly& r) {
+    if (l.empty() || r.empty()) return Poly(1);
+    const size_t len = l.size() + r.size() - 1;
+    size_t size = 1;
+    while (size < len) size <<= 1;
+    Poly a = l, b = r;
+    a.resize(size);
+    b.resize(size);
+    Fe w = root_of_unity(size), wi, ni;
+    ntt_inplace(a, w);
+    ntt_inplace(b, w);
+    for (size_t i = 0; i < size; ++i) fmul(FR, a[i], a[i], b[i]);
+    finv(FR, wi, w);
+    ntt_inplace(a, wi);
+    finv(FR, ni, fe_small(size));
+    for (auto& v : a) fmul(FR, v, v, ni);
+    a.resize(len);
+    poly_trim(a);
+    return a;
+}
+static Poly poly_sub(const Poly& l, const Poly& r) {
+    Poly out(std::max<size_t>(std::max(l.size(), r.size()), 1));
+    for (size_t i = 0; i < l.size(); ++i) fadd(FR, out[i], out[i], l[i]);
+    for (size_t i = 0; i < r.size(); ++i) fsub(FR, out[i], out[i], r[i]);
+    poly_trim(out);
+    return out;
+}
+static Poly poly_diff(const Poly& p) {
+    Poly d;
+    for (size_t i = 1; i < p.size(); ++i) {
+        Fe v;
+        fmul(FR, v, p[i], fe_small(i));
+        d.push_back(v);
+    }
+    poly_trim(d);
+    return d;
+}
+static bool poly_all_zero(const Poly& p) {
+    for (auto& v : p)
+        if (!fzero(v)) return false;
+    return true;
+}
+// 0 ok, -2 zero divisor.
+static int poly_div_rem(const Poly& numerator, const Poly& denominator, Poly& quotient, Poly& remainder) {
+    Poly num = numerator, den = denominator;
+    poly_trim(num);
+    poly_trim(den);
+    if (fzero(den.back())) return -2;
+    if (num.size() < den.size() || poly_all_zero(num)) {
+        quotient = Poly(1);
+        remainder = num;
+        return 0;
+    }
+    const size_t len = num.size() - den.size() + 1;
+    Poly rev(den.rbegin(), den.rend());
+    Poly inv(1);
+    finv(FR, inv[0], rev[0]);
+    while (inv.size() < len) {
+        const size_t next = std::min(inv.size() * 2, len);
+        Poly head(rev.begin(), rev.begin() + std::min(rev.size(), next));
+        Poly corr = poly_mul(head, inv);
+        corr.resize(next);
+        for (auto& c : corr) fneg(FR, c, c);
+        Fe two = fe_small(2);
+        fadd(FR, corr[0], corr[0], two);
+        inv = poly_mul(inv, corr);
+        inv.resize(next);
+    }
+    Poly rnum(num.rbegin(), num.rbegin() + len);
+    Poly q = poly_mul(rnum, Poly(inv.begin(), inv.begin() + len));
+    q.resize(len);
+    std::reverse(q.begin(), q.end());
+    poly_trim(q);
+    remainder = poly_sub(num, poly_mul(q, den));
+    quotient = q;
+    return 0;
+}
+
+struct OTree {
+    Poly points;
+    std::vector<std::vector<Poly>> levels;
+    Poly inv_deriv;
+    const Poly& vanishing() const { return levels.back()[0]; }
+
+    Poly eval(const Poly& poly) const {
+        if (points.empty()) return Poly();
+        Poly q, r;
+        poly_div_rem(poly, vanishing(), q, r);
+        std::vector<Poly> rems{r};
+        for (int level = (int)levels.size() - 2; level >= 0; --level) {
+            std::vector<Poly> next;
+            for (size_t i = 0; i < levels[level].size(); ++i) {
+                poly_div_rem(rems[i / 2], levels[level][i], q, r);
+                next.push_back(r);
+            }
+            rems.swap(next);
+        }
+        Poly out;
+        for (auto& rem : rems) out.push_back(rem[0]);
+        return out;
+    }
+    Poly interpolate(const Poly& values) const {
+        if (values.empty()) return Poly(1);
+        std::vector<Poly> polys;
+        for (size_t i = 0; i < values.size(); ++i) {
+            Fe v;
+            fmul(FR, v, values[i], inv_deriv[i]);
+            polys.push_back(Poly{v});
+        }
+        for (size_t level = 0; level + 1 < levels.size(); ++level) {
+            std::vector<Poly> next;
+            for (size_t i = 0; i < polys.size(); i += 2) {
+                if (i + 1 == polys.size()) {
+                    next.push_back(polys[i]);
+                    continue;
+                }
+                Poly left = poly_mul(polys[i], levels[level][i + 1]);
+                Poly right = poly_mul(polys[i + 1], levels[level][i]);
+                Poly comb(std::max(left.size(), right.size()));
+                for (size_t j = 0; j < left.size(); ++j) fadd(FR, comb[j], comb[j], left[j]);
+                for (size_t j = 0; j < right.size(); ++j) fadd(FR, comb[j], comb[j], right[j]);
+                poly_trim(comb);
+                next.push_back(comb);
+            }
+            polys.swap(next);
+        }
+        return polys.back();
+    }
+    Poly cauchy(const Poly& weights) const {
+        Poly numv;
+        for (size_t i = 0; i < weights.size(); ++i) {
+            Fe d, v;
+            finv(FR, d, inv_deriv[i]);
+            fmul(FR, v, weights[i], d);
+            numv.push_back(v);
+        }
+        Poly first = eval(poly_diff(interpolate(numv)));
+        Poly second = eval(poly_diff(poly_diff(vanishing())));
+        Fe half;
+        finv(FR, half, fe_small(2));
+        Poly sums;
+        for (size_t i = 0; i < weights.size(); ++i) {
+            Fe t, s;
+            fmul(FR, t, weights[i], second[i]);
+            fmul(FR, t, t, half);
+            fsub(FR, s, first[i], t);
+            fmul(FR, s, s, inv_deriv[i]);
+            sums.push_back(s);
+        }
+        return sums;
+    }
+};
+
+// nullptr for a repeated point.
+static OTree* tree_new(const Poly& points) {
+    for (size_t i = 0; i < points.size(); ++i)
+        for (size_t j = 0; j < i; ++j)
+            if (feq(points[i], points[j])) return nullptr;
+    OTree* t = new OTree;
+    t->points = points;
+    std::vector<Poly> leaves;
+    for (auto& x : points) {
+        Fe nx;
+        fneg(FR, nx, x);
+        leaves.push_back(Poly{nx, FR.one});
+    }
+    if (leaves.empty()) leaves.push_back(Poly{FR.one});
+    t->levels.push_back(leaves);
+    while (t->levels.back().size() > 1) {
+        const std::vector<Poly>& prev = t->levels.back();
+        std::vector<Poly> next;
+        for (size_t i = 0; i < prev.size(); i += 2)
+            next.push_back(i + 1 < prev.size() ? poly_mul(prev[i], prev[i + 1]) : prev[i]);
+        t->levels.push_back(next);
+    }
+    Poly d = t->eval(poly_diff(t->vanishing()));
+    for (auto& v : d) {
+        if (fzero(v)) { delete t; return nullptr; }
+        finv(FR, v, v);
+    }
+    t->inv_deriv = d;
+    return t;
+}
+static bool read_poly(const uint8_t* b, size_t n, Poly& out) {
+    out.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        uint64_t c[4];
+        if (!read_canon(b + 32 * i, c, R_LIMBS)) return false;
+        to_mont(FR, out[i], c);
+    }
+    return true;
+}
+static void write_poly(uint8_t* b, const Poly& p) {
+    for (size_t i = 0; i < p.size(); ++i) fe_to_bytes(FR, b + 32 * i, p[i]);
+}
+
 struct Init { Init() { init_psi(); } } init_once;
 
 // ------------------------------------------------------------------ ChaCha20
@@ -1098,6 +1318,60 @@ int oracle_g2_mul_r(const uint8_t* a, uint8_t* out) {
     if (!g2_read(a, pa)) return -1;
     g2_write(out, jac_to_aff(mul_bits(pa, R_LIMBS, 254)));
     return 0;
+}
+
+// Polynomial toolkit (restatement of domain/fast.rs, see above).  Coefficient
+// and value buffers: canonical Fr bytes.
+size_t oracle_poly_mul(const uint8_t* l, size_t ll, const uint8_t* r, size_t rl, uint8_t* out) {
+    Poly a, b;
+    if (!read_poly(l, ll, a) || !read_poly(r, rl, b)) return 0;
+    Poly p = poly_mul(a, b);
+    write_poly(out, p);
+    return p.size();
+}
+// 0 ok (quotient in out, length in *out_len), -1 bad input, -2 zero divisor,
+// -3 nonzero remainder.
+int oracle_poly_div_exact(const uint8_t* num, size_t nl, const uint8_t* den, size_t dl, uint8_t* out,
+                          size_t* out_len) {
+    Poly a, b, q, rem;
+    if (!read_poly(num, nl, a) || !read_poly(den, dl, b)) return -1;
+    if (poly_div_rem(a, b, q, rem) != 0) return -2;
+    if (!poly_all_zero(rem)) return -3;
+    write_poly(out, q);
+    *out_len = q.size();
+    return 0;
+}
+void* oracle_tree_new(const uint8_t* points, size_t n) {
+    Poly p;
+    if (!read_poly(points, n, p)) return nullptr;
+    return tree_new(p);
+}
+void oracle_tree_free(void* t) { delete static_cast<OTree*>(t); }
+size_t oracle_tree_vanishing(void* t, uint8_t* out) {
+    const Poly& v = static_cast<OTree*>(t)->vanishing();
+    write_poly(out, v);
+    return v.size();
+}
+void oracle_tree_inverse_derivatives(void* t, uint8_t* out) { write_poly(out, static_cast<OTree*>(t)->inv_deriv); }
+int oracle_tree_eval(void* t, const uint8_t* poly, size_t len, uint8_t* out) {
+    Poly p;
+    if (!read_poly(poly, len, p)) return -1;
+    write_poly(out, static_cast<OTree*>(t)->eval(p));
+    return 0;
+}
+size_t oracle_tree_interpolate(void* t, const uint8_t* values, uint8_t* out) {
+    OTree* tr = static_cast<OTree*>(t);
+    Poly v;
+    if (!read_poly(values, tr->points.size(), v)) return 0;
+    Poly f = tr->interpolate(v);
+    write_poly(out, f);
+    return f.size();
+}
+void oracle_tree_cauchy(void* t, const uint8_t* weights, uint8_t* out) {
+    OTree* tr = static_cast<OTree*>(t);
+    Poly w;
+    if (!read_poly(weights, tr->points.size(), w)) return;
+    write_poly(out, tr->cauchy(w));
 }
 
 }  // extern "C"

@@ -48,6 +48,19 @@ def lib():
         L.oracle_g1_add.argtypes = [u8p, u8p, u8p]
         L.oracle_g2_add.argtypes = [u8p, u8p, u8p]
         L.oracle_g2_mul_r.argtypes = [u8p, u8p]
+        L.oracle_poly_mul.argtypes = [u8p, sz, u8p, sz, u8p]
+        L.oracle_poly_mul.restype = sz
+        L.oracle_poly_div_exact.argtypes = [u8p, sz, u8p, sz, u8p, ctypes.POINTER(sz)]
+        L.oracle_tree_new.argtypes = [u8p, sz]
+        L.oracle_tree_new.restype = ctypes.c_void_p
+        L.oracle_tree_free.argtypes = [ctypes.c_void_p]
+        L.oracle_tree_vanishing.argtypes = [ctypes.c_void_p, u8p]
+        L.oracle_tree_vanishing.restype = sz
+        L.oracle_tree_inverse_derivatives.argtypes = [ctypes.c_void_p, u8p]
+        L.oracle_tree_eval.argtypes = [ctypes.c_void_p, u8p, sz, u8p]
+        L.oracle_tree_interpolate.argtypes = [ctypes.c_void_p, u8p, u8p]
+        L.oracle_tree_interpolate.restype = sz
+        L.oracle_tree_cauchy.argtypes = [ctypes.c_void_p, u8p, u8p]
         _lib = L
     return _lib
 
@@ -183,3 +196,78 @@ def srs_g1(seed: int, n: int, threads=0):
 def srs_g2(seed: int, n: int, threads=0):
     tau = uniform_fr(seed, 1)
     return fixed_base_g2(fr_powers(tau, n), threads), tau
+
+
+# ---------------------------------------------------------------- polynomial toolkit
+# Restatement of crates/protocol/src/domain/fast.rs (bn254_oracle.cpp):
+# coefficient vectors are canonical Fr bytes, lowest degree first, trimmed.
+def poly_mul(left: bytes, right: bytes) -> bytes:
+    out = _buf(max(32, len(left) + len(right)))
+    n = lib().oracle_poly_mul(left, len(left) // 32, right, len(right) // 32, out)
+    return out.raw[:32 * n]
+
+
+def poly_div_exact(numerator: bytes, denominator: bytes) -> bytes:
+    """Quotient of an exact division; ValueError with the reference's message
+    otherwise (domain/fast.rs:163-170, 236-240)."""
+    out = _buf(max(32, len(numerator)))
+    n = ctypes.c_size_t()
+    rc = lib().oracle_poly_div_exact(numerator, len(numerator) // 32, denominator, len(denominator) // 32, out,
+                                     ctypes.byref(n))
+    if rc == -2:
+        raise ValueError("cannot divide by zero polynomial")
+    if rc == -3:
+        raise ValueError("polynomial division has a nonzero remainder")
+    if rc != 0:
+        raise ValueError("oracle: bad polynomial input")
+    return out.raw[:32 * n.value]
+
+
+class Tree:
+    """SubproductTree (domain/fast.rs:11-139) over canonical Fr points."""
+
+    def __init__(self, points: bytes):
+        self.n = len(points) // 32
+        self._h = lib().oracle_tree_new(points, self.n)
+        if not self._h:
+            raise ValueError("duplicate interpolation point")
+
+    def close(self):
+        if self._h:
+            lib().oracle_tree_free(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def vanishing(self) -> bytes:
+        out = _buf(32 * (self.n + 1))
+        k = lib().oracle_tree_vanishing(self._h, out)
+        return out.raw[:32 * k]
+
+    def inverse_derivatives(self) -> bytes:
+        out = _buf(max(32, 32 * self.n))
+        lib().oracle_tree_inverse_derivatives(self._h, out)
+        return out.raw[:32 * self.n]
+
+    def multipoint_eval(self, poly: bytes) -> bytes:
+        out = _buf(max(32, 32 * self.n))
+        assert lib().oracle_tree_eval(self._h, poly, len(poly) // 32, out) == 0
+        return out.raw[:32 * self.n]
+
+    def interpolate(self, values: bytes) -> bytes:
+        assert len(values) == 32 * self.n
+        out = _buf(max(32, 32 * self.n))
+        k = lib().oracle_tree_interpolate(self._h, values, out)
+        return out.raw[:32 * k]
+
+    def cauchy_sums(self, weights: bytes) -> bytes:
+        assert len(weights) == 32 * self.n
+        out = _buf(max(32, 32 * self.n))
+        lib().oracle_tree_cauchy(self._h, weights, out)
+        return out.raw[:32 * self.n]

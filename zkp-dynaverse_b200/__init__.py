@@ -163,6 +163,15 @@ SIGNATURES = [
     ("dvgpu_g2_random_twist_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
     ("dvgpu_bn254_g1_ntt_rows", ctypes.c_int, [_P, _P, _SZ, _SZ, ctypes.c_int, _B] + _E),
     ("dvgpu_bn254_g1_ntt_rows_device", ctypes.c_int, [_P, _P, _SZ, _SZ, ctypes.c_int, _P, _P] + _E),
+    ("dvgpu_bn254_poly_multiply", ctypes.c_int, [_P, _B, _SZ, _B, _SZ, _B, _SZ, ctypes.POINTER(_SZ)] + _E),
+    ("dvgpu_bn254_poly_divide_exact", ctypes.c_int, [_P, _B, _SZ, _B, _SZ, _B, _SZ, ctypes.POINTER(_SZ)] + _E),
+    ("dvgpu_bn254_tree_create", ctypes.c_int, [_P, _B, _SZ, ctypes.POINTER(ctypes.c_uint64)] + _E),
+    ("dvgpu_bn254_tree_destroy", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
+    ("dvgpu_bn254_tree_vanishing", ctypes.c_int, [_P, ctypes.c_uint64, _B, _SZ, ctypes.POINTER(_SZ)] + _E),
+    ("dvgpu_bn254_tree_inverse_derivatives", ctypes.c_int, [_P, ctypes.c_uint64, _B, _SZ] + _E),
+    ("dvgpu_bn254_tree_evaluate", ctypes.c_int, [_P, ctypes.c_uint64, _B, _SZ, _SZ, _B] + _E),
+    ("dvgpu_bn254_tree_interpolate", ctypes.c_int, [_P, ctypes.c_uint64, _B, _SZ, _SZ, _B, ctypes.POINTER(_SZ)] + _E),
+    ("dvgpu_bn254_tree_cauchy_sums", ctypes.c_int, [_P, ctypes.c_uint64, _B, _SZ, _SZ, _B] + _E),
     ("dvgpu_bn254_ntt_batch", ctypes.c_int, [_P, _P, _P, _P, _SZ, _B] + _E),
     ("dvgpu_bn254_ntt_batch_device", ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P] + _E),
     ("dvgpu_batch_plan_create", ctypes.c_int,
@@ -634,6 +643,30 @@ class DvgpuBackend:
     def g1_ntt_rows_device(self, d_points: int, row_len: int, rows: int, inverse: bool, d_out: int, stream=None):
         self._call("dvgpu_bn254_g1_ntt_rows_device", d_points, row_len, rows, int(inverse), d_out, stream)
 
+    # ------------------------------------------------------------------ polynomial toolkit
+    # crates/protocol/src/domain/fast.rs over canonical Fr coefficient bytes
+    # (lowest degree first); results trimmed as domain.rs:339-346.
+    def poly_multiply(self, left: bytes, right: bytes) -> bytes:
+        """fft_multiply_with_backend (fast.rs:213-234)."""
+        cap = max(1, (len(left) // FR_BYTES + len(right) // FR_BYTES - 1) if left and right else 1)
+        out = ctypes.create_string_buffer(FR_BYTES * cap)
+        n = ctypes.c_size_t()
+        self._call("dvgpu_bn254_poly_multiply", left, len(left) // FR_BYTES, right, len(right) // FR_BYTES, out, cap,
+                   ctypes.byref(n))
+        return out.raw[:FR_BYTES * n.value]
+
+    def poly_divide_exact(self, numerator: bytes, denominator: bytes) -> bytes:
+        """newton_divide_exact_with_backend (fast.rs:236-240)."""
+        cap = max(1, len(numerator) // FR_BYTES)
+        out = ctypes.create_string_buffer(FR_BYTES * cap)
+        n = ctypes.c_size_t()
+        self._call("dvgpu_bn254_poly_divide_exact", numerator, len(numerator) // FR_BYTES, denominator,
+                   len(denominator) // FR_BYTES, out, cap, ctypes.byref(n))
+        return out.raw[:FR_BYTES * n.value]
+
+    def tree_create(self, points: bytes) -> "SubproductTree":
+        return SubproductTree(self, points)
+
     # ------------------------------------------------------------------ resident buffers
     # RebuildBackend (crates/protocol/src/incremental_rebuild/operators.rs) over
     # the resident ABI, with the reference binding's field encoding
@@ -798,3 +831,60 @@ class DvgpuBackend:
         v = ctypes.c_double()
         self._call("dvgpu_probe_imad_rate", ctypes.byref(v))
         return v.value
+
+
+class SubproductTree:
+    """SubproductTree::new_with_backend (crates/protocol/src/domain/fast.rs:11-139)
+    held on the device: distinct canonical Fr points in input order."""
+
+    def __init__(self, backend: DvgpuBackend, points: bytes):
+        self.backend = backend
+        self.count = len(points) // FR_BYTES
+        h = ctypes.c_uint64()
+        backend._call("dvgpu_bn254_tree_create", points, self.count, ctypes.byref(h))
+        self.handle = h.value
+
+    def close(self):
+        if getattr(self, "handle", None) and getattr(self.backend, "handle", None):
+            self.backend._call("dvgpu_bn254_tree_destroy", self.handle)
+        self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def vanishing(self) -> bytes:
+        out = ctypes.create_string_buffer(FR_BYTES * (self.count + 1))
+        n = ctypes.c_size_t()
+        self.backend._call("dvgpu_bn254_tree_vanishing", self.handle, out, self.count + 1, ctypes.byref(n))
+        return out.raw[:FR_BYTES * n.value]
+
+    def inverse_derivatives(self) -> bytes:
+        out = ctypes.create_string_buffer(max(1, FR_BYTES * self.count))
+        self.backend._call("dvgpu_bn254_tree_inverse_derivatives", self.handle, out, self.count)
+        return out.raw[:FR_BYTES * self.count]
+
+    def multipoint_eval(self, polynomial: bytes, rows: int = 1) -> bytes:
+        """Values of `rows` polynomials (equal lengths, concatenated) at the points."""
+        length = len(polynomial) // (FR_BYTES * rows)
+        out = ctypes.create_string_buffer(max(1, FR_BYTES * self.count * rows))
+        self.backend._call("dvgpu_bn254_tree_evaluate", self.handle, polynomial, length, rows, out)
+        return out.raw[:FR_BYTES * self.count * rows]
+
+    def interpolate(self, values: bytes, rows: int = 1):
+        """Trimmed coefficients of each row (a list of bytes when rows > 1)."""
+        count = len(values) // (FR_BYTES * rows)
+        stride = max(1, self.count)
+        out = ctypes.create_string_buffer(FR_BYTES * stride * rows)
+        lens = (ctypes.c_size_t * rows)()
+        self.backend._call("dvgpu_bn254_tree_interpolate", self.handle, values, count, rows, out, lens)
+        res = [out.raw[FR_BYTES * stride * r:FR_BYTES * (stride * r + lens[r])] for r in range(rows)]
+        return res[0] if rows == 1 else res
+
+    def cauchy_sums(self, weights: bytes, rows: int = 1) -> bytes:
+        count = len(weights) // (FR_BYTES * rows)
+        out = ctypes.create_string_buffer(max(1, FR_BYTES * self.count * rows))
+        self.backend._call("dvgpu_bn254_tree_cauchy_sums", self.handle, weights, count, rows, out)
+        return out.raw[:FR_BYTES * self.count * rows]

@@ -189,6 +189,7 @@ __global__ void k_probe_madc(uint32_t seed, uint32_t iters, uint32_t* sink) {
 void Backend::release_all() noexcept {
     plans.clear();
     resident.reset();
+    poly.reset();
     bases.clear();
     MsmTimeline& tl = msm.timeline;
     for (auto& e : tl.ev)

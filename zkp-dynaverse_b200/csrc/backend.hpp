@@ -33,6 +33,7 @@ struct ResidentBases {
 };
 
 struct ResidentState;  // resident.cu
+struct PolyState;      // poly.cu
 
 struct Backend {
     int device = 0;
@@ -59,6 +60,7 @@ struct Backend {
     std::map<uint64_t, std::unique_ptr<ResidentBases>> bases;
     std::map<uint64_t, std::unique_ptr<BatchPlan>> plans;  // CUDA-graph batch plans
     std::shared_ptr<ResidentState> resident;                // resident transactional buffers
+    std::shared_ptr<PolyState> poly;                        // subproduct trees and polynomial scratch
     uint64_t next_handle = 1;
 
     void release_all() noexcept;
