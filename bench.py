@@ -29,6 +29,9 @@ output vector).
                         Peak = IMAD rate measured in this run.
   cpu_baseline        : the CPU oracle (C++ restatement of arkworks
                         semantics) on the same inputs, all host threads.
+  --op poly           : the polynomial field work of one sparse update over
+                        2^log-n affected points (host-buffer entry points;
+                        value = e2e).
   --impl reference    : that CPU implementation alone, on the same workload
                         (the reference's Rust + arkworks + ICICLE code cannot
                         be built in this image).
@@ -55,7 +58,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch", "g2check",
-                                                         "serve", "ecntt"])
+                                                         "serve", "ecntt", "poly"])
     ap.add_argument("--log-n", type=int, default=None)
     ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
     ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
@@ -68,11 +71,11 @@ def parse():
     a = ap.parse_args()
     if a.log_n is None:
         a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20, "batch": 18,
-                   "g2check": 16, "serve": 16, "ecntt": 12}[a.op]
+                   "g2check": 16, "serve": 16, "ecntt": 12, "poly": 12}[a.op]
     if a.steps is None:
         a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100,
                    "batch": 20, "g2check": 50, "serve": 1,
-                   "ecntt": 10}[a.op]
+                   "ecntt": 10, "poly": 20}[a.op]
     return a
 
 
@@ -945,11 +948,153 @@ class BatchOp:
         return None, ms, sample
 
 
+R_MOD = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+
+
+def fr_sub_bytes(a: bytes, b: bytes) -> bytes:
+    """subtract_polynomials (crates/protocol/src/domain.rs:169-179) on
+    canonical Fr coefficient bytes, vectorised: limb-wise borrow chain, + r
+    where negative, trimmed."""
+    import numpy as np
+    n = max(len(a), len(b), 32) // 32
+    x = np.zeros((n, 4), dtype=np.uint64)
+    y = np.zeros((n, 4), dtype=np.uint64)
+    x[:len(a) // 32] = np.frombuffer(a, dtype=np.uint64).reshape(-1, 4)
+    y[:len(b) // 32] = np.frombuffer(b, dtype=np.uint64).reshape(-1, 4)
+    r = np.array([(R_MOD >> (64 * i)) & (2**64 - 1) for i in range(4)], dtype=np.uint64)
+    out = np.zeros_like(x)
+    borrow = np.zeros(n, dtype=np.uint64)
+    for i in range(4):
+        t = x[:, i] - y[:, i]
+        b1 = (x[:, i] < y[:, i]).astype(np.uint64)
+        out[:, i] = t - borrow
+        borrow = b1 | ((t < borrow).astype(np.uint64))
+    neg = borrow == 1
+    carry = np.zeros(n, dtype=np.uint64)
+    for i in range(4):
+        t = out[:, i] + r[i]
+        c1 = (t < out[:, i]).astype(np.uint64)
+        s_ = t + carry
+        carry = c1 | (s_ < t).astype(np.uint64)
+        out[:, i] = np.where(neg, s_, out[:, i])
+    raw = out.tobytes()
+    k = n
+    while k > 1 and not any(raw[32 * (k - 1):32 * k]):
+        k -= 1
+    return raw[:32 * k]
+
+
+def poly_work_fme(a):
+    """Fr multiplications of one sparse-update polynomial step in the flat
+    kernels of poly.cu: vanishing values N a and derivatives a^2 at tree
+    creation; Cauchy pair sums 1 + 2R products per pair for R rows sharing
+    the den chain (one call of 1 row, one of 3); power sums a^2 per
+    interpolation row (9 rows); N = next_pow2(a).  Transforms, inversions,
+    additions and shuffles are not counted."""
+    big_n = max(2, 1 << (a - 1).bit_length())
+    return big_n * a + a * a + 3 * a * a + 7 * a * a + 9 * a * a
+
+
+class PolyOp:
+    """The field work of one sparse update over an affected set of a points
+    (crates/protocol/src/dynaverse/sparse.rs:125-236): subproduct tree,
+    Cauchy weights, nine interpolations (anchor/changed/zero-quotient locals
+    of the three multiplication wires), three Cauchy sums, the product
+    updated_0 updated_1 and its exact division by the vanishing polynomial.
+    Values are seeded uniform Fr; the third wire's values are the products of
+    the first two at the points, so the division is exact as in the
+    reference."""
+
+    def __init__(self, args):
+        self.a = 1 << args.log_n
+        self.metric = f"sparse-update polynomial work a={self.a} ms"
+        self.workload = (f"SubproductTree over {self.a} points + Cauchy weights + 9 interpolations + 3 Cauchy "
+                         f"sums + product + exact division by the vanishing polynomial")
+        self.profile = f"poly_sparse_update_{self.a}"
+
+    def setup(self, torch, b, s, rank):
+        from oracle import oracle
+        a = self.a
+        self.points = oracle.uniform_fr(9100 + rank, a)
+        u0 = oracle.uniform_fr(9101, a)
+        u1 = oracle.uniform_fr(9102, a)
+        w = lambda buf, i: int.from_bytes(buf[32 * i:32 * i + 32], "little")
+        u2 = b"".join((w(u0, i) * w(u1, i) % R_MOD).to_bytes(32, "little") for i in range(a))
+        self.values9 = u0 + u1 + u2 + b"".join(oracle.uniform_fr(9110 + r, a) for r in range(6))
+        self.weighted3 = b"".join(oracle.uniform_fr(9120 + r, a) for r in range(3))
+        self.tune_log = None
+        self.config = {"points": a, "interpolation_rows": 9, "cauchy_rows": 4}
+        self.h2d = 32 * (a + 9 * a + 3 * a + a) + 0
+        self.d2h = 0
+
+    def run(self, b):
+        import hashlib
+        t = b.tree_create(self.points)
+        try:
+            weights = t.inverse_derivatives()
+            cauchy_weights = t.cauchy_sums(weights)
+            polys = t.interpolate(self.values9, 9)
+            cauchy_values = t.cauchy_sums(self.weighted3, 3)
+            product = b.poly_multiply(polys[0], polys[1])
+            quotient = b.poly_divide_exact(fr_sub_bytes(product, polys[2]), t.vanishing())
+        finally:
+            t.close()
+        self.last = (weights, cauchy_weights, polys, cauchy_values, quotient)
+        h = hashlib.sha256()
+        for part in (weights, cauchy_weights, b"".join(polys), cauchy_values, quotient):
+            h.update(part)
+        return h.hexdigest()
+
+    def step(self, b, s):
+        return self.run(b)
+
+    def host_inputs(self, torch):
+        pass
+
+    def e2e_step(self, dv, b):
+        return self.run(b)
+
+    def e2e_bytes(self):
+        a = self.a
+        # H2D: points, weights (cauchy), 9 value rows, 3 weight rows, two product
+        # operands, numerator and divisor; D2H: every returned vector
+        h2d = 32 * (a + a + 9 * a + 3 * a + 2 * a + 3 * a + (a + 1))
+        d2h = 32 * (a + a + 9 * a + 3 * a + 2 * a + (a + 1) + a)
+        return h2d, d2h
+
+    def roofline(self, tl, imad_peak, step_ms):
+        macs = poly_work_fme(self.a) * 136
+        ach = macs / (step_ms * 1e-3) / 1e12
+        return ({"bound": "imad", "kernel": "whole step (k_powsum power sums and k_fracsum pair sums dominant)", "achieved": ach,
+                 "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
+                 "algorithmic_macs_per_launch": macs, "launch_ms": step_ms}, None)
+
+    def cpu(self, oracle, threads):
+        t0 = time.perf_counter()
+        out = poly_cpu(oracle, self.points, self.values9, self.weighted3)
+        ms = (time.perf_counter() - t0) * 1e3
+        agree = out == self.last if hasattr(self, "last") else None
+        return None, ms, (f"one full step (a={self.a}) through the oracle's restatement of "
+                          f"domain/fast.rs, 1 thread; identical to the GPU's: {agree}")
+
+
+def poly_cpu(oracle, points, values9, weighted3):
+    a = len(points) // 32
+    with oracle.Tree(points) as t:
+        weights = t.inverse_derivatives()
+        cauchy_weights = t.cauchy_sums(weights)
+        polys = [t.interpolate(values9[32 * a * r:32 * a * (r + 1)]) for r in range(9)]
+        cauchy_values = b"".join(t.cauchy_sums(weighted3[32 * a * r:32 * a * (r + 1)]) for r in range(3))
+        product = oracle.poly_mul(polys[0], polys[1])
+        quotient = oracle.poly_div_exact(fr_sub_bytes(product, polys[2]), t.vanishing())
+    return weights, cauchy_weights, polys, cauchy_values, quotient
+
+
 def make_op(args):
     return {"msm": lambda: MsmOp(args), "msmres": lambda: ResidentMsmOp(args), "g2msm": lambda: MsmOp(args, g2=True),
             "ntt": lambda: NttOp(args), "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args),
             "batch": lambda: BatchOp(args), "g2check": lambda: G2CheckOp(args), "serve": lambda: ServeOp(args),
-            "ecntt": lambda: EcNttOp(args)}[args.op]()
+            "ecntt": lambda: EcNttOp(args), "poly": lambda: PolyOp(args)}[args.op]()
 
 
 # ----------------------------------------------------------------- reference arm
@@ -1019,6 +1164,16 @@ def run_reference(args, rank, world):
 
         metric = BatchOp(args).metric
         sample = "batch estimates"
+    elif op == "poly":
+        pop = PolyOp(args)
+
+        class _B:  # setup needs no device
+            pass
+        pop.setup(None, _B(), None, 0)
+        fn = lambda: poly_cpu(oracle, pop.points, pop.values9, pop.weighted3)
+        metric = pop.metric
+        sample = f"full sparse-update polynomial steps (a={pop.a}) through domain/fast.rs restated, 1 thread"
+        threads = 1
     else:
         sc = oracle.fr_powers(oracle.uniform_fr(2812, 1), n)
         fn = lambda: oracle.fixed_base_g1(sc, threads=threads)
@@ -1199,7 +1354,7 @@ def main():
         threads = os.cpu_count() or 1
         cpu_out, cpu_ms, sample = op.cpu(oracle, threads)
         line["cpu_baseline"] = {"value": cpu_ms * scale, "unit": unit,
-                                "cores": 1 if args.op == "ntt" else threads, "kind": "port", "sample": sample}
+                                "cores": 1 if args.op in ("ntt", "poly") else threads, "kind": "port", "sample": sample}
         if cpu_out is not None:
             line["cpu_baseline"]["matches_gpu"] = cpu_out == result
     if rank == 0:

@@ -25,18 +25,21 @@
 //    into the constant term and is moved back);
 //  * A'(x_i) = prod_{j != i} (x_i - x_j) directly; 1/A'(x_i) by Fermat.  A
 //    zero A'(x_i) means a repeated point;
-//  * interpolation f = sum_i c_i A/(X - x_i), c_i = v_i/A'(x_i): the values
-//    f(w^k) = sum_i c_i prod_{j != i} (w^k - x_j) come from the running
-//    pair (num, den) <- (num d + c den, den d), d = w^k - x_i, with no
-//    inversion (so also exact when w^k is one of the points), then one
-//    inverse NTT of size N >= n > deg f;
-//  * Cauchy sums sum_{j != i} w_j/(x_i - x_j): the same running pair over
-//    j != i at t = x_i, whose den is A'(x_i), times 1/A'(x_i);
+//  * interpolation f = sum_i c_i A/(X - x_i), c_i = v_i/A'(x_i): synthetic
+//    division gives A/(X - x_i) = sum_k X^k sum_{m>k} A_m x_i^(m-k-1), so
+//    f_k = sum_{m>k} A_m P_(m-k-1) with the power sums P_j = sum_i c_i x_i^j
+//    (j < n, one product per (i, j)); the Toeplitz sum is coefficients
+//    n .. 2n-1 of the product A * reverse(P), one NTT product of size
+//    next_pow2(2n) against the tree's transformed A;
+//  * Cauchy sums sum_{j != i} w_j/(x_i - x_j): the running pair
+//    (num, den) <- (num d + w_j den, den d), d = x_i - x_j, over j != i (no
+//    inversion); den ends as A'(x_i), so the sum is num / A'(x_i).  Rows
+//    of weights share the den chain (1 + 2R products per pair for R rows);
 //  * multipoint evaluation: Horner over chunks of coefficients, combined
 //    with x^B per chunk.
 //
-// The pair sums and Horner chunks are quadratic in the point count but run
-// as one launch over every SM (targets x source chunks x rows), where the
+// The pair sums, power sums and Horner chunks are quadratic in the point
+// count but run as one launch over every SM, where the
 // reference's remainder tree is a chain of small dependent products; for
 // the supports of sparse updates (up to a few thousand points) the flat
 // form is the faster one on this GPU.  Trees are capped at 2^20 points.
@@ -55,17 +58,19 @@
 namespace dv {
 
 struct PolyTree {
-    uint32_t n = 0, big_n = 0;  // points, transform size max(2, next_pow2(n))
+    uint32_t n = 0, big_n = 0;  // points, max(2, next_pow2(n))
+    uint32_t conv_n = 0;        // max(2, next_pow2(2 n)): the interpolation product size
     DevBuf xs;                  // Montgomery points
-    DevBuf domain;              // Montgomery w^k, k < big_n
     DevBuf deriv, invd;         // Montgomery A'(x_i), 1/A'(x_i)
     DevBuf vanishing;           // canonical A, n + 1 coefficients
+    DevBuf vanishing_hat;       // forward NTT of A padded to conv_n
 };
 
 struct PolyState {
     std::map<uint64_t, std::unique_ptr<PolyTree>> trees;
     DevBuf a, b, c, part_num, part_den, flag, shift;
-    NttBatch batch;
+    uint32_t shift_k = 0;       // the coset shift g^k held in `shift`
+    NttBatch batch, batch2;
 };
 
 namespace {
@@ -111,74 +116,78 @@ __global__ void k_domain(const Fr* __restrict__ tw, uint32_t big_n, Fr* __restri
     out[k] = k < half ? tw[k] : Fr::neg(tw[k - half]);
 }
 
-// Partial pair (num, den) of target t over the sources of chunk blockIdx.y:
-//   den = prod (T - x_j),  num = sum c_j prod_{l != j} (T - x_l)
-// (SELF: targets are the sources and j = t is left out).  c_j is the
-// canonical weight of row blockIdx.z, times 1/A'(x_j) when SCALED.
-template <bool SELF, bool WEIGHTED, bool SCALED>
+// Partial pair sums of target t over the sources of chunk blockIdx.y:
+//   den = prod (T - x_j),  num_r = sum c_(r,j) prod_(l != j) (T - x_l)
+// for the R weight rows of group blockIdx.z (R = 0: den alone); SELF: the
+// targets are the sources and j = t is left out.  num is canonical (the
+// weights are), den Montgomery.
+template <bool SELF, int R>
 __global__ void __launch_bounds__(PT) k_fracsum(const Fr* __restrict__ targets, uint32_t nt,
                                                 const Fr* __restrict__ xs, uint32_t n,
-                                                const Fr* __restrict__ cs, const Fr* __restrict__ invd,
-                                                uint32_t chunk, Fr* __restrict__ num_part,
-                                                Fr* __restrict__ den_part) {
+                                                const Fr* __restrict__ cs, uint32_t rows, uint32_t chunk,
+                                                Fr* __restrict__ num_part, Fr* __restrict__ den_part) {
+    constexpr int RS = R > 0 ? R : 1;
     __shared__ Fr sx[STAGE];
-    __shared__ Fr sc[WEIGHTED ? STAGE : 1];
+    __shared__ Fr sc[RS][R > 0 ? STAGE : 1];
     const uint32_t t = blockIdx.x * PT + threadIdx.x;
-    const uint32_t row = blockIdx.z;
+    const uint32_t row0 = blockIdx.z * RS;
     const uint32_t j0 = blockIdx.y * chunk, j1 = min(n, j0 + chunk);
     const bool live = t < nt;
     const Fr tv = live ? targets[t] : Fr::zero();
-    Fr num = Fr::zero(), den = Fr::one();
+    Fr num[RS];
+#pragma unroll
+    for (int r = 0; r < RS; ++r) num[r] = Fr::zero();
+    Fr den = Fr::one();
     for (uint32_t base = j0; base < j1; base += STAGE) {
         const uint32_t m = min(STAGE, j1 - base);
         __syncthreads();
         for (uint32_t s = threadIdx.x; s < m; s += PT) {
             sx[s] = xs[base + s];
-            if (WEIGHTED) {
-                Fr c = cs[(uint64_t)row * n + base + s];
-                if (SCALED) c = Fr::mul(c, invd[base + s]);
-                sc[s] = c;
-            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                sc[r][s] = row0 + r < rows ? cs[(uint64_t)(row0 + r) * n + base + s] : Fr::zero();
         }
         __syncthreads();
         if (!live) continue;
         for (uint32_t s = 0; s < m; ++s) {
             if (SELF && base + s == t) continue;
             const Fr d = Fr::sub(tv, sx[s]);
-            if (WEIGHTED) {
-                const Fr::Pair p = Fr::mul2(num, d, sc[WEIGHTED ? s : 0], den);
-                num = Fr::add(p.r0, p.r1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const Fr::Pair p = Fr::mul2(num[r], d, sc[r][s], den);
+                num[r] = Fr::add(p.r0, p.r1);
             }
             den = Fr::mul(den, d);
         }
     }
-    if (live) {
-        const uint64_t o = ((uint64_t)row * gridDim.y + blockIdx.y) * nt + t;
-        if (WEIGHTED) num_part[o] = num;
-        den_part[o] = den;
-    }
+    if (!live) return;
+    const uint32_t chunks = gridDim.y;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (row0 + r < rows) num_part[((uint64_t)(row0 + r) * chunks + blockIdx.y) * nt + t] = num[r];
+    den_part[((uint64_t)blockIdx.z * chunks + blockIdx.y) * nt + t] = den;
 }
 
-enum FracOut { OUT_DEN_CANON, OUT_DEN_MONT, OUT_NUM, OUT_NUM_TIMES_INVD };
+enum FracOut { OUT_DEN_CANON, OUT_DEN_MONT, OUT_NUM_TIMES_INVD };
 
 // Folds the chunk pairs of every (row, target): (n1, d1) + (n2, d2) =
-// (n1 d2 + n2 d1, d1 d2).
-template <bool WEIGHTED, int OUT>
+// (n1 d2 + n2 d1, d1 d2); rows of group z = row / R share its den partials.
+template <int R, int OUT>
 __global__ void __launch_bounds__(PT) k_frac_combine(const Fr* __restrict__ num_part,
                                                      const Fr* __restrict__ den_part, uint32_t nt,
                                                      uint32_t chunks, uint32_t rows, const Fr* __restrict__ invd,
                                                      Fr* __restrict__ out, uint32_t* __restrict__ zero_at) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (uint64_t)rows * nt) return;
+    if (i >= (uint64_t)(R > 0 ? rows : 1) * nt) return;
     const uint32_t row = (uint32_t)(i / nt), t = (uint32_t)(i % nt);
-    const uint64_t first = (uint64_t)row * chunks * nt + t;
-    Fr num = WEIGHTED ? num_part[first] : Fr::zero();
-    Fr den = den_part[first];
+    const uint64_t dfirst = (uint64_t)(R > 0 ? row / R : 0) * chunks * nt + t;
+    const uint64_t nfirst = (uint64_t)row * chunks * nt + t;
+    Fr num = R > 0 ? num_part[nfirst] : Fr::zero();
+    Fr den = den_part[dfirst];
     for (uint32_t c = 1; c < chunks; ++c) {
-        const uint64_t o = first + (uint64_t)c * nt;
-        const Fr d2 = den_part[o];
-        if (WEIGHTED) {
-            const Fr::Pair p = Fr::mul2(num, d2, num_part[o], den);
+        const Fr d2 = den_part[dfirst + (uint64_t)c * nt];
+        if (R > 0) {
+            const Fr::Pair p = Fr::mul2(num, d2, num_part[nfirst + (uint64_t)c * nt], den);
             num = Fr::add(p.r0, p.r1);
         }
         den = Fr::mul(den, d2);
@@ -188,8 +197,68 @@ __global__ void __launch_bounds__(PT) k_frac_combine(const Fr* __restrict__ num_
         out[i] = den;
         if (den.is_zero()) atomicMin(zero_at, t);
     }
-    if (OUT == OUT_NUM) out[i] = num;
     if (OUT == OUT_NUM_TIMES_INVD) out[i] = Fr::mul(num, invd[t]);
+}
+
+constexpr int PS_G = 8;  // powers per round: one PS_G x PT tile in shared memory
+
+// Partial power sums P_j = sum_i c_i x_i^j, c_i = v_i / A'(x_i), over the PT
+// points of block blockIdx.x, for j in [blockIdx.y jt, +jt) of row
+// blockIdx.z.  Each round a thread writes c_i x_i^j for PS_G consecutive j;
+// then each tile row is summed by 16 threads (8 values each, columns 16
+// apart so a half-warp reads consecutive elements) and a half-warp butterfly.
+__global__ void __launch_bounds__(PT) k_powsum(const Fr* __restrict__ xs, uint32_t n, const Fr* __restrict__ vals,
+                                               const Fr* __restrict__ invd, uint32_t jt, Fr* __restrict__ part) {
+    __shared__ Fr tile[PS_G][PT];
+    const uint32_t i = blockIdx.x * PT + threadIdx.x;
+    const uint32_t row = blockIdx.z;
+    const uint32_t j0 = blockIdx.y * jt, j1 = min(n, j0 + jt);
+    Fr x = Fr::zero(), y = Fr::zero();
+    if (i < n) {
+        x = xs[i];
+        const Fr c = Fr::mul(vals[(uint64_t)row * n + i], invd[i]);  // canonical
+        y = Fr::mul(c, pow_u32(x, j0));
+    }
+    const uint32_t g = threadIdx.x >> 4, seg = threadIdx.x & 15;
+    for (uint32_t j = j0; j < j1; j += PS_G) {
+#pragma unroll
+        for (int k = 0; k < PS_G; ++k) {
+            tile[k][threadIdx.x] = y;
+            y = Fr::mul(y, x);
+        }
+        __syncthreads();
+        Fr acc = tile[g][seg];
+#pragma unroll
+        for (int k = 1; k < PT / 16; ++k) acc = Fr::add(acc, tile[g][seg + 16 * k]);
+#pragma unroll
+        for (int off = 8; off >= 1; off >>= 1) {
+            Fr o;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) o.v[w] = __shfl_xor_sync(0xffffffffu, acc.v[w], off);
+            acc = Fr::add(acc, o);
+        }
+        if (seg == 0 && j + g < j1) part[((uint64_t)row * gridDim.x + blockIdx.x) * n + j + g] = acc;
+        __syncthreads();
+    }
+}
+
+// P_j of every row (sum of the block partials), stored reversed at
+// conv[row conv_n + n - 1 - j] (the rest of the row is zero).
+__global__ void __launch_bounds__(PT) k_powsum_combine(const Fr* __restrict__ part, uint32_t blocks, uint32_t n,
+                                                       uint32_t rows, uint32_t conv_n, Fr* __restrict__ conv) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)rows * n) return;
+    const uint32_t row = (uint32_t)(i / n), j = (uint32_t)(i % n);
+    const uint64_t first = (uint64_t)row * blocks * n + j;
+    Fr acc = part[first];
+    for (uint32_t b = 1; b < blocks; ++b) acc = Fr::add(acc, part[first + (uint64_t)b * n]);
+    conv[(uint64_t)row * conv_n + (n - 1 - j)] = acc;
+}
+
+// a[row conv_n + i] <- a[row conv_n + i] h[i] (canonical).
+__global__ void k_pointwise_rows(Fr* __restrict__ a, const Fr* __restrict__ h, uint32_t conv_n, uint32_t rows) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < (uint64_t)rows * conv_n) a[i] = Fr::mul(Fr::mul(a[i], Fr::r2()), h[i % conv_n]);
 }
 
 __global__ void k_invert(const Fr* __restrict__ in, uint32_t n, Fr* __restrict__ out) {
@@ -361,32 +430,34 @@ uint32_t source_chunk(uint64_t targets, uint32_t rows, uint32_t n) {
     return (uint32_t)std::max<uint64_t>(1, chunk);
 }
 
-// Pair sums over all sources for every (row, target), folded into `out`.
-template <bool SELF, bool WEIGHTED, bool SCALED, int OUT>
+// Pair sums over all sources for every (row, target), folded into `out`;
+// R weight rows per thread group (R = 0: den alone).
+template <bool SELF, int R, int OUT>
 void fracsum(PolyState& ps, const Fr* targets, uint32_t nt, const Fr* xs, uint32_t n, const Fr* cs, uint32_t rows,
              const Fr* invd, Fr* out, uint32_t* zero_at, cudaStream_t st) {
-    const uint32_t chunk = source_chunk(nt, rows, n);
+    const uint32_t groups = R > 0 ? (rows + R - 1) / R : 1;
+    const uint32_t chunk = source_chunk(nt, groups, n);
     const uint32_t chunks = n ? (n + chunk - 1) / chunk : 1;
-    const uint64_t parts = (uint64_t)rows * chunks * nt;
-    Fr* pn = WEIGHTED ? ps.part_num.as<Fr>(parts) : nullptr;
-    Fr* pd = ps.part_den.as<Fr>(parts);
-    const dim3 grid(blocks_for(nt), chunks, rows);
-    k_fracsum<SELF, WEIGHTED, SCALED><<<grid, PT, 0, st>>>(targets, nt, xs, n, cs, invd, chunk, pn, pd);
+    Fr* pn = R > 0 ? ps.part_num.as<Fr>((uint64_t)rows * chunks * nt) : nullptr;
+    Fr* pd = ps.part_den.as<Fr>((uint64_t)groups * chunks * nt);
+    k_fracsum<SELF, R><<<dim3(blocks_for(nt), chunks, groups), PT, 0, st>>>(targets, nt, xs, n, cs, rows, chunk, pn,
+                                                                           pd);
     DV_LAUNCH();
-    k_frac_combine<WEIGHTED, OUT><<<blocks_for((uint64_t)rows * nt), PT, 0, st>>>(pn, pd, nt, chunks, rows, invd,
-                                                                                  out, zero_at);
+    k_frac_combine<R, OUT><<<blocks_for((uint64_t)(R > 0 ? rows : 1) * nt), PT, 0, st>>>(pn, pd, nt, chunks, rows,
+                                                                                         invd, out, zero_at);
     DV_LAUNCH();
 }
 
-// Transforms `rows` consecutive vectors of 2^logn canonical elements in place.
-void ntt_rows(Backend& b, PolyState& ps, Fr* data, int logn, uint32_t rows, int kind, cudaStream_t st) {
+// Transforms `rows` consecutive vectors of 2^logn canonical elements in place
+// (one persistent batch launch; ntt_batch_check after the stream is done).
+void ntt_rows(Backend& b, NttBatch& batch, Fr* data, int logn, uint32_t rows, int kind, cudaStream_t st) {
     std::vector<NttBatchItem> items(rows);
     for (uint32_t r = 0; r < rows; ++r) {
         uint8_t* p = reinterpret_cast<uint8_t*>(data + ((uint64_t)r << logn));
         items[r] = NttBatchItem{p, p, logn, kind};
     }
-    ntt_batch_prepare(b.ntt, ps.batch, items, st);
-    ntt_batch_enqueue(ps.batch, st);
+    ntt_batch_prepare(b.ntt, batch, items, st);
+    ntt_batch_enqueue(batch, st);
 }
 
 PolyTree& tree_of(PolyState& ps, uint64_t h) {
@@ -395,13 +466,15 @@ PolyTree& tree_of(PolyState& ps, uint64_t h) {
     return *it->second;
 }
 
-// SubproductTree::new (fast.rs:38-62): vanishing polynomial and inverse
-// derivative values of `count` distinct canonical points.
+// SubproductTree::new (fast.rs:38-62): vanishing polynomial (and its
+// transform of size conv_n) and inverse derivative values of `count`
+// distinct canonical points.
 std::unique_ptr<PolyTree> tree_build(Backend& b, PolyState& ps, const uint8_t* points, uint32_t count,
                                      cudaStream_t st) {
     auto t = std::make_unique<PolyTree>();
     t->n = count;
     t->big_n = (uint32_t)std::max<uint64_t>(2, 1ull << log2_ceil(count));
+    t->conv_n = (uint32_t)std::max<uint64_t>(2, 1ull << log2_ceil(2ull * count));
     const int logn = log2_ceil(t->big_n);
     Fr* van = t->vanishing.as<Fr>((uint64_t)t->big_n + 1);
     if (count == 0) {
@@ -410,28 +483,77 @@ std::unique_ptr<PolyTree> tree_build(Backend& b, PolyState& ps, const uint8_t* p
         DV_CUDA(cudaStreamSynchronize(st));
         return t;
     }
-    Fr* stage = ps.a.as<Fr>(count);
+    Fr* stage = ps.a.as<Fr>(std::max<uint64_t>(count, t->big_n));
     DV_CUDA(cudaMemcpyAsync(stage, points, 32ull * count, cudaMemcpyHostToDevice, st));
     Fr* xs = t->xs.as<Fr>(count);
     k_to_mont<<<blocks_for(count), PT, 0, st>>>(stage, count, xs);
     DV_LAUNCH();
-    Fr* dom = t->domain.as<Fr>(t->big_n);
+    Fr* dom = stage;  // the points are converted: reuse the staging buffer for w^k
     const Fr* tw = ntt_tables(b.ntt, logn, NTT_FORWARD, st).tw.as<Fr>(1);
     k_domain<<<blocks_for(t->big_n), PT, 0, st>>>(tw, t->big_n, dom);
     DV_LAUNCH();
-    fracsum<false, false, false, OUT_DEN_CANON>(ps, dom, t->big_n, xs, count, nullptr, 1, nullptr, van, nullptr, st);
-    ntt_rows(b, ps, van, logn, 1, NTT_INVERSE, st);
+    fracsum<false, 0, OUT_DEN_CANON>(ps, dom, t->big_n, xs, count, nullptr, 1, nullptr, van, nullptr, st);
+    ntt_rows(b, ps.batch, van, logn, 1, NTT_INVERSE, st);
     k_vanishing_fix<<<1, 32, 0, st>>>(van, count, t->big_n);
     DV_LAUNCH();
+    Fr* hat = t->vanishing_hat.as<Fr>(t->conv_n);
+    DV_CUDA(cudaMemsetAsync(hat, 0, 32ull * t->conv_n, st));
+    DV_CUDA(cudaMemcpyAsync(hat, van, 32ull * (count + 1), cudaMemcpyDeviceToDevice, st));
+    ntt_rows(b, ps.batch2, hat, log2_ceil(t->conv_n), 1, NTT_FORWARD, st);
     uint32_t* zero_at = ps.flag.as<uint32_t>(1);
     DV_CUDA(cudaMemsetAsync(zero_at, 0xff, sizeof(uint32_t), st));
     Fr* deriv = t->deriv.as<Fr>(count);
-    fracsum<true, false, false, OUT_DEN_MONT>(ps, xs, count, xs, count, nullptr, 1, nullptr, deriv, zero_at, st);
+    fracsum<true, 0, OUT_DEN_MONT>(ps, xs, count, xs, count, nullptr, 1, nullptr, deriv, zero_at, st);
     k_invert<<<blocks_for(count), PT, 0, st>>>(deriv, count, t->invd.as<Fr>(count));
     DV_LAUNCH();
     ntt_batch_check(ps.batch, st);
+    ntt_batch_check(ps.batch2, st);
     if (read_err_word(b, zero_at, st) != 0xffffffffu) throw InvalidArgument("duplicate interpolation point");
     return t;
+}
+
+// Cauchy sums of `rows` weight rows (device, canonical) into out (rows x n).
+void cauchy_rows(PolyState& ps, PolyTree& t, const Fr* w, uint32_t rows, Fr* out, cudaStream_t st) {
+    const Fr* xs = t.xs.view<Fr>();
+    const Fr* invd = t.invd.view<Fr>();
+    if (rows >= 4)
+        fracsum<true, 4, OUT_NUM_TIMES_INVD>(ps, xs, t.n, xs, t.n, w, rows, invd, out, nullptr, st);
+    else if (rows == 3)
+        fracsum<true, 3, OUT_NUM_TIMES_INVD>(ps, xs, t.n, xs, t.n, w, rows, invd, out, nullptr, st);
+    else if (rows == 2)
+        fracsum<true, 2, OUT_NUM_TIMES_INVD>(ps, xs, t.n, xs, t.n, w, rows, invd, out, nullptr, st);
+    else
+        fracsum<true, 1, OUT_NUM_TIMES_INVD>(ps, xs, t.n, xs, t.n, w, rows, invd, out, nullptr, st);
+}
+
+// Interpolation of `rows` value rows (device, canonical): the coefficients
+// of row r end up at conv[r conv_n + n ..], n of them.
+Fr* interpolate_rows(Backend& b, PolyState& ps, PolyTree& t, const Fr* vals, uint32_t rows, cudaStream_t st) {
+    const uint32_t n = t.n;
+    const uint32_t blocks = blocks_for(n);
+    // j tiles: enough blocks for every SM, at least 128 powers per tile (the
+    // tile's starting power x^j0 costs about 2 log2 j0 products)
+    const uint64_t goal = (uint64_t)sm_count() * 8;
+    uint64_t tiles = (goal + (uint64_t)blocks * rows - 1) / ((uint64_t)blocks * rows);
+    tiles = std::max<uint64_t>(1, std::min<uint64_t>(tiles, (n + 127) / 128));
+    uint32_t jt = (uint32_t)((n + tiles - 1) / tiles);
+    jt = (jt + PS_G - 1) / PS_G * PS_G;
+    tiles = (n + jt - 1) / jt;
+    Fr* part = ps.part_num.as<Fr>((uint64_t)rows * blocks * n);
+    k_powsum<<<dim3(blocks, (uint32_t)tiles, rows), PT, 0, st>>>(t.xs.view<Fr>(), n, vals, t.invd.view<Fr>(), jt,
+                                                                 part);
+    DV_LAUNCH();
+    Fr* conv = ps.c.as<Fr>((uint64_t)rows * t.conv_n);
+    DV_CUDA(cudaMemsetAsync(conv, 0, 32ull * rows * t.conv_n, st));
+    k_powsum_combine<<<blocks_for((uint64_t)rows * n), PT, 0, st>>>(part, blocks, n, rows, t.conv_n, conv);
+    DV_LAUNCH();
+    const int logc = log2_ceil(t.conv_n);
+    ntt_rows(b, ps.batch, conv, logc, rows, NTT_FORWARD, st);
+    k_pointwise_rows<<<blocks_for((uint64_t)rows * t.conv_n), PT, 0, st>>>(conv, t.vanishing_hat.view<Fr>(),
+                                                                           t.conv_n, rows);
+    DV_LAUNCH();
+    ntt_rows(b, ps.batch2, conv, logc, rows, NTT_INVERSE, st);
+    return conv;
 }
 
 void copy_out(void* dst, const void* src, uint64_t bytes, cudaStream_t st) {
@@ -469,11 +591,11 @@ extern "C" int dvgpu_bn254_poly_multiply(void* opaque, const uint8_t* left, size
         DV_CUDA(cudaMemsetAsync(two, 0, 64 * big_n, st));
         DV_CUDA(cudaMemcpyAsync(l, left, 32 * left_len, cudaMemcpyHostToDevice, st));
         DV_CUDA(cudaMemcpyAsync(r, right, 32 * right_len, cudaMemcpyHostToDevice, st));
-        ntt_rows(b, ps, two, logn, 2, NTT_FORWARD, st);
+        ntt_rows(b, ps.batch, two, logn, 2, NTT_FORWARD, st);
         k_pointwise<<<blocks_for(big_n), PT, 0, st>>>(l, r, big_n);
         DV_LAUNCH();
         ntt_batch_check(ps.batch, st);
-        ntt_rows(b, ps, l, logn, 1, NTT_INVERSE, st);
+        ntt_rows(b, ps.batch, l, logn, 1, NTT_INVERSE, st);
         copy_out(result, l, 32 * out_len, st);
         ntt_batch_check(ps.batch, st);  // synchronises
         *result_len = trimmed(result, out_len);
@@ -510,7 +632,7 @@ extern "C" int dvgpu_bn254_poly_divide_exact(void* opaque, const uint8_t* numera
         const uint64_t big_n = 1ull << logn;
         Fr* orig = ps.b.as<Fr>(2 * big_n);  // numerator | denominator coefficients
         Fr* work = ps.a.as<Fr>(2 * big_n);  // their coset values
-        Fr* shift = ps.shift.as<Fr>(2);
+        Fr* shift = ps.shift.as<Fr>(2);  // grow-only: allocated once, so a cached shift stays valid
         uint32_t* flag = ps.flag.as<uint32_t>(1);
         DV_CUDA(cudaMemcpyAsync(orig, numerator, 32 * nl, cudaMemcpyHostToDevice, st));
         DV_CUDA(cudaMemcpyAsync(orig + big_n, denominator, 32 * dl, cudaMemcpyHostToDevice, st));
@@ -518,20 +640,23 @@ extern "C" int dvgpu_bn254_poly_divide_exact(void* opaque, const uint8_t* numera
         // A coset meets at most dl - 1 roots of the divisor, so dl shifts suffice.
         for (uint32_t k = 1;; ++k) {
             require(k <= dl, "no coset avoids the divisor's roots");
-            k_shift<<<1, 32, 0, st>>>(k, shift);
-            DV_LAUNCH();
+            if (ps.shift_k != k) {
+                k_shift<<<1, 32, 0, st>>>(k, shift);
+                DV_LAUNCH();
+                ps.shift_k = k;
+            }
             k_scale_powers<<<scale_blocks, PT, 0, st>>>(orig, nl, work, big_n, shift, big_n, nullptr);
             DV_LAUNCH();
             k_scale_powers<<<scale_blocks, PT, 0, st>>>(orig + big_n, dl, work + big_n, big_n, shift, big_n, nullptr);
             DV_LAUNCH();
-            ntt_rows(b, ps, work, logn, 2, NTT_FORWARD, st);
+            ntt_rows(b, ps.batch, work, logn, 2, NTT_FORWARD, st);
             DV_CUDA(cudaMemsetAsync(flag, 0, sizeof(uint32_t), st));
             k_div_values<<<blocks_for((big_n + DIV_RUN - 1) / DIV_RUN), PT, 0, st>>>(work, work + big_n, big_n, flag);
             DV_LAUNCH();
             ntt_batch_check(ps.batch, st);
             if (read_err_word(b, flag, st) == 0) break;
         }
-        ntt_rows(b, ps, work, logn, 1, NTT_INVERSE, st);
+        ntt_rows(b, ps.batch, work, logn, 1, NTT_INVERSE, st);
         DV_CUDA(cudaMemsetAsync(flag, 0, sizeof(uint32_t), st));
         // unscale by s^-j into the spare half and flag any coefficient at or above qlen
         k_scale_powers<<<scale_blocks, PT, 0, st>>>(work, big_n, work + big_n, big_n, shift + 1, qlen, flag);
@@ -641,7 +766,7 @@ extern "C" int dvgpu_bn254_tree_interpolate(void* opaque, uint64_t tree, const u
         require(count == t.n, "interpolation value count differs from points");
         require(rows >= 1 && rows <= 65535 && (values || !count) && coefficients && lengths,
                 "invalid interpolation arguments");
-        require((uint64_t)rows * t.big_n <= ROWS_MAX, "interpolation batch larger than 2^26 elements");
+        require((uint64_t)rows * t.conv_n <= ROWS_MAX, "interpolation batch larger than 2^26 elements");
         require_canonical(values, (uint64_t)count * rows, "interpolation value");
         if (!t.n) {
             memset(coefficients, 0, 32 * rows);
@@ -649,16 +774,13 @@ extern "C" int dvgpu_bn254_tree_interpolate(void* opaque, uint64_t tree, const u
             return;
         }
         const cudaStream_t st = b.stream;
-        const int logn = log2_ceil(t.big_n);
         Fr* vals = ps.b.as<Fr>((uint64_t)rows * t.n);
         DV_CUDA(cudaMemcpyAsync(vals, values, 32ull * rows * t.n, cudaMemcpyHostToDevice, st));
-        Fr* out = ps.c.as<Fr>((uint64_t)rows * t.big_n);
-        fracsum<false, true, true, OUT_NUM>(ps, t.domain.view<Fr>(), t.big_n, t.xs.view<Fr>(), t.n, vals,
-                                            (uint32_t)rows, t.invd.view<Fr>(), out, nullptr, st);
-        ntt_rows(b, ps, out, logn, (uint32_t)rows, NTT_INVERSE, st);
-        DV_CUDA(cudaMemcpy2DAsync(coefficients, 32ull * t.n, out, 32ull * t.big_n, 32ull * t.n, rows,
+        const Fr* conv = interpolate_rows(b, ps, t, vals, (uint32_t)rows, st);
+        DV_CUDA(cudaMemcpy2DAsync(coefficients, 32ull * t.n, conv + t.n, 32ull * t.conv_n, 32ull * t.n, rows,
                                   cudaMemcpyDeviceToHost, st));
-        ntt_batch_check(ps.batch, st);  // synchronises
+        ntt_batch_check(ps.batch, st);
+        ntt_batch_check(ps.batch2, st);  // synchronises
         for (size_t r = 0; r < rows; ++r) lengths[r] = trimmed(coefficients + 32ull * t.n * r, t.n);
     });
 }
@@ -680,8 +802,7 @@ extern "C" int dvgpu_bn254_tree_cauchy_sums(void* opaque, uint64_t tree, const u
         Fr* w = ps.b.as<Fr>(total);
         DV_CUDA(cudaMemcpyAsync(w, weights, 32 * total, cudaMemcpyHostToDevice, st));
         Fr* out = ps.c.as<Fr>(total);
-        fracsum<true, true, false, OUT_NUM_TIMES_INVD>(ps, t.xs.view<Fr>(), t.n, t.xs.view<Fr>(), t.n, w,
-                                                       (uint32_t)rows, t.invd.view<Fr>(), out, nullptr, st);
+        cauchy_rows(ps, t, w, (uint32_t)rows, out, st);
         copy_out(sums, out, 32 * total, st);
         DV_CUDA(cudaStreamSynchronize(st));
     });
