@@ -262,6 +262,25 @@ int dvgpu_bn254_g1_ntt_rows(void* backend, const uint8_t* points, size_t row_len
 int dvgpu_bn254_g1_ntt_rows_device(void* backend, const uint8_t* d_points, size_t row_len, size_t rows, int inverse,
                                    uint8_t* d_results, void* stream, char* error, size_t error_capacity);
 
+/* ---------------------------------------------------------------- pairing checks
+ * The verifier's pairing-product checks (crates/protocol/src/verification.rs
+ * :37-144, PairingChecks::equal / equal_prepared / product_equal over
+ * Bn254::multi_miller_loop + final_exponentiation).  Terms are (G1 64 B,
+ * G2 128 B) wire points, canonical, on their curves (all zero = infinity,
+ * which contributes one); the caller negates right-hand G1 points as
+ * product_equal does.  Equation e holds iff the product over terms
+ * [offsets[e], offsets[e+1]) of e(P_k, Q_k) is one; verdicts[e] = 1 / 0.
+ * offsets has equations + 1 entries, offsets[0] = 0; at most 2^24 terms and
+ * equations.  An invalid point: -1 naming the term. */
+int dvgpu_bn254_pairing_check(void* backend, const uint8_t* g1, const uint8_t* g2, const uint64_t* offsets,
+                              size_t equations, uint8_t* verdicts, char* error, size_t error_capacity);
+/* e(P_i, Q_i) for n pairs: 384-byte GT elements, Fq12 in tower order
+ * (c0.c0.c0, c0.c0.c1, c0.c1.c0, ..., c1.c2.c1; Fq12 = Fq6 + Fq6 w,
+ * Fq6 = Fq2 + Fq2 v + Fq2 v^2), canonical 32-byte LE Fq.  The final
+ * exponent is (q^12 - 1)/r times 2z(6z^2 + 3z + 1). */
+int dvgpu_bn254_pairing(void* backend, const uint8_t* g1, const uint8_t* g2, size_t n, uint8_t* gt, char* error,
+                        size_t error_capacity);
+
 /* ---------------------------------------------------------------- polynomial toolkit
  * The field work of a sparse update (crates/protocol/src/domain/fast.rs,
  * called from crates/protocol/src/dynaverse/sparse.rs:125-236), which the

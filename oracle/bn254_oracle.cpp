@@ -28,6 +28,9 @@
 //    division, FFT products) over the NTT above.  Outputs are fixed by
 //    exact arithmetic, so the restatement follows the reference's algorithm
 //    step by step and is pinned by the reference tests' direct definitions.
+//  * Pairing: the optimal ate pairing and product checks of
+//    crates/protocol/src/verification.rs:37-144 (Bn254 multi_miller_loop +
+//    final_exponentiation), pinned to a pure-Python flat-Fq12 pairing.
 //  * Codec: canonical little-endian, all-zero = infinity
 //    (crates/gpu/src/codec.rs:25-111, crates/gpu/src/resident.rs:419-431).
 //
@@ -707,6 +710,7 @@ static Jac<OpsFq2> psi(const Jac<OpsFq2>& p) {
     return r;
 }
 static const uint64_t BN_SEED = 4965661367192848881ull;
+static const uint64_t BN_SEED_VALUE = BN_SEED;
 
 static bool subgroup_check(const Aff<OpsFq2>& a, uint32_t algorithm) {
     Jac<OpsFq2> p;
@@ -1044,7 +1048,225 @@ static void write_poly(uint8_t* b, const Poly& p) {
     for (size_t i = 0; i < p.size(); ++i) fe_to_bytes(FR, b + 32 * i, p[i]);
 }
 
-struct Init { Init() { init_psi(); } } init_once;
+// ------------------------------------------------------------------ pairing
+// Optimal ate pairing (what Bn254::multi_miller_loop + final_exponentiation
+// compute for crates/protocol/src/verification.rs:37-144).  Tower Fq6 =
+// Fq2[v]/(v^3 - xi), Fq12 = Fq6[w]/(w^2 - v), xi = 9 + u.  The Miller loop
+// keeps T in affine twist coordinates (one Fq2 inversion per step); the
+// line through T with slope lam, untwisted by (x, y) -> (x w^2, y w^3), at
+// P = (xp, yp) is yp - lam xp w + (lam xT - yT) w^3, i.e. the Fq6 pair
+// (yp, 0, 0) + (-lam xp, lam xT - yT, 0) w.  Final exponentiation: the easy
+// part (q^6 - 1)(q^2 + 1), then the exponent 2z(6z^2 + 3z + 1)(q^4 - q^2 +
+// 1)/r written in base q (Fuentes-Castaneda, Knapp, Rodriguez-Henriquez,
+// "Faster hashing to G2", SAC 2011), each digit by plain square-and-multiply.
+struct Fe6 { Fe2 c0, c1, c2; };
+struct Fe12 { Fe6 c0, c1; };
+typedef OpsFq2 F2;
+
+static Fe2 XI;
+static Fe2 FROB_W[6];  // xi^(k (q-1)/6), the q-power Frobenius of w^k is w^k FROB_W[k]
+
+static Fe2 f2_mul(const Fe2& a, const Fe2& b) { Fe2 r; F2::mul(r, a, b); return r; }
+static Fe2 f2_add(const Fe2& a, const Fe2& b) { Fe2 r; F2::add(r, a, b); return r; }
+static Fe2 f2_sub(const Fe2& a, const Fe2& b) { Fe2 r; F2::sub(r, a, b); return r; }
+static Fe2 f2_neg(const Fe2& a) { Fe2 r; F2::neg(r, a); return r; }
+static Fe2 f2_conj(const Fe2& a) { Fe2 r = a; fneg(FQ, r.c1, a.c1); return r; }
+static Fe2 f2_inv(const Fe2& a) { Fe2 r; F2::inv(r, a); return r; }
+static Fe2 f2_scale(const Fe2& a, const Fe& s) { Fe2 r; fmul(FQ, r.c0, a.c0, s); fmul(FQ, r.c1, a.c1, s); return r; }
+
+static Fe6 f6_add(const Fe6& a, const Fe6& b) { return {f2_add(a.c0, b.c0), f2_add(a.c1, b.c1), f2_add(a.c2, b.c2)}; }
+static Fe6 f6_sub(const Fe6& a, const Fe6& b) { return {f2_sub(a.c0, b.c0), f2_sub(a.c1, b.c1), f2_sub(a.c2, b.c2)}; }
+static Fe6 f6_neg(const Fe6& a) { return {f2_neg(a.c0), f2_neg(a.c1), f2_neg(a.c2)}; }
+static Fe6 f6_mul(const Fe6& a, const Fe6& b) {  // schoolbook, v^3 = xi
+    Fe6 r;
+    r.c0 = f2_add(f2_mul(a.c0, b.c0), f2_mul(XI, f2_add(f2_mul(a.c1, b.c2), f2_mul(a.c2, b.c1))));
+    r.c1 = f2_add(f2_add(f2_mul(a.c0, b.c1), f2_mul(a.c1, b.c0)), f2_mul(XI, f2_mul(a.c2, b.c2)));
+    r.c2 = f2_add(f2_add(f2_mul(a.c0, b.c2), f2_mul(a.c1, b.c1)), f2_mul(a.c2, b.c0));
+    return r;
+}
+static Fe6 f6_mul_v(const Fe6& a) { return {f2_mul(XI, a.c2), a.c0, a.c1}; }
+static Fe6 f6_inv(const Fe6& a) {
+    const Fe2 t0 = f2_sub(f2_mul(a.c0, a.c0), f2_mul(XI, f2_mul(a.c1, a.c2)));
+    const Fe2 t1 = f2_sub(f2_mul(XI, f2_mul(a.c2, a.c2)), f2_mul(a.c0, a.c1));
+    const Fe2 t2 = f2_sub(f2_mul(a.c1, a.c1), f2_mul(a.c0, a.c2));
+    const Fe2 d = f2_add(f2_mul(a.c0, t0), f2_mul(XI, f2_add(f2_mul(a.c2, t1), f2_mul(a.c1, t2))));
+    const Fe2 di = f2_inv(d);
+    return {f2_mul(t0, di), f2_mul(t1, di), f2_mul(t2, di)};
+}
+static Fe12 f12_one() {
+    Fe12 r;
+    r.c0 = {F2::one(), F2::zero_v(), F2::zero_v()};
+    r.c1 = {F2::zero_v(), F2::zero_v(), F2::zero_v()};
+    return r;
+}
+static Fe12 f12_mul(const Fe12& a, const Fe12& b) {
+    Fe12 r;
+    r.c0 = f6_add(f6_mul(a.c0, b.c0), f6_mul_v(f6_mul(a.c1, b.c1)));
+    r.c1 = f6_add(f6_mul(a.c0, b.c1), f6_mul(a.c1, b.c0));
+    return r;
+}
+static Fe12 f12_conj(const Fe12& a) { return {a.c0, f6_neg(a.c1)}; }
+static Fe12 f12_inv(const Fe12& a) {
+    const Fe6 d = f6_inv(f6_sub(f6_mul(a.c0, a.c0), f6_mul_v(f6_mul(a.c1, a.c1))));
+    return {f6_mul(a.c0, d), f6_neg(f6_mul(a.c1, d))};
+}
+static bool f12_eq(const Fe12& a, const Fe12& b) {
+    const Fe2* x = &a.c0.c0;
+    const Fe2* y = &b.c0.c0;
+    for (int i = 0; i < 6; ++i)
+        if (!F2::eq(x[i], y[i])) return false;
+    return true;
+}
+// q^k-power Frobenius: coefficient of w^j (c0.c0 = w^0, c0.c1 = w^2,
+// c0.c2 = w^4, c1.c0 = w^1, c1.c1 = w^3, c1.c2 = w^5) goes to
+// conj^k(a) (FROB_W[j])^(1 + q + .. + q^(k-1)).
+static Fe12 f12_frob(const Fe12& a, int k) {
+    Fe12 r = a;
+    Fe2* c = &r.c0.c0;
+    static const int wpow[6] = {0, 2, 4, 1, 3, 5};
+    for (int t = 0; t < k; ++t)
+        for (int i = 0; i < 6; ++i) c[i] = f2_mul(f2_conj(c[i]), FROB_W[wpow[i]]);
+    return r;
+}
+static Fe12 f12_pow(const Fe12& a, const uint64_t* e, int words) {
+    Fe12 r = f12_one();
+    for (int i = 64 * words - 1; i >= 0; --i) {
+        r = f12_mul(r, r);
+        if ((e[i / 64] >> (i % 64)) & 1) r = f12_mul(r, a);
+    }
+    return r;
+}
+static Fe12 line_at(const Fe2& lam, const Fe2& xt, const Fe2& yt, const Fe& xp, const Fe& yp) {
+    Fe12 l;
+    Fe2 c0 = F2::zero_v();
+    c0.c0 = yp;
+    l.c0 = {c0, F2::zero_v(), F2::zero_v()};
+    Fe xn;
+    fneg(FQ, xn, xp);
+    l.c1 = {f2_scale(lam, xn), f2_sub(f2_mul(lam, xt), yt), F2::zero_v()};
+    return l;
+}
+static int NAF_6Z2[70];
+static int NAF_LEN = 0;
+static void init_pairing() {
+    uint64_t c9[4] = {9, 0, 0, 0}, c1[4] = {1, 0, 0, 0};
+    to_mont(FQ, XI.c0, c9);
+    to_mont(FQ, XI.c1, c1);
+    uint64_t e6[4];
+    u128 rem = 0;
+    const uint64_t qm1[4] = {Q_LIMBS[0] - 1, Q_LIMBS[1], Q_LIMBS[2], Q_LIMBS[3]};
+    for (int i = 3; i >= 0; --i) {
+        u128 v = (rem << 64) | qm1[i];
+        e6[i] = (uint64_t)(v / 6);
+        rem = v % 6;
+    }
+    Fe2 g = F2::one(), base = XI;
+    for (int i = 0; i < 256; ++i) {
+        if ((e6[i / 64] >> (i % 64)) & 1) g = f2_mul(g, base);
+        base = f2_mul(base, base);
+    }
+    FROB_W[0] = F2::one();
+    for (int k = 1; k < 6; ++k) FROB_W[k] = f2_mul(FROB_W[k - 1], g);
+    // NAF of 6z + 2, least significant first
+    u128 k = (u128)6 * BN_SEED_VALUE + 2;
+    NAF_LEN = 0;
+    while (k) {
+        int d = 0;
+        if (k & 1) {
+            d = 2 - (int)(k & 3);
+            k = d > 0 ? k - 1 : k + 1;
+        }
+        NAF_6Z2[NAF_LEN++] = d;
+        k >>= 1;
+    }
+}
+// Affine twist points; inf flags.
+static Fe12 miller_loop(const Aff<OpsFq>& p, const Aff<OpsFq2>& q) {
+    if (p.inf || q.inf) return f12_one();
+    Fe12 f = f12_one();
+    Fe2 xt = q.x, yt = q.y;
+    Fe2 three;
+    {
+        uint64_t c3[4] = {3, 0, 0, 0};
+        three = F2::zero_v();
+        to_mont(FQ, three.c0, c3);
+    }
+    auto add_line = [&](const Fe2& xs, const Fe2& ys) {
+        const Fe2 lam = f2_mul(f2_sub(ys, yt), f2_inv(f2_sub(xs, xt)));
+        f = f12_mul(f, line_at(lam, xt, yt, p.x, p.y));
+        const Fe2 x3 = f2_sub(f2_sub(f2_mul(lam, lam), xt), xs);
+        yt = f2_sub(f2_mul(lam, f2_sub(xt, x3)), yt);
+        xt = x3;
+    };
+    for (int i = NAF_LEN - 2; i >= 0; --i) {
+        const Fe2 lam = f2_mul(f2_mul(three, f2_mul(xt, xt)), f2_inv(f2_add(yt, yt)));
+        f = f12_mul(f12_mul(f, f), line_at(lam, xt, yt, p.x, p.y));
+        const Fe2 x3 = f2_sub(f2_mul(lam, lam), f2_add(xt, xt));
+        yt = f2_sub(f2_mul(lam, f2_sub(xt, x3)), yt);
+        xt = x3;
+        if (NAF_6Z2[i] == 1) add_line(q.x, q.y);
+        if (NAF_6Z2[i] == -1) add_line(q.x, f2_neg(q.y));
+    }
+    // pi(Q) = (conj(x) xi^((q-1)/3), conj(y) xi^((q-1)/2)); -pi^2(Q) likewise twice, y negated
+    const Fe2 x1 = f2_mul(f2_conj(q.x), FROB_W[2]), y1 = f2_mul(f2_conj(q.y), FROB_W[3]);
+    const Fe2 x2 = f2_mul(f2_conj(x1), FROB_W[2]), y2 = f2_neg(f2_mul(f2_conj(y1), FROB_W[3]));
+    add_line(x1, y1);
+    add_line(x2, y2);
+    return f;
+}
+// The four base-q digits of 2z(6z^2 + 3z + 1)(q^4 - q^2 + 1)/r, z = BN seed:
+// 12z^3 + 12z^2 + 6z + 1, 12z^3 + 6z^2 + 4z, 12z^3 + 6z^2 + 6z, 12z^3 + 6z^2 + 4z - 1.
+static void hard_digits(uint64_t d[4][4]) {
+    auto mul = [](const uint64_t* a, uint64_t m, uint64_t* o) {
+        u128 c = 0;
+        for (int i = 0; i < 4; ++i) { c += (u128)a[i] * m; o[i] = (uint64_t)c; c >>= 64; }
+    };
+    auto add = [](uint64_t* a, const uint64_t* b) {
+        u128 c = 0;
+        for (int i = 0; i < 4; ++i) { c += (u128)a[i] + b[i]; a[i] = (uint64_t)c; c >>= 64; }
+    };
+    const uint64_t z = BN_SEED_VALUE;
+    uint64_t z1[4] = {z, 0, 0, 0}, z2[4], z3[4];
+    mul(z1, z, z2);
+    mul(z2, z, z3);
+    const int coef[4][4] = {{12, 12, 6, 1}, {12, 6, 4, 0}, {12, 6, 6, 0}, {12, 6, 4, -1}};
+    for (int k = 0; k < 4; ++k) {
+        uint64_t acc[4] = {0, 0, 0, 0}, t[4];
+        mul(z3, coef[k][0], t); add(acc, t);
+        mul(z2, coef[k][1], t); add(acc, t);
+        mul(z1, coef[k][2], t); add(acc, t);
+        if (coef[k][3] > 0) { uint64_t one[4] = {1, 0, 0, 0}; add(acc, one); }
+        if (coef[k][3] < 0) {  // acc - 1 (acc > 0)
+            for (int i = 0; i < 4; ++i) { if (acc[i]--) break; }
+        }
+        memcpy(d[k], acc, 32);
+    }
+}
+static Fe12 final_exponentiation(const Fe12& f) {
+    Fe12 t = f12_mul(f12_conj(f), f12_inv(f));  // f^(q^6 - 1)
+    t = f12_mul(f12_frob(t, 2), t);             // ^(q^2 + 1)
+    uint64_t d[4][4];
+    hard_digits(d);
+    Fe12 r = f12_pow(t, d[0], 4);
+    for (int k = 1; k < 4; ++k) r = f12_mul(r, f12_frob(f12_pow(t, d[k], 4), k));
+    return r;
+}
+static void gt_write(uint8_t* out, const Fe12& a) {
+    const Fe2* c = &a.c0.c0;
+    for (int i = 0; i < 6; ++i) {
+        fe_to_bytes(FQ, out + 64 * i, c[i].c0);
+        fe_to_bytes(FQ, out + 64 * i + 32, c[i].c1);
+    }
+}
+// Reads one (G1, G2) term; false for a non-canonical or off-curve point.
+static bool pairing_term(const uint8_t* g1, const uint8_t* g2, Aff<OpsFq>& p, Aff<OpsFq2>& q) {
+    if (!g1_read(g1, p) || !g2_read(g2, q)) return false;
+    if (!p.inf && !on_curve(p, g1_b())) return false;
+    if (!q.inf && !on_curve(q, g2_b())) return false;
+    return true;
+}
+
+struct Init { Init() { init_psi(); init_pairing(); } } init_once;
 
 // ------------------------------------------------------------------ ChaCha20
 static inline uint32_t rotl(uint32_t v, int c) { return (v << c) | (v >> (32 - c)); }
@@ -1372,6 +1594,40 @@ void oracle_tree_cauchy(void* t, const uint8_t* weights, uint8_t* out) {
     Poly w;
     if (!read_poly(weights, tr->points.size(), w)) return;
     write_poly(out, tr->cauchy(w));
+}
+
+// e(P_i, Q_i) for n independent pairs (G1 64 B, G2 128 B wire form), GT
+// elements of 384 bytes.  -1 for an invalid point.
+int oracle_pairing(const uint8_t* g1, const uint8_t* g2, size_t n, uint8_t* out, int threads) {
+    std::atomic<int> bad{0};
+    parallel_for(n, num_threads(threads), [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) {
+            Aff<OpsFq> p;
+            Aff<OpsFq2> q;
+            if (!pairing_term(g1 + 64 * i, g2 + 128 * i, p, q)) { bad = 1; continue; }
+            gt_write(out + 384 * i, final_exponentiation(miller_loop(p, q)));
+        }
+    });
+    return bad ? -1 : 0;
+}
+// Equation e holds iff prod over terms [offsets[e], offsets[e + 1]) of
+// e(P_k, Q_k) is one (one final exponentiation per equation).
+int oracle_pairing_check(const uint8_t* g1, const uint8_t* g2, const uint64_t* offsets, size_t equations,
+                         uint8_t* verdicts, int threads) {
+    std::atomic<int> bad{0};
+    parallel_for(equations, num_threads(threads), [&](size_t lo, size_t hi) {
+        for (size_t e = lo; e < hi; ++e) {
+            Fe12 f = f12_one();
+            for (uint64_t k = offsets[e]; k < offsets[e + 1]; ++k) {
+                Aff<OpsFq> p;
+                Aff<OpsFq2> q;
+                if (!pairing_term(g1 + 64 * k, g2 + 128 * k, p, q)) { bad = 1; break; }
+                f = f12_mul(f, miller_loop(p, q));
+            }
+            verdicts[e] = f12_eq(final_exponentiation(f), f12_one()) ? 1 : 0;
+        }
+    });
+    return bad ? -1 : 0;
 }
 
 }  // extern "C"

@@ -61,6 +61,8 @@ def lib():
         L.oracle_tree_interpolate.argtypes = [ctypes.c_void_p, u8p, u8p]
         L.oracle_tree_interpolate.restype = sz
         L.oracle_tree_cauchy.argtypes = [ctypes.c_void_p, u8p, u8p]
+        L.oracle_pairing.argtypes = [u8p, u8p, sz, u8p, ctypes.c_int]
+        L.oracle_pairing_check.argtypes = [u8p, u8p, ctypes.c_void_p, sz, u8p, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -271,3 +273,26 @@ class Tree:
         out = _buf(max(32, 32 * self.n))
         lib().oracle_tree_cauchy(self._h, weights, out)
         return out.raw[:32 * self.n]
+
+
+# ---------------------------------------------------------------- pairing
+# Optimal ate pairing and product checks (crates/protocol/src/verification.rs:37-144).
+def pairing(g1: bytes, g2: bytes, threads=0) -> bytes:
+    """e(P_i, Q_i) for concatenated G1 (64 B) and G2 (128 B) points: 384-byte
+    GT elements in tower order."""
+    n = len(g1) // 64
+    assert len(g2) == 128 * n
+    out = _buf(max(1, 384 * n))
+    if lib().oracle_pairing(g1, g2, n, out, threads) != 0:
+        raise ValueError("oracle: invalid pairing input")
+    return out.raw[:384 * n]
+
+
+def pairing_check(g1: bytes, g2: bytes, offsets, threads=0):
+    """Verdicts of prod_{k in [offsets[e], offsets[e+1])} e(P_k, Q_k) == 1."""
+    off = np.ascontiguousarray(np.asarray(offsets, dtype=np.uint64))
+    eqs = len(off) - 1
+    out = _buf(max(1, eqs))
+    if lib().oracle_pairing_check(g1, g2, off.ctypes.data, eqs, out, threads) != 0:
+        raise ValueError("oracle: invalid pairing input")
+    return [bool(x) for x in out.raw[:eqs]]

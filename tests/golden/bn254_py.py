@@ -323,3 +323,108 @@ def g2_wire_mask(b, predicate=subgroup_full_order):
     if not g2_on_curve(p):
         return 2
     return 0 if predicate(p) else 4
+
+
+# ---------------------------------------------------------------- pairing
+# The optimal ate pairing with plain Python integers, for pinning the
+# oracle: Fq12 is the flat field Fq[w] / (w^12 - 18 w^6 + 82) (w^6 = xi =
+# 9 + u, u^2 = -1), lists of 12 coefficients.  The twist point T stays in
+# affine Fq2 coordinates; the line through T with slope lam, untwisted by
+# (x, y) -> (x w^2, y w^3), evaluated at P = (xp, yp) is
+#     yp - lam xp w + (lam xT - yT) w^3.
+# Loop: the NAF of 6z + 2, then the lines to pi(Q) and -pi^2(Q).  Final
+# exponentiation: (q^12 - 1)/r times 2z(6z^2 + 3z + 1) (the exponent of the
+# Fuentes-Castaneda, Knapp and Rodriguez-Henriquez hard part).
+F12_ONE = [1] + [0] * 11
+FINAL_EXP_MULTIPLE = 2 * BN_SEED * (6 * BN_SEED ** 2 + 3 * BN_SEED + 1)
+
+
+def f12mul(a, b):
+    t = [0] * 23
+    for i, x in enumerate(a):
+        if x:
+            for j, y in enumerate(b):
+                t[i + j] += x * y
+    for k in range(22, 11, -1):  # w^12 = 18 w^6 - 82
+        c = t[k]
+        if c:
+            t[k - 6] += 18 * c
+            t[k - 12] -= 82 * c
+    return [v % Q for v in t[:12]]
+
+
+def f12pow(a, e):
+    out = F12_ONE
+    while e:
+        if e & 1:
+            out = f12mul(out, a)
+        a = f12mul(a, a)
+        e >>= 1
+    return out
+
+
+def _f2_at(line, k, a):
+    """line += a w^k for a in Fq2 (u = w^6 - 9)."""
+    line[k] = (line[k] + a[0] - 9 * a[1]) % Q
+    line[k + 6] = (line[k + 6] + a[1]) % Q
+
+
+def _line(lam, t, p):
+    out = [0] * 12
+    out[0] = p[1] % Q
+    _f2_at(out, 1, f2neg(f2mul(lam, (p[0], 0))))
+    _f2_at(out, 3, f2sub(f2mul(lam, t[0]), t[1]))
+    return out
+
+
+def naf(k):
+    digits = []
+    while k:
+        if k & 1:
+            d = 2 - (k & 3)
+            k -= d
+        else:
+            d = 0
+        digits.append(d)
+        k >>= 1
+    return digits[::-1]  # most significant first
+
+
+def miller_loop(p, q):
+    if p is None or q is None:
+        return F12_ONE
+    t, f = q, F12_ONE
+    for d in naf(6 * BN_SEED + 2)[1:]:
+        lam = f2mul(f2mul((3, 0), f2mul(t[0], t[0])), f2inv(f2add(t[1], t[1])))
+        f = f12mul(f12mul(f, f), _line(lam, t, p))
+        t = g2_add(t, t)
+        if d:
+            s = q if d == 1 else g2_neg(q)
+            lam = f2mul(f2sub(s[1], t[1]), f2inv(f2sub(s[0], t[0])))
+            f = f12mul(f, _line(lam, t, p))
+            t = g2_add(t, s)
+    q1 = psi(q)
+    q2 = g2_neg(psi(q1))
+    for s in (q1, q2):
+        lam = f2mul(f2sub(s[1], t[1]), f2inv(f2sub(s[0], t[0])))
+        f = f12mul(f, _line(lam, t, p))
+        t = g2_add(t, s)
+    return f
+
+
+def final_exponentiation(f):
+    return f12pow(f, (Q ** 12 - 1) // R * FINAL_EXP_MULTIPLE)
+
+
+def pairing(p, q):
+    return final_exponentiation(miller_loop(p, q))
+
+
+def gt_bytes(f):
+    """Tower serialisation (c0.c0.c0, c0.c0.c1, c0.c1.c0, ..., c1.c2.c1), Fq12 =
+    Fq6 + Fq6 w, Fq6 = Fq2 + Fq2 v + Fq2 v^2, v = w^2: the Fq2 coefficient of
+    w^k is (f[k] + 9 f[k + 6], f[k + 6])."""
+    out = b""
+    for k in (0, 2, 4, 1, 3, 5):
+        out += fe_bytes((f[k] + 9 * f[k + 6]) % Q) + fe_bytes(f[k + 6])
+    return out

@@ -163,6 +163,8 @@ SIGNATURES = [
     ("dvgpu_g2_random_twist_device", ctypes.c_int, [_P, ctypes.c_uint64, _SZ, _P, _P] + _E),
     ("dvgpu_bn254_g1_ntt_rows", ctypes.c_int, [_P, _P, _SZ, _SZ, ctypes.c_int, _B] + _E),
     ("dvgpu_bn254_g1_ntt_rows_device", ctypes.c_int, [_P, _P, _SZ, _SZ, ctypes.c_int, _P, _P] + _E),
+    ("dvgpu_bn254_pairing_check", ctypes.c_int, [_P, _B, _B, _P, _SZ, _B] + _E),
+    ("dvgpu_bn254_pairing", ctypes.c_int, [_P, _B, _B, _SZ, _B] + _E),
     ("dvgpu_bn254_poly_multiply", ctypes.c_int, [_P, _B, _SZ, _B, _SZ, _B, _SZ, ctypes.POINTER(_SZ)] + _E),
     ("dvgpu_bn254_poly_divide_exact", ctypes.c_int, [_P, _B, _SZ, _B, _SZ, _B, _SZ, ctypes.POINTER(_SZ)] + _E),
     ("dvgpu_bn254_tree_create", ctypes.c_int, [_P, _B, _SZ, ctypes.POINTER(ctypes.c_uint64)] + _E),
@@ -642,6 +644,24 @@ class DvgpuBackend:
 
     def g1_ntt_rows_device(self, d_points: int, row_len: int, rows: int, inverse: bool, d_out: int, stream=None):
         self._call("dvgpu_bn254_g1_ntt_rows_device", d_points, row_len, rows, int(inverse), d_out, stream)
+
+    # ------------------------------------------------------------------ pairing checks
+    # crates/protocol/src/verification.rs:37-144
+    def pairing_check(self, g1: bytes, g2: bytes, offsets) -> list:
+        """Verdicts of prod_{k in [offsets[e], offsets[e+1])} e(P_k, Q_k) == 1."""
+        import numpy as np
+        off = np.ascontiguousarray(np.asarray(offsets, dtype=np.uint64))
+        eqs = len(off) - 1
+        out = ctypes.create_string_buffer(max(1, eqs))
+        self._call("dvgpu_bn254_pairing_check", g1, g2, off.ctypes.data, eqs, out)
+        return [bool(x) for x in out.raw[:eqs]]
+
+    def pairing(self, g1: bytes, g2: bytes) -> bytes:
+        """e(P_i, Q_i): 384-byte GT elements (tower order, canonical)."""
+        n = len(g1) // G1_BYTES
+        out = ctypes.create_string_buffer(max(1, 384 * n))
+        self._call("dvgpu_bn254_pairing", g1, g2, n, out)
+        return out.raw[:384 * n]
 
     # ------------------------------------------------------------------ polynomial toolkit
     # crates/protocol/src/domain/fast.rs over canonical Fr coefficient bytes
