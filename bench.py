@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch", "g2check",
-                                                         "serve", "ecntt", "poly"])
+                                                         "serve", "ecntt", "poly", "pairing"])
     ap.add_argument("--log-n", type=int, default=None)
     ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
     ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
@@ -71,11 +71,11 @@ def parse():
     a = ap.parse_args()
     if a.log_n is None:
         a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20, "batch": 18,
-                   "g2check": 16, "serve": 16, "ecntt": 12, "poly": 12}[a.op]
+                   "g2check": 16, "serve": 16, "ecntt": 12, "poly": 12, "pairing": 12}[a.op]
     if a.steps is None:
         a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100,
                    "batch": 20, "g2check": 50, "serve": 1,
-                   "ecntt": 10, "poly": 20}[a.op]
+                   "ecntt": 10, "poly": 20, "pairing": 20}[a.op]
     return a
 
 
@@ -1090,11 +1090,96 @@ def poly_cpu(oracle, points, values9, weighted3):
     return weights, cauchy_weights, polys, cauchy_values, quotient
 
 
+def pairing_fme(equations, terms_per_eq):
+    """Fq multiplications of the lane-group pairing as implemented, all six
+    lanes of a group counted: an Fq12 product is 36 Fq2 products (108
+    Fq-mul), a square 24 (72), a sparse line product 18 (54); every lane
+    repeats the twist doubling (35 Fq-mul) and addition (39).  Per term 65
+    doubling steps and 26 addition steps (the NAF of 6z + 2 and the two
+    Frobenius lines); per equation a final exponentiation of 3 x (62
+    squares + 27 products) plus about 42 products."""
+    dbl, add, sq, mul, line = 35 * 6, 39 * 6, 72, 108, 54
+    miller = 65 * (dbl + sq + line) + 26 * (add + line)
+    final = 3 * (62 * sq + 27 * mul) + 40 * mul + 2 * mul
+    return equations * (terms_per_eq * miller + (terms_per_eq - 1) * mul + final)
+
+
+class PairingOp:
+    """Pairing-product checks in the verifier's shape
+    (crates/protocol/src/verification.rs:55-103): each equation is a left
+    pair (aP, cQ) and a right pair (acP, Q) moved left with its G1 point
+    negated, one final exponentiation per equation; every third equation
+    has its scalar relation broken, so a third of the verdicts are false."""
+
+    def __init__(self, args):
+        self.eqs = 1 << args.log_n
+        self.metric = f"pairing checks, {self.eqs} equations x 2 terms, ms"
+        self.workload = (f"{self.eqs} BN254 pairing-product equations e(aP, cQ) e(-acP, Q) = 1 (one in three "
+                         f"broken), Miller loops + one final exponentiation each")
+        self.profile = f"pairing_check_{self.eqs}"
+
+    def setup(self, torch, b, s, rank):
+        from oracle import oracle
+        n = self.eqs
+        sa, sc = oracle.uniform_fr(6100 + rank, n), oracle.uniform_fr(6200 + rank, n)
+        ints = lambda buf: [int.from_bytes(buf[32 * i:32 * i + 32], "little") for i in range(n)]
+        a, c = ints(sa), ints(sc)
+        ac = b"".join(((x * y + (k % 3 == 1)) % R_MOD).to_bytes(32, "little") for k, (x, y) in enumerate(zip(a, c)))
+        q_mod = 0x30644E72E131A029B85045B68181585D97816A916871CA8D3C208C16D87CFD47
+        pa, pac = oracle.fixed_base_g1(sa), oracle.fixed_base_g1(ac)
+        qc = oracle.fixed_base_g2(sc)
+        gen2 = oracle.fixed_base_g2((1).to_bytes(32, "little"))
+        neg = lambda p: p[:32] + ((q_mod - int.from_bytes(p[32:], "little")) % q_mod).to_bytes(32, "little")
+        self.g1 = b"".join(pa[64 * i:64 * i + 64] + neg(pac[64 * i:64 * i + 64]) for i in range(n))
+        self.g2 = b"".join(qc[128 * i:128 * i + 128] + gen2 for i in range(n))
+        self.offsets = list(range(0, 2 * n + 1, 2))
+        self.tune_log = None
+        self.config = {"equations": n, "terms_per_equation": 2}
+
+    def run(self, b):
+        return tuple(b.pairing_check(self.g1, self.g2, self.offsets))
+
+    def step(self, b, s):
+        return self.run(b)
+
+    def host_inputs(self, torch):
+        pass
+
+    def e2e_step(self, dv, b):
+        return self.run(b)
+
+    def e2e_bytes(self):
+        return len(self.g1) + len(self.g2) + 8 * len(self.offsets), self.eqs
+
+    def roofline(self, tl, imad_peak, step_ms):
+        macs = pairing_fme(self.eqs, 2) * 136
+        ach = macs / (step_ms * 1e-3) / 1e12
+        return ({"bound": "imad", "kernel": "k_miller + k_final_exp (whole call)", "achieved": ach,
+                 "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
+                 "algorithmic_macs_per_launch": macs, "launch_ms": step_ms}, None)
+
+    def extra(self, torch, dv, b, s):
+        one = (self.g1[:128], self.g2[:256], [0, 2])
+        b.pairing_check(*one)
+        t0 = time.perf_counter()
+        for _ in range(5):
+            b.pairing_check(*one)
+        return {"single_equation_ms": (time.perf_counter() - t0) * 1e3 / 5}
+
+    def cpu(self, oracle, threads):
+        k = min(self.eqs, 32 * threads)
+        t0 = time.perf_counter()
+        out = oracle.pairing_check(self.g1[:128 * k], self.g2[:256 * k], self.offsets[:k + 1], threads=threads)
+        ms = (time.perf_counter() - t0) * 1e3
+        return None, ms * self.eqs / k, (f"{k} equations on {threads} threads, scaled to {self.eqs}; "
+                                         f"verdicts identical to the GPU's: {out == list(self.run(self._b))[:k]}")
+
+
 def make_op(args):
     return {"msm": lambda: MsmOp(args), "msmres": lambda: ResidentMsmOp(args), "g2msm": lambda: MsmOp(args, g2=True),
             "ntt": lambda: NttOp(args), "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args),
             "batch": lambda: BatchOp(args), "g2check": lambda: G2CheckOp(args), "serve": lambda: ServeOp(args),
-            "ecntt": lambda: EcNttOp(args), "poly": lambda: PolyOp(args)}[args.op]()
+            "ecntt": lambda: EcNttOp(args), "poly": lambda: PolyOp(args), "pairing": lambda: PairingOp(args)}[args.op]()
 
 
 # ----------------------------------------------------------------- reference arm
@@ -1164,6 +1249,14 @@ def run_reference(args, rank, world):
 
         metric = BatchOp(args).metric
         sample = "batch estimates"
+    elif op == "pairing":
+        pop = PairingOp(args)
+        pop.setup(None, None, None, 0)
+        k = min(pop.eqs, 32 * threads)
+        fn = lambda: oracle.pairing_check(pop.g1[:128 * k], pop.g2[:256 * k], pop.offsets[:k + 1], threads=threads)
+        metric = pop.metric
+        sample = f"{k}-equation checks on {threads} threads, scaled to {pop.eqs} equations"
+        pairing_scale = pop.eqs / k
     elif op == "poly":
         pop = PolyOp(args)
 
@@ -1194,6 +1287,8 @@ def run_reference(args, rank, world):
         sample = f"batch estimates, each from {est[-1][1]}"
     if op == "ecntt":
         value *= ecntt_scale
+    if op == "pairing":
+        value *= pairing_scale
     higher = False
     ms_step = value
     if op == "serve":

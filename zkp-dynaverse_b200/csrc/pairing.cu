@@ -4,23 +4,27 @@
 // PairingChecks::equal / equal_prepared / product_equal reduce one equation
 // to prod_k e(P_k, Q_k) = 1 (right-hand G1 points negated by the caller),
 // computed by Bn254::multi_miller_loop and final_exponentiation.  Here a
-// launch takes many equations: one thread per term runs the Miller loop,
-// one thread per equation multiplies its terms' values and runs the final
-// exponentiation.  The reference's native Miller probe
+// launch takes many equations: a group of six lanes runs the Miller loop of
+// one term, then a group per equation multiplies its terms' values and runs
+// the final exponentiation.  The reference's native Miller probe
 // (native/include/dynaverse_bn254_miller.h) is a diagnostic of line traces
 // and is not reproduced.
 //
-// Tower: Fq2 = Fq[u]/(u^2 + 1), Fq6 = Fq2[v]/(v^3 - xi), Fq12 = Fq6[w]/(w^2 - v),
-// xi = 9 + u; the coefficient of w^j (c0.c0 = w^0, c0.c1 = w^2, c0.c2 = w^4,
-// c1.c0 = w^1, c1.c1 = w^3, c1.c2 = w^5) maps under the q-power Frobenius
-// to conj(a) xi^(j(q-1)/6).
+// Fq12 = Fq2[w]/(w^6 - xi), xi = 9 + u, held by six lanes: lane k owns the
+// coefficient of w^k.  A product is c_k = sum_i a_i b_(k-i) (times xi where
+// the index wraps), six Fq2 products per lane from shuffled operands; a
+// square takes four; the sparse line product three; the q-power Frobenius
+// is conj(a_k) xi^(k(q-1)/6) per lane; f^(q^6) negates the odd lanes.  The
+// serialised GT element uses the tower Fq12 = Fq6[w]/(w^2 - v), Fq6 =
+// Fq2[v]/(v^3 - xi), v = w^2: c0 = (w^0, w^2, w^4), c1 = (w^1, w^3, w^5).
 //
 // Miller loop over the NAF of 6z + 2 (z the BN seed), then the lines to
 // pi(Q) and -pi^2(Q).  T is kept in Jacobian coordinates on the twist
 // E': y^2 = x^3 + 3/xi, untwisted by (x, y) -> (x w^2, y w^3).  The line
 // through T (slope lam) at P = (xp, yp) is yp - lam xp w + (lam xT - yT) w^3;
 // each step multiplies it by a nonzero Fq2 factor (killed by the final
-// exponentiation, since Fq2* lies in the kernel of q^6 - 1):
+// exponentiation, since Fq2* lies in the kernel of q^6 - 1).  Every lane of
+// the group computes T and the line (no exchange):
 //   doubling, x = X/Z^2, y = Y/Z^3, factor 2 Y Z^3:
 //     (2 Y Z^3 yp) + (-3 X^2 Z^2 xp) w + (3 X^3 - 2 Y^2) w^3
 //   addition of affine S = (xs, ys), H = xs Z^2 - X, R = ys Z^3 - Y, factor 2 Z H:
@@ -38,8 +42,10 @@
 //   T = c^12 b^6, f^l1 = T a^4, f^l2 = T a^6, f^l3 = f^l1 conj(f),
 //   f^l0 = c^12 b^12 a^6 f, result = f^l0 (f^l1)^q (f^l2)^(q^2) (f^l3)^(q^3).
 // conj is the inverse after the easy part (the result is in the
-// cyclotomic subgroup).  A verdict is result == 1; the value written for a
-// single pairing is the GT element in the tower order above, canonical.
+// cyclotomic subgroup); the easy part's inverse is conj(f) / N with N =
+// f conj(f) in Fq6 inverted in every lane.  A verdict is result == 1; the
+// value written for a single pairing is the GT element in the tower order
+// above, canonical.
 #include <cstring>
 #include <string>
 #include <vector>
@@ -50,15 +56,8 @@
 namespace dv {
 namespace {
 
-// Out-of-line tower functions take their operands by const reference: a
-// 384-byte Fq12 passed by value into a __noinline__ function that hands it
-// on to further __noinline__ calls came back altered on sm_100a (nvcc 12.9);
-// by reference it is never copied.
 struct Fq6 {
     Fq2 c0, c1, c2;
-};
-struct Fq12 {
-    Fq6 c0, c1;
 };
 
 // xi^(j (q-1)/6), j = 0..5, Montgomery (c0, c1).
@@ -101,28 +100,8 @@ DV_INL Fq mul9(const Fq& a) { return Fq::add(Fq::dbl(Fq::dbl(Fq::dbl(a))), a); }
 // (a0 + a1 u)(9 + u) = (9 a0 - a1) + (a0 + 9 a1) u
 DV_INL Fq2 mul_xi(const Fq2& a) { return {Fq::sub(mul9(a.c0), a.c1), Fq::add(a.c0, mul9(a.c1))}; }
 
-DV_INL Fq6 f6_add(const Fq6& a, const Fq6& b) { return {Fq2::add(a.c0, b.c0), Fq2::add(a.c1, b.c1), Fq2::add(a.c2, b.c2)}; }
-DV_INL Fq6 f6_sub(const Fq6& a, const Fq6& b) { return {Fq2::sub(a.c0, b.c0), Fq2::sub(a.c1, b.c1), Fq2::sub(a.c2, b.c2)}; }
-DV_INL Fq6 f6_neg(const Fq6& a) { return {Fq2::neg(a.c0), Fq2::neg(a.c1), Fq2::neg(a.c2)}; }
-DV_INL Fq6 f6_mul_v(const Fq6& a) { return {mul_xi(a.c2), a.c0, a.c1}; }
 
-// Karatsuba over v^3 = xi: 6 Fq2 products.
-__device__ __noinline__ Fq6 f6_mul(const Fq6& a, const Fq6& b) {
-    const Fq2 v0 = Fq2::mul(a.c0, b.c0), v1 = Fq2::mul(a.c1, b.c1), v2 = Fq2::mul(a.c2, b.c2);
-    const Fq2 t0 = Fq2::mul(Fq2::add(a.c1, a.c2), Fq2::add(b.c1, b.c2));
-    const Fq2 t1 = Fq2::mul(Fq2::add(a.c0, a.c1), Fq2::add(b.c0, b.c1));
-    const Fq2 t2 = Fq2::mul(Fq2::add(a.c0, a.c2), Fq2::add(b.c0, b.c2));
-    return {Fq2::add(v0, mul_xi(Fq2::sub(Fq2::sub(t0, v1), v2))),
-            Fq2::add(Fq2::sub(Fq2::sub(t1, v0), v1), mul_xi(v2)),
-            Fq2::add(Fq2::sub(Fq2::sub(t2, v0), v2), v1)};
-}
-// (x0 + x1 v + x2 v^2)(b0 + b1 v): 5 Fq2 products.
-__device__ __noinline__ Fq6 f6_mul_01(const Fq6& x, const Fq2& b0, const Fq2& b1) {
-    const Fq2 v0 = Fq2::mul(x.c0, b0), v1 = Fq2::mul(x.c1, b1);
-    const Fq2 t = Fq2::mul(Fq2::add(x.c0, x.c1), Fq2::add(b0, b1));
-    return {Fq2::add(v0, mul_xi(Fq2::mul(x.c2, b1))), Fq2::sub(Fq2::sub(t, v0), v1),
-            Fq2::add(v1, Fq2::mul(x.c2, b0))};
-}
+// 1 / a in Fq6 (one Fq inversion).
 __device__ __noinline__ Fq6 f6_inv(const Fq6& a) {
     const Fq2 t0 = Fq2::sub(Fq2::sqr(a.c0), mul_xi(Fq2::mul(a.c1, a.c2)));
     const Fq2 t1 = Fq2::sub(mul_xi(Fq2::sqr(a.c2)), Fq2::mul(a.c0, a.c1));
@@ -132,70 +111,110 @@ __device__ __noinline__ Fq6 f6_inv(const Fq6& a) {
     return {Fq2::mul(t0, di), Fq2::mul(t1, di), Fq2::mul(t2, di)};
 }
 
-DV_INL Fq12 f12_one() {
-    Fq12 r;
-    r.c0 = {Fq2::one(), Fq2::zero(), Fq2::zero()};
-    r.c1 = {Fq2::zero(), Fq2::zero(), Fq2::zero()};
+// ------------------------------------------------------------------ lane groups
+// One Fq12 lives in a group of GL = 6 lanes: lane k holds the Fq2
+// coefficient of w^k (w^6 = xi).  A warp holds 5 groups (lanes 30, 31 run
+// along on copies and write nothing); every group in a warp executes the
+// same instruction stream, so the shuffles below always see full warps.
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int GL = 6;
+constexpr int GROUPS_PER_WARP = 5;
+
+DV_INL Fq shfl_fq(const Fq& a, int src) {
+    Fq r;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) r.v[w] = __shfl_sync(FULL, a.v[w], src);
     return r;
 }
-DV_INL Fq12 f12_conj(const Fq12& a) { return {a.c0, f6_neg(a.c1)}; }
-// Karatsuba: 3 Fq6 products.
-__device__ __noinline__ Fq12 f12_mul(const Fq12& a, const Fq12& b) {
-    const Fq6 t0 = f6_mul(a.c0, b.c0), t1 = f6_mul(a.c1, b.c1);
-    const Fq6 t2 = f6_mul(f6_add(a.c0, a.c1), f6_add(b.c0, b.c1));
-    return {f6_add(t0, f6_mul_v(t1)), f6_sub(f6_sub(t2, t0), t1)};
+DV_INL Fq2 shfl2(const Fq2& a, int src) { return {shfl_fq(a.c0, src), shfl_fq(a.c1, src)}; }
+DV_INL int mod6(int x) { return x < 0 ? x + 6 : (x >= 6 ? x - 6 : x); }
+
+// Two independent Fq2 products, their base products issued in pairs.
+DV_INL PairOf<Fq2> fq2_mul_pair(const Fq2& a, const Fq2& b, const Fq2& c, const Fq2& d) {
+    const Fq::Pair p0 = Fq::mul2(a.c0, b.c0, a.c1, b.c1);
+    const Fq::Pair p1 = Fq::mul2(c.c0, d.c0, c.c1, d.c1);
+    const Fq::Pair p2 = Fq::mul2(Fq::add(a.c0, a.c1), Fq::add(b.c0, b.c1), Fq::add(c.c0, c.c1), Fq::add(d.c0, d.c1));
+    return {{Fq::sub(p0.r0, p0.r1), Fq::sub(Fq::sub(p2.r0, p0.r0), p0.r1)},
+            {Fq::sub(p1.r0, p1.r1), Fq::sub(Fq::sub(p2.r1, p1.r0), p1.r1)}};
 }
-// (g + h w)^2 = (g + h)(g + h v) - t - t v + 2 t w, t = g h: 2 Fq6 products.
-__device__ __noinline__ Fq12 f12_sqr(const Fq12& a) {
-    const Fq6 t = f6_mul(a.c0, a.c1);
-    const Fq6 m = f6_mul(f6_add(a.c0, a.c1), f6_add(a.c0, f6_mul_v(a.c1)));
-    return {f6_sub(f6_sub(m, t), f6_mul_v(t)), f6_add(t, t)};
-}
-// f (l0 + (l1 + l3 v) w) with l0 in Fq2 (the line's w^0 term), l1, l3 its
-// w^1 and w^3 terms: 13 Fq2 products.
-__device__ __noinline__ Fq12 f12_mul_line(const Fq12& f, const Fq2& l0, const Fq2& l1, const Fq2& l3) {
-    const Fq6 t0 = {Fq2::mul(f.c0.c0, l0), Fq2::mul(f.c0.c1, l0), Fq2::mul(f.c0.c2, l0)};
-    const Fq6 t1 = f6_mul_01(f.c1, l1, l3);
-    const Fq6 t2 = f6_mul_01(f6_add(f.c0, f.c1), Fq2::add(l0, l1), l3);
-    return {f6_add(t0, f6_mul_v(t1)), f6_sub(f6_sub(t2, t0), t1)};
-}
-__device__ __noinline__ Fq12 f12_inv(const Fq12& a) {
-    const Fq6 d = f6_inv(f6_sub(f6_mul(a.c0, a.c0), f6_mul_v(f6_mul(a.c1, a.c1))));
-    return {f6_mul(a.c0, d), f6_neg(f6_mul(a.c1, d))};
-}
-// q^k-power Frobenius, k = 1, 2, 3.
-__device__ __noinline__ Fq12 f12_frob(const Fq12& in, int k) {
-    Fq12 a = in;
-    Fq2* c = &a.c0.c0;
-    const int wpow[6] = {0, 2, 4, 1, 3, 5};
-    for (int i = 0; i < 6; ++i) {
-        const int j = wpow[i];
-        if (k == 2) {
-            c[i] = Fq2::mul_fq(c[i], frob2(j));
-        } else {
-            Fq2 g = frob1(j);
-            if (k == 3) g = Fq2::mul_fq(g, frob2(j));
-            c[i] = Fq2::mul(Fq2::conj(c[i]), g);
-        }
+
+// c = a b: lane k sums a_i b_(k-i) over i, times xi where i > k.
+__device__ __noinline__ Fq2 g_mul(const Fq2& a, const Fq2& b, int k, int base) {
+    Fq2 acc = Fq2::zero();
+#pragma unroll
+    for (int i = 0; i < GL; i += 2) {
+        const PairOf<Fq2> p = fq2_mul_pair(shfl2(a, base + i), shfl2(b, base + mod6(k - i)), shfl2(a, base + i + 1),
+                                           shfl2(b, base + mod6(k - i - 1)));
+        acc = Fq2::add(acc, i > k ? mul_xi(p.r0) : p.r0);
+        acc = Fq2::add(acc, i + 1 > k ? mul_xi(p.r1) : p.r1);
     }
-    return a;
+    return acc;
 }
-DV_INL bool f12_is_one(const Fq12& a) {
-    const Fq2* c = &a.c0.c0;
-    if (!(c[0].c0 == Fq::one()) || !c[0].c1.is_zero()) return false;
-    for (int i = 1; i < 6; ++i)
-        if (!c[i].is_zero()) return false;
-    return true;
+// c = a^2: each unordered pair (i, j), i + j = k mod 6, once (doubled off
+// the diagonal).  Even k: (m, m), (m+3, m+3), (m+1, k-m-1), (m+2, k-m-2),
+// m = k/2; odd k: (m, m+1), (m+2, m+5), (m+3, m+4), m = (k-1)/2.
+__device__ __noinline__ Fq2 g_sqr(const Fq2& a, int k, int base) {
+    int i[4], j[4];
+    bool dbl[4];
+    if (!(k & 1)) {
+        const int m = k >> 1;
+        i[0] = m; j[0] = m; i[1] = mod6(m + 3); j[1] = i[1];
+        i[2] = mod6(m + 1); j[2] = mod6(k - m - 1); i[3] = mod6(m + 2); j[3] = mod6(k - m - 2);
+        dbl[0] = dbl[1] = false; dbl[2] = dbl[3] = true;
+    } else {
+        const int m = k >> 1;
+        i[0] = m; j[0] = m + 1; i[1] = mod6(m + 2); j[1] = mod6(m + 5); i[2] = mod6(m + 3); j[2] = mod6(m + 4);
+        i[3] = 0; j[3] = 0;
+        dbl[0] = dbl[1] = dbl[2] = true; dbl[3] = false;
+    }
+    Fq2 acc = Fq2::zero();
+#pragma unroll
+    for (int s = 0; s < 4; s += 2) {
+        const PairOf<Fq2> p = fq2_mul_pair(shfl2(a, base + i[s]), shfl2(a, base + j[s]), shfl2(a, base + i[s + 1]),
+                                           shfl2(a, base + j[s + 1]));
+        Fq2 t0 = dbl[s] ? Fq2::dbl(p.r0) : p.r0;
+        Fq2 t1 = dbl[s + 1] ? Fq2::dbl(p.r1) : p.r1;
+        if (i[s] + j[s] >= GL) t0 = mul_xi(t0);
+        if (i[s + 1] + j[s + 1] >= GL) t1 = mul_xi(t1);
+        if ((k & 1) && s == 2) t1 = Fq2::zero();
+        acc = Fq2::add(Fq2::add(acc, t0), t1);
+    }
+    return acc;
 }
-// a^z, z the BN seed (63 bits), left to right.
-__device__ __noinline__ Fq12 f12_pow_z(const Fq12& a) {
-    Fq12 r = a;
+// f (l0 + l1 w + l3 w^3).
+__device__ __noinline__ Fq2 g_mul_line(const Fq2& f, const Fq2& l0, const Fq2& l1, const Fq2& l3, int k, int base) {
+    const Fq2 f1 = shfl2(f, base + mod6(k - 1)), f3 = shfl2(f, base + mod6(k - 3));
+    const PairOf<Fq2> p = fq2_mul_pair(f, l0, f1, l1);
+    const Fq2 t3 = Fq2::mul(f3, l3);
+    return Fq2::add(Fq2::add(p.r0, k < 1 ? mul_xi(p.r1) : p.r1), k < 3 ? mul_xi(t3) : t3);
+}
+// f^(q^6): w -> -w.
+DV_INL Fq2 g_conj(const Fq2& f, int k) { return (k & 1) ? Fq2::neg(f) : f; }
+// q^e-power Frobenius, e = 1, 2, 3.
+DV_INL Fq2 g_frob(const Fq2& f, int k, int e) {
+    if (e == 2) return Fq2::mul_fq(f, frob2(k));
+    Fq2 g = frob1(k);
+    if (e == 3) g = Fq2::mul_fq(g, frob2(k));
+    return Fq2::mul(Fq2::conj(f), g);
+}
+// f^-1 = conj(f) / N, N = f conj(f) in Fq6 (the even lanes, v = w^2).
+__device__ __noinline__ Fq2 g_inv(const Fq2& f, int k, int base) {
+    const Fq2 c = g_conj(f, k);
+    const Fq2 n = g_mul(f, c, k, base);
+    const Fq6 nn = {shfl2(n, base), shfl2(n, base + 2), shfl2(n, base + 4)};
+    const Fq6 ni = f6_inv(nn);
+    const Fq2 mine = (k & 1) ? Fq2::zero() : (k == 0 ? ni.c0 : (k == 2 ? ni.c1 : ni.c2));
+    return g_mul(c, mine, k, base);
+}
+__device__ __noinline__ Fq2 g_pow_z(const Fq2& a, int k, int base) {
+    Fq2 r = a;
     for (int i = 61; i >= 0; --i) {
-        r = f12_sqr(r);
-        if ((BN_Z >> i) & 1) r = f12_mul(r, a);
+        r = g_sqr(r, k, base);
+        if ((BN_Z >> i) & 1) r = g_mul(r, a, k, base);
     }
     return r;
 }
+DV_INL Fq2 g_one(int k) { return k == 0 ? Fq2::one() : Fq2::zero(); }
 
 struct Tw {
     Fq2 x, y, z;  // Jacobian on the twist
@@ -236,75 +255,106 @@ __device__ __noinline__ void add_step(Tw& t, const Fq2& xs, const Fq2& ys, const
     t.z = z3;
 }
 
-__device__ Fq12 miller_loop(const G1A& p, const G2A& q) {
+// Miller value of (P, Q) as this lane's coefficient; T and the lines are
+// computed in every lane of the group.
+__device__ Fq2 g_miller(const G1A& p, const G2A& q, int k, int base) {
     Tw t{q.x, q.y, Fq2::one()};
-    Fq12 f = f12_one();
+    Fq2 f = g_one(k);
     Fq2 l0, l1, l3;
     const Fq2 nqy = Fq2::neg(q.y);
     for (int i = 1; i < NAF_LEN; ++i) {
         dbl_step(t, p.x, p.y, l0, l1, l3);
-        f = f12_mul_line(f12_sqr(f), l0, l1, l3);
+        f = g_mul_line(g_sqr(f, k, base), l0, l1, l3, k, base);
         const int d = NAF_6Z2[i];
         if (d) {
             add_step(t, q.x, d > 0 ? q.y : nqy, p.x, p.y, l0, l1, l3);
-            f = f12_mul_line(f, l0, l1, l3);
+            f = g_mul_line(f, l0, l1, l3, k, base);
         }
     }
     // pi(Q) = (conj(x) xi^((q-1)/3), conj(y) xi^((q-1)/2)); -pi^2(Q) = (x xi^((q^2-1)/3), -y xi^((q^2-1)/2))
     const Fq2 x1 = Fq2::mul(Fq2::conj(q.x), frob1(2)), y1 = Fq2::mul(Fq2::conj(q.y), frob1(3));
     const Fq2 x2 = Fq2::mul_fq(q.x, frob2(2)), y2 = Fq2::neg(Fq2::mul_fq(q.y, frob2(3)));
     add_step(t, x1, y1, p.x, p.y, l0, l1, l3);
-    f = f12_mul_line(f, l0, l1, l3);
+    f = g_mul_line(f, l0, l1, l3, k, base);
     add_step(t, x2, y2, p.x, p.y, l0, l1, l3);
-    return f12_mul_line(f, l0, l1, l3);
+    return g_mul_line(f, l0, l1, l3, k, base);
 }
 
-__device__ Fq12 final_exponentiation(const Fq12& m) {
-    Fq12 f = f12_mul(f12_conj(m), f12_inv(m));  // ^(q^6 - 1)
-    f = f12_mul(f12_frob(f, 2), f);             // ^(q^2 + 1)
-    const Fq12 a = f12_pow_z(f);
-    const Fq12 b = f12_pow_z(a);
-    const Fq12 c = f12_pow_z(b);
-    const Fq12 a2 = f12_sqr(a), a4 = f12_sqr(a2), a6 = f12_mul(a4, a2);
-    const Fq12 b2 = f12_sqr(b), b6 = f12_mul(f12_sqr(b2), b2), b12 = f12_sqr(b6);
-    const Fq12 c4 = f12_sqr(f12_sqr(c)), c12 = f12_mul(f12_sqr(c4), c4);
-    const Fq12 tt = f12_mul(c12, b6);
-    const Fq12 l1 = f12_mul(tt, a4);
-    const Fq12 l2 = f12_mul(tt, a6);
-    const Fq12 l3 = f12_mul(l1, f12_conj(f));
-    const Fq12 l0 = f12_mul(f12_mul(f12_mul(c12, b12), a6), f);
-    Fq12 r = f12_mul(l0, f12_frob(l1, 1));
-    r = f12_mul(r, f12_frob(l2, 2));
-    return f12_mul(r, f12_frob(l3, 3));
+__device__ Fq2 g_final_exponentiation(const Fq2& m, int k, int base) {
+    Fq2 f = g_mul(g_conj(m, k), g_inv(m, k, base), k, base);  // ^(q^6 - 1)
+    f = g_mul(g_frob(f, k, 2), f, k, base);                    // ^(q^2 + 1)
+    const Fq2 a = g_pow_z(f, k, base);
+    const Fq2 b = g_pow_z(a, k, base);
+    const Fq2 c = g_pow_z(b, k, base);
+    const Fq2 a2 = g_sqr(a, k, base), a4 = g_sqr(a2, k, base), a6 = g_mul(a4, a2, k, base);
+    const Fq2 b2 = g_sqr(b, k, base), b6 = g_mul(g_sqr(b2, k, base), b2, k, base), b12 = g_sqr(b6, k, base);
+    const Fq2 c4 = g_sqr(g_sqr(c, k, base), k, base), c12 = g_mul(g_sqr(c4, k, base), c4, k, base);
+    const Fq2 tt = g_mul(c12, b6, k, base);
+    const Fq2 l1 = g_mul(tt, a4, k, base);
+    const Fq2 l2 = g_mul(tt, a6, k, base);
+    const Fq2 l3 = g_mul(l1, g_conj(f, k), k, base);
+    const Fq2 l0 = g_mul(g_mul(g_mul(c12, b12, k, base), a6, k, base), f, k, base);
+    Fq2 r = g_mul(l0, g_frob(l1, k, 1), k, base);
+    r = g_mul(r, g_frob(l2, k, 2), k, base);
+    return g_mul(r, g_frob(l3, k, 3), k, base);
 }
 
-// Miller value of every term (one thread each); infinity on either side gives one.
+struct GroupLane {
+    int k, base;
+    uint64_t group;  // global group index
+    bool live;       // lanes 0..29 of the warp
+};
+DV_INL GroupLane group_lane() {
+    const int l = threadIdx.x & 31;
+    const int k = l < GL * GROUPS_PER_WARP ? l % GL : l - GL * GROUPS_PER_WARP;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    return {k, l - k, warp * GROUPS_PER_WARP + (uint64_t)(l / GL), l < GL * GROUPS_PER_WARP};
+}
+
+// Miller value of every term, one lane group per term (coefficient k of
+// term t at out[6 t + k]); infinity on either side gives one.
 __global__ void __launch_bounds__(128) k_miller(const G1A* __restrict__ g1, const G2A* __restrict__ g2,
-                                                uint64_t terms, Fq12* __restrict__ out) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= terms) return;
-    const G1A p = g1[i];
-    const G2A q = g2[i];
-    out[i] = (p.is_inf() || q.is_inf()) ? f12_one() : miller_loop(p, q);
+                                                uint64_t terms, Fq2* __restrict__ out) {
+    const GroupLane g = group_lane();
+    const bool mine = g.live && g.group < terms;
+    const uint64_t t = mine ? g.group : 0;  // idle lanes compute on term 0
+    const G1A p = g1[t];
+    const G2A q = g2[t];
+    const Fq2 f = g_miller(p, q, g.k, g.base);
+    if (mine) out[6 * t + g.k] = (p.is_inf() || q.is_inf()) ? g_one(g.k) : f;
 }
 
-// Per equation: product of its terms' values, final exponentiation; the
-// verdict (result == 1) and, with gt, the canonical GT element.
-__global__ void __launch_bounds__(128) k_final_exp(const Fq12* __restrict__ miller, const uint64_t* __restrict__ offsets,
+// One lane group per equation: product of its terms' values (every group of
+// a warp runs the warp's largest term count, multiplying by one past its
+// own), final exponentiation, verdict, and with gt the canonical GT element.
+__global__ void __launch_bounds__(128) k_final_exp(const Fq2* __restrict__ miller, const uint64_t* __restrict__ offsets,
                                                    uint64_t equations, uint8_t* __restrict__ verdicts,
                                                    uint8_t* __restrict__ gt) {
-    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= equations) return;
-    Fq12 f = f12_one();
-    for (uint64_t k = offsets[e]; k < offsets[e + 1]; ++k) f = f12_mul(f, miller[k]);
-    const Fq12 r = final_exponentiation(f);
-    if (verdicts) verdicts[e] = f12_is_one(r) ? 1 : 0;
+    const GroupLane g = group_lane();
+    const bool mine = g.live && g.group < equations;
+    const uint64_t e = mine ? g.group : 0;
+    const uint64_t first = mine ? offsets[e] : 0, count = mine ? offsets[e + 1] - first : 0;
+    uint64_t most = count;
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        const uint64_t o = __shfl_xor_sync(FULL, most, off);
+        most = o > most ? o : most;
+    }
+    Fq2 f = g_one(g.k);
+    for (uint64_t t = 0; t < most; ++t) {
+        const Fq2 v = t < count ? miller[6 * (first + t) + g.k] : g_one(g.k);
+        f = t == 0 ? v : g_mul(f, v, g.k, g.base);
+    }
+    const Fq2 r = g_final_exponentiation(f, g.k, g.base);
+    const bool coef_ok = g.k == 0 ? (r.c0 == Fq::one() && r.c1.is_zero()) : r.is_zero();
+    const unsigned ok = __ballot_sync(FULL, coef_ok);
+    if (!mine) return;
+    if (verdicts && g.k == 0) verdicts[e] = ((ok >> g.base) & 0x3fu) == 0x3fu ? 1 : 0;
     if (gt) {
-        const Fq2* c = &r.c0.c0;
-        for (int i = 0; i < 6; ++i) {
-            store_canonical(gt + 384 * e + 64 * i, c[i].c0);
-            store_canonical(gt + 384 * e + 64 * i + 32, c[i].c1);
-        }
+        // tower order: w^0, w^2, w^4, w^1, w^3, w^5
+        const int slot = (g.k & 1) ? 3 + (g.k >> 1) : (g.k >> 1);
+        store_canonical(gt + 384 * e + 64 * slot, r.c0);
+        store_canonical(gt + 384 * e + 64 * slot + 32, r.c1);
     }
 }
 
@@ -319,9 +369,10 @@ void pairing_run(Backend& b, const uint8_t* g1, const uint8_t* g2, uint64_t term
     DV_CUDA(cudaMemsetAsync(bad, 0xff, 2 * sizeof(uint32_t), st));
     convert_points<Fq>(d_in, p, terms, bad, st);
     convert_points<Fq2>(d_in + 64 * terms, q, terms, bad + 1, st);
-    Fq12* mil = b.aux.as<Fq12>(terms);
+    Fq2* mil = b.aux.as<Fq2>(6 * terms);
+    constexpr uint64_t groups_per_block = 128 / 32 * GROUPS_PER_WARP;
     if (terms) {
-        k_miller<<<(unsigned)((terms + 127) / 128), 128, 0, st>>>(p, q, terms, mil);
+        k_miller<<<(unsigned)((terms + groups_per_block - 1) / groups_per_block), 128, 0, st>>>(p, q, terms, mil);
         DV_LAUNCH();
     }
     uint64_t* d_off = b.idx.as<uint64_t>(equations + 1);
@@ -329,8 +380,8 @@ void pairing_run(Backend& b, const uint8_t* g1, const uint8_t* g2, uint64_t term
     // GT elements first (16-byte aligned stores), then the verdict bytes
     uint8_t* d_gt = b.out_buf.as<uint8_t>(equations * ((gt ? 384 : 0) + 1));
     uint8_t* d_out = d_gt + (gt ? 384 * equations : 0);
-    k_final_exp<<<(unsigned)((equations + 127) / 128), 128, 0, st>>>(mil, d_off, equations, d_out,
-                                                                     gt ? d_gt : nullptr);
+    k_final_exp<<<(unsigned)((equations + groups_per_block - 1) / groups_per_block), 128, 0, st>>>(
+        mil, d_off, equations, d_out, gt ? d_gt : nullptr);
     DV_LAUNCH();
     uint32_t hbad[2];
     DV_CUDA(cudaMemcpyAsync(hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, st));
