@@ -23,8 +23,8 @@
 // E': y^2 = x^3 + 3/xi, untwisted by (x, y) -> (x w^2, y w^3).  The line
 // through T (slope lam) at P = (xp, yp) is yp - lam xp w + (lam xT - yT) w^3;
 // each step multiplies it by a nonzero Fq2 factor (killed by the final
-// exponentiation, since Fq2* lies in the kernel of q^6 - 1).  Every lane of
-// the group computes T and the line (no exchange):
+// exponentiation, since Fq2* lies in the kernel of q^6 - 1).  The products
+// of a step are spread over the group's lanes level by level:
 //   doubling, x = X/Z^2, y = Y/Z^3, factor 2 Y Z^3:
 //     (2 Y Z^3 yp) + (-3 X^2 Z^2 xp) w + (3 X^3 - 2 Y^2) w^3
 //   addition of affine S = (xs, ys), H = xs Z^2 - X, R = ys Z^3 - Y, factor 2 Z H:
@@ -129,13 +129,32 @@ DV_INL Fq shfl_fq(const Fq& a, int src) {
 DV_INL Fq2 shfl2(const Fq2& a, int src) { return {shfl_fq(a.c0, src), shfl_fq(a.c1, src)}; }
 DV_INL int mod6(int x) { return x < 0 ? x + 6 : (x >= 6 ? x - 6 : x); }
 
-// Two independent Fq2 products, their base products issued in pairs.
-DV_INL PairOf<Fq2> fq2_mul_pair(const Fq2& a, const Fq2& b, const Fq2& c, const Fq2& d) {
-    const Fq::Pair p0 = Fq::mul2(a.c0, b.c0, a.c1, b.c1);
-    const Fq::Pair p1 = Fq::mul2(c.c0, d.c0, c.c1, d.c1);
-    const Fq::Pair p2 = Fq::mul2(Fq::add(a.c0, a.c1), Fq::add(b.c0, b.c1), Fq::add(c.c0, c.c1), Fq::add(d.c0, d.c1));
-    return {{Fq::sub(p0.r0, p0.r1), Fq::sub(Fq::sub(p2.r0, p0.r0), p0.r1)},
-            {Fq::sub(p1.r0, p1.r1), Fq::sub(Fq::sub(p2.r1, p1.r0), p1.r1)}};
+// n Fq2 products (Karatsuba, 3 base products each) with their 3n base
+// products issued two at a time (one out-of-line body interleaves the two
+// chains, which a lone warp needs to hide the multiply latency).
+template <int N>
+DV_INL void fq2_mul_n(const Fq2* a, const Fq2* b, Fq2* out) {
+    constexpr int M = 3 * N, G = (M + 1) / 2;
+    Fq x[2 * G], y[2 * G], z[2 * G];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        x[3 * i] = a[i].c0; y[3 * i] = b[i].c0;
+        x[3 * i + 1] = a[i].c1; y[3 * i + 1] = b[i].c1;
+        x[3 * i + 2] = Fq::add(a[i].c0, a[i].c1); y[3 * i + 2] = Fq::add(b[i].c0, b[i].c1);
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        if (2 * g + 1 < M) {
+            const Fq::Pair q = Fq::mul2(x[2 * g], y[2 * g], x[2 * g + 1], y[2 * g + 1]);
+            z[2 * g] = q.r0;
+            z[2 * g + 1] = q.r1;
+        } else {
+            z[2 * g] = Fq::mul(x[2 * g], y[2 * g]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        out[i] = {Fq::sub(z[3 * i], z[3 * i + 1]), Fq::sub(Fq::sub(z[3 * i + 2], z[3 * i]), z[3 * i + 1])};
 }
 
 // c = a b: lane k sums a_i b_(k-i) over i, times xi where i > k.
@@ -143,10 +162,12 @@ __device__ __noinline__ Fq2 g_mul(const Fq2& a, const Fq2& b, int k, int base) {
     Fq2 acc = Fq2::zero();
 #pragma unroll
     for (int i = 0; i < GL; i += 2) {
-        const PairOf<Fq2> p = fq2_mul_pair(shfl2(a, base + i), shfl2(b, base + mod6(k - i)), shfl2(a, base + i + 1),
-                                           shfl2(b, base + mod6(k - i - 1)));
-        acc = Fq2::add(acc, i > k ? mul_xi(p.r0) : p.r0);
-        acc = Fq2::add(acc, i + 1 > k ? mul_xi(p.r1) : p.r1);
+        const Fq2 x[2] = {shfl2(a, base + i), shfl2(a, base + i + 1)};
+        const Fq2 y[2] = {shfl2(b, base + mod6(k - i)), shfl2(b, base + mod6(k - i - 1))};
+        Fq2 p[2];
+        fq2_mul_n<2>(x, y, p);
+        acc = Fq2::add(acc, i > k ? mul_xi(p[0]) : p[0]);
+        acc = Fq2::add(acc, i + 1 > k ? mul_xi(p[1]) : p[1]);
     }
     return acc;
 }
@@ -170,23 +191,27 @@ __device__ __noinline__ Fq2 g_sqr(const Fq2& a, int k, int base) {
     Fq2 acc = Fq2::zero();
 #pragma unroll
     for (int s = 0; s < 4; s += 2) {
-        const PairOf<Fq2> p = fq2_mul_pair(shfl2(a, base + i[s]), shfl2(a, base + j[s]), shfl2(a, base + i[s + 1]),
-                                           shfl2(a, base + j[s + 1]));
-        Fq2 t0 = dbl[s] ? Fq2::dbl(p.r0) : p.r0;
-        Fq2 t1 = dbl[s + 1] ? Fq2::dbl(p.r1) : p.r1;
-        if (i[s] + j[s] >= GL) t0 = mul_xi(t0);
-        if (i[s + 1] + j[s + 1] >= GL) t1 = mul_xi(t1);
-        if ((k & 1) && s == 2) t1 = Fq2::zero();
-        acc = Fq2::add(Fq2::add(acc, t0), t1);
+        const Fq2 x[2] = {shfl2(a, base + i[s]), shfl2(a, base + i[s + 1])};
+        const Fq2 y[2] = {shfl2(a, base + j[s]), shfl2(a, base + j[s + 1])};
+        Fq2 p[2];
+        fq2_mul_n<2>(x, y, p);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            Fq2 t = dbl[s + h] ? Fq2::dbl(p[h]) : p[h];
+            if (i[s + h] + j[s + h] >= GL) t = mul_xi(t);
+            if ((k & 1) && s + h == 3) t = Fq2::zero();
+            acc = Fq2::add(acc, t);
+        }
     }
     return acc;
 }
 // f (l0 + l1 w + l3 w^3).
 __device__ __noinline__ Fq2 g_mul_line(const Fq2& f, const Fq2& l0, const Fq2& l1, const Fq2& l3, int k, int base) {
-    const Fq2 f1 = shfl2(f, base + mod6(k - 1)), f3 = shfl2(f, base + mod6(k - 3));
-    const PairOf<Fq2> p = fq2_mul_pair(f, l0, f1, l1);
-    const Fq2 t3 = Fq2::mul(f3, l3);
-    return Fq2::add(Fq2::add(p.r0, k < 1 ? mul_xi(p.r1) : p.r1), k < 3 ? mul_xi(t3) : t3);
+    const Fq2 x[3] = {f, shfl2(f, base + mod6(k - 1)), shfl2(f, base + mod6(k - 3))};
+    const Fq2 y[3] = {l0, l1, l3};
+    Fq2 p[3];
+    fq2_mul_n<3>(x, y, p);
+    return Fq2::add(Fq2::add(p[0], k < 1 ? mul_xi(p[1]) : p[1]), k < 3 ? mul_xi(p[2]) : p[2]);
 }
 // f^(q^6): w -> -w.
 DV_INL Fq2 g_conj(const Fq2& f, int k) { return (k & 1) ? Fq2::neg(f) : f; }
@@ -220,63 +245,98 @@ struct Tw {
     Fq2 x, y, z;  // Jacobian on the twist
 };
 
-// T <- 2T; returns the line's (w^0, w^1, w^3) terms at P.
-__device__ __noinline__ void dbl_step(Tw& t, const Fq& xp, const Fq& yp, Fq2& l0, Fq2& l1, Fq2& l3) {
-    const Fq2 a = Fq2::sqr(t.x), b = Fq2::sqr(t.y), c = Fq2::sqr(b), zz = Fq2::sqr(t.z);
-    const Fq2 e = Fq2::add(Fq2::dbl(a), a);
-    const Fq2 d = Fq2::dbl(Fq2::sub(Fq2::sub(Fq2::sqr(Fq2::add(t.x, b)), a), c));
-    const Fq2 z3 = Fq2::dbl(Fq2::mul(t.y, t.z));
-    l0 = Fq2::mul_fq(Fq2::mul(z3, zz), yp);
-    l1 = Fq2::neg(Fq2::mul_fq(Fq2::mul(e, zz), xp));
-    l3 = Fq2::sub(Fq2::mul(e, t.x), Fq2::dbl(b));
-    const Fq2 x3 = Fq2::sub(Fq2::sqr(e), Fq2::dbl(d));
-    const Fq2 c8 = Fq2::dbl(Fq2::dbl(Fq2::dbl(c)));
-    t.y = Fq2::sub(Fq2::mul(e, Fq2::sub(d, x3)), c8);
+// a b with the two base products a0 b0, a1 b1 issued as a pair.
+DV_INL Fq2 fq2_mul_fast(const Fq2& a, const Fq2& b) {
+    const Fq::Pair p = Fq::mul2(a.c0, b.c0, a.c1, b.c1);
+    const Fq t = Fq::mul(Fq::add(a.c0, a.c1), Fq::add(b.c0, b.c1));
+    return {Fq::sub(p.r0, p.r1), Fq::sub(Fq::sub(t, p.r0), p.r1)};
+}
+DV_INL Fq2 pick(int k, const Fq2& v0, const Fq2& v1, const Fq2& v2, const Fq2& v3, const Fq2& v4, const Fq2& v5) {
+    return k == 0 ? v0 : k == 1 ? v1 : k == 2 ? v2 : k == 3 ? v3 : k == 4 ? v4 : v5;
+}
+// Each lane of the group computes one Fq2 product, its operands chosen by
+// k, and gets every lane's product back.
+DV_INL void level(const Fq2& a, const Fq2& b, int base, Fq2* out, int n) {
+    Fq2 p;
+    fq2_mul_n<1>(&a, &b, &p);
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+        if (j < n) out[j] = shfl2(p, base + j);
+}
+DV_INL Fq2 fq2_of(const Fq& x) { return {x, Fq::zero()}; }
+
+// T <- 2T and the line's (w^0, w^1, w^3) terms at P, the products spread
+// over the group in three dependency levels:
+//   A = X^2, B = Y^2, ZZ = Z^2, YZ = Y Z;
+//   C = B^2, S = (X + B)^2, E ZZ, Z3 ZZ, E X, E^2   (E = 3A, Z3 = 2 Y Z);
+//   E (D - X3), Z3 ZZ yp, E ZZ xp                   (D = 2(S - A - C), X3 = E^2 - 2D).
+__device__ __noinline__ void dbl_step(Tw& t, const Fq& xp, const Fq& yp, Fq2& l0, Fq2& l1, Fq2& l3, int k, int base) {
+    Fq2 v[6];
+    level(pick(k, t.x, t.y, t.z, t.y, t.x, t.x), pick(k, t.x, t.y, t.z, t.z, t.x, t.x), base, v, 4);
+    const Fq2 a = v[0], b = v[1], zz = v[2];
+    const Fq2 e = Fq2::add(Fq2::dbl(a), a), z3 = Fq2::dbl(v[3]), xb = Fq2::add(t.x, b);
+    level(pick(k, b, xb, e, z3, e, e), pick(k, b, xb, zz, zz, t.x, e), base, v, 6);
+    const Fq2 c = v[0], ezz = v[2], z3zz = v[3], ex = v[4];
+    const Fq2 d = Fq2::dbl(Fq2::sub(Fq2::sub(v[1], a), c));
+    const Fq2 x3 = Fq2::sub(v[5], Fq2::dbl(d));
+    level(pick(k, e, z3zz, ezz, e, e, e), pick(k, Fq2::sub(d, x3), fq2_of(yp), fq2_of(xp), e, e, e), base, v, 3);
+    l0 = v[1];
+    l1 = Fq2::neg(v[2]);
+    l3 = Fq2::sub(ex, Fq2::dbl(b));
+    t.y = Fq2::sub(v[0], Fq2::dbl(Fq2::dbl(Fq2::dbl(c))));
     t.x = x3;
     t.z = z3;
 }
-// T <- T + S (S affine); returns the line's terms at P.
+// T <- T + S (S affine) and the line at P, in five levels:
+//   ZZ = Z^2 (every lane); U2 = xs ZZ, ZZZ = Z ZZ;
+//   S2 = ys ZZZ, HH = H^2, (Z + H)^2              (H = U2 - X);
+//   J = H I, V = X I, r^2, r xs, r xp, Z3 ys      (I = 4 HH, r = 2(S2 - Y), Z3 = (Z + H)^2 - ZZ - HH);
+//   r (V - X3), Y J, Z3 yp                        (X3 = r^2 - J - 2V).
 __device__ __noinline__ void add_step(Tw& t, const Fq2& xs, const Fq2& ys, const Fq& xp, const Fq& yp, Fq2& l0,
-                                      Fq2& l1, Fq2& l3) {
-    const Fq2 zz = Fq2::sqr(t.z);
-    const Fq2 h = Fq2::sub(Fq2::mul(xs, zz), t.x);
-    const Fq2 r = Fq2::dbl(Fq2::sub(Fq2::mul(ys, Fq2::mul(t.z, zz)), t.y));
-    const Fq2 hh = Fq2::sqr(h);
+                                      Fq2& l1, Fq2& l3, int k, int base) {
+    Fq2 v[6];
+    const Fq2 zz = fq2_mul_fast(t.z, t.z);
+    level(pick(k, xs, t.z, xs, xs, xs, xs), pick(k, zz, zz, zz, zz, zz, zz), base, v, 2);
+    const Fq2 h = Fq2::sub(v[0], t.x), zh = Fq2::add(t.z, h);
+    level(pick(k, ys, h, zh, h, h, h), pick(k, v[1], h, zh, h, h, h), base, v, 3);
+    const Fq2 hh = v[1];
     const Fq2 i = Fq2::dbl(Fq2::dbl(hh));
-    const Fq2 j = Fq2::mul(h, i);
-    const Fq2 v = Fq2::mul(t.x, i);
-    const Fq2 z3 = Fq2::sub(Fq2::sub(Fq2::sqr(Fq2::add(t.z, h)), zz), hh);
-    l0 = Fq2::mul_fq(z3, yp);
-    l1 = Fq2::neg(Fq2::mul_fq(r, xp));
-    l3 = Fq2::sub(Fq2::mul(r, xs), Fq2::mul(z3, ys));
-    const Fq2 x3 = Fq2::sub(Fq2::sub(Fq2::sqr(r), j), Fq2::dbl(v));
-    t.y = Fq2::sub(Fq2::mul(r, Fq2::sub(v, x3)), Fq2::dbl(Fq2::mul(t.y, j)));
+    const Fq2 r = Fq2::dbl(Fq2::sub(v[0], t.y));
+    const Fq2 z3 = Fq2::sub(Fq2::sub(v[2], zz), hh);
+    level(pick(k, h, t.x, r, r, r, z3), pick(k, i, i, r, xs, fq2_of(xp), ys), base, v, 6);
+    const Fq2 j = v[0], vv = v[1], rxs = v[3], rxp = v[4], z3ys = v[5];
+    const Fq2 x3 = Fq2::sub(Fq2::sub(v[2], j), Fq2::dbl(vv));
+    level(pick(k, r, t.y, z3, r, r, r), pick(k, Fq2::sub(vv, x3), j, fq2_of(yp), r, r, r), base, v, 3);
+    l0 = v[2];
+    l1 = Fq2::neg(rxp);
+    l3 = Fq2::sub(rxs, z3ys);
+    t.y = Fq2::sub(v[0], Fq2::dbl(v[1]));
     t.x = x3;
     t.z = z3;
 }
 
-// Miller value of (P, Q) as this lane's coefficient; T and the lines are
-// computed in every lane of the group.
+// Miller value of (P, Q) as this lane's coefficient; every lane holds T and
+// the lines (their products are spread over the group).
 __device__ Fq2 g_miller(const G1A& p, const G2A& q, int k, int base) {
     Tw t{q.x, q.y, Fq2::one()};
     Fq2 f = g_one(k);
     Fq2 l0, l1, l3;
     const Fq2 nqy = Fq2::neg(q.y);
     for (int i = 1; i < NAF_LEN; ++i) {
-        dbl_step(t, p.x, p.y, l0, l1, l3);
+        dbl_step(t, p.x, p.y, l0, l1, l3, k, base);
         f = g_mul_line(g_sqr(f, k, base), l0, l1, l3, k, base);
         const int d = NAF_6Z2[i];
         if (d) {
-            add_step(t, q.x, d > 0 ? q.y : nqy, p.x, p.y, l0, l1, l3);
+            add_step(t, q.x, d > 0 ? q.y : nqy, p.x, p.y, l0, l1, l3, k, base);
             f = g_mul_line(f, l0, l1, l3, k, base);
         }
     }
     // pi(Q) = (conj(x) xi^((q-1)/3), conj(y) xi^((q-1)/2)); -pi^2(Q) = (x xi^((q^2-1)/3), -y xi^((q^2-1)/2))
     const Fq2 x1 = Fq2::mul(Fq2::conj(q.x), frob1(2)), y1 = Fq2::mul(Fq2::conj(q.y), frob1(3));
     const Fq2 x2 = Fq2::mul_fq(q.x, frob2(2)), y2 = Fq2::neg(Fq2::mul_fq(q.y, frob2(3)));
-    add_step(t, x1, y1, p.x, p.y, l0, l1, l3);
+    add_step(t, x1, y1, p.x, p.y, l0, l1, l3, k, base);
     f = g_mul_line(f, l0, l1, l3, k, base);
-    add_step(t, x2, y2, p.x, p.y, l0, l1, l3);
+    add_step(t, x2, y2, p.x, p.y, l0, l1, l3, k, base);
     return g_mul_line(f, l0, l1, l3, k, base);
 }
 
