@@ -42,7 +42,7 @@
 //   T = c^12 b^6, f^l1 = T a^4, f^l2 = T a^6, f^l3 = f^l1 conj(f),
 //   f^l0 = c^12 b^12 a^6 f, result = f^l0 (f^l1)^q (f^l2)^(q^2) (f^l3)^(q^3).
 // conj is the inverse after the easy part (the result is in the
-// cyclotomic subgroup); the easy part's inverse is conj(f) / N with N =
+// cyclotomic subgroup, where squares take the Granger-Scott form); the easy part's inverse is conj(f) / N with N =
 // f conj(f) in Fq6 inverted in every lane.  A verdict is result == 1; the
 // value written for a single pairing is the GT element in the tower order
 // above, canonical.
@@ -205,6 +205,40 @@ __device__ __noinline__ Fq2 g_sqr(const Fq2& a, int k, int base) {
     }
     return acc;
 }
+// Square of an element of the cyclotomic subgroup (every value after the
+// easy part of the final exponentiation), by Granger and Scott ("Faster
+// squaring in the cyclotomic subgroup of sixth degree extensions", PKC
+// 2010): with A_i = f_i + f_(i+3) t over Fq4 = Fq2[t]/(t^2 - xi), t = w^3,
+//   f^2 = (3 A0^2 - 2 conj A0) + (3 t A2^2 + 2 conj A1) w + (3 A1^2 - 2 conj A2) w^2.
+// Lane j < 3 squares a_j = f_j and b_j = f_(j+3), lane j + 3 squares
+// a_j + b_j; A^2 = (a^2 + xi b^2) + ((a + b)^2 - a^2 - b^2) t.
+__device__ __noinline__ Fq2 g_cyc_sqr(const Fq2& f, int k, int base) {
+    const int j = k < 3 ? k : k - 3;
+    const Fq2 a = shfl2(f, base + j), b = shfl2(f, base + j + 3);
+    const Fq2 u = k < 3 ? a : Fq2::add(a, b), v = k < 3 ? b : u;
+    // u^2, v^2: (c0 + c1)(c0 - c1) and c0 c1 of each, four base products in two pairs
+    const Fq::Pair p0 = Fq::mul2(Fq::add(u.c0, u.c1), Fq::sub(u.c0, u.c1), Fq::add(v.c0, v.c1), Fq::sub(v.c0, v.c1));
+    const Fq::Pair p1 = Fq::mul2(u.c0, u.c1, v.c0, v.c1);
+    const Fq2 x = {p0.r0, Fq::dbl(p1.r0)}, y = {p0.r1, Fq::dbl(p1.r1)};
+    Fq2 sa[3], sb[3], sab[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        sa[m] = shfl2(x, base + m);
+        sb[m] = shfl2(y, base + m);
+        sab[m] = shfl2(x, base + 3 + m);
+    }
+    // m = index of the A whose square lane k needs; real part S, t part P
+    const int m = k == 0 || k == 3 ? 0 : (k == 2 || k == 5 ? 1 : 2);
+    const Fq2 sq_a = m == 0 ? sa[0] : (m == 1 ? sa[1] : sa[2]);
+    const Fq2 sq_b = m == 0 ? sb[0] : (m == 1 ? sb[1] : sb[2]);
+    const Fq2 sq_ab = m == 0 ? sab[0] : (m == 1 ? sab[1] : sab[2]);
+    const Fq2 sr = Fq2::add(sq_a, mul_xi(sq_b));
+    const Fq2 pt = Fq2::sub(Fq2::sub(sq_ab, sq_a), sq_b);
+    // k = 0: 3 S0 - 2 f0; 3: 3 P0 + 2 f3; 2: 3 S1 - 2 f2; 5: 3 P1 + 2 f5; 4: 3 S2 - 2 f4; 1: 3 xi P2 + 2 f1
+    const Fq2 term = k == 0 || k == 2 || k == 4 ? sr : (k == 1 ? mul_xi(pt) : pt);
+    const Fq2 t3 = Fq2::add(Fq2::dbl(term), term), f2 = Fq2::dbl(f);
+    return k == 0 || k == 2 || k == 4 ? Fq2::sub(t3, f2) : Fq2::add(t3, f2);
+}
 // f (l0 + l1 w + l3 w^3).
 __device__ __noinline__ Fq2 g_mul_line(const Fq2& f, const Fq2& l0, const Fq2& l1, const Fq2& l3, int k, int base) {
     const Fq2 x[3] = {f, shfl2(f, base + mod6(k - 1)), shfl2(f, base + mod6(k - 3))};
@@ -231,10 +265,11 @@ __device__ __noinline__ Fq2 g_inv(const Fq2& f, int k, int base) {
     const Fq2 mine = (k & 1) ? Fq2::zero() : (k == 0 ? ni.c0 : (k == 2 ? ni.c1 : ni.c2));
     return g_mul(c, mine, k, base);
 }
+// a^z for a in the cyclotomic subgroup, z the BN seed, left to right.
 __device__ __noinline__ Fq2 g_pow_z(const Fq2& a, int k, int base) {
     Fq2 r = a;
     for (int i = 61; i >= 0; --i) {
-        r = g_sqr(r, k, base);
+        r = g_cyc_sqr(r, k, base);
         if ((BN_Z >> i) & 1) r = g_mul(r, a, k, base);
     }
     return r;
@@ -346,9 +381,10 @@ __device__ Fq2 g_final_exponentiation(const Fq2& m, int k, int base) {
     const Fq2 a = g_pow_z(f, k, base);
     const Fq2 b = g_pow_z(a, k, base);
     const Fq2 c = g_pow_z(b, k, base);
-    const Fq2 a2 = g_sqr(a, k, base), a4 = g_sqr(a2, k, base), a6 = g_mul(a4, a2, k, base);
-    const Fq2 b2 = g_sqr(b, k, base), b6 = g_mul(g_sqr(b2, k, base), b2, k, base), b12 = g_sqr(b6, k, base);
-    const Fq2 c4 = g_sqr(g_sqr(c, k, base), k, base), c12 = g_mul(g_sqr(c4, k, base), c4, k, base);
+    const Fq2 a2 = g_cyc_sqr(a, k, base), a4 = g_cyc_sqr(a2, k, base), a6 = g_mul(a4, a2, k, base);
+    const Fq2 b2 = g_cyc_sqr(b, k, base), b6 = g_mul(g_cyc_sqr(b2, k, base), b2, k, base);
+    const Fq2 b12 = g_cyc_sqr(b6, k, base);
+    const Fq2 c4 = g_cyc_sqr(g_cyc_sqr(c, k, base), k, base), c12 = g_mul(g_cyc_sqr(c4, k, base), c4, k, base);
     const Fq2 tt = g_mul(c12, b6, k, base);
     const Fq2 l1 = g_mul(tt, a4, k, base);
     const Fq2 l2 = g_mul(tt, a6, k, base);
