@@ -73,3 +73,5 @@ def test_device_pairing_constants():
     m = re.search(r"NAF_6Z2\[(\d+)\]\s*=\s*\{([^}]*)\}", src)
     assert [int(x) for x in m.group(2).split(",")] == b.naf(6 * b.BN_SEED + 2)
     assert int(re.search(r"BN_Z = (\d+)ull", src).group(1)) == b.BN_SEED
+    m = re.search(r"NAF_Z\[(\d+)\]\s*=\s*\{([^}]*)\}", src)
+    assert [int(x) for x in m.group(2).split(",")] == b.naf(b.BN_SEED)

@@ -86,6 +86,9 @@ __device__ __constant__ uint32_t FROB2[6][8] = {
 __device__ __constant__ int8_t NAF_6Z2[66] = {1, 0, -1, 0, 1, 0, 0, 0, -1, 0, -1, 0, 0, 0, -1, 0, 1, 0, -1, 0, 0, -1, 0, 0, 0, 0, 0, 1, 0, 0, -1, 0, 1, 0, 0, -1, 0, 0, 0, 0, -1, 0, 1, 0, 0, 0, -1, 0, -1, 0, 0, 1, 0, 0, 0, -1, 0, 0, -1, 0, 1, 0, 1, 0, 0, 0};
 constexpr int NAF_LEN = 66;
 constexpr uint64_t BN_Z = 4965661367192848881ull;
+// NAF of z, most significant digit first (weight 24 against 28 binary).
+__device__ __constant__ int8_t NAF_Z[63] = {1, 0, 0, 0, 1, 0, 1, 0, 0, -1, 0, 1, 0, 1, 0, -1, 0, 0, 1, 0, 1, 0, -1, 0, -1, 0, -1, 0, 1, 0, 0, 0, 1, 0, 0, 1, 0, 1, 0, 1, 0, -1, 0, 1, 0, 0, 1, 0, 0, 0, 0, 1, 0, 1, 0, 0, 0, 0, -1, 0, 0, 0, 1};
+constexpr int NAF_Z_LEN = 63;
 
 DV_INL Fq load_fq(const uint32_t* w) {
     Fq r;
@@ -265,12 +268,15 @@ __device__ __noinline__ Fq2 g_inv(const Fq2& f, int k, int base) {
     const Fq2 mine = (k & 1) ? Fq2::zero() : (k == 0 ? ni.c0 : (k == 2 ? ni.c1 : ni.c2));
     return g_mul(c, mine, k, base);
 }
-// a^z for a in the cyclotomic subgroup, z the BN seed, left to right.
+// a^z for a in the cyclotomic subgroup (a^-1 = conj a), z the BN seed, over
+// its NAF.
 __device__ __noinline__ Fq2 g_pow_z(const Fq2& a, int k, int base) {
+    const Fq2 ai = g_conj(a, k);
     Fq2 r = a;
-    for (int i = 61; i >= 0; --i) {
+    for (int i = 1; i < NAF_Z_LEN; ++i) {
         r = g_cyc_sqr(r, k, base);
-        if ((BN_Z >> i) & 1) r = g_mul(r, a, k, base);
+        const int d = NAF_Z[i];
+        if (d) r = g_mul(r, d > 0 ? a : ai, k, base);
     }
     return r;
 }
