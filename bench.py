@@ -1312,6 +1312,23 @@ def run_reference(args, rank, world):
 
 
 # ----------------------------------------------------------------- our arm
+def max_over_ranks(ms, world, device="cuda"):
+    """The slowest rank's time (every rank calls this at the same point)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rates(total_ms, steps, world):
+    """N independent replicas (nothing is sharded): per-step time of the
+    slowest rank, and the whole-job time per unit of work = that / N."""
+    return total_ms / steps, total_ms / (steps * world)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -1388,13 +1405,8 @@ def main():
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
-    value = total_ms / (args.steps * world)
+    total_ms = max_over_ranks(sum(step_ms), world)
+    ms_per_step, value = replica_rates(total_ms, args.steps, world)
 
     # ---- end to end through the C-ABI with pinned host buffers
     op.host_inputs(torch)
@@ -1407,12 +1419,8 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         op.e2e_step(dv, b)
-    e2e_total = (time.perf_counter() - t0) * 1e3
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_ms = e2e_total / (args.e2e_steps * world)
+    e2e_total = max_over_ranks((time.perf_counter() - t0) * 1e3, world)
+    e2e_ms = replica_rates(e2e_total, args.e2e_steps, world)[1]
 
     extra = op.extra(torch, dv, b, s) if hasattr(op, "extra") else {}
     imad_peak = b.probe_imad_rate()
