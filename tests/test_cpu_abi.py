@@ -97,3 +97,39 @@ def test_device_curve_and_psi_constants():
     assert _int_of(_c_array(body, "c1")) == b.B2[1]
     ntt = open(os.path.join(CSRC, "ntt.cu")).read()
     assert _int_of(_c_array(ntt, "ROOT28")) == b.root_of_unity(1 << 28)
+
+
+def test_glv_constants_of_the_g1_transform():
+    """beta/lambda of the G1 endomorphism and the lattice and rounding
+    constants of the GLV split in ecntt.cu, derived here with Python integers
+    (cube roots of unity matched on the generator; the short basis from the
+    extended Euclidean algorithm on (r, lambda), Gallant-Lambert-Vanstone)."""
+    import math
+    src = open(os.path.join(CSRC, "ecntt.cu")).read()
+    q, r = b.Q, b.R
+    roots = lambda p: [pow(g, (p - 1) // 3, p) for g in range(2, 50) if pow(g, (p - 1) // 3, p) != 1][:1]
+    w_q, w_r = roots(q)[0], roots(r)[0]
+    pairs = [(be, la) for be in (w_q, w_q * w_q % q) for la in (w_r, w_r * w_r % r)
+             if (be * b.G1_GEN[0] % q, b.G1_GEN[1]) == b.g1_mul(b.G1_GEN, la)]
+    assert len(pairs) == 2  # (beta, lambda) and (beta^2, lambda^2)
+    mine = [(be, la) for be, la in pairs if (be << 256) % q == _int_of(_c_array(src, "GLV_BETA"))]
+    assert len(mine) == 1
+    beta, lam = mine[0]
+    r0, r1, t0, t1 = r, lam, 0, 1
+    rs, ts = [r0, r1], [t0, t1]
+    while r1:
+        k = r0 // r1
+        r0, r1, t0, t1 = r1, r0 - k * r1, t1, t0 - k * t1
+        rs.append(r1)
+        ts.append(t1)
+    m = max(i for i in range(len(rs)) if rs[i] >= math.isqrt(r))
+    a1, b1 = rs[m + 1], -ts[m + 1]
+    a2, b2 = min([(rs[m], -ts[m]), (rs[m + 2], -ts[m + 2])], key=lambda v: v[0] ** 2 + v[1] ** 2)
+    assert a1 * b2 - a2 * b1 == r
+    g1 = ((b2 << 256) + r // 2) // r
+    g2 = ((-b1 << 256) + r // 2) // r
+    words = lambda name: int("".join(reversed(re.findall(r"0x([0-9a-f]+)ull",
+                                                          re.search(name + r" = \{\{(.*?)\}\}", src).group(1)))), 16)
+    assert int(re.search(r"GLV_A1 = (\d+)ull", src).group(1)) == a1 == b2
+    assert words("GLV_B1ABS") == -b1 and words("GLV_A2") == a2
+    assert words("GLV_G1") == g1 and words("GLV_G2") == g2

@@ -44,6 +44,8 @@ struct NttTables {
     DevBuf pre_hi, pre_lo, post_hi, post_lo;  // two-level scaling tables
     DevBuf consts;     // per-(size, kind) field constants
     int split = 0;     // bits in the low table index
+    DevBuf glv;        // G1 transform: GLV halves of every twiddle and of 1/n (ecntt.cu)
+    int glv_ready = 0;
 };
 
 struct NttWorkspace {
