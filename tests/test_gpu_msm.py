@@ -176,6 +176,55 @@ def test_sparse_resident_matches_oracle(backend, oracle):
         backend.release_bases(h)
 
 
+def test_sparse_direct_small_supports(backend, oracle, dv):
+    """Small sparse requests over a table of window multiples take the direct
+    path (one thread per entry and window, no bucket sort): results equal the
+    oracle's for repeated indices, zero scalars, empty requests and many tiny
+    requests, on both sides of the size limit, and bad inputs are rejected
+    with the owner left healthy."""
+    import torch
+    n = 1 << 12
+    bases, _ = oracle.srs_g1(4096, n)
+    h = backend.register_bases(bases)
+    try:
+        rng = np.random.default_rng(11)
+        sizes = [16, 1, 0, 3, 40] + [2] * 20
+        reqs = []
+        for j, k in enumerate(sizes):
+            idx = rng.choice(n, size=k, replace=False).astype(np.uint64)
+            reqs.append((idx, oracle.uniform_fr(1200 + j, k)))
+        reqs.append((np.array([5, 5, 9], dtype=np.uint64), (3).to_bytes(32, "little") + bytes(32) + (7).to_bytes(32, "little")))
+        idx_all = np.concatenate([r[0] for r in reqs])
+        vals_all = b"".join(r[1] for r in reqs)
+        offs = np.concatenate([[0], np.cumsum([len(r[0]) for r in reqs])])
+        expect = [oracle.sparse_msm_g1(bases, idx, vals) for idx, vals in reqs]
+        for c in (8, 11, 0):
+            backend.precompute_bases(h, c)
+            assert backend.sparse_msm_resident(h, idx_all, vals_all, offs) == expect, c
+            d_idx = torch.from_numpy(idx_all.view(np.int64)).cuda()
+            d_vals = torch.frombuffer(bytearray(vals_all), dtype=torch.uint8).cuda()
+            assert backend.sparse_msm_device(h, d_idx.data_ptr(), d_vals.data_ptr(), offs) == expect, c
+        # just below and above the direct path's limit (c = 8: 32 windows, 2^14 terms)
+        backend.precompute_bases(h, 8)
+        for k in (512, 513):
+            idx = rng.choice(n, size=k, replace=False).astype(np.uint64)
+            vals = oracle.uniform_fr(1300 + k, k)
+            assert backend.sparse_msm_resident(h, idx, vals, [0, k]) == [oracle.sparse_msm_g1(bases, idx, vals)]
+        bad_idx = torch.tensor([1, n], dtype=torch.int64, device="cuda")
+        two = torch.frombuffer(bytearray(oracle.uniform_fr(1400, 2)), dtype=torch.uint8).cuda()
+        with pytest.raises(dv.DvgpuError) as e:
+            backend.sparse_msm_device(h, bad_idx.data_ptr(), two.data_ptr(), [0, 2])
+        assert e.value.status == -1 and "out of range" in e.value.message
+        r_mod = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+        with pytest.raises(dv.DvgpuError) as e:
+            backend.sparse_msm_resident(h, np.array([1, 2], dtype=np.uint64), bytes(32) + r_mod.to_bytes(32, "little"),
+                                        [0, 2])
+        assert e.value.status == -1 and "non-canonical scalar at index 1" in e.value.message
+        assert backend.sparse_msm_resident(h, idx_all, vals_all, offs) == expect  # owner still healthy
+    finally:
+        backend.release_bases(h)
+
+
 def test_autotune_picks_a_window_and_results_stay_exact(dv, oracle):
     with dv.DvgpuBackend() as b:
         c, log = b.autotune_msm(4096)

@@ -394,6 +394,12 @@ void sparse_run(Backend& b, const ResidentBases& rb, const uint64_t* d_idx, cons
     const uint64_t k_total = offs[count];
     uint32_t* bad = b.err.as<uint32_t>(1);
     DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
+    if (rb.pre_c && k_total * (uint64_t)rb.pre_windows <= SPARSE_DIRECT_MAX_TERMS) {
+        const MsmPrecomp<Fq> pre{rb.pre_table.view<G1A>(), rb.pre_c, rb.pre_windows};
+        msm_sparse_direct(b.msm, pre, rb.n, d_idx, reinterpret_cast<const uint32_t*>(d_vals), offs.data(), count,
+                          out, st);
+        return;
+    }
     if (rb.pre_c) {
         G1A* gathered = b.conv_points.as<G1A>(k_total * rb.pre_windows);
         gather_table<Fq>(rb.pre_table.view<G1A>(), rb.n, rb.pre_windows, d_idx, k_total, gathered, bad, st);

@@ -781,6 +781,121 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
     }
 }
 
+// ---------------------------------------------------------------- direct small sparse MSMs
+constexpr int SD_BLOCK = 256;
+struct SdJob {
+    uint32_t request, first, items, pad;  // terms first .. first + items - 1 (term = entry W + window)
+};
+
+__global__ void __launch_bounds__(SD_BLOCK) k_sparse_direct(const G1A* __restrict__ table, uint64_t nbases, int c,
+                                                            int W, const uint64_t* __restrict__ idx,
+                                                            const uint32_t* __restrict__ vals,
+                                                            const SdJob* __restrict__ jobs,
+                                                            XYZZ<Fq>* __restrict__ partial, uint32_t* __restrict__ err) {
+    __shared__ XYZZ<Fq> sm[SD_BLOCK];
+    const SdJob job = jobs[blockIdx.x];
+    XYZZ<Fq> p = XYZZ<Fq>::inf();
+    if (threadIdx.x < job.items) {
+        const uint32_t term = job.first + threadIdx.x;
+        const uint32_t e = term / (uint32_t)W, w = term % (uint32_t)W;
+        uint32_t s[8];
+        load_scalar(vals, e, s);
+        const uint64_t ix = idx[e];
+        if (!Fr::is_canonical(s)) {
+            if (w == 0) atomicMin(err, e);
+        } else if (ix >= nbases) {
+            if (w == 0) atomicMin(err + 1, e);
+        } else {
+            // signed digit of window w (the recoding of k_hist)
+            const uint32_t B = 1u << (c - 1), full = 1u << c;
+            uint32_t carry = 0, mag = 0;
+            bool neg = false;
+            for (uint32_t v = 0; v <= w; ++v) {
+                const uint32_t d = window_raw(s, (int)v * c, c) + carry;
+                neg = d > B;
+                mag = neg ? full - d : d;
+                carry = neg ? 1u : 0u;
+            }
+            const G1A t = table[ix * (uint64_t)W + w];
+            if (mag && !t.is_inf()) {
+                p = XYZZ<Fq>::from_affine(t);
+                for (int b = 30 - __clz(mag); b >= 0; --b) {
+                    p = XYZZ<Fq>::dbl_paired(p);
+                    if ((mag >> b) & 1) p = XYZZ<Fq>::add_affine(p, t);
+                }
+                if (neg) p = p.neg();
+            }
+        }
+    }
+    sm[threadIdx.x] = p;
+    __syncthreads();
+    for (int stride = SD_BLOCK / 2; stride > 0; stride >>= 1) {
+        if (threadIdx.x < (unsigned)stride)
+            sm[threadIdx.x] = XYZZ<Fq>::add_paired(sm[threadIdx.x], sm[threadIdx.x + stride]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+
+constexpr int SD_FINAL = 64;
+__global__ void __launch_bounds__(SD_FINAL) k_sparse_direct_final(const XYZZ<Fq>* __restrict__ partial,
+                                                                  const uint32_t* __restrict__ req_blocks,
+                                                                  XYZZ<Fq>* __restrict__ out) {
+    __shared__ XYZZ<Fq> sm[SD_FINAL];
+    const uint32_t r = blockIdx.x;
+    XYZZ<Fq> p = XYZZ<Fq>::inf();
+    for (uint32_t b = req_blocks[r] + threadIdx.x; b < req_blocks[r + 1]; b += SD_FINAL)
+        p = XYZZ<Fq>::add_paired(p, partial[b]);
+    sm[threadIdx.x] = p;
+    __syncthreads();
+    for (int stride = SD_FINAL / 2; stride > 0; stride >>= 1) {
+        if (threadIdx.x < (unsigned)stride)
+            sm[threadIdx.x] = XYZZ<Fq>::add_paired(sm[threadIdx.x], sm[threadIdx.x + stride]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[r] = sm[0];
+}
+
+void msm_sparse_direct(MsmWorkspace& ws, const MsmPrecomp<Fq>& pre, uint64_t nbases, const uint64_t* d_idx,
+                       const uint32_t* d_vals, const uint32_t* offs, uint32_t count, uint8_t* host_out,
+                       cudaStream_t st) {
+    const uint32_t W = (uint32_t)pre.windows;
+    std::vector<SdJob> jobs;
+    std::vector<uint32_t> req_blocks(count + 1, 0);
+    for (uint32_t r = 0; r < count; ++r) {
+        const uint32_t first = offs[r] * W, terms = (offs[r + 1] - offs[r]) * W;
+        for (uint32_t t = 0; t < terms; t += SD_BLOCK)
+            jobs.push_back(SdJob{r, first + t, std::min<uint32_t>(SD_BLOCK, terms - t), 0});
+        req_blocks[r + 1] = (uint32_t)jobs.size();
+    }
+    if (jobs.empty()) {
+        memset(host_out, 0, (size_t)count * 64);
+        return;
+    }
+    SdJob* d_jobs = ws.sd_jobs.as<SdJob>(jobs.size());
+    uint32_t* d_req = ws.sd_req.as<uint32_t>(count + 1);
+    XYZZ<Fq>* d_partial = ws.sd_partial.as<XYZZ<Fq>>(jobs.size());
+    XYZZ<Fq>* d_out = ws.sd_out.as<XYZZ<Fq>>(count);
+    uint32_t* d_err = ws.err.as<uint32_t>(2);
+    DV_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(SdJob), cudaMemcpyHostToDevice, st));
+    DV_CUDA(cudaMemcpyAsync(d_req, req_blocks.data(), (count + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    DV_CUDA(cudaMemsetAsync(d_err, 0xff, 2 * sizeof(uint32_t), st));
+    k_sparse_direct<<<(unsigned)jobs.size(), SD_BLOCK, 0, st>>>(pre.table, nbases, pre.c, (int)W, d_idx, d_vals,
+                                                               d_jobs, d_partial, d_err);
+    DV_LAUNCH();
+    k_sparse_direct_final<<<count, SD_FINAL, 0, st>>>(d_partial, d_req, d_out);
+    DV_LAUNCH();
+    XYZZ<Fq>* h_out = ws.host_windows.as<XYZZ<Fq>>(count);
+    uint32_t* h_err = ws.host_err.as<uint32_t>(2);
+    DV_CUDA(cudaMemcpyAsync(h_out, d_out, (size_t)count * sizeof(XYZZ<Fq>), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaMemcpyAsync(h_err, d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaStreamSynchronize(st));
+    if (h_err[0] != NO_INDEX) throw InvalidArgument("non-canonical scalar at index " + std::to_string(h_err[0]));
+    if (h_err[1] != NO_INDEX) throw InvalidArgument("sparse MSM index out of range");
+    static_assert(sizeof(XYZZ<Fq>) == sizeof(dvh::XYZZ<dvh::Fq>), "host/device XYZZ layout");
+    dvh::xyzz_batch_to_affine_bytes(reinterpret_cast<const dvh::XYZZ<dvh::Fq>*>(h_out), count, host_out);
+}
+
 template void msm_run<Fq>(MsmWorkspace&, const Affine<Fq>*, const uint32_t*, const uint32_t*, uint32_t, int,
                           cudaStream_t, uint8_t*, MsmStats*, const MsmPrecomp<Fq>*);
 template void msm_run<Fq2>(MsmWorkspace&, const Affine<Fq2>*, const uint32_t*, const uint32_t*, uint32_t, int,

@@ -59,6 +59,7 @@ struct MsmTimeline {
 struct MsmWorkspace {
     DevBuf set_off, counts, offsets, cursor, scan_tiles, sorted, buckets, pgid, ppt, fix_list, fix_count, segs, windows,
         err;
+    DevBuf sd_jobs, sd_req, sd_partial, sd_out;  // direct small sparse MSMs
     PinnedBuf host_windows, host_err;
     MsmTimeline timeline;
 };
@@ -82,6 +83,19 @@ struct MsmPrecomp {
 // set_offsets (host, count + 1 entries) delimit the sets.  host_out receives
 // count canonical affine points (2 * sizeof(F) bytes each, all-zero for
 // infinity).  Throws InvalidArgument for non-canonical scalars.
+// Sparse MSMs over a resident table of window multiples, summed directly:
+// each (entry, window) term d T is formed by one thread (double-and-add on
+// the signed c-bit digit d), then block and request sums.  For small
+// supports, where the bucket pipeline's launch chain dominates.  d_idx:
+// entry base indices (checked < nbases), d_vals: canonical scalars (checked),
+// offs (host, count + 1): entries of each request.  host_out: count
+// canonical affine G1 points.  Throws InvalidArgument as msm_run does.
+void msm_sparse_direct(MsmWorkspace& ws, const MsmPrecomp<Fq>& pre, uint64_t nbases, const uint64_t* d_idx,
+                       const uint32_t* d_vals, const uint32_t* offs, uint32_t count, uint8_t* host_out,
+                       cudaStream_t stream);
+// Terms (entries x windows) up to which sparse calls take the direct path.
+constexpr uint64_t SPARSE_DIRECT_MAX_TERMS = 1u << 14;
+
 template <class F>
 void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const uint32_t* set_offsets,
              uint32_t count, int force_c, cudaStream_t stream, uint8_t* host_out, MsmStats* stats,
