@@ -349,6 +349,14 @@ __global__ void __launch_bounds__(128) k_segments(const XYZZ<F>* __restrict__ bu
 // Upper levels: blocks of P pairs (G = P), suffix scan and tree in shared
 // memory.  Windows of S pairs; S <= P is the last level (one block per
 // window, its U' is S_w).
+// Additions of the upper levels: few threads per window on a dependent
+// chain, so over Fq the products go out in pairs.
+template <class F>
+DV_INL XYZZ<F> wadd(const XYZZ<F>& p, const XYZZ<F>& q) {
+    if constexpr (sizeof(F) == sizeof(Fq)) return XYZZ<F>::add_paired(p, q);
+    else return XYZZ<F>::add(p, q);
+}
+
 template <class F, int P>
 __global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, const XYZZ<F>* __restrict__ v_in,
                                               uint32_t S, XYZZ<F>* __restrict__ u_out, XYZZ<F>* __restrict__ v_out) {
@@ -365,17 +373,17 @@ __global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, 
     for (uint32_t d = 1; d < width; d <<= 1) {
         const XYZZ<F> o = t + d < width ? sh[t + d] : XYZZ<F>::inf();
         __syncthreads();
-        if (t + d < width) sh[t] = XYZZ<F>::add(sh[t], o);
+        if (t + d < width) sh[t] = wadd<F>(sh[t], o);
         __syncthreads();
     }
     XYZZ<F> x = t + 1 < width ? sh[t + 1] : XYZZ<F>::inf();  // Suf_{t+1}
     XYZZ<F> vsum = sh[0];
     __syncthreads();
-    if (live) x = XYZZ<F>::add(x, u_in[idx]);
+    if (live) x = wadd<F>(x, u_in[idx]);
     sh[t] = x;
     __syncthreads();
     for (uint32_t d = (uint32_t)P / 2; d > 0; d >>= 1) {
-        if (t < d) sh[t] = XYZZ<F>::add(sh[t], sh[t + d]);
+        if (t < d) sh[t] = wadd<F>(sh[t], sh[t + d]);
         __syncthreads();
     }
     if (t == 0) {
