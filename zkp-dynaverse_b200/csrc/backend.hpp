@@ -1,7 +1,9 @@
 // Owner ("backend") object behind the opaque void* of the C-ABI.
 //
-// Mirrors the reference owner (native/src/icicle_msm.cu:92-144): created on
-// visible device 0, used by one caller thread at a time, retired by any CUDA
+// Mirrors the reference owner (native/src/icicle_msm.cu:92-144), which is
+// created on visible device 0; here it is created on the calling thread's
+// current device (device 0 unless the caller chose another, e.g. one GPU per
+// rank).  Used by one caller thread at a time, retired by any CUDA
 // failure (later calls return -4), destroyed by dvgpu_backend_destroy.
 // Unlike the reference it uses the device's primary context, so device
 // pointers from other runtime users (e.g. torch) are valid in the

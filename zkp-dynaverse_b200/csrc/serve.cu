@@ -452,7 +452,7 @@ extern "C" int dvgpu_serve_create(uint64_t hbm_budget_bytes, uint32_t max_batch,
     return dv::serve_guard(error, cap, [&] {
         if (!server) throw dv::InvalidArgument("null server output");
         *server = nullptr;
-        DV_CUDA(cudaSetDevice(0));
+        // the calling thread's current device (one server per GPU, e.g. one per rank)
         *server = new Server(hbm_budget_bytes, max_batch);
     });
 }
