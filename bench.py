@@ -697,7 +697,7 @@ class ServeOp:
                 "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1], "mean_ms": sum(lat) / len(lat),
                 "batches": st.batches - before.batches, "largest_batch": max(r.batch_requests for _, r in outs)}
 
-    def run_standalone(self, args, torch, dv, b, s, sampler, imad_peak_fn):
+    def run_standalone(self, args, torch, dv, b, s, sampler, imad_peak_fn, world=1):
         import numpy as np
         self._inputs(torch, b, s)
         zeros = [0.0] * self.requests
@@ -705,7 +705,9 @@ class ServeOp:
         self._run(srv, 64, zeros)  # warm-up: workspaces reach their working size
         self._run(srv, 1, zeros[:200])
         sampler.start()
+        launches0 = b.launch_count()
         sat_served = self._run(srv, 64, zeros)
+        launches = b.launch_count() - launches0
         sat_plain = self._run(srv, 1, zeros)
         rate = 0.8 * sat_plain["per_s"]
         arrivals = np.cumsum(np.random.default_rng(5001).exponential(1.0 / rate, self.requests)).tolist()
@@ -728,15 +730,18 @@ class ServeOp:
         ach = macs / sat_served["wall_s"] / 1e12
         peak = imad_peak_fn() / 1e12
         strip = lambda r: {k: v for k, v in r.items() if k != "commitments"}
+        # N replicas (one server per GPU): whole-job rate over the slowest rank's saturation run
+        job_per_s = world * self.requests / max_over_ranks(sat_served["wall_s"], world)
         line = {
-            "metric": self.metric, "value": sat_served["per_s"], "unit": "updates/s", "n_gpus": 1,
+            "metric": self.metric, "value": job_per_s, "unit": "updates/s", "n_gpus": world,
             "steps": self.requests, "warmup": 1, "ms_per_step": 1e3 / sat_served["per_s"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Fq/Fr Montgomery, exact)",
             "data": "synthetic",
-            "config": {"workload": self.workload, "op": "serve", "parallelism": "single GPU",
+            "config": {"workload": self.workload, "op": "serve",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "sessions": len(self.SIZES), "requests": self.requests, "entries": self.entries,
                        "l2": "not flushed: a stream of small requests against resident sessions"},
-            "e2e": {"value": sat_served["per_s"], "unit": "updates/s",
+            "e2e": {"value": job_per_s, "unit": "updates/s",
                     "h2d_bytes_per_step": 40 * self.entries / self.requests, "d2h_bytes_per_step": 64,
                     "call": "dvgpu_serve_submit/wait from host memory (the serving API is host-to-host)"},
             "serving": {"saturation": {"served": strip(sat_served), "per_call": strip(sat_plain),
@@ -748,9 +753,9 @@ class ServeOp:
             "roofline": {"bound": "imad", "kernel": "all launches of the saturation run (sparse delta MSMs)",
                          "achieved": ach, "peak": peak, "unit": "TMAC/s", "frac": ach / peak,
                          "algorithmic_macs_per_launch": macs, "traffic": None},
-            "gpu_launches": None, "clocks": clocks,
+            "gpu_launches": launches, "clocks": clocks,
         }
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:
             from oracle import oracle
             threads = os.cpu_count() or 1
             sample = self.reqs[:200]
@@ -1371,10 +1376,12 @@ def main():
         except AttributeError:
             bus = None
         sampler = ClockSampler(bus if isinstance(bus, str) else None)
-        line = op.run_standalone(args, torch, dv, b, s, sampler, b.probe_imad_rate)
+        line = op.run_standalone(args, torch, dv, b, s, sampler, b.probe_imad_rate, world)
         if rank == 0:
             print(json.dumps(line), flush=True)
         b.close()
+        if world > 1:
+            dist.destroy_process_group()
         return
     op.setup(torch, b, s, rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
