@@ -280,6 +280,21 @@ int dvgpu_bn254_pairing_check(void* backend, const uint8_t* g1, const uint8_t* g
  * exponent is (q^12 - 1)/r times 2z(6z^2 + 3z + 1). */
 int dvgpu_bn254_pairing(void* backend, const uint8_t* g1, const uint8_t* g2, size_t n, uint8_t* gt, char* error,
                         size_t error_capacity);
+/* Prepared G2 points (arkworks G2Prepared; the verifier caches one per
+ * distinct G2 point, crates/protocol/src/verification.rs:105-126, and the
+ * rebuild checks use fixed preparations, :55-77): the 88 lines of each
+ * point's Miller loop are computed once and kept on the device under a
+ * handle (at most 2^17 points, 17 KB each).  dvgpu_bn254_pairing_check
+ * prepares the distinct G2 points of a call by itself when some repeat;
+ * these entry points keep preparations across calls.  In
+ * dvgpu_bn254_pairing_check_prepared term k pairs g1[k] with prepared point
+ * q_index[k]; equations and verdicts as dvgpu_bn254_pairing_check. */
+int dvgpu_bn254_g2_prepare(void* backend, const uint8_t* g2, size_t n, uint64_t* prepared, char* error,
+                           size_t error_capacity);
+int dvgpu_bn254_g2_prepared_release(void* backend, uint64_t prepared, char* error, size_t error_capacity);
+int dvgpu_bn254_pairing_check_prepared(void* backend, const uint8_t* g1, uint64_t prepared, const uint32_t* q_index,
+                                       const uint64_t* offsets, size_t equations, uint8_t* verdicts, char* error,
+                                       size_t error_capacity);
 
 /* ---------------------------------------------------------------- polynomial toolkit
  * The field work of a sparse update (crates/protocol/src/domain/fast.rs,

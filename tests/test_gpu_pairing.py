@@ -106,3 +106,49 @@ def test_invalid_points_are_rejected(backend, oracle, dv):
     with pytest.raises(dv.DvgpuError):
         backend.pairing_check(gen1, gen2, [1, 1])
     assert backend.pairing_check(gen1, gen2, [0, 0, 1]) == [True, False]
+
+
+def test_prepared_g2_points_across_calls(backend, oracle, dv):
+    """Preparations kept on the device (G2Prepared): the same verdicts as the
+    plain check for equations that share prepared points, through two calls,
+    plus infinity, empty equations and bad handles or indices."""
+    n = 48
+    sa, sc = oracle.uniform_fr(5101, n), oracle.uniform_fr(5102, n)
+    ints = lambda buf: [int.from_bytes(buf[32 * i:32 * i + 32], "little") for i in range(len(buf) // 32)]
+    a, c = ints(sa), ints(sc)
+    one = (1).to_bytes(32, "little")
+    # prepared points: [c_0]G2 .. [c_3]G2, the generator, infinity
+    qs = oracle.fixed_base_g2(sc[:128] + one) + bytes(128)
+    h = backend.g2_prepare(qs)
+    try:
+        g1, qidx, plain_g2, offsets = [], [], [], [0]
+        for k in range(n):
+            j = k % 4
+            x = a[k] * c[j] % R_MOD
+            if k % 3 == 1:
+                x = (x + 1) % R_MOD
+            p1 = oracle.fixed_base_g1(sa[32 * k:32 * k + 32])
+            p2 = _neg_g1(oracle.fixed_base_g1(x.to_bytes(32, "little")))
+            terms = [(p1, j), (p2, 4)]
+            if k % 5 == 0:
+                terms.append((p1, 5))  # infinity on the G2 side contributes one
+            for p, q in terms:
+                g1.append(p)
+                qidx.append(q)
+                plain_g2.append(qs[128 * q:128 * q + 128])
+            offsets.append(offsets[-1] + len(terms))
+        offsets.append(offsets[-1])  # an empty equation holds
+        g1 = b"".join(g1)
+        expect = backend.pairing_check(g1, b"".join(plain_g2), offsets)
+        assert expect == oracle.pairing_check(g1, b"".join(plain_g2), offsets)
+        assert expect[-1] and sum(expect) == 1 + sum(1 for k in range(n) if k % 3 != 1)
+        for _ in range(2):
+            assert backend.pairing_check_prepared(g1, h, qidx, offsets) == expect
+        with pytest.raises(dv.DvgpuError, match="index out of range"):
+            backend.pairing_check_prepared(g1[:64], h, [6], [0, 1])
+    finally:
+        backend.g2_prepared_release(h)
+    with pytest.raises(dv.DvgpuError, match="unknown prepared"):
+        backend.pairing_check_prepared(g1[:64], h, [0], [0, 1])
+    with pytest.raises(dv.DvgpuError, match="invalid G2 point at index 1"):
+        backend.g2_prepare(qs[:128] + one + one + bytes(64))

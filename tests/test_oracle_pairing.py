@@ -73,5 +73,8 @@ def test_device_pairing_constants():
     m = re.search(r"NAF_6Z2\[(\d+)\]\s*=\s*\{([^}]*)\}", src)
     assert [int(x) for x in m.group(2).split(",")] == b.naf(6 * b.BN_SEED + 2)
     assert int(re.search(r"BN_Z = (\d+)ull", src).group(1)) == b.BN_SEED
+    naf = b.naf(6 * b.BN_SEED + 2)
+    lines = (len(naf) - 1) + sum(1 for d in naf[1:] if d) + 2  # doublings, additions, two Frobenius lines
+    assert int(re.search(r"constexpr int LINES = (\d+);", src).group(1)) == lines
     m = re.search(r"NAF_Z\[(\d+)\]\s*=\s*\{([^}]*)\}", src)
     assert [int(x) for x in m.group(2).split(",")] == b.naf(b.BN_SEED)

@@ -165,6 +165,9 @@ SIGNATURES = [
     ("dvgpu_bn254_g1_ntt_rows_device", ctypes.c_int, [_P, _P, _SZ, _SZ, ctypes.c_int, _P, _P] + _E),
     ("dvgpu_bn254_pairing_check", ctypes.c_int, [_P, _B, _B, _P, _SZ, _B] + _E),
     ("dvgpu_bn254_pairing", ctypes.c_int, [_P, _B, _B, _SZ, _B] + _E),
+    ("dvgpu_bn254_g2_prepare", ctypes.c_int, [_P, _B, _SZ, ctypes.POINTER(ctypes.c_uint64)] + _E),
+    ("dvgpu_bn254_g2_prepared_release", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
+    ("dvgpu_bn254_pairing_check_prepared", ctypes.c_int, [_P, _B, ctypes.c_uint64, _P, _P, _SZ, _B] + _E),
     ("dvgpu_bn254_poly_multiply", ctypes.c_int, [_P, _B, _SZ, _B, _SZ, _B, _SZ, ctypes.POINTER(_SZ)] + _E),
     ("dvgpu_bn254_poly_divide_exact", ctypes.c_int, [_P, _B, _SZ, _B, _SZ, _B, _SZ, ctypes.POINTER(_SZ)] + _E),
     ("dvgpu_bn254_tree_create", ctypes.c_int, [_P, _B, _SZ, ctypes.POINTER(ctypes.c_uint64)] + _E),
@@ -654,6 +657,26 @@ class DvgpuBackend:
         eqs = len(off) - 1
         out = ctypes.create_string_buffer(max(1, eqs))
         self._call("dvgpu_bn254_pairing_check", g1, g2, off.ctypes.data, eqs, out)
+        return [bool(x) for x in out.raw[:eqs]]
+
+    def g2_prepare(self, g2: bytes) -> int:
+        """Prepared G2 points (their Miller-loop lines kept on the device)."""
+        h = ctypes.c_uint64()
+        self._call("dvgpu_bn254_g2_prepare", g2, len(g2) // G2_BYTES, ctypes.byref(h))
+        return h.value
+
+    def g2_prepared_release(self, handle: int):
+        self._call("dvgpu_bn254_g2_prepared_release", handle)
+
+    def pairing_check_prepared(self, g1: bytes, handle: int, q_index, offsets) -> list:
+        """Verdicts with term k = (g1[k], prepared point q_index[k])."""
+        import numpy as np
+        qi = np.ascontiguousarray(np.asarray(q_index, dtype=np.uint32))
+        off = np.ascontiguousarray(np.asarray(offsets, dtype=np.uint64))
+        eqs = len(off) - 1
+        out = ctypes.create_string_buffer(max(1, eqs))
+        self._call("dvgpu_bn254_pairing_check_prepared", g1, handle, qi.ctypes.data if qi.size else None,
+                   off.ctypes.data, eqs, out)
         return [bool(x) for x in out.raw[:eqs]]
 
     def pairing(self, g1: bytes, g2: bytes) -> bytes:

@@ -190,6 +190,7 @@ void Backend::release_all() noexcept {
     plans.clear();
     resident.reset();
     poly.reset();
+    pairing.reset();
     bases.clear();
     MsmTimeline& tl = msm.timeline;
     for (auto& e : tl.ev)

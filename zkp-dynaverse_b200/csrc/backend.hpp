@@ -36,6 +36,7 @@ struct ResidentBases {
 
 struct ResidentState;  // resident.cu
 struct PolyState;      // poly.cu
+struct PairingState;   // pairing.cu
 
 struct Backend {
     int device = 0;
@@ -63,6 +64,7 @@ struct Backend {
     std::map<uint64_t, std::unique_ptr<BatchPlan>> plans;  // CUDA-graph batch plans
     std::shared_ptr<ResidentState> resident;                // resident transactional buffers
     std::shared_ptr<PolyState> poly;                        // subproduct trees and polynomial scratch
+    std::shared_ptr<PairingState> pairing;                  // prepared G2 points and pairing scratch
     uint64_t next_handle = 1;
 
     void release_all() noexcept;

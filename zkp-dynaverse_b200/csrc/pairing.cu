@@ -47,6 +47,9 @@
 // value written for a single pairing is the GT element in the tower order
 // above, canonical.
 #include <cstring>
+#include <map>
+#include <memory>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -356,6 +359,127 @@ __device__ __noinline__ void add_step(Tw& t, const Fq2& xs, const Fq2& ys, const
     t.z = z3;
 }
 
+struct GroupLane {
+    int k, base;
+    uint64_t group;  // global group index
+    bool live;       // lanes 0..29 of the warp
+};
+DV_INL GroupLane group_lane() {
+    const int l = threadIdx.x & 31;
+    const int k = l < GL * GROUPS_PER_WARP ? l % GL : l - GL * GROUPS_PER_WARP;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    return {k, l - k, warp * GROUPS_PER_WARP + (uint64_t)(l / GL), l < GL * GROUPS_PER_WARP};
+}
+
+// ------------------------------------------------------------------ prepared G2 points
+// A line of the Miller loop at P = (xp, yp) is A yp + (B xp) w + C w^3 with
+// A, B, C depending on Q alone (the doubling: A = 2 Y Z^3, B = -3 X^2 Z^2,
+// C = 3 X^3 - 2 Y^2; the addition: A = 2 Z H, B = -2 R, C = 2 R xs - 2 Z H ys).
+// Preparing Q records the LINES triples of its loop once -- arkworks'
+// G2Prepared, which the reference caches per distinct G2 point
+// (crates/protocol/src/verification.rs:105-126) -- so the loop of every term
+// that shares Q only scales them by its P and multiplies them in.
+struct __align__(16) Line {
+    Fq2 a, b, c;
+};
+constexpr int LINES = 88;  // 65 doublings, 21 NAF additions (nonzero digits after the first), 2 Frobenius additions
+
+// The doubling and addition steps without P: the same levels, minus the
+// products by xp and yp.
+__device__ __noinline__ void prep_dbl(Tw& t, Line& l, int k, int base) {
+    Fq2 v[6];
+    level(pick(k, t.x, t.y, t.z, t.y, t.x, t.x), pick(k, t.x, t.y, t.z, t.z, t.x, t.x), base, v, 4);
+    const Fq2 a = v[0], b = v[1], zz = v[2];
+    const Fq2 e = Fq2::add(Fq2::dbl(a), a), z3 = Fq2::dbl(v[3]), xb = Fq2::add(t.x, b);
+    level(pick(k, b, xb, e, z3, e, e), pick(k, b, xb, zz, zz, t.x, e), base, v, 6);
+    const Fq2 c = v[0], ezz = v[2], z3zz = v[3], ex = v[4];
+    const Fq2 d = Fq2::dbl(Fq2::sub(Fq2::sub(v[1], a), c));
+    const Fq2 x3 = Fq2::sub(v[5], Fq2::dbl(d));
+    level(e, Fq2::sub(d, x3), base, v, 1);
+    l = {z3zz, Fq2::neg(ezz), Fq2::sub(ex, Fq2::dbl(b))};
+    t.y = Fq2::sub(v[0], Fq2::dbl(Fq2::dbl(Fq2::dbl(c))));
+    t.x = x3;
+    t.z = z3;
+}
+__device__ __noinline__ void prep_add(Tw& t, const Fq2& xs, const Fq2& ys, Line& l, int k, int base) {
+    Fq2 v[6];
+    const Fq2 zz = fq2_mul_fast(t.z, t.z);
+    level(pick(k, xs, t.z, xs, xs, xs, xs), pick(k, zz, zz, zz, zz, zz, zz), base, v, 2);
+    const Fq2 h = Fq2::sub(v[0], t.x), zh = Fq2::add(t.z, h);
+    level(pick(k, ys, h, zh, h, h, h), pick(k, v[1], h, zh, h, h, h), base, v, 3);
+    const Fq2 hh = v[1];
+    const Fq2 i = Fq2::dbl(Fq2::dbl(hh));
+    const Fq2 r = Fq2::dbl(Fq2::sub(v[0], t.y));
+    const Fq2 z3 = Fq2::sub(Fq2::sub(v[2], zz), hh);
+    level(pick(k, h, t.x, r, r, z3, r), pick(k, i, i, r, xs, ys, r), base, v, 5);
+    const Fq2 j = v[0], vv = v[1], rxs = v[3], z3ys = v[4];
+    const Fq2 x3 = Fq2::sub(Fq2::sub(v[2], j), Fq2::dbl(vv));
+    level(pick(k, r, t.y, r, r, r, r), pick(k, Fq2::sub(vv, x3), j, r, r, r, r), base, v, 2);
+    l = {z3, Fq2::neg(r), Fq2::sub(rxs, z3ys)};
+    t.y = Fq2::sub(v[0], Fq2::dbl(v[1]));
+    t.x = x3;
+    t.z = z3;
+}
+
+// The LINES triples of every Q (one lane group each) at lines[LINES q ..].
+__global__ void __launch_bounds__(128) k_prepare(const G2A* __restrict__ g2, uint64_t nq, Line* __restrict__ lines) {
+    const GroupLane g = group_lane();
+    const bool mine = g.live && g.group < nq;
+    const uint64_t qi = mine ? g.group : 0;
+    const G2A q = g2[qi];
+    Line* out = lines + (uint64_t)LINES * qi;
+    Tw t{q.x, q.y, Fq2::one()};
+    Line l;
+    int n = 0;
+    const Fq2 nqy = Fq2::neg(q.y);
+    auto put = [&](const Line& x) {
+        if (mine && g.k < 3) (&out[n].a)[g.k] = (&x.a)[g.k];
+        ++n;
+    };
+    for (int i = 1; i < NAF_LEN; ++i) {
+        prep_dbl(t, l, g.k, g.base);
+        put(l);
+        const int d = NAF_6Z2[i];
+        if (d) {
+            prep_add(t, q.x, d > 0 ? q.y : nqy, l, g.k, g.base);
+            put(l);
+        }
+    }
+    const Fq2 x1 = Fq2::mul(Fq2::conj(q.x), frob1(2)), y1 = Fq2::mul(Fq2::conj(q.y), frob1(3));
+    const Fq2 x2 = Fq2::mul_fq(q.x, frob2(2)), y2 = Fq2::neg(Fq2::mul_fq(q.y, frob2(3)));
+    prep_add(t, x1, y1, l, g.k, g.base);
+    put(l);
+    prep_add(t, x2, y2, l, g.k, g.base);
+    put(l);
+}
+
+// Miller value of term t from its P and its prepared Q (one lane group per
+// term; coefficient k at out[6 t + k]); infinity on either side gives one.
+__global__ void __launch_bounds__(128) k_miller_prepared(const G1A* __restrict__ g1, const uint32_t* __restrict__ qidx,
+                                                         const G2A* __restrict__ g2, const Line* __restrict__ lines,
+                                                         uint64_t terms, Fq2* __restrict__ out) {
+    const GroupLane g = group_lane();
+    const bool mine = g.live && g.group < terms;
+    const uint64_t t = mine ? g.group : 0;
+    const G1A p = g1[t];
+    const uint32_t qi = qidx[t];
+    const Line* ln = lines + (uint64_t)LINES * qi;
+    Fq2 f = g_one(g.k);
+    int n = 0;
+    auto apply = [&](const Fq2& fin) {
+        const Line x = ln[n++];
+        const Fq::Pair ay = Fq::mul2(x.a.c0, p.y, x.a.c1, p.y), bx = Fq::mul2(x.b.c0, p.x, x.b.c1, p.x);
+        return g_mul_line(fin, {ay.r0, ay.r1}, {bx.r0, bx.r1}, x.c, g.k, g.base);
+    };
+    for (int i = 1; i < NAF_LEN; ++i) {
+        f = apply(g_sqr(f, g.k, g.base));
+        if (NAF_6Z2[i]) f = apply(f);
+    }
+    f = apply(f);
+    f = apply(f);
+    if (mine) out[6 * t + g.k] = (p.is_inf() || g2[qi].is_inf()) ? g_one(g.k) : f;
+}
+
 // Miller value of (P, Q) as this lane's coefficient; every lane holds T and
 // the lines (their products are spread over the group).
 __device__ Fq2 g_miller(const G1A& p, const G2A& q, int k, int base) {
@@ -399,18 +523,6 @@ __device__ Fq2 g_final_exponentiation(const Fq2& m, int k, int base) {
     Fq2 r = g_mul(l0, g_frob(l1, k, 1), k, base);
     r = g_mul(r, g_frob(l2, k, 2), k, base);
     return g_mul(r, g_frob(l3, k, 3), k, base);
-}
-
-struct GroupLane {
-    int k, base;
-    uint64_t group;  // global group index
-    bool live;       // lanes 0..29 of the warp
-};
-DV_INL GroupLane group_lane() {
-    const int l = threadIdx.x & 31;
-    const int k = l < GL * GROUPS_PER_WARP ? l % GL : l - GL * GROUPS_PER_WARP;
-    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    return {k, l - k, warp * GROUPS_PER_WARP + (uint64_t)(l / GL), l < GL * GROUPS_PER_WARP};
 }
 
 // Miller value of every term, one lane group per term (coefficient k of
@@ -460,38 +572,121 @@ __global__ void __launch_bounds__(128) k_final_exp(const Fq2* __restrict__ mille
     }
 }
 
-void pairing_run(Backend& b, const uint8_t* g1, const uint8_t* g2, uint64_t terms, const uint64_t* offsets,
-                 uint64_t equations, uint8_t* verdicts, uint8_t* gt, cudaStream_t st) {
-    uint8_t* d_in = b.in_points.as<uint8_t>(192 * terms);
-    DV_CUDA(cudaMemcpyAsync(d_in, g1, 64 * terms, cudaMemcpyHostToDevice, st));
-    DV_CUDA(cudaMemcpyAsync(d_in + 64 * terms, g2, 128 * terms, cudaMemcpyHostToDevice, st));
-    G1A* p = b.conv_points.as<G1A>(terms * 3);  // G1A (64 B) then G2A (128 B)
-    G2A* q = reinterpret_cast<G2A*>(p + terms);
-    uint32_t* bad = b.err.as<uint32_t>(2);
-    DV_CUDA(cudaMemsetAsync(bad, 0xff, 2 * sizeof(uint32_t), st));
-    convert_points<Fq>(d_in, p, terms, bad, st);
-    convert_points<Fq2>(d_in + 64 * terms, q, terms, bad + 1, st);
-    Fq2* mil = b.aux.as<Fq2>(6 * terms);
-    constexpr uint64_t groups_per_block = 128 / 32 * GROUPS_PER_WARP;
-    if (terms) {
-        k_miller<<<(unsigned)((terms + groups_per_block - 1) / groups_per_block), 128, 0, st>>>(p, q, terms, mil);
-        DV_LAUNCH();
+constexpr uint64_t PREP_MAX = 1ull << 17;  // distinct G2 points prepared in one call (17.5 KB each)
+constexpr uint64_t GROUPS_PER_BLOCK = 128 / 32 * GROUPS_PER_WARP;
+
+unsigned group_blocks(uint64_t groups) { return (unsigned)((groups + GROUPS_PER_BLOCK - 1) / GROUPS_PER_BLOCK); }
+
+// 128-byte G2 wire points as hash keys (FNV-1a over the words).
+struct G2Key {
+    uint64_t w[16];
+    bool operator==(const G2Key& o) const { return memcmp(w, o.w, sizeof(w)) == 0; }
+};
+struct G2KeyHash {
+    size_t operator()(const G2Key& k) const {
+        uint64_t h = 1469598103934665603ull;
+        for (uint64_t x : k.w) h = (h ^ x) * 1099511628211ull;
+        return (size_t)h;
     }
+};
+
+// Product over the terms of each equation, final exponentiation, verdicts /
+// GT elements back to the host (after the caller's Miller values in mil).
+void finish_equations(Backend& b, Fq2* mil, const uint64_t* offsets, uint64_t equations, uint8_t* verdicts,
+                      uint8_t* gt, const uint32_t* bad, const std::vector<uint64_t>* g2_first, cudaStream_t st) {
     uint64_t* d_off = b.idx.as<uint64_t>(equations + 1);
     DV_CUDA(cudaMemcpyAsync(d_off, offsets, 8 * (equations + 1), cudaMemcpyHostToDevice, st));
     // GT elements first (16-byte aligned stores), then the verdict bytes
     uint8_t* d_gt = b.out_buf.as<uint8_t>(equations * ((gt ? 384 : 0) + 1));
     uint8_t* d_out = d_gt + (gt ? 384 * equations : 0);
-    k_final_exp<<<(unsigned)((equations + groups_per_block - 1) / groups_per_block), 128, 0, st>>>(
-        mil, d_off, equations, d_out, gt ? d_gt : nullptr);
+    k_final_exp<<<group_blocks(equations), 128, 0, st>>>(mil, d_off, equations, d_out, gt ? d_gt : nullptr);
     DV_LAUNCH();
     uint32_t hbad[2];
     DV_CUDA(cudaMemcpyAsync(hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaStreamSynchronize(st));
     if (hbad[0] != 0xffffffffu) throw InvalidArgument("invalid G1 point at term " + std::to_string(hbad[0]));
-    if (hbad[1] != 0xffffffffu) throw InvalidArgument("invalid G2 point at term " + std::to_string(hbad[1]));
+    if (hbad[1] != 0xffffffffu)
+        throw InvalidArgument("invalid G2 point at term " +
+                              std::to_string(g2_first ? (*g2_first)[hbad[1]] : (uint64_t)hbad[1]));
     if (verdicts) DV_CUDA(cudaMemcpy(verdicts, d_out, equations, cudaMemcpyDeviceToHost));
     if (gt) DV_CUDA(cudaMemcpy(gt, d_gt, 384 * equations, cudaMemcpyDeviceToHost));
+}
+
+}  // namespace
+
+struct PreparedG2 {
+    uint64_t n = 0;
+    DevBuf points;  // G2A (Montgomery affine)
+    DevBuf lines;   // LINES per point
+};
+struct PairingState {
+    std::map<uint64_t, std::unique_ptr<PreparedG2>> prepared;
+    DevBuf lines, qidx;
+};
+
+namespace {
+
+PairingState& pairing_state(Backend& b) {
+    if (!b.pairing) b.pairing = std::make_shared<PairingState>();
+    return *b.pairing;
+}
+
+void pairing_run(Backend& b, const uint8_t* g1, const uint8_t* g2, uint64_t terms, const uint64_t* offsets,
+                 uint64_t equations, uint8_t* verdicts, uint8_t* gt, cudaStream_t st) {
+    // the distinct G2 points of the call: shared ones are prepared once
+    std::vector<uint32_t> qidx;
+    std::vector<uint64_t> first;
+    std::vector<uint8_t> distinct;
+    if (terms > 1) {
+        std::unordered_map<G2Key, uint32_t, G2KeyHash> seen;
+        seen.reserve(terms);
+        qidx.resize(terms);
+        for (uint64_t t = 0; t < terms; ++t) {
+            G2Key key;
+            memcpy(key.w, g2 + 128 * t, 128);
+            const auto it = seen.emplace(key, (uint32_t)first.size());
+            if (it.second) {
+                first.push_back(t);
+                distinct.insert(distinct.end(), g2 + 128 * t, g2 + 128 * (t + 1));
+            }
+            qidx[t] = it.first->second;
+        }
+    }
+    const uint64_t nq = first.size();
+    const bool prepared = terms > 1 && nq < terms && nq <= PREP_MAX;
+    const uint64_t g2_count = prepared ? nq : terms;
+    uint8_t* d_in = b.in_points.as<uint8_t>(64 * terms + 128 * g2_count);
+    DV_CUDA(cudaMemcpyAsync(d_in, g1, 64 * terms, cudaMemcpyHostToDevice, st));
+    DV_CUDA(cudaMemcpyAsync(d_in + 64 * terms, prepared ? distinct.data() : g2, 128 * g2_count,
+                            cudaMemcpyHostToDevice, st));
+    G1A* p = b.conv_points.as<G1A>(terms + 2 * g2_count);  // G1A (64 B) then G2A (128 B)
+    G2A* q = reinterpret_cast<G2A*>(p + terms);
+    uint32_t* bad = b.err.as<uint32_t>(2);
+    DV_CUDA(cudaMemsetAsync(bad, 0xff, 2 * sizeof(uint32_t), st));
+    convert_points<Fq>(d_in, p, terms, bad, st);
+    convert_points<Fq2>(d_in + 64 * terms, q, g2_count, bad + 1, st);
+    Fq2* mil = b.aux.as<Fq2>(6 * terms);
+    if (prepared) {
+        PairingState& ps = pairing_state(b);
+        Line* lines = ps.lines.as<Line>((uint64_t)LINES * nq);
+        uint32_t* d_qidx = ps.qidx.as<uint32_t>(terms);
+        DV_CUDA(cudaMemcpyAsync(d_qidx, qidx.data(), 4 * terms, cudaMemcpyHostToDevice, st));
+        k_prepare<<<group_blocks(nq), 128, 0, st>>>(q, nq, lines);
+        DV_LAUNCH();
+        k_miller_prepared<<<group_blocks(terms), 128, 0, st>>>(p, d_qidx, q, lines, terms, mil);
+        DV_LAUNCH();
+    } else if (terms) {
+        k_miller<<<group_blocks(terms), 128, 0, st>>>(p, q, terms, mil);
+        DV_LAUNCH();
+    }
+    finish_equations(b, mil, offsets, equations, verdicts, gt, bad, prepared ? &first : nullptr, st);
+}
+
+void check_offsets(const uint64_t* offsets, size_t equations) {
+    require(offsets && equations >= 1 && equations <= (1u << 24), "invalid pairing check arguments");
+    require(offsets[0] == 0, "pairing offsets must start at 0");
+    for (size_t e = 0; e < equations; ++e) require(offsets[e + 1] >= offsets[e], "pairing offsets must not decrease");
+    require(offsets[equations] <= (1u << 24), "invalid pairing terms");
 }
 
 }  // namespace
@@ -502,11 +697,9 @@ using namespace dv;
 extern "C" int dvgpu_bn254_pairing_check(void* opaque, const uint8_t* g1, const uint8_t* g2, const uint64_t* offsets,
                                          size_t equations, uint8_t* verdicts, char* error, size_t cap) {
     return guarded(opaque, error, cap, [&](Backend& b) {
-        require(offsets && verdicts && equations >= 1 && equations <= (1u << 24), "invalid pairing check arguments");
-        require(offsets[0] == 0, "pairing offsets must start at 0");
-        for (size_t e = 0; e < equations; ++e) require(offsets[e + 1] >= offsets[e], "pairing offsets must not decrease");
+        check_offsets(offsets, equations);
         const uint64_t terms = offsets[equations];
-        require(terms <= (1u << 24) && (g1 || !terms) && (g2 || !terms), "invalid pairing terms");
+        require(verdicts && (g1 || !terms) && (g2 || !terms), "invalid pairing terms");
         pairing_run(b, g1, g2, terms, offsets, equations, verdicts, nullptr, b.stream);
     });
 }
@@ -518,5 +711,68 @@ extern "C" int dvgpu_bn254_pairing(void* opaque, const uint8_t* g1, const uint8_
         std::vector<uint64_t> off(n + 1);
         for (size_t i = 0; i <= n; ++i) off[i] = i;
         pairing_run(b, g1, g2, n, off.data(), n, nullptr, gt, b.stream);
+    });
+}
+
+extern "C" int dvgpu_bn254_g2_prepare(void* opaque, const uint8_t* g2, size_t n, uint64_t* prepared, char* error,
+                                      size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(g2 && prepared && n >= 1 && n <= PREP_MAX, "invalid G2 preparation arguments (1..2^17 points)");
+        const cudaStream_t st = b.stream;
+        auto pg = std::make_unique<PreparedG2>();
+        pg->n = n;
+        uint8_t* d_in = b.in_points.as<uint8_t>(128 * n);
+        DV_CUDA(cudaMemcpyAsync(d_in, g2, 128 * n, cudaMemcpyHostToDevice, st));
+        uint32_t* bad = b.err.as<uint32_t>(1);
+        DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
+        G2A* q = pg->points.as<G2A>(n);
+        convert_points<Fq2>(d_in, q, n, bad, st);
+        k_prepare<<<group_blocks(n), 128, 0, st>>>(q, n, pg->lines.as<Line>((uint64_t)LINES * n));
+        DV_LAUNCH();
+        const uint32_t first_bad = read_err_word(b, bad, st);
+        if (first_bad != 0xffffffffu) throw InvalidArgument("invalid G2 point at index " + std::to_string(first_bad));
+        const uint64_t h = b.next_handle++;
+        pairing_state(b).prepared[h] = std::move(pg);
+        *prepared = h;
+    });
+}
+
+extern "C" int dvgpu_bn254_g2_prepared_release(void* opaque, uint64_t prepared, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        PairingState& ps = pairing_state(b);
+        require(ps.prepared.count(prepared) != 0, "unknown prepared G2 handle");
+        DV_CUDA(cudaStreamSynchronize(b.stream));
+        ps.prepared.erase(prepared);
+    });
+}
+
+extern "C" int dvgpu_bn254_pairing_check_prepared(void* opaque, const uint8_t* g1, uint64_t prepared,
+                                                  const uint32_t* q_index, const uint64_t* offsets, size_t equations,
+                                                  uint8_t* verdicts, char* error, size_t cap) {
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        check_offsets(offsets, equations);
+        const uint64_t terms = offsets[equations];
+        require(verdicts && ((g1 && q_index) || !terms), "invalid pairing terms");
+        PairingState& ps = pairing_state(b);
+        const auto it = ps.prepared.find(prepared);
+        require(it != ps.prepared.end(), "unknown prepared G2 handle");
+        const PreparedG2& pg = *it->second;
+        for (uint64_t t = 0; t < terms; ++t) require(q_index[t] < pg.n, "prepared G2 index out of range");
+        const cudaStream_t st = b.stream;
+        uint8_t* d_in = b.in_points.as<uint8_t>(64 * terms);
+        DV_CUDA(cudaMemcpyAsync(d_in, g1, 64 * terms, cudaMemcpyHostToDevice, st));
+        G1A* p = b.conv_points.as<G1A>(std::max<uint64_t>(1, terms));
+        uint32_t* bad = b.err.as<uint32_t>(2);
+        DV_CUDA(cudaMemsetAsync(bad, 0xff, 2 * sizeof(uint32_t), st));
+        convert_points<Fq>(d_in, p, terms, bad, st);
+        Fq2* mil = b.aux.as<Fq2>(6 * std::max<uint64_t>(1, terms));
+        if (terms) {
+            uint32_t* d_qidx = ps.qidx.as<uint32_t>(terms);
+            DV_CUDA(cudaMemcpyAsync(d_qidx, q_index, 4 * terms, cudaMemcpyHostToDevice, st));
+            k_miller_prepared<<<group_blocks(terms), 128, 0, st>>>(p, d_qidx, pg.points.view<G2A>(),
+                                                                    pg.lines.view<Line>(), terms, mil);
+            DV_LAUNCH();
+        }
+        finish_equations(b, mil, offsets, equations, verdicts, nullptr, bad, nullptr, st);
     });
 }
