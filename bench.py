@@ -1105,18 +1105,25 @@ def poly_cpu(oracle, points, values9, weighted3):
 
 def pairing_fme(equations, terms_per_eq, distinct_g2):
     """Fq multiplications of the lane-group pairing as implemented, all six
-    lanes of a group counted: an Fq12 product is 36 Fq2 products (108
-    Fq-mul), a square 24 (72), a sparse line product 18 (54) plus the
-    line's scaling by P (4 per lane, 24).  Each distinct G2 point is prepared
-    once: 65 doublings and 23 additions whose Fq2 products are spread over
-    the group (13 and 16 per step, 3 Fq-mul each).  Per term: 65 squares and
-    88 line products; per equation a final exponentiation of 3 x (62
-    cyclotomic squares (12 Fq2 squares, 24 Fq-mul) + 24 products) plus about
-    42 products."""
+    lanes of a group counted: an Fq12 product is a three-term Karatsuba over
+    Fq4, 18 Fq2 products (54 Fq-mul); a square the same with Fq4 squares, 18
+    Fq2 squares (36); a cyclotomic square 12 Fq2 squares (24); a sparse line
+    product 18 Fq2 products (54) plus the line's scaling by P (4 per lane,
+    24).  Each distinct G2 point is prepared once: 65 doublings and 23
+    additions whose Fq2 products are spread over the group (13 and 16 per
+    step, 3 Fq-mul each).  Per term: 65 squares and 88 line products.  Per
+    equation: the product of its terms' values; the easy part (an Fq6
+    inverse, counted once although every lane of the group repeats it: 37
+    Fq-mul and a Fermat inversion of 256 squares and 110 products; four
+    products, two of them inside the inverse, and a q^2 Frobenius); three
+    exponentiations by z over its width-4 NAF (63 cyclotomic squares and 16
+    products each); and the hard part's 13 products, 8 cyclotomic squares
+    and three Frobenius maps (18 + 12 + 30)."""
     prep = 65 * 13 * 3 + 23 * 16 * 3
-    term = 65 * 72 + 88 * (54 + 24)
-    final = 3 * (62 * 24 + 24 * 108) + 42 * 108
-    return distinct_g2 * prep + equations * (terms_per_eq * term + (terms_per_eq - 1) * 108 + final)
+    term = 65 * 36 + 88 * (54 + 24)
+    easy = (37 + 256 + 110) + 4 * 54 + 12
+    hard = 3 * (63 * 24 + 16 * 54) + 13 * 54 + 8 * 24 + (18 + 12 + 30)
+    return distinct_g2 * prep + equations * (terms_per_eq * term + (terms_per_eq - 1) * 54 + easy + hard)
 
 
 class PairingOp:

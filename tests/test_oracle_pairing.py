@@ -72,9 +72,31 @@ def test_device_pairing_constants():
         assert words(f2[8 * j:8 * j + 8]) == mont((gj[0] ** 2 + gj[1] ** 2) % q)
     m = re.search(r"NAF_6Z2\[(\d+)\]\s*=\s*\{([^}]*)\}", src)
     assert [int(x) for x in m.group(2).split(",")] == b.naf(6 * b.BN_SEED + 2)
-    assert int(re.search(r"BN_Z = (\d+)ull", src).group(1)) == b.BN_SEED
     naf = b.naf(6 * b.BN_SEED + 2)
     lines = (len(naf) - 1) + sum(1 for d in naf[1:] if d) + 2  # doublings, additions, two Frobenius lines
     assert int(re.search(r"constexpr int LINES = (\d+);", src).group(1)) == lines
-    m = re.search(r"NAF_Z\[(\d+)\]\s*=\s*\{([^}]*)\}", src)
-    assert [int(x) for x in m.group(2).split(",")] == b.naf(b.BN_SEED)
+    m = re.search(r"WNAF_Z\[(\d+)\]\s*=\s*\{([^}]*)\}", src)
+    digits = [int(x) for x in m.group(2).split(",")]
+    assert len(digits) == int(m.group(1)) == int(re.search(r"WNAF_Z_LEN = (\d+);", src).group(1))
+    assert digits == _wnaf(b.BN_SEED, 4)
+    value = 0
+    for d in digits:
+        value = 2 * value + d
+    assert value == b.BN_SEED and digits[0] > 0
+    assert sum(1 for d in digits if d) == 14
+
+
+def _wnaf(k, w):
+    """Width-w NAF of k, most significant digit first: odd digits in
+    (-2^(w-1), 2^(w-1)), any two nonzero digits at least w places apart."""
+    out = []
+    while k:
+        d = 0
+        if k & 1:
+            d = k % (1 << w)
+            if d >= 1 << (w - 1):
+                d -= 1 << w
+            k -= d
+        out.append(d)
+        k >>= 1
+    return out[::-1]

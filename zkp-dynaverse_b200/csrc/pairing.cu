@@ -11,9 +11,11 @@
 // and is not reproduced.
 //
 // Fq12 = Fq2[w]/(w^6 - xi), xi = 9 + u, held by six lanes: lane k owns the
-// coefficient of w^k.  A product is c_k = sum_i a_i b_(k-i) (times xi where
-// the index wraps), six Fq2 products per lane from shuffled operands; a
-// square takes four; the sparse line product three; the q-power Frobenius
+// coefficient of w^k.  A product is a three-term Karatsuba over
+// Fq4 = Fq2[w^3], one Fq4 product (three Fq2 products) per lane from
+// shuffled operands; a square the same with Fq4 squares; the sparse line
+// product is c_k = sum_i f_i l_(k-i) over the line's three coefficients,
+// three Fq2 products per lane; the q-power Frobenius
 // is conj(a_k) xi^(k(q-1)/6) per lane; f^(q^6) negates the odd lanes.  The
 // serialised GT element uses the tower Fq12 = Fq6[w]/(w^2 - v), Fq6 =
 // Fq2[v]/(v^3 - xi), v = w^2: c0 = (w^0, w^2, w^4), c1 = (w^1, w^3, w^5).
@@ -88,10 +90,10 @@ __device__ __constant__ uint32_t FROB2[6][8] = {
 // NAF of 6z + 2, most significant digit first.
 __device__ __constant__ int8_t NAF_6Z2[66] = {1, 0, -1, 0, 1, 0, 0, 0, -1, 0, -1, 0, 0, 0, -1, 0, 1, 0, -1, 0, 0, -1, 0, 0, 0, 0, 0, 1, 0, 0, -1, 0, 1, 0, 0, -1, 0, 0, 0, 0, -1, 0, 1, 0, 0, 0, -1, 0, -1, 0, 0, 1, 0, 0, 0, -1, 0, 0, -1, 0, 1, 0, 1, 0, 0, 0};
 constexpr int NAF_LEN = 66;
-constexpr uint64_t BN_Z = 4965661367192848881ull;
-// NAF of z, most significant digit first (weight 24 against 28 binary).
-__device__ __constant__ int8_t NAF_Z[63] = {1, 0, 0, 0, 1, 0, 1, 0, 0, -1, 0, 1, 0, 1, 0, -1, 0, 0, 1, 0, 1, 0, -1, 0, -1, 0, -1, 0, 1, 0, 0, 0, 1, 0, 0, 1, 0, 1, 0, 1, 0, -1, 0, 1, 0, 0, 1, 0, 0, 0, 0, 1, 0, 1, 0, 0, 0, 0, -1, 0, 0, 0, 1};
-constexpr int NAF_Z_LEN = 63;
+// Width-4 NAF of z, most significant digit first: 14 odd digits in
+// {+-1, +-3, +-5, +-7} (against 24 in the plain NAF and 28 binary).
+__device__ __constant__ int8_t WNAF_Z[63] = {1, 0, 0, 0, 0, 0, 5, 0, 0, 0, 0, -3, 0, 0, 0, 3, 0, 0, 0, 0, 5, 0, 0, 0, -5, 0, 0, 0, -3, 0, 0, 0, 1, 0, 0, 0, 0, 5, 0, 0, 0, 0, 7, 0, 0, 0, -7, 0, 0, 0, 0, 0, 0, 5, 0, 0, 0, 0, -1, 0, 0, 0, 1};
+constexpr int WNAF_Z_LEN = 63;
 
 DV_INL Fq load_fq(const uint32_t* w) {
     Fq r;
@@ -163,53 +165,78 @@ DV_INL void fq2_mul_n(const Fq2* a, const Fq2* b, Fq2* out) {
         out[i] = {Fq::sub(z[3 * i], z[3 * i + 1]), Fq::sub(Fq::sub(z[3 * i + 2], z[3 * i]), z[3 * i + 1])};
 }
 
-// c = a b: lane k sums a_i b_(k-i) over i, times xi where i > k.
-__device__ __noinline__ Fq2 g_mul(const Fq2& a, const Fq2& b, int k, int base) {
-    Fq2 acc = Fq2::zero();
-#pragma unroll
-    for (int i = 0; i < GL; i += 2) {
-        const Fq2 x[2] = {shfl2(a, base + i), shfl2(a, base + i + 1)};
-        const Fq2 y[2] = {shfl2(b, base + mod6(k - i)), shfl2(b, base + mod6(k - i - 1))};
-        Fq2 p[2];
-        fq2_mul_n<2>(x, y, p);
-        acc = Fq2::add(acc, i > k ? mul_xi(p[0]) : p[0]);
-        acc = Fq2::add(acc, i + 1 > k ? mul_xi(p[1]) : p[1]);
-    }
-    return acc;
+// Products and squares by Karatsuba over Fq4 = Fq2[t]/(t^2 - xi), t = w^3:
+// f = F0 + F1 w + F2 w^2 with F_i = f_i + f_(i+3) t and w^3 = t.  The six
+// Fq4 products of a three-term Karatsuba, one per lane (three Fq2 products
+// each, 18 for the group against 36 for the schoolbook form):
+//   lanes 0, 1, 2:  m_i = A_i B_i;
+//   lanes 3, 4, 5:  m12 = (A1 + A2)(B1 + B2), m01 = (A0 + A1)(B0 + B1), m02 = (A0 + A2)(B0 + B2);
+// and C0 = m0 + t (m12 - m1 - m2), C1 = m01 - m0 - m1 + t m2,
+// C2 = m02 - m0 - m2 + m1, C_i = c_i + c_(i+3) t.
+struct Fq4 {
+    Fq2 r, s;  // r + s t
+};
+DV_INL Fq4 shfl4(const Fq4& a, int src) { return {shfl2(a.r, src), shfl2(a.s, src)}; }
+DV_INL Fq4 add4(const Fq4& a, const Fq4& b) { return {Fq2::add(a.r, b.r), Fq2::add(a.s, b.s)}; }
+DV_INL Fq4 sub4(const Fq4& a, const Fq4& b) { return {Fq2::sub(a.r, b.r), Fq2::sub(a.s, b.s)}; }
+
+// Lane k's Karatsuba operand from the group's coefficients: A_k for k < 3,
+// the pair sums A1 + A2, A0 + A1, A0 + A2 on lanes 3, 4, 5.  After the
+// rotations by 1, 2 and 3 lanes, lane j holds f_j + f_(j+1) and
+// f_j + f_(j+2); lanes 3..5 fetch their two halves from lanes (1, 4),
+// (0, 3) and (3, 0), each source lane publishing the one sum asked of it.
+DV_INL Fq4 k_operand(const Fq2& a, int k, int base) {
+    const Fq2 a1 = shfl2(a, base + mod6(k + 1)), a2 = shfl2(a, base + mod6(k + 2));
+    const Fq2 a3 = shfl2(a, base + mod6(k + 3));
+    const Fq2 s1 = Fq2::add(a, a1), s2 = Fq2::add(a, a2);
+    const Fq2 h0 = shfl2(k == 3 ? s2 : s1, base + (k == 3 ? 1 : k == 4 ? 0 : k == 5 ? 3 : k));
+    const Fq2 h1 = shfl2(k == 0 ? s2 : s1, base + (k == 3 ? 4 : k == 4 ? 3 : k == 5 ? 0 : k));
+    if (k < 3) return {a, a3};
+    return k == 5 ? Fq4{h1, h0} : Fq4{h0, h1};
 }
-// c = a^2: each unordered pair (i, j), i + j = k mod 6, once (doubled off
-// the diagonal).  Even k: (m, m), (m+3, m+3), (m+1, k-m-1), (m+2, k-m-2),
-// m = k/2; odd k: (m, m+1), (m+2, m+5), (m+3, m+4), m = (k-1)/2.
+// Lane k's coefficient of the product from the six Fq4 products m (one per
+// lane): lane i < 3 forms C_i = U + t V from its own m_i, the pair product
+// on lane i + 3 and the other two m_j; lane i + 3 takes the t part of C_i.
+DV_INL Fq2 k_combine(const Fq4& m, int k, int base) {
+    const int i = k < 3 ? k : k - 3;
+    const Fq4 q = shfl4(m, base + mod6(k + 3));
+    const Fq4 n1 = shfl4(m, base + (i == 2 ? 0 : i + 1));
+    const Fq4 n2 = shfl4(m, base + (i == 0 ? 2 : i - 1));
+    const Fq4 t = sub4(sub4(q, n1), n2);
+    // i = 0: U = m0, V = q - n1 - n2; i = 1: U = q - m1 - n0 = t + n2 - m1 (n2 = m0, n1 = m2),
+    // V = n1; i = 2: U = q - m2 - m0 + m1 = t + 2 n2 - m2 (n1 = m0, n2 = m1), V = 0.
+    const Fq4 w = i == 1 ? n1 : add4(n2, n2);
+    const Fq4 u = i == 0 ? m : sub4(add4(t, w), m);
+    const Fq2 vr = i == 0 ? t.r : (i == 1 ? n1.r : Fq2::zero());
+    const Fq2 vs = i == 0 ? t.s : (i == 1 ? n1.s : Fq2::zero());
+    const Fq2 cr = Fq2::add(u.r, mul_xi(vs)), cs = Fq2::add(u.s, vr);
+    const Fq2 hi = shfl2(cs, base + mod6(k + 3));
+    return k < 3 ? cr : hi;
+}
+// x^2 for three Fq2 values, (c0 + c1)(c0 - c1) + 2 c0 c1 u each, the six
+// base products in pairs.
+DV_INL void fq2_sqr_3(const Fq2* a, Fq2* out) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const Fq::Pair p = Fq::mul2(Fq::add(a[i].c0, a[i].c1), Fq::sub(a[i].c0, a[i].c1), a[i].c0, a[i].c1);
+        out[i] = {p.r0, Fq::dbl(p.r1)};
+    }
+}
+// c = a b.
+__device__ __noinline__ Fq2 g_mul(const Fq2& a, const Fq2& b, int k, int base) {
+    const Fq4 x = k_operand(a, k, base), y = k_operand(b, k, base);
+    const Fq2 xs[3] = {x.r, x.s, Fq2::add(x.r, x.s)}, ys[3] = {y.r, y.s, Fq2::add(y.r, y.s)};
+    Fq2 p[3];
+    fq2_mul_n<3>(xs, ys, p);
+    return k_combine({Fq2::add(p[0], mul_xi(p[1])), Fq2::sub(Fq2::sub(p[2], p[0]), p[1])}, k, base);
+}
+// c = a^2 (the same Karatsuba with Fq4 squares: three Fq2 squares a lane).
 __device__ __noinline__ Fq2 g_sqr(const Fq2& a, int k, int base) {
-    int i[4], j[4];
-    bool dbl[4];
-    if (!(k & 1)) {
-        const int m = k >> 1;
-        i[0] = m; j[0] = m; i[1] = mod6(m + 3); j[1] = i[1];
-        i[2] = mod6(m + 1); j[2] = mod6(k - m - 1); i[3] = mod6(m + 2); j[3] = mod6(k - m - 2);
-        dbl[0] = dbl[1] = false; dbl[2] = dbl[3] = true;
-    } else {
-        const int m = k >> 1;
-        i[0] = m; j[0] = m + 1; i[1] = mod6(m + 2); j[1] = mod6(m + 5); i[2] = mod6(m + 3); j[2] = mod6(m + 4);
-        i[3] = 0; j[3] = 0;
-        dbl[0] = dbl[1] = dbl[2] = true; dbl[3] = false;
-    }
-    Fq2 acc = Fq2::zero();
-#pragma unroll
-    for (int s = 0; s < 4; s += 2) {
-        const Fq2 x[2] = {shfl2(a, base + i[s]), shfl2(a, base + i[s + 1])};
-        const Fq2 y[2] = {shfl2(a, base + j[s]), shfl2(a, base + j[s + 1])};
-        Fq2 p[2];
-        fq2_mul_n<2>(x, y, p);
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            Fq2 t = dbl[s + h] ? Fq2::dbl(p[h]) : p[h];
-            if (i[s + h] + j[s + h] >= GL) t = mul_xi(t);
-            if ((k & 1) && s + h == 3) t = Fq2::zero();
-            acc = Fq2::add(acc, t);
-        }
-    }
-    return acc;
+    const Fq4 x = k_operand(a, k, base);
+    const Fq2 xs[3] = {x.r, x.s, Fq2::add(x.r, x.s)};
+    Fq2 p[3];
+    fq2_sqr_3(xs, p);
+    return k_combine({Fq2::add(p[0], mul_xi(p[1])), Fq2::sub(Fq2::sub(p[2], p[0]), p[1])}, k, base);
 }
 // Square of an element of the cyclotomic subgroup (every value after the
 // easy part of the final exponentiation), by Granger and Scott ("Faster
@@ -272,14 +299,23 @@ __device__ __noinline__ Fq2 g_inv(const Fq2& f, int k, int base) {
     return g_mul(c, mine, k, base);
 }
 // a^z for a in the cyclotomic subgroup (a^-1 = conj a), z the BN seed, over
-// its NAF.
+// its width-4 NAF: a, a^3, a^5, a^7 first (one square, three products), then
+// 62 squares and 13 products.
 __device__ __noinline__ Fq2 g_pow_z(const Fq2& a, int k, int base) {
-    const Fq2 ai = g_conj(a, k);
-    Fq2 r = a;
-    for (int i = 1; i < NAF_Z_LEN; ++i) {
+    Fq2 tab[4];
+    tab[0] = a;
+    const Fq2 a2 = g_cyc_sqr(a, k, base);
+#pragma unroll 1
+    for (int j = 1; j < 4; ++j) tab[j] = g_mul(tab[j - 1], a2, k, base);
+    Fq2 r = tab[WNAF_Z[0] >> 1];
+#pragma unroll 1
+    for (int i = 1; i < WNAF_Z_LEN; ++i) {
         r = g_cyc_sqr(r, k, base);
-        const int d = NAF_Z[i];
-        if (d) r = g_mul(r, d > 0 ? a : ai, k, base);
+        const int d = WNAF_Z[i];
+        if (d) {
+            const Fq2 t = tab[(d < 0 ? -d : d) >> 1];
+            r = g_mul(r, d > 0 ? t : g_conj(t, k), k, base);
+        }
     }
     return r;
 }
