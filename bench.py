@@ -1103,27 +1103,35 @@ def poly_cpu(oracle, points, values9, weighted3):
     return weights, cauchy_weights, polys, cauchy_values, quotient
 
 
-def pairing_fme(equations, terms_per_eq, distinct_g2):
+def pairing_fme(equations, terms_per_eq, distinct_g2, per_equation):
     """Fq multiplications of the lane-group pairing as implemented, all six
     lanes of a group counted: an Fq12 product is a three-term Karatsuba over
     Fq4, 18 Fq2 products (54 Fq-mul); a square the same with Fq4 squares, 18
     Fq2 squares (36); a cyclotomic square 12 Fq2 squares (24); a sparse line
-    product 18 Fq2 products (54) plus the line's scaling by P (4 per lane,
-    24).  Each distinct G2 point is prepared once: 65 doublings and 23
-    additions whose Fq2 products are spread over the group (13 and 16 per
-    step, 3 Fq-mul each).  Per term: 65 squares and 88 line products.  Per
-    equation: the product of its terms' values; the easy part (an Fq6
-    inverse, counted once although every lane of the group repeats it: 37
-    Fq-mul and a Fermat inversion of 256 squares and 110 products; four
-    products, two of them inside the inverse, and a q^2 Frobenius); three
-    exponentiations by z over its width-4 NAF (63 cyclotomic squares and 16
-    products each); and the hard part's 13 products, 8 cyclotomic squares
-    and three Frobenius maps (18 + 12 + 30)."""
+    product 18 Fq2 products (54); the product of two lines 6 Fq2 products
+    (18); scaling a line by its P 4 Fq-mul.  Each distinct G2 point is
+    prepared once: 65 doublings and 23 additions whose Fq2 products are
+    spread over the group (13 and 16 per step, 3 Fq-mul each).  The Miller
+    loops, 65 squares and 88 line steps: one per term (per_equation false;
+    the terms' values then meet in one product each), or the multi-Miller
+    loop of two-term equations (per_equation true: one square per step, both
+    lines scaled, multiplied together and into f by one product).  Per
+    equation: the easy part (an Fq6 inverse, counted once although every
+    lane of the group repeats it: 37 Fq-mul and a Fermat inversion of 256
+    squares and 110 products; four products, two of them inside the inverse,
+    and a q^2 Frobenius); three exponentiations by z over its width-4 NAF
+    (63 cyclotomic squares and 16 products each); and the hard part's 13
+    products, 8 cyclotomic squares and three Frobenius maps
+    (18 + 12 + 30)."""
     prep = 65 * 13 * 3 + 23 * 16 * 3
-    term = 65 * 36 + 88 * (54 + 24)
+    if per_equation:
+        assert terms_per_eq == 2
+        miller = 65 * 36 + 88 * (8 + 18 + 54)
+    else:
+        miller = terms_per_eq * (65 * 36 + 88 * (4 + 54)) + (terms_per_eq - 1) * 54
     easy = (37 + 256 + 110) + 4 * 54 + 12
     hard = 3 * (63 * 24 + 16 * 54) + 13 * 54 + 8 * 24 + (18 + 12 + 30)
-    return distinct_g2 * prep + equations * (terms_per_eq * term + (terms_per_eq - 1) * 54 + easy + hard)
+    return distinct_g2 * prep + equations * (miller + easy + hard)
 
 
 class PairingOp:
@@ -1181,10 +1189,20 @@ class PairingOp:
     def e2e_bytes(self):
         return len(self.g1) + len(self.g2) + 8 * len(self.offsets), self.eqs
 
+    def per_equation(self, torch):
+        """Whether the library runs the multi-Miller loop for this batch: more
+        terms than one wave of per-term groups (k_miller_multi at 206
+        registers holds 2 blocks of 20 groups per SM)."""
+        return 2 * self.eqs > torch.cuda.get_device_properties(0).multi_processor_count * 2 * 20
+
     def roofline(self, tl, imad_peak, step_ms):
-        macs = pairing_fme(self.eqs, 2, 0) * 136
+        import torch
+        per_eq = self.per_equation(torch)
+        macs = pairing_fme(self.eqs, 2, 0, per_eq) * 136
         ach = macs / (step_ms * 1e-3) / 1e12
-        return ({"bound": "imad", "kernel": "k_miller_prepared + k_final_exp (whole call)", "achieved": ach,
+        kernel = "k_miller_multi (%s) + k_final_exp (whole call)" % ("a group per equation" if per_eq
+                                                                       else "a group per term")
+        return ({"bound": "imad", "kernel": kernel, "achieved": ach,
                  "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
                  "algorithmic_macs_per_launch": macs, "launch_ms": step_ms}, None)
 

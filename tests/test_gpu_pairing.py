@@ -81,6 +81,8 @@ def test_random_batches_match_oracle(backend, oracle):
     assert sum(got) > 0 and not all(got)
     m = 24
     assert backend.pairing(pa[:64 * m], qc[:128 * m]) == oracle.pairing(pa[:64 * m], qc[:128 * m])
+    # one G2 point repeated: prepared once inside the call
+    assert backend.pairing(pa[:64 * m], gen2 * m) == oracle.pairing(pa[:64 * m], gen2 * m)
 
 
 def test_bilinearity_on_device(backend, oracle):
@@ -152,3 +154,52 @@ def test_prepared_g2_points_across_calls(backend, oracle, dv):
         backend.pairing_check_prepared(g1[:64], h, [0], [0, 1])
     with pytest.raises(dv.DvgpuError, match="invalid G2 point at index 1"):
         backend.g2_prepare(qs[:128] + one + one + bytes(64))
+
+
+def test_multi_miller_loop_in_large_batches(backend, oracle):
+    """Batches of more prepared terms than one wave of per-term groups run
+    one multi-Miller loop per equation: 3100 cache-check equations
+    e(L, G) e(-R, D_j) = 1 over three divisors (every third one broken), with
+    three-term equations (an infinity term on either side), one-term and
+    empty ones; verdicts by construction, through the kept preparations and
+    through the plain call, and the oracle on a sample."""
+    n = 3100
+    sa = oracle.uniform_fr(5201, n)
+    sd = oracle.uniform_fr(5202, 3)
+    a = [int.from_bytes(sa[32 * i:32 * i + 32], "little") for i in range(n)]
+    d = [int.from_bytes(sd[32 * j:32 * j + 32], "little") for j in range(3)]
+    one = (1).to_bytes(32, "little")
+    qs = oracle.fixed_base_g2(one + sd) + bytes(128)  # G, D_0, D_1, D_2, infinity
+    rs = b"".join(((a[i] * pow(d[i % 3], R_MOD - 2, R_MOD) + (i % 3 == 2)) % R_MOD).to_bytes(32, "little")
+                  for i in range(n))
+    left, right = oracle.fixed_base_g1(sa), oracle.fixed_base_g1(rs)
+    g1, qidx, offsets, expect = [], [], [0], []
+    for i in range(n):
+        lp, rp = left[64 * i:64 * i + 64], _neg_g1(right[64 * i:64 * i + 64])
+        terms = [(lp, 0), (rp, 1 + i % 3)]
+        if i % 13 == 5:
+            terms.append((lp, 4))
+        if i % 17 == 6:
+            terms.insert(1, (bytes(64), 2))
+        if i % 29 == 7:
+            terms = [(bytes(64), 0)]
+        if i % 31 == 8:
+            terms = []
+        for p, q in terms:
+            g1.append(p)
+            qidx.append(q)
+        offsets.append(offsets[-1] + len(terms))
+        expect.append(len(terms) < 2 or i % 3 != 2)
+    assert offsets[-1] > 148 * 8 * 5
+    g1 = b"".join(g1)
+    g2 = b"".join(qs[128 * q:128 * q + 128] for q in qidx)
+    h = backend.g2_prepare(qs)
+    try:
+        assert backend.pairing_check_prepared(g1, h, qidx, offsets) == expect
+    finally:
+        backend.g2_prepared_release(h)
+    assert backend.pairing_check(g1, g2, offsets) == expect
+    m = 64
+    sub = offsets[m]
+    assert backend.pairing_check(g1[:64 * sub], g2[:128 * sub], offsets[:m + 1]) == \
+        oracle.pairing_check(g1[:64 * sub], g2[:128 * sub], offsets[:m + 1])

@@ -5,8 +5,9 @@
 // to prod_k e(P_k, Q_k) = 1 (right-hand G1 points negated by the caller),
 // computed by Bn254::multi_miller_loop and final_exponentiation.  Here a
 // launch takes many equations: a group of six lanes runs the Miller loop of
-// one term, then a group per equation multiplies its terms' values and runs
-// the final exponentiation.  The reference's native Miller probe
+// one term (or, with prepared G2 points in large batches, the multi-Miller
+// loop of one equation), then a group per equation multiplies its terms'
+// values and runs the final exponentiation.  The reference's native Miller probe
 // (native/include/dynaverse_bn254_miller.h) is a diagnostic of line traces
 // and is not reproduced.
 //
@@ -57,6 +58,7 @@
 
 #include "abi_util.hpp"
 #include "backend.hpp"
+#include "engine.hpp"
 
 namespace dv {
 namespace {
@@ -457,12 +459,15 @@ __device__ __noinline__ void prep_add(Tw& t, const Fq2& xs, const Fq2& ys, Line&
     t.z = z3;
 }
 
-// The LINES triples of every Q (one lane group each) at lines[LINES q ..].
-__global__ void __launch_bounds__(128) k_prepare(const G2A* __restrict__ g2, uint64_t nq, Line* __restrict__ lines) {
+// The LINES triples of every Q (one lane group each) at lines[LINES q ..],
+// and inf[q] = 1 for Q at infinity (whose lines count as 1).
+__global__ void __launch_bounds__(128) k_prepare(const G2A* __restrict__ g2, uint64_t nq, Line* __restrict__ lines,
+                                                 uint32_t* __restrict__ inf) {
     const GroupLane g = group_lane();
     const bool mine = g.live && g.group < nq;
     const uint64_t qi = mine ? g.group : 0;
     const G2A q = g2[qi];
+    if (mine && g.k == 0) inf[qi] = q.is_inf() ? 1u : 0u;
     Line* out = lines + (uint64_t)LINES * qi;
     Tw t{q.x, q.y, Fq2::one()};
     Line l;
@@ -489,31 +494,113 @@ __global__ void __launch_bounds__(128) k_prepare(const G2A* __restrict__ g2, uin
     put(l);
 }
 
-// Miller value of term t from its P and its prepared Q (one lane group per
-// term; coefficient k at out[6 t + k]); infinity on either side gives one.
-__global__ void __launch_bounds__(128) k_miller_prepared(const G1A* __restrict__ g1, const uint32_t* __restrict__ qidx,
-                                                         const G2A* __restrict__ g2, const Line* __restrict__ lines,
-                                                         uint64_t terms, Fq2* __restrict__ out) {
+// A line A yp + (B xp) w + C w^3 scaled to its P: coefficients of w^0,
+// w^1, w^3.  A term with P or Q at infinity, or past its equation's count,
+// takes the line 1.
+struct SLine {
+    Fq2 l0, l1, l3;
+};
+DV_INL SLine line_one() { return {Fq2::one(), Fq2::zero(), Fq2::zero()}; }
+// One term's scaling: the four base products A yp, B xp one per lane
+// (lanes 0..3), shared by shuffles.
+DV_INL SLine scale_one(const Line& x, const G1A& p, bool one, int k, int base) {
+    const Fq u = k == 0 ? x.a.c0 : k == 1 ? x.a.c1 : k == 2 ? x.b.c0 : x.b.c1;
+    const Fq r = Fq::mul(u, k < 2 ? p.y : p.x);
+    const SLine l = {{shfl_fq(r, base), shfl_fq(r, base + 1)}, {shfl_fq(r, base + 2), shfl_fq(r, base + 3)}, x.c};
+    return one ? line_one() : l;
+}
+// Two terms' scaling: eight base products, lane k forms product k and lanes
+// 0, 1 also products 6, 7 (x: A yp, B xp of the first term, then of the
+// second).
+DV_INL void scale_two(const Line& x, const G1A& p, bool one_x, const Line& y, const G1A& q, bool one_y, int k,
+                      int base, SLine& a, SLine& b) {
+    const Fq u0 = k == 0 ? x.a.c0 : k == 1 ? x.a.c1 : k == 2 ? x.b.c0 : k == 3 ? x.b.c1 : k == 4 ? y.a.c0 : y.a.c1;
+    const Fq v0 = k < 2 ? p.y : (k < 4 ? p.x : q.y);
+    const Fq::Pair r = Fq::mul2(u0, v0, k == 0 ? y.b.c0 : y.b.c1, q.x);
+    const SLine la = {{shfl_fq(r.r0, base), shfl_fq(r.r0, base + 1)}, {shfl_fq(r.r0, base + 2), shfl_fq(r.r0, base + 3)},
+                      x.c};
+    const SLine lb = {{shfl_fq(r.r0, base + 4), shfl_fq(r.r0, base + 5)}, {shfl_fq(r.r1, base), shfl_fq(r.r1, base + 1)},
+                      y.c};
+    a = one_x ? line_one() : la;
+    b = one_y ? line_one() : lb;
+}
+// (a0 + a1 w + a3 w^3)(b0 + b1 w + b3 w^3): the Karatsuba products p0 = a0 b0,
+// p1 = a1 b1, p2 = a3 b3, p3 = (a0 + a1)(b0 + b1), p4 = (a0 + a3)(b0 + b3),
+// p5 = (a1 + a3)(b1 + b3), one per lane; c0 = p0 + xi p2, c1 = p3 - p0 - p1,
+// c2 = p1, c3 = p4 - p0 - p2, c4 = p5 - p1 - p2, c5 = 0.
+__device__ __noinline__ Fq2 g_line_line(const SLine& a, const SLine& b, int k, int base) {
+    const Fq2 x = k == 0 ? a.l0 : k == 1 ? a.l1 : k == 2 ? a.l3 : Fq2::add(k == 5 ? a.l1 : a.l0, k == 3 ? a.l1 : a.l3);
+    const Fq2 y = k == 0 ? b.l0 : k == 1 ? b.l1 : k == 2 ? b.l3 : Fq2::add(k == 5 ? b.l1 : b.l0, k == 3 ? b.l1 : b.l3);
+    Fq2 p;
+    fq2_mul_n<1>(&x, &y, &p);
+    const Fq2 m = shfl2(p, base + (k == 1 ? 3 : k == 2 ? 1 : k == 3 ? 4 : k == 4 ? 5 : 0));
+    const Fq2 p0 = shfl2(p, base), p1 = shfl2(p, base + 1), p2 = shfl2(p, base + 2);
+    const Fq2 d = Fq2::sub(Fq2::sub(m, k == 4 ? p1 : p0), k == 1 ? p1 : p2);
+    return k == 0 ? Fq2::add(p0, mul_xi(p2)) : k == 2 ? m : k == 5 ? Fq2::zero() : d;
+}
+
+// Miller value of every equation from its terms' P and prepared Q, one lane
+// group per equation and one f for all its terms (the multi-Miller loop):
+// every step squares f once and multiplies in the lines of all the terms,
+// two terms' lines first multiplied together (six Fq2 products, one per
+// lane) and then into f by one product, a last odd term by the sparse line
+// product.  Every group of a warp runs the warp's largest term count.
+// Value of equation e at out[6 e + k]; without offsets every term is its own
+// equation (a group per term, for batches too small to fill the GPU, whose
+// terms then meet in the final exponentiation).
+__global__ void __launch_bounds__(128) k_miller_multi(const G1A* __restrict__ g1, const uint32_t* __restrict__ qidx,
+                                                      const uint32_t* __restrict__ qinf,
+                                                      const Line* __restrict__ lines,
+                                                      const uint64_t* __restrict__ offsets, uint64_t equations,
+                                                      Fq2* __restrict__ out) {
     const GroupLane g = group_lane();
-    const bool mine = g.live && g.group < terms;
-    const uint64_t t = mine ? g.group : 0;
-    const G1A p = g1[t];
-    const uint32_t qi = qidx[t];
-    const Line* ln = lines + (uint64_t)LINES * qi;
-    Fq2 f = g_one(g.k);
-    int n = 0;
-    auto apply = [&](const Fq2& fin) {
-        const Line x = ln[n++];
-        const Fq::Pair ay = Fq::mul2(x.a.c0, p.y, x.a.c1, p.y), bx = Fq::mul2(x.b.c0, p.x, x.b.c1, p.x);
-        return g_mul_line(fin, {ay.r0, ay.r1}, {bx.r0, bx.r1}, x.c, g.k, g.base);
-    };
-    for (int i = 1; i < NAF_LEN; ++i) {
-        f = apply(g_sqr(f, g.k, g.base));
-        if (NAF_6Z2[i]) f = apply(f);
+    const bool mine = g.live && g.group < equations;
+    const uint64_t e = mine ? g.group : 0;
+    const uint64_t first = !mine ? 0 : offsets ? offsets[e] : e;
+    const uint64_t count = !mine ? 0 : offsets ? offsets[e + 1] - first : 1;
+    uint64_t most = count;
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        const uint64_t o = __shfl_xor_sync(FULL, most, off);
+        most = o > most ? o : most;
     }
-    f = apply(f);
-    f = apply(f);
-    if (mine) out[6 * t + g.k] = (p.is_inf() || g2[qi].is_inf()) ? g_one(g.k) : f;
+    // term j of this group at line n (term 0 of the call stands in past the
+    // group's count, which is then nonzero somewhere in the warp); true when
+    // its line counts as 1
+    auto term = [&](uint64_t j, int n, G1A& p, Line& l) {
+        const bool have = j < count;
+        const uint64_t t = have ? first + j : 0;
+        p = g1[t];
+        const uint32_t qi = qidx[t];
+        l = lines[(uint64_t)LINES * qi + n];
+        return !have || p.is_inf() || qinf[qi] != 0;
+    };
+    Fq2 f = g_one(g.k);
+    auto apply = [&](int n) {
+        for (uint64_t j = 0; j < most; j += 2) {
+            G1A pa, pb;
+            Line la, lb;
+            const bool oa = term(j, n, pa, la);
+            if (j + 1 < most) {
+                const bool ob = term(j + 1, n, pb, lb);
+                SLine a, b;
+                scale_two(la, pa, oa, lb, pb, ob, g.k, g.base, a, b);
+                f = g_mul(f, g_line_line(a, b, g.k, g.base), g.k, g.base);
+            } else {
+                const SLine a = scale_one(la, pa, oa, g.k, g.base);
+                f = g_mul_line(f, a.l0, a.l1, a.l3, g.k, g.base);
+            }
+        }
+    };
+    int n = 0;
+    for (int i = 1; i < NAF_LEN; ++i) {
+        if (i > 1) f = g_sqr(f, g.k, g.base);
+        apply(n++);
+        if (NAF_6Z2[i]) apply(n++);
+    }
+    apply(n++);
+    apply(n++);
+    if (mine) out[6 * e + g.k] = f;
 }
 
 // Miller value of (P, Q) as this lane's coefficient; every lane holds T and
@@ -576,14 +663,16 @@ __global__ void __launch_bounds__(128) k_miller(const G1A* __restrict__ g1, cons
 
 // One lane group per equation: product of its terms' values (every group of
 // a warp runs the warp's largest term count, multiplying by one past its
-// own), final exponentiation, verdict, and with gt the canonical GT element.
+// own; without offsets one value per equation), final exponentiation,
+// verdict, and with gt the canonical GT element.
 __global__ void __launch_bounds__(128) k_final_exp(const Fq2* __restrict__ miller, const uint64_t* __restrict__ offsets,
                                                    uint64_t equations, uint8_t* __restrict__ verdicts,
                                                    uint8_t* __restrict__ gt) {
     const GroupLane g = group_lane();
     const bool mine = g.live && g.group < equations;
     const uint64_t e = mine ? g.group : 0;
-    const uint64_t first = mine ? offsets[e] : 0, count = mine ? offsets[e + 1] - first : 0;
+    const uint64_t first = !mine ? 0 : offsets ? offsets[e] : e;
+    const uint64_t count = !mine ? 0 : offsets ? offsets[e + 1] - first : 1;
     uint64_t most = count;
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) {
@@ -609,9 +698,23 @@ __global__ void __launch_bounds__(128) k_final_exp(const Fq2* __restrict__ mille
 }
 
 constexpr uint64_t PREP_MAX = 1ull << 17;  // distinct G2 points prepared in one call (17.5 KB each)
+
 constexpr uint64_t GROUPS_PER_BLOCK = 128 / 32 * GROUPS_PER_WARP;
 
 unsigned group_blocks(uint64_t groups) { return (unsigned)((groups + GROUPS_PER_BLOCK - 1) / GROUPS_PER_BLOCK); }
+
+// Whether the prepared Miller loops run one group per equation (the
+// multi-Miller loop, fewer instructions) rather than one per term (shorter
+// chains): per equation once a group per term would take more than one wave
+// of resident blocks (on B200, 2 blocks of 20 groups per SM: 5920 terms).
+bool miller_per_equation(uint64_t terms) {
+    static const uint64_t wave = [] {
+        int blocks = 0;
+        DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_miller_multi, 128, 0));
+        return (uint64_t)sm_count() * (uint64_t)std::max(1, blocks) * GROUPS_PER_BLOCK;
+    }();
+    return terms > wave;
+}
 
 // 128-byte G2 wire points as hash keys (FNV-1a over the words).
 struct G2Key {
@@ -626,12 +729,18 @@ struct G2KeyHash {
     }
 };
 
-// Product over the terms of each equation, final exponentiation, verdicts /
-// GT elements back to the host (after the caller's Miller values in mil).
-void finish_equations(Backend& b, Fq2* mil, const uint64_t* offsets, uint64_t equations, uint8_t* verdicts,
-                      uint8_t* gt, const uint32_t* bad, const std::vector<uint64_t>* g2_first, cudaStream_t st) {
+// Device copy of the equations' term offsets.
+uint64_t* upload_offsets(Backend& b, const uint64_t* offsets, uint64_t equations, cudaStream_t st) {
     uint64_t* d_off = b.idx.as<uint64_t>(equations + 1);
     DV_CUDA(cudaMemcpyAsync(d_off, offsets, 8 * (equations + 1), cudaMemcpyHostToDevice, st));
+    return d_off;
+}
+
+// Final exponentiation of the Miller values in mil (one per term, folded per
+// equation by the device offsets d_off; one per equation when d_off is
+// null), verdicts / GT elements back to the host.
+void finish_equations(Backend& b, Fq2* mil, const uint64_t* d_off, uint64_t equations, uint8_t* verdicts,
+                      uint8_t* gt, const uint32_t* bad, const std::vector<uint64_t>* g2_first, cudaStream_t st) {
     // GT elements first (16-byte aligned stores), then the verdict bytes
     uint8_t* d_gt = b.out_buf.as<uint8_t>(equations * ((gt ? 384 : 0) + 1));
     uint8_t* d_out = d_gt + (gt ? 384 * equations : 0);
@@ -654,10 +763,11 @@ struct PreparedG2 {
     uint64_t n = 0;
     DevBuf points;  // G2A (Montgomery affine)
     DevBuf lines;   // LINES per point
+    DevBuf inf;     // u32 per point: 1 at infinity
 };
 struct PairingState {
     std::map<uint64_t, std::unique_ptr<PreparedG2>> prepared;
-    DevBuf lines, qidx;
+    DevBuf lines, inf, qidx;
 };
 
 namespace {
@@ -690,6 +800,7 @@ void pairing_run(Backend& b, const uint8_t* g1, const uint8_t* g2, uint64_t term
     }
     const uint64_t nq = first.size();
     const bool prepared = terms > 1 && nq < terms && nq <= PREP_MAX;
+    const bool multi = prepared && miller_per_equation(terms);
     const uint64_t g2_count = prepared ? nq : terms;
     uint8_t* d_in = b.in_points.as<uint8_t>(64 * terms + 128 * g2_count);
     DV_CUDA(cudaMemcpyAsync(d_in, g1, 64 * terms, cudaMemcpyHostToDevice, st));
@@ -701,21 +812,27 @@ void pairing_run(Backend& b, const uint8_t* g1, const uint8_t* g2, uint64_t term
     DV_CUDA(cudaMemsetAsync(bad, 0xff, 2 * sizeof(uint32_t), st));
     convert_points<Fq>(d_in, p, terms, bad, st);
     convert_points<Fq2>(d_in + 64 * terms, q, g2_count, bad + 1, st);
-    Fq2* mil = b.aux.as<Fq2>(6 * terms);
+    uint64_t* d_off = upload_offsets(b, offsets, equations, st);
+    Fq2* mil = b.aux.as<Fq2>(6 * std::max<uint64_t>(1, std::max(terms, equations)));
     if (prepared) {
         PairingState& ps = pairing_state(b);
         Line* lines = ps.lines.as<Line>((uint64_t)LINES * nq);
+        uint32_t* qinf = ps.inf.as<uint32_t>(nq);
         uint32_t* d_qidx = ps.qidx.as<uint32_t>(terms);
         DV_CUDA(cudaMemcpyAsync(d_qidx, qidx.data(), 4 * terms, cudaMemcpyHostToDevice, st));
-        k_prepare<<<group_blocks(nq), 128, 0, st>>>(q, nq, lines);
+        k_prepare<<<group_blocks(nq), 128, 0, st>>>(q, nq, lines, qinf);
         DV_LAUNCH();
-        k_miller_prepared<<<group_blocks(terms), 128, 0, st>>>(p, d_qidx, q, lines, terms, mil);
+        if (multi)
+            k_miller_multi<<<group_blocks(equations), 128, 0, st>>>(p, d_qidx, qinf, lines, d_off, equations, mil);
+        else
+            k_miller_multi<<<group_blocks(terms), 128, 0, st>>>(p, d_qidx, qinf, lines, nullptr, terms, mil);
         DV_LAUNCH();
     } else if (terms) {
         k_miller<<<group_blocks(terms), 128, 0, st>>>(p, q, terms, mil);
         DV_LAUNCH();
     }
-    finish_equations(b, mil, offsets, equations, verdicts, gt, bad, prepared ? &first : nullptr, st);
+    finish_equations(b, mil, prepared && multi ? nullptr : d_off, equations, verdicts, gt, bad,
+                     prepared ? &first : nullptr, st);
 }
 
 void check_offsets(const uint64_t* offsets, size_t equations) {
@@ -763,7 +880,8 @@ extern "C" int dvgpu_bn254_g2_prepare(void* opaque, const uint8_t* g2, size_t n,
         DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
         G2A* q = pg->points.as<G2A>(n);
         convert_points<Fq2>(d_in, q, n, bad, st);
-        k_prepare<<<group_blocks(n), 128, 0, st>>>(q, n, pg->lines.as<Line>((uint64_t)LINES * n));
+        k_prepare<<<group_blocks(n), 128, 0, st>>>(q, n, pg->lines.as<Line>((uint64_t)LINES * n),
+                                                   pg->inf.as<uint32_t>(n));
         DV_LAUNCH();
         const uint32_t first_bad = read_err_word(b, bad, st);
         if (first_bad != 0xffffffffu) throw InvalidArgument("invalid G2 point at index " + std::to_string(first_bad));
@@ -801,14 +919,21 @@ extern "C" int dvgpu_bn254_pairing_check_prepared(void* opaque, const uint8_t* g
         uint32_t* bad = b.err.as<uint32_t>(2);
         DV_CUDA(cudaMemsetAsync(bad, 0xff, 2 * sizeof(uint32_t), st));
         convert_points<Fq>(d_in, p, terms, bad, st);
-        Fq2* mil = b.aux.as<Fq2>(6 * std::max<uint64_t>(1, terms));
-        if (terms) {
-            uint32_t* d_qidx = ps.qidx.as<uint32_t>(terms);
-            DV_CUDA(cudaMemcpyAsync(d_qidx, q_index, 4 * terms, cudaMemcpyHostToDevice, st));
-            k_miller_prepared<<<group_blocks(terms), 128, 0, st>>>(p, d_qidx, pg.points.view<G2A>(),
-                                                                    pg.lines.view<Line>(), terms, mil);
+        uint64_t* d_off = upload_offsets(b, offsets, equations, st);
+        Fq2* mil = b.aux.as<Fq2>(6 * std::max<uint64_t>(1, std::max(terms, equations)));
+        uint32_t* d_qidx = ps.qidx.as<uint32_t>(std::max<uint64_t>(1, terms));
+        if (terms) DV_CUDA(cudaMemcpyAsync(d_qidx, q_index, 4 * terms, cudaMemcpyHostToDevice, st));
+        const bool multi = miller_per_equation(terms);
+        if (multi) {
+            // with no terms every equation's value is one (the kernel reads only the offsets)
+            k_miller_multi<<<group_blocks(equations), 128, 0, st>>>(p, d_qidx, pg.inf.view<uint32_t>(),
+                                                                   pg.lines.view<Line>(), d_off, equations, mil);
+            DV_LAUNCH();
+        } else if (terms) {
+            k_miller_multi<<<group_blocks(terms), 128, 0, st>>>(p, d_qidx, pg.inf.view<uint32_t>(),
+                                                               pg.lines.view<Line>(), nullptr, terms, mil);
             DV_LAUNCH();
         }
-        finish_equations(b, mil, offsets, equations, verdicts, nullptr, bad, nullptr, st);
+        finish_equations(b, mil, multi ? nullptr : d_off, equations, verdicts, nullptr, bad, nullptr, st);
     });
 }
