@@ -1117,9 +1117,10 @@ def pairing_fme(equations, terms_per_eq, distinct_g2, per_equation):
     loop of two-term equations (per_equation true: one square per step, both
     lines scaled, multiplied together and into f by one product).  Per
     equation: the easy part (an Fq6 inverse, counted once although every
-    lane of the group repeats it: 37 Fq-mul and a Fermat inversion of 256
-    squares and 110 products; four products, two of them inside the inverse,
-    and a q^2 Frobenius); three exponentiations by z over its width-4 NAF
+    lane of the group repeats it: 37 Fq-mul and an Fq inverse by divsteps,
+    integer work counted as its one closing Montgomery product; four
+    products, two of them inside the inverse, and a q^2 Frobenius); three
+    exponentiations by z over its width-4 NAF
     (63 cyclotomic squares and 16 products each); and the hard part's 13
     products, 8 cyclotomic squares and three Frobenius maps
     (18 + 12 + 30)."""
@@ -1129,7 +1130,7 @@ def pairing_fme(equations, terms_per_eq, distinct_g2, per_equation):
         miller = 65 * 36 + 88 * (8 + 18 + 54)
     else:
         miller = terms_per_eq * (65 * 36 + 88 * (4 + 54)) + (terms_per_eq - 1) * 54
-    easy = (37 + 256 + 110) + 4 * 54 + 12
+    easy = (37 + 1) + 4 * 54 + 12
     hard = 3 * (63 * 24 + 16 * 54) + 13 * 54 + 8 * 24 + (18 + 12 + 30)
     return distinct_g2 * prep + equations * (miller + easy + hard)
 

@@ -100,3 +100,16 @@ def _wnaf(k, w):
         out.append(d)
         k >>= 1
     return out[::-1]
+
+
+def test_divstep_inverse_constants():
+    """The constants of the device's divstep Fq inverse: p in 30-bit limbs,
+    p^-1 mod 2^30 and R^3 mod p (R = 2^256) in 32-bit limbs."""
+    src = open(os.path.join(ROOT, "zkp-dynaverse_b200", "csrc", "pairing.cu")).read()
+    q = b.Q
+    p9 = [int(x) for x in re.search(r"P9\[9\]\s*=\s*\{([^}]*)\}", src).group(1).split(",")]
+    assert sum(v << (30 * i) for i, v in enumerate(p9)) == q and all(0 <= v < 1 << 30 for v in p9)
+    pinv = int(re.search(r"PINV30 = (\d+)u;", src).group(1))
+    assert pinv * q % (1 << 30) == 1
+    r3 = [int(x.strip().rstrip("u"), 16) for x in re.search(r"R3\[8\]\s*=\s*\{([^}]*)\}", src).group(1).split(",")]
+    assert sum(v << (32 * i) for i, v in enumerate(r3)) == pow(1 << 256, 3, q)
