@@ -103,13 +103,14 @@ def _wnaf(k, w):
 
 
 def test_divstep_inverse_constants():
-    """The constants of the device's divstep Fq inverse: p in 30-bit limbs,
-    p^-1 mod 2^30 and R^3 mod p (R = 2^256) in 32-bit limbs."""
-    src = open(os.path.join(ROOT, "zkp-dynaverse_b200", "csrc", "pairing.cu")).read()
-    q = b.Q
-    p9 = [int(x) for x in re.search(r"P9\[9\]\s*=\s*\{([^}]*)\}", src).group(1).split(",")]
-    assert sum(v << (30 * i) for i, v in enumerate(p9)) == q and all(0 <= v < 1 << 30 for v in p9)
-    pinv = int(re.search(r"PINV30 = (\d+)u;", src).group(1))
-    assert pinv * q % (1 << 30) == 1
-    r3 = [int(x.strip().rstrip("u"), 16) for x in re.search(r"R3\[8\]\s*=\s*\{([^}]*)\}", src).group(1).split(",")]
-    assert sum(v << (32 * i) for i, v in enumerate(r3)) == pow(1 << 256, 3, q)
+    """R^3 mod p (R = 2^256) of both fields, the constant that turns the
+    divstep inverse of a Montgomery value back into Montgomery form."""
+    src = open(os.path.join(ROOT, "zkp-dynaverse_b200", "csrc", "field.cuh")).read()
+    fr = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+    for cfg, mod in (("FqCfg", b.Q), ("FrCfg", fr)):
+        body = src[src.index("struct " + cfg):]
+        body = body[:body.index("};")]
+        words = [int(re.search(r"R3%d = 0x([0-9a-f]+)u" % i, body).group(1), 16) for i in range(8)]
+        assert sum(w << (32 * i) for i, w in enumerate(words)) == pow(1 << 256, 3, mod)
+        inv = int(re.search(r"INV = 0x([0-9a-f]+)u", body).group(1), 16)
+        assert (inv * mod) % (1 << 32) == (1 << 32) - 1  # -p^-1 mod 2^32, whose negation mod 2^30 is p^-1

@@ -20,6 +20,7 @@ struct FqCfg {
     static constexpr uint32_t INV = 0xe4866389u;  // -p^{-1} mod 2^32
     static constexpr uint32_t ONE0 = 0xc58f0d9du, ONE1 = 0xd35d438du, ONE2 = 0xf5c70b3du, ONE3 = 0x0a78eb28u, ONE4 = 0x7879462cu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
     static constexpr uint32_t R20 = 0x538afa89u, R21 = 0xf32cfc5bu, R22 = 0xd44501fbu, R23 = 0xb5e71911u, R24 = 0x0a417ff6u, R25 = 0x47ab1effu, R26 = 0xcab8351fu, R27 = 0x06d89f71u;
+    static constexpr uint32_t R30 = 0xda1530dfu, R31 = 0xb1cd6dafu, R32 = 0xa7283db6u, R33 = 0x62f210e6u, R34 = 0x0ada0afbu, R35 = 0xef7f0b0cu, R36 = 0x2d592544u, R37 = 0x20fd6e90u;
 };
 struct FrCfg {
     static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u,
@@ -27,6 +28,7 @@ struct FrCfg {
     static constexpr uint32_t INV = 0xefffffffu;
     static constexpr uint32_t ONE0 = 0x4ffffffbu, ONE1 = 0xac96341cu, ONE2 = 0x9f60cd29u, ONE3 = 0x36fc7695u, ONE4 = 0x7879462eu, ONE5 = 0x666ea36fu, ONE6 = 0x9a07df2fu, ONE7 = 0x0e0a77c1u;
     static constexpr uint32_t R20 = 0xae216da7u, R21 = 0x1bb8e645u, R22 = 0xe35c59e3u, R23 = 0x53fe3ab1u, R24 = 0x53bb8085u, R25 = 0x8c49833du, R26 = 0x7f4e44a5u, R27 = 0x0216d0b1u;
+    static constexpr uint32_t R30 = 0xb4bf0040u, R31 = 0x5e94d8e1u, R32 = 0x1cfbb6b8u, R33 = 0x2a489cbeu, R34 = 0xa19fcfedu, R35 = 0x893cc664u, R36 = 0x7fcc657cu, R37 = 0x0cf8594bu;
 };
 
 #define DV_INL __device__ __forceinline__
@@ -265,9 +267,150 @@ struct __align__(16) Fp {  // 16-byte aligned: global copies move as 128-bit acc
         }
         return r;
     }
+    // 1 / a (0 for a = 0) by the divsteps of Bernstein and Yang ("Fast
+    // constant-time gcd computation and modular inversion", TCHES 2019),
+    // run variable-time: with f = p, g = aR, d = 0, e = 1 (f = d aR and
+    // g = e aR mod p throughout), each batch takes 30 divsteps on the low 30
+    // bits of f and g into a transition matrix scaled by 2^30, then applies
+    // it to f, g (exact division by 2^30) and to d, e (division by 2^30 mod
+    // p, adding md p with md = -(u d + v e) p^-1 mod 2^30).  Numbers are 9
+    // limbs of 30 bits, the top one signed.  736 divsteps bring g to 0 for
+    // inputs below 2^254, so 25 batches bound the loop, which ends when
+    // g = 0.  Then f = +-1 and (aR)^-1 = f d with |d| < 26 p; the
+    // Montgomery product with R^3 mod p turns (aR)^-1 into a^-1 R.
     DV_INL static Fp inv(const Fp& a) {
-        const uint32_t e[8] = {C::P0 - 2, C::P1, C::P2, C::P3, C::P4, C::P5, C::P6, C::P7};
-        return pow(a, e);
+        constexpr uint32_t M30 = (1u << 30) - 1;
+        constexpr uint32_t PINV30 = (0u - C::INV) & M30;  // p^-1 mod 2^30
+        N9 f, g, d, e;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            f.l[i] = limb30(i);
+            d.l[i] = 0;
+            e.l[i] = i == 0;
+            g.l[i] = (int32_t)(bits30(a, i));
+        }
+        int delta = 1;
+#pragma unroll 1
+        for (int batch = 0; batch < 25 && g.nonzero(); ++batch) {
+            int32_t t[4];
+            delta = divsteps30(delta, (uint32_t)f.l[0], (uint32_t)g.l[0], t);
+            // (f, g) <- t (f, g) / 2^30 exactly; (d, e) <- t (d, e) / 2^30 mod p
+            int64_t cf = (int64_t)t[0] * f.l[0] + (int64_t)t[1] * g.l[0];
+            int64_t cg = (int64_t)t[2] * f.l[0] + (int64_t)t[3] * g.l[0];
+            int64_t cd = (int64_t)t[0] * d.l[0] + (int64_t)t[1] * e.l[0];
+            int64_t ce = (int64_t)t[2] * d.l[0] + (int64_t)t[3] * e.l[0];
+            const int32_t md = (int32_t)((0u - (uint32_t)cd * PINV30) & M30);
+            const int32_t me = (int32_t)((0u - (uint32_t)ce * PINV30) & M30);
+            cd += (int64_t)md * limb30(0);
+            ce += (int64_t)me * limb30(0);
+            cf >>= 30;
+            cg >>= 30;
+            cd >>= 30;
+            ce >>= 30;
+#pragma unroll
+            for (int i = 1; i < 9; ++i) {
+                cf += (int64_t)t[0] * f.l[i] + (int64_t)t[1] * g.l[i];
+                cg += (int64_t)t[2] * f.l[i] + (int64_t)t[3] * g.l[i];
+                cd += (int64_t)t[0] * d.l[i] + (int64_t)t[1] * e.l[i] + (int64_t)md * limb30(i);
+                ce += (int64_t)t[2] * d.l[i] + (int64_t)t[3] * e.l[i] + (int64_t)me * limb30(i);
+                f.l[i - 1] = (int32_t)((uint32_t)cf & M30);
+                g.l[i - 1] = (int32_t)((uint32_t)cg & M30);
+                d.l[i - 1] = (int32_t)((uint32_t)cd & M30);
+                e.l[i - 1] = (int32_t)((uint32_t)ce & M30);
+                cf >>= 30;
+                cg >>= 30;
+                cd >>= 30;
+                ce >>= 30;
+            }
+            f.l[8] = (int32_t)cf;
+            g.l[8] = (int32_t)cg;
+            d.l[8] = (int32_t)cd;
+            e.l[8] = (int32_t)ce;
+        }
+        // x = 32 p + f d in (6 p, 58 p), then conditional subtractions of 32 p .. p
+        const bool neg = f.l[8] < 0;
+        N9 x;
+        int64_t c = 0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            c += 32 * (int64_t)limb30(i) + (neg ? -(int64_t)d.l[i] : (int64_t)d.l[i]);
+            x.l[i] = i < 8 ? (int32_t)((uint32_t)c & M30) : (int32_t)c;
+            c >>= 30;
+        }
+#pragma unroll
+        for (int k = 5; k >= 0; --k) {
+            N9 y;
+            int64_t cy = 0;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                cy += (int64_t)x.l[i] - ((int64_t)limb30(i) << k);
+                y.l[i] = i < 8 ? (int32_t)((uint32_t)cy & M30) : (int32_t)cy;
+                cy >>= 30;
+            }
+            if (y.l[8] >= 0) x = y;
+        }
+        Fp r, r3;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            // bits [32 w, 32 w + 32) of x; 32 w mod 30 <= 14
+            const int i = 32 * w / 30, s = 32 * w % 30;
+            r.v[w] = ((uint32_t)x.l[i] >> s) | ((uint32_t)x.l[i + 1] << (30 - s));
+        }
+        r3.v[0] = C::R30; r3.v[1] = C::R31; r3.v[2] = C::R32; r3.v[3] = C::R33;
+        r3.v[4] = C::R34; r3.v[5] = C::R35; r3.v[6] = C::R36; r3.v[7] = C::R37;
+        return mul(r, r3);
+    }
+
+  private:
+    // Signed 30-bit-limb numbers of the divstep inverse.
+    struct N9 {
+        int32_t l[9];
+        DV_INL bool nonzero() const {
+            int32_t o = 0;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) o |= l[i];
+            return o != 0;
+        }
+    };
+    // bits [30 i, 30 i + 30) of p and of a
+    DV_INL static constexpr int32_t limb30(int i) {
+        const uint32_t p[8] = {C::P0, C::P1, C::P2, C::P3, C::P4, C::P5, C::P6, C::P7};
+        const int b = 30 * i, w = b >> 5, s = b & 31;
+        const uint32_t lo = p[w] >> s, hi = (s > 2 && w + 1 < 8) ? p[w + 1] << (32 - s) : 0u;
+        return (int32_t)((lo | hi) & ((1u << 30) - 1));
+    }
+    DV_INL static uint32_t bits30(const Fp& a, int i) {
+        const int b = 30 * i, w = b >> 5, s = b & 31;
+        uint32_t x = a.v[w] >> s;
+        if (s > 2 && w + 1 < 8) x |= a.v[w + 1] << (32 - s);
+        return x & ((1u << 30) - 1);
+    }
+    // 30 divsteps on the low bits of f and g (f odd): delta and the matrix
+    // t = (u, v, q, r) with t (f, g) = 2^30 (f', g').  A step with g odd and
+    // delta > 0 swaps first: (f, g) <- (g, -f), (u, v, q, r) <- (q, r, -u, -v),
+    // delta <- -delta; then g odd adds f to g and (u, v) to (q, r); then g
+    // halves, (u, v) double and delta grows by one.
+    DV_INL static int divsteps30(int delta, uint32_t f, uint32_t g, int32_t* t) {
+        int32_t u = 1, v = 0, q = 0, r = 1;
+#pragma unroll
+        for (int i = 0; i < 30; ++i) {
+            const bool odd = g & 1u, swap = odd && delta > 0;
+            const uint32_t f1 = swap ? g : f, g1 = swap ? 0u - f : g;
+            const int32_t u1 = swap ? q : u, v1 = swap ? r : v, q1 = swap ? -u : q, r1 = swap ? -v : r;
+            delta = swap ? -delta : delta;
+            f = f1;
+            g = (odd ? g1 + f1 : g1) >> 1;
+            q = odd ? q1 + u1 : q1;
+            r = odd ? r1 + v1 : r1;
+            u = 2 * u1;
+            v = 2 * v1;
+            ++delta;
+        }
+        t[0] = u;
+        t[1] = v;
+        t[2] = q;
+        t[3] = r;
+        return delta;
     }
 };
 

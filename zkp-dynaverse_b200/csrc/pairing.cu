@@ -111,169 +111,13 @@ DV_INL Fq mul9(const Fq& a) { return Fq::add(Fq::dbl(Fq::dbl(Fq::dbl(a))), a); }
 DV_INL Fq2 mul_xi(const Fq2& a) { return {Fq::sub(mul9(a.c0), a.c1), Fq::add(a.c0, mul9(a.c1))}; }
 
 
-// ------------------------------------------------------------------ Fq inverse by divsteps
-// 1 / a for a in Montgomery form, by the divsteps of Bernstein and Yang
-// ("Fast constant-time gcd computation and modular inversion", TCHES 2019),
-// run variable-time: with f = p, g = aR, d = 0, e = 1 (f = d aR and
-// g = e aR mod p throughout), each batch takes 30 divsteps on the low 30
-// bits of f and g into a transition matrix scaled by 2^30, then applies it
-// to f, g (exact division by 2^30) and to d, e (division by 2^30 mod p,
-// adding md p with md = -(u d + v e) p^-1 mod 2^30).  Numbers are 9 limbs
-// of 30 bits, the top one signed.  736 divsteps bring g to 0 for 254-bit
-// inputs, so 25 batches bound the loop; it stops once g = 0 in every lane
-// of the warp.  Then f = +-1 and (aR)^-1 = f d, |d| < 26 p; the Montgomery
-// product with R^3 mod p turns (aR)^-1 into a^-1 R.  a = 0 gives 0.
-namespace inv30 {
-constexpr uint32_t M30 = (1u << 30) - 1;
-constexpr uint32_t PINV30 = 460954743u;  // p^-1 mod 2^30
-__device__ __constant__ int32_t P9[9] = {410844487, 813838427, 119318739, 542811226, 22568343,
-                                         18274822,  436378501, 329037900, 12388};
-__device__ __constant__ uint32_t R3[8] = {0xda1530dfu, 0xb1cd6dafu, 0xa7283db6u, 0x62f210e6u,
-                                          0x0ada0afbu, 0xef7f0b0cu, 0x2d592544u, 0x20fd6e90u};
-struct N9 {
-    int32_t l[9];
-};
-struct Matrix {
-    int32_t u, v, q, r;
-};
-// 30 divsteps on the low bits of f and g (f odd): delta and the matrix t
-// with t (f, g) = 2^30 (f', g').
-DV_INL int divsteps30(int delta, uint32_t f, uint32_t g, Matrix& t) {
-    int32_t u = 1, v = 0, q = 0, r = 1;
-#pragma unroll
-    for (int i = 0; i < 30; ++i) {
-        const bool odd = g & 1u, swap = odd && delta > 0;
-        // a swap turns the step into (f, g) <- (g, -f), (u, v, q, r) <- (q, r, -u, -v), delta <- -delta
-        const uint32_t f1 = swap ? g : f, g1 = swap ? 0u - f : g;
-        const int32_t u1 = swap ? q : u, v1 = swap ? r : v, q1 = swap ? -u : q, r1 = swap ? -v : r;
-        delta = swap ? -delta : delta;
-        f = f1;
-        g = (odd ? g1 + f1 : g1) >> 1;
-        q = odd ? q1 + u1 : q1;
-        r = odd ? r1 + v1 : r1;
-        u = 2 * u1;
-        v = 2 * v1;
-        ++delta;
-    }
-    t = {u, v, q, r};
-    return delta;
-}
-// (f, g) <- t (f, g) / 2^30, exact.
-DV_INL void update_fg(N9& f, N9& g, const Matrix& t) {
-    int64_t cf = (int64_t)t.u * f.l[0] + (int64_t)t.v * g.l[0];
-    int64_t cg = (int64_t)t.q * f.l[0] + (int64_t)t.r * g.l[0];
-    cf >>= 30;
-    cg >>= 30;
-#pragma unroll
-    for (int i = 1; i < 9; ++i) {
-        cf += (int64_t)t.u * f.l[i] + (int64_t)t.v * g.l[i];
-        cg += (int64_t)t.q * f.l[i] + (int64_t)t.r * g.l[i];
-        f.l[i - 1] = (int32_t)((uint32_t)cf & M30);
-        g.l[i - 1] = (int32_t)((uint32_t)cg & M30);
-        cf >>= 30;
-        cg >>= 30;
-    }
-    f.l[8] = (int32_t)cf;
-    g.l[8] = (int32_t)cg;
-}
-// (d, e) <- t (d, e) / 2^30 mod p (|d|, |e| grow by less than p a batch).
-DV_INL void update_de(N9& d, N9& e, const Matrix& t) {
-    int64_t cd = (int64_t)t.u * d.l[0] + (int64_t)t.v * e.l[0];
-    int64_t ce = (int64_t)t.q * d.l[0] + (int64_t)t.r * e.l[0];
-    const int32_t md = (int32_t)((0u - (uint32_t)cd * PINV30) & M30);
-    const int32_t me = (int32_t)((0u - (uint32_t)ce * PINV30) & M30);
-    cd += (int64_t)md * P9[0];
-    ce += (int64_t)me * P9[0];
-    cd >>= 30;
-    ce >>= 30;
-#pragma unroll
-    for (int i = 1; i < 9; ++i) {
-        cd += (int64_t)t.u * d.l[i] + (int64_t)t.v * e.l[i] + (int64_t)md * P9[i];
-        ce += (int64_t)t.q * d.l[i] + (int64_t)t.r * e.l[i] + (int64_t)me * P9[i];
-        d.l[i - 1] = (int32_t)((uint32_t)cd & M30);
-        e.l[i - 1] = (int32_t)((uint32_t)ce & M30);
-        cd >>= 30;
-        ce >>= 30;
-    }
-    d.l[8] = (int32_t)cd;
-    e.l[8] = (int32_t)ce;
-}
-DV_INL bool nonzero(const N9& x) {
-    int32_t o = 0;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) o |= x.l[i];
-    return o != 0;
-}
-}  // namespace inv30
-
-__device__ __noinline__ Fq fq_inv(const Fq& a) {
-    using namespace inv30;
-    N9 f, g, d, e;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        f.l[i] = P9[i];
-        d.l[i] = 0;
-        e.l[i] = i == 0;
-        // bits [30 i, 30 i + 30) of a
-        const int b = 30 * i, w = b >> 5, s = b & 31;
-        uint32_t x = a.v[w] >> s;
-        if (s > 2 && w + 1 < 8) x |= a.v[w + 1] << (32 - s);
-        g.l[i] = (int32_t)(x & M30);
-    }
-    int delta = 1;
-#pragma unroll 1
-    for (int batch = 0; batch < 25 && __any_sync(0xffffffffu, nonzero(g)); ++batch) {
-        Matrix t;
-        delta = divsteps30(delta, (uint32_t)f.l[0], (uint32_t)g.l[0], t);
-        update_fg(f, g, t);
-        update_de(d, e, t);
-    }
-    // x = 32 p + f d in (6 p, 58 p), then conditional subtractions of 32 p .. p
-    const bool neg = f.l[8] < 0;
-    N9 x;
-    int64_t c = 0;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        c += 32 * (int64_t)P9[i] + (neg ? -(int64_t)d.l[i] : (int64_t)d.l[i]);
-        x.l[i] = i < 8 ? (int32_t)((uint32_t)c & M30) : (int32_t)c;
-        c >>= 30;
-    }
-#pragma unroll
-    for (int k = 5; k >= 0; --k) {
-        N9 y;
-        int64_t cy = 0;
-#pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            cy += (int64_t)x.l[i] - ((int64_t)P9[i] << k);
-            y.l[i] = i < 8 ? (int32_t)((uint32_t)cy & M30) : (int32_t)cy;
-            cy >>= 30;
-        }
-        if (y.l[8] >= 0) x = y;
-    }
-    Fq r;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) {
-        // bits [32 w, 32 w + 32) of x
-        const int b = 32 * w, i = b / 30, s = b % 30;
-        uint32_t v = (uint32_t)x.l[i] >> s;
-        if (i + 1 < 9) v |= (uint32_t)x.l[i + 1] << (30 - s);
-        if (s > 28 && i + 2 < 9) v |= (uint32_t)x.l[i + 2] << (60 - s);
-        r.v[w] = v;
-    }
-    Fq c3;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) c3.v[w] = R3[w];
-    return Fq::mul(r, c3);
-}
-
 // 1 / a in Fq6 (one Fq inversion).
 __device__ __noinline__ Fq6 f6_inv(const Fq6& a) {
     const Fq2 t0 = Fq2::sub(Fq2::sqr(a.c0), mul_xi(Fq2::mul(a.c1, a.c2)));
     const Fq2 t1 = Fq2::sub(mul_xi(Fq2::sqr(a.c2)), Fq2::mul(a.c0, a.c1));
     const Fq2 t2 = Fq2::sub(Fq2::sqr(a.c1), Fq2::mul(a.c0, a.c2));
     const Fq2 d = Fq2::add(Fq2::mul(a.c0, t0), mul_xi(Fq2::add(Fq2::mul(a.c2, t1), Fq2::mul(a.c1, t2))));
-    const Fq ni = fq_inv(Fq::add(Fq::sqr(d.c0), Fq::sqr(d.c1)));
-    const Fq2 di = {Fq::mul(d.c0, ni), Fq::neg(Fq::mul(d.c1, ni))};
+    const Fq2 di = Fq2::inv(d);
     return {Fq2::mul(t0, di), Fq2::mul(t1, di), Fq2::mul(t2, di)};
 }
 
