@@ -539,12 +539,12 @@ class G2CheckOp:
 def ecntt_fme(logn, rows):
     """Fq multiplications of a G1 transform: per stage, every butterfly costs
     two XYZZ additions (2 x 14) and every butterfly with a twiddle other than
-    1 a GLV scalar multiplication: the endomorphism (1), the table entry
-    P + phi(P) (14) and a joint double-and-add over 127-bit halves (127
-    doublings x 9, about 95 additions x 14: a pair of bits is nonzero with
-    probability 3/4)."""
+    1 a GLV scalar multiplication over signed 5-bit windows of its two
+    127-bit halves: the table of 1..16 multiples (8 doublings x 9, 7
+    additions x 14), then 26 windows (125 doublings x 9, two additions x 14
+    and one product beta X a window)."""
     n = 1 << logn
-    smul = 1 + 14 + 127 * 9 + 95 * 14
+    smul = 8 * 9 + 7 * 14 + 125 * 9 + 26 * (2 * 14 + 1)
     nontrivial = sum(rows * (n // 2 - (1 << s)) for s in range(logn))
     return rows * (n // 2) * logn * 28 + nontrivial * smul
 

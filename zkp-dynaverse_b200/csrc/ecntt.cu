@@ -49,21 +49,57 @@ struct __align__(16) GlvScalar {
 __device__ __constant__ uint32_t GLV_BETA[8] = {0xd782e155u, 0x71930c11u, 0xffbe3323u, 0xa6bb947cu,
                                                 0xd4741444u, 0xaa303344u, 0x26594943u, 0x2c3b3f0du};
 
-// [k] p = [k1] p + [k2] phi(p), jointly, left to right.
+// [k] p = [k1] p + [k2] phi(p) over signed fixed windows of 5 bits: both
+// halves recoded into digits in [-16, 16) (k = sum d_j 32^j, at most 26
+// windows for halves below 2^128), one table of |d| p for |d| = 1..16 (8
+// doublings and 7 additions, in local memory) serving both halves, the
+// second through phi (one product: beta X).  Every lane of a warp adds at
+// the same window positions, so a warp runs 5 doublings and 2 additions a
+// window; a sparse signed-digit form would make each warp add wherever any
+// of its lanes has a digit, nearly every bit.
+DV_INL void recode5(const uint32_t* k, int nw, int8_t* d) {
+    uint32_t carry = 0;
+    for (int j = 0; j < nw; ++j) {
+        const int b = 5 * j, w = b >> 5, sh = b & 31;
+        uint32_t x = k[w] >> sh;
+        if (sh > 27 && w + 1 < 4) x |= k[w + 1] << (32 - sh);
+        const int v = (int)((x & 31u) + carry);
+        carry = v >= 16 ? 1u : 0u;
+        d[j] = (int8_t)(v >= 16 ? v - 32 : v);
+    }
+}
 DV_INL XYZZ<Fq> scalar_mul(const XYZZ<Fq>& p, const GlvScalar& g) {
     if (p.is_inf() || g.bits == 0) return XYZZ<Fq>::inf();
     Fq beta;
 #pragma unroll
     for (int i = 0; i < 8; ++i) beta.v[i] = GLV_BETA[i];
-    const XYZZ<Fq> p1 = (g.flags & 1) ? p.neg() : p;
-    XYZZ<Fq> p2 = {Fq::mul(p.x, beta), p.y, p.zz, p.zzz};
-    if (g.flags & 2) p2 = p2.neg();
-    const XYZZ<Fq> p12 = XYZZ<Fq>::add_paired(p1, p2);
+    // the top window holds at most 3 bits, so the recoding's carry never leaves it
+    const int nw = ((int)g.bits + 1) / 5 + 1;
+    int8_t d1[26], d2[26];
+    recode5(g.k1, nw, d1);
+    recode5(g.k2, nw, d2);
+    XYZZ<Fq> tab[16];
+    tab[0] = p;
+#pragma unroll 1
+    for (int m = 2; m <= 16; ++m)
+        tab[m - 1] = (m & 1) ? XYZZ<Fq>::add_paired(tab[m - 2], p) : XYZZ<Fq>::dbl_paired(tab[m / 2 - 1]);
+    const bool n1 = g.flags & 1, n2 = g.flags & 2;
     XYZZ<Fq> r = XYZZ<Fq>::inf();
-    for (int i = (int)g.bits - 1; i >= 0; --i) {
-        r = XYZZ<Fq>::dbl_paired(r);
-        const uint32_t b1 = (g.k1[i >> 5] >> (i & 31)) & 1, b2 = (g.k2[i >> 5] >> (i & 31)) & 1;
-        if (b1 | b2) r = XYZZ<Fq>::add_paired(r, b1 ? (b2 ? p12 : p1) : p2);
+#pragma unroll 1
+    for (int j = nw - 1; j >= 0; --j) {
+        if (j != nw - 1)
+#pragma unroll 1
+            for (int i = 0; i < 5; ++i) r = XYZZ<Fq>::dbl_paired(r);
+        const int a = d1[j], b = d2[j];
+        if (a) {
+            const XYZZ<Fq> t = tab[(a < 0 ? -a : a) - 1];
+            r = XYZZ<Fq>::add_paired(r, (a < 0) != n1 ? t.neg() : t);
+        }
+        if (b) {
+            XYZZ<Fq> t = tab[(b < 0 ? -b : b) - 1];
+            t.x = Fq::mul(t.x, beta);
+            r = XYZZ<Fq>::add_paired(r, (b < 0) != n2 ? t.neg() : t);
+        }
     }
     return r;
 }

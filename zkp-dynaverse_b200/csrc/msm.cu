@@ -324,6 +324,27 @@ __global__ void __launch_bounds__(TH) k_fixup_long(const int* __restrict__ pgid,
 // with Suf the group's suffix sums of V; the doublings for G apply to one
 // sum per group, so the critical path holds log2(total weight) of them.
 
+// Additions and doublings of the reduction: few threads per bucket set on a
+// dependent chain, so over Fq the products go out in pairs.
+template <class F>
+DV_INL XYZZ<F> wadd(const XYZZ<F>& p, const XYZZ<F>& q) {
+    if constexpr (sizeof(F) == sizeof(Fq)) return XYZZ<F>::add_paired(p, q);
+    else return XYZZ<F>::add(p, q);
+}
+template <class F>
+DV_INL XYZZ<F> wdbl(const XYZZ<F>& p) {
+    if constexpr (sizeof(F) == sizeof(Fq)) return XYZZ<F>::dbl_paired(p);
+    else return XYZZ<F>::dbl(p);
+}
+template <class F>
+DV_INL XYZZ<F> shfl_down_xyzz(const XYZZ<F>& p, int d) {
+    return {shfl_down(p.x, d), shfl_down(p.y, d), shfl_down(p.zz, d), shfl_down(p.zzz, d)};
+}
+template <class F>
+DV_INL XYZZ<F> shfl_idx_xyzz(const XYZZ<F>& p, int l) {
+    return {shfl_idx(p.x, l), shfl_idx(p.y, l), shfl_idx(p.zz, l), shfl_idx(p.zzz, l)};
+}
+
 // Level 1: one segment of s buckets per thread.
 template <class F>
 __global__ void __launch_bounds__(128) k_segments(const XYZZ<F>* __restrict__ buckets, const uint32_t* __restrict__ offsets,
@@ -338,59 +359,85 @@ __global__ void __launch_bounds__(128) k_segments(const XYZZ<F>* __restrict__ bu
     const size_t base = (size_t)w * B + (size_t)j * s;
     for (int b = (int)s - 1; b >= 0; --b) {
         const size_t g = base + b;
-        if (offsets[g + 1] != offsets[g]) R = XYZZ<F>::add(R, buckets[g]);
-        U = XYZZ<F>::add(U, R);
+        if (offsets[g + 1] != offsets[g]) R = wadd<F>(R, buckets[g]);
+        U = wadd<F>(U, R);
     }
-    for (int i = 0; i < seg_log; ++i) R = XYZZ<F>::dbl(R);  // V = s R
+    for (int i = 0; i < seg_log; ++i) R = wdbl<F>(R);  // V = s R
     seg_u[tid] = U;
     seg_v[tid] = R;
 }
 
-// Upper levels: blocks of P pairs (G = P), suffix scan and tree in shared
-// memory.  Windows of S pairs; S <= P is the last level (one block per
-// window, its U' is S_w).
-// Additions of the upper levels: few threads per window on a dependent
-// chain, so over Fq the products go out in pairs.
-template <class F>
-DV_INL XYZZ<F> wadd(const XYZZ<F>& p, const XYZZ<F>& q) {
-    if constexpr (sizeof(F) == sizeof(Fq)) return XYZZ<F>::add_paired(p, q);
-    else return XYZZ<F>::add(p, q);
-}
-
+// Upper levels: blocks of P pairs (G = P), windows of S pairs; S <= P is the
+// last level (one block per window, its U' is S_w).  Suffix sums of V by
+// warp shuffles (five rounds in a warp, three across the block's warp
+// totals), then the block sum of U + Suf_{+1} the same way: about 18
+// dependent additions and three barriers per block, then log2 P doublings
+// for V'.  A block's time is this chain's latency (measured the same as a
+// shared-memory Hillis-Steele scan and tree of equal depth), so the
+// levels cost about one block latency per wave of blocks: 16-bucket
+// segments for 2^19 buckets keep the first upper level to one wave.
 template <class F, int P>
 __global__ void __launch_bounds__(P) k_wlevel(const XYZZ<F>* __restrict__ u_in, const XYZZ<F>* __restrict__ v_in,
                                               uint32_t S, XYZZ<F>* __restrict__ u_out, XYZZ<F>* __restrict__ v_out) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    XYZZ<F>* sh = reinterpret_cast<XYZZ<F>*>(smem_raw);
+    constexpr int NWARP = P / 32;
+    static_assert(NWARP >= 1 && NWARP <= 32 && (NWARP & (NWARP - 1)) == 0, "block of 32..1024 threads, power of 2");
+    __shared__ XYZZ<F> warp_v[NWARP], warp_later[NWARP], warp_x[NWARP];
+    __shared__ XYZZ<F> block_v;
     const uint32_t nblk = S > (uint32_t)P ? S / P : 1u;
     const uint32_t w = blockIdx.x / nblk, k = blockIdx.x % nblk;
     const uint32_t width = S < (uint32_t)P ? S : (uint32_t)P;
     const uint32_t t = threadIdx.x;
+    const int lane = (int)(t & 31), warp = (int)(t >> 5);
     const size_t idx = (size_t)w * S + (size_t)k * P + t;
     const bool live = t < width;
-    sh[t] = live ? v_in[idx] : XYZZ<F>::inf();
-    __syncthreads();
-    for (uint32_t d = 1; d < width; d <<= 1) {
-        const XYZZ<F> o = t + d < width ? sh[t + d] : XYZZ<F>::inf();
-        __syncthreads();
-        if (t + d < width) sh[t] = wadd<F>(sh[t], o);
-        __syncthreads();
+    // inclusive suffix sums of V inside the warp
+    XYZZ<F> sv = live ? v_in[idx] : XYZZ<F>::inf();
+#pragma unroll 1
+    for (int d = 1; d < 32; d <<= 1) {
+        const XYZZ<F> o = shfl_down_xyzz(sv, d);
+        if (lane + d < 32) sv = wadd<F>(sv, o);
     }
-    XYZZ<F> x = t + 1 < width ? sh[t + 1] : XYZZ<F>::inf();  // Suf_{t+1}
-    XYZZ<F> vsum = sh[0];
+    if (lane == 0) warp_v[warp] = sv;
     __syncthreads();
+    // suffix sums over the warp totals (warp 0): later warps' V for every warp
+    if (warp == 0) {
+        XYZZ<F> c = lane < NWARP ? warp_v[lane] : XYZZ<F>::inf();
+#pragma unroll 1
+        for (int d = 1; d < NWARP; d <<= 1) {
+            const XYZZ<F> o = shfl_down_xyzz(c, d);
+            if (lane + d < NWARP) c = wadd<F>(c, o);
+        }
+        const XYZZ<F> after = shfl_down_xyzz(c, 1);
+        if (lane < NWARP) warp_later[lane] = lane + 1 < NWARP ? after : XYZZ<F>::inf();
+        if (lane == 0) block_v = c;
+    }
+    __syncthreads();
+    // Suf_{t+1} + U_t
+    const XYZZ<F> nxt = shfl_down_xyzz(sv, 1);
+    XYZZ<F> x = wadd<F>(lane < 31 ? nxt : XYZZ<F>::inf(), warp_later[warp]);
     if (live) x = wadd<F>(x, u_in[idx]);
-    sh[t] = x;
-    __syncthreads();
-    for (uint32_t d = (uint32_t)P / 2; d > 0; d >>= 1) {
-        if (t < d) sh[t] = wadd<F>(sh[t], sh[t + d]);
-        __syncthreads();
+    // block sum: butterfly in the warp, then the warp sums in warp 0
+#pragma unroll 1
+    for (int d = 16; d >= 1; d >>= 1) {
+        const XYZZ<F> o = shfl_down_xyzz(x, d);
+        if (lane < d) x = wadd<F>(x, o);
     }
-    if (t == 0) {
-        u_out[blockIdx.x] = sh[0];
-        if (nblk > 1) {
-            for (int i = 0; i < __builtin_ctz((unsigned)P); ++i) vsum = XYZZ<F>::dbl(vsum);  // V' = P sum V
-            v_out[blockIdx.x] = vsum;
+    if (lane == 0) warp_x[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        XYZZ<F> y = lane < NWARP ? warp_x[lane] : XYZZ<F>::inf();
+#pragma unroll 1
+        for (int d = NWARP / 2; d >= 1; d >>= 1) {
+            const XYZZ<F> o = shfl_down_xyzz(y, d);
+            if (lane < d) y = wadd<F>(y, o);
+        }
+        if (lane == 0) {
+            u_out[blockIdx.x] = y;
+            if (nblk > 1) {
+                XYZZ<F> vsum = block_v;
+                for (int i = 0; i < __builtin_ctz((unsigned)P); ++i) vsum = wdbl<F>(vsum);  // V' = P sum V
+                v_out[blockIdx.x] = vsum;
+            }
         }
     }
 }
@@ -680,15 +727,6 @@ void msm_enqueue(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_
     XYZZ<F>* d_lvl_r = d_lvl_u + (size_t)NW * S;
     XYZZ<F>* d_win = ws.windows.as<XYZZ<F>>(NW);
     constexpr int P = sizeof(F) == sizeof(Fq) ? 256 : 128;
-    const size_t smem = (size_t)P * sizeof(XYZZ<F>);
-    static bool smem_set[64] = {};
-    int dev = 0;
-    DV_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) throw InvalidArgument("device ordinal out of range");
-    if (!smem_set[dev]) {
-        DV_CUDA(cudaFuncSetAttribute(k_wlevel<F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        smem_set[dev] = true;
-    }
 
     if (tl.enabled) DV_CUDA(cudaEventRecord(tl.acc_ev[0], st));
     k_accum<F><<<grid, 128, 0, st>>>(pre ? pre->table : d_points, d_sorted, d_offsets, NB, d_buckets, d_pgid, d_ppt);
@@ -716,7 +754,7 @@ void msm_enqueue(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_
     for (;;) {
         const uint32_t nblk = len > (uint32_t)P ? len / P : 1u;
         XYZZ<F>* u_dst = nblk == 1 ? d_win : u2;
-        k_wlevel<F, P><<<NW * nblk, P, smem, st>>>(u, r, len, u_dst, r2);
+        k_wlevel<F, P><<<NW * nblk, P, 0, st>>>(u, r, len, u_dst, r2);
         DV_LAUNCH();
         if (nblk == 1) break;
         len = nblk;
