@@ -435,7 +435,7 @@ class FixedBaseOp:
         return self.n * 32, self.n * 64
 
     def roofline(self, tl, imad_peak, step_ms):
-        macs = self.n * (64 * 10 + 10) * 136  # 64 mixed adds + warp-shared normalisation per point
+        macs = self.n * (16 * 10 + 10) * 136  # 16 mixed adds (16-bit signed windows) + warp-shared normalisation
         ach = macs / (step_ms * 1e-3) / 1e12
         return ({"bound": "imad", "kernel": "k_fb_generate", "achieved": ach, "peak": imad_peak / 1e12,
                  "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12), "algorithmic_macs_per_launch": macs,

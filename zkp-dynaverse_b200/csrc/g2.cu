@@ -125,20 +125,50 @@ DV_INL Affine<Fq2> generator<Fq2>() {
     return {{Fq::from_canonical(w[0]), Fq::from_canonical(w[1])}, {Fq::from_canonical(w[2]), Fq::from_canonical(w[3])}};
 }
 
-// One thread per window w < 64: table[w][d] = d * 16^w * G (affine).
+// Fixed-base tables: scalars as 16 signed digits of 16 bits,
+// s = sum d_w 2^(16 w) with d_w in [-2^15, 2^15) (s < r < 2^254, so the top
+// digit takes the last carry), and table[w 2^15 + |d| - 1] = |d| 2^(16 w) G
+// in affine Montgomery form: 2^19 entries, 32 MB for G1 and 64 MB for G2,
+// built once per backend and read from L2.  A scalar then costs 16 mixed
+// additions.
+constexpr int FB_WINDOWS = 16;
+constexpr uint32_t FB_HALF = 1u << 15;
+constexpr uint32_t FB_RUN = 16;  // table entries per build thread
+
+// bases[w] = 2^(16 w) G, one thread per window.
 template <class F>
-__global__ void k_fb_table(Affine<F>* __restrict__ table) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= 64) return;
-    XYZZ<F> base = XYZZ<F>::from_affine(generator<F>());
-    for (int k = 0; k < 4 * w; ++k) base = XYZZ<F>::dbl(base);
-    XYZZ<F> acc = XYZZ<F>::inf();
-    for (int d = 0; d < 16; ++d) {
-        table[w * 16 + d] = acc.to_affine();
-        acc = XYZZ<F>::add(acc, base);
-    }
+__global__ void k_fb_bases(XYZZ<F>* __restrict__ bases) {
+    const int w = threadIdx.x;
+    if (w >= FB_WINDOWS) return;
+    XYZZ<F> b = XYZZ<F>::from_affine(generator<F>());
+    for (int k = 0; k < 16 * w; ++k) b = XYZZ<F>::dbl(b);
+    bases[w] = b;
 }
 
+// Thread t of window w builds entries j0 .. j0 + 15 (j0 = 16 (t mod 2^11)):
+// (j0 + 1) B by double-and-add, then B added per entry; every entry is
+// normalised by a warp-wide inversion (all lanes run the same 16 steps).
+template <class F>
+__global__ void __launch_bounds__(128) k_fb_table(const XYZZ<F>* __restrict__ bases, Affine<F>* __restrict__ table) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;  // grid covers exactly 16 * 2^11 threads
+    const uint32_t per_w = FB_HALF / FB_RUN;
+    const uint32_t w = t / per_w, j0 = (t % per_w) * FB_RUN;
+    const XYZZ<F> b = bases[w];
+    XYZZ<F> p = XYZZ<F>::inf();
+    const uint32_t m = j0 + 1;
+    for (int bit = 15; bit >= 0; --bit) {
+        p = XYZZ<F>::dbl(p);
+        if ((m >> bit) & 1u) p = XYZZ<F>::add(p, b);
+    }
+    for (uint32_t e = 0; e < FB_RUN; ++e) {
+        const bool inf = p.is_inf();
+        const F d = warp_batch_inverse<F>(inf ? F::one() : F::mul(p.zz, p.zzz));
+        Affine<F> a = Affine<F>::inf();
+        if (!inf) a = {F::mul(p.x, F::mul(d, p.zzz)), F::mul(p.y, F::mul(d, p.zz))};
+        table[(size_t)w * FB_HALF + j0 + e] = a;
+        p = XYZZ<F>::add(p, b);
+    }
+}
 
 template <class F>
 __global__ void __launch_bounds__(128) k_fb_generate(const uint8_t* __restrict__ scalars, uint64_t n,
@@ -153,9 +183,17 @@ __global__ void __launch_bounds__(128) k_fb_generate(const uint8_t* __restrict__
         if (!Fr::is_canonical(s)) {
             atomicMin(first_bad, (uint32_t)i);
         } else {
-            for (int w = 0; w < 64; ++w) {
-                const uint32_t d = (s[w >> 3] >> (4 * (w & 7))) & 15u;
-                if (d) acc = XYZZ<F>::add_affine(acc, table[w * 16 + d]);
+            uint32_t carry = 0;
+#pragma unroll 1
+            for (int w = 0; w < FB_WINDOWS; ++w) {
+                const uint32_t v = ((s[w >> 1] >> (16 * (w & 1))) & 0xffffu) + carry;
+                carry = v >= FB_HALF ? 1u : 0u;
+                const int d = carry ? (int)v - (int)(2 * FB_HALF) : (int)v;
+                if (d) {
+                    Affine<F> e = table[(size_t)w * FB_HALF + (uint32_t)(d < 0 ? -d : d) - 1];
+                    if (d < 0) e.y = F::neg(e.y);
+                    acc = XYZZ<F>::add_affine(acc, e);
+                }
             }
         }
     }
@@ -190,18 +228,26 @@ void g2_check_launch(const uint8_t* d_wire, uint64_t n, uint32_t algorithm, uint
 void fixed_base_launch(FixedBaseTables& tabs, const uint8_t* d_scalars, uint64_t n, int g2, uint8_t* d_out,
                        uint32_t* d_first_bad, cudaStream_t st) {
     if (!n) return;
+    const uint64_t entries = (uint64_t)FB_WINDOWS * FB_HALF;
+    const unsigned build_blocks = (unsigned)(entries / FB_RUN / 128);
     if (g2) {
-        G2A* t = tabs.g2.as<G2A>(64 * 16);
+        G2A* t = tabs.g2.as<G2A>(entries);
         if (!tabs.g2_ready) {
-            k_fb_table<Fq2><<<1, 64, 0, st>>>(t);
+            G2X* bases = tabs.bases.as<G2X>(FB_WINDOWS);
+            k_fb_bases<Fq2><<<1, 32, 0, st>>>(bases);
+            DV_LAUNCH();
+            k_fb_table<Fq2><<<build_blocks, 128, 0, st>>>(bases, t);
             DV_LAUNCH();
             tabs.g2_ready = true;
         }
         k_fb_generate<Fq2><<<blocks_for(n, 128), 128, 0, st>>>(d_scalars, n, t, d_out, d_first_bad);
     } else {
-        G1A* t = tabs.g1.as<G1A>(64 * 16);
+        G1A* t = tabs.g1.as<G1A>(entries);
         if (!tabs.g1_ready) {
-            k_fb_table<Fq><<<1, 64, 0, st>>>(t);
+            G1X* bases = tabs.bases.as<G1X>(FB_WINDOWS);
+            k_fb_bases<Fq><<<1, 32, 0, st>>>(bases);
+            DV_LAUNCH();
+            k_fb_table<Fq><<<build_blocks, 128, 0, st>>>(bases, t);
             DV_LAUNCH();
             tabs.g1_ready = true;
         }

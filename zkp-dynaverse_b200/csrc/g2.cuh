@@ -35,7 +35,8 @@ void g2_check_launch(const uint8_t* d_wire, uint64_t n, uint32_t algorithm, uint
                      cudaStream_t stream);
 
 struct FixedBaseTables {
-    DevBuf g1, g2;  // 64 * 16 affine entries each
+    DevBuf g1, g2;  // 16 * 2^15 affine entries each: |d| 2^(16 w) G
+    DevBuf bases;   // the 16 window bases while a table is built
     bool g1_ready = false, g2_ready = false;
 };
 
