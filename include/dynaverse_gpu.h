@@ -106,6 +106,31 @@ int dvgpu_g2_validation_traffic(void* owner, DvgpuG2ValidationTraffic* stats);
 int dvgpu_bn254_fixed_base_g2_checked(void* owner, const uint8_t* scalars, size_t n, uint32_t algorithm,
                                       uint8_t* output, DvgpuG2ValidationReport* report, char* error,
                                       size_t error_capacity);
+/* G2 check kernel diagnostics (native/include/dynaverse_g2_experiments.h:6-17,
+ * bound by crates/gpu/src/g2_validation.rs:91-94).  config: threads 64, 128
+ * or 256 is the check kernel's block size; schedule, layout and fused (0 or
+ * 1) name the reference's experimental variants and are accepted and kept
+ * without effect (this library has one check kernel, with the fixed-base
+ * normalisation always fused).  resources: the check kernel's attributes and
+ * theoretical occupancy at the configured block size, and those of the
+ * checked G2 fixed-base generation.  experiment stats: no repacking
+ * (repack fields 0); subgroup_kernel_ns sums the check kernel's device time. */
+typedef struct DvgpuG2KernelConfig {
+    uint32_t threads, schedule, layout, fused;
+} DvgpuG2KernelConfig;
+typedef struct DvgpuG2ExperimentStats {
+    uint64_t repack_device_ns, subgroup_kernel_ns, logical_repack_bytes;
+} DvgpuG2ExperimentStats;
+typedef struct DvgpuG2KernelResources {
+    uint32_t registers, block_threads, active_blocks, max_threads_per_sm;
+    uint64_t local_bytes, shared_bytes;
+    uint32_t normalize_registers, normalize_active_blocks;
+    uint64_t normalize_local_bytes, normalize_shared_bytes;
+} DvgpuG2KernelResources;
+int dvgpu_g2_kernel_config_set(void* owner, const DvgpuG2KernelConfig* config);
+int dvgpu_g2_kernel_config_get(void* owner, DvgpuG2KernelConfig* config);
+int dvgpu_g2_kernel_resources(void* owner, uint32_t algorithm, DvgpuG2KernelResources* output);
+int dvgpu_g2_experiment_stats(void* owner, DvgpuG2ExperimentStats* output);
 int dvgpu_backend_batch_stats(void* backend, DvgpuBatchStats* stats);
 typedef struct DvgpuMemoryInfo {
     uint64_t free_bytes;
@@ -127,6 +152,37 @@ typedef struct DvgpuMsmTimings {
 } DvgpuMsmTimings;
 int dvgpu_bn254_msm_profiled(void* backend, const uint8_t* points, const uint8_t* scalars, size_t length,
                              uint8_t* result, DvgpuMsmTimings* timings, char* error, size_t error_capacity);
+/* One MSM with its phase timeline (native/include/dynaverse_gpu.h:169-192,
+ * bound by crates/gpu/src/icicle.rs:54, used at :250).  Phases: 0
+ * allocation_preparation, 1 point_h2d, 2 scalar_h2d, 3 kernel_submission
+ * (point conversion, digit sort, accumulation, reduction, window
+ * combination), 4 synchronization, 5 output_d2h, 6 remaining_overhead, 7
+ * metadata_d2h (the point-validation word), 8 free (nothing is freed: the
+ * workspaces grow only).  wall_ns is the host clock, event_ns CUDA events on
+ * the owner's stream: different clocks, not additive.  Kernel slots: 0
+ * digit histogram, 1 offsets scan, 2 scatter, 6 bucket accumulation with its
+ * split-bucket merges, 7 bucket reduction, 8 window combination (host), 9
+ * point conversion (not timed alone: 0).  label names the call in the
+ * reference's NVTX ranges and is unused here. */
+enum { DVGPU_TIMELINE_PHASES = 9, DVGPU_TIMELINE_KERNELS = 10 };
+typedef struct DvgpuMsmTimeline {
+    uint64_t wall_ns[DVGPU_TIMELINE_PHASES];
+    uint64_t event_ns[DVGPU_TIMELINE_PHASES];
+    uint64_t calls[DVGPU_TIMELINE_PHASES];
+    uint64_t event_calls[DVGPU_TIMELINE_PHASES];
+    uint64_t bytes[DVGPU_TIMELINE_PHASES];
+    uint64_t kernel_ns[DVGPU_TIMELINE_KERNELS];
+    uint64_t kernel_calls[DVGPU_TIMELINE_KERNELS];
+    uint64_t instrumentation_inclusive_ns;
+    uint64_t instrumentation_total_ns;
+    uint64_t c;
+    uint64_t bitsize;
+    uint64_t windows;
+    uint64_t buckets;
+} DvgpuMsmTimeline;
+int dvgpu_bn254_msm_timeline(void* backend, const uint8_t* points, const uint8_t* scalars, size_t length,
+                             uint8_t* result, const char* label, DvgpuMsmTimings* timings, DvgpuMsmTimeline* timeline,
+                             char* error, size_t error_capacity);
 
 /* ======================= additive entry points ========================= */
 
@@ -406,6 +462,21 @@ void dvgpu_resident_seal(void* backend);
 void dvgpu_resident_commit(void* backend);
 int dvgpu_resident_stats(void* backend, DvgpuResidentStats* stats);
 int dvgpu_resident_diagnostics(void* backend, DvgpuResidentDiagnostics* stats);
+/* dvgpu_resident_call with its costs (native/include/dynaverse_gpu.h:147-158,
+ * bound by crates/gpu/src/resident_profile.rs:40).  native_wall_ns and
+ * operation_host_ns: host clock around the call; wait_host_ns: the closing
+ * stream synchronisation; journal and conversion host times are inside the
+ * operation (0); event_total_ns: CUDA events around the call on the owner's
+ * stream (event_mask 4, total only); h2d / d2h / d2d bytes: this call's
+ * change in the owner's resident counters. */
+typedef struct DvgpuResidentProfile {
+    uint64_t native_wall_ns, journal_host_ns, conversion_host_ns;
+    uint64_t operation_host_ns, wait_host_ns;
+    uint64_t event_total_ns, event_journal_ns, event_operation_ns, event_mask;
+    uint64_t h2d_bytes, d2h_bytes, d2d_bytes;
+} DvgpuResidentProfile;
+int dvgpu_resident_call_profiled(void* backend, const DvgpuResidentOp* operation, uint64_t* result,
+                                 DvgpuResidentProfile* profile, char* error, size_t error_capacity);
 
 /* ---------------------------------------------------------------- batching
  * No counterpart in the reference ABI (its batch path is

@@ -4,6 +4,7 @@ the CUDA sources equal the values computed here with Python integers."""
 import ctypes
 import os
 import re
+import subprocess
 import sys
 
 import pytest
@@ -31,8 +32,40 @@ def test_header_declares_reference_entry_points():
               "dvgpu_bn254_msm", "dvgpu_bn254_msm_batch", "dvgpu_bn254_g2_msm", "dvgpu_bn254_ntt",
               "dvgpu_bn254_msm_profiled", "dvgpu_bn254_fixed_base", "dvgpu_setup_mode", "dvgpu_setup_stats",
               "dvgpu_bn254_g2_validation_inspect", "dvgpu_g2_validation_stats", "dvgpu_g2_validation_traffic",
-              "dvgpu_bn254_fixed_base_g2_checked", "dvgpu_reserve_batch"]:
+              "dvgpu_bn254_fixed_base_g2_checked", "dvgpu_reserve_batch",
+              # diagnostics bound by icicle.rs:54, g2_validation.rs:91-94, resident_profile.rs:40
+              "dvgpu_bn254_msm_timeline", "dvgpu_g2_kernel_config_set", "dvgpu_g2_kernel_config_get",
+              "dvgpu_g2_kernel_resources", "dvgpu_g2_experiment_stats", "dvgpu_resident_call_profiled"]:
         assert n in names, n
+
+
+def test_diagnostic_struct_layouts(dv, tmp_path):
+    """The byte layouts the reference's Rust bindings assert
+    (crates/gpu/src/g2_validation.rs:48-49) and the timeline / profile
+    records, in C and in the Python mirror."""
+    src = tmp_path / "sizes.c"
+    src.write_text('#include "dynaverse_gpu.h"\n'
+                   "_Static_assert(sizeof(DvgpuG2KernelConfig) == 16, \"config\");\n"
+                   "_Static_assert(sizeof(DvgpuG2KernelResources) == 56, \"resources\");\n"
+                   "_Static_assert(sizeof(DvgpuG2ExperimentStats) == 24, \"experiment\");\n"
+                   "_Static_assert(sizeof(DvgpuMsmTimeline) == 8 * (5 * 9 + 2 * 10 + 6), \"timeline\");\n"
+                   "_Static_assert(sizeof(DvgpuResidentProfile) == 96, \"profile\");\n")
+    subprocess.run(["gcc", "-fsyntax-only", "-I", os.path.dirname(HEADER), str(src)], check=True)
+    assert ctypes.sizeof(dv.G2KernelConfig) == 16 and ctypes.sizeof(dv.G2KernelResources) == 56
+    assert ctypes.sizeof(dv.G2ExperimentStats) == 24 and ctypes.sizeof(dv.ResidentProfile) == 96
+    assert ctypes.sizeof(dv.MsmTimeline) == 8 * (5 * 9 + 2 * 10 + 6)
+
+
+def test_diagnostics_reject_null_owner(dv):
+    lib = dv.lib()
+    cfg = dv.G2KernelConfig(128, 0, 0, 0)
+    assert lib.dvgpu_g2_kernel_config_set(None, ctypes.byref(cfg)) == -1
+    assert lib.dvgpu_g2_kernel_config_get(None, ctypes.byref(cfg)) == -1
+    assert lib.dvgpu_g2_experiment_stats(None, ctypes.byref(dv.G2ExperimentStats())) == -1
+    assert lib.dvgpu_g2_kernel_resources(None, 3, ctypes.byref(dv.G2KernelResources())) == -1
+    prof = dv.ResidentProfile()
+    assert lib.dvgpu_resident_call_profiled(None, None, None, ctypes.byref(prof), None, 0) == -1
+    assert lib.dvgpu_bn254_msm_timeline(None, None, None, 0, None, None, None, None, None, 0) == -1
 
 
 def test_library_exports_every_declared_symbol(dv):

@@ -110,6 +110,44 @@ class SetupStats(ctypes.Structure):
                 ("device_ns", ctypes.c_uint64 * 5), ("native_wall_ns", ctypes.c_uint64)]
 
 
+class G2KernelConfig(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("threads", "schedule", "layout", "fused")]
+
+
+class G2ExperimentStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("repack_device_ns", "subgroup_kernel_ns", "logical_repack_bytes")]
+
+
+class G2KernelResources(ctypes.Structure):
+    _fields_ = [("registers", ctypes.c_uint32), ("block_threads", ctypes.c_uint32),
+                ("active_blocks", ctypes.c_uint32), ("max_threads_per_sm", ctypes.c_uint32),
+                ("local_bytes", ctypes.c_uint64), ("shared_bytes", ctypes.c_uint64),
+                ("normalize_registers", ctypes.c_uint32), ("normalize_active_blocks", ctypes.c_uint32),
+                ("normalize_local_bytes", ctypes.c_uint64), ("normalize_shared_bytes", ctypes.c_uint64)]
+
+
+class MsmTimings(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("conversion_ns", "icicle_ns", "output_ns")]
+
+
+TIMELINE_PHASES, TIMELINE_KERNELS = 9, 10
+
+
+class MsmTimeline(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64 * TIMELINE_PHASES) for n in ("wall_ns", "event_ns", "calls", "event_calls",
+                                                                   "bytes")] + \
+               [(n, ctypes.c_uint64 * TIMELINE_KERNELS) for n in ("kernel_ns", "kernel_calls")] + \
+               [(n, ctypes.c_uint64) for n in ("instrumentation_inclusive_ns", "instrumentation_total_ns", "c",
+                                               "bitsize", "windows", "buckets")]
+
+
+class ResidentProfile(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "native_wall_ns", "journal_host_ns", "conversion_host_ns", "operation_host_ns", "wait_host_ns",
+        "event_total_ns", "event_journal_ns", "event_operation_ns", "event_mask", "h2d_bytes", "d2h_bytes",
+        "d2d_bytes")]
+
+
 # (name, restype, argtypes)
 _P = ctypes.c_void_p
 _B = ctypes.c_char_p
@@ -132,6 +170,12 @@ SIGNATURES = [
      [_P, _P, _SZ, ctypes.c_uint32, _P, ctypes.POINTER(G2ValidationReport)] + _E),
     ("dvgpu_g2_validation_stats", ctypes.c_int, [_P, _P]),
     ("dvgpu_g2_validation_traffic", ctypes.c_int, [_P, _P]),
+    ("dvgpu_g2_kernel_config_set", ctypes.c_int, [_P, ctypes.POINTER(G2KernelConfig)]),
+    ("dvgpu_g2_kernel_config_get", ctypes.c_int, [_P, ctypes.POINTER(G2KernelConfig)]),
+    ("dvgpu_g2_kernel_resources", ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(G2KernelResources)]),
+    ("dvgpu_g2_experiment_stats", ctypes.c_int, [_P, ctypes.POINTER(G2ExperimentStats)]),
+    ("dvgpu_bn254_msm_timeline", ctypes.c_int, [_P, _P, _P, _SZ, _B, _B, ctypes.POINTER(MsmTimings),
+                                                 ctypes.POINTER(MsmTimeline)] + _E),
     ("dvgpu_bn254_fixed_base_g2_checked", ctypes.c_int,
      [_P, _P, _SZ, ctypes.c_uint32, _B, ctypes.POINTER(G2ValidationReport)] + _E),
     ("dvgpu_bn254_fixed_base", ctypes.c_int, [_P, _P, _SZ, ctypes.c_int, _B] + _E),
@@ -192,6 +236,8 @@ SIGNATURES = [
     ("dvgpu_resident_commit", None, [_P]),
     ("dvgpu_resident_stats", ctypes.c_int, [_P, ctypes.POINTER(ResidentStats)]),
     ("dvgpu_resident_diagnostics", ctypes.c_int, [_P, ctypes.POINTER(ResidentDiagnostics)]),
+    ("dvgpu_resident_call_profiled", ctypes.c_int, [_P, ctypes.POINTER(ResidentOp), ctypes.POINTER(ctypes.c_uint64),
+                                                    ctypes.POINTER(ResidentProfile)] + _E),
     ("dvgpu_serve_create", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(_P)] + _E),
     ("dvgpu_serve_destroy", None, [_P]),
     ("dvgpu_serve_open_session", ctypes.c_int, [_P, _P, _P, _SZ, ctypes.POINTER(ctypes.c_uint64), _B] + _E),
@@ -412,6 +458,17 @@ class DvgpuBackend:
         self._call("dvgpu_bn254_msm", _ptr(points), _ptr(scalars), n, out)
         return out.raw
 
+    def msm_with_timeline(self, points: bytes, scalars: bytes, label: bytes = b"msm"):
+        """dvgpu_bn254_msm_timeline: (64-byte affine, MsmTimings, MsmTimeline)."""
+        n = len(scalars) // FR_BYTES
+        if len(points) != n * G1_BYTES or len(scalars) != n * FR_BYTES:
+            raise ValueError("MSM length mismatch")
+        out = ctypes.create_string_buffer(G1_BYTES)
+        tm, tl = MsmTimings(), MsmTimeline()
+        self._call("dvgpu_bn254_msm_timeline", _ptr(points), _ptr(scalars), n, out, label, ctypes.byref(tm),
+                   ctypes.byref(tl))
+        return out.raw, tm, tl
+
     def msm_g2_host(self, points: bytes, scalars: bytes) -> bytes:
         """G2 sum s_i Q_i -> 128-byte affine (types.rs:351-356)."""
         n = len(scalars) // FR_BYTES
@@ -578,6 +635,33 @@ class DvgpuBackend:
                    ctypes.byref(rep))
         return masks[:n], rep
 
+    def g2_kernel_config(self, config=None):
+        """Get (config None) or set the G2 check kernel configuration
+        (G2KernelConfig or a (threads, schedule, layout, fused) tuple)."""
+        if config is None:
+            c = G2KernelConfig()
+            if self._L.dvgpu_g2_kernel_config_get(self.handle, ctypes.byref(c)) != 0:
+                raise DvgpuError(-1, "invalid G2 kernel config owner")
+            return c
+        c = config if isinstance(config, G2KernelConfig) else G2KernelConfig(*config)
+        rc = self._L.dvgpu_g2_kernel_config_set(self.handle, ctypes.byref(c))
+        if rc != 0:
+            raise DvgpuError(rc, "invalid or retired G2 kernel config")
+        return c
+
+    def g2_kernel_resources(self, algorithm: int):
+        r = G2KernelResources()
+        rc = self._L.dvgpu_g2_kernel_resources(self.handle, algorithm, ctypes.byref(r))
+        if rc != 0:
+            raise DvgpuError(rc, "G2 kernel resource query failed")
+        return r
+
+    def g2_experiment_stats(self):
+        st = G2ExperimentStats()
+        if self._L.dvgpu_g2_experiment_stats(self.handle, ctypes.byref(st)) != 0:
+            raise DvgpuError(-1, "invalid G2 experiment owner")
+        return st
+
     def fixed_base_g2_checked(self, scalars: bytes, algorithm: int):
         n = len(scalars) // FR_BYTES
         out = ctypes.create_string_buffer(max(1, n) * G2_BYTES)
@@ -726,6 +810,17 @@ class DvgpuBackend:
         r = ctypes.c_uint64()
         self._call("dvgpu_resident_call", ctypes.byref(op), ctypes.byref(r))
         return r.value
+
+    def resident_call_profiled(self, opcode: str, **fields):
+        """dvgpu_resident_call_profiled: (result, ResidentProfile)."""
+        op = ResidentOp()
+        op.opcode = RESIDENT_OPS[opcode]
+        for k, v in fields.items():
+            setattr(op, k, v)
+        r = ctypes.c_uint64()
+        prof = ResidentProfile()
+        self._call("dvgpu_resident_call_profiled", ctypes.byref(op), ctypes.byref(r), ctypes.byref(prof))
+        return r.value, prof
 
     def rb_alloc(self, kind: int, length: int, writable: bool) -> int:
         return self.resident_call("ALLOC", kind=kind, length=length, flags=int(writable))

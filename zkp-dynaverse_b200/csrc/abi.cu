@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -18,6 +19,32 @@
 using namespace dv;
 
 namespace {
+
+// A pair of timing events, destroyed with the pair.
+struct EventPair {
+    cudaEvent_t start = nullptr, end = nullptr;
+    EventPair() {
+        DV_CUDA(cudaEventCreate(&start));
+        DV_CUDA(cudaEventCreate(&end));
+    }
+    ~EventPair() {
+        if (start) cudaEventDestroy(start);
+        if (end) cudaEventDestroy(end);
+    }
+    EventPair(const EventPair&) = delete;
+    EventPair& operator=(const EventPair&) = delete;
+    // after both events completed
+    uint64_t ns() const {
+        float ms = 0.f;
+        DV_CUDA(cudaEventElapsedTime(&ms, start, end));
+        return (uint64_t)((double)ms * 1e6);
+    }
+};
+
+using steady = std::chrono::steady_clock;
+uint64_t ns_since(steady::time_point t) {
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(steady::now() - t).count();
+}
 
 // Window width: an explicit dvgpu_msm_set_window wins, then the autotuned
 // width for the size class of the largest set, then the cost model (0).
@@ -671,6 +698,7 @@ extern "C" int dvgpu_setup_stats(void* opaque, DvgpuSetupStats* stats) {
 
 // ============================================================ G2 validation
 namespace {
+
 DvgpuG2ValidationReport g2_check_device(Backend& b, const uint8_t* d_wire, size_t n, uint32_t algorithm,
                                         uint32_t* d_masks, cudaStream_t st) {
     G2CheckAccum* acc = b.aux.as<G2CheckAccum>(1);
@@ -678,9 +706,15 @@ DvgpuG2ValidationReport g2_check_device(Backend& b, const uint8_t* d_wire, size_
     G2CheckAccum* h = b.pin_out.as<G2CheckAccum>(1);
     *h = init;
     DV_CUDA(cudaMemcpyAsync(acc, h, sizeof(init), cudaMemcpyHostToDevice, st));
-    g2_check_launch(d_wire, n, algorithm, d_masks, acc, st);
+    EventPair ev;
+    DV_CUDA(cudaEventRecord(ev.start, st));
+    g2_check_launch(d_wire, n, algorithm, d_masks, acc, st, b.g2_kernel.threads);
+    DV_CUDA(cudaEventRecord(ev.end, st));
     DV_CUDA(cudaMemcpyAsync(h, acc, sizeof(init), cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaStreamSynchronize(st));
+    const uint64_t kernel_ns = ev.ns();
+    b.g2_stats.subgroup_device_ns += kernel_ns;
+    b.g2_experiment.subgroup_kernel_ns += kernel_ns;
     DvgpuG2ValidationReport r;
     r.checked_points = n;
     r.invalid_points = h->invalid;
@@ -772,6 +806,39 @@ extern "C" int dvgpu_bn254_fixed_base_g2_checked(void* opaque, const uint8_t* sc
     return rc;
 }
 
+extern "C" int dvgpu_g2_kernel_config_set(void* opaque, const DvgpuG2KernelConfig* config) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b) return -1;
+    if (b->retired) return -4;
+    if (!config || (config->threads != 64 && config->threads != 128 && config->threads != 256) ||
+        config->schedule > 1 || config->layout > 1 || config->fused > 1)
+        return -1;
+    b->g2_kernel = *config;
+    return 0;
+}
+
+extern "C" int dvgpu_g2_kernel_config_get(void* opaque, DvgpuG2KernelConfig* config) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || !config) return -1;
+    *config = b->g2_kernel;
+    return 0;
+}
+
+extern "C" int dvgpu_g2_kernel_resources(void* opaque, uint32_t algorithm, DvgpuG2KernelResources* output) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b) return -1;
+    if (b->retired) return -4;
+    if (!output || algorithm < 1 || algorithm > 3) return -1;
+    return guarded(opaque, nullptr, 0, [&](Backend& bb) { g2_kernel_resources(bb.g2_kernel.threads, *output); });
+}
+
+extern "C" int dvgpu_g2_experiment_stats(void* opaque, DvgpuG2ExperimentStats* output) {
+    auto* b = static_cast<Backend*>(opaque);
+    if (!b || !output) return -1;
+    *output = b->g2_experiment;
+    return 0;
+}
+
 extern "C" int dvgpu_g2_validation_stats(void* opaque, DvgpuG2ValidationStats* stats) {
     auto* b = static_cast<Backend*>(opaque);
     if (!b || !stats) return -1;
@@ -815,6 +882,160 @@ extern "C" int dvgpu_probe_imad_rate(void* opaque, double* macs_per_second, char
         const double macs = (double)blocks * threads * iters * 4.0 * 4.0;
         *macs_per_second = macs / (best * 1e-3);
     });
+}
+
+namespace {
+// dvgpu_bn254_msm_timeline: the reference's phases around one single-set
+// MSM, with the device phases from the owner's MSM timeline (turned on for
+// the call, and its totals left as they were when it was off).
+void msm_timeline_call(Backend& b, const uint8_t* points, const uint8_t* scalars, size_t n, uint8_t* result,
+                       DvgpuMsmTimings& tm, DvgpuMsmTimeline& out) {
+    enum { ALLOC, POINT_H2D, SCALAR_H2D, KERNELS, SYNC, OUTPUT_D2H, OTHER, METADATA_D2H, FREE };
+    const auto t_all = steady::now();
+    out.bitsize = 254;
+    if (n == 0) {
+        memset(result, 0, 64);
+        return;
+    }
+    MsmTimeline& tl = b.msm.timeline;
+    if (!tl.ev[0]) {
+        for (auto& e : tl.ev) DV_CUDA(cudaEventCreate(&e));
+        for (auto& e : tl.acc_ev) DV_CUDA(cudaEventCreate(&e));
+    }
+    const bool was_on = tl.enabled;
+    double before[MSM_PHASES];
+    for (int k = 0; k < MSM_PHASES; ++k) before[k] = tl.ms[k];
+    const uint64_t calls_before = tl.calls, adds_before = tl.accum_mixed_adds;
+    auto restore = [&] {
+        if (was_on) return;
+        tl.enabled = false;
+        for (int k = 0; k < MSM_PHASES; ++k) tl.ms[k] = before[k];
+        tl.calls = calls_before;
+        tl.accum_mixed_adds = adds_before;
+    };
+    tl.enabled = true;
+    double phase_ms[MSM_PHASES];
+    try {
+        EventPair e_pts, e_sc, e_k;
+        auto t = steady::now();
+        uint8_t* d_pts = b.in_points.as<uint8_t>(n * 64);
+        uint8_t* d_sc = b.in_scalars.as<uint8_t>(n * 32);
+        out.wall_ns[ALLOC] += ns_since(t);
+        out.calls[ALLOC]++;
+        t = steady::now();
+        DV_CUDA(cudaEventRecord(e_pts.start, b.stream));
+        DV_CUDA(cudaMemcpyAsync(d_pts, points, n * 64, cudaMemcpyHostToDevice, b.stream));
+        DV_CUDA(cudaEventRecord(e_pts.end, b.stream));
+        out.wall_ns[POINT_H2D] += ns_since(t);
+        t = steady::now();
+        DV_CUDA(cudaEventRecord(e_sc.start, b.stream));
+        DV_CUDA(cudaMemcpyAsync(d_sc, scalars, n * 32, cudaMemcpyHostToDevice, b.stream));
+        DV_CUDA(cudaEventRecord(e_sc.end, b.stream));
+        out.wall_ns[SCALAR_H2D] += ns_since(t);
+        // conversion, sort, accumulation, reduction, the validation word, the
+        // window sums' copy and the host window combination
+        t = steady::now();
+        DV_CUDA(cudaEventRecord(e_k.start, b.stream));
+        msm_sets_device<Fq>(b, d_pts, d_sc, single_set(n), result, b.stream);
+        DV_CUDA(cudaEventRecord(e_k.end, b.stream));
+        out.wall_ns[KERNELS] += ns_since(t);
+        t = steady::now();
+        DV_CUDA(cudaStreamSynchronize(b.stream));
+        out.wall_ns[SYNC] += ns_since(t);
+        const auto t_inst = steady::now();
+        out.event_ns[POINT_H2D] += e_pts.ns();
+        out.event_ns[SCALAR_H2D] += e_sc.ns();
+        out.event_ns[KERNELS] += e_k.ns();
+        out.instrumentation_total_ns += ns_since(t_inst);
+        for (int k = 0; k < MSM_PHASES; ++k) phase_ms[k] = tl.ms[k] - before[k];
+    } catch (...) {
+        restore();
+        throw;
+    }
+    restore();
+    out.calls[POINT_H2D]++;
+    out.calls[SCALAR_H2D]++;
+    out.calls[KERNELS]++;
+    out.calls[SYNC]++;
+    out.calls[OUTPUT_D2H]++;
+    out.calls[METADATA_D2H]++;
+    out.event_calls[POINT_H2D]++;
+    out.event_calls[SCALAR_H2D]++;
+    out.event_calls[KERNELS]++;
+    out.bytes[POINT_H2D] += n * 64;
+    out.bytes[SCALAR_H2D] += n * 32;
+    out.bytes[OUTPUT_D2H] += 64;
+    out.bytes[METADATA_D2H] += 4;
+    auto put = [&](int slot, double ms) {
+        out.kernel_ns[slot] += (uint64_t)(ms * 1e6);
+        out.kernel_calls[slot]++;
+    };
+    put(0, phase_ms[0]);                // digit histogram
+    put(1, phase_ms[1]);                // offsets scan
+    put(2, phase_ms[2]);                // scatter
+    put(6, phase_ms[3] + phase_ms[4]);  // accumulation and split-bucket merges
+    put(7, phase_ms[5]);                // bucket reduction
+    put(8, phase_ms[7]);                // window sums' copy and host combination
+    out.kernel_calls[9]++;              // point conversion (inside the kernel span)
+    const uint64_t c = b.msm_stats.last_c ? b.msm_stats.last_c : 1;
+    out.c = c;
+    out.windows = (255 + c - 1) / c;
+    out.buckets = out.windows << (c - 1);
+    out.instrumentation_inclusive_ns = ns_since(t_all);
+    tm.icicle_ns = out.wall_ns[POINT_H2D] + out.wall_ns[SCALAR_H2D] + out.wall_ns[KERNELS] + out.wall_ns[SYNC];
+}
+}  // namespace
+
+extern "C" int dvgpu_bn254_msm_timeline(void* opaque, const uint8_t* points, const uint8_t* scalars, size_t length,
+                                        uint8_t* result, const char* label, DvgpuMsmTimings* timings,
+                                        DvgpuMsmTimeline* timeline, char* error, size_t cap) {
+    (void)label;  // names the call in the reference's NVTX ranges
+    if (!timings || !timeline) return fail(-1, "null diagnostic outputs", error, cap);
+    *timings = {};
+    *timeline = {};
+    return guarded(opaque, error, cap, [&](Backend& b) {
+        require(result && length <= DVGPU_MAX_MSM_SIZE && (!length || (points && scalars)),
+                "invalid MSM buffers or length");
+        msm_timeline_call(b, points, scalars, length, result, *timings, *timeline);
+    });
+}
+
+extern "C" int dvgpu_resident_call_profiled(void* opaque, const DvgpuResidentOp* operation, uint64_t* result,
+                                            DvgpuResidentProfile* profile, char* error, size_t cap) {
+    if (!profile) return fail(-1, "null resident profile", error, cap);
+    *profile = {};
+    DvgpuResidentProfile p{};
+    std::unique_ptr<EventPair> ev;
+    int rc = guarded(opaque, error, cap, [&](Backend& b) {
+        ev = std::make_unique<EventPair>();
+        DV_CUDA(cudaEventRecord(ev->start, b.stream));
+    });
+    if (rc) return rc;
+    DvgpuResidentStats s0{}, s1{};
+    DvgpuResidentDiagnostics d0{}, d1{};
+    dvgpu_resident_stats(opaque, &s0);
+    dvgpu_resident_diagnostics(opaque, &d0);
+    const auto t0 = steady::now();
+    rc = dvgpu_resident_call(opaque, operation, result, error, cap);
+    p.operation_host_ns = ns_since(t0);
+    if (rc) return rc;
+    rc = guarded(opaque, error, cap, [&](Backend& b) {
+        DV_CUDA(cudaEventRecord(ev->end, b.stream));
+        const auto w0 = steady::now();
+        DV_CUDA(cudaStreamSynchronize(b.stream));
+        p.wait_host_ns = ns_since(w0);
+        p.event_total_ns = ev->ns();
+    });
+    if (rc) return rc;
+    p.native_wall_ns = ns_since(t0);
+    p.event_mask = 4;
+    dvgpu_resident_stats(opaque, &s1);
+    dvgpu_resident_diagnostics(opaque, &d1);
+    p.h2d_bytes = s1.h2d_bytes - s0.h2d_bytes;
+    p.d2h_bytes = s1.d2h_bytes - s0.d2h_bytes;
+    p.d2d_bytes = d1.explicit_d2d_bytes - d0.explicit_d2d_bytes;
+    *profile = p;
+    return 0;
 }
 
 // ============================================================ diagnostics

@@ -55,6 +55,8 @@ struct Backend {
     DvgpuSetupStats setup_stats{};
     DvgpuG2ValidationStats g2_stats{};
     DvgpuG2ValidationTraffic g2_traffic{};
+    DvgpuG2KernelConfig g2_kernel{128, 0, 0, 0};
+    DvgpuG2ExperimentStats g2_experiment{};
     int setup_mode = 2;
     int force_c = 0;
     int tuned_c_g1[40] = {};  // autotuned window width per ceil(log2(points per set))

@@ -90,7 +90,7 @@ DV_INL uint32_t g2_wire_check(const uint8_t* b, uint32_t algorithm) {
     return ok ? 0 : 4;
 }
 
-__global__ void __launch_bounds__(128) k_g2_check(const uint8_t* __restrict__ wire, uint64_t n, uint32_t algorithm,
+__global__ void __launch_bounds__(256) k_g2_check(const uint8_t* __restrict__ wire, uint64_t n, uint32_t algorithm,
                                                   uint32_t* __restrict__ masks, G2CheckAccum* __restrict__ acc) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -219,10 +219,33 @@ inline unsigned blocks_for(uint64_t n, unsigned threads) { return (unsigned)((n 
 }  // namespace
 
 void g2_check_launch(const uint8_t* d_wire, uint64_t n, uint32_t algorithm, uint32_t* d_masks, G2CheckAccum* d_acc,
-                     cudaStream_t st) {
+                     cudaStream_t st, unsigned threads) {
     if (!n) return;
-    k_g2_check<<<blocks_for(n, 128), 128, 0, st>>>(d_wire, n, algorithm, d_masks, d_acc);
+    k_g2_check<<<blocks_for(n, threads), threads, 0, st>>>(d_wire, n, algorithm, d_masks, d_acc);
     DV_LAUNCH();
+}
+
+void g2_kernel_resources(unsigned threads, DvgpuG2KernelResources& out) {
+    int dev = 0, max_threads = 0, blocks = 0, nblocks = 0;
+    DV_CUDA(cudaGetDevice(&dev));
+    DV_CUDA(cudaDeviceGetAttribute(&max_threads, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+    cudaFuncAttributes a{}, na{};
+    DV_CUDA(cudaFuncGetAttributes(&a, k_g2_check));
+    DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_g2_check, (int)threads, 0));
+    // the checked fixed-base normalisation is fused into its generation kernel
+    DV_CUDA(cudaFuncGetAttributes(&na, k_fb_generate<Fq2>));
+    DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nblocks, k_fb_generate<Fq2>, 128, 0));
+    out = {};
+    out.registers = (uint32_t)a.numRegs;
+    out.block_threads = threads;
+    out.active_blocks = (uint32_t)blocks;
+    out.max_threads_per_sm = (uint32_t)max_threads;
+    out.local_bytes = a.localSizeBytes;
+    out.shared_bytes = a.sharedSizeBytes;
+    out.normalize_registers = (uint32_t)na.numRegs;
+    out.normalize_active_blocks = (uint32_t)nblocks;
+    out.normalize_local_bytes = na.localSizeBytes;
+    out.normalize_shared_bytes = na.sharedSizeBytes;
 }
 
 void fixed_base_launch(FixedBaseTables& tabs, const uint8_t* d_scalars, uint64_t n, int g2, uint8_t* d_out,

@@ -32,7 +32,10 @@ struct G2CheckAccum {
 
 // wire: device bytes (n * 128); masks: device u32[n]; acc: device accumulator.
 void g2_check_launch(const uint8_t* d_wire, uint64_t n, uint32_t algorithm, uint32_t* d_masks, G2CheckAccum* d_acc,
-                     cudaStream_t stream);
+                     cudaStream_t stream, unsigned threads = 128);
+// Attributes and theoretical occupancy of the check kernel at a block size,
+// and of the checked fixed-base generation (whose normalisation is fused).
+void g2_kernel_resources(unsigned threads, DvgpuG2KernelResources& out);
 
 struct FixedBaseTables {
     DevBuf g1, g2;  // 16 * 2^15 affine entries each: |d| 2^(16 w) G
