@@ -184,6 +184,28 @@ int dvgpu_bn254_msm_timeline(void* backend, const uint8_t* points, const uint8_t
                              uint8_t* result, const char* label, DvgpuMsmTimings* timings, DvgpuMsmTimeline* timeline,
                              char* error, size_t error_capacity);
 
+/* ---- research probes: declared so the crate's extern blocks link --------
+ * The reference's tower, line and Miller-loop inspectors and G2 psi probe
+ * (crates/gpu/src/bn254_tower.rs:40, bn254_lines.rs:24, bn254_miller.rs:38,
+ * g2_validation/tests.rs:273) and its test-only corruption hook
+ * (g2_validation/tuning_tests.rs:7) are diagnostics outside the compute
+ * path; here each returns -1 with "not provided" in the error text and
+ * writes no output.  The pairing checks they were built towards are
+ * dvgpu_bn254_pairing_check and friends. */
+int dvgpu_bn254_tower_inspect(void* owner, uint32_t degree, uint32_t operation, uint32_t power, const uint8_t* left,
+                              size_t left_bytes, const uint8_t* right, size_t right_bytes, uint8_t* output,
+                              size_t output_bytes, uint32_t* statuses, size_t statuses_count, char* error,
+                              size_t error_capacity);
+int dvgpu_bn254_lines_inspect(void* owner, const uint8_t* points, size_t points_bytes, uint8_t* output,
+                              size_t output_bytes, uint32_t* counts, size_t counts_count, uint32_t* statuses,
+                              size_t statuses_count, char* error, size_t error_capacity);
+int dvgpu_bn254_miller_inspect(void* owner, const uint8_t* p, size_t p_bytes, const uint8_t* q, size_t q_bytes,
+                               uint8_t* output, size_t output_bytes, uint32_t* metadata, size_t metadata_count,
+                               char* error, size_t error_capacity);
+int dvgpu_g2_psi_probe(void* owner, const uint8_t* points, size_t n, uint8_t* output, char* error,
+                       size_t error_capacity);
+int dvgpu_g2_test_corrupt_next(void* owner, uint64_t index);
+
 /* ======================= additive entry points ========================= */
 
 /* NTT of any kind: 0 forward, 1 inverse, 2 coset forward, 3 coset inverse

@@ -56,6 +56,32 @@ def test_diagnostic_struct_layouts(dv, tmp_path):
     assert ctypes.sizeof(dv.MsmTimeline) == 8 * (5 * 9 + 2 * 10 + 6)
 
 
+def test_every_symbol_the_reference_crate_binds_is_declared():
+    """Every dvgpu_* function named in the reference's Rust extern blocks
+    (crates/gpu/src) is declared, so the crate links against the library
+    (the research probes among them return -1)."""
+    bound = {"dvgpu_backend_create", "dvgpu_backend_create_with_large_bucket_factor", "dvgpu_backend_destroy",
+             "dvgpu_backend_device_identity", "dvgpu_backend_memory_info", "dvgpu_backend_batch_stats",
+             "dvgpu_bn254_msm", "dvgpu_bn254_msm_profiled", "dvgpu_bn254_msm_timeline", "dvgpu_bn254_msm_batch",
+             "dvgpu_bn254_g2_msm", "dvgpu_bn254_ntt", "dvgpu_bn254_fixed_base", "dvgpu_setup_mode",
+             "dvgpu_setup_stats", "dvgpu_reserve_batch", "dvgpu_bn254_g2_validation_inspect",
+             "dvgpu_g2_validation_stats", "dvgpu_g2_validation_traffic", "dvgpu_bn254_fixed_base_g2_checked",
+             "dvgpu_g2_kernel_config_set", "dvgpu_g2_kernel_config_get", "dvgpu_g2_kernel_resources",
+             "dvgpu_g2_experiment_stats", "dvgpu_resident_configure", "dvgpu_resident_call",
+             "dvgpu_resident_seal", "dvgpu_resident_commit", "dvgpu_resident_stats", "dvgpu_resident_diagnostics",
+             "dvgpu_resident_call_profiled", "dvgpu_bn254_tower_inspect", "dvgpu_bn254_lines_inspect",
+             "dvgpu_bn254_miller_inspect", "dvgpu_g2_psi_probe", "dvgpu_g2_test_corrupt_next"}
+    assert not bound - set(declared_functions())
+
+
+def test_research_probes_report_not_provided(dv):
+    lib = dv.lib()
+    err = ctypes.create_string_buffer(128)
+    assert lib.dvgpu_bn254_miller_inspect(None, None, 0, None, 0, None, 0, None, 0, err, 128) == -1
+    assert b"not provided" in err.value
+    assert lib.dvgpu_g2_test_corrupt_next(None, 0) == -1
+
+
 def test_diagnostics_reject_null_owner(dv):
     lib = dv.lib()
     cfg = dv.G2KernelConfig(128, 0, 0, 0)

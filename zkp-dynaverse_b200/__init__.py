@@ -174,6 +174,12 @@ SIGNATURES = [
     ("dvgpu_g2_kernel_config_get", ctypes.c_int, [_P, ctypes.POINTER(G2KernelConfig)]),
     ("dvgpu_g2_kernel_resources", ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(G2KernelResources)]),
     ("dvgpu_g2_experiment_stats", ctypes.c_int, [_P, ctypes.POINTER(G2ExperimentStats)]),
+    ("dvgpu_bn254_tower_inspect", ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P, _SZ, _P,
+                                                  _SZ, _P, _SZ, _P, _SZ] + _E),
+    ("dvgpu_bn254_lines_inspect", ctypes.c_int, [_P, _P, _SZ, _P, _SZ, _P, _SZ, _P, _SZ] + _E),
+    ("dvgpu_bn254_miller_inspect", ctypes.c_int, [_P, _P, _SZ, _P, _SZ, _P, _SZ, _P, _SZ] + _E),
+    ("dvgpu_g2_psi_probe", ctypes.c_int, [_P, _P, _SZ, _P] + _E),
+    ("dvgpu_g2_test_corrupt_next", ctypes.c_int, [_P, ctypes.c_uint64]),
     ("dvgpu_bn254_msm_timeline", ctypes.c_int, [_P, _P, _P, _SZ, _B, _B, ctypes.POINTER(MsmTimings),
                                                  ctypes.POINTER(MsmTimeline)] + _E),
     ("dvgpu_bn254_fixed_base_g2_checked", ctypes.c_int,

@@ -1038,6 +1038,25 @@ extern "C" int dvgpu_resident_call_profiled(void* opaque, const DvgpuResidentOp*
     return 0;
 }
 
+// ============================================================ research probes
+// Declared for link compatibility with the crate's extern blocks; not provided.
+extern "C" int dvgpu_bn254_tower_inspect(void*, uint32_t, uint32_t, uint32_t, const uint8_t*, size_t, const uint8_t*,
+                                         size_t, uint8_t*, size_t, uint32_t*, size_t, char* error, size_t cap) {
+    return fail(-1, "dvgpu_bn254_tower_inspect: research probe not provided by this library", error, cap);
+}
+extern "C" int dvgpu_bn254_lines_inspect(void*, const uint8_t*, size_t, uint8_t*, size_t, uint32_t*, size_t, uint32_t*,
+                                         size_t, char* error, size_t cap) {
+    return fail(-1, "dvgpu_bn254_lines_inspect: research probe not provided by this library", error, cap);
+}
+extern "C" int dvgpu_bn254_miller_inspect(void*, const uint8_t*, size_t, const uint8_t*, size_t, uint8_t*, size_t,
+                                          uint32_t*, size_t, char* error, size_t cap) {
+    return fail(-1, "dvgpu_bn254_miller_inspect: research probe not provided by this library", error, cap);
+}
+extern "C" int dvgpu_g2_psi_probe(void*, const uint8_t*, size_t, uint8_t*, char* error, size_t cap) {
+    return fail(-1, "dvgpu_g2_psi_probe: research probe not provided by this library", error, cap);
+}
+extern "C" int dvgpu_g2_test_corrupt_next(void*, uint64_t) { return -1; }
+
 // ============================================================ diagnostics
 namespace dv {
 void random_fr_launch(uint64_t seed, uint64_t n, uint8_t* d_out, cudaStream_t st);
