@@ -5,6 +5,8 @@ forward/inverse, round trips, invalid lengths), setup_tables.rs /
 fixed_base_cpu.rs, and g2_validation/tests.rs (wire corpus, masks 1/2/4,
 all three subgroup algorithms).
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -90,6 +92,25 @@ def test_fixed_base_matches_oracle(backend, oracle):
     for n in (1, 33, 700):
         sc = oracle.uniform_fr(20 + n, n)
         assert backend.fixed_base_g2(sc) == oracle.fixed_base_g2(sc), n
+
+
+def test_fixed_base_chunked_calls(backend, oracle, dv):
+    """Calls longer than one 2^17-point chunk (generation of a chunk overlaps
+    the host copy of the previous one), and a non-canonical scalar in a
+    later chunk: the call fails and writes no output."""
+    n = (1 << 17) + 1000
+    sc = oracle.uniform_fr(31, n)
+    assert backend.fixed_base_g1(sc) == oracle.fixed_base_g1(sc)
+    sc2 = sc[:32 * 70000]
+    assert backend.fixed_base_g2(sc2 + sc[32 * 131000:32 * 131100]) == \
+        oracle.fixed_base_g2(sc2 + sc[32 * 131000:32 * 131100])
+    bad = bytearray(sc)
+    bad[32 * 131500:32 * 131501] = b"\xff" * 32           # >= r, in the second chunk
+    out = ctypes.create_string_buffer(b"\xab" * (n * 64), n * 64)
+    err = ctypes.create_string_buffer(256)
+    rc = dv.lib().dvgpu_bn254_fixed_base(backend.handle, bytes(bad), n, 0, out, err, 256)
+    assert rc == -1 and b"131500" in err.value
+    assert out.raw == b"\xab" * (n * 64)
 
 
 @pytest.mark.parametrize("algorithm", [1, 2, 3])

@@ -225,6 +225,11 @@ void Backend::release_all() noexcept {
     for (auto& e : tl.acc_ev)
         if (e) { cudaEventDestroy(e); e = nullptr; }
     tl.enabled = false;
+    if (copy_stream) {
+        cudaStreamSynchronize(copy_stream);
+        cudaStreamDestroy(copy_stream);
+        copy_stream = nullptr;
+    }
     if (stream) {
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
@@ -632,16 +637,21 @@ extern "C" int dvgpu_bn254_ntt_device(void* opaque, const uint8_t* d_values, siz
 
 // ============================================================ fixed base
 namespace {
-void fixed_base_device(Backend& b, const uint8_t* d_scalars, size_t n, int g2, uint8_t* d_out, cudaStream_t st) {
+// [s_i] G on the device; with check (the default) the scalars' canonical
+// check is read back (one synchronisation), without it the caller has
+// checked them already and nothing waits.
+void fixed_base_device(Backend& b, const uint8_t* d_scalars, size_t n, int g2, uint8_t* d_out, cudaStream_t st,
+                       bool check = true) {
     uint32_t* bad = b.err.as<uint32_t>(1);
-    DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
+    if (check) DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), st));
     FixedBaseTables& t = b.fixed_base;
     const bool had = g2 ? t.g2_ready : t.g1_ready;
     fixed_base_launch(t, d_scalars, n, g2, d_out, bad, st);
     if (!had) {
         b.setup_stats.table_builds[g2]++;
-        b.setup_stats.table_bytes += 64 * 16 * (g2 ? 128 : 64);
+        b.setup_stats.table_bytes += fixed_base_table_entries() * (g2 ? 128 : 64);
     }
+    if (!check) return;  // a chunk of a call that counts itself
     const uint32_t first_bad = read_err_word(b, bad, st);
     if (first_bad != 0xffffffffu) throw InvalidArgument("non-canonical scalar at index " + std::to_string(first_bad));
     b.setup_stats.calls[g2]++;
@@ -660,9 +670,38 @@ extern "C" int dvgpu_bn254_fixed_base(void* opaque, const uint8_t* scalars, size
         uint8_t* d_sc = b.in_scalars.as<uint8_t>(length * 32);
         uint8_t* d_out = b.out_buf.as<uint8_t>(length * psize);
         DV_CUDA(cudaMemcpyAsync(d_sc, scalars, length * 32, cudaMemcpyHostToDevice, b.stream));
-        fixed_base_device(b, d_sc, length, g2, d_out, b.stream);  // synchronises and checks the scalars
-        DV_CUDA(cudaMemcpyAsync(output, d_out, length * psize, cudaMemcpyDeviceToHost, b.stream));
-        DV_CUDA(cudaStreamSynchronize(b.stream));
+        // every scalar is checked before any output is written
+        uint32_t* bad = b.err.as<uint32_t>(1);
+        DV_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), b.stream));
+        fixed_base_validate(d_sc, length, bad, b.stream);
+        const uint32_t first_bad = read_err_word(b, bad, b.stream);
+        if (first_bad != 0xffffffffu)
+            throw InvalidArgument("non-canonical scalar at index " + std::to_string(first_bad));
+        // chunks of 2^17 points: the copy of chunk k to the host overlaps the
+        // generation of chunk k + 1
+        if (!b.copy_stream) DV_CUDA(cudaStreamCreateWithFlags(&b.copy_stream, cudaStreamNonBlocking));
+        constexpr size_t CHUNK = size_t(1) << 17;
+        std::vector<cudaEvent_t> done((length + CHUNK - 1) / CHUNK, nullptr);
+        try {
+            for (size_t k = 0; k < done.size(); ++k) {
+                const size_t off = k * CHUNK, m = std::min(CHUNK, length - off);
+                fixed_base_device(b, d_sc + 32 * off, m, g2, d_out + psize * off, b.stream, false);
+                DV_CUDA(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+                DV_CUDA(cudaEventRecord(done[k], b.stream));
+                DV_CUDA(cudaStreamWaitEvent(b.copy_stream, done[k], 0));
+                DV_CUDA(cudaMemcpyAsync(output + psize * off, d_out + psize * off, m * psize, cudaMemcpyDeviceToHost,
+                                        b.copy_stream));
+            }
+            DV_CUDA(cudaStreamSynchronize(b.copy_stream));
+            DV_CUDA(cudaStreamSynchronize(b.stream));
+        } catch (...) {
+            for (cudaEvent_t e : done)
+                if (e) cudaEventDestroy(e);
+            throw;
+        }
+        for (cudaEvent_t e : done) DV_CUDA(cudaEventDestroy(e));
+        b.setup_stats.calls[g2]++;
+        b.setup_stats.points[g2] += length;
         b.setup_stats.native_wall_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
                                             std::chrono::steady_clock::now() - t0)
                                             .count();

@@ -41,6 +41,7 @@ struct PairingState;   // pairing.cu
 struct Backend {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // device-to-host copies overlapping the main stream (lazy)
     bool retired = false;
     uint32_t large_bucket_factor = 0;
     std::string identity;

@@ -248,6 +248,24 @@ void g2_kernel_resources(unsigned threads, DvgpuG2KernelResources& out) {
     out.normalize_shared_bytes = na.sharedSizeBytes;
 }
 
+namespace {
+__global__ void k_fb_validate(const uint8_t* __restrict__ scalars, uint64_t n, uint32_t* __restrict__ first_bad) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t s[8];
+    load_words(scalars + 32 * i, s);
+    if (!Fr::is_canonical(s)) atomicMin(first_bad, (uint32_t)i);
+}
+}  // namespace
+
+void fixed_base_validate(const uint8_t* d_scalars, uint64_t n, uint32_t* d_first_bad, cudaStream_t st) {
+    if (!n) return;
+    k_fb_validate<<<blocks_for(n, 256), 256, 0, st>>>(d_scalars, n, d_first_bad);
+    DV_LAUNCH();
+}
+
+uint64_t fixed_base_table_entries() { return (uint64_t)FB_WINDOWS * FB_HALF; }
+
 void fixed_base_launch(FixedBaseTables& tabs, const uint8_t* d_scalars, uint64_t n, int g2, uint8_t* d_out,
                        uint32_t* d_first_bad, cudaStream_t st) {
     if (!n) return;

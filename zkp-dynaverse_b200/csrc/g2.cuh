@@ -46,5 +46,9 @@ struct FixedBaseTables {
 // scalars: device canonical; out: device canonical affine bytes (64 / 128 each).
 void fixed_base_launch(FixedBaseTables& tabs, const uint8_t* d_scalars, uint64_t n, int g2, uint8_t* d_out,
                        uint32_t* d_first_bad, cudaStream_t stream);
+// The smallest index of a non-canonical scalar into d_first_bad (atomicMin).
+void fixed_base_validate(const uint8_t* d_scalars, uint64_t n, uint32_t* d_first_bad, cudaStream_t stream);
+// Entries of one fixed-base table (16 windows of 2^15 multiples).
+uint64_t fixed_base_table_entries();
 
 }  // namespace dv
