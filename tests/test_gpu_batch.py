@@ -8,6 +8,8 @@ The reference batches MSMs with next-pow2 padding and 64-set groups
 runs NTTs one call per vector (icicle.rs:429-456); its tests compare every
 batched result with arkworks (crates/gpu/tests/icicle_backend.rs:131-189).
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -107,7 +109,7 @@ def _plan_sizes(seed, nbases, count):
     return sizes
 
 
-def test_batch_plan_matches_oracle_and_replays(backend, oracle):
+def test_batch_plan_matches_oracle_and_replays(backend, oracle, dv):
     nbases = 4096
     pts, _ = oracle.srs_g1(5150, nbases)
     sizes = _plan_sizes(5151, nbases, 40)
@@ -130,6 +132,28 @@ def test_batch_plan_matches_oracle_and_replays(backend, oracle):
             assert msm[3] == bytes(64)
             for j, part in enumerate(_split(ntt, logs)):
                 assert part == oracle.ntt(vals[j], KINDS[kinds[j]]), f"rep {rep} NTT {j}"
+        # host-buffer runs check every input before writing any output: a bad
+        # scalar or NTT value fails the call, the output buffers stay as they
+        # were, and the plan runs again afterwards
+        total = sum(sizes)
+        nvals = sum(1 << L for L in logs)
+        lib = dv.lib()
+        for bad_scalar in (True, False):
+            sc = bytearray(b"".join(scs))
+            vv = bytearray(b"".join(vals))
+            if bad_scalar:
+                sc[32 * (total - 5):32 * (total - 4)] = b"\xff" * 32
+            else:
+                vv[32 * (nvals - 3):32 * (nvals - 2)] = b"\xff" * 32
+            mo = ctypes.create_string_buffer(b"\xab" * (64 * len(sizes)), 64 * len(sizes))
+            no = ctypes.create_string_buffer(b"\xcd" * (32 * nvals), 32 * nvals)
+            err = ctypes.create_string_buffer(256)
+            rc = lib.dvgpu_batch_plan_run(backend.handle, plan, bytes(sc), bytes(vv), mo, no, err, 256)
+            assert rc == -1 and b"non-canonical" in err.value
+            assert mo.raw == b"\xab" * (64 * len(sizes)) and no.raw == b"\xcd" * (32 * nvals)
+        msm, ntt = backend.batch_plan_run(plan, b"".join(scs), b"".join(vals), len(sizes))
+        assert msm[0] == oracle.msm_g1(pts[:64 * sizes[0]], scs[0])
+        assert _split(ntt, logs)[1] == oracle.ntt(vals[1], KINDS[kinds[1]])
         backend.batch_plan_destroy(plan)
     finally:
         backend.release_bases(h)

@@ -8,6 +8,7 @@
 #include "abi_util.hpp"
 #include "backend.hpp"
 #include "batch.hpp"
+#include "g2.cuh"
 
 namespace dv {
 
@@ -48,6 +49,11 @@ void enqueue_class(BatchPlan& p, BatchClass& k, cudaStream_t st) {
 }
 
 // Enqueues the whole plan on p.stream (NTTs forked onto p.side).
+void enqueue_msms(BatchPlan& p) {
+    DV_CUDA(cudaMemsetAsync(p.err.view<uint32_t>(), 0xff, sizeof(uint32_t), p.stream));
+    for (auto& k : p.classes) enqueue_class(p, *k, p.stream);
+}
+
 void enqueue_all(BatchPlan& p) {
     const bool ntts = p.ntt.count > 0;
     if (ntts) {
@@ -56,8 +62,7 @@ void enqueue_all(BatchPlan& p) {
         ntt_batch_enqueue(p.ntt, p.side);
         DV_CUDA(cudaEventRecord(p.join, p.side));
     }
-    DV_CUDA(cudaMemsetAsync(p.err.view<uint32_t>(), 0xff, sizeof(uint32_t), p.stream));
-    for (auto& k : p.classes) enqueue_class(p, *k, p.stream);
+    enqueue_msms(p);
     if (ntts) DV_CUDA(cudaStreamWaitEvent(p.stream, p.join, 0));
 }
 
@@ -86,9 +91,17 @@ double time_class(BatchPlan& p, BatchClass& k, int reps) {
 BatchPlan::~BatchPlan() {
     if (stream) cudaStreamSynchronize(stream);
     if (side) cudaStreamSynchronize(side);
+    if (copy) cudaStreamSynchronize(copy);
     if (last && last != stream && last != side) cudaStreamSynchronize(last);
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    if (exec_msm) cudaGraphExecDestroy(exec_msm);
+    if (graph_msm) cudaGraphDestroy(graph_msm);
+    if (exec_ntt) cudaGraphExecDestroy(exec_ntt);
+    if (graph_ntt) cudaGraphDestroy(graph_ntt);
+    if (ntt_ready) cudaEventDestroy(ntt_ready);
+    if (ntt_done) cudaEventDestroy(ntt_done);
+    if (copy) cudaStreamDestroy(copy);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
     if (side) cudaStreamDestroy(side);
@@ -106,6 +119,9 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
     DV_CUDA(cudaStreamCreateWithFlags(&p.side, cudaStreamNonBlocking));
     DV_CUDA(cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming));
     DV_CUDA(cudaEventCreateWithFlags(&p.join, cudaEventDisableTiming));
+    DV_CUDA(cudaStreamCreateWithFlags(&p.copy, cudaStreamNonBlocking));
+    DV_CUDA(cudaEventCreateWithFlags(&p.ntt_ready, cudaEventDisableTiming));
+    DV_CUDA(cudaEventCreateWithFlags(&p.ntt_done, cudaEventDisableTiming));
 
     // ---- MSM sets: offsets in the scalar array, size classes
     p.msm_sizes = msm_sizes;
@@ -230,6 +246,33 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
         DV_CUDA(cudaGraphNodeGetType(node, &type));
         if (type == cudaGraphNodeTypeKernel) ++p.graph_kernels;
     }
+    // the two halves alone, for host-buffer runs
+    if (!p.classes.empty()) {
+        DV_CUDA(cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueue_msms(p);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(p.stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        DV_CUDA(cudaStreamEndCapture(p.stream, &p.graph_msm));
+        DV_CUDA(cudaGraphInstantiate(&p.exec_msm, p.graph_msm, 0));
+    }
+    if (p.ntt.count) {
+        DV_CUDA(cudaStreamBeginCapture(p.side, cudaStreamCaptureModeThreadLocal));
+        try {
+            ntt_batch_enqueue(p.ntt, p.side);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(p.side, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        DV_CUDA(cudaStreamEndCapture(p.side, &p.graph_ntt));
+        DV_CUDA(cudaGraphInstantiate(&p.exec_ntt, p.graph_ntt, 0));
+    }
     log += ",\"graph_nodes\":" + std::to_string(p.graph_nodes) +
            ",\"graph_kernels\":" + std::to_string(p.graph_kernels) + "}";
     p.last = p.stream;
@@ -239,6 +282,48 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
 void batch_plan_launch(BatchPlan& p, cudaStream_t st) {
     p.last = st ? st : p.stream;
     DV_CUDA(cudaGraphLaunch(p.exec, p.last));
+}
+
+void batch_plan_run_host(BatchPlan& p, const uint8_t* scalars, const uint8_t* ntt_values, uint8_t* msm_results,
+                         uint8_t* ntt_results) {
+    const bool msms = p.total_scalars > 0, ntts = p.ntt_elements > 0;
+    if (msms) {
+        DV_CUDA(cudaMemcpyAsync(p.scalars.view<uint8_t>(), scalars, p.total_scalars * 32, cudaMemcpyHostToDevice,
+                                p.stream));
+        DV_CUDA(cudaMemsetAsync(p.err.view<uint32_t>(), 0xff, sizeof(uint32_t), p.stream));
+        fixed_base_validate(p.scalars.view<uint8_t>(), p.total_scalars, p.err.view<uint32_t>(), p.stream);
+        uint32_t bad = 0;
+        DV_CUDA(cudaMemcpyAsync(&bad, p.err.view<uint32_t>(), sizeof(uint32_t), cudaMemcpyDeviceToHost, p.stream));
+        DV_CUDA(cudaStreamSynchronize(p.stream));
+        if (bad != 0xffffffffu) throw InvalidArgument("non-canonical scalar at index " + std::to_string(bad));
+        DV_CUDA(cudaGraphLaunch(p.exec_msm, p.stream));
+    }
+    if (ntts) {
+        DV_CUDA(cudaMemcpyAsync(p.ntt_in.view<uint8_t>(), ntt_values, p.ntt_elements * 32, cudaMemcpyHostToDevice,
+                                p.copy));
+        DV_CUDA(cudaEventRecord(p.ntt_ready, p.copy));
+        DV_CUDA(cudaStreamWaitEvent(p.side, p.ntt_ready, 0));
+        DV_CUDA(cudaGraphLaunch(p.exec_ntt, p.side));
+        DV_CUDA(cudaEventRecord(p.ntt_done, p.side));
+        try {
+            ntt_batch_check(p.ntt, p.side);  // waits for the NTTs only
+        } catch (...) {
+            cudaStreamSynchronize(p.stream);  // leave the plan idle
+            throw;
+        }
+        DV_CUDA(cudaMemcpyAsync(ntt_results, p.ntt_out.view<uint8_t>(), p.ntt_elements * 32, cudaMemcpyDeviceToHost,
+                                p.copy));
+    }
+    if (msms) {
+        DV_CUDA(cudaStreamSynchronize(p.stream));
+        uint32_t bad = 0;
+        DV_CUDA(cudaMemcpy(&bad, p.err.view<uint32_t>(), sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        if (bad != 0xffffffffu) throw InvalidArgument("non-canonical scalar at index " + std::to_string(bad));
+        DV_CUDA(cudaMemcpyAsync(msm_results, p.msm_out.view<uint8_t>(), p.msm_sizes.size() * 64,
+                                cudaMemcpyDeviceToHost, p.copy));
+    }
+    DV_CUDA(cudaStreamSynchronize(p.copy));
+    p.last = p.stream;
 }
 
 void batch_plan_check(BatchPlan& p) {
@@ -385,21 +470,7 @@ extern "C" int dvgpu_batch_plan_run(void* opaque, uint64_t handle, const uint8_t
         BatchPlan& p = plan_of(b, handle);
         require((!p.total_scalars || (scalars && msm_results)) && (!p.ntt_elements || (ntt_values && ntt_results)),
                 "invalid batch plan buffers");
-        if (p.total_scalars)
-            DV_CUDA(cudaMemcpyAsync(p.scalars.view<uint8_t>(), scalars, p.total_scalars * 32, cudaMemcpyHostToDevice,
-                                    p.stream));
-        if (p.ntt_elements)
-            DV_CUDA(cudaMemcpyAsync(p.ntt_in.view<uint8_t>(), ntt_values, p.ntt_elements * 32,
-                                    cudaMemcpyHostToDevice, p.stream));
-        batch_plan_launch(p, p.stream);
-        batch_plan_check(p);
-        if (p.total_scalars)
-            DV_CUDA(cudaMemcpyAsync(msm_results, p.msm_out.view<uint8_t>(), p.msm_sizes.size() * 64,
-                                    cudaMemcpyDeviceToHost, p.stream));
-        if (p.ntt_elements)
-            DV_CUDA(cudaMemcpyAsync(ntt_results, p.ntt_out.view<uint8_t>(), p.ntt_elements * 32,
-                                    cudaMemcpyDeviceToHost, p.stream));
-        DV_CUDA(cudaStreamSynchronize(p.stream));
+        batch_plan_run_host(p, scalars, ntt_values, msm_results, ntt_results);
     });
 }
 

@@ -43,6 +43,12 @@ struct BatchPlan {
     cudaEvent_t fork = nullptr, join = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // host-buffer runs: the MSM and NTT halves as separate graphs, a copy
+    // stream and the events that order them
+    cudaStream_t copy = nullptr;
+    cudaEvent_t ntt_ready = nullptr, ntt_done = nullptr;
+    cudaGraph_t graph_msm = nullptr, graph_ntt = nullptr;
+    cudaGraphExec_t exec_msm = nullptr, exec_ntt = nullptr;
     size_t graph_nodes = 0, graph_kernels = 0;
 
     std::vector<uint64_t> msm_sizes, scalar_off;
@@ -74,5 +80,10 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
 void batch_plan_launch(BatchPlan& plan, cudaStream_t stream);
 // Waits for the last replay; throws InvalidArgument for invalid inputs.
 void batch_plan_check(BatchPlan& plan);
+// One run from host buffers: scalars up and checked first (no output is
+// written on a bad input), the MSM graph on them while the NTT inputs go up,
+// the NTT graph beside the MSMs, its outputs down while the MSMs run.
+void batch_plan_run_host(BatchPlan& plan, const uint8_t* scalars, const uint8_t* ntt_values, uint8_t* msm_results,
+                         uint8_t* ntt_results);
 
 }  // namespace dv
