@@ -1314,6 +1314,15 @@ def run_reference(args, rank, world):
 
         metric = BatchOp(args).metric
         sample = "batch estimates"
+    elif op == "g2check":
+        gop = G2CheckOp(args)
+        k = min(n, 1 << 13)
+        wire = (oracle.fixed_base_g2(oracle.uniform_fr(2900, k // 2), threads=threads) +
+                oracle.g2_twist_points(2901, k - k // 2))
+        fn = lambda: oracle.g2_check(wire, gop.alg, threads=threads)
+        metric = gop.metric
+        sample = f"{k}-point checks (half [s]G2, half twist points) on {threads} threads, scaled to 2^{args.log_n}"
+        g2check_scale = n / k
     elif op == "pairing":
         pop = PairingOp(args)
         pop.setup(None, None, None, 0)
@@ -1337,6 +1346,8 @@ def run_reference(args, rank, world):
         fn = lambda: oracle.fixed_base_g1(sc, threads=threads)
         metric = f"fixed-base G1 2^{args.log_n} ms"
         sample = f"full 2^{args.log_n}-point fixed-base generations"
+    ours = make_op(args)  # the GPU arm's metric and workload, for the same line shape
+    metric = ours.metric
     t0 = time.perf_counter()
     fn()
     first = (time.perf_counter() - t0) * 1e3
@@ -1354,6 +1365,8 @@ def run_reference(args, rank, world):
         value *= ecntt_scale
     if op == "pairing":
         value *= pairing_scale
+    if op == "g2check":
+        value *= g2check_scale
     higher = False
     ms_step = value
     if op == "serve":
@@ -1366,7 +1379,7 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": higher,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 limbs (Fq/Fr, exact)", "data": "synthetic",
-        "config": {"workload": metric, "parallelism": "host threads"},
+        "config": {"workload": ours.workload, "op": op, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
                          "sample": f"{steps} {sample} (after 1 warm-up)"},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
