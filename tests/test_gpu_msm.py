@@ -6,6 +6,8 @@ and crates/gpu/tests/sparse_msm_backend.rs / batch_backend.rs.  The
 expected values come from the CPU oracle and the golden vectors; results
 must be byte-identical.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -284,3 +286,29 @@ def test_precomputed_resident_msm_matches_oracle(backend, oracle):
         assert backend.msm_resident(h2, d_sc2.data_ptr(), 2000, g2=True) == oracle.msm_g2(pts2, scs2)
     finally:
         backend.release_bases(h2)
+
+
+def test_resident_host_msm(backend, oracle, dv):
+    """Host-scalar MSMs over registered bases with a precomputed table
+    (dvgpu_bn254_msm_resident_host, the e2e call of the headline bench): the
+    same result as the oracle and the plain call; a bad scalar late in the
+    call is reported with its index and leaves the result untouched."""
+    n = (1 << 18) + 3
+    pts, _ = oracle.srs_g1(6400, n, threads=16)
+    sc = oracle.uniform_fr(6401, n)
+    h = backend.register_bases(pts)
+    try:
+        backend.precompute_bases(h, 0)
+        expect = oracle.msm_g1(pts, sc, threads=16)
+        assert backend.msm_resident_host(h, sc) == expect == backend.msm(pts, sc)
+        m = (1 << 18) - 5
+        assert backend.msm_resident_host(h, sc[:32 * m]) == oracle.msm_g1(pts[:64 * m], sc[:32 * m], threads=16)
+        bad = bytearray(sc)
+        bad[32 * (n - 7):32 * (n - 6)] = b"\xff" * 32
+        out = ctypes.create_string_buffer(b"\x5a" * 64, 64)
+        err = ctypes.create_string_buffer(256)
+        rc = dv.lib().dvgpu_bn254_msm_resident_host(backend.handle, h, bytes(bad), n, out, err, 256)
+        assert rc == -1 and str(n - 7).encode() in err.value and out.raw == b"\x5a" * 64
+        assert backend.msm_resident_host(h, sc) == expect  # owner still healthy
+    finally:
+        backend.release_bases(h)

@@ -689,6 +689,12 @@ class DvgpuBackend:
         raw = out.raw
         return [raw[i * G1_BYTES:(i + 1) * G1_BYTES] for i in range(count)]
 
+    def msm_resident_host(self, handle: int, scalars: bytes, g2=False) -> bytes:
+        """MSM over registered bases with host scalars (dvgpu_bn254_msm_resident_host)."""
+        out = ctypes.create_string_buffer(G2_BYTES if g2 else G1_BYTES)
+        self._call("dvgpu_bn254_msm_resident_host", handle, _ptr(scalars), len(scalars) // FR_BYTES, out)
+        return out.raw
+
     def msm_resident(self, handle: int, d_scalars: int, n: int, stream=None, g2=False) -> bytes:
         out = ctypes.create_string_buffer(G2_BYTES if g2 else G1_BYTES)
         self._call("dvgpu_bn254_msm_resident", handle, d_scalars, n, out, stream)
