@@ -206,9 +206,9 @@ def test_sparse_direct_small_supports(backend, oracle, dv):
             d_idx = torch.from_numpy(idx_all.view(np.int64)).cuda()
             d_vals = torch.frombuffer(bytearray(vals_all), dtype=torch.uint8).cuda()
             assert backend.sparse_msm_device(h, d_idx.data_ptr(), d_vals.data_ptr(), offs) == expect, c
-        # just below and above the direct path's limit (c = 8: 32 windows, 2^14 terms)
+        # just below and above the direct path's limit (c = 8: 32 windows, 2^16 terms)
         backend.precompute_bases(h, 8)
-        for k in (512, 513):
+        for k in (512, 2048, 2049):
             idx = rng.choice(n, size=k, replace=False).astype(np.uint64)
             vals = oracle.uniform_fr(1300 + k, k)
             assert backend.sparse_msm_resident(h, idx, vals, [0, k]) == [oracle.sparse_msm_g1(bases, idx, vals)]

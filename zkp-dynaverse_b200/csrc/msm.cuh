@@ -93,8 +93,11 @@ struct MsmPrecomp {
 void msm_sparse_direct(MsmWorkspace& ws, const MsmPrecomp<Fq>& pre, uint64_t nbases, const uint64_t* d_idx,
                        const uint32_t* d_vals, const uint32_t* offs, uint32_t count, uint8_t* host_out,
                        cudaStream_t stream);
-// Terms (entries x windows) up to which sparse calls take the direct path.
-constexpr uint64_t SPARSE_DIRECT_MAX_TERMS = 1u << 14;
+// Terms (entries x windows) up to which sparse calls take the direct path:
+// with a c = 8 table (32 windows) the direct path wins up to 2048 entries
+// (k = 1024: 0.29 against 0.73 ms; 2048: 0.48 against 0.71 ms) and the
+// bucket pipeline from 3072 (0.46 against 0.67 ms).
+constexpr uint64_t SPARSE_DIRECT_MAX_TERMS = 1u << 16;
 
 template <class F>
 void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scalars, const uint32_t* set_offsets,
