@@ -63,8 +63,13 @@ int dvgpu_bn254_msm_batch(void* backend, const uint8_t* points, const uint8_t* s
                           uint8_t* results, char* error, size_t error_capacity);
 
 /* ---- NTT (native/include/dynaverse_gpu.h:39-45) ------------------------ */
-/* root: the canonical primitive 2^20-th root of unity of the CPU reference;
- * checked to have order exactly 2^20.  length: power of two. */
+/* root: the canonical primitive 2^20-th root of unity of the CPU reference
+ * (Fr::get_root_of_unity(2^20), icicle.rs:442-443); checked to have order
+ * exactly 2^20 and to equal that root (the reference fixes whichever root of
+ * order 2^20 an owner sees first; this library fixes arkworks' one, since
+ * another root defines a different, conjugate, transform).  length: a power
+ * of two up to 2^20, the longest transform such a root defines; longer ones
+ * go through dvgpu_bn254_ntt_ex. */
 int dvgpu_bn254_ntt(void* backend, const uint8_t* values, size_t length, int inverse, const uint8_t* root,
                     uint8_t* result, char* error, size_t error_capacity);
 

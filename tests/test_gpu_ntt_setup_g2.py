@@ -48,6 +48,10 @@ def test_ntt_reference_root_abi(backend, golden, oracle):
     bad_root = (5).to_bytes(32, "little")
     with pytest.raises(Exception):
         backend.ntt_with_root(vals, False, bad_root)
+    # a root of order 2^20 defines no longer transform: the reference's cap
+    with pytest.raises(Exception):
+        backend.ntt_with_root(bytes(32 << 21), False, root)
+    assert backend.ntt_with_root(vals, False, root) == oracle.ntt(vals, "forward")  # owner still healthy
 
 
 def test_ntt_roundtrip_large_and_invalid_lengths(backend, oracle, dv):

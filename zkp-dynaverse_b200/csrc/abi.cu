@@ -604,9 +604,12 @@ void ntt_host(Backend& b, const uint8_t* values, size_t length, int kind, uint8_
 extern "C" int dvgpu_bn254_ntt(void* opaque, const uint8_t* values, size_t length, int inverse, const uint8_t* root,
                                uint8_t* result, char* error, size_t cap) {
     return guarded(opaque, error, cap, [&](Backend& b) {
-        require(values && result && root && length && length <= DVGPU_MAX_NTT_SIZE && !(length & (length - 1)) &&
+        // The root passed here has order 2^20, which defines transforms of at
+        // most 2^20 elements (the reference's cap, icicle.rs:61-63); longer
+        // ones go through dvgpu_bn254_ntt_ex / _device.
+        require(values && result && root && length && length <= (1u << 20) && !(length & (length - 1)) &&
                     (inverse == 0 || inverse == 1),
-                "invalid NTT buffers, direction or length");
+                "invalid NTT buffers, direction or length (1..2^20, a power of two)");
         require(root_has_order_2_20(root), "NTT root must have order 2^20");
         // Orientation is pinned to the CPU reference's root; another root of
         // the same order would define a different (conjugate) transform.

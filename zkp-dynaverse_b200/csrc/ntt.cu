@@ -1,6 +1,7 @@
 // Fr NTT kernels and launch sequence (see ntt.cuh).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "curve.cuh"
@@ -648,16 +649,22 @@ static __device__ __align__(256) Fr noalloc_scratch[NA_TOTAL];  // about 3.1 MB 
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 Fr* noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+cudaError_t noalloc_status[NOALLOC_MAX_DEVICES] = {};
+std::once_flag noalloc_once[NOALLOC_MAX_DEVICES];
 
-// Device address of the scratch array on the current device (looked up once
-// per device; host code must not use the symbol itself as a pointer).
+// Device address of the scratch array on the current device, looked up once
+// per device (std::call_once: host threads making their first call on one
+// device at the same time wait for a single lookup).  Host code must not use
+// the symbol itself as a pointer.  The cached address belongs to the
+// device's primary context: it is not valid after cudaDeviceReset.
 Fr* noalloc_scratch_on(int dev) {
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) throw InvalidArgument("device ordinal out of range");
-    if (!noalloc_ptr[dev]) {
+    std::call_once(noalloc_once[dev], [dev] {
         void* p = nullptr;
-        DV_CUDA(cudaGetSymbolAddress(&p, noalloc_scratch));
-        noalloc_ptr[dev] = static_cast<Fr*>(p);
-    }
+        noalloc_status[dev] = cudaGetSymbolAddress(&p, noalloc_scratch);
+        if (noalloc_status[dev] == cudaSuccess) noalloc_ptr[dev] = static_cast<Fr*>(p);
+    });
+    DV_CUDA(noalloc_status[dev]);
     return noalloc_ptr[dev];
 }
 

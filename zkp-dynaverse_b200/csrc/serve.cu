@@ -80,10 +80,21 @@ dvh::XYZZ<dvh::Fq> xyzz_of(const uint8_t* p) {
 constexpr int SERVE_C = 8;
 constexpr int SERVE_W = (255 + SERVE_C - 1) / SERVE_C;  // 32 windows
 
+// Request of update entry e: the largest r with req_off[r] <= e.
+DV_INL uint32_t serve_request_of(uint32_t e, const uint32_t* __restrict__ req_off, uint32_t count) {
+    uint32_t lo = 0, hi = count;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (req_off[mid] <= e) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 // One thread per (update entry, window): find the entry's request, gather
 // the window multiple 2^(c w) G_i from the session's table; the window-0
-// thread also replaces the resident value by the new one and emits the
-// delta new - old (mod r) as the MSM scalar.
+// thread also emits the delta new - old (mod r) as the MSM scalar.  The
+// resident values are not touched here: k_serve_commit writes them once the
+// batch's MSM has completed.
 __global__ void k_serve_prepare(uint32_t total, const uint32_t* __restrict__ req_off, uint32_t count,
                                 const G1A* const* __restrict__ tables, uint8_t* const* __restrict__ values,
                                 const uint32_t* __restrict__ idx, const uint8_t* __restrict__ new_vals,
@@ -91,21 +102,27 @@ __global__ void k_serve_prepare(uint32_t total, const uint32_t* __restrict__ req
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (uint64_t)total * SERVE_W) return;
     const uint32_t e = (uint32_t)(t / SERVE_W), w = (uint32_t)(t % SERVE_W);
-    uint32_t lo = 0, hi = count;  // largest r with req_off[r] <= e
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (req_off[mid] <= e) lo = mid; else hi = mid;
-    }
+    const uint32_t r = serve_request_of(e, req_off, count);
     const uint32_t i = idx[e];
-    gathered[t] = tables[lo][(uint64_t)i * SERVE_W + w];
+    gathered[t] = tables[r][(uint64_t)i * SERVE_W + w];
     if (w) return;
-    uint8_t* slot = values[lo] + 32ull * i;
     Fr oldv, newv;
-    load_words(slot, oldv.v);
+    load_words(values[r] + 32ull * i, oldv.v);
     load_words(new_vals + 32ull * e, newv.v);
     const Fr d = Fr::sub(newv, oldv);  // canonical operands: canonical difference
     store_words(deltas + 32ull * e, d.v);
-    store_words(slot, newv.v);
+}
+
+// After a successful batch: the resident values take the new ones.
+__global__ void k_serve_commit(uint32_t total, const uint32_t* __restrict__ req_off, uint32_t count,
+                               uint8_t* const* __restrict__ values, const uint32_t* __restrict__ idx,
+                               const uint8_t* __restrict__ new_vals) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const uint32_t r = serve_request_of(e, req_off, count);
+    uint32_t w[8];
+    load_words(new_vals + 32ull * e, w);
+    store_words(values[r] + 32ull * idx[e], w);
 }
 
 struct Session {
@@ -196,16 +213,8 @@ public:
         r.session = session;
         r.idx.resize(k);
         r.vals.assign(vals, vals + 32 * k);
-        uint64_t n = 0;
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            auto it = sessions_.find(session);
-            if (it == sessions_.end()) throw InvalidArgument("unknown session");
-            n = it->second->n;
-        }
-        if (k == 0 || k > n) throw InvalidArgument("update support must hold 1..n indices");
         for (size_t j = 0; j < k; ++j) {
-            if (idx[j] >= n) throw InvalidArgument("update index out of range");
+            if (idx[j] > 0xffffffffull) throw InvalidArgument("update index out of range");
             if (!fr_canonical(vals + 32 * j)) throw InvalidArgument("non-canonical update value");
             r.idx[j] = (uint32_t)idx[j];
         }
@@ -213,7 +222,15 @@ public:
         std::sort(sorted.begin(), sorted.end());
         if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
             throw InvalidArgument("update indices must be distinct");
+        // The session's existence and size are checked under the same lock
+        // that queues the request, so a concurrent close_session either sees
+        // the pending request (and refuses) or runs before this check.
         std::lock_guard<std::mutex> lk(mu_);
+        auto it = sessions_.find(session);
+        if (it == sessions_.end()) throw InvalidArgument("unknown session");
+        const uint64_t n = it->second->n;
+        if (k == 0 || k > n) throw InvalidArgument("update support must hold 1..n indices");
+        if (!sorted.empty() && sorted.back() >= n) throw InvalidArgument("update index out of range");
         r.ticket = next_ticket_++;
         outcomes_[r.ticket];
         queue_.push_back(std::move(r));
@@ -297,7 +314,23 @@ private:
                 it = queue_.erase(it);
             }
             std::vector<Session*> sess;
-            for (const Request& r : batch) sess.push_back(sessions_.at(r.session).get());
+            for (size_t r = 0; r < batch.size();) {
+                auto it = sessions_.find(batch[r].session);
+                if (it != sessions_.end()) {
+                    sess.push_back(it->second.get());
+                    ++r;
+                    continue;
+                }
+                // cannot happen while close_session refuses sessions with
+                // pending requests; fail the ticket rather than the process
+                Outcome& o = outcomes_[batch[r].ticket];
+                o.status = -1;
+                o.error = "unknown session";
+                o.ready = true;
+                batch.erase(batch.begin() + r);
+                done_cv_.notify_all();
+            }
+            if (batch.empty()) continue;
             lk.unlock();
             int status = 0;
             std::string error;
@@ -396,6 +429,10 @@ private:
         DV_CUDA(cudaMemcpyAsync(deltas_out, ws_.windows.view<XYZZ<Fq>>(), sizeof(XYZZ<Fq>) * count,
                                 cudaMemcpyDeviceToHost, stream_));
         DV_CUDA(cudaStreamSynchronize(stream_));
+        // Every fallible step is done: publish the new values.  Later
+        // batches run on the same stream, so they read the committed ones.
+        k_serve_commit<<<(total + 127) / 128, 128, 0, stream_>>>(total, d_off, count, d_vals, d_idx, d_val);
+        DV_LAUNCH();
     }
 
     int device_ = 0;
