@@ -595,6 +595,91 @@ int dvgpu_serve_wait(void* server, uint64_t ticket, uint8_t* commitment, DvgpuSe
 int dvgpu_serve_set_max_batch(void* server, uint32_t max_batch);
 int dvgpu_serve_stats(void* server, DvgpuServeStats* out);
 
+/* ---------------------------------------------------------------- Dynaverse update proofs
+ * The prover of crates/protocol/src/dynaverse: DynaverseParams (setup from
+ * the two trapdoors, dynaverse.rs:104-147 over srs.rs:147-197),
+ * UpdateSession (dynaverse/session.rs:17-142: start_update_session,
+ * update_with_public_inputs, including the synchronous re-anchor of
+ * update_proof_backend, dynaverse.rs:379-470), and
+ * DynaverseVerifyingKey::verify (dynaverse.rs:978-1016), with the whole
+ * proof composed on the device.  In the reference this is Rust host code
+ * that calls OperatorBackend once per MSM (about 70 calls per sparse
+ * update); these entry points replace that loop.
+ *
+ * Values are 32-byte canonical little-endian Fr; a witness holds 6n wires,
+ * an instance n public inputs (ToyCircuit, toy_circuit.rs).  A proof is
+ * DVGPU_DYNAVERSE_PROOF_BYTES: the AnchorProof fields (3968 B), the
+ * DeltaProof fields (5312 B, zero when absent), then u64 has_delta,
+ * anchor_generation, generation (little-endian); every field in the
+ * declaration order of types.rs:64-172, G1 64 B and G2 128 B in the wire
+ * format (infinity all zero).
+ *
+ * An engine owns a worker thread, a stream and workspaces on the calling
+ * thread's current device.  Parameters and sessions are admitted against
+ * its HBM budget (-1 when they do not fit).  dvgpu_dynaverse_submit queues
+ * an update (witness edits and public-input edits, session.rs:39-41) and
+ * returns a ticket; the worker merges the pending updates of up to
+ * max_batch sessions (one per session per batch, in submission order) into
+ * shared launches and verifies every proof on the device before it is
+ * published; requests arriving meanwhile form the next batch.
+ * dvgpu_dynaverse_wait returns the proof, or -1 with the reference's error
+ * text for an invalid update (the session is then unchanged).
+ * dvgpu_dynaverse_update is submit + wait (with max_batch = 1, the per-call
+ * form).  n: a power of two in 1..2^17. */
+#define DVGPU_DYNAVERSE_PROOF_BYTES 9304
+typedef struct DvgpuDynaverseParamsInfo {
+    uint64_t n, m, rebuild_interval, resident_bytes;
+    uint8_t g1_generator[64];
+    uint8_t multiplication_vanishing_g1[64];
+    /* the verifying key's G2 points: u, [x^m - 1], x, 1/m, [y^m - 1], y^m,
+     * x^m, x^2, [1], z_in of the six slices, x - y, x - y^(m/n), I_x, x^n - 1 */
+    uint8_t vk_g2[19][128];
+} DvgpuDynaverseParamsInfo;
+typedef struct DvgpuDynaverseResult {
+    uint64_t submit_ns, start_ns, done_ns; /* steady-clock nanoseconds */
+    uint32_t batch_requests, batch_id;
+    uint32_t rebuilt; /* 1: the update re-anchored (delta reached ceil(sqrt(n))) */
+    uint32_t pad;
+} DvgpuDynaverseResult;
+typedef struct DvgpuDynaverseStats {
+    uint64_t requests, batches, sessions, resident_bytes, budget_bytes;
+    uint64_t max_batch, largest_batch, busy_ns, pending;
+    uint64_t sparse_proofs, rebuilds, launches;
+} DvgpuDynaverseStats;
+int dvgpu_dynaverse_create(uint64_t hbm_budget_bytes, uint32_t max_batch, void** engine, char* error,
+                           size_t error_capacity);
+void dvgpu_dynaverse_destroy(void* engine);
+/* SRS, window tables and verifying key of ToyCircuit(n) from the trapdoors
+ * tau_x, tau_y (canonical Fr; rejected as in srs.rs:158-178). */
+int dvgpu_dynaverse_params_create(void* engine, size_t n, const uint8_t* tau_x, const uint8_t* tau_y,
+                                  uint64_t* params, char* error, size_t error_capacity);
+int dvgpu_dynaverse_params_destroy(void* engine, uint64_t params, char* error, size_t error_capacity);
+int dvgpu_dynaverse_params_info(void* engine, uint64_t params, DvgpuDynaverseParamsInfo* info, char* error,
+                                size_t error_capacity);
+/* start_update_session: the anchor proof of (public_inputs, witness),
+ * verified, written to proof. */
+int dvgpu_dynaverse_session_open(void* engine, uint64_t params, const uint8_t* public_inputs, const uint8_t* witness,
+                                 uint64_t* session, uint8_t* proof, char* error, size_t error_capacity);
+int dvgpu_dynaverse_session_close(void* engine, uint64_t session, char* error, size_t error_capacity);
+/* The session's current witness (6n), instance (n), proof and anchor
+ * distance (UpdateSession::current_witness / current_instance / proof /
+ * anchor_distance); any output may be NULL. */
+int dvgpu_dynaverse_session_state(void* engine, uint64_t session, uint8_t* witness, uint8_t* public_inputs,
+                                  uint8_t* proof, uint64_t* anchor_distance, char* error, size_t error_capacity);
+int dvgpu_dynaverse_submit(void* engine, uint64_t session, const uint64_t* indices, const uint8_t* values,
+                           size_t count, const uint64_t* public_indices, const uint8_t* public_values,
+                           size_t public_count, uint64_t* ticket, char* error, size_t error_capacity);
+int dvgpu_dynaverse_wait(void* engine, uint64_t ticket, uint8_t* proof, DvgpuDynaverseResult* result, char* error,
+                         size_t error_capacity);
+int dvgpu_dynaverse_update(void* engine, uint64_t session, const uint64_t* indices, const uint8_t* values,
+                           size_t count, const uint64_t* public_indices, const uint8_t* public_values,
+                           size_t public_count, uint8_t* proof, char* error, size_t error_capacity);
+/* accepted = 1 iff the proof parses and passes every check of verify. */
+int dvgpu_dynaverse_verify(void* engine, uint64_t params, const uint8_t* public_inputs, const uint8_t* proof,
+                           uint8_t* accepted, char* error, size_t error_capacity);
+int dvgpu_dynaverse_set_max_batch(void* engine, uint32_t max_batch);
+int dvgpu_dynaverse_stats(void* engine, DvgpuDynaverseStats* out);
+
 #ifdef __cplusplus
 }
 #endif

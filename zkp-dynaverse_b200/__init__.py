@@ -148,6 +148,24 @@ class ResidentProfile(ctypes.Structure):
         "d2d_bytes")]
 
 
+class DynaverseParamsInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("m", ctypes.c_uint64), ("rebuild_interval", ctypes.c_uint64),
+                ("resident_bytes", ctypes.c_uint64), ("g1_generator", ctypes.c_uint8 * 64),
+                ("multiplication_vanishing_g1", ctypes.c_uint8 * 64), ("vk_g2", (ctypes.c_uint8 * 128) * 19)]
+
+
+class DynaverseResult(ctypes.Structure):
+    _fields_ = [("submit_ns", ctypes.c_uint64), ("start_ns", ctypes.c_uint64), ("done_ns", ctypes.c_uint64),
+                ("batch_requests", ctypes.c_uint32), ("batch_id", ctypes.c_uint32), ("rebuilt", ctypes.c_uint32),
+                ("pad", ctypes.c_uint32)]
+
+
+class DynaverseStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in ("requests", "batches", "sessions", "resident_bytes", "budget_bytes",
+                                              "max_batch", "largest_batch", "busy_ns", "pending", "sparse_proofs",
+                                              "rebuilds", "launches")]
+
+
 # (name, restype, argtypes)
 _P = ctypes.c_void_p
 _B = ctypes.c_char_p
@@ -252,6 +270,23 @@ SIGNATURES = [
     ("dvgpu_serve_wait", ctypes.c_int, [_P, ctypes.c_uint64, _B, ctypes.POINTER(ServeResult)] + _E),
     ("dvgpu_serve_set_max_batch", ctypes.c_int, [_P, ctypes.c_uint32]),
     ("dvgpu_serve_stats", ctypes.c_int, [_P, ctypes.POINTER(ServeStats)]),
+    ("dvgpu_dynaverse_create", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(_P)] + _E),
+    ("dvgpu_dynaverse_destroy", None, [_P]),
+    ("dvgpu_dynaverse_params_create", ctypes.c_int, [_P, _SZ, _B, _B, ctypes.POINTER(ctypes.c_uint64)] + _E),
+    ("dvgpu_dynaverse_params_destroy", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
+    ("dvgpu_dynaverse_params_info", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.POINTER(DynaverseParamsInfo)] + _E),
+    ("dvgpu_dynaverse_session_open", ctypes.c_int,
+     [_P, ctypes.c_uint64, _P, _P, ctypes.POINTER(ctypes.c_uint64), _B] + _E),
+    ("dvgpu_dynaverse_session_close", ctypes.c_int, [_P, ctypes.c_uint64] + _E),
+    ("dvgpu_dynaverse_session_state", ctypes.c_int,
+     [_P, ctypes.c_uint64, _B, _B, _B, ctypes.POINTER(ctypes.c_uint64)] + _E),
+    ("dvgpu_dynaverse_submit", ctypes.c_int,
+     [_P, ctypes.c_uint64, _P, _P, _SZ, _P, _P, _SZ, ctypes.POINTER(ctypes.c_uint64)] + _E),
+    ("dvgpu_dynaverse_wait", ctypes.c_int, [_P, ctypes.c_uint64, _B, ctypes.POINTER(DynaverseResult)] + _E),
+    ("dvgpu_dynaverse_update", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _SZ, _P, _P, _SZ, _B] + _E),
+    ("dvgpu_dynaverse_verify", ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _B] + _E),
+    ("dvgpu_dynaverse_set_max_batch", ctypes.c_int, [_P, ctypes.c_uint32]),
+    ("dvgpu_dynaverse_stats", ctypes.c_int, [_P, ctypes.POINTER(DynaverseStats)]),
 ]
 
 
@@ -315,6 +350,140 @@ def ntt_noalloc(d_values: int, n: int, kind: int, d_result: int, stream=None):
     rc = lib().dvgpu_bn254_ntt_noalloc(d_values, n, kind, d_result, stream, err, len(err))
     if rc != 0:
         raise DvgpuError(rc, err.value.decode(errors="replace"))
+
+
+DYNAVERSE_PROOF_BYTES = 9304
+
+
+def _fr_bytes(values) -> bytes:
+    """Field elements as concatenated canonical bytes (ints or bytes)."""
+    if isinstance(values, (bytes, bytearray)):
+        return bytes(values)
+    return b"".join(encode_fr(v % R_MODULUS) for v in values)
+
+
+class DynaverseEngine:
+    """Dynaverse update proofs on the device (dvgpu_dynaverse_*): the
+    prover behind UpdateSession (crates/protocol/src/dynaverse/session.rs)
+    with every proof composed and verified on the GPU.  Parameters and
+    sessions stay resident; submit() queues an update from any thread, the
+    worker merges the pending updates of up to max_batch sessions into
+    shared launches (continuous batching); max_batch = 1 is the per-call
+    form.  Proof bytes: DYNAVERSE_PROOF_BYTES in the layout of
+    include/dynaverse_gpu.h."""
+
+    def __init__(self, hbm_budget_bytes: int, max_batch: int = 64):
+        self._L = lib()
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        rc = self._L.dvgpu_dynaverse_create(hbm_budget_bytes, max_batch, ctypes.byref(h), err, len(err))
+        if rc != 0:
+            raise DvgpuError(rc, err.value.decode(errors="replace"))
+        self._h = h
+
+    def _call(self, name, *args):
+        err = ctypes.create_string_buffer(512)
+        rc = getattr(self._L, name)(self._h, *args, err, len(err))
+        if rc != 0:
+            raise DvgpuError(rc, err.value.decode(errors="replace"))
+
+    def params_create(self, n: int, tau_x: int, tau_y: int) -> int:
+        """DynaverseParams for ToyCircuit(n) from the two trapdoors."""
+        h = ctypes.c_uint64()
+        self._call("dvgpu_dynaverse_params_create", n, encode_fr(tau_x % R_MODULUS), encode_fr(tau_y % R_MODULUS),
+                   ctypes.byref(h))
+        return h.value
+
+    def params_destroy(self, params: int):
+        self._call("dvgpu_dynaverse_params_destroy", params)
+
+    def params_info(self, params: int) -> DynaverseParamsInfo:
+        info = DynaverseParamsInfo()
+        self._call("dvgpu_dynaverse_params_info", params, ctypes.byref(info))
+        return info
+
+    def open_session(self, params: int, public_inputs, witness):
+        """start_update_session: returns (session, anchor proof bytes)."""
+        pub, wit = _fr_bytes(public_inputs), _fr_bytes(witness)
+        s = ctypes.c_uint64()
+        proof = ctypes.create_string_buffer(DYNAVERSE_PROOF_BYTES)
+        self._call("dvgpu_dynaverse_session_open", params, _ptr(pub), _ptr(wit), ctypes.byref(s), proof)
+        return s.value, proof.raw
+
+    def close_session(self, session: int):
+        self._call("dvgpu_dynaverse_session_close", session)
+
+    def session_state(self, session: int, n: int):
+        """(witness bytes, public input bytes, proof bytes, anchor distance)."""
+        w = ctypes.create_string_buffer(32 * 6 * n)
+        p = ctypes.create_string_buffer(32 * n)
+        proof = ctypes.create_string_buffer(DYNAVERSE_PROOF_BYTES)
+        d = ctypes.c_uint64()
+        self._call("dvgpu_dynaverse_session_state", session, w, p, proof, ctypes.byref(d))
+        return w.raw, p.raw, proof.raw, d.value
+
+    @staticmethod
+    def _update_args(indices, values, public_indices, public_values):
+        idx = np.ascontiguousarray(np.asarray(list(indices), dtype=np.uint64))
+        pidx = np.ascontiguousarray(np.asarray(list(public_indices), dtype=np.uint64))
+        vals, pvals = _fr_bytes(values), _fr_bytes(public_values)
+        if len(vals) != 32 * idx.size or len(pvals) != 32 * pidx.size:
+            raise ValueError("update indices/values length mismatch")
+        return idx, vals, pidx, pvals
+
+    def submit(self, session: int, indices, values, public_indices=(), public_values=()) -> int:
+        idx, vals, pidx, pvals = self._update_args(indices, values, public_indices, public_values)
+        t = ctypes.c_uint64()
+        self._call("dvgpu_dynaverse_submit", session, _ptr(idx), _ptr(vals), idx.size, _ptr(pidx), _ptr(pvals),
+                   pidx.size, ctypes.byref(t))
+        return t.value
+
+    def wait(self, ticket: int):
+        """(proof bytes, DynaverseResult) of a submitted update."""
+        proof = ctypes.create_string_buffer(DYNAVERSE_PROOF_BYTES)
+        res = DynaverseResult()
+        self._call("dvgpu_dynaverse_wait", ticket, proof, ctypes.byref(res))
+        return proof.raw, res
+
+    def update(self, session: int, indices, values, public_indices=(), public_values=()) -> bytes:
+        """UpdateSession::update_with_public_inputs (session.rs:39-41)."""
+        idx, vals, pidx, pvals = self._update_args(indices, values, public_indices, public_values)
+        proof = ctypes.create_string_buffer(DYNAVERSE_PROOF_BYTES)
+        self._call("dvgpu_dynaverse_update", session, _ptr(idx), _ptr(vals), idx.size, _ptr(pidx), _ptr(pvals),
+                   pidx.size, proof)
+        return proof.raw
+
+    def verify(self, params: int, public_inputs, proof: bytes) -> bool:
+        """DynaverseVerifyingKey::verify on the device."""
+        pub = _fr_bytes(public_inputs)
+        ok = ctypes.create_string_buffer(1)
+        self._call("dvgpu_dynaverse_verify", params, _ptr(pub), _ptr(bytes(proof)), ok)
+        return ok.raw[0] == 1
+
+    def set_max_batch(self, m: int):
+        self._L.dvgpu_dynaverse_set_max_batch(self._h, m)
+
+    def stats(self) -> DynaverseStats:
+        s = DynaverseStats()
+        self._L.dvgpu_dynaverse_stats(self._h, ctypes.byref(s))
+        return s
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.dvgpu_dynaverse_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class DvgpuServer:

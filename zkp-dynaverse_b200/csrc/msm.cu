@@ -47,8 +47,8 @@ DV_INL uint32_t set_of(const uint32_t* set_off, uint32_t count, uint32_t i) {
 DV_INL void locate(const SetMap& m, uint32_t i, uint32_t& set, uint32_t& sidx, uint32_t& pidx) {
     set = m.count > 1 ? set_of(m.off, m.count, i) : 0;
     const uint32_t rel = i - (m.count > 1 ? m.off[set] : 0u);
-    sidx = m.src ? m.src[set] + rel : i;
-    pidx = m.prefix ? rel : sidx;
+    sidx = m.term_scalar ? m.term_scalar[i] : m.src ? m.src[set] + rel : i;
+    pidx = m.term_point ? m.term_point[i] : m.prefix ? rel : sidx;
 }
 
 // 1. Histogram of signed digits.

@@ -108,12 +108,18 @@ void msm_run(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_scal
 // Digit i (0 <= i < off[count]) belongs to the set k with
 // off[k] <= i < off[k + 1]; its scalar is src[k] + (i - off[k]) (i itself
 // when src is null); its point is i - off[k] with prefix (every set uses a
-// prefix of one base array), else the scalar's index.
+// prefix of one base array), else the scalar's index.  With per-term arrays
+// (term_point, term_scalar, device, off[count] entries each) term i takes
+// point term_point[i] and scalar term_scalar[i] instead: the sets of one
+// launch can then draw entries from anywhere in a base array (or its table)
+// and share scalars, with no gathered copy.
 struct SetMap {
     const uint32_t* off;  // device, count + 1 entries
     const uint32_t* src;  // device or null
     uint32_t count;
     int prefix;
+    const uint32_t* term_point = nullptr;
+    const uint32_t* term_scalar = nullptr;
 };
 
 // Window plan of a launch sequence of count sets (largest max_set, total

@@ -835,6 +835,42 @@ void pairing_run(Backend& b, const uint8_t* g1, const uint8_t* g2, uint64_t term
                      prepared ? &first : nullptr, st);
 }
 
+}  // namespace
+
+// Pairing-product checks over device inputs, with no host synchronisation:
+// equation e holds iff prod over terms [d_off[e], d_off[e+1]) of
+// e(p[k], q[d_qidx[k]]) is one; d_verdicts[e] = 1 / 0.  p: Montgomery affine
+// G1 terms, q: nq Montgomery affine G2 points (each prepared once here).
+// Scratch comes from the backend's pairing state.  For callers that build
+// their equations on the device (the Dynaverse verifier, dynaverse.cu).
+void pairing_check_device(Backend& b, const G1A* p, uint64_t terms, const G2A* q, uint64_t nq,
+                          const uint32_t* d_qidx, const uint64_t* d_off, uint64_t equations, uint8_t* d_verdicts,
+                          cudaStream_t st) {
+    if (!equations) return;
+    if (nq > PREP_MAX) throw InvalidArgument("too many distinct G2 points in one check");
+    PairingState& ps = pairing_state(b);
+    Line* lines = ps.lines.as<Line>((uint64_t)LINES * std::max<uint64_t>(1, nq));
+    uint32_t* qinf = ps.inf.as<uint32_t>(std::max<uint64_t>(1, nq));
+    if (nq) {
+        k_prepare<<<group_blocks(nq), 128, 0, st>>>(q, nq, lines, qinf);
+        DV_LAUNCH();
+    }
+    Fq2* mil = b.aux.as<Fq2>(6 * std::max<uint64_t>(1, std::max(terms, equations)));
+    const bool multi = miller_per_equation(terms);
+    if (multi) {
+        k_miller_multi<<<group_blocks(equations), 128, 0, st>>>(p, d_qidx, qinf, lines, d_off, equations, mil);
+        DV_LAUNCH();
+    } else if (terms) {
+        k_miller_multi<<<group_blocks(terms), 128, 0, st>>>(p, d_qidx, qinf, lines, nullptr, terms, mil);
+        DV_LAUNCH();
+    }
+    k_final_exp<<<group_blocks(equations), 128, 0, st>>>(mil, multi ? nullptr : d_off, equations, d_verdicts,
+                                                         nullptr);
+    DV_LAUNCH();
+}
+
+namespace {
+
 void check_offsets(const uint64_t* offsets, size_t equations) {
     require(offsets && equations >= 1 && equations <= (1u << 24), "invalid pairing check arguments");
     require(offsets[0] == 0, "pairing offsets must start at 0");
