@@ -58,12 +58,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch", "g2check",
-                                                         "serve", "ecntt", "poly", "pairing"])
+                                                         "serve", "ecntt", "poly", "pairing", "proofs"])
     ap.add_argument("--log-n", type=int, default=None)
     ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
     ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
     ap.add_argument("--alg", type=int, default=3, choices=[1, 2, 3], help="g2check: subgroup algorithm")
-    ap.add_argument("--requests", type=int, default=4000, help="serve: update requests per run")
+    ap.add_argument("--requests", type=int, default=None, help="serve / proofs: update requests per run")
+    ap.add_argument("--sessions", type=int, default=16, help="proofs: sessions of n = 2^log-n")
+    ap.add_argument("--mix", action="store_true", help="proofs: 64 sessions, n in {256, 4096, 65536}, 37:18:9")
+    ap.add_argument("--umax", type=float, default=10.0, help="proofs: supports of floor(2^U) gates, U~U[0,umax]")
     ap.add_argument("--rows", type=int, default=16, help="ecntt: rows per transform call")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
@@ -71,10 +74,12 @@ def parse():
     a = ap.parse_args()
     if a.log_n is None:
         a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20, "batch": 18,
-                   "g2check": 16, "serve": 16, "ecntt": 12, "poly": 12, "pairing": 12}[a.op]
+                   "g2check": 16, "serve": 16, "ecntt": 12, "poly": 12, "pairing": 12, "proofs": 16}[a.op]
+    if a.requests is None:
+        a.requests = {"serve": 4000, "proofs": 256}.get(a.op, 4000)
     if a.steps is None:
         a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100,
-                   "batch": 20, "g2check": 50, "serve": 1,
+                   "batch": 20, "g2check": 50, "serve": 1, "proofs": 1,
                    "ecntt": 10, "poly": 20, "pairing": 20}[a.op]
     return a
 
@@ -776,6 +781,175 @@ class ServeOp:
         return line
 
 
+R_FR = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+
+
+def valid_witness(n, seed):
+    """A uniform valid ToyCircuit(n) instance (toy_circuit.rs:45-90): left,
+    right and multiplier uniform in Fr per gate; sum and product follow."""
+    import random
+    rng = random.Random(seed)
+    pub, w = [0] * n, [0] * (6 * n)
+    for i in range(n):
+        left, right, mul = rng.randrange(R_FR), rng.randrange(R_FR), rng.randrange(R_FR)
+        s = (left + right) % R_FR
+        pub[i] = left
+        w[i], w[n + i], w[2 * n + i], w[3 * n + i], w[4 * n + i], w[5 * n + i] = left, right, s, s, mul, s * mul % R_FR
+    return pub, w
+
+
+def proof_stream(sizes, witnesses, count, umax, seed):
+    """The seeded update stream of the serving workload: a session, a support
+    of floor(2^U) gates (U ~ U[0, umax], capped at n), half in the session's
+    64-gate hotspot window and half uniform over [0, n), every gate given a
+    fresh uniform s5 value u and s6 = s4 u so the circuit stays valid."""
+    import random
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    vr = random.Random(seed + 1)
+    hot = [int(rng.integers(0, max(1, n - 64))) for n in sizes]
+    out = []
+    for t in range(count):
+        j = int(rng.integers(len(sizes)))
+        n = sizes[j]
+        g = min(n, int(2 ** rng.uniform(0, umax)))
+        if t % 2:
+            gates = hot[j] + rng.choice(min(64, n), size=min(g, 64, n), replace=False)
+        else:
+            gates = rng.choice(n, size=g, replace=False)
+        w = witnesses[j]
+        idx, vals = [], []
+        for gate in gates.tolist():
+            u = vr.randrange(R_FR)
+            idx += [4 * n + gate, 5 * n + gate]
+            vals += [u, w[3 * n + gate] * u % R_FR]
+        out.append((j, idx, b"".join(v.to_bytes(32, "little") for v in vals)))
+    return out
+
+
+class ProofServeOp:
+    """Dynaverse update proofs (row a10): sessions of ToyCircuit(n) with
+    resident parameters and state; a stream of sparse witness updates; each
+    request returns a complete DynaverseProof, verified on the device before
+    it is published (the reference session verifies each proof too,
+    session.rs:126-131).  The same stream runs through the served form
+    (continuous batching, max_batch 64) and the per-call form (max_batch 1:
+    one update at a time, each a full pipeline with its own launches), at
+    saturation (all requests queued at once) and as a Poisson stream at 80 %
+    of the per-call capacity (latency).  Proofs are identical between the
+    forms.  Default: 16 sessions of n = 65536; --mix: 64 sessions with
+    n in {256, 4096, 65536} in ratio 37:18:9."""
+
+    def __init__(self, args):
+        self.mix = args.mix
+        n = 1 << args.log_n
+        self.sizes = [256] * 37 + [4096] * 18 + [65536] * 9 if args.mix else [n] * args.sessions
+        self.requests = args.requests
+        self.umax = args.umax
+        label = "n 256/4096/65536 mix" if args.mix else f"n={n}"
+        self.metric = f"update proofs/s ({label}, served, every proof verified)"
+        self.workload = (f"Dynaverse update proofs over {len(self.sizes)} sessions ({label}), {self.requests} requests; "
+                         f"supports of floor(2^U) gates, U~U[0,{self.umax}], half in a 64-gate hotspot window, half "
+                         "uniform; every gate's s5 a fresh uniform Fr and s6 = s4 s5; re-anchor when the delta "
+                         "reaches ceil(sqrt(n)) (session.rs:92)")
+        self.profile = "dynaverse_serve"
+
+    def _setup(self, dv):
+        import random
+        self.eng = dv.DynaverseEngine(150 << 30, 64)
+        rng = random.Random(9900)
+        self.params = {}
+        for n in sorted(set(self.sizes)):
+            while True:
+                try:
+                    self.params[n] = self.eng.params_create(n, rng.randrange(1, R_FR), rng.randrange(1, R_FR))
+                    break
+                except dv.DvgpuError:
+                    continue
+        self.wit = [valid_witness(n, 9000 + j) for j, n in enumerate(self.sizes)]
+        self.pub_b = [b"".join(v.to_bytes(32, "little") for v in p) for p, _ in self.wit]
+        self.wit_b = [b"".join(v.to_bytes(32, "little") for v in w) for _, w in self.wit]
+        self.reqs = proof_stream(self.sizes, [w for _, w in self.wit], self.requests, self.umax, 9100)
+
+    def _run(self, max_batch, arrivals):
+        e = self.eng
+        e.set_max_batch(max_batch)
+        ids = [e.open_session(self.params[n], self.pub_b[j], self.wit_b[j])[0] for j, n in enumerate(self.sizes)]
+        before = e.stats()
+        t0 = time.perf_counter()
+        tickets = []
+        for (j, idx, vals), at in zip(self.reqs, arrivals):
+            while time.perf_counter() - t0 < at:
+                pass
+            tickets.append(e.submit(ids[j], idx, vals))
+        outs = [e.wait(t) for t in tickets]
+        wall = time.perf_counter() - t0
+        st = e.stats()
+        for sid in ids:
+            e.close_session(sid)
+        lat = sorted((r.done_ns - r.submit_ns) / 1e6 for _, r in outs)
+        pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
+        return {"proofs": [p for p, _ in outs], "wall_s": wall, "per_s": len(outs) / wall,
+                "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1], "mean_ms": sum(lat) / len(lat),
+                "batches": st.batches - before.batches, "largest_batch": max(r.batch_requests for _, r in outs),
+                "rebuilds": sum(r.rebuilt for _, r in outs), "launches": st.launches - before.launches,
+                "msm_fme": st.msm_fme - before.msm_fme}
+
+    def run_standalone(self, args, torch, dv, b, s, sampler, imad_peak_fn, world=1):
+        import numpy as np
+        self._setup(dv)
+        zeros = [0.0] * self.requests
+        self._run(64, zeros[:64])  # warm-up: workspaces, tables and NTT plans reach their sizes
+        self._run(1, zeros[:8])
+        sampler.start()
+        sat_served = self._run(64, zeros)
+        sat_plain = self._run(1, zeros)
+        rate = 0.8 * sat_plain["per_s"]
+        arrivals = np.cumsum(np.random.default_rng(9200).exponential(1.0 / rate, self.requests)).tolist()
+        poi_served = self._run(64, arrivals)
+        poi_plain = self._run(1, arrivals)
+        clocks = sampler.stop()
+        runs = (sat_served, sat_plain, poi_served, poi_plain)
+        exact = all(r["proofs"] == sat_served["proofs"] for r in runs)
+        # every proof was verified before publication; re-check a sample with the device verifier
+        e = self.eng
+        sample_ok = True
+        for (j, _, _), proof in list(zip(self.reqs, sat_served["proofs"]))[:32]:
+            sample_ok &= e.verify(self.params[self.sizes[j]], self.pub_b[j], proof)
+        peak = imad_peak_fn() / 1e12
+        macs = sat_served["msm_fme"] * 136
+        ach = macs / sat_served["wall_s"] / 1e12
+        strip = lambda r: {k: v for k, v in r.items() if k != "proofs"}
+        job_per_s = world * self.requests / max_over_ranks(sat_served["wall_s"], world)
+        in_bytes = sum(8 * len(idx) + len(vals) for _, idx, vals in self.reqs) / self.requests
+        line = {
+            "metric": self.metric, "value": job_per_s, "unit": "proofs/s", "n_gpus": world,
+            "steps": self.requests, "warmup": 1, "ms_per_step": 1e3 / sat_served["per_s"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Fq/Fr Montgomery, exact)",
+            "data": "synthetic (seeded trapdoors, uniform valid witnesses, seeded update stream)",
+            "config": {"workload": self.workload, "op": "proofs",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "sessions": len(self.sizes), "requests": self.requests,
+                       "l2": "not flushed: a stream of requests against resident sessions"},
+            "e2e": {"value": job_per_s, "unit": "proofs/s", "h2d_bytes_per_step": in_bytes,
+                    "d2h_bytes_per_step": 9304,
+                    "call": "dvgpu_dynaverse_submit/wait from host memory (update in, proof out)"},
+            "serving": {"saturation": {"served": strip(sat_served), "per_call": strip(sat_plain),
+                                       "speedup": sat_served["per_s"] / sat_plain["per_s"]},
+                        "poisson": {"rate_per_s": rate, "served": strip(poi_served), "per_call": strip(poi_plain),
+                                    "p99_ratio": poi_plain["p99_ms"] / poi_served["p99_ms"]},
+                        "bit_exact": exact, "device_verifier_sample_accepted": bool(sample_ok)},
+            "roofline": {"bound": "imad", "kernel": "the whole saturation run (every MSM of every proof)",
+                         "achieved": ach, "peak": peak, "unit": "TMAC/s", "frac": ach / peak,
+                         "algorithmic_macs_per_launch": macs,
+                         "convention": "sum over MSM sets of min_c ceil(254/c)(10k + 14 2^c) x 136 (x3 G2)",
+                         "traffic": None},
+            "gpu_launches": sat_served["launches"], "clocks": clocks,
+        }
+        self.eng.close()
+        return line
+
+
 def batch_workload(log_bases):
     """The batching workload: 512 G1 MSMs of floor(2^U) points, U ~ U[8, 18],
     over prefixes of the SRS, and 256 forward NTTs of 2^floor(U) elements,
@@ -1244,6 +1418,7 @@ def make_op(args):
     return {"msm": lambda: MsmOp(args), "msmres": lambda: ResidentMsmOp(args), "g2msm": lambda: MsmOp(args, g2=True),
             "ntt": lambda: NttOp(args), "sparse": lambda: SparseOp(args), "fixedbase": lambda: FixedBaseOp(args),
             "batch": lambda: BatchOp(args), "g2check": lambda: G2CheckOp(args), "serve": lambda: ServeOp(args),
+            "proofs": lambda: ProofServeOp(args),
             "ecntt": lambda: EcNttOp(args), "poly": lambda: PolyOp(args), "pairing": lambda: PairingOp(args)}[args.op]()
 
 

@@ -645,6 +645,9 @@ typedef struct DvgpuDynaverseStats {
     uint64_t requests, batches, sessions, resident_bytes, budget_bytes;
     uint64_t max_batch, largest_batch, busy_ns, pending;
     uint64_t sparse_proofs, rebuilds, launches;
+    /* algorithmic G1 field multiplications of every MSM run (min over c of
+     * ceil(254/c) (10 k + 14 2^c) per k-term set, x3 for G2 sets) */
+    uint64_t msm_fme;
 } DvgpuDynaverseStats;
 int dvgpu_dynaverse_create(uint64_t hbm_budget_bytes, uint32_t max_batch, void** engine, char* error,
                            size_t error_capacity);

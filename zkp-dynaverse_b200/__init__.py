@@ -163,7 +163,7 @@ class DynaverseResult(ctypes.Structure):
 class DynaverseStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("requests", "batches", "sessions", "resident_bytes", "budget_bytes",
                                               "max_batch", "largest_batch", "busy_ns", "pending", "sparse_proofs",
-                                              "rebuilds", "launches")]
+                                              "rebuilds", "launches", "msm_fme")]
 
 
 # (name, restype, argtypes)

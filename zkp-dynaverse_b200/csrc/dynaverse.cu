@@ -50,6 +50,7 @@
 // then u64 has_delta, u64 anchor_generation, u64 generation.
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -328,10 +329,13 @@ constexpr uint64_t D_WIRES = 0, D_W = 384, D_H = 448, D_DYN = 512, D_CONS = 1024
 // a_degree, b_degree, d_degree (448 B each).
 constexpr int DY_IZ = 6, DY_IH = 7;
 
-// Per-job record in the output arena: the proof part it produces (anchor or
-// delta bytes), then side slots: public_h input, public-diff MSM, public_h out.
-constexpr uint64_t JOB_BYTES = 5312 + 3 * 64;
-constexpr uint64_t SIDE_PUB = 5312, SIDE_PDIFF = 5312 + 64, SIDE_PUBNEW = 5312 + 128;
+// Per-job record in the output arena: delta fields (5312 B; for a re-anchor
+// the delta's linear fields), side slots ([public]_h before the update, the
+// MSM of the public differences -- or of all public inputs for a fresh
+// anchor --, [public]_h after), then anchor fields (3968 B).
+constexpr uint64_t SIDE_PUB = 5312, SIDE_PDIFF = 5312 + 64, SIDE_PUBNEW = 5312 + 128, REC_ANCHOR = 5504;
+constexpr uint64_t JOB_BYTES = REC_ANCHOR + 3968;
+static_assert(REC_ANCHOR % 128 == 0 && JOB_BYTES % 128 == 0, "record alignment");
 
 // ================================================================ device kernels
 // Canonical words <-> Montgomery.
@@ -787,6 +791,54 @@ struct Emit {
 DV_INL G1A g1_sub(const G1A& a, const G1A& b) { return G1X::add_affine(G1X::from_affine(a), b.neg()).to_affine(); }
 DV_INL G1A g1_add(const G1A& a, const G1A& b) { return G1X::add_affine(G1X::from_affine(a), b).to_affine(); }
 
+// ---------------------------------------------------------------- incremental re-anchor
+// Every anchor field but the multiplication quotient is a commitment linear
+// in the witness (prove_anchor_traced, dynaverse.rs:149-248): for the new
+// anchor w' = w + delta it is the old field plus the same commitment of the
+// delta, which the sparse pipeline computes anyway (the reference's
+// FixedLinear, dynaverse/sparse_linear.rs:495-559, adds them the same way).
+// Field f of a re-anchor: (anchor offset, offset of the delta's field).
+DV_INL void rebase_field(uint32_t f, uint64_t& ao, uint64_t& dof) {
+    if (f < 6) { ao = A_WIRES + 64 * f; dof = D_WIRES + 64 * f; }
+    else if (f == 6) { ao = A_W; dof = D_DYN + 64 * 6; }
+    else if (f == 7) { ao = A_H; dof = D_DYN + 64 * 7; }
+    else if (f < 16) { ao = A_DYN + 64 * (f - 8); dof = D_DYN + 64 * (f - 8); }
+    else if (f < 58) { ao = A_CONS + 64 * (f - 16); dof = D_CONS + 64 * (f - 16); }
+    else if (f == 58) { ao = A_PZQ; dof = D_PZQ; }
+    else { ao = A_S5G2; dof = D_AFF2; }  // G2: s5 over the delta of wire s5
+}
+constexpr uint32_t REBASE_FIELDS = 60;
+struct RebaseJob {
+    uint8_t* rec;       // the job's record: delta fields, then the new anchor at REC_ANCHOR
+    const uint8_t* old; // the current anchor proof bytes
+};
+__global__ void k_dv_rebase(const RebaseJob* __restrict__ jobs, uint32_t njobs) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= njobs * REBASE_FIELDS) return;
+    const RebaseJob J = jobs[i / REBASE_FIELDS];
+    const uint32_t f = i % REBASE_FIELDS;
+    uint64_t ao, dof;
+    rebase_field(f, ao, dof);
+    uint8_t* out = J.rec + REC_ANCHOR + ao;
+    if (f + 1 < REBASE_FIELDS) {
+        store_g1(out, g1_add(load_g1(J.old + ao), load_g1(J.rec + dof)));
+    } else {
+        const G2A r = G2X::add_affine(G2X::from_affine(load_g2(J.old + ao)), load_g2(J.rec + dof)).to_affine();
+        store_canonical(out, r.x);
+        store_canonical(out + 64, r.y);
+    }
+}
+// arena[dst[k]] = arena[src[k]]
+__global__ void k_dv_scatter(const uint32_t* __restrict__ pairs, uint32_t count, Fr* __restrict__ arena) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) arena[pairs[2 * k]] = arena[pairs[2 * k + 1]];
+}
+// out = x + y (canonical)
+__global__ void k_dv_vadd(Fr* __restrict__ out, const Fr* __restrict__ x, const Fr* __restrict__ y, uint64_t count) {
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) out[k] = Fr::add(x[k], y[k]);
+}
+
 // Dynamo fields at p (alpha, beta, h, z, b, q, instance_z, instance_h).
 DV_INL void emit_dynamo(Emit& e, const uint8_t* p) {
     const G1A alpha = load_g1(p), beta = load_g1(p + 64), h = load_g1(p + 128), z = load_g1(p + 192),
@@ -838,13 +890,12 @@ __global__ void k_dv_terms(const VerifyJob* __restrict__ jobs, uint32_t njobs, G
         const G1X s12 = G1X::add_affine(G1X::from_affine(load_g1(A + A_WIRES)), load_g1(A + A_WIRES + 64));
         ok &= G1X::equal(s12, G1X::from_affine(load_g1(A + A_WIRES + 128)));
         // h + [public]_h == 0 (dynaverse.rs:1008-1015) when the proof has no
-        // delta (kind 0); [public]_h in the side slot
-        const G1A pub = load_g1(r + SIDE_PDIFF);
-        if (J.kind == 0) ok &= G1X::add_affine(G1X::from_affine(load_g1(A + A_H)), pub).is_inf();
-        const uint8_t* src = r + SIDE_PDIFF;
-        uint8_t* dst = r + SIDE_PUBNEW;
-        for (int i = 0; i < 64; i += 16)
-            *reinterpret_cast<uint4*>(dst + i) = *reinterpret_cast<const uint4*>(src + i);
+        // delta (kind 0); [public]_h = the side slots' value before the update
+        // plus the public differences (a fresh anchor: zero plus the MSM of
+        // all public inputs)
+        const G1X pub = G1X::add_affine(G1X::from_affine(load_g1(r + SIDE_PUB)), load_g1(r + SIDE_PDIFF));
+        if (J.kind == 0) ok &= G1X::add(G1X::add_affine(G1X::inf(), load_g1(A + A_H)), pub).is_inf();
+        store_g1(r + SIDE_PUBNEW, pub.to_affine());
     } else {
         const uint32_t aff2 = V_COUNT + J.fresh, unaff2 = aff2 + 1, us5 = aff2 + 2;
         q[aff2] = load_g2(r + D_AFF2);
@@ -996,9 +1047,19 @@ struct MsmBuild {
         seg_off.push_back(terms);
     }
     void end(uint64_t out) {
+        const uint32_t k = terms - set_off.back();
         set_off.push_back(terms);
         out_off.push_back(out);
+        // algorithmic work of a k-term MSM: min over c of ceil(254/c) (10 k + 14 2^c) field
+        // multiplications (XYZZ mixed additions and bucket reduction)
+        if (k) {
+            double best = 1e300;
+            for (int c = 1; c <= 24; ++c)
+                best = std::min(best, (double)((254 + c - 1) / c) * (10.0 * k + 14.0 * (double)(1u << c)));
+            fme += best;
+        }
     }
+    double fme = 0;  // G1 field multiplications (x3 for G2 sets)
     size_t sets() const { return out_off.size(); }
     struct Dev {
         size_t segs, seg_off, set_off, out_off;
@@ -1171,6 +1232,7 @@ public:
         s.sparse_proofs = stat_sparse_;
         s.rebuilds = stat_rebuilds_;
         s.launches = stat_launches_;
+        s.msm_fme = stat_fme_.load();
         return s;
     }
 
@@ -1268,7 +1330,7 @@ private:
     uint64_t budget_, resident_ = 0;
     uint32_t max_batch_;
     MsmWorkspace ws1_, ws2_;
-    NttBatch nb_fwd_, nb_inv_;
+    NttBatch nb_fwd_, nb_inv_, nb_r1_, nb_r2_, nb_r3_;
     DevBuf stage_, arena_, scr_, out_, status_, verdicts_, tpoint_, tscalar_, lrow_, lsc_, terms_p_, terms_q_, g2q_,
         tmp_, tmp2_, err_;
     PinnedBuf pstage_, pstage2_, parena_, pout_;
@@ -1284,6 +1346,7 @@ private:
     uint64_t next_id_ = 1, next_ticket_ = 1;
     uint64_t stat_requests_ = 0, stat_batches_ = 0, stat_largest_ = 0, stat_busy_ns_ = 0, stat_sparse_ = 0,
              stat_rebuilds_ = 0, stat_launches_ = 0;
+    std::atomic<uint64_t> stat_fme_{0};  // written by the worker, read by stats()
     std::thread worker_;
 };
 
@@ -1621,21 +1684,22 @@ void Engine::run_anchor(Params& P, const std::vector<Canon>& w, const std::vecto
     // every commitment of the anchor in one G1 launch and one G2 launch
     MsmBuild g1, g2;
     auto fo = [&](int f) { return P.fam_off[f]; };
+    const uint64_t RA = REC_ANCHOR;
     for (int t = 0; t < 6; ++t) {
         g1.seg(0, n, fo(F_LAG), W + t * n, 0);
-        g1.end(A_WIRES + 64 * t);
+        g1.end(RA + A_WIRES + 64 * t);
     }
     g1.seg(0, 6 * n, fo(F_LX), W, 0);
-    g1.end(A_W);
+    g1.end(RA + A_W);
     g1.seg(0, 7 * n, fo(F_LY), H, 0);
-    g1.end(A_H);
+    g1.end(RA + A_H);
     const int dyf[5] = {F_ALPHA, F_BETA, F_H, F_Z, F_B};
     for (int k = 0; k < 5; ++k) {
         g1.seg(0, 6 * n, fo(dyf[k]), W, 0);
-        g1.end(A_DYN + 64 * k);
+        g1.end(RA + A_DYN + 64 * k);
     }
     for (int t = 0; t < 6; ++t) {
-        const uint64_t base = A_CONS + 448 * t;
+        const uint64_t base = RA + A_CONS + 448 * t;
         g1.seg(0, 6 * n, fo(F_QAC0 + t), W, 0);
         g1.end(base);
         const int cf[3] = {F_QCD, F_QBD, F_D};
@@ -1653,16 +1717,17 @@ void Engine::run_anchor(Params& P, const std::vector<Canon>& w, const std::vecto
         g1.end(base + 384);
     }
     g1.seg(0, 6 * n, fo(F_PQ), W, 0);
-    g1.end(A_PZQ);
+    g1.end(RA + A_PZQ);
     g1.seg(0, n - 1, fo(F_KZG), Q, 0);
-    g1.end(A_MQ);
+    g1.end(RA + A_MQ);
     g1.seg(0, n, fo(F_PUBH), PB, 0);
     g1.end(SIDE_PDIFF);
     g2.seg(0, n, P.fam2_off[F2_LAG], W + 4 * n, 0);
-    g2.end(A_S5G2);
-    std::vector<CopyDesc> cp = {{rec + A_DYN + 64 * DY_IZ, rec + A_W, 64}, {rec + A_DYN + 64 * DY_IH, rec + A_H, 64}};
-    for (int t = 1; t < 6; ++t) cp.push_back({rec + A_CONS + 448 * t + 256, rec + A_CONS + 256, 64});
-    const VerifyJob vj{rec, rec, 0, 0, 0, 0};
+    g2.end(RA + A_S5G2);
+    uint8_t* an = rec + RA;
+    std::vector<CopyDesc> cp = {{an + A_DYN + 64 * DY_IZ, an + A_W, 64}, {an + A_DYN + 64 * DY_IH, an + A_H, 64}};
+    for (int t = 1; t < 6; ++t) cp.push_back({an + A_CONS + 448 * t + 256, an + A_CONS + 256, 64});
+    const VerifyJob vj{rec, an, 0, 0, 0, 0};
     const std::vector<uint64_t> off = eq_offsets(1, false);
     Stager stg;
     g1.stage(stg);
@@ -1672,13 +1737,14 @@ void Engine::run_anchor(Params& P, const std::vector<Canon>& w, const std::vecto
     const uint8_t* d = stage_.view<uint8_t>();
     tpoint_.as<uint32_t>(std::max(g1.terms, g2.terms) + 1);
     tscalar_.as<uint32_t>(std::max(g1.terms, g2.terms) + 1);
+    stat_fme_ += (uint64_t)(g1.fme + 3 * g2.fme);
     run_msm<Fq>(ws1_, P.table.view<G1A>(), g1, d, nullptr, nullptr, arena, rec, err);
     run_msm<Fq2>(ws2_, P.table2.view<G2A>(), g2, d, nullptr, nullptr, arena, rec, err + 1);
     k_dv_copy<<<dim3(1, (unsigned)cp.size()), 32, 0, st>>>((uint32_t)cp.size(), reinterpret_cast<const CopyDesc*>(d + at_cp));
     DV_LAUNCH();
     run_verify(P, 1, 1, ANCHOR_TERMS, ANCHOR_EQS, reinterpret_cast<const VerifyJob*>(d + at_vj),
                reinterpret_cast<const uint64_t*>(d + at_off), verd, status);
-    DV_CUDA(cudaMemcpyAsync(anc, rec, ANCHOR_BYTES, cudaMemcpyDeviceToDevice, st));
+    DV_CUDA(cudaMemcpyAsync(anc, an, ANCHOR_BYTES, cudaMemcpyDeviceToDevice, st));
     uint8_t* hout = pout_.as<uint8_t>(JOB_BYTES + 64 + ANCHOR_EQS);
     DV_CUDA(cudaMemcpyAsync(hout, rec, JOB_BYTES, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaMemcpyAsync(hout + JOB_BYTES, status, 4, cudaMemcpyDeviceToHost, st));
@@ -1692,7 +1758,7 @@ void Engine::run_anchor(Params& P, const std::vector<Canon>& w, const std::vecto
     bool ok = hst == 0;
     for (uint32_t e = 0; e < ANCHOR_EQS; ++e) ok &= hout[JOB_BYTES + 64 + e] == 1;
     job.ok = ok;
-    job.anchor_bytes.assign(hout, hout + ANCHOR_BYTES);
+    job.anchor_bytes.assign(hout + RA, hout + RA + ANCHOR_BYTES);
     memcpy(job.public_h, hout + SIDE_PUBNEW, 64);
     if (!ok) job.error = hst & 4 ? "multiplication relation is not divisible by X^n - 1" : "proof failed verification";
 }
@@ -1712,25 +1778,32 @@ std::map<uint32_t, hf::Fr> h_sparse(uint32_t n, const std::map<uint32_t, Canon>&
     return h;
 }
 
-// A batch of sparse updates of sessions over the same parameters
-// (prove_delta_sparse_traced, dynaverse/sparse.rs:79-276, for every job at
-// once) and the verification of each new delta (verify_delta_with_checks
-// and the public-input identity, session.rs:126-131).
+// A batch of updates of sessions over the same parameters, in one set of
+// launches: sparse proofs (prove_delta_sparse_traced, dynaverse/sparse.rs:
+// 79-276, for every job at once) and re-anchors (the anchor of the new
+// witness: the old anchor plus the delta's linear commitments, and a fresh
+// multiplication quotient), each verified on the device before it is
+// published (verify_delta_with_checks / verify_anchor_with_checks and the
+// public-input identity, session.rs:126-131, dynaverse.rs:447).
 void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     const uint32_t n = P.n, B = (uint32_t)jobs.size();
     const cudaStream_t st = st_;
     struct JL {
+        bool rb = false;
         uint32_t d = 0, h = 0, pd = 0, a = 0;
-        uint64_t E = 0, Hs = 0, FI = 0, PD = 0, FO = 0, DN = 0;
+        uint64_t E = 0, Hs = 0, FI = 0, PD = 0, FO = 0, DN = 0, R0 = 0;
         uint64_t LE = 0, LH = 0, LS[6] = {}, LSN[6] = {}, LA = 0, LPD = 0;
     };
     std::vector<JL> jl(B);
     std::vector<Canon> ain;
     std::vector<uint32_t> lrow, lsc;
+    std::vector<std::pair<uint32_t, uint64_t>> scat;  // (job, arena source) for re-anchor rows; dst below
+    std::vector<uint64_t> scat_rel;
     for (uint32_t j = 0; j < B; ++j) {
         Job& J = *jobs[j];
         Session& S = *J.S;
         JL& L = jl[j];
+        L.rb = J.rebuild;
         L.d = (uint32_t)J.delta.size();
         L.E = ain.size();
         L.LE = lrow.size();
@@ -1738,7 +1811,12 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         for (const auto& kv : J.delta) {
             ain.push_back(kv.second);
             lrow.push_back(kv.first);
-            lsc.push_back((uint32_t)(L.E + e++));
+            lsc.push_back((uint32_t)(L.E + e));
+            if (L.rb && kv.first >= 3 * n) {  // the delta of wires s4..s6 for the new coefficients
+                scat.push_back({j, L.E + e});
+                scat_rel.push_back((uint64_t)(kv.first / n - 3) * n + kv.first % n);
+            }
+            ++e;
         }
         const auto hm = h_sparse(n, J.delta);
         L.h = (uint32_t)hm.size();
@@ -1765,8 +1843,9 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
             L.LSN[t] = lrow.size() - L.LS[t];
         }
         std::set<uint32_t> aff;
-        for (const auto& kv : J.delta)
-            if (kv.first >= 3 * n) aff.insert(kv.first % n);
+        if (!L.rb)
+            for (const auto& kv : J.delta)
+                if (kv.first >= 3 * n) aff.insert(kv.first % n);
         L.a = (uint32_t)aff.size();
         L.FI = ain.size();
         for (int t = 0; t < 3; ++t)
@@ -1798,7 +1877,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
             lsc.push_back(0);
         }
     }
-    // outputs and scratch
+    // arena outputs and scratch
     uint64_t top = ain.size(), scr = 0, amax = 0;
     std::vector<FieldJob> fj(B);
     std::vector<uint32_t> kjob(B + 1, 0);
@@ -1815,6 +1894,10 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
             L.DN = top;
             top += 4ull * n;
         }
+        if (L.rb) {  // delta rows (3n), s4' padded (2n), s5' padded (2n), quotient (n)
+            L.R0 = top;
+            top += 8ull * n;
+        }
         FieldJob& F = fj[j];
         F.a = L.a;
         F.aff = (uint32_t)L.LA;
@@ -1830,13 +1913,22 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     }
     if (top >= (1ull << 31) || scr >= (1ull << 31) || lrow.size() >= (1ull << 31))
         throw InvalidArgument("batch too large");
+    std::vector<uint32_t> pairs;
+    for (size_t k = 0; k < scat.size(); ++k) {
+        pairs.push_back((uint32_t)(jl[scat[k].first].R0 + scat_rel[k]));
+        pairs.push_back((uint32_t)scat[k].second);
+    }
     // MSM launches: the linear fields (dynamo, wires, consistency, public
-    // quotient, public differences), the affected-set fields, the G2 fields
+    // quotient, public differences); the affected-set fields and re-anchor
+    // quotients; the G2 fields
     MsmBuild m1, m2, m3;
     std::vector<CopyDesc> cp;
     std::vector<VerifyJob> vj(B);
+    std::vector<RebaseJob> rj;
+    std::vector<uint64_t> off{0};
     uint8_t* out = out_.as<uint8_t>((uint64_t)B * JOB_BYTES);
     auto fo = [&](int f) { return P.fam_off[f]; };
+    uint64_t terms = 0, fresh = 0;
     for (uint32_t j = 0; j < B; ++j) {
         const JL& L = jl[j];
         Session& S = *jobs[j]->S;
@@ -1881,7 +1973,20 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         m1.end(rec + SIDE_PDIFF);
         cp.push_back({R + D_W, R + D_DYN + 64 * DY_IZ, 64});
         cp.push_back({R + D_H, R + D_DYN + 64 * DY_IH, 64});
-        // affected-set fields
+        if (L.rb) {
+            // s5 of the delta (G2) and the new multiplication quotient
+            m3.seg(1, L.LSN[4], P.fam2_off[F2_LAG], 0, L.LS[4]);
+            m3.end(rec + D_AFF2);
+            m2.seg(0, n - 1, fo(F_KZG), L.R0 + 7ull * n, 0);
+            m2.end(rec + REC_ANCHOR + A_MQ);
+            rj.push_back({R, S.d_anchor.view<uint8_t>()});
+            vj[j] = VerifyJob{R, R + REC_ANCHOR, 0, (uint32_t)terms, (uint32_t)fresh, j};
+            terms += ANCHOR_TERMS;
+            fresh += 1;
+            for (uint32_t c : eq_terms(false)) off.push_back(off.back() + c);
+            continue;
+        }
+        // affected-set fields of a sparse proof
         const uint32_t a = L.a;
         const uint64_t FO = L.FO;
         m2.seg(0, a + 1, fo(F_KZG), FO + 0, 0);
@@ -1920,9 +2025,11 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         }
         m3.seg(0, a, P.fam2_off[F2_KZG], FO + 17 * a + 1, 0);
         m3.end(rec + D_US5);
-        vj[j] = VerifyJob{R, S.d_anchor.view<uint8_t>(), 1, j * DELTA_TERMS, 3 * j, j};
+        vj[j] = VerifyJob{R, S.d_anchor.view<uint8_t>(), 1, (uint32_t)terms, (uint32_t)fresh, j};
+        terms += DELTA_TERMS;
+        fresh += 3;
+        for (uint32_t c : eq_terms(true)) off.push_back(off.back() + c);
     }
-    const std::vector<uint64_t> off = eq_offsets(B, true);
     // the session's [public]_h goes to each record's input slot
     std::vector<uint8_t> pubh(64ull * B);
     for (uint32_t j = 0; j < B; ++j) memcpy(&pubh[64ull * j], jobs[j]->S->public_h, 64);
@@ -1931,8 +2038,8 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     m2.stage(stg);
     m3.stage(stg);
     const size_t at_lrow = stg.add(lrow), at_lsc = stg.add(lsc), at_fj = stg.add(fj), at_kj = stg.add(kjob),
-                 at_vj = stg.add(vj), at_off = stg.add(off), at_pub = stg.add(pubh);
-    // copies of the public_h inputs need device addresses: appended after upload
+                 at_vj = stg.add(vj), at_off = stg.add(off), at_pub = stg.add(pubh), at_pairs = stg.add(pairs),
+                 at_rj = stg.add(rj);
     upload(stg);
     const uint8_t* d = stage_.view<uint8_t>();
     std::vector<CopyDesc> cp0;
@@ -1947,7 +2054,8 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     Fr* arena = arena_.as<Fr>(std::max<uint64_t>(1, top));
     Fr* scratch = scr_.as<Fr>(std::max<uint64_t>(1, scr));
     uint32_t* status = status_.as<uint32_t>(B);
-    uint8_t* verd = verdicts_.as<uint8_t>((uint64_t)B * DELTA_EQS);
+    const uint64_t eqs = off.size() - 1;
+    uint8_t* verd = verdicts_.as<uint8_t>(std::max<uint64_t>(1, eqs));
     uint32_t* err = err_.as<uint32_t>(3);
     if (!ain.empty()) {
         Canon* h = parena_.as<Canon>(ain.size());
@@ -1964,6 +2072,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     tscalar_.as<uint32_t>(maxterms);
     const uint32_t* d_lrow = reinterpret_cast<const uint32_t*>(d + at_lrow);
     const uint32_t* d_lsc = reinterpret_cast<const uint32_t*>(d + at_lsc);
+    stat_fme_ += (uint64_t)(m1.fme + m2.fme + 3 * m3.fme);
     run_msm<Fq>(ws1_, P.table.view<G1A>(), m1, d, d_lrow, d_lsc, arena, out, err);
     // field work of the affected sets
     FieldCtx c{reinterpret_cast<const FieldJob*>(d + at_fj), reinterpret_cast<const uint32_t*>(d + at_kj), B, d_lrow,
@@ -1982,6 +2091,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     }
     k_dv_vanish<<<B, 256, (amax + 1) * sizeof(Fr), st>>>(c);
     DV_LAUNCH();
+    bool dense = false;
     if (K) {
         k_dv_lagmat<<<(K + 127) / 128, 128, 0, st>>>(c);
         DV_LAUNCH();
@@ -2010,6 +2120,59 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         ntt_batch_enqueue(nb_inv_, st);
         k_dv_degcheck<<<(unsigned)((3ull * n * B + 255) / 256), 256, 0, st>>>(c);
         DV_LAUNCH();
+        dense = true;
+    }
+    // re-anchors: new coefficients s_t + delta_t, then (s4 s5 - s6) / (X^n - 1)
+    bool rebuild = false;
+    std::vector<std::pair<uint32_t, Fr*>> coefs;  // job, new coefficient buffer
+    for (uint32_t j = 0; j < B; ++j)
+        if (jl[j].rb) coefs.push_back({j, jobs[j]->new_coef.as<Fr>(3ull * n)});
+    if (!coefs.empty()) {
+        rebuild = true;
+        for (auto& jc : coefs)
+            DV_CUDA(cudaMemsetAsync(arena + jl[jc.first].R0, 0, 32ull * 3 * n, st));
+        if (!scat.empty()) {
+            k_dv_scatter<<<(unsigned)((scat.size() + 255) / 256), 256, 0, st>>>(
+                reinterpret_cast<const uint32_t*>(d + at_pairs), (uint32_t)scat.size(), arena);
+            DV_LAUNCH();
+        }
+        std::vector<NttBatchItem> r1, r2, r3;
+        for (auto& jc : coefs) {
+            uint8_t* base = reinterpret_cast<uint8_t*>(arena + jl[jc.first].R0);
+            for (int t = 0; t < 3; ++t) r1.push_back({base + 32ull * t * n, base + 32ull * t * n, (int)P.logn, NTT_INVERSE});
+            r2.push_back({base + 32ull * 3 * n, base + 32ull * 3 * n, (int)P.logn + 1, NTT_FORWARD});
+            r2.push_back({base + 32ull * 5 * n, base + 32ull * 5 * n, (int)P.logn + 1, NTT_FORWARD});
+            r3.push_back({base + 32ull * 3 * n, base + 32ull * 3 * n, (int)P.logn + 1, NTT_INVERSE});
+        }
+        if (P.logn) {  // a transform of one element is the identity
+            ntt_batch_prepare(b_->ntt, nb_r1_, r1, st);
+            ntt_batch_enqueue(nb_r1_, st);
+        }
+        const unsigned g3 = (unsigned)((3ull * n + 255) / 256), g2n = (unsigned)((2ull * n + 255) / 256);
+        for (auto& jc : coefs) {
+            Fr* rows = arena + jl[jc.first].R0;
+            k_dv_vadd<<<g3, 256, 0, st>>>(jc.second, jobs[jc.first]->S->d_coef.view<Fr>(), rows, 3ull * n);
+            DV_LAUNCH();
+            k_dv_pad<<<g2n, 256, 0, st>>>(jc.second, n, rows + 3ull * n, 2ull * n);
+            DV_LAUNCH();
+            k_dv_pad<<<g2n, 256, 0, st>>>(jc.second + n, n, rows + 5ull * n, 2ull * n);
+            DV_LAUNCH();
+        }
+        ntt_batch_prepare(b_->ntt, nb_r2_, r2, st);
+        ntt_batch_enqueue(nb_r2_, st);
+        for (auto& jc : coefs) {
+            Fr* rows = arena + jl[jc.first].R0;
+            k_dv_pmul<<<g2n, 256, 0, st>>>(rows + 3ull * n, rows + 5ull * n, 2ull * n);
+            DV_LAUNCH();
+        }
+        ntt_batch_prepare(b_->ntt, nb_r3_, r3, st);
+        ntt_batch_enqueue(nb_r3_, st);
+        for (auto& jc : coefs) {
+            Fr* rows = arena + jl[jc.first].R0;
+            k_dv_mq<<<(n + 255) / 256, 256, 0, st>>>(rows + 3ull * n, jc.second + 2ull * n, n, rows + 7ull * n,
+                                                     status + jc.first);
+            DV_LAUNCH();
+        }
     }
     run_msm<Fq>(ws1_, P.table.view<G1A>(), m2, d, d_lrow, d_lsc, arena, out, err + 1);
     run_msm<Fq2>(ws2_, P.table2.view<G2A>(), m3, d, d_lrow, d_lsc, arena, out, err + 2);
@@ -2017,19 +2180,33 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         k_dv_copy<<<dim3(1, (unsigned)cp.size()), 32, 0, st>>>((uint32_t)cp.size(), reinterpret_cast<const CopyDesc*>(d2 + at_cp));
         DV_LAUNCH();
     }
-    run_verify(P, B, 3ull * B, (uint64_t)B * DELTA_TERMS, (uint64_t)B * DELTA_EQS,
-               reinterpret_cast<const VerifyJob*>(d + at_vj), reinterpret_cast<const uint64_t*>(d + at_off), verd,
-               status);
+    if (!rj.empty()) {
+        const uint32_t tot = (uint32_t)rj.size() * REBASE_FIELDS;
+        k_dv_rebase<<<(tot + 63) / 64, 64, 0, st>>>(reinterpret_cast<const RebaseJob*>(d + at_rj), (uint32_t)rj.size());
+        DV_LAUNCH();
+    }
+    run_verify(P, B, fresh, terms, eqs, reinterpret_cast<const VerifyJob*>(d + at_vj),
+               reinterpret_cast<const uint64_t*>(d + at_off), verd, status);
+    for (auto& jc : coefs) {
+        uint8_t* an = jobs[jc.first]->new_anchor.as<uint8_t>(ANCHOR_BYTES);
+        DV_CUDA(cudaMemcpyAsync(an, out + (uint64_t)jc.first * JOB_BYTES + REC_ANCHOR, ANCHOR_BYTES,
+                                cudaMemcpyDeviceToDevice, st));
+    }
     const uint64_t ob = (uint64_t)B * JOB_BYTES;
-    uint8_t* hout = pout_.as<uint8_t>(ob + 4ull * B + 16 + (uint64_t)B * DELTA_EQS);
+    uint8_t* hout = pout_.as<uint8_t>(ob + 4ull * B + 16 + eqs);
     DV_CUDA(cudaMemcpyAsync(hout, out, ob, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaMemcpyAsync(hout + ob, status, 4ull * B, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B, err, 12, cudaMemcpyDeviceToHost, st));
-    DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B + 16, verd, (uint64_t)B * DELTA_EQS, cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B + 16, verd, eqs, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaStreamSynchronize(st));
-    if (K) {
+    if (dense) {
         ntt_batch_check(nb_fwd_, st);
         ntt_batch_check(nb_inv_, st);
+    }
+    if (rebuild) {
+        if (P.logn) ntt_batch_check(nb_r1_, st);
+        ntt_batch_check(nb_r2_, st);
+        ntt_batch_check(nb_r3_, st);
     }
     uint32_t herr[3];
     memcpy(herr, hout + ob + 4ull * B, 12);
@@ -2039,21 +2216,35 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         Job& J = *jobs[j];
         uint32_t hst;
         memcpy(&hst, hout + ob + 4ull * j, 4);
-        bool ok = hst == 0;
-        const uint8_t* v = hout + ob + 4ull * B + 16 + (uint64_t)j * DELTA_EQS;
-        for (uint32_t e = 0; e < DELTA_EQS; ++e) ok &= v[e] == 1;
-        J.ok = ok;
-        if (!ok)
-            J.error = hst & 1   ? "polynomial division has a nonzero remainder"
-                      : hst & 2 ? "anchor opening division has a nonzero remainder"
-                                : "sparse session proof failed verification";
+        const bool ok = hst == 0;
         const uint8_t* r = hout + (uint64_t)j * JOB_BYTES;
-        J.proof.resize(PROOF_BYTES);
-        memcpy(J.proof.data(), J.S->anchor_bytes.data(), ANCHOR_BYTES);
-        memcpy(J.proof.data() + ANCHOR_BYTES, r, DELTA_BYTES);
-        const uint64_t tail[3] = {1, J.S->anchor_generation, J.generation};
-        memcpy(J.proof.data() + ANCHOR_BYTES + DELTA_BYTES, tail, 24);
+        J.proof.assign(PROOF_BYTES, 0);
+        if (J.rebuild) {
+            J.anchor_bytes.assign(r + REC_ANCHOR, r + REC_ANCHOR + ANCHOR_BYTES);
+            memcpy(J.proof.data(), r + REC_ANCHOR, ANCHOR_BYTES);
+            const uint64_t tail[3] = {0, J.generation, J.generation};
+            memcpy(J.proof.data() + ANCHOR_BYTES + DELTA_BYTES, tail, 24);
+        } else {
+            memcpy(J.proof.data(), J.S->anchor_bytes.data(), ANCHOR_BYTES);
+            memcpy(J.proof.data() + ANCHOR_BYTES, r, DELTA_BYTES);
+            const uint64_t tail[3] = {1, J.S->anchor_generation, J.generation};
+            memcpy(J.proof.data() + ANCHOR_BYTES + DELTA_BYTES, tail, 24);
+        }
         memcpy(J.public_h, r + SIDE_PUBNEW, 64);
+        J.ok = ok;
+        J.error = hst & 1   ? "polynomial division has a nonzero remainder"
+                  : hst & 2 ? "anchor opening division has a nonzero remainder"
+                  : hst & 4 ? "multiplication relation is not divisible by X^n - 1"
+                            : (J.rebuild ? "updated proof failed public verification"
+                                         : "sparse session proof failed verification");
+    }
+    // verdicts: each job's equations are a contiguous range of `off`
+    uint64_t eq = 0;
+    for (uint32_t j = 0; j < B; ++j) {
+        const uint64_t cnt = jl[j].rb ? ANCHOR_EQS : DELTA_EQS;
+        const uint8_t* v = hout + ob + 4ull * B + 16 + eq;
+        for (uint64_t e = 0; e < cnt; ++e) jobs[j]->ok &= v[e] == 1;
+        eq += cnt;
     }
 }
 
@@ -2159,7 +2350,7 @@ bool Engine::verify_impl(uint64_t pid, const uint8_t* pubb, const uint8_t* proof
     const cudaStream_t st = st_;
     uint8_t* out = out_.as<uint8_t>(2 * JOB_BYTES);
     DV_CUDA(cudaMemsetAsync(out, 0, 2 * JOB_BYTES, st));
-    DV_CUDA(cudaMemcpyAsync(out, proof, ANCHOR_BYTES, cudaMemcpyHostToDevice, st));
+    DV_CUDA(cudaMemcpyAsync(out + REC_ANCHOR, proof, ANCHOR_BYTES, cudaMemcpyHostToDevice, st));
     DV_CUDA(cudaMemcpyAsync(out + JOB_BYTES, proof + ANCHOR_BYTES, DELTA_BYTES, cudaMemcpyHostToDevice, st));
     // every G1 / G2 field must parse (codec.rs:25-111): checked by converting
     // them all; the G2 fields of the layout are known
@@ -2197,8 +2388,8 @@ bool Engine::verify_impl(uint64_t pid, const uint8_t* pubb, const uint8_t* proof
     mb.seg(0, n, P->fam_off[F_PUBH], 0, 0);
     mb.end(has ? JOB_BYTES + SIDE_PDIFF : SIDE_PDIFF);
     std::vector<VerifyJob> vj;
-    vj.push_back(VerifyJob{out, out, has ? 2u : 0u, 0, 0, 0});
-    if (has) vj.push_back(VerifyJob{out + JOB_BYTES, out, 1, ANCHOR_TERMS, 1, 1});
+    vj.push_back(VerifyJob{out, out + REC_ANCHOR, has ? 2u : 0u, 0, 0, 0});
+    if (has) vj.push_back(VerifyJob{out + JOB_BYTES, out + REC_ANCHOR, 1, ANCHOR_TERMS, 1, 1});
     std::vector<uint64_t> off = eq_offsets(1, false);
     if (has) {
         const std::vector<uint64_t> d2 = eq_offsets(1, true);
@@ -2295,7 +2486,6 @@ void Engine::stage_job(Request& r, Session* S, Job& job) {
 void Engine::process(std::vector<Request>& batch, std::vector<Session*>& sess, std::vector<Outcome>& outs) {
     std::vector<Job> jobs(batch.size());
     std::map<Params*, std::vector<Job*>> groups;
-    std::vector<Job*> rebuilds;
     std::vector<bool> active(batch.size(), false);
     for (size_t r = 0; r < batch.size(); ++r) {
         if (!sess[r]) {
@@ -2315,15 +2505,10 @@ void Engine::process(std::vector<Request>& batch, std::vector<Session*>& sess, s
             continue;
         }
         active[r] = true;
-        if (jobs[r].rebuild) rebuilds.push_back(&jobs[r]);
-        else groups[sess[r]->P].push_back(&jobs[r]);
+        groups[sess[r]->P].push_back(&jobs[r]);  // sparse proofs and re-anchors share the batch
     }
     try {
         for (auto& g : groups) run_sparse(*g.first, g.second);
-        for (Job* j : rebuilds) {
-            run_anchor(*j->S->P, j->witness, j->pub, *j);
-            if (!j->ok) j->error = "updated proof failed public verification (" + j->error + ")";
-        }
     } catch (const InvalidArgument& e) {
         for (size_t r = 0; r < batch.size(); ++r)
             if (active[r]) {
