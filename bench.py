@@ -798,6 +798,62 @@ def valid_witness(n, seed):
     return pub, w
 
 
+def bench_trapdoors(sizes, seed=9900):
+    """Seeded trapdoor pairs per circuit size, drawn until they meet the
+    setup's rejection rules (srs.rs:158-178): nonzero, distinct, outside the
+    8n-point domain, tau_x != tau_y^8."""
+    import random
+    rng = random.Random(seed)
+    out = {}
+    for n in sorted(set(sizes)):
+        m = 8 * n
+        while True:
+            tx, ty = rng.randrange(1, R_FR), rng.randrange(1, R_FR)
+            if tx != ty and pow(tx, m, R_FR) != 1 and pow(ty, m, R_FR) != 1 and tx != pow(ty, 8, R_FR):
+                out[n] = (tx, ty)
+                break
+    return out
+
+
+def proofs_cpu(sizes, wit, reqs, threads, budget_s):
+    """The CPU restatement of the reference's sparse update path (oracle,
+    bases route: sparse MSMs over the SRS points, the subproduct tree,
+    FFT products and exact division, then the pairing verifier) on the
+    stream's requests of session 0, until budget_s of timed work.  Setup is
+    not timed: the SRS points, and the session's anchor and opening cache
+    from the trapdoor scalars (identical values).  Updates that re-anchor
+    are left out of the sample (on the CPU the dense anchor and its opening
+    cache take minutes at n = 65536), so the rate counts sparse proofs
+    only."""
+    from oracle import dynaverse as D
+    n = sizes[0]
+    tx, ty = bench_trapdoors(sizes)[n]
+    P = D.Params(n, tx, ty, "bases", threads=threads)
+    pub, w = wit[0]
+    S = D.Session(P, pub, w, verify=False, scalar_anchors=True)
+    times, rebuilds, seen = [], 0, 0
+    for j, idx, vals in reqs:
+        if j != 0:
+            continue
+        seen += 1
+        values = [int.from_bytes(vals[32 * i:32 * i + 32], "little") for i in range(len(idx))]
+        t0 = time.perf_counter()
+        S.update(idx, values, verify=True)
+        dt = time.perf_counter() - t0
+        if S.last_rebuilt:
+            rebuilds += 1
+        else:
+            times.append(dt)
+        if sum(times) >= budget_s:
+            break
+    if not times:
+        return None, "no sparse update of session 0 in the stream"
+    rate = len(times) / sum(times)
+    return rate, (f"{len(times)} sparse update proofs of session 0 (n = {n}) in stream order, each proved by the "
+                  f"oracle's restatement of the reference's steps and verified with its pairing checks "
+                  f"({rebuilds} re-anchoring updates of that session left out)")
+
+
 def proof_stream(sizes, witnesses, count, umax, seed):
     """The seeded update stream of the serving workload: a session, a support
     of floor(2^U) gates (U ~ U[0, umax], capped at n), half in the session's
@@ -857,15 +913,10 @@ class ProofServeOp:
     def _setup(self, dv):
         import random
         self.eng = dv.DynaverseEngine(150 << 30, 64)
-        rng = random.Random(9900)
-        self.params = {}
-        for n in sorted(set(self.sizes)):
-            while True:
-                try:
-                    self.params[n] = self.eng.params_create(n, rng.randrange(1, R_FR), rng.randrange(1, R_FR))
-                    break
-                except dv.DvgpuError:
-                    continue
+        self.params = {n: self.eng.params_create(n, tx, ty) for n, (tx, ty) in bench_trapdoors(self.sizes).items()}
+        self._inputs()
+
+    def _inputs(self):
         self.wit = [valid_witness(n, 9000 + j) for j, n in enumerate(self.sizes)]
         self.pub_b = [b"".join(v.to_bytes(32, "little") for v in p) for p, _ in self.wit]
         self.wit_b = [b"".join(v.to_bytes(32, "little") for v in w) for _, w in self.wit]
@@ -947,6 +998,12 @@ class ProofServeOp:
             "gpu_launches": sat_served["launches"], "clocks": clocks,
         }
         self.eng.close()
+        if not args.no_cpu_baseline and world == 1:
+            threads = os.cpu_count() or 1
+            rate, sample = proofs_cpu(self.sizes, self.wit, self.reqs, threads, 20.0)
+            if rate is not None:
+                line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
+                                        "sample": sample}
         return line
 
 
@@ -1431,6 +1488,24 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     op = args.op
     n = 1 << args.log_n
+    if op == "proofs":
+        p = ProofServeOp(args)
+        p._inputs()
+        steps = max(1, args.steps)
+        rates, sample = [], None
+        for _ in range(steps):
+            rate, sample = proofs_cpu(p.sizes, p.wit, p.reqs, threads, 30.0 / steps)
+            if rate is not None:
+                rates.append(rate)
+        value = sum(rates) / len(rates) if rates else None
+        print(json.dumps({"impl": "reference", "metric": p.metric, "value": value, "unit": "proofs/s",
+                          "n_gpus": 1, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
+                          "config": {"workload": p.workload, "op": "proofs"},
+                          "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port",
+                                           "sample": sample},
+                          "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
     if op in ("msm", "msmres", "g2msm"):
         g2 = op == "g2msm"
         tau = oracle.uniform_fr(2812, 1)

@@ -803,7 +803,7 @@ static Fe root_of_unity(size_t n) {
 // G1Projective, as called by RebuildBackend::transform_rows,
 // crates/protocol/src/incremental_rebuild/operators.rs:413-440): the same
 // radix-2 butterflies as ntt_inplace with the twiddle acting on the point.
-static void g1_fft_inplace(std::vector<Jac<OpsFq>>& a, const Fe& omega) {
+static void g1_fft_inplace(std::vector<Jac<OpsFq>>& a, const Fe& omega, int threads = 1) {
     size_t n = a.size();
     int logn = 0;
     while (((size_t)1 << logn) < n) ++logn;
@@ -818,18 +818,21 @@ static void g1_fft_inplace(std::vector<Jac<OpsFq>>& a, const Fe& omega) {
         std::vector<Fe> tw(len / 2);
         tw[0] = FR.one;
         for (size_t j = 1; j < len / 2; ++j) fmul(FR, tw[j], tw[j - 1], wlen);
-        for (size_t i = 0; i < n; i += len) {
-            for (size_t j = 0; j < len / 2; ++j) {
+        // the n/2 butterflies of a stage are independent: split them over threads
+        const size_t half = len / 2;
+        parallel_for(n / 2, threads, [&](size_t lo, size_t hi) {
+            for (size_t b = lo; b < hi; ++b) {
+                const size_t i = (b / half) * len, j = b % half;
                 uint64_t k[4];
                 from_mont(FR, k, tw[j]);
                 const Jac<OpsFq> u = a[i + j];
-                const Jac<OpsFq> v = mul_bits_jac(a[i + j + len / 2], k, 256);
+                const Jac<OpsFq> v = mul_bits_jac(a[i + j + half], k, 256);
                 jac_add(a[i + j], u, v);
                 Jac<OpsFq> nv;
                 jac_neg(nv, v);
-                jac_add(a[i + j + len / 2], u, nv);
+                jac_add(a[i + j + half], u, nv);
             }
-        }
+        });
     }
 }
 
@@ -1364,7 +1367,7 @@ int oracle_g1_fft(const uint8_t* points, size_t n, size_t rows, int inverse, uin
             g1_read(points + 64 * (r * n + i), p);
             a[i] = p.inf ? jac_zero<OpsFq>() : Jac<OpsFq>{p.x, p.y, OpsFq::one()};
         }
-        if (n > 1) g1_fft_inplace(a, w);
+        if (n > 1) g1_fft_inplace(a, w, rows == 1 ? num_threads(threads) : 1);
         if (inverse)
             for (auto& v : a) v = mul_bits_jac(v, ninv_c, 256);
         std::vector<Aff<OpsFq>> aff(n);
@@ -1373,6 +1376,28 @@ int oracle_g1_fft(const uint8_t* points, size_t n, size_t rows, int inverse, uin
       }
     });
     return 0;
+}
+
+// out_i = [s_i] P_i for n points (wire form; infinity all zero).
+int oracle_g1_scale(const uint8_t* points, const uint8_t* scalars, size_t n, uint8_t* out, int threads) {
+    std::atomic<int> bad{0};
+    parallel_for(n, num_threads(threads), [&](size_t lo, size_t hi) {
+        std::vector<Jac<OpsFq>> acc(hi - lo);
+        for (size_t i = lo; i < hi; ++i) {
+            Aff<OpsFq> p;
+            uint64_t k[4];
+            if (!g1_read(points + 64 * i, p) || !read_canon(scalars + 32 * i, k, R_LIMBS)) {
+                bad = 1;
+                acc[i - lo] = jac_zero<OpsFq>();
+                continue;
+            }
+            acc[i - lo] = p.inf ? jac_zero<OpsFq>() : mul_bits(p, k, 256);
+        }
+        std::vector<Aff<OpsFq>> aff(hi - lo);
+        batch_to_aff(acc.data(), aff.data(), hi - lo);
+        for (size_t i = lo; i < hi; ++i) g1_write(out + 64 * i, aff[i - lo]);
+    });
+    return bad ? -1 : 0;
 }
 
 int oracle_ntt(uint8_t* values, size_t n, int kind) {

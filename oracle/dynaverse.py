@@ -375,47 +375,39 @@ class Params:
 
     # ------------------------------------------------------------ bases route setup
     def _build_bases(self):
-        """SRS points from the base scalars (setup.rs:13-31).  The dense
-        families span the big domain m; only their first 7n entries can be
-        reached by a proof, but the dense anchor MSMs of the reference run
-        over all m, so the full vectors are built here."""
+        """SRS points from the base scalars (setup.rs:13-31).  The reference's
+        dense families span the big domain m, but a witness is zero from 6n
+        on and its Dynamo h from 7n on, so every MSM of a proof touches only
+        the families' first 6n (7n for ly) bases: those are built.  The KZG
+        G1 powers span m (the anchor commits the m interpolation
+        coefficients of the padded witness); G2 commitments span at most n + 1."""
         n, m = self.n, self.m
         th = self.threads
         f1 = lambda s: _split(O.fixed_base_g1(frs(s), th), 64)
-        lx_full = lagrange_values(self.tx, m)
-        ly_full = lagrange_values(self.ty, m)
-        y_full = [(ly_full[i] - ly_full[sigma(n, i)]) % R for i in range(m)]
-        inv_m = inv(m)
-        xv_inv = inv(self.txm - 1)
-        tx_inv = inv(self.tx)
+        six = 6 * n
         self.B = {}
-        self.B["lx"] = f1(lx_full)
-        self.B["ly"] = f1(ly_full)
-        self.B["alpha"] = f1([lx_full[i] * (self.u - y_full[i]) % R * xv_inv for i in range(m)])
-        common = [y_full[i] * (lx_full[i] - inv_m) % R for i in range(m)]
-        self.B["beta"] = f1([c * tx_inv for c in common])
-        self.B["z"] = f1([self.tym * l for l in lx_full])
-        self.B["h"] = f1([self.txm * y for y in y_full])
-        self.B["b"] = f1([c * self.tx for c in common])
-        z_in_inv = [inv(z) for z in self.z_in]
+        self.B["lx"] = f1(self.lx[:six])
+        self.B["ly"] = f1(self.ly)
+        self.B["alpha"] = f1(self.alpha[:six])
+        self.B["beta"] = f1(self.beta[:six])
+        self.B["z"] = f1(self.zb[:six])
+        self.B["h"] = f1(self.hb[:six])
+        self.B["b"] = f1(self.bb[:six])
         for t in range(6):
-            col = []
-            for i in range(m):
-                mapped = self.cx[i - t * n] if t * n <= i < (t + 1) * n else 0
-                col.append((lx_full[i] - mapped) * z_in_inv[t] % R)
-            self.B[f"qac{t}"] = f1(col)
+            self.B[f"qac{t}"] = f1(self.qac[t])
         self.B["qcd"] = f1(self.qcd)
         self.B["qbd"] = f1(self.qbd)
         self.B["d"] = f1(self.dd)
-        self.B["adeg"] = f1([l * self.tym for l in lx_full])
+        self.B["adeg"] = f1(self.adeg)
         self.B["bdeg"] = f1(self.bdeg)
         self.B["ddeg"] = f1(self.ddeg)
         self.B["lag"] = f1(self.lsx)
         self.B["open_u"] = f1(self.open_u)
         self.B["pq"] = f1(self.pq)
         self.kzg_g1 = O.fixed_base_g1(O.fr_powers(fr(self.tx), m), th)
-        self.kzg_g2 = O.fixed_base_g2(O.fr_powers(fr(self.tx), m), th)
+        self.kzg_g2 = O.fixed_base_g2(O.fr_powers(fr(self.tx), 2 * n), th)  # A has up to n + 1 coefficients
         self.lag_g2 = _split(O.fixed_base_g2(frs(self.lsx), th), 128)
+        self._prepared = None  # G1 transform of the powers for the opening cache (kzg.rs:248-275)
 
     # ------------------------------------------------------------ shared helpers
     def h_sparse(self, entries):
@@ -499,16 +491,17 @@ class Params:
         a.w_commitment, a.h_commitment = w_commitment, dyn[7]
         a.dynamo = dyn
         cons = []
+        full = padded[:6 * n]  # zero from 6n on
+        dense = lambda fam, vec: O.msm_g1(b"".join(self.B[fam][:len(vec)]), frs(vec), threads=self.threads)
+        adeg = dense("adeg", full)
         for t in range(6):
             sl = padded[t * n:(t + 1) * n]
-            dense = lambda fam, vec: O.msm_g1(b"".join(self.B[fam][:len(vec)]), frs(vec), threads=self.threads)
-            cons += [dense(f"qac{t}", padded), dense("qcd", sl), dense("qbd", sl), dense("d", sl),
-                     dense("adeg", padded), dense("bdeg", sl), dense("ddeg", sl)]
+            cons += [dense(f"qac{t}", full), dense("qcd", sl), dense("qbd", sl), dense("d", sl),
+                     adeg, dense("bdeg", sl), dense("ddeg", sl)]
         a.consistency = cons
-        # public quotient: w / I_x exactly (PreparedExactDivision, domain.rs:268-300)
-        ix = [1]
-        for i in range(6 * n, m):
-            ix = _pmul(ix, [(-pow(self.wm, i, R)) % R, 1])
+        # public quotient: w / I_x exactly (PreparedExactDivision, domain.rs:268-300),
+        # I_x by a balanced product tree (vanishing_polynomial_balanced, domain.rs:60-75)
+        ix = _product_tree([pow(self.wm, i, R) for i in range(6 * n, m)])
         qx = ints(O.poly_div_exact(frs(w_coeffs), frs(ix)))
         a.public_zero_quotient = self.commit(qx)
         prod = ints(O.poly_mul(frs(wire_coeffs[3]), frs(wire_coeffs[4])))
@@ -537,19 +530,36 @@ class Params:
         for t in range(3, 6):
             vals = w[t * n:(t + 1) * n]
             if self.route == "bases":
-                coeffs = ints(O.ntt(frs(vals), "inverse"))
-                col = []
-                for i in range(n):
-                    num = list(coeffs)
-                    num[0] = (num[0] - vals[i]) % R
-                    qt = ints(O.poly_div_exact(frs(num), frs([(-self.small_points[i]) % R, 1])))
-                    col.append(self.commit(qt))
+                col = self._single_openings(ints(O.ntt(frs(vals), "inverse")))
             else:
                 st = sum(v * l for v, l in zip(vals, self.lsx)) % R
                 invs = batch_inv([(self.tx - x) % R for x in self.small_points])
                 col = g1_of([(st - vals[i]) * invs[i] for i in range(n)])
             cache.append(col)
         return cache
+
+    def _single_openings(self, coeffs):
+        """KzgParams::precompute_single_openings (kzg.rs:207-246): the
+        Toeplitz product H_j = sum_(l > j) f_l [tau^(l-1-j)] as a circular
+        convolution (scalar FFT of the reversed coefficients times the group
+        FFT of the powers, one group IFFT), then a group FFT of H over the
+        n-point domain gives every opening [(f - f(x_i)) / (X - x_i)]."""
+        n = self.n
+        degree = len(coeffs) - 1
+        if degree == 0:
+            return [G1_ZERO] * n
+        conv = 1
+        while conv < 2 * degree - 1:
+            conv <<= 1
+        rev = list(reversed(coeffs[1:])) + [0] * (conv - degree)
+        scalar_fft = O.ntt(frs(rev), "forward")
+        if self._prepared is None or self._prepared[0] != degree:
+            powers = self.kzg_g1[:64 * degree] + G1_ZERO * (conv - degree)
+            self._prepared = (degree, O.g1_fft(powers, conv, False, threads=self.threads))
+        prod = O.g1_scale(self._prepared[1], scalar_fft, threads=self.threads)
+        h = O.g1_fft(prod, conv, True, threads=self.threads)
+        hs = _split(h[:64 * degree], 64)[::-1] + [G1_ZERO] * (n - degree)
+        return _split(O.g1_fft(b"".join(hs), n, False, threads=self.threads), 64)
 
     # ------------------------------------------------------------ sparse delta proof
     def prove_delta(self, anchor_w, entries, anchor_wires, cache):
@@ -878,23 +888,39 @@ def parse_proof(b: bytes) -> Proof:
 
 # ------------------------------------------------------------------ session
 class Session:
-    """UpdateSession (dynaverse/session.rs:10-142) over Params."""
+    """UpdateSession (dynaverse/session.rs:10-142) over Params.  With
+    scalar_anchors, anchors and opening caches (session start and
+    re-anchors) come from the scalar route even on the bases route, whose
+    sparse proofs and verifier then run on them: the values are identical
+    (tests/test_oracle_dynaverse.py), and the CPU baseline times the sparse
+    path without minutes of dense setup per anchor."""
 
-    def __init__(self, params: Params, pub, witness, verify=True):
+    def __init__(self, params: Params, pub, witness, verify=True, scalar_anchors=False):
         p = self.p = params
         n = p.n
         if len(pub) != n or len(witness) != 6 * n:
             raise ValueError("instance or witness length differs from circuit")
         check_gates(n, pub, witness, range(n))
+        self.scalar_anchors = scalar_anchors
         self.pub = list(pub)
         self.anchor = list(witness)
         self.current = list(witness)
-        a = p.prove_anchor(witness)
-        self.cache = p.opening_cache(witness) if p.route == "bases" else None
+        a, self.cache = self._anchor(witness)
         self.proof = Proof(a, None, 0, 0)
         if verify and not p.verify(self.pub, self.proof):
             raise AssertionError("initial session proof failed verification")
         self.delta = {}
+        self.last_rebuilt = False
+
+    def _anchor(self, w):
+        p = self.p
+        if self.scalar_anchors and p.route == "bases":
+            p.route = "scalar"
+            try:
+                return p.prove_anchor(w), p.opening_cache(w)
+            finally:
+                p.route = "bases"
+        return p.prove_anchor(w), (p.opening_cache(w) if p.route == "bases" else None)
 
     def anchor_distance(self):
         return len(self.delta)
@@ -936,13 +962,14 @@ class Session:
         if len(delta) >= p.rebuild_interval:
             # update_proof_backend's rebuild branch (dynaverse.rs:423-437)
             check_gates(n, pub, w, range(n))
-            a = p.prove_anchor(w)
+            a, cache = self._anchor(w)
             proof = Proof(a, None, generation, generation)
             if verify and not p.verify(pub, proof):
                 raise ValueError("updated proof failed public verification")
             self.anchor = list(w)
-            self.cache = p.opening_cache(w) if p.route == "bases" else None
+            self.cache = cache
             self.delta = {}
+            self.last_rebuilt = True
         else:
             entries = sorted(delta.items())
             d = p.prove_delta(self.anchor, entries, self.proof.anchor.wires, self.cache)
@@ -950,6 +977,7 @@ class Session:
             if verify and not p.verify(pub, proof):
                 raise ValueError("sparse session proof failed verification")
             self.delta = delta
+            self.last_rebuilt = False
         self.current, self.pub, self.proof = w, pub, proof
         return proof
 
@@ -957,6 +985,21 @@ class Session:
 # ------------------------------------------------------------------ small polynomial helpers
 def _split(b: bytes, size: int):
     return [b[i:i + size] for i in range(0, len(b), size)]
+
+
+def _product_tree(roots):
+    """prod (X - r) by pairwise products (the oracle's FFT poly_mul)."""
+    if not roots:
+        return [1]
+    level = [[(-r) % R, 1] for r in roots]
+    while len(level) > 1:
+        nxt = []
+        for i in range(0, len(level) - 1, 2):
+            nxt.append(ints(O.poly_mul(frs(level[i]), frs(level[i + 1]))))
+        if len(level) % 2:
+            nxt.append(level[-1])
+        level = nxt
+    return level[0]
 
 
 def _pmul(a, b):

@@ -36,6 +36,7 @@ def lib():
         L.oracle_sparse_msm_g1.argtypes = [u8p, sz, ctypes.c_void_p, u8p, sz, u8p, ctypes.c_int]
         L.oracle_ntt.argtypes = [u8p, sz, ctypes.c_int]
         L.oracle_g1_fft.argtypes = [u8p, sz, sz, ctypes.c_int, u8p, ctypes.c_int]
+        L.oracle_g1_scale.argtypes = [u8p, u8p, sz, u8p, ctypes.c_int]
         L.oracle_fixed_base_g1.argtypes = [u8p, sz, u8p, ctypes.c_int]
         L.oracle_fixed_base_g2.argtypes = [u8p, sz, u8p, ctypes.c_int]
         L.oracle_g2_check.argtypes = [u8p, sz, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int]
@@ -108,6 +109,16 @@ def g1_fft(points: bytes, n: int, inverse=False, threads=0) -> bytes:
     out = _buf(64 * n * rows)
     assert lib().oracle_g1_fft(points, n, rows, int(inverse), out, threads) == 0
     return out.raw
+
+
+def g1_scale(points: bytes, scalars: bytes, threads=0) -> bytes:
+    """[s_i] P_i for each point (wire form)."""
+    n = len(scalars) // 32
+    assert len(points) == 64 * n
+    out = _buf(max(1, 64 * n))
+    if lib().oracle_g1_scale(points, scalars, n, out, threads) != 0:
+        raise ValueError("oracle: bad point or scalar")
+    return out.raw[:64 * n]
 
 
 def ntt(values: bytes, kind="forward") -> bytes:
