@@ -57,7 +57,7 @@ resident.rs:419-431, infinity all zero):
                         updated_s5_g2 | anchor_openings s4..s6 |
                         changed_openings s4..s6 | unaffected_zero s4..s6 |
                         local_multiplication_quotient
-  DynaverseProof 9304 B anchor | u64 has_delta | delta (zero when absent) |
+  DynaverseProof 9304 B anchor | delta (zero when absent) | u64 has_delta |
                         u64 anchor_generation | u64 generation  (LE)
 """
 import struct
@@ -71,7 +71,7 @@ G1_ZERO = bytes(64)
 G2_ZERO = bytes(128)
 ANCHOR_BYTES = 3968
 DELTA_BYTES = 5312
-PROOF_BYTES = ANCHOR_BYTES + 8 + DELTA_BYTES + 16
+PROOF_BYTES = ANCHOR_BYTES + DELTA_BYTES + 24
 
 
 # ------------------------------------------------------------------ field
@@ -844,8 +844,8 @@ class Proof:
 
     def to_bytes(self) -> bytes:
         d = self.delta.to_bytes() if self.delta is not None else bytes(DELTA_BYTES)
-        return self.anchor.to_bytes() + struct.pack("<Q", 1 if self.delta is not None else 0) + d + \
-            struct.pack("<QQ", self.anchor_generation, self.generation)
+        return self.anchor.to_bytes() + d + \
+            struct.pack("<QQQ", 1 if self.delta is not None else 0, self.anchor_generation, self.generation)
 
 
 def parse_proof(b: bytes) -> Proof:
@@ -865,7 +865,6 @@ def parse_proof(b: bytes) -> Proof:
     a.dynamo = [g() for _ in range(8)]
     a.consistency = [g() for _ in range(42)]
     a.public_zero_quotient, a.multiplication_quotient = g(), g()
-    has = struct.unpack("<Q", take(8))[0]
     d = DeltaFields()
     d.changed_wires = [g() for _ in range(6)]
     d.changed_w, d.changed_h = g(), g()
@@ -882,7 +881,7 @@ def parse_proof(b: bytes) -> Proof:
     d.changed_openings = [g() for _ in range(3)]
     d.unaffected_zero = [g() for _ in range(3)]
     d.local_quotient = g()
-    ag, gen = struct.unpack("<QQ", take(16))
+    has, ag, gen = struct.unpack("<QQQ", take(24))
     return Proof(a, d if has else None, ag, gen)
 
 

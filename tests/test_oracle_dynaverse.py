@@ -130,12 +130,12 @@ def test_verifier_rejects_any_replaced_field(params8):
     assert pb.verify(pub, D.parse_proof(good))
     g = D.g1_gen()
     # replace G1 fields across the anchor and the delta (offsets of 64-byte slots)
-    for off in (0, 6 * 64 + 128, 3968 + 8, 3968 + 8 + 9 * 64, 3968 + 8 + 59 * 64, D.PROOF_BYTES - 16 - 64):
+    for off in (0, 6 * 64 + 128, 3968, 3968 + 9 * 64, 3968 + 59 * 64, D.PROOF_BYTES - 24 - 64):
         bad = bytearray(good)
         bad[off:off + 64] = g if bytes(bad[off:off + 64]) != g else bytes(64)
         assert not pb.verify(pub, D.parse_proof(bytes(bad))), off
     bad = bytearray(good)
-    bad[3968 + 8 + 60 * 64] ^= 1  # affected_g2 moved off the twist curve
+    bad[3968 + 60 * 64] ^= 1  # affected_g2 moved off the twist curve
     assert not pb.verify(pub, D.parse_proof(bytes(bad)))
     wrong_pub = list(pub)
     wrong_pub[0] = (wrong_pub[0] + 1) % R

@@ -2055,6 +2055,38 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     Fr* scratch = scr_.as<Fr>(std::max<uint64_t>(1, scr));
     uint32_t* status = status_.as<uint32_t>(B);
     const uint64_t eqs = off.size() - 1;
+    // Every NTT batch of this pipeline is prepared before the first launch:
+    // preparing synchronises the stream, which mid-pipeline would stall the
+    // host behind the queued work and leave the GPU idle meanwhile.
+    std::vector<std::pair<uint32_t, Fr*>> coefs;  // re-anchor jobs and their new coefficient buffers
+    for (uint32_t j = 0; j < B; ++j)
+        if (jl[j].rb) coefs.push_back({j, jobs[j]->new_coef.as<Fr>(3ull * n)});
+    const bool dense = kjob[B] > 0, rebuild = !coefs.empty();
+    {
+        std::vector<NttBatchItem> fwd, inv, r1, r2, r3;
+        for (uint32_t j = 0; j < B; ++j) {
+            if (!jl[j].a) continue;
+            uint8_t* base = reinterpret_cast<uint8_t*>(arena + jl[j].DN);
+            for (int r = 0; r < 4; ++r) fwd.push_back({base + 32ull * r * n, base + 32ull * r * n, (int)P.logn, NTT_COSET_FORWARD});
+            for (int r = 0; r < 3; ++r) inv.push_back({base + 32ull * r * n, base + 32ull * r * n, (int)P.logn, NTT_COSET_INVERSE});
+        }
+        for (auto& jc : coefs) {
+            uint8_t* base = reinterpret_cast<uint8_t*>(arena + jl[jc.first].R0);
+            for (int t = 0; t < 3; ++t) r1.push_back({base + 32ull * t * n, base + 32ull * t * n, (int)P.logn, NTT_INVERSE});
+            r2.push_back({base + 32ull * 3 * n, base + 32ull * 3 * n, (int)P.logn + 1, NTT_FORWARD});
+            r2.push_back({base + 32ull * 5 * n, base + 32ull * 5 * n, (int)P.logn + 1, NTT_FORWARD});
+            r3.push_back({base + 32ull * 3 * n, base + 32ull * 3 * n, (int)P.logn + 1, NTT_INVERSE});
+        }
+        if (dense) {
+            ntt_batch_prepare(b_->ntt, nb_fwd_, fwd, st);
+            ntt_batch_prepare(b_->ntt, nb_inv_, inv, st);
+        }
+        if (rebuild) {
+            if (P.logn) ntt_batch_prepare(b_->ntt, nb_r1_, r1, st);  // a transform of one element is the identity
+            ntt_batch_prepare(b_->ntt, nb_r2_, r2, st);
+            ntt_batch_prepare(b_->ntt, nb_r3_, r3, st);
+        }
+    }
     uint8_t* verd = verdicts_.as<uint8_t>(std::max<uint64_t>(1, eqs));
     uint32_t* err = err_.as<uint32_t>(3);
     if (!ain.empty()) {
@@ -2091,7 +2123,6 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     }
     k_dv_vanish<<<B, 256, (amax + 1) * sizeof(Fr), st>>>(c);
     DV_LAUNCH();
-    bool dense = false;
     if (K) {
         k_dv_lagmat<<<(K + 127) / 128, 128, 0, st>>>(c);
         DV_LAUNCH();
@@ -2105,30 +2136,15 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         const uint64_t t4 = 4ull * n * B;
         k_dv_numer<<<(unsigned)((t4 + 255) / 256), 256, 0, st>>>(c);
         DV_LAUNCH();
-        std::vector<NttBatchItem> fwd, inv;
-        for (uint32_t j = 0; j < B; ++j) {
-            if (!jl[j].a) continue;
-            uint8_t* base = reinterpret_cast<uint8_t*>(arena + jl[j].DN);
-            for (int r = 0; r < 4; ++r) fwd.push_back({base + 32ull * r * n, base + 32ull * r * n, (int)P.logn, NTT_COSET_FORWARD});
-            for (int r = 0; r < 3; ++r) inv.push_back({base + 32ull * r * n, base + 32ull * r * n, (int)P.logn, NTT_COSET_INVERSE});
-        }
-        ntt_batch_prepare(b_->ntt, nb_fwd_, fwd, st);
         ntt_batch_enqueue(nb_fwd_, st);
         k_dv_divq<<<(unsigned)(((uint64_t)n * B + 255) / 256), 256, 0, st>>>(c);
         DV_LAUNCH();
-        ntt_batch_prepare(b_->ntt, nb_inv_, inv, st);
         ntt_batch_enqueue(nb_inv_, st);
         k_dv_degcheck<<<(unsigned)((3ull * n * B + 255) / 256), 256, 0, st>>>(c);
         DV_LAUNCH();
-        dense = true;
     }
     // re-anchors: new coefficients s_t + delta_t, then (s4 s5 - s6) / (X^n - 1)
-    bool rebuild = false;
-    std::vector<std::pair<uint32_t, Fr*>> coefs;  // job, new coefficient buffer
-    for (uint32_t j = 0; j < B; ++j)
-        if (jl[j].rb) coefs.push_back({j, jobs[j]->new_coef.as<Fr>(3ull * n)});
-    if (!coefs.empty()) {
-        rebuild = true;
+    if (rebuild) {
         for (auto& jc : coefs)
             DV_CUDA(cudaMemsetAsync(arena + jl[jc.first].R0, 0, 32ull * 3 * n, st));
         if (!scat.empty()) {
@@ -2136,18 +2152,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
                 reinterpret_cast<const uint32_t*>(d + at_pairs), (uint32_t)scat.size(), arena);
             DV_LAUNCH();
         }
-        std::vector<NttBatchItem> r1, r2, r3;
-        for (auto& jc : coefs) {
-            uint8_t* base = reinterpret_cast<uint8_t*>(arena + jl[jc.first].R0);
-            for (int t = 0; t < 3; ++t) r1.push_back({base + 32ull * t * n, base + 32ull * t * n, (int)P.logn, NTT_INVERSE});
-            r2.push_back({base + 32ull * 3 * n, base + 32ull * 3 * n, (int)P.logn + 1, NTT_FORWARD});
-            r2.push_back({base + 32ull * 5 * n, base + 32ull * 5 * n, (int)P.logn + 1, NTT_FORWARD});
-            r3.push_back({base + 32ull * 3 * n, base + 32ull * 3 * n, (int)P.logn + 1, NTT_INVERSE});
-        }
-        if (P.logn) {  // a transform of one element is the identity
-            ntt_batch_prepare(b_->ntt, nb_r1_, r1, st);
-            ntt_batch_enqueue(nb_r1_, st);
-        }
+        if (P.logn) ntt_batch_enqueue(nb_r1_, st);
         const unsigned g3 = (unsigned)((3ull * n + 255) / 256), g2n = (unsigned)((2ull * n + 255) / 256);
         for (auto& jc : coefs) {
             Fr* rows = arena + jl[jc.first].R0;
@@ -2158,14 +2163,12 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
             k_dv_pad<<<g2n, 256, 0, st>>>(jc.second + n, n, rows + 5ull * n, 2ull * n);
             DV_LAUNCH();
         }
-        ntt_batch_prepare(b_->ntt, nb_r2_, r2, st);
         ntt_batch_enqueue(nb_r2_, st);
         for (auto& jc : coefs) {
             Fr* rows = arena + jl[jc.first].R0;
             k_dv_pmul<<<g2n, 256, 0, st>>>(rows + 3ull * n, rows + 5ull * n, 2ull * n);
             DV_LAUNCH();
         }
-        ntt_batch_prepare(b_->ntt, nb_r3_, r3, st);
         ntt_batch_enqueue(nb_r3_, st);
         for (auto& jc : coefs) {
             Fr* rows = arena + jl[jc.first].R0;
