@@ -139,8 +139,7 @@ def test_served_batches_equal_per_call_proofs(engine, dv):
         pub, w = D.valid_instance(n)
         s, _ = engine.open_session(ph, pub, w)
         sessions.append((n, s, D.Session(P, pub, w)))
-    expected = {}
-    tickets = []
+    expected, updates = {}, []
     for step in range(3):
         for k, (n, s, ref) in enumerate(sessions):
             gates = rng.choice(n, size=1 + step % 2, replace=False)
@@ -151,7 +150,9 @@ def test_served_batches_equal_per_call_proofs(engine, dv):
                 idx += ii
                 v += vv
             expected[(k, step)] = ref.update(idx, v).to_bytes()
-            tickets.append(((k, step), engine.submit(s, idx, v)))
+            updates.append(((k, step), s, idx, v))
+    # all submitted at once: while one batch is on the GPU the rest queue up
+    tickets = [(key, engine.submit(s, idx, v)) for key, s, idx, v in updates]
     batches = set()
     for key, t in tickets:
         proof, res = engine.wait(t)

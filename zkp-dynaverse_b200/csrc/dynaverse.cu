@@ -79,6 +79,11 @@ namespace dv {
 void pairing_check_device(Backend& b, const G1A* p, uint64_t terms, const G2A* q, uint64_t nq,
                           const uint32_t* d_qidx, const uint64_t* d_off, uint64_t equations, uint8_t* d_verdicts,
                           cudaStream_t st);
+uint64_t pairing_prepared_bytes();
+void pairing_prepare_device(const G2A* q, uint64_t nq, void* lines, uint32_t* qinf, cudaStream_t st);
+void pairing_check_prepared(Backend& b, const G1A* p, uint64_t terms, const void* lines, const uint32_t* qinf,
+                            const uint32_t* d_qidx, const uint64_t* d_off, uint64_t equations, uint8_t* d_verdicts,
+                            cudaStream_t st);
 
 namespace {
 
@@ -285,6 +290,10 @@ uint64_t now_ns() {
 
 // ================================================================ layout
 constexpr int TC = 8, TW = 32;  // window table: c = 8, 32 windows
+// The dense sets (anchor openings, a re-anchor's multiplication quotient)
+// run over the first n KZG bases with wider windows: c = 16 halves their
+// additions and digits against the c = 8 table at 2^15 buckets a set.
+constexpr int TCD = 16, TWD = 16;
 constexpr uint64_t ANCHOR_BYTES = 3968, DELTA_BYTES = 5312;
 constexpr uint64_t PROOF_BYTES = DVGPU_DYNAVERSE_PROOF_BYTES;
 static_assert(PROOF_BYTES == ANCHOR_BYTES + DELTA_BYTES + 24, "proof layout");
@@ -765,7 +774,7 @@ __global__ void k_dv_degcheck(FieldCtx c) {
 // ---------------------------------------------------------------- verification
 // The pairing-product equations of verify_traced (dynaverse.rs:1018-1119;
 // dynamo_verify_with_checks, dynamo.rs:326-342; verify_six_with_checks /
-// verify_with_checks, consistency.rs:49-114), one thread per proof, right-
+// verify_with_checks, consistency.rs:49-114), one warp per proof, right-
 // hand sides negated as product_equal does (verification.rs:80-92).  G2
 // terms index the batch's G2 array: the verifying-key constants (Vk2), then
 // each proof's own G2 points.
@@ -812,11 +821,14 @@ struct RebaseJob {
     uint8_t* rec;       // the job's record: delta fields, then the new anchor at REC_ANCHOR
     const uint8_t* old; // the current anchor proof bytes
 };
-__global__ void k_dv_rebase(const RebaseJob* __restrict__ jobs, uint32_t njobs) {
+// Fields [f0, f1) of every job (the G1 fields and the G2 field run on
+// different streams, each after the MSM that produces its delta).
+__global__ void k_dv_rebase(const RebaseJob* __restrict__ jobs, uint32_t njobs, uint32_t f0, uint32_t f1) {
+    const uint32_t w = f1 - f0;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= njobs * REBASE_FIELDS) return;
-    const RebaseJob J = jobs[i / REBASE_FIELDS];
-    const uint32_t f = i % REBASE_FIELDS;
+    if (i >= njobs * w) return;
+    const RebaseJob J = jobs[i / w];
+    const uint32_t f = f0 + i % w;
     uint64_t ao, dof;
     rebase_field(f, ao, dof);
     uint8_t* out = J.rec + REC_ANCHOR + ao;
@@ -848,90 +860,134 @@ DV_INL void emit_dynamo(Emit& e, const uint8_t* p) {
     e.t(ih, V_XM); e.t(h.neg(), V_G2);
     e.t(beta, V_X2); e.t(b.neg(), V_G2);
 }
-// Six slices: a = the big-domain commitment, wires at w, fields at c.
-DV_INL void emit_consistency(Emit& e, const G1A& a, const uint8_t* w, const uint8_t* c) {
-    for (int t = 0; t < 6; ++t) {
-        const uint8_t* s = c + 448 * t;
-        const G1A b = load_g1(w + 64 * t);
-        const G1A qac = load_g1(s), qcd = load_g1(s + 64), qbd = load_g1(s + 128), d = load_g1(s + 192),
-                  adeg = load_g1(s + 256), bdeg = load_g1(s + 320), ddeg = load_g1(s + 384);
-        e.t(g1_sub(a, d), V_G2); e.t(qac.neg(), V_ZIN0 + t); e.t(qcd.neg(), V_XMY);
-        e.t(g1_sub(b, d), V_G2); e.t(qbd.neg(), V_XMLY);
-        e.t(a, V_YM); e.t(adeg.neg(), V_G2);
-        e.t(b, V_YM); e.t(bdeg.neg(), V_G2);
-        e.t(d, V_XM); e.t(ddeg.neg(), V_G2);
-    }
+// Consistency slice t: a = the big-domain commitment, wires at w, fields at c.
+DV_INL void emit_slice(Emit& e, const G1A& a, const uint8_t* w, const uint8_t* c, int t) {
+    const uint8_t* s = c + 448 * t;
+    const G1A b = load_g1(w + 64 * t);
+    const G1A qac = load_g1(s), qcd = load_g1(s + 64), qbd = load_g1(s + 128), d = load_g1(s + 192),
+              adeg = load_g1(s + 256), bdeg = load_g1(s + 320), ddeg = load_g1(s + 384);
+    e.t(g1_sub(a, d), V_G2); e.t(qac.neg(), V_ZIN0 + t); e.t(qcd.neg(), V_XMY);
+    e.t(g1_sub(b, d), V_G2); e.t(qbd.neg(), V_XMLY);
+    e.t(a, V_YM); e.t(adeg.neg(), V_G2);
+    e.t(b, V_YM); e.t(bdeg.neg(), V_G2);
+    e.t(d, V_XM); e.t(ddeg.neg(), V_G2);
 }
+constexpr uint32_t DYNAMO_TERMS = 11, SLICE_TERMS = 11, TAIL_TERMS = DYNAMO_TERMS + 6 * SLICE_TERMS;
 
-__global__ void k_dv_terms(const VerifyJob* __restrict__ jobs, uint32_t njobs, G1A g1, G1A mvg1,
-                           G1A* __restrict__ p, uint32_t* __restrict__ qidx, G2A* __restrict__ q,
-                           uint32_t* __restrict__ status) {
+// Each job's own G2 points into q (the batch's G2 array, after the
+// verifying key): an anchor's s5 commitment; a delta's affected, unaffected
+// and updated-s5 commitments.  One thread per job.
+__global__ void k_dv_fresh(const VerifyJob* __restrict__ jobs, uint32_t njobs, G2A* __restrict__ q) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= njobs) return;
     const VerifyJob J = jobs[j];
-    Emit e{p + J.term, qidx + J.term, 0};
+    G2A* o = q + V_COUNT + J.fresh;
+    if (J.kind != 1) {
+        o[0] = load_g2(J.anchor + A_S5G2);
+    } else {
+        o[0] = load_g2(J.rec + D_AFF2);
+        o[1] = load_g2(J.rec + D_UNAFF2);
+        o[2] = load_g2(J.rec + D_US5);
+    }
+}
+
+// One warp per proof.  Every term has a fixed position, so the lanes write
+// their pieces independently: lane 0 the dynamo terms, lanes 1..6 the six
+// consistency slices, then the tail (the public-zero, multiplication and,
+// for a delta, the affected-set and opening equations) over lanes 7..13,
+// and the group identities and the new [public]_h on the last lane.  Each
+// affine normalisation takes a field inversion, so spreading them over the
+// lanes shortens the chain about tenfold.
+__global__ void k_dv_terms(const VerifyJob* __restrict__ jobs, uint32_t njobs, G1A g1, G1A mvg1,
+                           G1A* __restrict__ p, uint32_t* __restrict__ qidx, uint32_t* __restrict__ status) {
+    if (blockIdx.x >= njobs) return;
+    const uint32_t lane = threadIdx.x;
+    const VerifyJob J = jobs[blockIdx.x];
     const uint8_t* A = J.anchor;
     uint8_t* r = J.rec;
-    const G1X inf = G1X::inf();
+    const bool delta = J.kind == 1;
+    const uint8_t* dyn = delta ? r + D_DYN : A + A_DYN;
+    const uint8_t* wires = delta ? r + D_WIRES : A + A_WIRES;
+    auto at = [&](uint32_t k) { return Emit{p + J.term, qidx + J.term, k}; };
+    if (lane == 0) {
+        Emit e = at(0);
+        emit_dynamo(e, dyn);
+        return;
+    }
+    if (lane <= 6) {
+        Emit e = at(DYNAMO_TERMS + SLICE_TERMS * (lane - 1));
+        emit_slice(e, load_g1(delta ? r + D_W : A + A_W), wires, delta ? r + D_CONS : A + A_CONS, (int)lane - 1);
+        return;
+    }
     bool ok = true;
-    if (J.kind != 1) {
-        const G1A w = load_g1(A + A_W);
+    if (!delta) {
         const uint32_t s5 = V_COUNT + J.fresh;
-        q[s5] = load_g2(A + A_S5G2);
-        emit_dynamo(e, A + A_DYN);
-        emit_consistency(e, w, A + A_WIRES, A + A_CONS);
-        const G1A w3 = load_g1(A + A_WIRES + 192), w4 = load_g1(A + A_WIRES + 256), w5 = load_g1(A + A_WIRES + 320);
-        e.t(load_g1(A + A_PZQ), V_PZD); e.t(w.neg(), V_G2);
-        e.t(w4, V_G2); e.t(g1.neg(), s5);
-        e.t(w3, s5); e.t(w5.neg(), V_G2); e.t(load_g1(A + A_MQ).neg(), V_MD);
-        // group identities: w == instance_z, h == instance_h, s1 + s2 == s3
-        ok &= G1X::equal(G1X::from_affine(w), G1X::from_affine(load_g1(A + A_DYN + 384)));
-        ok &= G1X::equal(G1X::from_affine(load_g1(A + A_H)), G1X::from_affine(load_g1(A + A_DYN + 448)));
-        const G1X s12 = G1X::add_affine(G1X::from_affine(load_g1(A + A_WIRES)), load_g1(A + A_WIRES + 64));
-        ok &= G1X::equal(s12, G1X::from_affine(load_g1(A + A_WIRES + 128)));
-        // h + [public]_h == 0 (dynaverse.rs:1008-1015) when the proof has no
-        // delta (kind 0); [public]_h = the side slots' value before the update
-        // plus the public differences (a fresh anchor: zero plus the MSM of
-        // all public inputs)
-        const G1X pub = G1X::add_affine(G1X::from_affine(load_g1(r + SIDE_PUB)), load_g1(r + SIDE_PDIFF));
-        if (J.kind == 0) ok &= G1X::add(G1X::add_affine(G1X::inf(), load_g1(A + A_H)), pub).is_inf();
-        store_g1(r + SIDE_PUBNEW, pub.to_affine());
+        if (lane == 7) {
+            const G1A w = load_g1(A + A_W);
+            const G1A w3 = load_g1(A + A_WIRES + 192), w4 = load_g1(A + A_WIRES + 256), w5 = load_g1(A + A_WIRES + 320);
+            Emit e = at(TAIL_TERMS);
+            e.t(load_g1(A + A_PZQ), V_PZD); e.t(w.neg(), V_G2);
+            e.t(w4, V_G2); e.t(g1.neg(), s5);
+            e.t(w3, s5); e.t(w5.neg(), V_G2); e.t(load_g1(A + A_MQ).neg(), V_MD);
+        } else if (lane == 8) {
+            // group identities: w == instance_z, h == instance_h, s1 + s2 == s3
+            ok &= G1X::equal(G1X::from_affine(load_g1(A + A_W)), G1X::from_affine(load_g1(A + A_DYN + 384)));
+            ok &= G1X::equal(G1X::from_affine(load_g1(A + A_H)), G1X::from_affine(load_g1(A + A_DYN + 448)));
+            const G1X s12 = G1X::add_affine(G1X::from_affine(load_g1(A + A_WIRES)), load_g1(A + A_WIRES + 64));
+            ok &= G1X::equal(s12, G1X::from_affine(load_g1(A + A_WIRES + 128)));
+            // h + [public]_h == 0 (dynaverse.rs:1008-1015) when the proof has no
+            // delta (kind 0); [public]_h = the side slots' value before the update
+            // plus the public differences (a fresh anchor: zero plus the MSM of
+            // all public inputs)
+            const G1X pub = G1X::add_affine(G1X::from_affine(load_g1(r + SIDE_PUB)), load_g1(r + SIDE_PDIFF));
+            if (J.kind == 0) ok &= G1X::add(G1X::add_affine(G1X::inf(), load_g1(A + A_H)), pub).is_inf();
+            store_g1(r + SIDE_PUBNEW, pub.to_affine());
+        }
     } else {
         const uint32_t aff2 = V_COUNT + J.fresh, unaff2 = aff2 + 1, us5 = aff2 + 2;
-        q[aff2] = load_g2(r + D_AFF2);
-        q[unaff2] = load_g2(r + D_UNAFF2);
-        q[us5] = load_g2(r + D_US5);
-        const G1A cw = load_g1(r + D_W);
-        emit_dynamo(e, r + D_DYN);
-        emit_consistency(e, cw, r + D_WIRES, r + D_CONS);
-        const G1A aff1 = load_g1(r + D_AFF1), unaff1 = load_g1(r + D_UNAFF1);
-        e.t(load_g1(r + D_PZQ), V_PZD); e.t(cw.neg(), V_G2);
-        e.t(aff1, V_G2); e.t(g1.neg(), aff2);
-        e.t(unaff1, V_G2); e.t(g1.neg(), unaff2);
-        e.t(aff1, unaff2); e.t(mvg1.neg(), V_G2);
-        G1A ru[3];
-        for (int i = 0; i < 3; ++i) ru[i] = g1_add(load_g1(r + D_ALOC + 64 * i), load_g1(r + D_CLOC + 64 * i));
-        e.t(ru[1], V_G2); e.t(g1.neg(), us5);
-        e.t(ru[0], us5); e.t(ru[2].neg(), V_G2); e.t(load_g1(r + D_LQ).neg(), aff2);
-        for (int i = 0; i < 3; ++i) {
+        if (lane == 7) {
+            const G1A aff1 = load_g1(r + D_AFF1), unaff1 = load_g1(r + D_UNAFF1);
+            Emit e = at(TAIL_TERMS);
+            e.t(load_g1(r + D_PZQ), V_PZD); e.t(load_g1(r + D_W).neg(), V_G2);
+            e.t(aff1, V_G2); e.t(g1.neg(), aff2);
+            e.t(unaff1, V_G2); e.t(g1.neg(), unaff2);
+            e.t(aff1, unaff2); e.t(mvg1.neg(), V_G2);
+            // the local multiplication equation: ru[1] (lane 9), g1, ru[0] (lane 8), ru[2] (lane 10), quotient
+            e.k = TAIL_TERMS + 9;
+            e.t(g1.neg(), us5);
+            e.k = TAIL_TERMS + 12;
+            e.t(load_g1(r + D_LQ).neg(), aff2);
+        } else if (lane <= 10) {
+            // ru[i] = anchor local + changed local of wire s4 + i
+            const uint32_t i = lane - 8;
+            const G1A ru = g1_add(load_g1(r + D_ALOC + 64 * i), load_g1(r + D_CLOC + 64 * i));
+            const uint32_t pos[3] = {TAIL_TERMS + 10, TAIL_TERMS + 8, TAIL_TERMS + 11};
+            Emit e = at(pos[i]);
+            if (i == 0) e.t(ru, us5);
+            else if (i == 1) e.t(ru, V_G2);
+            else e.t(ru.neg(), V_G2);
+        } else if (lane <= 13) {
+            // the openings of wire s4 + i against the affected and unaffected sets
+            const uint32_t i = lane - 11;
             const G1A aw = load_g1(A + A_WIRES + 64 * (3 + i)), chw = load_g1(r + D_WIRES + 64 * (3 + i));
+            Emit e = at(TAIL_TERMS + 13 + 6 * i);
             e.t(load_g1(r + D_AOPEN + 64 * i), aff2); e.t(g1_sub(aw, load_g1(r + D_ALOC + 64 * i)).neg(), V_G2);
             e.t(load_g1(r + D_COPEN + 64 * i), aff2); e.t(g1_sub(chw, load_g1(r + D_CLOC + 64 * i)).neg(), V_G2);
             e.t(load_g1(r + D_UZERO + 64 * i), unaff2); e.t(chw.neg(), V_G2);
+        } else if (lane == 14) {
+            ok &= G1X::equal(G1X::from_affine(load_g1(r + D_W)), G1X::from_affine(load_g1(r + D_DYN + 384)));
+            ok &= G1X::equal(G1X::from_affine(load_g1(r + D_H)), G1X::from_affine(load_g1(r + D_DYN + 448)));
+            const G1X s12 = G1X::add_affine(G1X::from_affine(load_g1(r + D_WIRES)), load_g1(r + D_WIRES + 64));
+            ok &= G1X::equal(s12, G1X::from_affine(load_g1(r + D_WIRES + 128)));
+            // anchor h + changed h + [public]_h == 0 (session.rs:127-131), with
+            // [public]_h = the session's value plus this update's public differences
+            const G1X pub_new = G1X::add_affine(G1X::from_affine(load_g1(r + SIDE_PUB)), load_g1(r + SIDE_PDIFF));
+            G1X sum = G1X::add_affine(G1X::from_affine(load_g1(A + A_H)), load_g1(r + D_H));
+            sum = G1X::add(sum, pub_new);
+            ok &= sum.is_inf();
+            store_g1(r + SIDE_PUBNEW, pub_new.to_affine());
         }
-        ok &= G1X::equal(G1X::from_affine(cw), G1X::from_affine(load_g1(r + D_DYN + 384)));
-        ok &= G1X::equal(G1X::from_affine(load_g1(r + D_H)), G1X::from_affine(load_g1(r + D_DYN + 448)));
-        const G1X s12 = G1X::add_affine(G1X::from_affine(load_g1(r + D_WIRES)), load_g1(r + D_WIRES + 64));
-        ok &= G1X::equal(s12, G1X::from_affine(load_g1(r + D_WIRES + 128)));
-        // anchor h + changed h + [public]_h == 0 (session.rs:127-131), with
-        // [public]_h = the session's value plus this update's public differences
-        const G1X pub_new = G1X::add_affine(G1X::from_affine(load_g1(r + SIDE_PUB)), load_g1(r + SIDE_PDIFF));
-        G1X sum = G1X::add_affine(G1X::from_affine(load_g1(A + A_H)), load_g1(r + D_H));
-        sum = G1X::add(sum, pub_new);
-        ok &= sum.is_inf();
-        store_g1(r + SIDE_PUBNEW, pub_new.to_affine());
     }
-    (void)inf;
     if (!ok) atomicOr(status + J.status, 8u);
 }
 
@@ -942,8 +998,10 @@ struct Params {
     uint64_t fam_off[F_COUNT + 1] = {};
     uint64_t fam2_off[F2_COUNT + 1] = {};
     DevBuf srs, table, srs2, table2;  // Montgomery affine bases; c = 8 window multiples
+    DevBuf table_dense;               // c = 16 window multiples of KZG bases [0, n)
     DevBuf wpow, inv1m;               // w^k, 1/(1 - w^k) (Montgomery)
     DevBuf vk2;                       // V_COUNT Montgomery G2 points
+    DevBuf vk_lines, vk_inf;          // their Miller-loop lines, prepared once
     DevBuf consts;                    // canonical: [1]G1 | [X^n - 1]G1 | [X^n - 1]G2
     uint8_t vk2_bytes[V_COUNT][128] = {};
     uint8_t g1[64] = {}, mvg1[64] = {};
@@ -969,7 +1027,7 @@ uint32_t sigma_of(uint32_t n, uint32_t i) {
 
 uint64_t params_bytes(uint64_t n) {
     const uint64_t rows = 100 * n, rows2 = 2 * n;
-    return rows * 64 * (1 + TW) + rows2 * 128 * (1 + TW) + 2 * n * 32 + V_COUNT * 128 + 256;
+    return rows * 64 * (1 + TW) + n * 64 * TWD + rows2 * 128 * (1 + TW) + 2 * n * 32 + V_COUNT * 128 + 256;
 }
 
 // ================================================================ host: sessions and jobs
@@ -977,8 +1035,10 @@ struct Session {
     uint64_t id = 0;
     Params* P = nullptr;
     uint32_t n = 0;
-    std::vector<Canon> pub, anchor, current;
-    std::map<uint32_t, Canon> delta;  // witness index -> anchor difference (nonzero)
+    // The current witness and instance.  The anchor's witness is not kept:
+    // it is current minus `delta`, the nonzero differences by witness index.
+    std::vector<Canon> pub, current;
+    std::map<uint32_t, Canon> delta;
     std::vector<uint8_t> anchor_bytes;
     std::vector<uint8_t> proof;
     uint64_t anchor_generation = 0, generation = 0;
@@ -986,6 +1046,22 @@ struct Session {
     DevBuf d_anchor, d_coef;  // anchor proof bytes; s4 | s5 | s6 coefficients
     uint64_t footprint = 0;
 };
+
+hf::Fr as_fr(const Canon& c) {
+    hf::Fr r;
+    memcpy(r.v, c.data(), 32);
+    return r;
+}
+
+// The anchor's value at witness index i (current less the recorded difference).
+Canon anchor_value(const Session& S, uint64_t i) {
+    const auto it = S.delta.find((uint32_t)i);
+    if (it == S.delta.end()) return S.current[i];
+    const hf::Fr v = hf::sub(as_fr(S.current[i]), as_fr(it->second));
+    Canon c;
+    memcpy(c.data(), v.v, 32);
+    return c;
+}
 
 struct Request {
     uint64_t ticket = 0, session = 0, submit_ns = 0;
@@ -1009,7 +1085,6 @@ struct Job {
     uint64_t generation = 0;
     std::map<uint64_t, Canon> edits, pedits;   // canonical new values
     std::map<uint32_t, Canon> delta;           // the new anchor differences
-    std::vector<Canon> witness, pub;           // rebuild: the new witness and instance
     // results
     bool ok = false;
     std::string error;
@@ -1100,6 +1175,9 @@ public:
             b_->device = device_;
             DV_CUDA(cudaStreamCreateWithFlags(&b_->stream, cudaStreamNonBlocking));
             st_ = b_->stream;
+            DV_CUDA(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
+            DV_CUDA(cudaEventCreateWithFlags(&ev_fields_, cudaEventDisableTiming));
+            DV_CUDA(cudaEventCreateWithFlags(&ev_g2_, cudaEventDisableTiming));
         });
     }
     ~Engine() {
@@ -1305,6 +1383,9 @@ private:
             stat_launches_ += launch_counter() - l0;
             done_cv_.notify_all();
         }
+        if (ev_fields_) cudaEventDestroy(ev_fields_);
+        if (ev_g2_) cudaEventDestroy(ev_g2_);
+        if (st2_) cudaStreamDestroy(st2_);
         b_.reset();
     }
 
@@ -1313,7 +1394,11 @@ private:
     // ------------------------------------------------------------ pipelines
     template <class F>
     void run_msm(MsmWorkspace& ws, const Affine<F>* table, MsmBuild& mb, const uint8_t* d_stage,
-                 const uint32_t* lrow, const uint32_t* lsc, const Fr* arena, uint8_t* out, uint32_t* d_err);
+                 const uint32_t* lrow, const uint32_t* lsc, const Fr* arena, uint8_t* out, uint32_t* d_err,
+                 DevBuf& tpoint, DevBuf& tscalar, cudaStream_t st, int tc = TC, int tw = TW);
+    // The batch's pairing lines: the verifying key's (prepared with the
+    // parameters), then the nfresh own G2 points at q + V_COUNT, prepared on st.
+    void prepare_lines(Params& P, const G2A* q, uint64_t nfresh, cudaStream_t st);
     void run_anchor(Params& P, const std::vector<Canon>& w, const std::vector<Canon>& pub, Job& job);
     void run_sparse(Params& P, std::vector<Job*>& jobs);
     void run_verify(Params& P, uint32_t njobs, uint64_t nfresh, uint64_t terms, uint64_t eqs, const VerifyJob* d_jobs,
@@ -1331,8 +1416,13 @@ private:
     uint32_t max_batch_;
     MsmWorkspace ws1_, ws2_;
     NttBatch nb_fwd_, nb_inv_, nb_r1_, nb_r2_, nb_r3_;
-    DevBuf stage_, arena_, scr_, out_, status_, verdicts_, tpoint_, tscalar_, lrow_, lsc_, terms_p_, terms_q_, g2q_,
-        tmp_, tmp2_, err_;
+    DevBuf stage_, arena_, scr_, out_, status_, verdicts_, tpoint_, tscalar_, tpoint2_, tscalar2_, lrow_, lsc_,
+        terms_p_, terms_q_, g2q_, lines_, qinf_, tmp_, tmp2_, err_;
+    // The G2 side of an update batch (its MSM, then preparing the fresh G2
+    // points for the pairings) runs on st2_ beside the dense G1 work on st_.
+    cudaStream_t st2_ = nullptr;
+    cudaEvent_t ev_fields_ = nullptr, ev_g2_ = nullptr;
+    bool quot_smem_ = false;
     PinnedBuf pstage_, pstage2_, parena_, pout_;
 
     std::mutex mu_;
@@ -1523,6 +1613,7 @@ uint64_t Engine::build_params(uint64_t n, const uint8_t* txb, const uint8_t* tyb
         G1A* srs = P->srs.as<G1A>(rows);
         convert_points<Fq>(d_pt, srs, rows, bad + 1, st);
         msm_precompute<Fq>(srs, rows, TC, TW, P->table.as<G1A>(rows * TW), st);
+        msm_precompute<Fq>(srs + P->fam_off[F_KZG], n, TCD, TWD, P->table_dense.as<G1A>(n * TWD), st);
         DV_CUDA(cudaStreamSynchronize(st));
     }
     {
@@ -1544,6 +1635,8 @@ uint64_t Engine::build_params(uint64_t n, const uint8_t* txb, const uint8_t* tyb
         fixed_base_launch(b_->fixed_base, d_sc, V_COUNT, 1, d_pt, bad, st);
         fixed_base_launch(b_->fixed_base, d_sc + 32 * V_COUNT, 2, 0, d_pt + 128 * V_COUNT, bad, st);
         convert_points<Fq2>(d_pt, P->vk2.as<G2A>(V_COUNT), V_COUNT, bad + 3, st);
+        pairing_prepare_device(P->vk2.view<G2A>(), V_COUNT, P->vk_lines.as<uint8_t>(V_COUNT * pairing_prepared_bytes()),
+                               P->vk_inf.as<uint32_t>(V_COUNT), st);
         uint8_t* consts = P->consts.as<uint8_t>(256);
         DV_CUDA(cudaMemcpyAsync(consts, d_pt + 128 * V_COUNT, 128, cudaMemcpyDeviceToDevice, st));
         DV_CUDA(cudaMemcpyAsync(consts + 128, d_pt + 128 * V_MD, 128, cudaMemcpyDeviceToDevice, st));
@@ -1572,20 +1665,21 @@ uint64_t Engine::build_params(uint64_t n, const uint8_t* txb, const uint8_t* tyb
 // ================================================================ pipelines
 template <class F>
 void Engine::run_msm(MsmWorkspace& ws, const Affine<F>* table, MsmBuild& mb, const uint8_t* d_stage,
-                     const uint32_t* lrow, const uint32_t* lsc, const Fr* arena, uint8_t* out, uint32_t* d_err) {
+                     const uint32_t* lrow, const uint32_t* lsc, const Fr* arena, uint8_t* out, uint32_t* d_err,
+                     DevBuf& tpoint, DevBuf& tscalar, cudaStream_t st, int tc, int tw) {
     if (!mb.sets() || !mb.terms) return;  // no terms: every field stays zero bytes (infinity)
-    uint32_t* tp = tpoint_.as<uint32_t>(mb.terms);
-    uint32_t* ts = tscalar_.as<uint32_t>(mb.terms);
-    k_dv_expand<<<(mb.terms + 255) / 256, 256, 0, st_>>>(
+    uint32_t* tp = tpoint.as<uint32_t>(mb.terms);
+    uint32_t* ts = tscalar.as<uint32_t>(mb.terms);
+    k_dv_expand<<<(mb.terms + 255) / 256, 256, 0, st>>>(
         mb.terms, (uint32_t)mb.segs.size(), reinterpret_cast<const uint32_t*>(d_stage + mb.at.seg_off),
         reinterpret_cast<const SetDesc*>(d_stage + mb.at.segs), lrow, lsc, tp, ts);
     DV_LAUNCH();
-    const MsmPrecomp<F> pre{table, TC, TW};
+    const MsmPrecomp<F> pre{table, tc, tw};
     const uint32_t sets = (uint32_t)mb.sets();
     const MsmPlan plan = msm_plan_batch<F>(sets, 0, mb.terms, 0, &pre);
     SetMap map{reinterpret_cast<const uint32_t*>(d_stage + mb.at.set_off), nullptr, sets, 0, tp, ts};
-    msm_enqueue<F>(ws, nullptr, reinterpret_cast<const uint32_t*>(arena), map, mb.terms, plan, &pre, d_err, st_);
-    k_dv_affine<F><<<(sets + 127) / 128, 128, 0, st_>>>(ws.windows.view<XYZZ<F>>(), sets,
+    msm_enqueue<F>(ws, nullptr, reinterpret_cast<const uint32_t*>(arena), map, mb.terms, plan, &pre, d_err, st);
+    k_dv_affine<F><<<(sets + 127) / 128, 128, 0, st>>>(ws.windows.view<XYZZ<F>>(), sets,
                                                         reinterpret_cast<const uint64_t*>(d_stage + mb.at.out_off),
                                                         out);
     DV_LAUNCH();
@@ -1617,10 +1711,22 @@ void Engine::run_verify(Params& P, uint32_t njobs, uint64_t nfresh, uint64_t ter
     uint32_t* qi = terms_q_.as<uint32_t>(std::max<uint64_t>(1, terms));
     G2A* q = g2q_.as<G2A>(V_COUNT + nfresh);
     DV_CUDA(cudaMemcpyAsync(q, P.vk2.view<G2A>(), V_COUNT * sizeof(G2A), cudaMemcpyDeviceToDevice, st_));
-    k_dv_terms<<<(njobs + 31) / 32, 32, 0, st_>>>(d_jobs, njobs, host_g1(P.g1), host_g1(P.mvg1), p, qi, q,
-                                                   d_status);
+    k_dv_fresh<<<(njobs + 31) / 32, 32, 0, st_>>>(d_jobs, njobs, q);
     DV_LAUNCH();
-    pairing_check_device(*b_, p, terms, q, V_COUNT + nfresh, qi, d_off, eqs, d_verdicts, st_);
+    k_dv_terms<<<njobs, 32, 0, st_>>>(d_jobs, njobs, host_g1(P.g1), host_g1(P.mvg1), p, qi, d_status);
+    DV_LAUNCH();
+    prepare_lines(P, q, nfresh, st_);
+    pairing_check_prepared(*b_, p, terms, lines_.view<uint8_t>(), qinf_.view<uint32_t>(), qi, d_off, eqs, d_verdicts,
+                           st_);
+}
+
+void Engine::prepare_lines(Params& P, const G2A* q, uint64_t nfresh, cudaStream_t st) {
+    const uint64_t lb = pairing_prepared_bytes();
+    uint8_t* lines = lines_.as<uint8_t>((V_COUNT + nfresh) * lb);
+    uint32_t* qinf = qinf_.as<uint32_t>(V_COUNT + nfresh);
+    DV_CUDA(cudaMemcpyAsync(lines, P.vk_lines.view<uint8_t>(), V_COUNT * lb, cudaMemcpyDeviceToDevice, st));
+    DV_CUDA(cudaMemcpyAsync(qinf, P.vk_inf.view<uint32_t>(), 4 * V_COUNT, cudaMemcpyDeviceToDevice, st));
+    pairing_prepare_device(q + V_COUNT, nfresh, lines + V_COUNT * lb, qinf + V_COUNT, st);
 }
 
 void Engine::upload(Stager& stg) {
@@ -1738,8 +1844,8 @@ void Engine::run_anchor(Params& P, const std::vector<Canon>& w, const std::vecto
     tpoint_.as<uint32_t>(std::max(g1.terms, g2.terms) + 1);
     tscalar_.as<uint32_t>(std::max(g1.terms, g2.terms) + 1);
     stat_fme_ += (uint64_t)(g1.fme + 3 * g2.fme);
-    run_msm<Fq>(ws1_, P.table.view<G1A>(), g1, d, nullptr, nullptr, arena, rec, err);
-    run_msm<Fq2>(ws2_, P.table2.view<G2A>(), g2, d, nullptr, nullptr, arena, rec, err + 1);
+    run_msm<Fq>(ws1_, P.table.view<G1A>(), g1, d, nullptr, nullptr, arena, rec, err, tpoint_, tscalar_, st_);
+    run_msm<Fq2>(ws2_, P.table2.view<G2A>(), g2, d, nullptr, nullptr, arena, rec, err + 1, tpoint_, tscalar_, st_);
     k_dv_copy<<<dim3(1, (unsigned)cp.size()), 32, 0, st>>>((uint32_t)cp.size(), reinterpret_cast<const CopyDesc*>(d + at_cp));
     DV_LAUNCH();
     run_verify(P, 1, 1, ANCHOR_TERMS, ANCHOR_EQS, reinterpret_cast<const VerifyJob*>(d + at_vj),
@@ -1849,7 +1955,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         L.a = (uint32_t)aff.size();
         L.FI = ain.size();
         for (int t = 0; t < 3; ++t)
-            for (uint32_t i : aff) ain.push_back(S.anchor[(3 + t) * n + i]);
+            for (uint32_t i : aff) ain.push_back(anchor_value(S, (3 + t) * n + i));
         for (int t = 0; t < 3; ++t)
             for (uint32_t i : aff) {
                 auto it = J.delta.find((3 + t) * n + i);
@@ -1921,8 +2027,8 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     // MSM launches: the linear fields (dynamo, wires, consistency, public
     // quotient, public differences); the affected-set fields and re-anchor
     // quotients; the G2 fields
-    MsmBuild m1, m2, m3;
-    std::vector<CopyDesc> cp;
+    MsmBuild m1, m2, m3, md;  // md: the dense sets, over the c = 16 table
+    std::vector<CopyDesc> cp, cp2;  // fixed fields: G1 on st_, G2 on st2_
     std::vector<VerifyJob> vj(B);
     std::vector<RebaseJob> rj;
     std::vector<uint64_t> off{0};
@@ -1977,8 +2083,8 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
             // s5 of the delta (G2) and the new multiplication quotient
             m3.seg(1, L.LSN[4], P.fam2_off[F2_LAG], 0, L.LS[4]);
             m3.end(rec + D_AFF2);
-            m2.seg(0, n - 1, fo(F_KZG), L.R0 + 7ull * n, 0);
-            m2.end(rec + REC_ANCHOR + A_MQ);
+            md.seg(0, n - 1, 0, L.R0 + 7ull * n, 0);
+            md.end(rec + REC_ANCHOR + A_MQ);
             rj.push_back({R, S.d_anchor.view<uint8_t>()});
             vj[j] = VerifyJob{R, R + REC_ANCHOR, 0, (uint32_t)terms, (uint32_t)fresh, j};
             terms += ANCHOR_TERMS;
@@ -1996,7 +2102,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
             m2.end(rec + D_UNAFF1);
         } else {
             cp.push_back({R + D_UNAFF1, P.consts.view<uint8_t>() + 64, 64});
-            cp.push_back({R + D_UNAFF2, P.consts.view<uint8_t>() + 128, 128});
+            cp2.push_back({R + D_UNAFF2, P.consts.view<uint8_t>() + 128, 128});
         }
         for (int t = 0; t < 3; ++t) {
             m2.seg(0, a, fo(F_KZG), FO + 2 * a + 1 + t * a, 0);
@@ -2009,8 +2115,8 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
             m2.seg(0, a, fo(F_KZG), FO + 8 * a + 1 + t * a, 0);
             m2.end(rec + D_UZERO + 64 * t);
             if (a) {
-                m2.seg(0, n - a, fo(F_KZG), L.DN + (uint64_t)t * n, 0);
-                m2.end(rec + D_AOPEN + 64 * t);
+                md.seg(0, n - a, 0, L.DN + (uint64_t)t * n, 0);
+                md.end(rec + D_AOPEN + 64 * t);
             } else {
                 cp.push_back({R + D_AOPEN + 64 * t, S.d_anchor.view<uint8_t>() + A_WIRES + 64 * (3 + t), 64});
             }
@@ -2037,6 +2143,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     m1.stage(stg);
     m2.stage(stg);
     m3.stage(stg);
+    md.stage(stg);
     const size_t at_lrow = stg.add(lrow), at_lsc = stg.add(lsc), at_fj = stg.add(fj), at_kj = stg.add(kjob),
                  at_vj = stg.add(vj), at_off = stg.add(off), at_pub = stg.add(pubh), at_pairs = stg.add(pairs),
                  at_rj = stg.add(rj);
@@ -2045,7 +2152,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     std::vector<CopyDesc> cp0;
     for (uint32_t j = 0; j < B; ++j) cp0.push_back({out + (uint64_t)j * JOB_BYTES + SIDE_PUB, d + at_pub + 64ull * j, 64});
     Stager stg2;
-    const size_t at_cp0 = stg2.add(cp0), at_cp = stg2.add(cp);
+    const size_t at_cp0 = stg2.add(cp0), at_cp = stg2.add(cp), at_cp2 = stg2.add(cp2);
     uint8_t* hs2 = pstage2_.as<uint8_t>(stg2.h.size());
     memcpy(hs2, stg2.h.data(), stg2.h.size());
     uint8_t* d2 = tmp_.as<uint8_t>(stg2.h.size());
@@ -2099,23 +2206,22 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     DV_CUDA(cudaMemsetAsync(err, 0xff, 12, st));
     k_dv_copy<<<dim3(1, B), 32, 0, st>>>(B, reinterpret_cast<const CopyDesc*>(d2 + at_cp0));
     DV_LAUNCH();
-    const uint32_t maxterms = std::max(m1.terms, std::max(m2.terms, m3.terms)) + 1;
+    const uint32_t maxterms = std::max(std::max(m1.terms, m2.terms), md.terms) + 1;
     tpoint_.as<uint32_t>(maxterms);
     tscalar_.as<uint32_t>(maxterms);
     const uint32_t* d_lrow = reinterpret_cast<const uint32_t*>(d + at_lrow);
     const uint32_t* d_lsc = reinterpret_cast<const uint32_t*>(d + at_lsc);
-    stat_fme_ += (uint64_t)(m1.fme + m2.fme + 3 * m3.fme);
-    run_msm<Fq>(ws1_, P.table.view<G1A>(), m1, d, d_lrow, d_lsc, arena, out, err);
+    stat_fme_ += (uint64_t)(m1.fme + m2.fme + md.fme + 3 * m3.fme);
+    run_msm<Fq>(ws1_, P.table.view<G1A>(), m1, d, d_lrow, d_lsc, arena, out, err, tpoint_, tscalar_, st);
     // field work of the affected sets
     FieldCtx c{reinterpret_cast<const FieldJob*>(d + at_fj), reinterpret_cast<const uint32_t*>(d + at_kj), B, d_lrow,
                P.wpow.view<Fr>(), P.inv1m.view<Fr>(), n, Fr{}, Fr{}, arena, scratch, status};
     memcpy(&c.n_m, P.n_m.v, 32);
     memcpy(&c.ninv_m, P.ninv_m.v, 32);
     const uint32_t K = kjob[B];
-    static bool smem_set = false;
-    if (!smem_set) {
+    if (!quot_smem_) {
         DV_CUDA(cudaFuncSetAttribute(k_dv_quot, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-        smem_set = true;
+        quot_smem_ = true;
     }
     if (K) {
         k_dv_geom<<<(K + 127) / 128, 128, 0, st>>>(c);
@@ -2132,6 +2238,34 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         DV_LAUNCH();
         k_dv_quot<<<B, 256, std::max<uint64_t>(1, 4 * amax) * sizeof(Fr), st>>>(c);
         DV_LAUNCH();
+    }
+    // The G2 side on st2_, once the field rows it reads exist: the G2 MSM,
+    // the re-anchors' G2 field, the fresh G2 points and their pairing lines.
+    // It overlaps the dense G1 work below, which touches none of its inputs.
+    G2A* q = g2q_.as<G2A>(V_COUNT + fresh);
+    lines_.as<uint8_t>((V_COUNT + fresh) * pairing_prepared_bytes());
+    qinf_.as<uint32_t>(V_COUNT + fresh);
+    tpoint2_.as<uint32_t>(m3.terms + 1);
+    tscalar2_.as<uint32_t>(m3.terms + 1);
+    DV_CUDA(cudaEventRecord(ev_fields_, st));
+    DV_CUDA(cudaStreamWaitEvent(st2_, ev_fields_, 0));
+    run_msm<Fq2>(ws2_, P.table2.view<G2A>(), m3, d, d_lrow, d_lsc, arena, out, err + 2, tpoint2_, tscalar2_, st2_);
+    if (!cp2.empty()) {
+        k_dv_copy<<<dim3(1, (unsigned)cp2.size()), 32, 0, st2_>>>((uint32_t)cp2.size(),
+                                                                  reinterpret_cast<const CopyDesc*>(d2 + at_cp2));
+        DV_LAUNCH();
+    }
+    if (!rj.empty()) {
+        k_dv_rebase<<<(unsigned)((rj.size() + 63) / 64), 64, 0, st2_>>>(reinterpret_cast<const RebaseJob*>(d + at_rj),
+                                                                    (uint32_t)rj.size(), REBASE_FIELDS - 1,
+                                                                    REBASE_FIELDS);
+        DV_LAUNCH();
+    }
+    k_dv_fresh<<<(B + 31) / 32, 32, 0, st2_>>>(reinterpret_cast<const VerifyJob*>(d + at_vj), B, q);
+    DV_LAUNCH();
+    prepare_lines(P, q, fresh, st2_);
+    DV_CUDA(cudaEventRecord(ev_g2_, st2_));
+    if (K) {
         // anchor openings: (s_t - r_t) / A on the coset 5 H
         const uint64_t t4 = 4ull * n * B;
         k_dv_numer<<<(unsigned)((t4 + 255) / 256), 256, 0, st>>>(c);
@@ -2177,19 +2311,28 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
             DV_LAUNCH();
         }
     }
-    run_msm<Fq>(ws1_, P.table.view<G1A>(), m2, d, d_lrow, d_lsc, arena, out, err + 1);
-    run_msm<Fq2>(ws2_, P.table2.view<G2A>(), m3, d, d_lrow, d_lsc, arena, out, err + 2);
+    run_msm<Fq>(ws1_, P.table.view<G1A>(), m2, d, d_lrow, d_lsc, arena, out, err + 1, tpoint_, tscalar_, st);
+    run_msm<Fq>(ws1_, P.table_dense.view<G1A>(), md, d, d_lrow, d_lsc, arena, out, err + 1, tpoint_, tscalar_, st, TCD,
+                TWD);
     if (!cp.empty()) {
         k_dv_copy<<<dim3(1, (unsigned)cp.size()), 32, 0, st>>>((uint32_t)cp.size(), reinterpret_cast<const CopyDesc*>(d2 + at_cp));
         DV_LAUNCH();
     }
     if (!rj.empty()) {
-        const uint32_t tot = (uint32_t)rj.size() * REBASE_FIELDS;
-        k_dv_rebase<<<(tot + 63) / 64, 64, 0, st>>>(reinterpret_cast<const RebaseJob*>(d + at_rj), (uint32_t)rj.size());
+        const uint32_t tot = (uint32_t)rj.size() * (REBASE_FIELDS - 1);
+        k_dv_rebase<<<(tot + 63) / 64, 64, 0, st>>>(reinterpret_cast<const RebaseJob*>(d + at_rj), (uint32_t)rj.size(),
+                                                    0, REBASE_FIELDS - 1);
         DV_LAUNCH();
     }
-    run_verify(P, B, fresh, terms, eqs, reinterpret_cast<const VerifyJob*>(d + at_vj),
-               reinterpret_cast<const uint64_t*>(d + at_off), verd, status);
+    // verification: the G1 terms here, then the pairings once st2_ is done
+    G1A* tp1 = terms_p_.as<G1A>(std::max<uint64_t>(1, terms));
+    uint32_t* tq1 = terms_q_.as<uint32_t>(std::max<uint64_t>(1, terms));
+    k_dv_terms<<<B, 32, 0, st>>>(reinterpret_cast<const VerifyJob*>(d + at_vj), B, host_g1(P.g1), host_g1(P.mvg1),
+                                 tp1, tq1, status);
+    DV_LAUNCH();
+    DV_CUDA(cudaStreamWaitEvent(st, ev_g2_, 0));
+    pairing_check_prepared(*b_, tp1, terms, lines_.view<uint8_t>(), qinf_.view<uint32_t>(), tq1,
+                           reinterpret_cast<const uint64_t*>(d + at_off), eqs, verd, st);
     for (auto& jc : coefs) {
         uint8_t* an = jobs[jc.first]->new_anchor.as<uint8_t>(ANCHOR_BYTES);
         DV_CUDA(cudaMemcpyAsync(an, out + (uint64_t)jc.first * JOB_BYTES + REC_ANCHOR, ANCHOR_BYTES,
@@ -2260,12 +2403,6 @@ void read_canon(const uint8_t* b, uint64_t count, std::vector<Canon>& out, const
     }
 }
 
-hf::Fr as_fr(const Canon& c) {
-    hf::Fr r;
-    memcpy(r.v, c.data(), 32);
-    return r;
-}
-
 // ToyCircuit::validate on the given gates (toy_circuit.rs:72-90).
 template <class Wire, class Input>
 void check_gates(uint64_t n, const std::vector<uint64_t>& gates, Wire wire, Input input) {
@@ -2309,9 +2446,8 @@ uint64_t Engine::open_impl(uint64_t pid, const uint8_t* pubb, const uint8_t* wit
     auto S = std::make_unique<Session>();
     S->P = P;
     S->n = (uint32_t)n;
-    S->pub = pub;
-    S->anchor = w;
-    S->current = w;
+    S->pub = std::move(pub);
+    S->current = std::move(w);
     S->anchor_bytes = job.anchor_bytes;
     std::swap(S->d_anchor.ptr, job.new_anchor.ptr);
     std::swap(S->d_anchor.cap, job.new_anchor.cap);
@@ -2409,7 +2545,7 @@ bool Engine::verify_impl(uint64_t pid, const uint8_t* pubb, const uint8_t* proof
     DV_CUDA(cudaMemsetAsync(err, 0xff, 4, st));
     tpoint_.as<uint32_t>(n + 1);
     tscalar_.as<uint32_t>(n + 1);
-    run_msm<Fq>(ws1_, P->table.view<G1A>(), mb, d, nullptr, nullptr, d_pub, out, err);
+    run_msm<Fq>(ws1_, P->table.view<G1A>(), mb, d, nullptr, nullptr, d_pub, out, err, tpoint_, tscalar_, st_);
     const uint64_t eqs = off.size() - 1;
     uint8_t* verd = verdicts_.as<uint8_t>(eqs);
     run_verify(*P, (uint32_t)vj.size(), has ? 4 : 1, off.back(), eqs, reinterpret_cast<const VerifyJob*>(d + at_vj),
@@ -2466,7 +2602,7 @@ void Engine::stage_job(Request& r, Session* S, Job& job) {
     job.generation = S->generation + 1;
     job.delta = S->delta;
     for (const auto& e : job.edits) {
-        const hf::Fr diff = hf::sub(as_fr(e.second), as_fr(S->anchor[e.first]));
+        const hf::Fr diff = hf::sub(as_fr(e.second), as_fr(anchor_value(*S, e.first)));
         if (hf::is_zero(diff)) job.delta.erase((uint32_t)e.first);
         else {
             Canon c;
@@ -2474,16 +2610,11 @@ void Engine::stage_job(Request& r, Session* S, Job& job) {
             job.delta[(uint32_t)e.first] = c;
         }
     }
-    if (job.delta.size() >= S->P->rebuild_interval) {
-        job.rebuild = true;
-        job.witness = S->current;
-        for (const auto& e : job.edits) job.witness[e.first] = e.second;
-        job.pub = S->pub;
-        for (const auto& e : job.pedits) job.pub[e.first] = e.second;
-        std::vector<uint64_t> all(n);
-        for (uint64_t i = 0; i < n; ++i) all[i] = i;
-        check_gates(n, all, [&](uint64_t i) { return job.witness[i]; }, [&](uint64_t i) { return job.pub[i]; });
-    }
+    // A re-anchor proves the updated witness from scratch (session.rs:92).
+    // Every gate of it holds: the session's witness satisfied the circuit
+    // (checked in full when the session opened) and this update's dirty
+    // gates were checked above, so no full pass is repeated here.
+    if (job.delta.size() >= S->P->rebuild_interval) job.rebuild = true;
 }
 
 void Engine::process(std::vector<Request>& batch, std::vector<Session*>& sess, std::vector<Outcome>& outs) {
@@ -2538,10 +2669,9 @@ void Engine::process(std::vector<Request>& batch, std::vector<Session*>& sess, s
             outs[r].error = J.error;
             continue;
         }
+        for (const auto& e : J.edits) S.current[e.first] = e.second;
+        for (const auto& e : J.pedits) S.pub[e.first] = e.second;
         if (J.rebuild) {
-            S.anchor = J.witness;
-            S.current = J.witness;
-            S.pub = J.pub;
             S.delta.clear();
             S.anchor_generation = J.generation;
             S.anchor_bytes = J.anchor_bytes;
@@ -2555,9 +2685,7 @@ void Engine::process(std::vector<Request>& batch, std::vector<Session*>& sess, s
             memcpy(J.proof.data() + ANCHOR_BYTES + DELTA_BYTES, tail, 24);
             stat_rebuilds_++;
         } else {
-            for (const auto& e : J.edits) S.current[e.first] = e.second;
-            for (const auto& e : J.pedits) S.pub[e.first] = e.second;
-            S.delta = J.delta;
+            S.delta = std::move(J.delta);
             stat_sparse_++;
         }
         S.generation = J.generation;

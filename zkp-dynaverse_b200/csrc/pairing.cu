@@ -837,12 +837,48 @@ void pairing_run(Backend& b, const uint8_t* g1, const uint8_t* g2, uint64_t term
 
 }  // namespace
 
-// Pairing-product checks over device inputs, with no host synchronisation:
-// equation e holds iff prod over terms [d_off[e], d_off[e+1]) of
-// e(p[k], q[d_qidx[k]]) is one; d_verdicts[e] = 1 / 0.  p: Montgomery affine
-// G1 terms, q: nq Montgomery affine G2 points (each prepared once here).
-// Scratch comes from the backend's pairing state.  For callers that build
-// their equations on the device (the Dynaverse verifier, dynaverse.cu).
+// Bytes of one prepared G2 point (its Miller loop's line triples).
+uint64_t pairing_prepared_bytes() { return (uint64_t)LINES * sizeof(Line); }
+
+// Prepares nq Montgomery affine G2 points of q: their lines into `lines`
+// (nq * pairing_prepared_bytes()) and a u32 per point into qinf (1 at
+// infinity).  No host synchronisation; the buffers are the caller's, so a
+// set of fixed points (a verifying key) can be prepared once and reused.
+void pairing_prepare_device(const G2A* q, uint64_t nq, void* lines, uint32_t* qinf, cudaStream_t st) {
+    if (!nq) return;
+    if (nq > PREP_MAX) throw InvalidArgument("too many distinct G2 points in one check");
+    k_prepare<<<group_blocks(nq), 128, 0, st>>>(q, nq, static_cast<Line*>(lines), qinf);
+    DV_LAUNCH();
+}
+
+// Pairing-product checks over prepared G2 points, with no host
+// synchronisation: equation e holds iff prod over terms
+// [d_off[e], d_off[e+1]) of e(p[k], Q[d_qidx[k]]) is one, where Q's lines
+// and infinity flags are at lines / qinf (pairing_prepare_device);
+// d_verdicts[e] = 1 / 0.  p: Montgomery affine G1 terms.  Scratch comes
+// from the backend.
+void pairing_check_prepared(Backend& b, const G1A* p, uint64_t terms, const void* lines, const uint32_t* qinf,
+                            const uint32_t* d_qidx, const uint64_t* d_off, uint64_t equations, uint8_t* d_verdicts,
+                            cudaStream_t st) {
+    if (!equations) return;
+    const Line* ln = static_cast<const Line*>(lines);
+    Fq2* mil = b.aux.as<Fq2>(6 * std::max<uint64_t>(1, std::max(terms, equations)));
+    const bool multi = miller_per_equation(terms);
+    if (multi) {
+        k_miller_multi<<<group_blocks(equations), 128, 0, st>>>(p, d_qidx, qinf, ln, d_off, equations, mil);
+        DV_LAUNCH();
+    } else if (terms) {
+        k_miller_multi<<<group_blocks(terms), 128, 0, st>>>(p, d_qidx, qinf, ln, nullptr, terms, mil);
+        DV_LAUNCH();
+    }
+    k_final_exp<<<group_blocks(equations), 128, 0, st>>>(mil, multi ? nullptr : d_off, equations, d_verdicts,
+                                                         nullptr);
+    DV_LAUNCH();
+}
+
+// The same checks with the nq G2 points of q prepared first (into the
+// backend's pairing scratch).  For callers that build their equations on
+// the device (the Dynaverse verifier, dynaverse.cu).
 void pairing_check_device(Backend& b, const G1A* p, uint64_t terms, const G2A* q, uint64_t nq,
                           const uint32_t* d_qidx, const uint64_t* d_off, uint64_t equations, uint8_t* d_verdicts,
                           cudaStream_t st) {
@@ -851,22 +887,8 @@ void pairing_check_device(Backend& b, const G1A* p, uint64_t terms, const G2A* q
     PairingState& ps = pairing_state(b);
     Line* lines = ps.lines.as<Line>((uint64_t)LINES * std::max<uint64_t>(1, nq));
     uint32_t* qinf = ps.inf.as<uint32_t>(std::max<uint64_t>(1, nq));
-    if (nq) {
-        k_prepare<<<group_blocks(nq), 128, 0, st>>>(q, nq, lines, qinf);
-        DV_LAUNCH();
-    }
-    Fq2* mil = b.aux.as<Fq2>(6 * std::max<uint64_t>(1, std::max(terms, equations)));
-    const bool multi = miller_per_equation(terms);
-    if (multi) {
-        k_miller_multi<<<group_blocks(equations), 128, 0, st>>>(p, d_qidx, qinf, lines, d_off, equations, mil);
-        DV_LAUNCH();
-    } else if (terms) {
-        k_miller_multi<<<group_blocks(terms), 128, 0, st>>>(p, d_qidx, qinf, lines, nullptr, terms, mil);
-        DV_LAUNCH();
-    }
-    k_final_exp<<<group_blocks(equations), 128, 0, st>>>(mil, multi ? nullptr : d_off, equations, d_verdicts,
-                                                         nullptr);
-    DV_LAUNCH();
+    pairing_prepare_device(q, nq, lines, qinf, st);
+    pairing_check_prepared(b, p, terms, lines, qinf, d_qidx, d_off, equations, d_verdicts, st);
 }
 
 namespace {
