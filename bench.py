@@ -57,26 +57,29 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--op", default="msmres", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch", "g2check",
+    ap.add_argument("--op", default="proofs", choices=["msmres", "msm", "g2msm", "ntt", "sparse", "fixedbase", "batch", "g2check",
                                                          "serve", "ecntt", "poly", "pairing", "proofs"])
     ap.add_argument("--log-n", type=int, default=None)
     ap.add_argument("--kind", default="forward", choices=list(NTT_KINDS))
     ap.add_argument("--k", type=int, default=4096, help="sparse: entries per request")
     ap.add_argument("--alg", type=int, default=3, choices=[1, 2, 3], help="g2check: subgroup algorithm")
     ap.add_argument("--requests", type=int, default=None, help="serve / proofs: update requests per run")
-    ap.add_argument("--sessions", type=int, default=16, help="proofs: sessions of n = 2^log-n")
+    ap.add_argument("--sessions", type=int, default=64, help="proofs: sessions of n = 2^log-n")
     ap.add_argument("--mix", action="store_true", help="proofs: 64 sessions, n in {256, 4096, 65536}, 37:18:9")
-    ap.add_argument("--umax", type=float, default=10.0, help="proofs: supports of floor(2^U) gates, U~U[0,umax]")
+    ap.add_argument("--umax", type=float, default=9.0,
+                    help="proofs: floor(2^U) multiplication gates, U~U[0,umax] (2 witness indices each)")
     ap.add_argument("--rows", type=int, default=16, help="ecntt: rows per transform call")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-operators", action="store_true",
+                    help="proofs: leave out the MSM 2^20 / NTT 2^22 operator points")
     a = ap.parse_args()
     if a.log_n is None:
         a.log_n = {"msm": 20, "msmres": 20, "g2msm": 16, "ntt": 22, "sparse": 16, "fixedbase": 20, "batch": 18,
                    "g2check": 16, "serve": 16, "ecntt": 12, "poly": 12, "pairing": 12, "proofs": 16}[a.op]
     if a.requests is None:
-        a.requests = {"serve": 4000, "proofs": 256}.get(a.op, 4000)
+        a.requests = {"serve": 4000, "proofs": 512}.get(a.op, 4000)
     if a.steps is None:
         a.steps = {"msm": 200, "msmres": 200, "g2msm": 50, "ntt": 200, "sparse": 200, "fixedbase": 100,
                    "batch": 20, "g2check": 50, "serve": 1, "proofs": 1,
@@ -706,6 +709,16 @@ class ServeOp:
             srv.close_session(sid)
         lat = sorted((r.done_ns - r.submit_ns) / 1e6 for _, r in outs)
         pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
+        # the slowest 1 %: time queued, time in their batch, batch sizes
+        worst = sorted(outs, key=lambda o: o[1].done_ns - o[1].submit_ns)[-max(1, len(outs) // 100):]
+        batch_ms = {}
+        for _, r in outs:
+            batch_ms[r.batch_id] = ((r.done_ns - r.start_ns) / 1e6, r.batch_requests)
+        slowest_batch = max(batch_ms.values())
+        tail = {"queued_ms": sum((r.start_ns - r.submit_ns) / 1e6 for _, r in worst) / len(worst),
+                "in_batch_ms": sum((r.done_ns - r.start_ns) / 1e6 for _, r in worst) / len(worst),
+                "batch_requests": [r.batch_requests for _, r in worst],
+                "slowest_batch_ms": slowest_batch[0], "slowest_batch_requests": slowest_batch[1]}
         return {"commitments": [c for c, _ in outs], "wall_s": wall, "per_s": len(outs) / wall,
                 "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1], "mean_ms": sum(lat) / len(lat),
                 "batches": st.batches - before.batches, "largest_batch": max(r.batch_requests for _, r in outs)}
@@ -815,43 +828,134 @@ def bench_trapdoors(sizes, seed=9900):
     return out
 
 
-def proofs_cpu(sizes, wit, reqs, threads, budget_s):
+class ProofsCpu:
     """The CPU restatement of the reference's sparse update path (oracle,
-    bases route: sparse MSMs over the SRS points, the subproduct tree,
-    FFT products and exact division, then the pairing verifier) on the
-    stream's requests of session 0, until budget_s of timed work.  Setup is
-    not timed: the SRS points, and the session's anchor and opening cache
-    from the trapdoor scalars (identical values).  Updates that re-anchor
-    are left out of the sample (on the CPU the dense anchor and its opening
-    cache take minutes at n = 65536), so the rate counts sparse proofs
-    only."""
-    from oracle import dynaverse as D
-    n = sizes[0]
-    tx, ty = bench_trapdoors(sizes)[n]
-    P = D.Params(n, tx, ty, "bases", threads=threads)
-    pub, w = wit[0]
-    S = D.Session(P, pub, w, verify=False, scalar_anchors=True)
-    times, rebuilds, seen = [], 0, 0
-    for j, idx, vals in reqs:
-        if j != 0:
-            continue
-        seen += 1
-        values = [int.from_bytes(vals[32 * i:32 * i + 32], "little") for i in range(len(idx))]
+    bases route: sparse MSMs over the SRS points, the subproduct tree, FFT
+    products and exact division, then the pairing verifier) on a sample of
+    the workload.  Setup is not timed: per distinct n the SRS points and
+    one session, whose anchor and opening cache come from the trapdoor
+    scalars (identical values).  The sample is a seeded stream of the same
+    distribution over the same sessions' sizes, each request applied to the
+    CPU session of its n (updates rewrite s5 and s6 = s4 u only, so every
+    one stays valid there).  Updates that re-anchor are left out of the
+    rate (on the CPU the dense anchor and its opening cache take minutes at
+    n = 65536), so the rate counts sparse proofs only."""
+
+    def __init__(self, sizes, umax, threads, seed=9300):
+        from oracle import dynaverse as D
+        self.sessions = {}
+        traps = bench_trapdoors(sizes)
+        for n in sorted(set(sizes)):
+            tx, ty = traps[n]
+            P = D.Params(n, tx, ty, "bases", threads=threads)
+            pub, w = valid_witness(n, 9000 + sizes.index(n))
+            self.sessions[n] = (D.Session(P, pub, w, verify=False, scalar_anchors=True), w)
+        wits = [self.sessions[n][1] for n in sizes]
+        self.sizes = sizes
+        self.reqs = proof_stream(sizes, wits, 4096, umax, seed)
+        self.pos = 0
+        self.rebuilds = 0
+        self.count = 0
+
+    def sample(self, budget_s):
+        """Sparse proofs/s over the next requests, until budget_s of timed work."""
+        times = []
+        while self.pos < len(self.reqs) and sum(times) < budget_s:
+            j, idx, vals = self.reqs[self.pos]
+            self.pos += 1
+            S = self.sessions[self.sizes[j]][0]
+            values = [int.from_bytes(vals[32 * i:32 * i + 32], "little") for i in range(len(idx))]
+            t0 = time.perf_counter()
+            S.update(idx, values, verify=True)
+            dt = time.perf_counter() - t0
+            if S.last_rebuilt:
+                self.rebuilds += 1
+            else:
+                times.append(dt)
+        self.count += len(times)
+        return (len(times) / sum(times)) if times else None
+
+    def describe(self):
+        ns = "/".join(str(n) for n in sorted(self.sessions))
+        return (f"{self.count} sparse update proofs (n = {ns}) of a seeded stream with the workload's distribution, "
+                f"each proved by the oracle's restatement of the reference's steps and verified with its pairing "
+                f"checks ({self.rebuilds} re-anchoring updates left out)")
+
+
+def operator_points(torch, dv, b, s, imad_peak, threads, with_cpu=True):
+    """The operator targets beside the proof rate: a plain 2^20-point G1 MSM
+    (bases and scalars passed on every call, dvgpu_bn254_msm, as the
+    reference's OperatorBackend::msm does) and a 2^22 forward Fr NTT.  Each:
+    device time with inputs resident and L2 flushed between steps (CUDA
+    events on the launching stream, mean of 20 after 3 warm-ups), end to end
+    through the C-ABI from pinned host buffers, the fraction of the measured
+    IMAD peak, and the CPU oracle on the same inputs with the results
+    compared."""
+    import types
+    from oracle import oracle
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(fn, steps=20, warm=3):
+        for _ in range(warm):
+            r = fn()
+        torch.cuda.synchronize()
+        total = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = fn()
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total / steps, r
+
+    def wall(fn, steps):
+        fn()
         t0 = time.perf_counter()
-        S.update(idx, values, verify=True)
-        dt = time.perf_counter() - t0
-        if S.last_rebuilt:
-            rebuilds += 1
-        else:
-            times.append(dt)
-        if sum(times) >= budget_s:
-            break
-    if not times:
-        return None, "no sparse update of session 0 in the stream"
-    rate = len(times) / sum(times)
-    return rate, (f"{len(times)} sparse update proofs of session 0 (n = {n}) in stream order, each proved by the "
-                  f"oracle's restatement of the reference's steps and verified with its pairing checks "
-                  f"({rebuilds} re-anchoring updates of that session left out)")
+        for _ in range(steps):
+            fn()
+        return (time.perf_counter() - t0) * 1e3 / steps
+
+    out = {}
+    m = MsmOp(types.SimpleNamespace(log_n=20, kind="forward"))
+    m.setup(torch, b, s, 0)
+    ms, res = timed(lambda: m.step(b, s))
+    m.host_inputs(torch)
+    e2e = wall(lambda: m.e2e_step(dv, b), 10)
+    macs = msm_fme(m.n) * 136
+    d = {"call": "dvgpu_bn254_msm (plain: bases and scalars from host memory every call)", "points": m.n,
+         "window_bits": m.tuned_c, "device_ms": ms, "e2e_ms": e2e,
+         "h2d_bytes": m.n * 96, "d2h_bytes": 64 + m.config["windows"] * 128,
+         "roofline": {"bound": "imad", "achieved": macs / (ms * 1e-3) / 1e12, "peak": imad_peak / 1e12,
+                      "unit": "TMAC/s", "frac": macs / (ms * 1e-3) / imad_peak,
+                      "convention": "min_c ceil(254/c)(10 n + 14 2^c) Fq products x 136 MACs"}}
+    if with_cpu:
+        cpu_out, cpu_ms, _ = m.cpu(oracle, threads)
+        d["cpu_oracle"] = {"ms": cpu_ms, "cores": threads, "matches_gpu": cpu_out == res}
+    out["msm_g1_2p20"] = d
+    del m
+    t = NttOp(types.SimpleNamespace(log_n=22, kind="forward"))
+    t.setup(torch, b, s, 0)
+    ms, _ = timed(lambda: t.step(b, s))
+    t.host_inputs(torch)
+    e2e = wall(lambda: t.e2e_step(dv, b), 5)
+    macs = t.fme() * 136
+    d = {"call": "dvgpu_bn254_ntt_ex (forward)", "elements": t.n, "device_ms": ms, "e2e_ms": e2e,
+         "h2d_bytes": 32 * t.n, "d2h_bytes": 32 * t.n,
+         "roofline": {"bound": "imad", "achieved": macs / (ms * 1e-3) / 1e12, "peak": imad_peak / 1e12,
+                      "unit": "TMAC/s", "frac": macs / (ms * 1e-3) / imad_peak,
+                      "convention": "(n/2) log2 n Fr products x 136 MACs",
+                      "hbm_gbs": 64 * t.n / (ms * 1e-3) / 1e9}}
+    if with_cpu:
+        vals = bytes(t.h_src.numpy().tobytes())
+        t0 = time.perf_counter()
+        ref = oracle.ntt(vals, "forward")
+        d["cpu_oracle"] = {"ms": (time.perf_counter() - t0) * 1e3, "cores": 1,
+                           "matches_gpu": ref == bytes(t.dst.cpu().numpy().tobytes())}
+    out["ntt_2p22"] = d
+    return out
 
 
 def proof_stream(sizes, witnesses, count, umax, seed):
@@ -893,7 +997,7 @@ class ProofServeOp:
     one update at a time, each a full pipeline with its own launches), at
     saturation (all requests queued at once) and as a Poisson stream at 80 %
     of the per-call capacity (latency).  Proofs are identical between the
-    forms.  Default: 16 sessions of n = 65536; --mix: 64 sessions with
+    forms.  Default: 64 sessions of n = 65536; --mix: 64 sessions with
     n in {256, 4096, 65536} in ratio 37:18:9."""
 
     def __init__(self, args):
@@ -905,10 +1009,17 @@ class ProofServeOp:
         label = "n 256/4096/65536 mix" if args.mix else f"n={n}"
         self.metric = f"update proofs/s ({label}, served, every proof verified)"
         self.workload = (f"Dynaverse update proofs over {len(self.sizes)} sessions ({label}), {self.requests} requests; "
-                         f"supports of floor(2^U) gates, U~U[0,{self.umax}], half in a 64-gate hotspot window, half "
+                         f"supports of 2 floor(2^U) witness indices (floor(2^U) multiplication gates, wires s5 and s6), "
+                         f"U~U[0,{self.umax}], half in a 64-gate hotspot window, half "
                          "uniform; every gate's s5 a fresh uniform Fr and s6 = s4 s5; re-anchor when the delta "
                          "reaches ceil(sqrt(n)) (session.rs:92)")
         self.profile = "dynaverse_serve"
+
+    def config(self, world):
+        return {"workload": self.workload, "op": "proofs",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "sessions": len(self.sizes), "requests": self.requests,
+                "l2": "not flushed: a stream of requests against resident sessions"}
 
     def _setup(self, dv):
         import random
@@ -940,17 +1051,32 @@ class ProofServeOp:
             e.close_session(sid)
         lat = sorted((r.done_ns - r.submit_ns) / 1e6 for _, r in outs)
         pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
+        # the slowest 1 %: time queued, time in their batch, batch sizes
+        worst = sorted(outs, key=lambda o: o[1].done_ns - o[1].submit_ns)[-max(1, len(outs) // 100):]
+        batch_ms = {}
+        for _, r in outs:
+            batch_ms[r.batch_id] = ((r.done_ns - r.start_ns) / 1e6, r.batch_requests)
+        slowest_batch = max(batch_ms.values())
+        tail = {"queued_ms": sum((r.start_ns - r.submit_ns) / 1e6 for _, r in worst) / len(worst),
+                "in_batch_ms": sum((r.done_ns - r.start_ns) / 1e6 for _, r in worst) / len(worst),
+                "batch_requests": [r.batch_requests for _, r in worst],
+                "slowest_batch_ms": slowest_batch[0], "slowest_batch_requests": slowest_batch[1]}
         return {"proofs": [p for p, _ in outs], "wall_s": wall, "per_s": len(outs) / wall,
                 "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1], "mean_ms": sum(lat) / len(lat),
                 "batches": st.batches - before.batches, "largest_batch": max(r.batch_requests for _, r in outs),
                 "rebuilds": sum(r.rebuilt for _, r in outs), "launches": st.launches - before.launches,
-                "msm_fme": st.msm_fme - before.msm_fme}
+                "msm_fme": st.msm_fme - before.msm_fme, "host_ms": (st.host_ns - before.host_ns) / 1e6,
+                "device_wait_ms": (st.device_wait_ns - before.device_wait_ns) / 1e6,
+                "dense_accum_ms": (st.dense_accum_ns - before.dense_accum_ns) / 1e6,
+                "dense_accum_adds": st.dense_accum_adds - before.dense_accum_adds, "tail": tail}
 
     def run_standalone(self, args, torch, dv, b, s, sampler, imad_peak_fn, world=1):
         import numpy as np
         self._setup(dv)
         zeros = [0.0] * self.requests
-        self._run(64, zeros[:64])  # warm-up: workspaces, tables and NTT plans reach their sizes
+        # warm-up: the whole stream once served (workspaces, tables, NTT plans
+        # and the re-anchor buffer pool reach their sizes), a few per call
+        self._run(64, zeros)
         self._run(1, zeros[:8])
         sampler.start()
         sat_served = self._run(64, zeros)
@@ -970,6 +1096,9 @@ class ProofServeOp:
         peak = imad_peak_fn() / 1e12
         macs = sat_served["msm_fme"] * 136
         ach = macs / sat_served["wall_s"] / 1e12
+        # the dominant kernel: the dense MSMs' bucket accumulation, timed live
+        acc_macs = sat_served["dense_accum_adds"] * 10 * 136
+        acc_ach = acc_macs / max(1e-9, sat_served["dense_accum_ms"] * 1e-3) / 1e12
         strip = lambda r: {k: v for k, v in r.items() if k != "proofs"}
         job_per_s = world * self.requests / max_over_ranks(sat_served["wall_s"], world)
         in_bytes = sum(8 * len(idx) + len(vals) for _, idx, vals in self.reqs) / self.requests
@@ -978,10 +1107,7 @@ class ProofServeOp:
             "steps": self.requests, "warmup": 1, "ms_per_step": 1e3 / sat_served["per_s"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Fq/Fr Montgomery, exact)",
             "data": "synthetic (seeded trapdoors, uniform valid witnesses, seeded update stream)",
-            "config": {"workload": self.workload, "op": "proofs",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "sessions": len(self.sizes), "requests": self.requests,
-                       "l2": "not flushed: a stream of requests against resident sessions"},
+            "config": self.config(world),
             "e2e": {"value": job_per_s, "unit": "proofs/s", "h2d_bytes_per_step": in_bytes,
                     "d2h_bytes_per_step": 9304,
                     "call": "dvgpu_dynaverse_submit/wait from host memory (update in, proof out)"},
@@ -990,20 +1116,30 @@ class ProofServeOp:
                         "poisson": {"rate_per_s": rate, "served": strip(poi_served), "per_call": strip(poi_plain),
                                     "p99_ratio": poi_plain["p99_ms"] / poi_served["p99_ms"]},
                         "bit_exact": exact, "device_verifier_sample_accepted": bool(sample_ok)},
-            "roofline": {"bound": "imad", "kernel": "the whole saturation run (every MSM of every proof)",
-                         "achieved": ach, "peak": peak, "unit": "TMAC/s", "frac": ach / peak,
-                         "algorithmic_macs_per_launch": macs,
-                         "convention": "sum over MSM sets of min_c ceil(254/c)(10k + 14 2^c) x 136 (x3 G2)",
-                         "traffic": None},
+            "roofline": {"bound": "imad",
+                         "kernel": "k_accum of the dense MSMs (anchor openings, re-anchor quotients; c = 16 table)",
+                         "achieved": acc_ach, "peak": peak, "unit": "TMAC/s", "frac": acc_ach / peak,
+                         "peak_source": "dvgpu_probe_imad_rate, measured in this run",
+                         "algorithmic_macs_per_launch": acc_macs / max(1, sat_served["batches"]),
+                         "launch_ms": sat_served["dense_accum_ms"] / max(1, sat_served["batches"]),
+                         "convention": "10 Fq products x 136 MACs per XYZZ mixed addition, 16 per dense term",
+                         "traffic": load_traffic("dynaverse_dense_accum")},
+            "msm_whole_run": {"achieved": ach, "frac": ach / peak, "algorithmic_macs": macs,
+                              "convention": "sum over MSM sets of min_c ceil(254/c)(10k + 14 2^c) x 136 (x3 G2), "
+                                            "over the saturation run's wall time"},
             "gpu_launches": sat_served["launches"], "clocks": clocks,
         }
         self.eng.close()
+        if world == 1 and not args.no_operators:
+            line["operators"] = operator_points(torch, dv, b, s, peak * 1e12, os.cpu_count() or 1,
+                                                with_cpu=not args.no_cpu_baseline)
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1
-            rate, sample = proofs_cpu(self.sizes, self.wit, self.reqs, threads, 20.0)
+            cpu = ProofsCpu(self.sizes, self.umax, threads)
+            rate = cpu.sample(20.0)
             if rate is not None:
                 line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
-                                        "sample": sample}
+                                        "sample": cpu.describe()}
         return line
 
 
@@ -1490,21 +1626,23 @@ def run_reference(args, rank, world):
     n = 1 << args.log_n
     if op == "proofs":
         p = ProofServeOp(args)
-        p._inputs()
+        cpu = ProofsCpu(p.sizes, p.umax, threads)
+        cpu.sample(2.0)  # warm-up
         steps = max(1, args.steps)
-        rates, sample = [], None
-        for _ in range(steps):
-            rate, sample = proofs_cpu(p.sizes, p.wit, p.reqs, threads, 30.0 / steps)
-            if rate is not None:
-                rates.append(rate)
+        rates = [r for r in (cpu.sample(30.0 / steps) for _ in range(steps)) if r is not None]
         value = sum(rates) / len(rates) if rates else None
         print(json.dumps({"impl": "reference", "metric": p.metric, "value": value, "unit": "proofs/s",
-                          "n_gpus": 1, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
-                          "config": {"workload": p.workload, "op": "proofs"},
+                          "n_gpus": world, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "u64 limbs (Fq/Fr, exact)",
+                          "data": "synthetic (seeded trapdoors, uniform valid witnesses, seeded update stream)",
+                          "config": p.config(1),
                           "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port",
-                                           "sample": sample},
+                                           "sample": cpu.describe()},
                           "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0,
-                                  "d2h_bytes_per_step": 0}}), flush=True)
+                                  "d2h_bytes_per_step": 0},
+                          "note": ("reference = the oracle's restatement of the reference's update-proof steps "
+                                   "(oracle/dynaverse.py over oracle/bn254_oracle.cpp); the reference's own "
+                                   "Rust/arkworks code cannot be built in this image")}), flush=True)
         return
     if op in ("msm", "msmres", "g2msm"):
         g2 = op == "g2msm"

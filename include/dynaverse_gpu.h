@@ -648,6 +648,13 @@ typedef struct DvgpuDynaverseStats {
     /* algorithmic G1 field multiplications of every MSM run (min over c of
      * ceil(254/c) (10 k + 14 2^c) per k-term set, x3 for G2 sets) */
     uint64_t msm_fme;
+    /* of busy_ns: host time (staging, checks, publishing) and time blocked
+     * on the device */
+    uint64_t host_ns, device_wait_ns;
+    /* the bucket accumulation of the dense MSMs (anchor openings and
+     * re-anchor quotients), timed by CUDA events on its stream, and its
+     * XYZZ mixed additions (terms x 16 windows) */
+    uint64_t dense_accum_ns, dense_accum_adds;
 } DvgpuDynaverseStats;
 int dvgpu_dynaverse_create(uint64_t hbm_budget_bytes, uint32_t max_batch, void** engine, char* error,
                            size_t error_capacity);

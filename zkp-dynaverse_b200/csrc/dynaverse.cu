@@ -40,10 +40,15 @@
 //    exact division on a coset of the n-point domain, instead of combining
 //    a cache of n single openings per wire (the Precompute policy): the
 //    points are the same (dynaverse.rs:1253-1272) and no G1 transform is
-//    needed at each re-anchor.
+//    needed at each re-anchor.  These dense sets (and a re-anchor's
+//    multiplication quotient) run over a second table of the first n KZG
+//    bases with c = 16 (16 windows), half the additions of the c = 8 one.
 //  * Verification: every equation of the delta (and, once per anchor, of
 //    the anchor) is built on the device from the proof bytes and checked by
-//    the pairing kernels (pairing.cu) in one call per batch.
+//    the pairing kernels (pairing.cu) in one call per batch.  The
+//    verifying key's G2 lines are prepared once per parameter set; the
+//    G2 MSM and the lines of each proof's own G2 points run on a second
+//    stream beside the dense G1 work.
 //
 // Proof bytes: oracle/dynaverse.py's layout, all fields in declaration
 // order (G1 64 B, G2 128 B, wire format): anchor 3968 B, delta 5312 B,
@@ -1178,6 +1183,11 @@ public:
             DV_CUDA(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
             DV_CUDA(cudaEventCreateWithFlags(&ev_fields_, cudaEventDisableTiming));
             DV_CUDA(cudaEventCreateWithFlags(&ev_g2_, cudaEventDisableTiming));
+            // phase events of the G1 workspace: the dense MSM, its last user in
+            // a batch, leaves its accumulation time there for the stats
+            for (auto& e : ws1_.timeline.ev) DV_CUDA(cudaEventCreate(&e));
+            for (auto& e : ws1_.timeline.acc_ev) DV_CUDA(cudaEventCreate(&e));
+            ws1_.timeline.enabled = true;
         });
     }
     ~Engine() {
@@ -1311,6 +1321,10 @@ public:
         s.rebuilds = stat_rebuilds_;
         s.launches = stat_launches_;
         s.msm_fme = stat_fme_.load();
+        s.device_wait_ns = stat_wait_ns_.load();
+        s.dense_accum_ns = stat_dense_ns_.load();
+        s.dense_accum_adds = stat_dense_adds_.load();
+        s.host_ns = s.busy_ns > s.device_wait_ns ? s.busy_ns - s.device_wait_ns : 0;
         return s;
     }
 
@@ -1383,6 +1397,13 @@ private:
             stat_launches_ += launch_counter() - l0;
             done_cv_.notify_all();
         }
+        ws1_.timeline.enabled = false;
+        for (auto& e : ws1_.timeline.ev)
+            if (e) cudaEventDestroy(e);
+        for (auto& e : ws1_.timeline.acc_ev)
+            if (e) cudaEventDestroy(e);
+        for (auto& sp : spare_) cudaFree(sp.first);
+        spare_.clear();
         if (ev_fields_) cudaEventDestroy(ev_fields_);
         if (ev_g2_) cudaEventDestroy(ev_g2_);
         if (st2_) cudaStreamDestroy(st2_);
@@ -1437,6 +1458,34 @@ private:
     uint64_t stat_requests_ = 0, stat_batches_ = 0, stat_largest_ = 0, stat_busy_ns_ = 0, stat_sparse_ = 0,
              stat_rebuilds_ = 0, stat_launches_ = 0;
     std::atomic<uint64_t> stat_fme_{0};  // written by the worker, read by stats()
+    std::atomic<uint64_t> stat_wait_ns_{0}, stat_dense_ns_{0}, stat_dense_adds_{0};
+    // Device buffers that re-anchors swap out of sessions (coefficients,
+    // anchor bytes), kept for the next re-anchor: a re-anchor allocates
+    // nothing once the pool holds a batch's worth, and frees nothing.
+    std::vector<std::pair<void*, size_t>> spare_;
+    void take(DevBuf& b, size_t bytes) {
+        if (b.ptr && b.cap >= bytes) return;
+        for (size_t i = 0; i < spare_.size(); ++i)
+            if (spare_[i].second >= bytes) {
+                b.release();
+                b.ptr = spare_[i].first;
+                b.cap = spare_[i].second;
+                spare_[i] = spare_.back();
+                spare_.pop_back();
+                return;
+            }
+        b.get(bytes);
+    }
+    void give(DevBuf& b) {
+        if (!b.ptr) return;
+        if (spare_.size() < 4ull * max_batch_ + 8) {
+            spare_.push_back({b.ptr, b.cap});
+            b.ptr = nullptr;
+            b.cap = 0;
+        } else {
+            b.release();
+        }
+    }
     std::thread worker_;
 };
 
@@ -1751,8 +1800,10 @@ void Engine::run_anchor(Params& P, const std::vector<Canon>& w, const std::vecto
     const uint64_t W = 0, H = 6 * n, PB = 13 * n, Q = 14 * n, P0 = 15 * n, P1 = 17 * n, TOT = 19 * n;
     const cudaStream_t st = st_;
     Fr* arena = arena_.as<Fr>(TOT);
-    Fr* coef = job.new_coef.as<Fr>(3 * n);
-    uint8_t* anc = job.new_anchor.as<uint8_t>(ANCHOR_BYTES);
+    take(job.new_coef, 3 * n * sizeof(Fr));
+    take(job.new_anchor, ANCHOR_BYTES);
+    Fr* coef = job.new_coef.view<Fr>();
+    uint8_t* anc = job.new_anchor.view<uint8_t>();
     uint8_t* rec = out_.as<uint8_t>(JOB_BYTES);
     uint32_t* status = status_.as<uint32_t>(1);
     uint8_t* verd = verdicts_.as<uint8_t>(ANCHOR_EQS);
@@ -2167,7 +2218,11 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     // host behind the queued work and leave the GPU idle meanwhile.
     std::vector<std::pair<uint32_t, Fr*>> coefs;  // re-anchor jobs and their new coefficient buffers
     for (uint32_t j = 0; j < B; ++j)
-        if (jl[j].rb) coefs.push_back({j, jobs[j]->new_coef.as<Fr>(3ull * n)});
+        if (jl[j].rb) {
+            take(jobs[j]->new_coef, 3ull * n * sizeof(Fr));
+            take(jobs[j]->new_anchor, ANCHOR_BYTES);
+            coefs.push_back({j, jobs[j]->new_coef.view<Fr>()});
+        }
     const bool dense = kjob[B] > 0, rebuild = !coefs.empty();
     {
         std::vector<NttBatchItem> fwd, inv, r1, r2, r3;
@@ -2334,7 +2389,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     pairing_check_prepared(*b_, tp1, terms, lines_.view<uint8_t>(), qinf_.view<uint32_t>(), tq1,
                            reinterpret_cast<const uint64_t*>(d + at_off), eqs, verd, st);
     for (auto& jc : coefs) {
-        uint8_t* an = jobs[jc.first]->new_anchor.as<uint8_t>(ANCHOR_BYTES);
+        uint8_t* an = jobs[jc.first]->new_anchor.view<uint8_t>();
         DV_CUDA(cudaMemcpyAsync(an, out + (uint64_t)jc.first * JOB_BYTES + REC_ANCHOR, ANCHOR_BYTES,
                                 cudaMemcpyDeviceToDevice, st));
     }
@@ -2344,7 +2399,15 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     DV_CUDA(cudaMemcpyAsync(hout + ob, status, 4ull * B, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B, err, 12, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B + 16, verd, eqs, cudaMemcpyDeviceToHost, st));
+    const uint64_t w0 = now_ns();
     DV_CUDA(cudaStreamSynchronize(st));
+    stat_wait_ns_ += now_ns() - w0;
+    if (md.terms) {
+        float ms = 0;
+        DV_CUDA(cudaEventElapsedTime(&ms, ws1_.timeline.acc_ev[0], ws1_.timeline.acc_ev[1]));
+        stat_dense_ns_ += (uint64_t)(ms * 1e6);
+        stat_dense_adds_ += (uint64_t)md.terms * TWD;
+    }
     if (dense) {
         ntt_batch_check(nb_fwd_, st);
         ntt_batch_check(nb_inv_, st);
@@ -2693,6 +2756,11 @@ void Engine::process(std::vector<Request>& batch, std::vector<Session*>& sess, s
         memcpy(S.public_h, J.public_h, 64);
         outs[r].proof = J.proof;
         outs[r].res.rebuilt = J.rebuild ? 1 : 0;
+    }
+    // the buffers a re-anchor swapped out of its session (or did not use)
+    for (auto& J : jobs) {
+        give(J.new_coef);
+        give(J.new_anchor);
     }
 }
 
