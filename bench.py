@@ -72,6 +72,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--probe", choices=["update", "batch"], default=None,
+                    help="proofs: run one fixed case for a profiler and exit (no timing line): 'update' = two "
+                         "sessions of n = 2^log-n opened, then one per-call update of 64 gates; 'batch' = 64 "
+                         "sessions, then one served batch of 64 updates")
     ap.add_argument("--no-operators", action="store_true",
                     help="proofs: leave out the MSM 2^20 / NTT 2^22 operator points")
     a = ap.parse_args()
@@ -166,14 +170,14 @@ def device_view(torch, ptr, nbytes):
     return torch.as_tensor(_DeviceBytes(ptr, nbytes), device="cuda")
 
 
-def load_traffic(name):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary profiles/<name>.txt (line 'traffic_bytes_per_launch: X')."""
+def load_traffic(name, key="traffic_bytes_per_launch"):
+    """DRAM bytes of the dominant kernel from the committed ncu summary
+    profiles/<name>.txt (line '<key>: X', per launch by default)."""
     path = os.path.join(ROOT, "profiles", name + ".txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1])
             except ValueError:
@@ -831,28 +835,27 @@ def bench_trapdoors(sizes, seed=9900):
 class ProofsCpu:
     """The CPU restatement of the reference's sparse update path (oracle,
     bases route: sparse MSMs over the SRS points, the subproduct tree, FFT
-    products and exact division, then the pairing verifier) on a sample of
-    the workload.  Setup is not timed: per distinct n the SRS points and
-    one session, whose anchor and opening cache come from the trapdoor
-    scalars (identical values).  The sample is a seeded stream of the same
-    distribution over the same sessions' sizes, each request applied to the
-    CPU session of its n (updates rewrite s5 and s6 = s4 u only, so every
-    one stays valid there).  Updates that re-anchor are left out of the
-    rate (on the CPU the dense anchor and its opening cache take minutes at
-    n = 65536), so the rate counts sparse proofs only."""
+    products and exact division, then the pairing verifier) on the GPU
+    arm's own request stream, in order.  Setup is not timed: per distinct n
+    the SRS points and one session on the sessions' common initial witness,
+    whose anchor and opening cache come from the trapdoor scalars (identical
+    values).  Each request goes to the CPU session of its n (updates rewrite
+    s5 and s6 = s4 u only, so every one stays valid there).  Updates that
+    re-anchor are left out of the rate (on the CPU the dense anchor and its
+    opening cache take minutes at n = 65536), so the rate counts sparse
+    proofs only."""
 
-    def __init__(self, sizes, umax, threads, seed=9300):
+    def __init__(self, op, threads):
         from oracle import dynaverse as D
         self.sessions = {}
-        traps = bench_trapdoors(sizes)
-        for n in sorted(set(sizes)):
+        traps = bench_trapdoors(op.sizes)
+        for n in sorted(set(op.sizes)):
             tx, ty = traps[n]
             P = D.Params(n, tx, ty, "bases", threads=threads)
-            pub, w = valid_witness(n, 9000 + sizes.index(n))
-            self.sessions[n] = (D.Session(P, pub, w, verify=False, scalar_anchors=True), w)
-        wits = [self.sessions[n][1] for n in sizes]
-        self.sizes = sizes
-        self.reqs = proof_stream(sizes, wits, 4096, umax, seed)
+            pub, w = op.wit[op.sizes.index(n)]
+            self.sessions[n] = D.Session(P, pub, w, verify=False, scalar_anchors=True)
+        self.sizes = op.sizes
+        self.reqs = op.reqs
         self.pos = 0
         self.rebuilds = 0
         self.count = 0
@@ -863,7 +866,7 @@ class ProofsCpu:
         while self.pos < len(self.reqs) and sum(times) < budget_s:
             j, idx, vals = self.reqs[self.pos]
             self.pos += 1
-            S = self.sessions[self.sizes[j]][0]
+            S = self.sessions[self.sizes[j]]
             values = [int.from_bytes(vals[32 * i:32 * i + 32], "little") for i in range(len(idx))]
             t0 = time.perf_counter()
             S.update(idx, values, verify=True)
@@ -877,9 +880,52 @@ class ProofsCpu:
 
     def describe(self):
         ns = "/".join(str(n) for n in sorted(self.sessions))
-        return (f"{self.count} sparse update proofs (n = {ns}) of a seeded stream with the workload's distribution, "
-                f"each proved by the oracle's restatement of the reference's steps and verified with its pairing "
-                f"checks ({self.rebuilds} re-anchoring updates left out)")
+        return (f"{self.count} sparse update proofs (n = {ns}): the benchmark's own request stream in order, each "
+                f"proved by the oracle's restatement of the reference's steps and verified with its pairing checks "
+                f"({self.rebuilds} re-anchoring updates left out)")
+
+
+def proof_probe(dv, kind, n):
+    """A fixed case of the update-proof pipeline for profiler captures.
+    k_accum launches: two per session open (G1, G2 sets), then per batch m1,
+    m3 (G2), m2 and md (the dense sets) -- so 'update' has md at k_accum
+    launch 7 and 'batch' at 131."""
+    import threading
+    import numpy as np
+    sessions, batch = (2, 1) if kind == "update" else (64, 64)
+    e = dv.DynaverseEngine(100 << 30, batch)
+    tx, ty = bench_trapdoors([n])[n]
+    ph = e.params_create(n, tx, ty)
+    enc = lambda xs: b"".join(v.to_bytes(32, "little") for v in xs)
+    pub, w = valid_witness(n, 9000)
+    pb, wb = enc(pub), enc(w)
+    ids = [e.open_session(ph, pb, wb)[0] for _ in range(sessions)]
+    rng = np.random.default_rng(5)
+    reqs = []
+    for sid in ids[:batch]:
+        g = 64 if kind == "update" else int(2 ** rng.uniform(0, 6))
+        idx, vals = [], []
+        for gate in rng.choice(n, size=g, replace=False).tolist():
+            u = int(rng.integers(1, 1 << 62))
+            idx += [4 * n + gate, 5 * n + gate]
+            vals += [u, w[3 * n + gate] * u % R_FR]
+        reqs.append((sid, idx, enc(vals)))
+    busy = None
+    if kind == "batch":
+        # a parameter build holds the engine's worker while all 64 requests queue
+        n2 = n // 4
+        tx2, ty2 = bench_trapdoors([n2])[n2]
+        busy = threading.Thread(target=lambda: e.params_create(n2, tx2, ty2))
+        busy.start()
+        time.sleep(0.01)
+    outs = [e.wait(t) for t in [e.submit(sid, idx, v) for sid, idx, v in reqs]]
+    if busy:
+        busy.join()
+    st = e.stats()
+    print(json.dumps({"probe": kind, "n": n, "batches": len(set(r.batch_id for _, r in outs)),
+                      "batch_ms": (outs[0][1].done_ns - outs[0][1].start_ns) / 1e6,
+                      "dense_accum_ms": st.dense_accum_ns / 1e6, "dense_accum_adds": st.dense_accum_adds}))
+    e.close()
 
 
 def operator_points(torch, dv, b, s, imad_peak, threads, with_cpu=True):
@@ -1028,9 +1074,15 @@ class ProofServeOp:
         self._inputs()
 
     def _inputs(self):
-        self.wit = [valid_witness(n, 9000 + j) for j, n in enumerate(self.sizes)]
-        self.pub_b = [b"".join(v.to_bytes(32, "little") for v in p) for p, _ in self.wit]
-        self.wit_b = [b"".join(v.to_bytes(32, "little") for v in w) for _, w in self.wit]
+        # sessions of one size open on the same seeded witness (their states
+        # then diverge), so the stream is valid on the CPU arm's one session
+        # per size and both arms process the same requests
+        by_n = {n: valid_witness(n, 9000 + n.bit_length()) for n in sorted(set(self.sizes))}
+        enc = {n: (b"".join(v.to_bytes(32, "little") for v in p), b"".join(v.to_bytes(32, "little") for v in w))
+               for n, (p, w) in by_n.items()}
+        self.wit = [by_n[n] for n in self.sizes]
+        self.pub_b = [enc[n][0] for n in self.sizes]
+        self.wit_b = [enc[n][1] for n in self.sizes]
         self.reqs = proof_stream(self.sizes, [w for _, w in self.wit], self.requests, self.umax, 9100)
 
     def _run(self, max_batch, arrivals):
@@ -1068,7 +1120,8 @@ class ProofServeOp:
                 "msm_fme": st.msm_fme - before.msm_fme, "host_ms": (st.host_ns - before.host_ns) / 1e6,
                 "device_wait_ms": (st.device_wait_ns - before.device_wait_ns) / 1e6,
                 "dense_accum_ms": (st.dense_accum_ns - before.dense_accum_ns) / 1e6,
-                "dense_accum_adds": st.dense_accum_adds - before.dense_accum_adds, "tail": tail}
+                "dense_accum_adds": st.dense_accum_adds - before.dense_accum_adds,
+                "allocations": st.allocations - before.allocations, "tail": tail}
 
     def run_standalone(self, args, torch, dv, b, s, sampler, imad_peak_fn, world=1):
         import numpy as np
@@ -1123,7 +1176,11 @@ class ProofServeOp:
                          "algorithmic_macs_per_launch": acc_macs / max(1, sat_served["batches"]),
                          "launch_ms": sat_served["dense_accum_ms"] / max(1, sat_served["batches"]),
                          "convention": "10 Fq products x 136 MACs per XYZZ mixed addition, 16 per dense term",
-                         "traffic": load_traffic("dynaverse_dense_accum")},
+                         "traffic": (None if load_traffic("dynaverse_dense_accum", "traffic_bytes_per_add") is None
+                                     else load_traffic("dynaverse_dense_accum", "traffic_bytes_per_add") *
+                                     sat_served["dense_accum_adds"] / max(1, sat_served["batches"])),
+                         "traffic_note": ("DRAM bytes per mixed addition of a captured 64-job launch "
+                                          "(profiles/dynaverse_dense_accum.txt) x this run's additions per launch")},
             "msm_whole_run": {"achieved": ach, "frac": ach / peak, "algorithmic_macs": macs,
                               "convention": "sum over MSM sets of min_c ceil(254/c)(10k + 14 2^c) x 136 (x3 G2), "
                                             "over the saturation run's wall time"},
@@ -1135,7 +1192,7 @@ class ProofServeOp:
                                                 with_cpu=not args.no_cpu_baseline)
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1
-            cpu = ProofsCpu(self.sizes, self.umax, threads)
+            cpu = ProofsCpu(self, threads)
             rate = cpu.sample(20.0)
             if rate is not None:
                 line["cpu_baseline"] = {"value": rate, "unit": "proofs/s", "cores": threads, "kind": "port",
@@ -1626,7 +1683,8 @@ def run_reference(args, rank, world):
     n = 1 << args.log_n
     if op == "proofs":
         p = ProofServeOp(args)
-        cpu = ProofsCpu(p.sizes, p.umax, threads)
+        p._inputs()
+        cpu = ProofsCpu(p, threads)
         cpu.sample(2.0)  # warm-up
         steps = max(1, args.steps)
         rates = [r for r in (cpu.sample(30.0 / steps) for _ in range(steps)) if r is not None]
@@ -1823,6 +1881,10 @@ def main():
     s = stream.cuda_stream
     op = make_op(args)
     op._b = b
+    if args.probe:
+        proof_probe(dv, args.probe, 1 << args.log_n)
+        b.close()
+        return
     if hasattr(op, "run_standalone"):
         try:
             bus = torch.cuda.get_device_properties(dev).pci_bus_id

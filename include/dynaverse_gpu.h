@@ -655,6 +655,9 @@ typedef struct DvgpuDynaverseStats {
      * re-anchor quotients), timed by CUDA events on its stream, and its
      * XYZZ mixed additions (terms x 16 windows) */
     uint64_t dense_accum_ns, dense_accum_adds;
+    /* device and pinned-host allocations made while serving (growth of the
+     * engine's grow-only workspaces) */
+    uint64_t allocations;
 } DvgpuDynaverseStats;
 int dvgpu_dynaverse_create(uint64_t hbm_budget_bytes, uint32_t max_batch, void** engine, char* error,
                            size_t error_capacity);

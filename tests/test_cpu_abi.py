@@ -56,6 +56,21 @@ def test_diagnostic_struct_layouts(dv, tmp_path):
     assert ctypes.sizeof(dv.MsmTimeline) == 8 * (5 * 9 + 2 * 10 + 6)
 
 
+def test_dynaverse_struct_layouts(dv, tmp_path):
+    """The update-proof engine's records agree in C and in the Python mirror."""
+    src = tmp_path / "dv_sizes.c"
+    stats = ctypes.sizeof(dv.DynaverseStats)
+    info = ctypes.sizeof(dv.DynaverseParamsInfo)
+    res = ctypes.sizeof(dv.DynaverseResult)
+    src.write_text('#include "dynaverse_gpu.h"\n'
+                   f"_Static_assert(sizeof(DvgpuDynaverseStats) == {stats}, \"stats\");\n"
+                   f"_Static_assert(sizeof(DvgpuDynaverseParamsInfo) == {info}, \"info\");\n"
+                   f"_Static_assert(sizeof(DvgpuDynaverseResult) == {res}, \"result\");\n"
+                   "_Static_assert(DVGPU_DYNAVERSE_PROOF_BYTES == 3968 + 5312 + 24, \"proof\");\n")
+    subprocess.run(["gcc", "-fsyntax-only", "-I", os.path.dirname(HEADER), str(src)], check=True)
+    assert stats == 8 * 18 and dv.DYNAVERSE_PROOF_BYTES == 9304
+
+
 def test_every_symbol_the_reference_crate_binds_is_declared():
     """Every dvgpu_* function named in the reference's Rust extern blocks
     (crates/gpu/src) is declared, so the crate links against the library

@@ -1324,6 +1324,7 @@ public:
         s.device_wait_ns = stat_wait_ns_.load();
         s.dense_accum_ns = stat_dense_ns_.load();
         s.dense_accum_adds = stat_dense_adds_.load();
+        s.allocations = stat_allocs_;
         s.host_ns = s.busy_ns > s.device_wait_ns ? s.busy_ns - s.device_wait_ns : 0;
         return s;
     }
@@ -1376,6 +1377,7 @@ private:
             lk.unlock();
             const uint64_t t0 = now_ns();
             const uint64_t l0 = launch_counter();
+            const uint64_t a0 = __atomic_load_n(&alloc_counter(), __ATOMIC_RELAXED);
             std::vector<Outcome> outs(batch.size());
             process(batch, sess, outs);
             const uint64_t t1 = now_ns();
@@ -1395,6 +1397,7 @@ private:
             stat_largest_ = std::max<uint64_t>(stat_largest_, batch.size());
             stat_busy_ns_ += t1 - t0;
             stat_launches_ += launch_counter() - l0;
+            stat_allocs_ += __atomic_load_n(&alloc_counter(), __ATOMIC_RELAXED) - a0;
             done_cv_.notify_all();
         }
         ws1_.timeline.enabled = false;
@@ -1459,6 +1462,7 @@ private:
              stat_rebuilds_ = 0, stat_launches_ = 0;
     std::atomic<uint64_t> stat_fme_{0};  // written by the worker, read by stats()
     std::atomic<uint64_t> stat_wait_ns_{0}, stat_dense_ns_{0}, stat_dense_adds_{0};
+    uint64_t stat_allocs_ = 0;  // under mu_
     // Device buffers that re-anchors swap out of sessions (coefficients,
     // anchor bytes), kept for the next re-anchor: a re-anchor allocates
     // nothing once the pool holds a batch's worth, and frees nothing.

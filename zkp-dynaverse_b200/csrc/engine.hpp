@@ -23,6 +23,9 @@ inline void cuda_check(cudaError_t s, const char* what) {
 }
 // Number of this library's kernel launches since load (all owners).
 uint64_t& launch_counter();
+// Number of this library's device and pinned-host allocations since load.
+uint64_t& alloc_counter();
+inline void allocated() { __atomic_add_fetch(&alloc_counter(), 1, __ATOMIC_RELAXED); }
 inline void launched() {
     cuda_check(cudaGetLastError(), "kernel launch");
     __atomic_add_fetch(&launch_counter(), 1, __ATOMIC_RELAXED);
@@ -43,6 +46,7 @@ struct DevBuf {
         size_t want = bytes < 256 ? 256 : bytes;
         if (regrow > want) want = regrow;
         DV_CUDA(cudaMalloc(&ptr, want));
+        allocated();
         cap = want;
         return ptr;
     }
@@ -65,15 +69,20 @@ struct DevBuf {
     DevBuf& operator=(const DevBuf&) = delete;
 };
 
-// Grow-only pinned host buffer.
+// Grow-only pinned host buffer, with the same 1.5x headroom (freeing pinned
+// memory synchronises the device, so a stream of slowly growing requests
+// must not reallocate every time).
 struct PinnedBuf {
     void* ptr = nullptr;
     size_t cap = 0;
     void* get(size_t bytes) {
         if (bytes <= cap && ptr) return ptr;
+        const size_t regrow = cap ? cap + cap / 2 : 0;
         release();
         size_t want = bytes < 256 ? 256 : bytes;
+        if (regrow > want) want = regrow;
         DV_CUDA(cudaMallocHost(&ptr, want));
+        allocated();
         cap = want;
         return ptr;
     }

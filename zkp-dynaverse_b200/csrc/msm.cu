@@ -850,12 +850,41 @@ struct SdJob {
     uint32_t request, first, items, pad;  // terms first .. first + items - 1 (term = entry W + window)
 };
 
+// XYZZ point read past L1: written by another block of this launch (made
+// visible by its __threadfence before the counter increment below).
+DV_INL XYZZ<Fq> load_cg(const XYZZ<Fq>* p) {
+    XYZZ<Fq> r;
+    const uint4* src = reinterpret_cast<const uint4*>(p);
+    uint4* dst = reinterpret_cast<uint4*>(&r);
+    for (int i = 0; i < (int)(sizeof(XYZZ<Fq>) / 16); ++i) dst[i] = __ldcg(src + i);
+    return r;
+}
+
+DV_INL void block_sum(XYZZ<Fq>* sm) {
+    for (int stride = SD_BLOCK / 2; stride > 0; stride >>= 1) {
+        if (threadIdx.x < (unsigned)stride)
+            sm[threadIdx.x] = XYZZ<Fq>::add_paired(sm[threadIdx.x], sm[threadIdx.x + stride]);
+        __syncthreads();
+    }
+}
+
+// Sparse MSMs over a window table in one launch.  Each block takes up to
+// SD_BLOCK (entry, window) terms of one request: a thread forms d T (the
+// signed c-bit digit d of the entry's window, T the table's multiple
+// 2^(c w) P) by double-and-add, the block sums its threads.  The last block
+// of a request to finish (a per-request counter, reset by that block for the
+// next call) sums the request's block partials, normalises to affine and
+// writes the canonical result bytes: no second launch and no host
+// arithmetic.
 __global__ void __launch_bounds__(SD_BLOCK) k_sparse_direct(const G1A* __restrict__ table, uint64_t nbases, int c,
                                                             int W, const uint64_t* __restrict__ idx,
                                                             const uint32_t* __restrict__ vals,
                                                             const SdJob* __restrict__ jobs,
-                                                            XYZZ<Fq>* __restrict__ partial, uint32_t* __restrict__ err) {
+                                                            const uint32_t* __restrict__ req_blocks,
+                                                            XYZZ<Fq>* __restrict__ partial, uint32_t* __restrict__ done,
+                                                            uint8_t* __restrict__ out, uint32_t* __restrict__ err) {
     __shared__ XYZZ<Fq> sm[SD_BLOCK];
+    __shared__ bool last;
     const SdJob job = jobs[blockIdx.x];
     XYZZ<Fq> p = XYZZ<Fq>::inf();
     if (threadIdx.x < job.items) {
@@ -892,31 +921,33 @@ __global__ void __launch_bounds__(SD_BLOCK) k_sparse_direct(const G1A* __restric
     }
     sm[threadIdx.x] = p;
     __syncthreads();
-    for (int stride = SD_BLOCK / 2; stride > 0; stride >>= 1) {
-        if (threadIdx.x < (unsigned)stride)
-            sm[threadIdx.x] = XYZZ<Fq>::add_paired(sm[threadIdx.x], sm[threadIdx.x + stride]);
-        __syncthreads();
+    block_sum(sm);
+    const uint32_t r = job.request, b0 = req_blocks[r], b1 = req_blocks[r + 1];
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = sm[0];
+        __threadfence();
+        last = atomicAdd(done + r, 1u) == b1 - b0 - 1;
     }
-    if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
-}
-
-constexpr int SD_FINAL = 64;
-__global__ void __launch_bounds__(SD_FINAL) k_sparse_direct_final(const XYZZ<Fq>* __restrict__ partial,
-                                                                  const uint32_t* __restrict__ req_blocks,
-                                                                  XYZZ<Fq>* __restrict__ out) {
-    __shared__ XYZZ<Fq> sm[SD_FINAL];
-    const uint32_t r = blockIdx.x;
-    XYZZ<Fq> p = XYZZ<Fq>::inf();
-    for (uint32_t b = req_blocks[r] + threadIdx.x; b < req_blocks[r + 1]; b += SD_FINAL)
-        p = XYZZ<Fq>::add_paired(p, partial[b]);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    p = XYZZ<Fq>::inf();
+    for (uint32_t b = b0 + threadIdx.x; b < b1; b += SD_BLOCK) p = XYZZ<Fq>::add_paired(p, load_cg(partial + b));
     sm[threadIdx.x] = p;
     __syncthreads();
-    for (int stride = SD_FINAL / 2; stride > 0; stride >>= 1) {
-        if (threadIdx.x < (unsigned)stride)
-            sm[threadIdx.x] = XYZZ<Fq>::add_paired(sm[threadIdx.x], sm[threadIdx.x + stride]);
-        __syncthreads();
+    block_sum(sm);
+    if (threadIdx.x == 0) {
+        done[r] = 0;
+        uint8_t* o = out + 64ull * r;
+        if (sm[0].is_inf()) {
+            const uint4 z = make_uint4(0, 0, 0, 0);
+            for (int i = 0; i < 4; ++i) reinterpret_cast<uint4*>(o)[i] = z;
+        } else {
+            const G1A a = sm[0].to_affine();
+            store_canonical(o, a.x);
+            store_canonical(o + 32, a.y);
+        }
     }
-    if (threadIdx.x == 0) out[r] = sm[0];
 }
 
 void msm_sparse_direct(MsmWorkspace& ws, const MsmPrecomp<Fq>& pre, uint64_t nbases, const uint64_t* d_idx,
@@ -925,38 +956,45 @@ void msm_sparse_direct(MsmWorkspace& ws, const MsmPrecomp<Fq>& pre, uint64_t nba
     const uint32_t W = (uint32_t)pre.windows;
     std::vector<SdJob> jobs;
     std::vector<uint32_t> req_blocks(count + 1, 0);
+    bool empty = false;
     for (uint32_t r = 0; r < count; ++r) {
         const uint32_t first = offs[r] * W, terms = (offs[r + 1] - offs[r]) * W;
         for (uint32_t t = 0; t < terms; t += SD_BLOCK)
             jobs.push_back(SdJob{r, first + t, std::min<uint32_t>(SD_BLOCK, terms - t), 0});
         req_blocks[r + 1] = (uint32_t)jobs.size();
+        empty |= terms == 0;
     }
     if (jobs.empty()) {
         memset(host_out, 0, (size_t)count * 64);
         return;
     }
-    SdJob* d_jobs = ws.sd_jobs.as<SdJob>(jobs.size());
-    uint32_t* d_req = ws.sd_req.as<uint32_t>(count + 1);
+    // one upload: the block list, then the per-request block offsets
+    const size_t jb = jobs.size() * sizeof(SdJob), rb = (count + 1) * sizeof(uint32_t);
+    uint8_t* h_desc = ws.host_desc.as<uint8_t>(jb + rb);
+    memcpy(h_desc, jobs.data(), jb);
+    memcpy(h_desc + jb, req_blocks.data(), rb);
+    uint8_t* d_desc = ws.sd_jobs.as<uint8_t>(jb + rb);
     XYZZ<Fq>* d_partial = ws.sd_partial.as<XYZZ<Fq>>(jobs.size());
-    XYZZ<Fq>* d_out = ws.sd_out.as<XYZZ<Fq>>(count);
-    uint32_t* d_err = ws.err.as<uint32_t>(2);
-    DV_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(SdJob), cudaMemcpyHostToDevice, st));
-    DV_CUDA(cudaMemcpyAsync(d_req, req_blocks.data(), (count + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    uint32_t* d_done = ws.sd_req.as<uint32_t>(count);
+    uint8_t* d_out = ws.sd_out.as<uint8_t>((size_t)count * 64 + 16);
+    uint32_t* d_err = reinterpret_cast<uint32_t*>(d_out + (size_t)count * 64);
+    DV_CUDA(cudaMemcpyAsync(d_desc, h_desc, jb + rb, cudaMemcpyHostToDevice, st));
+    DV_CUDA(cudaMemsetAsync(d_done, 0, count * sizeof(uint32_t), st));
+    if (empty) DV_CUDA(cudaMemsetAsync(d_out, 0, (size_t)count * 64, st));
     DV_CUDA(cudaMemsetAsync(d_err, 0xff, 2 * sizeof(uint32_t), st));
-    k_sparse_direct<<<(unsigned)jobs.size(), SD_BLOCK, 0, st>>>(pre.table, nbases, pre.c, (int)W, d_idx, d_vals,
-                                                               d_jobs, d_partial, d_err);
+    k_sparse_direct<<<(unsigned)jobs.size(), SD_BLOCK, 0, st>>>(
+        pre.table, nbases, pre.c, (int)W, d_idx, d_vals, reinterpret_cast<const SdJob*>(d_desc),
+        reinterpret_cast<const uint32_t*>(d_desc + jb), d_partial, d_done, d_out, d_err);
     DV_LAUNCH();
-    k_sparse_direct_final<<<count, SD_FINAL, 0, st>>>(d_partial, d_req, d_out);
-    DV_LAUNCH();
-    XYZZ<Fq>* h_out = ws.host_windows.as<XYZZ<Fq>>(count);
-    uint32_t* h_err = ws.host_err.as<uint32_t>(2);
-    DV_CUDA(cudaMemcpyAsync(h_out, d_out, (size_t)count * sizeof(XYZZ<Fq>), cudaMemcpyDeviceToHost, st));
-    DV_CUDA(cudaMemcpyAsync(h_err, d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    // one copy back: the results, then the two error words
+    uint8_t* h_out = ws.host_windows.as<uint8_t>((size_t)count * 64 + 16);
+    DV_CUDA(cudaMemcpyAsync(h_out, d_out, (size_t)count * 64 + 8, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaStreamSynchronize(st));
+    uint32_t h_err[2];
+    memcpy(h_err, h_out + (size_t)count * 64, 8);
     if (h_err[0] != NO_INDEX) throw InvalidArgument("non-canonical scalar at index " + std::to_string(h_err[0]));
     if (h_err[1] != NO_INDEX) throw InvalidArgument("sparse MSM index out of range");
-    static_assert(sizeof(XYZZ<Fq>) == sizeof(dvh::XYZZ<dvh::Fq>), "host/device XYZZ layout");
-    dvh::xyzz_batch_to_affine_bytes(reinterpret_cast<const dvh::XYZZ<dvh::Fq>*>(h_out), count, host_out);
+    memcpy(host_out, h_out, (size_t)count * 64);
 }
 
 template void msm_run<Fq>(MsmWorkspace&, const Affine<Fq>*, const uint32_t*, const uint32_t*, uint32_t, int,

@@ -60,7 +60,7 @@ struct MsmWorkspace {
     DevBuf set_off, counts, offsets, cursor, scan_tiles, sorted, buckets, pgid, ppt, fix_list, fix_count, segs, windows,
         err;
     DevBuf sd_jobs, sd_req, sd_partial, sd_out;  // direct small sparse MSMs
-    PinnedBuf host_windows, host_err;
+    PinnedBuf host_windows, host_err, host_desc;
     MsmTimeline timeline;
 };
 
