@@ -1121,7 +1121,9 @@ class ProofServeOp:
                 "device_wait_ms": (st.device_wait_ns - before.device_wait_ns) / 1e6,
                 "dense_accum_ms": (st.dense_accum_ns - before.dense_accum_ns) / 1e6,
                 "dense_accum_adds": st.dense_accum_adds - before.dense_accum_adds,
-                "allocations": st.allocations - before.allocations, "tail": tail}
+                "allocations": st.allocations - before.allocations,
+                "allocation_ms": (st.allocation_ns - before.allocation_ns) / 1e6,
+                "enqueue_ms": (st.enqueue_ns - before.enqueue_ns) / 1e6, "tail": tail}
 
     def run_standalone(self, args, torch, dv, b, s, sampler, imad_peak_fn, world=1):
         import numpy as np

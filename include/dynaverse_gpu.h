@@ -657,7 +657,10 @@ typedef struct DvgpuDynaverseStats {
     uint64_t dense_accum_ns, dense_accum_adds;
     /* device and pinned-host allocations made while serving (growth of the
      * engine's grow-only workspaces) */
-    uint64_t allocations;
+    uint64_t allocations, allocation_ns;
+    /* host time from a batch's first launch to its synchronisation (the
+     * enqueue phase, which allocation inside it lengthens) */
+    uint64_t enqueue_ns;
 } DvgpuDynaverseStats;
 int dvgpu_dynaverse_create(uint64_t hbm_budget_bytes, uint32_t max_batch, void** engine, char* error,
                            size_t error_capacity);

@@ -217,3 +217,92 @@ def test_n65536_sparse_updates_and_reanchor_match_oracle(engine):
     assert ref.proof.anchor_generation > 0  # the last update re-anchored
     engine.close_session(s)
     engine.params_destroy(ph)
+
+
+def test_admission_budget_and_lifecycle_rules(dv):
+    """HBM admission by measured footprint (parameters and sessions), unknown
+    handles, closing a session while its update is queued, and releasing
+    parameters that still have sessions: each refused with status -1 and the
+    engine still serving afterwards."""
+    import threading
+    n = 16
+    tx, ty = D.sample_trapdoors(15303, n)
+    pub, w = D.valid_instance(n)
+    with dv.DynaverseEngine(1 << 20, 8) as small:  # below one parameter set of n = 16
+        with pytest.raises(dv.DvgpuError) as e:
+            small.params_create(n, tx, ty)
+        assert e.value.status == -1 and "HBM budget" in e.value.message
+    with dv.DynaverseEngine(1 << 30, 8) as probe:
+        ph = probe.params_create(n, tx, ty)
+        params_bytes = probe.stats().resident_bytes
+        s, _ = probe.open_session(ph, pub, w)
+        session_bytes = probe.stats().resident_bytes - params_bytes
+        probe.close_session(s)
+    # room for the parameters and one session: the second session is refused
+    with dv.DynaverseEngine(params_bytes + session_bytes + session_bytes // 2, 8) as tight:
+        ph = tight.params_create(n, tx, ty)
+        s, _ = tight.open_session(ph, pub, w)
+        with pytest.raises(dv.DvgpuError) as err:
+            tight.open_session(ph, pub, w)
+        assert err.value.status == -1 and "HBM budget" in err.value.message
+        tight.close_session(s)
+        s, _ = tight.open_session(ph, pub, w)  # the footprint was returned
+    with dv.DynaverseEngine(1 << 30, 8) as e:
+        ph = e.params_create(n, tx, ty)
+        with pytest.raises(dv.DvgpuError) as err:
+            e.submit(987654321, [4 * n + 1], [1])
+        assert err.value.status == -1 and "unknown session" in err.value.message
+        s, proof = e.open_session(ph, pub, w)
+        ref = D.Session(D.Params(n, tx, ty, "scalar"), pub, w)
+        assert proof == ref.proof.to_bytes()
+        with pytest.raises(dv.DvgpuError) as err:
+            e.params_destroy(ph)
+        assert "open sessions" in err.value.message
+        # a parameter build holds the engine's worker while an update queues;
+        # the close that follows it finds the update pending
+        tx2, ty2 = D.sample_trapdoors(15304, 64)
+        extra = {}
+        busy = threading.Thread(target=lambda: extra.setdefault("p", e.params_create(64, tx2, ty2)))
+        busy.start()
+        import time
+        time.sleep(0.01)
+        idx, vals = _mul_edit(n, w, 3, 12345)
+        t = e.submit(s, idx, vals)
+        with pytest.raises(dv.DvgpuError) as err:
+            e.close_session(s)
+        assert "pending" in err.value.message
+        got, _ = e.wait(t)
+        busy.join()
+        assert got == ref.update(idx, vals).to_bytes()
+        e.close_session(s)
+        with pytest.raises(dv.DvgpuError):
+            e.close_session(s)
+        e.params_destroy(ph)
+        e.params_destroy(extra["p"])
+        assert e.stats().resident_bytes == 0
+
+
+@pytest.mark.parametrize("workload", ["hotspot", "spreading"])
+def test_reference_benchmark_workloads_n256(engine, workload):
+    """The reference's own CPU benchmark sequences (crates/bench/src/bin/
+    cpu_dynaverse.rs:240-256) at n = 256, 8 updates: Hotspot adds 1 to s5[0]
+    (s4[0] is zero in valid_instance, so the product stays valid); Spreading
+    adds 1 to the multiplier of gate 1 + (step - 1) mod (n - 1) and rewrites
+    its product.  Every proof against the oracle's."""
+    n = 256
+    ph, P = _setup(engine, n, 2814 if workload == "hotspot" else 2815)
+    pub, w = D.valid_instance(n)
+    s, proof = engine.open_session(ph, pub, w)
+    ref = D.Session(P, pub, w)
+    assert proof == ref.proof.to_bytes()
+    for step in range(1, 9):
+        cur = ref.current
+        if workload == "hotspot":
+            idx, vals = [4 * n], [(cur[4 * n] + 1) % R]
+        else:
+            gate = 1 + (step - 1) % (n - 1)
+            mult = (cur[4 * n + gate] + 1) % R
+            idx, vals = [4 * n + gate, 5 * n + gate], [mult, cur[3 * n + gate] * mult % R]
+        expect = ref.update(idx, vals)
+        assert engine.update(s, idx, vals) == expect.to_bytes(), (workload, step)
+    engine.close_session(s)

@@ -164,7 +164,8 @@ class DynaverseStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("requests", "batches", "sessions", "resident_bytes", "budget_bytes",
                                               "max_batch", "largest_batch", "busy_ns", "pending", "sparse_proofs",
                                               "rebuilds", "launches", "msm_fme", "host_ns", "device_wait_ns",
-                                              "dense_accum_ns", "dense_accum_adds", "allocations")]
+                                              "dense_accum_ns", "dense_accum_adds", "allocations",
+                                              "allocation_ns", "enqueue_ns")]
 
 
 # (name, restype, argtypes)

@@ -753,15 +753,33 @@ __global__ void k_dv_numer(FieldCtx c) {
 
 // Coset values of the numerators divided by those of A (5 H meets no root
 // of A: its roots are n-th roots of unity).
+// One thread per DQ consecutive coset points: their A values inverted
+// together by Montgomery's trick (one inversion, 3 (DQ - 1) products).  A has
+// its roots in H, so no value on the coset 5 H is zero.
+constexpr uint32_t DQ = 16;
 __global__ void k_dv_divq(FieldCtx c) {
+    const uint32_t chunks = (c.n + DQ - 1) / DQ;
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (uint64_t)c.n * c.njobs) return;
-    const uint32_t jb = (uint32_t)(i / c.n), k = (uint32_t)(i % c.n);
+    if (i >= (uint64_t)chunks * c.njobs) return;
+    const uint32_t jb = (uint32_t)(i / chunks), k0 = (uint32_t)(i % chunks) * DQ;
     const FieldJob J = c.jobs[jb];
     if (!J.a) return;
     Fr* rows = c.arena + J.dense;
-    const Fr ainv = Fr::inv(mont(rows[3ull * c.n + k]));
-    for (int t = 0; t < 3; ++t) rows[(uint64_t)t * c.n + k] = Fr::mul(rows[(uint64_t)t * c.n + k], ainv);
+    const Fr* av = rows + 3ull * c.n + k0;
+    const uint32_t m = min(DQ, c.n - k0);
+    Fr pre[DQ];  // pre[j] = a_0 ... a_(j-1) (Montgomery)
+    Fr acc = Fr::one();
+    for (uint32_t j = 0; j < m; ++j) {
+        pre[j] = acc;
+        acc = Fr::mul(acc, mont(av[j]));
+    }
+    Fr inv = Fr::inv(acc);  // 1 / (a_0 ... a_(m-1))
+    for (int j = (int)m - 1; j >= 0; --j) {
+        const Fr a = mont(av[j]);
+        const Fr ainv = Fr::mul(inv, pre[j]);
+        inv = Fr::mul(inv, a);
+        for (int t = 0; t < 3; ++t) rows[(uint64_t)t * c.n + k0 + j] = Fr::mul(rows[(uint64_t)t * c.n + k0 + j], ainv);
+    }
 }
 
 // An exact quotient has degree < n - a.
@@ -896,17 +914,20 @@ __global__ void k_dv_fresh(const VerifyJob* __restrict__ jobs, uint32_t njobs, G
     }
 }
 
-// One warp per proof.  Every term has a fixed position, so the lanes write
-// their pieces independently: lane 0 the dynamo terms, lanes 1..6 the six
-// consistency slices, then the tail (the public-zero, multiplication and,
-// for a delta, the affected-set and opening equations) over lanes 7..13,
-// and the group identities and the new [public]_h on the last lane.  Each
-// affine normalisation takes a field inversion, so spreading them over the
-// lanes shortens the chain about tenfold.
+// One 32-thread block per (proof, piece), its first lane working: pieces in
+// different blocks do not serialise on divergent branches, and a block of
+// one warp leaves the register budget to the field arithmetic.  Every term has a
+// fixed position, so the pieces write independently: piece 0 the dynamo
+// terms, 1..6 the six consistency slices, then the tail (the public-zero,
+// multiplication and, for a delta, the affected-set and opening equations)
+// over pieces 7..13, and the group identities and the new [public]_h on
+// piece 14.  Each affine normalisation takes a field inversion, so spreading
+// them over the pieces shortens the chain to two inversions.
+constexpr uint32_t TERM_PIECES = 15;
 __global__ void k_dv_terms(const VerifyJob* __restrict__ jobs, uint32_t njobs, G1A g1, G1A mvg1,
                            G1A* __restrict__ p, uint32_t* __restrict__ qidx, uint32_t* __restrict__ status) {
-    if (blockIdx.x >= njobs) return;
-    const uint32_t lane = threadIdx.x;
+    if (blockIdx.x >= njobs || threadIdx.x) return;
+    const uint32_t lane = blockIdx.y;  // the piece
     const VerifyJob J = jobs[blockIdx.x];
     const uint8_t* A = J.anchor;
     uint8_t* r = J.rec;
@@ -1245,6 +1266,8 @@ public:
             for (const Request& r : queue_)
                 if (r.session == id) throw InvalidArgument("session has pending requests");
             resident_ -= it->second->footprint;
+            give(it->second->d_coef);  // kept for the next session or re-anchor
+            give(it->second->d_anchor);
             sessions_.erase(it);
         });
     }
@@ -1325,6 +1348,8 @@ public:
         s.dense_accum_ns = stat_dense_ns_.load();
         s.dense_accum_adds = stat_dense_adds_.load();
         s.allocations = stat_allocs_;
+        s.allocation_ns = stat_alloc_ns_;
+        s.enqueue_ns = stat_enqueue_ns_.load();
         s.host_ns = s.busy_ns > s.device_wait_ns ? s.busy_ns - s.device_wait_ns : 0;
         return s;
     }
@@ -1378,6 +1403,7 @@ private:
             const uint64_t t0 = now_ns();
             const uint64_t l0 = launch_counter();
             const uint64_t a0 = __atomic_load_n(&alloc_counter(), __ATOMIC_RELAXED);
+            const uint64_t an0 = __atomic_load_n(&alloc_ns_counter(), __ATOMIC_RELAXED);
             std::vector<Outcome> outs(batch.size());
             process(batch, sess, outs);
             const uint64_t t1 = now_ns();
@@ -1398,6 +1424,7 @@ private:
             stat_busy_ns_ += t1 - t0;
             stat_launches_ += launch_counter() - l0;
             stat_allocs_ += __atomic_load_n(&alloc_counter(), __ATOMIC_RELAXED) - a0;
+            stat_alloc_ns_ += __atomic_load_n(&alloc_ns_counter(), __ATOMIC_RELAXED) - an0;
             done_cv_.notify_all();
         }
         ws1_.timeline.enabled = false;
@@ -1462,11 +1489,15 @@ private:
              stat_rebuilds_ = 0, stat_launches_ = 0;
     std::atomic<uint64_t> stat_fme_{0};  // written by the worker, read by stats()
     std::atomic<uint64_t> stat_wait_ns_{0}, stat_dense_ns_{0}, stat_dense_adds_{0};
-    uint64_t stat_allocs_ = 0;  // under mu_
-    // Device buffers that re-anchors swap out of sessions (coefficients,
-    // anchor bytes), kept for the next re-anchor: a re-anchor allocates
-    // nothing once the pool holds a batch's worth, and frees nothing.
+    uint64_t stat_allocs_ = 0, stat_alloc_ns_ = 0;  // under mu_
+    std::atomic<uint64_t> stat_enqueue_ns_{0};
+    // Device buffers that re-anchors swap out of sessions and that closed
+    // sessions leave (coefficients, anchor bytes), kept for the next
+    // re-anchor or session: once the pool holds a batch's worth, neither
+    // allocates nor frees (device allocation can take milliseconds and
+    // freeing waits for the device).  At most SPARE_MAX buffers are kept.
     std::vector<std::pair<void*, size_t>> spare_;
+    static constexpr size_t SPARE_MAX = 1024;
     void take(DevBuf& b, size_t bytes) {
         if (b.ptr && b.cap >= bytes) return;
         for (size_t i = 0; i < spare_.size(); ++i)
@@ -1482,7 +1513,7 @@ private:
     }
     void give(DevBuf& b) {
         if (!b.ptr) return;
-        if (spare_.size() < 4ull * max_batch_ + 8) {
+        if (spare_.size() < SPARE_MAX) {
             spare_.push_back({b.ptr, b.cap});
             b.ptr = nullptr;
             b.cap = 0;
@@ -1766,7 +1797,8 @@ void Engine::run_verify(Params& P, uint32_t njobs, uint64_t nfresh, uint64_t ter
     DV_CUDA(cudaMemcpyAsync(q, P.vk2.view<G2A>(), V_COUNT * sizeof(G2A), cudaMemcpyDeviceToDevice, st_));
     k_dv_fresh<<<(njobs + 31) / 32, 32, 0, st_>>>(d_jobs, njobs, q);
     DV_LAUNCH();
-    k_dv_terms<<<njobs, 32, 0, st_>>>(d_jobs, njobs, host_g1(P.g1), host_g1(P.mvg1), p, qi, d_status);
+    k_dv_terms<<<dim3(njobs, TERM_PIECES), 32, 0, st_>>>(d_jobs, njobs, host_g1(P.g1), host_g1(P.mvg1), p, qi,
+                                                         d_status);
     DV_LAUNCH();
     prepare_lines(P, q, nfresh, st_);
     pairing_check_prepared(*b_, p, terms, lines_.view<uint8_t>(), qinf_.view<uint32_t>(), qi, d_off, eqs, d_verdicts,
@@ -2260,6 +2292,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         memcpy(h, ain.data(), 32 * ain.size());
         DV_CUDA(cudaMemcpyAsync(arena, h, 32 * ain.size(), cudaMemcpyHostToDevice, st));
     }
+    const uint64_t e0 = now_ns();
     DV_CUDA(cudaMemsetAsync(out, 0, (uint64_t)B * JOB_BYTES, st));
     DV_CUDA(cudaMemsetAsync(status, 0, 4ull * B, st));
     DV_CUDA(cudaMemsetAsync(err, 0xff, 12, st));
@@ -2330,7 +2363,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         k_dv_numer<<<(unsigned)((t4 + 255) / 256), 256, 0, st>>>(c);
         DV_LAUNCH();
         ntt_batch_enqueue(nb_fwd_, st);
-        k_dv_divq<<<(unsigned)(((uint64_t)n * B + 255) / 256), 256, 0, st>>>(c);
+        k_dv_divq<<<(unsigned)(((uint64_t)((n + DQ - 1) / DQ) * B + 127) / 128), 128, 0, st>>>(c);
         DV_LAUNCH();
         ntt_batch_enqueue(nb_inv_, st);
         k_dv_degcheck<<<(unsigned)((3ull * n * B + 255) / 256), 256, 0, st>>>(c);
@@ -2386,7 +2419,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     // verification: the G1 terms here, then the pairings once st2_ is done
     G1A* tp1 = terms_p_.as<G1A>(std::max<uint64_t>(1, terms));
     uint32_t* tq1 = terms_q_.as<uint32_t>(std::max<uint64_t>(1, terms));
-    k_dv_terms<<<B, 32, 0, st>>>(reinterpret_cast<const VerifyJob*>(d + at_vj), B, host_g1(P.g1), host_g1(P.mvg1),
+    k_dv_terms<<<dim3(B, TERM_PIECES), 32, 0, st>>>(reinterpret_cast<const VerifyJob*>(d + at_vj), B, host_g1(P.g1), host_g1(P.mvg1),
                                  tp1, tq1, status);
     DV_LAUNCH();
     DV_CUDA(cudaStreamWaitEvent(st, ev_g2_, 0));
@@ -2404,6 +2437,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B, err, 12, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B + 16, verd, eqs, cudaMemcpyDeviceToHost, st));
     const uint64_t w0 = now_ns();
+    stat_enqueue_ns_ += w0 - e0;
     DV_CUDA(cudaStreamSynchronize(st));
     stat_wait_ns_ += now_ns() - w0;
     if (md.terms) {

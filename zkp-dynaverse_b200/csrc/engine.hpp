@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -23,9 +24,20 @@ inline void cuda_check(cudaError_t s, const char* what) {
 }
 // Number of this library's kernel launches since load (all owners).
 uint64_t& launch_counter();
-// Number of this library's device and pinned-host allocations since load.
+// Number of this library's device and pinned-host allocations since load,
+// and the nanoseconds spent in them (freeing the old buffer included: both
+// calls can wait for the device).
 uint64_t& alloc_counter();
-inline void allocated() { __atomic_add_fetch(&alloc_counter(), 1, __ATOMIC_RELAXED); }
+uint64_t& alloc_ns_counter();
+inline uint64_t steady_ns() {
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+inline void allocated(uint64_t t0) {
+    __atomic_add_fetch(&alloc_counter(), 1, __ATOMIC_RELAXED);
+    __atomic_add_fetch(&alloc_ns_counter(), steady_ns() - t0, __ATOMIC_RELAXED);
+}
 inline void launched() {
     cuda_check(cudaGetLastError(), "kernel launch");
     __atomic_add_fetch(&launch_counter(), 1, __ATOMIC_RELAXED);
@@ -41,12 +53,13 @@ struct DevBuf {
     size_t cap = 0;
     void* get(size_t bytes) {
         if (bytes <= cap && ptr) return ptr;
+        const uint64_t t0 = steady_ns();
         const size_t regrow = cap ? cap + cap / 2 : 0;
         release();
         size_t want = bytes < 256 ? 256 : bytes;
         if (regrow > want) want = regrow;
         DV_CUDA(cudaMalloc(&ptr, want));
-        allocated();
+        allocated(t0);
         cap = want;
         return ptr;
     }
@@ -77,12 +90,13 @@ struct PinnedBuf {
     size_t cap = 0;
     void* get(size_t bytes) {
         if (bytes <= cap && ptr) return ptr;
+        const uint64_t t0 = steady_ns();
         const size_t regrow = cap ? cap + cap / 2 : 0;
         release();
         size_t want = bytes < 256 ? 256 : bytes;
         if (regrow > want) want = regrow;
         DV_CUDA(cudaMallocHost(&ptr, want));
-        allocated();
+        allocated(t0);
         cap = want;
         return ptr;
     }

@@ -860,8 +860,12 @@ DV_INL XYZZ<Fq> load_cg(const XYZZ<Fq>* p) {
     return r;
 }
 
-DV_INL void block_sum(XYZZ<Fq>* sm) {
-    for (int stride = SD_BLOCK / 2; stride > 0; stride >>= 1) {
+// Tree sum of sm[0 .. live) into sm[0] (entries up to the next power of two
+// hold infinity): only the levels the live entries need.
+DV_INL void block_sum(XYZZ<Fq>* sm, uint32_t live) {
+    uint32_t span = 1;
+    while (span < live) span <<= 1;
+    for (uint32_t stride = span >> 1; stride > 0; stride >>= 1) {
         if (threadIdx.x < (unsigned)stride)
             sm[threadIdx.x] = XYZZ<Fq>::add_paired(sm[threadIdx.x], sm[threadIdx.x + stride]);
         __syncthreads();
@@ -873,16 +877,17 @@ DV_INL void block_sum(XYZZ<Fq>* sm) {
 // signed c-bit digit d of the entry's window, T the table's multiple
 // 2^(c w) P) by double-and-add, the block sums its threads.  The last block
 // of a request to finish (a per-request counter, reset by that block for the
-// next call) sums the request's block partials, normalises to affine and
-// writes the canonical result bytes: no second launch and no host
-// arithmetic.
+// next call) sums the request's block partials and writes the XYZZ sum.
+// The host normalises all requests with one batch inversion, as the
+// reference does (icicle_msm.cu:417-421): one thread's inversion on the
+// device takes longer than that copy and a host batch inversion.
 __global__ void __launch_bounds__(SD_BLOCK) k_sparse_direct(const G1A* __restrict__ table, uint64_t nbases, int c,
                                                             int W, const uint64_t* __restrict__ idx,
                                                             const uint32_t* __restrict__ vals,
                                                             const SdJob* __restrict__ jobs,
                                                             const uint32_t* __restrict__ req_blocks,
                                                             XYZZ<Fq>* __restrict__ partial, uint32_t* __restrict__ done,
-                                                            uint8_t* __restrict__ out, uint32_t* __restrict__ err) {
+                                                            XYZZ<Fq>* __restrict__ out, uint32_t* __restrict__ err) {
     __shared__ XYZZ<Fq> sm[SD_BLOCK];
     __shared__ bool last;
     const SdJob job = jobs[blockIdx.x];
@@ -921,7 +926,7 @@ __global__ void __launch_bounds__(SD_BLOCK) k_sparse_direct(const G1A* __restric
     }
     sm[threadIdx.x] = p;
     __syncthreads();
-    block_sum(sm);
+    block_sum(sm, job.items);
     const uint32_t r = job.request, b0 = req_blocks[r], b1 = req_blocks[r + 1];
     if (threadIdx.x == 0) {
         partial[blockIdx.x] = sm[0];
@@ -935,18 +940,10 @@ __global__ void __launch_bounds__(SD_BLOCK) k_sparse_direct(const G1A* __restric
     for (uint32_t b = b0 + threadIdx.x; b < b1; b += SD_BLOCK) p = XYZZ<Fq>::add_paired(p, load_cg(partial + b));
     sm[threadIdx.x] = p;
     __syncthreads();
-    block_sum(sm);
+    block_sum(sm, (b1 - b0) < (uint32_t)SD_BLOCK ? b1 - b0 : (uint32_t)SD_BLOCK);
     if (threadIdx.x == 0) {
         done[r] = 0;
-        uint8_t* o = out + 64ull * r;
-        if (sm[0].is_inf()) {
-            const uint4 z = make_uint4(0, 0, 0, 0);
-            for (int i = 0; i < 4; ++i) reinterpret_cast<uint4*>(o)[i] = z;
-        } else {
-            const G1A a = sm[0].to_affine();
-            store_canonical(o, a.x);
-            store_canonical(o + 32, a.y);
-        }
+        out[r] = sm[0];
     }
 }
 
@@ -976,25 +973,27 @@ void msm_sparse_direct(MsmWorkspace& ws, const MsmPrecomp<Fq>& pre, uint64_t nba
     uint8_t* d_desc = ws.sd_jobs.as<uint8_t>(jb + rb);
     XYZZ<Fq>* d_partial = ws.sd_partial.as<XYZZ<Fq>>(jobs.size());
     uint32_t* d_done = ws.sd_req.as<uint32_t>(count);
-    uint8_t* d_out = ws.sd_out.as<uint8_t>((size_t)count * 64 + 16);
-    uint32_t* d_err = reinterpret_cast<uint32_t*>(d_out + (size_t)count * 64);
+    constexpr size_t XB = sizeof(XYZZ<Fq>);
+    uint8_t* d_out = ws.sd_out.as<uint8_t>((size_t)count * XB + 16);
+    uint32_t* d_err = reinterpret_cast<uint32_t*>(d_out + (size_t)count * XB);
     DV_CUDA(cudaMemcpyAsync(d_desc, h_desc, jb + rb, cudaMemcpyHostToDevice, st));
     DV_CUDA(cudaMemsetAsync(d_done, 0, count * sizeof(uint32_t), st));
-    if (empty) DV_CUDA(cudaMemsetAsync(d_out, 0, (size_t)count * 64, st));
+    if (empty) DV_CUDA(cudaMemsetAsync(d_out, 0, (size_t)count * XB, st));  // all-zero XYZZ: infinity
     DV_CUDA(cudaMemsetAsync(d_err, 0xff, 2 * sizeof(uint32_t), st));
     k_sparse_direct<<<(unsigned)jobs.size(), SD_BLOCK, 0, st>>>(
         pre.table, nbases, pre.c, (int)W, d_idx, d_vals, reinterpret_cast<const SdJob*>(d_desc),
-        reinterpret_cast<const uint32_t*>(d_desc + jb), d_partial, d_done, d_out, d_err);
+        reinterpret_cast<const uint32_t*>(d_desc + jb), d_partial, d_done, reinterpret_cast<XYZZ<Fq>*>(d_out), d_err);
     DV_LAUNCH();
     // one copy back: the results, then the two error words
-    uint8_t* h_out = ws.host_windows.as<uint8_t>((size_t)count * 64 + 16);
-    DV_CUDA(cudaMemcpyAsync(h_out, d_out, (size_t)count * 64 + 8, cudaMemcpyDeviceToHost, st));
+    uint8_t* h_out = ws.host_windows.as<uint8_t>((size_t)count * XB + 16);
+    DV_CUDA(cudaMemcpyAsync(h_out, d_out, (size_t)count * XB + 8, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaStreamSynchronize(st));
     uint32_t h_err[2];
-    memcpy(h_err, h_out + (size_t)count * 64, 8);
+    memcpy(h_err, h_out + (size_t)count * XB, 8);
     if (h_err[0] != NO_INDEX) throw InvalidArgument("non-canonical scalar at index " + std::to_string(h_err[0]));
     if (h_err[1] != NO_INDEX) throw InvalidArgument("sparse MSM index out of range");
-    memcpy(host_out, h_out, (size_t)count * 64);
+    static_assert(sizeof(XYZZ<Fq>) == sizeof(dvh::XYZZ<dvh::Fq>), "host/device XYZZ layout");
+    dvh::xyzz_batch_to_affine_bytes(reinterpret_cast<const dvh::XYZZ<dvh::Fq>*>(h_out), count, host_out);
 }
 
 template void msm_run<Fq>(MsmWorkspace&, const Affine<Fq>*, const uint32_t*, const uint32_t*, uint32_t, int,

@@ -18,6 +18,11 @@ uint64_t& alloc_counter() {
     return counter;
 }
 
+uint64_t& alloc_ns_counter() {
+    static uint64_t counter = 0;
+    return counter;
+}
+
 namespace {
 
 DV_INL uint64_t mix64(uint64_t z) {
