@@ -1123,7 +1123,9 @@ class ProofServeOp:
                 "dense_accum_adds": st.dense_accum_adds - before.dense_accum_adds,
                 "allocations": st.allocations - before.allocations,
                 "allocation_ms": (st.allocation_ns - before.allocation_ns) / 1e6,
-                "enqueue_ms": (st.enqueue_ns - before.enqueue_ns) / 1e6, "tail": tail}
+                "enqueue_ms": (st.enqueue_ns - before.enqueue_ns) / 1e6,
+                "slowest_alloc": {"ms": st.slowest_alloc_ns / 1e6, "bytes": st.slowest_alloc_bytes,
+                                  "pinned": bool(st.slowest_alloc_pinned)}, "tail": tail}
 
     def run_standalone(self, args, torch, dv, b, s, sampler, imad_peak_fn, world=1):
         import numpy as np

@@ -661,6 +661,9 @@ typedef struct DvgpuDynaverseStats {
     /* host time from a batch's first launch to its synchronisation (the
      * enqueue phase, which allocation inside it lengthens) */
     uint64_t enqueue_ns;
+    /* the slowest single allocation of the library so far: nanoseconds,
+     * bytes, 1 if pinned host memory */
+    uint64_t slowest_alloc_ns, slowest_alloc_bytes, slowest_alloc_pinned;
 } DvgpuDynaverseStats;
 int dvgpu_dynaverse_create(uint64_t hbm_budget_bytes, uint32_t max_batch, void** engine, char* error,
                            size_t error_capacity);

@@ -68,7 +68,7 @@ def test_dynaverse_struct_layouts(dv, tmp_path):
                    f"_Static_assert(sizeof(DvgpuDynaverseResult) == {res}, \"result\");\n"
                    "_Static_assert(DVGPU_DYNAVERSE_PROOF_BYTES == 3968 + 5312 + 24, \"proof\");\n")
     subprocess.run(["gcc", "-fsyntax-only", "-I", os.path.dirname(HEADER), str(src)], check=True)
-    assert stats == 8 * 20 and dv.DYNAVERSE_PROOF_BYTES == 9304
+    assert stats == 8 * 23 and dv.DYNAVERSE_PROOF_BYTES == 9304
 
 
 def test_every_symbol_the_reference_crate_binds_is_declared():

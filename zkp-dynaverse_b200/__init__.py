@@ -165,7 +165,8 @@ class DynaverseStats(ctypes.Structure):
                                               "max_batch", "largest_batch", "busy_ns", "pending", "sparse_proofs",
                                               "rebuilds", "launches", "msm_fme", "host_ns", "device_wait_ns",
                                               "dense_accum_ns", "dense_accum_adds", "allocations",
-                                              "allocation_ns", "enqueue_ns")]
+                                              "allocation_ns", "enqueue_ns", "slowest_alloc_ns",
+                                              "slowest_alloc_bytes", "slowest_alloc_pinned")]
 
 
 # (name, restype, argtypes)

@@ -543,22 +543,52 @@ DV_INL uint32_t job_of(const uint32_t* pre, uint32_t njobs, uint32_t i) {
 // 1/A'(x_k) = x_k^-(a-1) prod_{j != k} 1/(1 - w^(e_j - e_k)); the B scalars
 // n w_k / x_k (Z'(x_k)/A'(x_k), sparse.rs:131-134) and the Montgomery rows
 // the interpolations and Cauchy sums read.
+// An element of Fr from lane (this lane xor m) of the warp.
+DV_INL Fr shfl_xor_fr(const Fr& a, int m) {
+    Fr r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r.v[i] = __shfl_xor_sync(0xffffffffu, a.v[i], m);
+    return r;
+}
+
+DV_INL Fr shfl_up_fr(const Fr& a, int d) {
+    Fr r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r.v[i] = __shfl_up_sync(0xffffffffu, a.v[i], d);
+    return r;
+}
+
+// One warp per affected point k: the products over j != k are split over
+// the lanes and combined by a butterfly, so the chain is a / 32 + 5 products
+// long instead of a.
 __global__ void k_dv_geom(FieldCtx c) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.kjob[c.njobs]) return;
-    const uint32_t jb = job_of(c.kjob, c.njobs, i);
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (gw >= c.kjob[c.njobs]) return;  // uniform across the warp
+    const uint32_t jb = job_of(c.kjob, c.njobs, gw);
     const FieldJob J = c.jobs[jb];
-    const uint32_t a = J.a, k = i - c.kjob[jb], mask = c.n - 1;
+    const uint32_t a = J.a, k = gw - c.kjob[jb], mask = c.n - 1;
     const uint32_t* e = c.list + J.aff;
     const uint32_t ek = e[k];
-    const Fr x = c.wpow[ek], xi = c.wpow[(c.n - ek) & mask];
-    Fr pinv = c.wpow[(uint32_t)(((uint64_t)((c.n - ek) & mask) * (a - 1)) & mask)];
-    Fr pd = c.wpow[(uint32_t)(((uint64_t)ek * (a - 1)) & mask)];
     const Fr one = Fr::one();
-    for (uint32_t j = 0; j < a; ++j) {
+    Fr pinv = one, pd = one;
+    for (uint32_t j = lane; j < a; j += 32) {
         if (j == k) continue;
         const uint32_t d = (e[j] - ek) & mask;
         const auto pr = Fr::mul2(pinv, c.inv1m[d], pd, Fr::sub(one, c.wpow[d]));
+        pinv = pr.r0;
+        pd = pr.r1;
+    }
+    for (int m = 16; m >= 1; m >>= 1) {
+        const Fr oi = shfl_xor_fr(pinv, m), od = shfl_xor_fr(pd, m);
+        const auto pr = Fr::mul2(pinv, oi, pd, od);
+        pinv = pr.r0;
+        pd = pr.r1;
+    }
+    if (lane) return;
+    const Fr x = c.wpow[ek], xi = c.wpow[(c.n - ek) & mask];
+    {
+        const auto pr = Fr::mul2(pinv, c.wpow[(uint32_t)(((uint64_t)((c.n - ek) & mask) * (a - 1)) & mask)], pd,
+                                 c.wpow[(uint32_t)(((uint64_t)ek * (a - 1)) & mask)]);
         pinv = pr.r0;
         pd = pr.r1;
     }
@@ -581,8 +611,12 @@ __global__ void k_dv_geom(FieldCtx c) {
     s[s_V(a, 9) + k] = pinv;  // Cauchy weights of the tree's own weights (sparse.rs:176)
 }
 
-// A = prod (X - x_k), one block per job, sequential products in shared
-// memory (a < 2^10).
+// A = prod (X - x_k), one block per job: A at the N-th roots of unity
+// (N = the power of two above a; a sparse job has a < sqrt(n), so N <= n and
+// the points come from the table of w^k), one warp per point with the
+// product split over its lanes, then an inverse transform of size N in
+// shared memory.  The chain is about a / 32 + log N + 5 products, against a
+// for the product taken one factor at a time.
 __global__ void k_dv_vanish(FieldCtx c) {
     extern __shared__ Fr sm[];
     const uint32_t jb = blockIdx.x;
@@ -590,45 +624,85 @@ __global__ void k_dv_vanish(FieldCtx c) {
     const FieldJob J = c.jobs[jb];
     const uint32_t a = J.a;
     Fr* s = c.scr + J.scr;
-    for (uint32_t j = threadIdx.x; j <= a; j += blockDim.x) sm[j] = j ? Fr::zero() : Fr::one();
+    uint32_t logN = 0;
+    while ((1u << logN) < a + 1) ++logN;
+    const uint32_t N = 1u << logN, step = c.n >> logN, mask = c.n - 1;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    for (uint32_t i = warp; i < N; i += nwarp) {
+        const Fr y = c.wpow[(i * step) & mask];
+        Fr p = Fr::one();
+        for (uint32_t k = lane; k < a; k += 32) p = Fr::mul(p, Fr::sub(y, s[s_X(a) + k]));
+        for (int m = 16; m >= 1; m >>= 1) p = Fr::mul(p, shfl_xor_fr(p, m));
+        if (lane == 0) sm[logN ? __brev(i) >> (32 - logN) : 0] = p;
+    }
     __syncthreads();
-    for (uint32_t k = 0; k < a; ++k) {
-        const Fr xk = s[s_X(a) + k];
-        // coefficients 0..k+1 of (X - x_k) * A_k, A_k of degree k
-        Fr nv[4];
-        int cnt = 0;
-        for (uint32_t j = threadIdx.x; j <= k + 1; j += blockDim.x, ++cnt) {
-            const Fr lo = j ? sm[j - 1] : Fr::zero();
-            const Fr hi = j <= k ? sm[j] : Fr::zero();
-            nv[cnt] = Fr::sub(lo, Fr::mul(xk, hi));
+    // inverse transform (decimation in time, bit-reversed input)
+    for (uint32_t half = 1; half < N; half <<= 1) {
+        const uint32_t stride = c.n / (2 * half);
+        for (uint32_t b = threadIdx.x; b < N / 2; b += blockDim.x) {
+            const uint32_t j = b % half, i0 = (b / half) * 2 * half + j, i1 = i0 + half;
+            const Fr tw = c.wpow[(c.n - j * stride) & mask];  // w_(2 half)^(-j)
+            const Fr u = sm[i0], t = Fr::mul(sm[i1], tw);
+            sm[i0] = Fr::add(u, t);
+            sm[i1] = Fr::sub(u, t);
         }
         __syncthreads();
-        cnt = 0;
-        for (uint32_t j = threadIdx.x; j <= k + 1; j += blockDim.x, ++cnt) sm[j] = nv[cnt];
-        __syncthreads();
     }
+    Fr sc;  // 1 / N = (n / N) / n
+    for (int i = 0; i < 8; ++i) sc.v[i] = i ? 0u : step;
+    const Fr ninv = Fr::mul(c.ninv_m, mont(sc));
     for (uint32_t j = threadIdx.x; j <= a; j += blockDim.x) {
-        s[s_AM(a) + j] = sm[j];
-        c.arena[J.out + o_A(a) + j] = canon(sm[j]);
+        const Fr v = Fr::mul(sm[j], ninv);
+        s[s_AM(a) + j] = v;
+        c.arena[J.out + o_A(a) + j] = canon(v);
     }
 }
 
 // Lagrange coefficient matrix of the affected set:
-// M[k][j] = w_k q_(k,j), q_k = A / (X - x_k) by synthetic division.
+// M[k][j] = w_k q_(k,j), q_k = A / (X - x_k) by synthetic division:
+// q_(a-1) = A_a, q_(t-1) = A_t + x q_t.  One warp per k: lane l runs the
+// steps of one chunk of t, whose effect is the affine map
+// q -> x^len q + C_l; a warp scan of those maps gives every lane the value
+// entering its chunk, so the chain is about a / 16 + 10 products long.
 __global__ void k_dv_lagmat(FieldCtx c) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.kjob[c.njobs]) return;
-    const uint32_t jb = job_of(c.kjob, c.njobs, i);
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (gw >= c.kjob[c.njobs]) return;  // uniform across the warp
+    const uint32_t jb = job_of(c.kjob, c.njobs, gw);
     const FieldJob J = c.jobs[jb];
-    const uint32_t a = J.a, k = i - c.kjob[jb];
+    const uint32_t a = J.a, k = gw - c.kjob[jb];
     const Fr* s = c.scr + J.scr;
+    const Fr* am = s + s_AM(a);
     Fr* m = c.scr + J.mat + (uint64_t)k * a;
     const Fr x = s[s_X(a) + k], w = s[s_W(a) + k];
-    Fr q = s[s_AM(a) + a];  // leading coefficient (one)
-    m[a - 1] = Fr::mul(w, q);
-    for (uint32_t j = a - 1; j >= 1; --j) {
-        q = Fr::add(s[s_AM(a) + j], Fr::mul(x, q));
-        m[j - 1] = Fr::mul(w, q);
+    // lane l: t from hi down to lo (lane 0 holds the top), steps t = hi .. lo
+    const int L = (int)((a + 31) / 32);
+    const int hi = (int)a - 1 - (int)lane * L, lo = hi - L + 1 < 0 ? 0 : hi - L + 1;
+    const bool live = hi >= 0;
+    Fr alpha = Fr::one(), cst = Fr::zero();
+    if (live)
+        for (int t = hi; t >= lo; --t) {
+            const auto pr = Fr::mul2(alpha, x, cst, x);
+            alpha = pr.r0;
+            cst = Fr::add(am[t], pr.r1);
+        }
+    // inclusive scan of the maps in lane order: (alpha, cst) after the earlier lanes' maps
+    for (int d = 1; d < 32; d <<= 1) {
+        const Fr pa = shfl_up_fr(alpha, d), pc = shfl_up_fr(cst, d);
+        if ((int)lane >= d) {
+            const auto pr = Fr::mul2(alpha, pa, alpha, pc);
+            alpha = pr.r0;
+            cst = Fr::add(pr.r1, cst);
+        }
+    }
+    // the value entering this lane's chunk: the earlier lanes' composition applied to A_a
+    const Fr ea = shfl_up_fr(alpha, 1), ec = shfl_up_fr(cst, 1);
+    const Fr top = am[a];
+    Fr q = lane == 0 ? top : Fr::add(Fr::mul(ea, top), ec);
+    if (!live) return;
+    m[hi] = Fr::mul(w, q);
+    for (int t = hi; t > lo; --t) {
+        q = Fr::add(am[t], Fr::mul(x, q));
+        m[t - 1] = Fr::mul(w, q);
     }
 }
 
@@ -638,10 +712,11 @@ __global__ void k_dv_lagmat(FieldCtx c) {
 // = (1/x_k) sum_(j != k) u_j / (1 - w^(e_j - e_k)) (SubproductTree::
 // cauchy_sums, domain/fast.rs:118-139) of the weights and of v x.
 __global__ void k_dv_rows(FieldCtx c) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= 13 * c.kjob[c.njobs]) return;
-    const uint32_t row_job = i / 13;  // flattened (job, idx) with 13 rows each
-    const uint32_t row = i % 13;
+    // one warp per (affected point, row); the lanes split the sum
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (gw >= 13 * c.kjob[c.njobs]) return;  // uniform across the warp
+    const uint32_t row_job = gw / 13;  // flattened (job, idx) with 13 rows each
+    const uint32_t row = gw % 13;
     const uint32_t jb = job_of(c.kjob, c.njobs, row_job);
     const FieldJob J = c.jobs[jb];
     const uint32_t a = J.a, idx = row_job - c.kjob[jb], mask = c.n - 1;
@@ -650,21 +725,21 @@ __global__ void k_dv_rows(FieldCtx c) {
     Fr acc = Fr::zero();
     if (row < 9) {
         const Fr* m = c.scr + J.mat + idx;
-        uint32_t k = 0;
-        for (; k + 1 < a; k += 2) {
-            const auto pr = Fr::mul2(m[(uint64_t)k * a], v[k], m[(uint64_t)(k + 1) * a], v[k + 1]);
-            acc = Fr::add(acc, Fr::add(pr.r0, pr.r1));
-        }
-        if (k < a) acc = Fr::add(acc, Fr::mul(m[(uint64_t)k * a], v[k]));
-        const uint32_t o = row < 3 ? o_R(a, row) : row < 6 ? o_RS(a, row - 3) : o_ZQ(a, row - 6);
-        c.arena[J.out + o + idx] = canon(acc);
+        for (uint32_t k = lane; k < a; k += 32) acc = Fr::add(acc, Fr::mul(m[(uint64_t)k * a], v[k]));
     } else {
         const uint32_t* e = c.list + J.aff;
         const uint32_t ek = e[idx];
-        for (uint32_t j = 0; j < a; ++j) {
+        for (uint32_t j = lane; j < a; j += 32) {
             if (j == idx) continue;
             acc = Fr::add(acc, Fr::mul(v[j], c.inv1m[(e[j] - ek) & mask]));
         }
+    }
+    for (int m = 16; m >= 1; m >>= 1) acc = Fr::add(acc, shfl_xor_fr(acc, m));
+    if (lane) return;
+    if (row < 9) {
+        const uint32_t o = row < 3 ? o_R(a, row) : row < 6 ? o_RS(a, row - 3) : o_ZQ(a, row - 6);
+        c.arena[J.out + o + idx] = canon(acc);
+    } else {
         acc = Fr::mul(acc, s[s_XI(a) + idx]);
         Fr* dst = c.scr + J.scr + (row == 9 ? s_CW(a) : s_CV(a, row - 10));
         dst[idx] = acc;
@@ -1202,8 +1277,11 @@ public:
             DV_CUDA(cudaStreamCreateWithFlags(&b_->stream, cudaStreamNonBlocking));
             st_ = b_->stream;
             DV_CUDA(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
+            DV_CUDA(cudaStreamCreateWithFlags(&st3_, cudaStreamNonBlocking));
             DV_CUDA(cudaEventCreateWithFlags(&ev_fields_, cudaEventDisableTiming));
             DV_CUDA(cudaEventCreateWithFlags(&ev_g2_, cudaEventDisableTiming));
+            DV_CUDA(cudaEventCreateWithFlags(&ev_start_, cudaEventDisableTiming));
+            DV_CUDA(cudaEventCreateWithFlags(&ev_m1_, cudaEventDisableTiming));
             // phase events of the G1 workspace: the dense MSM, its last user in
             // a batch, leaves its accumulation time there for the stats
             for (auto& e : ws1_.timeline.ev) DV_CUDA(cudaEventCreate(&e));
@@ -1350,6 +1428,7 @@ public:
         s.allocations = stat_allocs_;
         s.allocation_ns = stat_alloc_ns_;
         s.enqueue_ns = stat_enqueue_ns_.load();
+        for (int i = 0; i < 3; ++i) (&s.slowest_alloc_ns)[i] = __atomic_load_n(slowest_alloc() + i, __ATOMIC_RELAXED);
         s.host_ns = s.busy_ns > s.device_wait_ns ? s.busy_ns - s.device_wait_ns : 0;
         return s;
     }
@@ -1434,9 +1513,10 @@ private:
             if (e) cudaEventDestroy(e);
         for (auto& sp : spare_) cudaFree(sp.first);
         spare_.clear();
-        if (ev_fields_) cudaEventDestroy(ev_fields_);
-        if (ev_g2_) cudaEventDestroy(ev_g2_);
+        for (cudaEvent_t e : {ev_fields_, ev_g2_, ev_start_, ev_m1_})
+            if (e) cudaEventDestroy(e);
         if (st2_) cudaStreamDestroy(st2_);
+        if (st3_) cudaStreamDestroy(st3_);
         b_.reset();
     }
 
@@ -1470,9 +1550,13 @@ private:
     DevBuf stage_, arena_, scr_, out_, status_, verdicts_, tpoint_, tscalar_, tpoint2_, tscalar2_, lrow_, lsc_,
         terms_p_, terms_q_, g2q_, lines_, qinf_, tmp_, tmp2_, err_;
     // The G2 side of an update batch (its MSM, then preparing the fresh G2
-    // points for the pairings) runs on st2_ beside the dense G1 work on st_.
-    cudaStream_t st2_ = nullptr;
-    cudaEvent_t ev_fields_ = nullptr, ev_g2_ = nullptr;
+    // points for the pairings) runs on st2_ beside the dense G1 work on st_;
+    // the linear fields' MSM (m1), which only the record copies and the
+    // verification read, runs on st3_ from the start of the batch.
+    cudaStream_t st2_ = nullptr, st3_ = nullptr;
+    cudaEvent_t ev_fields_ = nullptr, ev_g2_ = nullptr, ev_start_ = nullptr, ev_m1_ = nullptr;
+    MsmWorkspace ws3_;
+    DevBuf tpoint3_, tscalar3_;
     bool quot_smem_ = false;
     PinnedBuf pstage_, pstage2_, parena_, pout_;
 
@@ -1500,15 +1584,18 @@ private:
     static constexpr size_t SPARE_MAX = 1024;
     void take(DevBuf& b, size_t bytes) {
         if (b.ptr && b.cap >= bytes) return;
+        size_t best = spare_.size();  // the smallest spare that fits, so small sessions leave large buffers
         for (size_t i = 0; i < spare_.size(); ++i)
-            if (spare_[i].second >= bytes) {
-                b.release();
-                b.ptr = spare_[i].first;
-                b.cap = spare_[i].second;
-                spare_[i] = spare_.back();
-                spare_.pop_back();
-                return;
-            }
+            if (spare_[i].second >= bytes && (best == spare_.size() || spare_[i].second < spare_[best].second))
+                best = i;
+        if (best < spare_.size()) {
+            b.release();
+            b.ptr = spare_[best].first;
+            b.cap = spare_[best].second;
+            spare_[best] = spare_.back();
+            spare_.pop_back();
+            return;
+        }
         b.get(bytes);
     }
     void give(DevBuf& b) {
@@ -2298,13 +2385,19 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     DV_CUDA(cudaMemsetAsync(err, 0xff, 12, st));
     k_dv_copy<<<dim3(1, B), 32, 0, st>>>(B, reinterpret_cast<const CopyDesc*>(d2 + at_cp0));
     DV_LAUNCH();
-    const uint32_t maxterms = std::max(std::max(m1.terms, m2.terms), md.terms) + 1;
+    const uint32_t maxterms = std::max(m2.terms, md.terms) + 1;
     tpoint_.as<uint32_t>(maxterms);
     tscalar_.as<uint32_t>(maxterms);
+    tpoint3_.as<uint32_t>(m1.terms + 1);
+    tscalar3_.as<uint32_t>(m1.terms + 1);
     const uint32_t* d_lrow = reinterpret_cast<const uint32_t*>(d + at_lrow);
     const uint32_t* d_lsc = reinterpret_cast<const uint32_t*>(d + at_lsc);
     stat_fme_ += (uint64_t)(m1.fme + m2.fme + md.fme + 3 * m3.fme);
-    run_msm<Fq>(ws1_, P.table.view<G1A>(), m1, d, d_lrow, d_lsc, arena, out, err, tpoint_, tscalar_, st);
+    // m1 on st3_ once the inputs and the zeroed records are in place
+    DV_CUDA(cudaEventRecord(ev_start_, st));
+    DV_CUDA(cudaStreamWaitEvent(st3_, ev_start_, 0));
+    run_msm<Fq>(ws3_, P.table.view<G1A>(), m1, d, d_lrow, d_lsc, arena, out, err, tpoint3_, tscalar3_, st3_);
+    DV_CUDA(cudaEventRecord(ev_m1_, st3_));
     // field work of the affected sets
     FieldCtx c{reinterpret_cast<const FieldJob*>(d + at_fj), reinterpret_cast<const uint32_t*>(d + at_kj), B, d_lrow,
                P.wpow.view<Fr>(), P.inv1m.view<Fr>(), n, Fr{}, Fr{}, arena, scratch, status};
@@ -2316,15 +2409,17 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         quot_smem_ = true;
     }
     if (K) {
-        k_dv_geom<<<(K + 127) / 128, 128, 0, st>>>(c);
+        k_dv_geom<<<(unsigned)((32ull * K + 127) / 128), 128, 0, st>>>(c);
         DV_LAUNCH();
     }
-    k_dv_vanish<<<B, 256, (amax + 1) * sizeof(Fr), st>>>(c);
+    uint64_t vanish_n = 1;  // the largest transform of k_dv_vanish
+    while (vanish_n < amax + 1) vanish_n <<= 1;
+    k_dv_vanish<<<B, 256, vanish_n * sizeof(Fr), st>>>(c);
     DV_LAUNCH();
     if (K) {
-        k_dv_lagmat<<<(K + 127) / 128, 128, 0, st>>>(c);
+        k_dv_lagmat<<<(unsigned)((32ull * K + 127) / 128), 128, 0, st>>>(c);
         DV_LAUNCH();
-        k_dv_rows<<<(13 * K + 127) / 128, 128, 0, st>>>(c);
+        k_dv_rows<<<(unsigned)((32ull * 13 * K + 127) / 128), 128, 0, st>>>(c);
         DV_LAUNCH();
         k_dv_combine<<<(K + 127) / 128, 128, 0, st>>>(c);
         DV_LAUNCH();
@@ -2406,6 +2501,9 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     run_msm<Fq>(ws1_, P.table.view<G1A>(), m2, d, d_lrow, d_lsc, arena, out, err + 1, tpoint_, tscalar_, st);
     run_msm<Fq>(ws1_, P.table_dense.view<G1A>(), md, d, d_lrow, d_lsc, arena, out, err + 1, tpoint_, tscalar_, st, TCD,
                 TWD);
+    // the record copies, the re-anchors' G1 fields and the verification
+    // terms read m1's outputs
+    DV_CUDA(cudaStreamWaitEvent(st, ev_m1_, 0));
     if (!cp.empty()) {
         k_dv_copy<<<dim3(1, (unsigned)cp.size()), 32, 0, st>>>((uint32_t)cp.size(), reinterpret_cast<const CopyDesc*>(d2 + at_cp));
         DV_LAUNCH();

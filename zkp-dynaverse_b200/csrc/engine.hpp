@@ -29,14 +29,24 @@ uint64_t& launch_counter();
 // calls can wait for the device).
 uint64_t& alloc_counter();
 uint64_t& alloc_ns_counter();
+// The slowest single allocation since load: its nanoseconds, its bytes and
+// whether it was pinned host memory (1) or device memory (0).
+uint64_t* slowest_alloc();
 inline uint64_t steady_ns() {
     return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
                std::chrono::steady_clock::now().time_since_epoch())
         .count();
 }
-inline void allocated(uint64_t t0) {
+inline void allocated(uint64_t t0, size_t bytes, bool pinned) {
+    const uint64_t dt = steady_ns() - t0;
     __atomic_add_fetch(&alloc_counter(), 1, __ATOMIC_RELAXED);
-    __atomic_add_fetch(&alloc_ns_counter(), steady_ns() - t0, __ATOMIC_RELAXED);
+    __atomic_add_fetch(&alloc_ns_counter(), dt, __ATOMIC_RELAXED);
+    uint64_t* s = slowest_alloc();
+    if (dt > __atomic_load_n(s, __ATOMIC_RELAXED)) {  // diagnostics: a race only mixes two records
+        __atomic_store_n(s, dt, __ATOMIC_RELAXED);
+        __atomic_store_n(s + 1, (uint64_t)bytes, __ATOMIC_RELAXED);
+        __atomic_store_n(s + 2, (uint64_t)pinned, __ATOMIC_RELAXED);
+    }
 }
 inline void launched() {
     cuda_check(cudaGetLastError(), "kernel launch");
@@ -59,7 +69,7 @@ struct DevBuf {
         size_t want = bytes < 256 ? 256 : bytes;
         if (regrow > want) want = regrow;
         DV_CUDA(cudaMalloc(&ptr, want));
-        allocated(t0);
+        allocated(t0, want, false);
         cap = want;
         return ptr;
     }
@@ -96,7 +106,7 @@ struct PinnedBuf {
         size_t want = bytes < 256 ? 256 : bytes;
         if (regrow > want) want = regrow;
         DV_CUDA(cudaMallocHost(&ptr, want));
-        allocated(t0);
+        allocated(t0, want, true);
         cap = want;
         return ptr;
     }
