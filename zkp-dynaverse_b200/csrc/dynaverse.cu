@@ -617,7 +617,7 @@ __global__ void k_dv_geom(FieldCtx c) {
 // product split over its lanes, then an inverse transform of size N in
 // shared memory.  The chain is about a / 32 + log N + 5 products, against a
 // for the product taken one factor at a time.
-__global__ void k_dv_vanish(FieldCtx c) {
+__global__ void __launch_bounds__(1024) k_dv_vanish(FieldCtx c) {
     extern __shared__ Fr sm[];
     const uint32_t jb = blockIdx.x;
     if (jb >= c.njobs) return;
@@ -828,10 +828,11 @@ __global__ void k_dv_numer(FieldCtx c) {
 
 // Coset values of the numerators divided by those of A (5 H meets no root
 // of A: its roots are n-th roots of unity).
-// One thread per DQ consecutive coset points: their A values inverted
+// One thread per DQ consecutive coset points (8: a longer chain costs more
+// latency in a lone update than it saves in a batch): their A values inverted
 // together by Montgomery's trick (one inversion, 3 (DQ - 1) products).  A has
 // its roots in H, so no value on the coset 5 H is zero.
-constexpr uint32_t DQ = 16;
+constexpr uint32_t DQ = 8;
 __global__ void k_dv_divq(FieldCtx c) {
     const uint32_t chunks = (c.n + DQ - 1) / DQ;
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2414,7 +2415,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     }
     uint64_t vanish_n = 1;  // the largest transform of k_dv_vanish
     while (vanish_n < amax + 1) vanish_n <<= 1;
-    k_dv_vanish<<<B, 256, vanish_n * sizeof(Fr), st>>>(c);
+    k_dv_vanish<<<B, 1024, vanish_n * sizeof(Fr), st>>>(c);
     DV_LAUNCH();
     if (K) {
         k_dv_lagmat<<<(unsigned)((32ull * K + 127) / 128), 128, 0, st>>>(c);

@@ -44,8 +44,12 @@ DV_INL G2X mul_int(const G2A& a, const uint32_t* k, int bits) {
     return r;
 }
 
-// Returns the reference mask (0 / 1 / 2 / 4).
-DV_INL uint32_t g2_wire_check(const uint8_t* b, uint32_t algorithm) {
+// Returns the reference mask (0 / 1 / 2 / 4).  One instantiation per
+// subgroup algorithm: each kernel then holds only its own algorithm's live
+// values (a single kernel with a runtime branch took the registers of the
+// largest and spilled).
+template <int ALG>
+DV_INL uint32_t g2_wire_check(const uint8_t* b) {
     uint32_t w[4][8];
     uint32_t any = 0;
     for (int j = 0; j < 4; ++j) {
@@ -66,35 +70,39 @@ DV_INL uint32_t g2_wire_check(const uint8_t* b, uint32_t algorithm) {
     // equation directly (0 = b' fails, as in the reference parser).
     if (!(Fq2::sqr(p.y) == Fq2::add(Fq2::mul(Fq2::sqr(p.x), p.x), g2_b()))) return 2;
     bool ok;
-    if (algorithm == 1) {
+    if constexpr (ALG == 1) {
         uint32_t r[8];
         for (int i = 0; i < 8; ++i) r[i] = R_INT[i];
         ok = mul_int<8>(p, r, 254).is_inf();
-    } else if (algorithm == 2) {
+    } else if constexpr (ALG == 2) {
         uint32_t l[4];
         for (int i = 0; i < 4; ++i) l[i] = LAMBDA[i];
         const G2X lhs = psi(G2X::from_affine(p), psi_cx(), psi_cy());
         ok = G2X::equal(lhs, mul_int<4>(p, l, 127));
     } else {
-        const Fq2 cx = psi_cx(), cy = psi_cy();
+        // [x]P + psi([x]P) + psi^2([x]P) + P == 2 psi^3([x]P), each point
+        // folded into the left side as soon as the next is formed, and the
+        // psi constants read from constant memory where used, so at most two
+        // projective points are live at once
         uint32_t s[2] = {SEED[0], SEED[1]};
-        const G2X a = mul_int<2>(p, s, 63);
-        const G2X b1 = psi(a, cx, cy);
-        const G2X c1 = psi(b1, cx, cy);
-        G2X lhs = G2X::add_affine(a, p);
-        lhs = G2X::add(lhs, b1);
-        lhs = G2X::add(lhs, c1);
-        const G2X rhs = G2X::dbl(psi(c1, cx, cy));
-        ok = G2X::equal(lhs, rhs);
+        G2X t = mul_int<2>(p, s, 63);
+        G2X lhs = G2X::add_affine(t, p);
+        t = psi(t, psi_cx(), psi_cy());
+        lhs = G2X::add(lhs, t);
+        t = psi(t, psi_cx(), psi_cy());
+        lhs = G2X::add(lhs, t);
+        t = G2X::dbl(psi(t, psi_cx(), psi_cy()));
+        ok = G2X::equal(lhs, t);
     }
     return ok ? 0 : 4;
 }
 
-__global__ void __launch_bounds__(256) k_g2_check(const uint8_t* __restrict__ wire, uint64_t n, uint32_t algorithm,
+template <int ALG>
+__global__ void __launch_bounds__(256) k_g2_check(const uint8_t* __restrict__ wire, uint64_t n,
                                                   uint32_t* __restrict__ masks, G2CheckAccum* __restrict__ acc) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t m = g2_wire_check(wire + 128 * i, algorithm);
+    const uint32_t m = g2_wire_check<ALG>(wire + 128 * i);
     masks[i] = m;
     if (m) {
         atomicAdd(&acc->invalid, 1ull);
@@ -221,7 +229,10 @@ inline unsigned blocks_for(uint64_t n, unsigned threads) { return (unsigned)((n 
 void g2_check_launch(const uint8_t* d_wire, uint64_t n, uint32_t algorithm, uint32_t* d_masks, G2CheckAccum* d_acc,
                      cudaStream_t st, unsigned threads) {
     if (!n) return;
-    k_g2_check<<<blocks_for(n, threads), threads, 0, st>>>(d_wire, n, algorithm, d_masks, d_acc);
+    // algorithm 3 unless 1 or 2 (the reference's selection)
+    if (algorithm == 1) k_g2_check<1><<<blocks_for(n, threads), threads, 0, st>>>(d_wire, n, d_masks, d_acc);
+    else if (algorithm == 2) k_g2_check<2><<<blocks_for(n, threads), threads, 0, st>>>(d_wire, n, d_masks, d_acc);
+    else k_g2_check<3><<<blocks_for(n, threads), threads, 0, st>>>(d_wire, n, d_masks, d_acc);
     DV_LAUNCH();
 }
 
@@ -230,8 +241,8 @@ void g2_kernel_resources(unsigned threads, DvgpuG2KernelResources& out) {
     DV_CUDA(cudaGetDevice(&dev));
     DV_CUDA(cudaDeviceGetAttribute(&max_threads, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
     cudaFuncAttributes a{}, na{};
-    DV_CUDA(cudaFuncGetAttributes(&a, k_g2_check));
-    DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_g2_check, (int)threads, 0));
+    DV_CUDA(cudaFuncGetAttributes(&a, k_g2_check<3>));  // the default algorithm's kernel
+    DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_g2_check<3>, (int)threads, 0));
     // the checked fixed-base normalisation is fused into its generation kernel
     DV_CUDA(cudaFuncGetAttributes(&na, k_fb_generate<Fq2>));
     DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nblocks, k_fb_generate<Fq2>, 128, 0));
