@@ -1553,7 +1553,8 @@ private:
     // The G2 side of an update batch (its MSM, then preparing the fresh G2
     // points for the pairings) runs on st2_ beside the dense G1 work on st_;
     // the linear fields' MSM (m1), which only the record copies and the
-    // verification read, runs on st3_ from the start of the batch.
+    // verification read, runs on st3_ from the start of the batch, then the
+    // affected-set MSM (m2) once the field rows exist, beside the dense MSM.
     cudaStream_t st2_ = nullptr, st3_ = nullptr;
     cudaEvent_t ev_fields_ = nullptr, ev_g2_ = nullptr, ev_start_ = nullptr, ev_m1_ = nullptr;
     MsmWorkspace ws3_;
@@ -2374,7 +2375,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         }
     }
     uint8_t* verd = verdicts_.as<uint8_t>(std::max<uint64_t>(1, eqs));
-    uint32_t* err = err_.as<uint32_t>(3);
+    uint32_t* err = err_.as<uint32_t>(4);  // one word per MSM: m1, md, m3, m2
     if (!ain.empty()) {
         Canon* h = parena_.as<Canon>(ain.size());
         memcpy(h, ain.data(), 32 * ain.size());
@@ -2383,14 +2384,14 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     const uint64_t e0 = now_ns();
     DV_CUDA(cudaMemsetAsync(out, 0, (uint64_t)B * JOB_BYTES, st));
     DV_CUDA(cudaMemsetAsync(status, 0, 4ull * B, st));
-    DV_CUDA(cudaMemsetAsync(err, 0xff, 12, st));
+    DV_CUDA(cudaMemsetAsync(err, 0xff, 16, st));
     k_dv_copy<<<dim3(1, B), 32, 0, st>>>(B, reinterpret_cast<const CopyDesc*>(d2 + at_cp0));
     DV_LAUNCH();
-    const uint32_t maxterms = std::max(m2.terms, md.terms) + 1;
+    const uint32_t maxterms = md.terms + 1;
     tpoint_.as<uint32_t>(maxterms);
     tscalar_.as<uint32_t>(maxterms);
-    tpoint3_.as<uint32_t>(m1.terms + 1);
-    tscalar3_.as<uint32_t>(m1.terms + 1);
+    tpoint3_.as<uint32_t>(std::max(m1.terms, m2.terms) + 1);  // m1 then m2 on st3_: sized once, before either
+    tscalar3_.as<uint32_t>(std::max(m1.terms, m2.terms) + 1);
     const uint32_t* d_lrow = reinterpret_cast<const uint32_t*>(d + at_lrow);
     const uint32_t* d_lsc = reinterpret_cast<const uint32_t*>(d + at_lsc);
     stat_fme_ += (uint64_t)(m1.fme + m2.fme + md.fme + 3 * m3.fme);
@@ -2398,7 +2399,6 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     DV_CUDA(cudaEventRecord(ev_start_, st));
     DV_CUDA(cudaStreamWaitEvent(st3_, ev_start_, 0));
     run_msm<Fq>(ws3_, P.table.view<G1A>(), m1, d, d_lrow, d_lsc, arena, out, err, tpoint3_, tscalar3_, st3_);
-    DV_CUDA(cudaEventRecord(ev_m1_, st3_));
     // field work of the affected sets
     FieldCtx c{reinterpret_cast<const FieldJob*>(d + at_fj), reinterpret_cast<const uint32_t*>(d + at_kj), B, d_lrow,
                P.wpow.view<Fr>(), P.inv1m.view<Fr>(), n, Fr{}, Fr{}, arena, scratch, status};
@@ -2437,6 +2437,10 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     tscalar2_.as<uint32_t>(m3.terms + 1);
     DV_CUDA(cudaEventRecord(ev_fields_, st));
     DV_CUDA(cudaStreamWaitEvent(st2_, ev_fields_, 0));
+    // m2 on st3_ after m1, once the field rows it reads exist
+    DV_CUDA(cudaStreamWaitEvent(st3_, ev_fields_, 0));
+    run_msm<Fq>(ws3_, P.table.view<G1A>(), m2, d, d_lrow, d_lsc, arena, out, err + 3, tpoint3_, tscalar3_, st3_);
+    DV_CUDA(cudaEventRecord(ev_m1_, st3_));
     run_msm<Fq2>(ws2_, P.table2.view<G2A>(), m3, d, d_lrow, d_lsc, arena, out, err + 2, tpoint2_, tscalar2_, st2_);
     if (!cp2.empty()) {
         k_dv_copy<<<dim3(1, (unsigned)cp2.size()), 32, 0, st2_>>>((uint32_t)cp2.size(),
@@ -2499,11 +2503,10 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
             DV_LAUNCH();
         }
     }
-    run_msm<Fq>(ws1_, P.table.view<G1A>(), m2, d, d_lrow, d_lsc, arena, out, err + 1, tpoint_, tscalar_, st);
     run_msm<Fq>(ws1_, P.table_dense.view<G1A>(), md, d, d_lrow, d_lsc, arena, out, err + 1, tpoint_, tscalar_, st, TCD,
                 TWD);
     // the record copies, the re-anchors' G1 fields and the verification
-    // terms read m1's outputs
+    // terms read m1's and m2's outputs
     DV_CUDA(cudaStreamWaitEvent(st, ev_m1_, 0));
     if (!cp.empty()) {
         k_dv_copy<<<dim3(1, (unsigned)cp.size()), 32, 0, st>>>((uint32_t)cp.size(), reinterpret_cast<const CopyDesc*>(d2 + at_cp));
@@ -2533,7 +2536,7 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
     uint8_t* hout = pout_.as<uint8_t>(ob + 4ull * B + 16 + eqs);
     DV_CUDA(cudaMemcpyAsync(hout, out, ob, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaMemcpyAsync(hout + ob, status, 4ull * B, cudaMemcpyDeviceToHost, st));
-    DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B, err, 12, cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B, err, 16, cudaMemcpyDeviceToHost, st));
     DV_CUDA(cudaMemcpyAsync(hout + ob + 4ull * B + 16, verd, eqs, cudaMemcpyDeviceToHost, st));
     const uint64_t w0 = now_ns();
     stat_enqueue_ns_ += w0 - e0;
@@ -2554,9 +2557,9 @@ void Engine::run_sparse(Params& P, std::vector<Job*>& jobs) {
         ntt_batch_check(nb_r2_, st);
         ntt_batch_check(nb_r3_, st);
     }
-    uint32_t herr[3];
-    memcpy(herr, hout + ob + 4ull * B, 12);
-    for (int i = 0; i < 3; ++i)
+    uint32_t herr[4];
+    memcpy(herr, hout + ob + 4ull * B, 16);
+    for (int i = 0; i < 4; ++i)
         if (herr[i] != 0xffffffffu) throw CudaFailure("update MSM read a non-canonical scalar");
     for (uint32_t j = 0; j < B; ++j) {
         Job& J = *jobs[j];
