@@ -2861,6 +2861,14 @@ void Engine::process(std::vector<Request>& batch, std::vector<Session*>& sess, s
                 active[r] = false;
             }
     }
+    if (std::any_of(outs.begin(), outs.end(), [](const Outcome& o) { return o.status != 0; })) {
+        // a batch that stopped part way may have left work queued on the three
+        // streams: let it finish before the next batch reuses the buffers (the
+        // statuses are ignored; a lost context shows in the next batch's calls)
+        for (cudaStream_t q : {st_, st2_, st3_})
+            if (q) cudaStreamSynchronize(q);
+        cudaGetLastError();
+    }
     // publish (session.rs:132-141): only proofs that verified change state
     std::lock_guard<std::mutex> lk(mu_);
     for (size_t r = 0; r < batch.size(); ++r) {
