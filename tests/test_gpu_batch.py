@@ -122,6 +122,10 @@ def test_batch_plan_matches_oracle_and_replays(backend, oracle, dv):
         assert sum(c["sets"] for c in log["classes"]) == len(sizes)
         for c in log["classes"]:
             assert c["best_c"] in [x["c"] for x in c["candidates"]]
+        # the NTT's register round is picked from radix 2, 4 and 8, each
+        # checked against the first on the device while the plan is built
+        radices = [x["radix"] for x in log["ntt"]["candidates"]]
+        assert radices == [2, 4, 8] and log["ntt"]["best_radix"] in radices
         for rep in range(2):  # the second run replays the graph on new inputs
             scs = [oracle.uniform_fr(5200 + 100 * rep + i, n) for i, n in enumerate(sizes)]
             scs[3] = bytes(32 * sizes[3])  # all-zero scalars: infinity

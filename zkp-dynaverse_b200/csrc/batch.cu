@@ -86,6 +86,77 @@ double time_class(BatchPlan& p, BatchClass& k, int reps) {
     return best;
 }
 
+// Best of `reps` timed runs of the plan's NTT batch alone on p.stream.
+double time_ntt(BatchPlan& p, int reps) {
+    cudaEvent_t e0, e1;
+    DV_CUDA(cudaEventCreate(&e0));
+    DV_CUDA(cudaEventCreate(&e1));
+    ntt_batch_enqueue(p.ntt, p.stream);  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < reps; ++r) {
+        DV_CUDA(cudaEventRecord(e0, p.stream));
+        ntt_batch_enqueue(p.ntt, p.stream);
+        DV_CUDA(cudaEventRecord(e1, p.stream));
+        DV_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        DV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+// differ[0] != 0 when the two arrays of n 16-byte words differ anywhere.
+__global__ void k_words_differ(const uint4* __restrict__ a, const uint4* __restrict__ b, uint64_t n,
+                               uint32_t* differ) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint4 x = a[i], y = b[i];
+        if ((x.x ^ y.x) | (x.y ^ y.y) | (x.z ^ y.z) | (x.w ^ y.w)) *differ = 1;
+    }
+}
+
+// Picks the batch NTT's register round (radix 2, 4 or 8) by timing each on
+// the plan's own transforms.  Every candidate must reproduce the first
+// candidate's output bytes; a disagreement fails the plan.  Returns the
+// candidates as JSON.
+std::string tune_ntt_radix(BatchPlan& p, const uint8_t* d_out) {
+    const uint64_t bytes = 32 * p.ntt_elements;
+    DevBuf first, differ;
+    uint8_t* ref = first.as<uint8_t>(bytes);
+    uint32_t* d_differ = differ.as<uint32_t>(1);
+    std::string cands;
+    double best_ms = 1e300;
+    int best_r = 0;
+    for (int r = 1; r <= 3; ++r) {
+        ntt_batch_set_radix(p.ntt, r);
+        const double ms = time_ntt(p, 3);
+        ntt_batch_check(p.ntt, p.stream);
+        if (r == 1) {
+            DV_CUDA(cudaMemcpyAsync(ref, d_out, bytes, cudaMemcpyDeviceToDevice, p.stream));
+        } else {
+            uint32_t h = 0;
+            DV_CUDA(cudaMemsetAsync(d_differ, 0, sizeof(uint32_t), p.stream));
+            const uint64_t words = bytes / 16;
+            const uint32_t grid = (uint32_t)std::min<uint64_t>((words + 255) / 256, 4ull * sm_count());
+            k_words_differ<<<std::max(1u, grid), 256, 0, p.stream>>>((const uint4*)ref, (const uint4*)d_out, words,
+                                                                     d_differ);
+            DV_LAUNCH();
+            DV_CUDA(cudaMemcpyAsync(&h, d_differ, sizeof(uint32_t), cudaMemcpyDeviceToHost, p.stream));
+            DV_CUDA(cudaStreamSynchronize(p.stream));
+            if (h) throw CudaFailure("batch NTT radix " + std::to_string(1 << r) + " disagrees with radix 2");
+        }
+        cands += std::string(cands.empty() ? "" : ",") + "{\"radix\":" + std::to_string(1 << r) +
+                 ",\"grid\":" + std::to_string(p.ntt.grid) + ",\"ms\":" + std::to_string(ms) + "}";
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_r = r;
+        }
+    }
+    ntt_batch_set_radix(p.ntt, best_r);
+    return cands;
+}
+
 }  // namespace
 
 BatchPlan::~BatchPlan() {
@@ -156,6 +227,7 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
         items.push_back(NttBatchItem{nin + 32 * p.ntt_off[j], nout + 32 * p.ntt_off[j], (int)ntt_logs[j],
                                      ntt_kinds.empty() ? 0 : (int)ntt_kinds[j]});
     ntt_batch_prepare(p.ntt_ws, p.ntt, items, p.stream);
+    const std::string ntt_cands = p.ntt.count ? tune_ntt_radix(p, nout) : std::string();
 
     // ---- classes: set maps, autotuned window width, precomputed table
     log = "{\"classes\":[";
@@ -222,7 +294,8 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
     }
     log += "],\"ntt\":{\"transforms\":" + std::to_string(p.ntt.count) +
            ",\"elements\":" + std::to_string(p.ntt.elements) + ",\"tiles\":" + std::to_string(p.ntt.ntiles) +
-           ",\"grid\":" + std::to_string(p.ntt.grid) + "}";
+           ",\"grid\":" + std::to_string(p.ntt.grid) + ",\"candidates\":[" + ntt_cands +
+           "],\"best_radix\":" + std::to_string(1 << p.ntt.radix_log) + "}";
 
     // ---- one uncaptured run (final workspace sizes), then capture
     enqueue_all(p);

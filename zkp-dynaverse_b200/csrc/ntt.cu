@@ -473,8 +473,10 @@ struct BatchTile {
 // dependency wait gave up), ctl[2 + 3 d + p]: finished tiles of pass p of
 // transform d.  Tiles are listed pass by pass, so a tile only waits for
 // tiles that running blocks took earlier.
+// Radix 8 holds 8 elements and 4 twiddles in registers: it gets two
+// resident blocks (128 registers) instead of three.
 template <int R_LOG>
-__global__ void __launch_bounds__(256, DV_NTT_MINB) k_ntt_batch(const BatchDesc* __restrict__ descs,
+__global__ void __launch_bounds__(256, R_LOG >= 3 ? 2 : DV_NTT_MINB) k_ntt_batch(const BatchDesc* __restrict__ descs,
                                                                 const BatchTile* __restrict__ tiles, uint32_t ntiles,
                                                                 uint32_t* __restrict__ ctl) {
     extern __shared__ __align__(16) uint32_t sm[];
@@ -571,14 +573,31 @@ void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttB
     if (count) DV_CUDA(cudaMemcpyAsync(d_descs, descs.data(), count * sizeof(BatchDesc), cudaMemcpyHostToDevice, st));
     if (!all.empty())
         DV_CUDA(cudaMemcpyAsync(d_tiles, all.data(), all.size() * sizeof(BatchTile), cudaMemcpyHostToDevice, st));
-    const int smem = 32 << BATCH_TILE_LOG;
-    DV_CUDA(cudaFuncSetAttribute(k_ntt_batch<DV_NTT_RADIX_LOG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    int per_sm = 0;
-    DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ntt_batch<DV_NTT_RADIX_LOG>, 256, smem));
-    batch.grid = (uint32_t)std::max<uint64_t>(
-        1, std::min<uint64_t>((uint64_t)sm_count() * (uint32_t)std::max(1, per_sm), batch.ntiles));
+    ntt_batch_set_radix(batch, DV_NTT_RADIX_LOG);
     // the host descriptor vectors must outlive the copies above
     DV_CUDA(cudaStreamSynchronize(st));
+}
+
+namespace {
+template <int R_LOG>
+uint32_t batch_grid(uint32_t ntiles) {
+    const int smem = 32 << BATCH_TILE_LOG;
+    DV_CUDA(cudaFuncSetAttribute(k_ntt_batch<R_LOG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ntt_batch<R_LOG>, 256, smem));
+    return (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>((uint64_t)sm_count() * (uint32_t)std::max(1, per_sm), ntiles));
+}
+}  // namespace
+
+void ntt_batch_set_radix(NttBatch& batch, int radix_log) {
+    switch (radix_log) {
+        case 1: batch.grid = batch_grid<1>(batch.ntiles); break;
+        case 2: batch.grid = batch_grid<2>(batch.ntiles); break;
+        case 3: batch.grid = batch_grid<3>(batch.ntiles); break;
+        default: throw InvalidArgument("batch NTT radix_log must be 1, 2 or 3");
+    }
+    batch.radix_log = radix_log;
 }
 
 void ntt_batch_enqueue(NttBatch& batch, cudaStream_t st) {
@@ -586,8 +605,14 @@ void ntt_batch_enqueue(NttBatch& batch, cudaStream_t st) {
     uint32_t* ctl = batch.ctl.as<uint32_t>(2 + 3ull * batch.count);
     DV_CUDA(cudaMemsetAsync(ctl, 0, (2 + 3ull * batch.count) * sizeof(uint32_t), st));
     DV_CUDA(cudaMemsetAsync(batch.errs.as<uint32_t>(batch.count), 0xff, batch.count * sizeof(uint32_t), st));
-    k_ntt_batch<DV_NTT_RADIX_LOG><<<batch.grid, 256, 32 << BATCH_TILE_LOG, st>>>(
-        batch.descs.as<BatchDesc>(batch.count), batch.tiles.as<BatchTile>(batch.ntiles), batch.ntiles, ctl);
+    const BatchDesc* descs = batch.descs.as<BatchDesc>(batch.count);
+    const BatchTile* tiles = batch.tiles.as<BatchTile>(batch.ntiles);
+    const int smem = 32 << BATCH_TILE_LOG;
+    switch (batch.radix_log) {
+        case 1: k_ntt_batch<1><<<batch.grid, 256, smem, st>>>(descs, tiles, batch.ntiles, ctl); break;
+        case 3: k_ntt_batch<3><<<batch.grid, 256, smem, st>>>(descs, tiles, batch.ntiles, ctl); break;
+        default: k_ntt_batch<2><<<batch.grid, 256, smem, st>>>(descs, tiles, batch.ntiles, ctl); break;
+    }
     DV_LAUNCH();
 }
 

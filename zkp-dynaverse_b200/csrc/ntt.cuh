@@ -87,12 +87,17 @@ struct NttBatchItem {
 struct NttBatch {
     DevBuf descs, tiles, ctl, work, errs;
     uint32_t count = 0, ntiles = 0, grid = 0;
+    int radix_log = 2;  // register round of the kernel: radix 2, 4 or 8
     uint64_t elements = 0;
     std::vector<uint64_t> work_off;
 };
 void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttBatchItem>& items,
                        cudaStream_t stream);
 void ntt_batch_enqueue(NttBatch& batch, cudaStream_t stream);
+// Selects the kernel's register round (radix_log 1, 2 or 3: radix 2, 4 or
+// 8 butterflies per round) and sizes the persistent grid from that
+// kernel's occupancy.  Every radix computes the same bytes.
+void ntt_batch_set_radix(NttBatch& batch, int radix_log);
 // After the stream has completed: throws InvalidArgument naming the first
 // transform with a non-canonical input, or CudaFailure if a dependency wait
 // gave up.
