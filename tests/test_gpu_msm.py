@@ -124,6 +124,23 @@ def test_uneven_batch_and_shared_scalars(backend, oracle):
     assert got[1] == oracle.msm_g1(pts[640:64 * 40], scs[160:160 + 960])
 
 
+def test_uneven_batch_with_long_reduction_segments(backend, oracle):
+    """128 sets of 2^15 points: the batch's window model picks c = 11, so the
+    launch holds 128 x 24 x 2^10 = 3.1 M buckets and the bucket reduction
+    takes 16-bucket segments (2^21 buckets or more) instead of 8.  Every set
+    is compared with the oracle."""
+    from concurrent.futures import ThreadPoolExecutor
+    count, n = 128, 1 << 15
+    base, _ = oracle.srs_g1(7700, n)
+    scs = oracle.uniform_fr(7701, count * n)
+    offs = [k * n for k in range(count + 1)]
+    got = backend.msm_batch_uneven(base * count, scs, offs)
+    with ThreadPoolExecutor(8) as pool:
+        want = list(pool.map(lambda k: oracle.msm_g1(base, scs[32 * k * n:32 * (k + 1) * n]), range(count)))
+    for k in range(count):
+        assert got[k] == want[k], f"set {k}"
+
+
 def test_golden_sparse(backend, golden):
     reqs, expect = [], []
     for case in golden["sparse_g1"]:

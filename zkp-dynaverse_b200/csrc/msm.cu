@@ -735,7 +735,14 @@ void msm_enqueue(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_
     const uint64_t all_buckets = (uint64_t)NW * B;
     int room = 0;
     while ((all_buckets >> (room + 1)) >= (1u << 15)) ++room;
-    seg_want = std::min(seg_want, room);
+    // Many buckets in all (a batch of sets over one table, 2^21 buckets or
+    // more): longer segments, up to 64 buckets, while at least 2^17
+    // first-level threads remain (several waves of k_segments at two blocks
+    // per SM).  Each halving of the segment count halves the first upper
+    // level, whose warp-0 phases and doublings leave most lanes idle.
+    int wide = 0;
+    while (wide < 6 && (all_buckets >> (wide + 1)) >= (1u << 17)) ++wide;
+    seg_want = std::min(std::max(seg_want, wide), room);
     const int seg_log = std::min(seg_want, c - 1);
     const uint32_t S = B >> seg_log;
     XYZZ<F>* d_seg_u = ws.segs.as<XYZZ<F>>(4ull * NW * S);
