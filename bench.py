@@ -21,8 +21,8 @@ output vector).
                         call with pinned HOST buffers (host->device input
                         copies and the result copy inside the timed region).
   roofline            : integer-multiply bound.  MSM: the bucket-accumulation
-                        kernel, (points x windows) XYZZ mixed additions x 10
-                        Fq multiplications x 136 32x32->64-bit
+                        kernel, (points x windows) XYZZ mixed additions x (8
+                        Fq products x 136 + 2 Fq squares x 108) 32x32->64-bit
                         multiply-accumulates per launch, over its CUDA-event
                         duration.  Other operators: the whole call, with the
                         algorithmic multiplication count stated in the line.
@@ -91,13 +91,26 @@ def parse():
     return a
 
 
-def msm_fme(n, g2=False):
-    """Algorithmic work of an MSM in Fq multiplications (Fq2 multiplication
-    = 3): min over c of ceil(254/c) * (10 n + 14 * 2^c), times 3 for G2."""
+# 32x32->64-bit multiply-accumulates of one Montgomery product and one
+# Montgomery square (cross products once, then the reduction) over Fq.
+MAC_MUL, MAC_SQR = 136, 108
+# XYZZ mixed addition (madd-2008-s: 8 products, 2 squares) and full addition
+# (add-2008-s: 12 products, 2 squares) over Fq; over Fq2 a product is three
+# Fq products (Karatsuba) and a square two.
+G1_MADD_MACS = 8 * MAC_MUL + 2 * MAC_SQR
+G1_ADD_MACS = 12 * MAC_MUL + 2 * MAC_SQR
+G2_MADD_MACS = (8 * 3 + 2 * 2) * MAC_MUL
+G2_ADD_MACS = (12 * 3 + 2 * 2) * MAC_MUL
+
+
+def msm_macs(n, g2=False):
+    """Algorithmic work of an n-point MSM in multiply-accumulates: min over c
+    of ceil(254/c) * (n mixed additions + 2^c full additions: two per bucket
+    of the bucket reduction)."""
     if n <= 0:
         return 0
-    w = min(math.ceil(254 / c) * (10 * n + 14 * (1 << c)) for c in range(2, 24))
-    return 3 * w if g2 else w
+    madd, add = (G2_MADD_MACS, G2_ADD_MACS) if g2 else (G1_MADD_MACS, G1_ADD_MACS)
+    return min(math.ceil(254 / c) * (madd * n + add * (1 << c)) for c in range(2, 24))
 
 
 class ClockSampler:
@@ -232,10 +245,10 @@ class MsmOp:
         return self.n * (self.size + 32), self.size + self.config["windows"] * 2 * self.size
 
     def roofline(self, tl, imad_peak, step_ms):
-        macs_total = msm_fme(self.n, self.g2) * 136
+        macs_total = msm_macs(self.n, self.g2)
         accum_ms = tl.ms[3] / max(1, tl.calls)
         adds = tl.accum_mixed_adds / max(1, tl.calls)
-        macs = adds * 10 * 136 * (3 if self.g2 else 1)
+        macs = adds * (G2_MADD_MACS if self.g2 else G1_MADD_MACS)
         ach = macs / (accum_ms * 1e-3) / 1e12
         return ({"bound": "imad", "kernel": "k_accum (bucket accumulation)", "achieved": ach,
                  "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
@@ -396,7 +409,7 @@ class SparseOp:
         return self.k * 40, 64
 
     def roofline(self, tl, imad_peak, step_ms):
-        macs = msm_fme(self.k) * 136
+        macs = msm_macs(self.k)
         ach = macs / (step_ms * 1e-3) / 1e12
         return ({"bound": "imad", "kernel": "whole sparse MSM (gather + Pippenger)", "achieved": ach,
                  "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
@@ -451,9 +464,9 @@ class FixedBaseOp:
     secondary_key = "convention_64_adds_roofline"
 
     def roofline(self, tl, imad_peak, step_ms):
-        macs = self.n * (16 * 10 + 10) * 136  # 16 mixed adds (16-bit signed windows) + warp-shared normalisation
+        macs = self.n * (16 * G1_MADD_MACS + 10 * MAC_MUL)  # 16 mixed adds (16-bit signed windows) + warp-shared normalisation
         ach = macs / (step_ms * 1e-3) / 1e12
-        conv = self.n * (64 * 10 + 10) * 136
+        conv = self.n * (64 * G1_MADD_MACS + 10 * MAC_MUL)
         conv_ach = conv / (step_ms * 1e-3) / 1e12
         return ({"bound": "imad", "kernel": "k_fb_generate", "achieved": ach, "peak": imad_peak / 1e12,
                  "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12), "algorithmic_macs_per_launch": macs,
@@ -556,17 +569,18 @@ class G2CheckOp:
                                             f"scaled linearly; verdicts identical to the GPU's: {agree}")
 
 
-def ecntt_fme(logn, rows):
-    """Fq multiplications of a G1 transform: per stage, every butterfly costs
-    two XYZZ additions (2 x 14) and every butterfly with a twiddle other than
-    1 a GLV scalar multiplication over signed 5-bit windows of its two
-    127-bit halves: the table of 1..16 multiples (8 doublings x 9, 7
-    additions x 14), then 26 windows (125 doublings x 9, two additions x 14
-    and one product beta X a window)."""
+def ecntt_macs(logn, rows):
+    """Multiply-accumulates of a G1 transform: per stage, every butterfly
+    costs two XYZZ additions and every butterfly with a twiddle other than 1
+    a GLV scalar multiplication over signed 5-bit windows of its two 127-bit
+    halves: the table of 1..16 multiples (8 doublings, 7 additions), then 26
+    windows (125 doublings, two additions and one product beta X a window).
+    A paired doubling is 7 products and 2 squares."""
     n = 1 << logn
-    smul = 8 * 9 + 7 * 14 + 125 * 9 + 26 * (2 * 14 + 1)
+    dbl = 7 * MAC_MUL + 2 * MAC_SQR
+    smul = 8 * dbl + 7 * G1_ADD_MACS + 125 * dbl + 26 * (2 * G1_ADD_MACS + MAC_MUL)
     nontrivial = sum(rows * (n // 2 - (1 << s)) for s in range(logn))
-    return rows * (n // 2) * logn * 28 + nontrivial * smul
+    return rows * (n // 2) * logn * 2 * G1_ADD_MACS + nontrivial * smul
 
 
 class EcNttOp:
@@ -614,7 +628,7 @@ class EcNttOp:
         return self.n * 64, self.n * 64
 
     def roofline(self, tl, imad_peak, step_ms):
-        macs = ecntt_fme(self.logn, self.rows) * 136
+        macs = ecntt_macs(self.logn, self.rows)
         ach = macs / (step_ms * 1e-3) / 1e12
         return ({"bound": "imad", "kernel": "k_ec_stage (all stages) + k_ec_store", "achieved": ach,
                  "peak": imad_peak / 1e12, "unit": "TMAC/s", "frac": ach / (imad_peak / 1e12),
@@ -756,7 +770,7 @@ class ServeOp:
             last[j] = sat_served["commitments"][t]
         for j, c in last.items():
             exact = exact and b.msm(self.sess[j][0], bytes(vecs[j])) == c
-        macs = sum(msm_fme(len(idx)) for _, idx, _ in self.reqs) * 136
+        macs = sum(msm_macs(len(idx)) for _, idx, _ in self.reqs)
         ach = macs / sat_served["wall_s"] / 1e12
         peak = imad_peak_fn() / 1e12
         strip = lambda r: {k: v for k, v in r.items() if k != "commitments"}
@@ -970,13 +984,13 @@ def operator_points(torch, dv, b, s, imad_peak, threads, with_cpu=True):
     ms, res = timed(lambda: m.step(b, s))
     m.host_inputs(torch)
     e2e = wall(lambda: m.e2e_step(dv, b), 10)
-    macs = msm_fme(m.n) * 136
+    macs = msm_macs(m.n)
     d = {"call": "dvgpu_bn254_msm (plain: bases and scalars from host memory every call)", "points": m.n,
          "window_bits": m.tuned_c, "device_ms": ms, "e2e_ms": e2e,
          "h2d_bytes": m.n * 96, "d2h_bytes": 64 + m.config["windows"] * 128,
          "roofline": {"bound": "imad", "achieved": macs / (ms * 1e-3) / 1e12, "peak": imad_peak / 1e12,
                       "unit": "TMAC/s", "frac": macs / (ms * 1e-3) / imad_peak,
-                      "convention": "min_c ceil(254/c)(10 n + 14 2^c) Fq products x 136 MACs"}}
+                      "convention": "min_c ceil(254/c)(n mixed + 2^c full XYZZ additions); a mixed addition 8 x 136 + 2 x 108 MACs, a full one 12 x 136 + 2 x 108"}}
     if with_cpu:
         cpu_out, cpu_ms, _ = m.cpu(oracle, threads)
         d["cpu_oracle"] = {"ms": cpu_ms, "cores": threads, "matches_gpu": cpu_out == res}
@@ -1154,7 +1168,7 @@ class ProofServeOp:
         macs = sat_served["msm_fme"] * 136
         ach = macs / sat_served["wall_s"] / 1e12
         # the dominant kernel: the dense MSMs' bucket accumulation, timed live
-        acc_macs = sat_served["dense_accum_adds"] * 10 * 136
+        acc_macs = sat_served["dense_accum_adds"] * G1_MADD_MACS
         acc_ach = acc_macs / max(1e-9, sat_served["dense_accum_ms"] * 1e-3) / 1e12
         strip = lambda r: {k: v for k, v in r.items() if k != "proofs"}
         job_per_s = world * self.requests / max_over_ranks(sat_served["wall_s"], world)
@@ -1179,14 +1193,14 @@ class ProofServeOp:
                          "peak_source": "dvgpu_probe_imad_rate, measured in this run",
                          "algorithmic_macs_per_launch": acc_macs / max(1, sat_served["batches"]),
                          "launch_ms": sat_served["dense_accum_ms"] / max(1, sat_served["batches"]),
-                         "convention": "10 Fq products x 136 MACs per XYZZ mixed addition, 16 per dense term",
+                         "convention": "8 Fq products x 136 + 2 Fq squares x 108 MACs per XYZZ mixed addition, 16 per dense term",
                          "traffic": (None if load_traffic("dynaverse_dense_accum", "traffic_bytes_per_add") is None
                                      else load_traffic("dynaverse_dense_accum", "traffic_bytes_per_add") *
                                      sat_served["dense_accum_adds"] / max(1, sat_served["batches"])),
                          "traffic_note": ("DRAM bytes per mixed addition of a captured 64-job launch "
                                           "(profiles/dynaverse_dense_accum.txt) x this run's additions per launch")},
             "msm_whole_run": {"achieved": ach, "frac": ach / peak, "algorithmic_macs": macs,
-                              "convention": "sum over MSM sets of min_c ceil(254/c)(10k + 14 2^c) x 136 (x3 G2), "
+                              "convention": "sum over MSM sets of min_c ceil(254/c)(10k + 14 2^c) Fq products x 136 (x3 G2; squares counted as products), "
                                             "over the saturation run's wall time"},
             "gpu_launches": sat_served["launches"], "clocks": clocks,
         }
@@ -1216,20 +1230,20 @@ def batch_workload(log_bases):
 
 
 def batch_macs(sizes, logs):
-    return (sum(msm_fme(n) for n in sizes) + sum((1 << L) // 2 * L for L in logs)) * 136
+    return sum(msm_macs(n) for n in sizes) + sum((1 << L) // 2 * L for L in logs) * MAC_MUL
 
 
 def batch_cpu(oracle, threads, bases, sizes, logs, scalars, ntt_vals):
     """CPU oracle on a bounded sample of the batch (MSMs in order until 2^20
     points, on all threads; the first 8 NTTs on 1 thread), scaled to the
     whole batch by algorithmic multiply-accumulates."""
-    msm_t, msm_macs, off, k = 0.0, 0, 0, 0
+    msm_t, msm_done, off, k = 0.0, 0, 0, 0
     while k < len(sizes) and (k == 0 or sum(sizes[:k]) < (1 << 20)):
         n = sizes[k]
         t0 = time.perf_counter()
         oracle.msm_g1(bases[:64 * n], scalars[32 * off:32 * (off + n)], threads=threads)
         msm_t += time.perf_counter() - t0
-        msm_macs += msm_fme(n) * 136
+        msm_done += msm_macs(n)
         off += n
         k += 1
     ntt_t, ntt_macs, noff = 0.0, 0, 0
@@ -1240,9 +1254,9 @@ def batch_cpu(oracle, threads, bases, sizes, logs, scalars, ntt_vals):
         ntt_t += time.perf_counter() - t0
         ntt_macs += n // 2 * L * 136
         noff += n
-    all_msm = sum(msm_fme(n) for n in sizes) * 136
+    all_msm = sum(msm_macs(n) for n in sizes)
     all_ntt = sum((1 << L) // 2 * L for L in logs) * 136
-    ms = (msm_t * all_msm / msm_macs + ntt_t * all_ntt / ntt_macs) * 1e3
+    ms = (msm_t * all_msm / msm_done + ntt_t * all_ntt / ntt_macs) * 1e3
     return ms, (f"{k} MSMs ({sum(sizes[:k])} points, {threads} threads) and 8 NTTs (1 thread), scaled to the "
                 f"whole batch by algorithmic multiply-accumulates")
 

@@ -76,7 +76,7 @@ struct XYZZ {
             const F pp_ = F::sub(us.r0, p.x);
             const F r = F::sub(us.r1, p.y);
             if (pp_.is_zero()) return add_affine_equal_x(a, r);
-            const auto sq = F::mul2(pp_, pp_, r, r);           // PP, R^2
+            const auto sq = F::sqr2(pp_, r);                   // PP, R^2
             const F pp = sq.r0;
             const auto pq = F::mul2(pp_, pp, p.x, pp);          // PPP, Q
             const F ppp = pq.r0, q = pq.r1;
@@ -127,7 +127,7 @@ struct XYZZ {
     DV_INL static XYZZ dbl_paired(const XYZZ& p) {
         if (p.is_inf()) return p;
         const F u = F::dbl(p.y);
-        const auto vx = F::mul2(u, u, p.x, p.x);      // V = U^2, X^2
+        const auto vx = F::sqr2(u, p.x);              // V = U^2, X^2
         const F v = vx.r0;
         const auto ws = F::mul2(u, v, p.x, v);         // W = U V, S = X V
         const F w = ws.r0, s = ws.r1;
@@ -149,7 +149,7 @@ struct XYZZ {
             if (r.is_zero()) return dbl_paired(p);
             return inf();
         }
-        const auto sq = F::mul2(pp_, pp_, r, r);        // PP, R^2
+        const auto sq = F::sqr2(pp_, r);                // PP, R^2
         const F pp = sq.r0;
         const auto pq = F::mul2(pp_, pp, u.r0, pp);     // PPP, Q
         const F ppp = pq.r0, qq = pq.r1;
