@@ -5,6 +5,7 @@
 // retire the owner (-2/-3), later calls return -4; outputs are written only
 // on success; C++ exceptions never cross the ABI.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cstring>
 #include <memory>
@@ -170,20 +171,20 @@ bool root_has_order_2_20(const uint8_t* root) {
 
 // The arkworks root of order 2^20 (TWO_ADIC_ROOT_OF_UNITY squared 8 times).
 bool is_default_root20(const uint8_t* root) {
-    static uint8_t expect[32];
-    static bool init = false;
-    if (!init) {
+    // computed once, under the thread-safe initialisation of a local static
+    static const std::array<uint8_t, 32> expect = [] {
         const uint64_t r28[4] = {0x9bd61b6e725b19f0ull, 0x402d111e41112ed4ull, 0x00e0a7eb8ef62abcull,
                                  0x2a3c09f0a58a7e85ull};
         uint64_t x[4], one_raw[4] = {1, 0, 0, 0};
         fr_mul(x, r28, FR_R2);
         for (int i = 0; i < 8; ++i) fr_mul(x, x, x);
         fr_mul(x, x, one_raw);
+        std::array<uint8_t, 32> e{};
         for (int i = 0; i < 4; ++i)
-            for (int k = 0; k < 8; ++k) expect[8 * i + k] = (uint8_t)(x[i] >> (8 * k));
-        init = true;
-    }
-    return !memcmp(root, expect, 32);
+            for (int k = 0; k < 8; ++k) e[8 * i + k] = (uint8_t)(x[i] >> (8 * k));
+        return e;
+    }();
+    return !memcmp(root, expect.data(), 32);
 }
 
 // IMAD roofline probe kernels: 16 independent accumulator rows per thread.

@@ -1481,7 +1481,7 @@ private:
             }
             lk.unlock();
             const uint64_t t0 = now_ns();
-            const uint64_t l0 = launch_counter();
+            const uint64_t l0 = __atomic_load_n(&launch_counter(), __ATOMIC_RELAXED);
             const uint64_t a0 = __atomic_load_n(&alloc_counter(), __ATOMIC_RELAXED);
             const uint64_t an0 = __atomic_load_n(&alloc_ns_counter(), __ATOMIC_RELAXED);
             std::vector<Outcome> outs(batch.size());
@@ -1502,7 +1502,7 @@ private:
             stat_batches_++;
             stat_largest_ = std::max<uint64_t>(stat_largest_, batch.size());
             stat_busy_ns_ += t1 - t0;
-            stat_launches_ += launch_counter() - l0;
+            stat_launches_ += __atomic_load_n(&launch_counter(), __ATOMIC_RELAXED) - l0;
             stat_allocs_ += __atomic_load_n(&alloc_counter(), __ATOMIC_RELAXED) - a0;
             stat_alloc_ns_ += __atomic_load_n(&alloc_ns_counter(), __ATOMIC_RELAXED) - an0;
             done_cv_.notify_all();

@@ -125,13 +125,15 @@ struct PinnedBuf {
     PinnedBuf& operator=(const PinnedBuf&) = delete;
 };
 
+// SM count of the device current at the first call (every device of a
+// node is the same part), read once under thread-safe static initialisation.
 inline int sm_count() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
+    static const int n = [] {
+        int dev = 0, v = 0;
         DV_CUDA(cudaGetDevice(&dev));
-        DV_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
-    }
+        DV_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        return v;
+    }();
     return n;
 }
 

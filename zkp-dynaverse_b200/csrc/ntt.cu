@@ -1,5 +1,6 @@
 // Fr NTT kernels and launch sequence (see ntt.cuh).
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -317,14 +318,15 @@ constexpr int MAX_DEVICES = 64;
 template <int THREADS>
 void launch_pass(const PassArgs& a, cudaStream_t st) {
     const size_t smem = (size_t)32 << a.k;  // two planes of 16 bytes per element
-    static bool configured[MAX_DEVICES] = {};
+    static std::atomic<bool> configured[MAX_DEVICES] = {};
     int dev = 0;
     DV_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= MAX_DEVICES) throw InvalidArgument("device ordinal out of range");
-    if (!configured[dev]) {
+    if (!configured[dev].load(std::memory_order_acquire)) {
+        // idempotent: threads racing here set the same attribute
         DV_CUDA(cudaFuncSetAttribute(k_dif_pass<THREADS, DV_NTT_RADIX_LOG>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-        configured[dev] = true;
+        configured[dev].store(true, std::memory_order_release);
     }
     const unsigned groups = 1u << (a.logn - a.k);
     k_dif_pass<THREADS, DV_NTT_RADIX_LOG><<<groups, THREADS, smem, st>>>(a);
