@@ -528,8 +528,12 @@ int dvgpu_bn254_ntt_batch_device(void* backend, const uint8_t* d_values, const u
  * the MSMs are grouped into size classes; the autotuner times candidate
  * window widths per class on random scalars, keeps a table of precomputed
  * window multiples for the best one and writes its log (JSON) to log_json.
- * Each class is one launch sequence over all its MSMs; the NTTs are one
- * persistent launch on a parallel branch of the graph.
+ * It also times the persistent NTT launch with radix 2, 4 and 8 register
+ * rounds on the plan's own transforms, requires every candidate's output to
+ * equal the first's (a mismatch fails the call) and keeps the fastest (log
+ * keys ntt.candidates, ntt.best_radix).  Each class is one launch sequence
+ * over all its MSMs; the NTTs are one persistent launch on a parallel
+ * branch of the graph.
  *
  * dvgpu_batch_plan_buffers: the plan's device buffers (inputs in request
  * order, outputs in request order: 64-byte affine G1 results, canonical NTT
