@@ -107,24 +107,43 @@ double time_ntt(BatchPlan& p, int reps) {
     return best;
 }
 
-// differ[0] != 0 when the two arrays of n 16-byte words differ anywhere.
-__global__ void k_words_differ(const uint4* __restrict__ a, const uint4* __restrict__ b, uint64_t n,
-                               uint32_t* differ) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint4 x = a[i], y = b[i];
-        if ((x.x ^ y.x) | (x.y ^ y.y) | (x.z ^ y.z) | (x.w ^ y.w)) *differ = 1;
+// Weight of word i in the output hash: the splitmix64 finaliser of i
+// (Steele, Lea, Flood 2014), odd so that no word's low bits are lost.
+DV_INL uint64_t word_weight(uint64_t i) {
+    uint64_t z = i + 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return (z ^ (z >> 31)) | 1ull;
+}
+
+// out += sum over the n 32-bit words w_i of w_i * word_weight(i) (mod 2^64):
+// independent of the order of the additions, so two arrays with the same
+// words give the same value and a difference anywhere changes it except
+// with negligible probability.
+__global__ void k_words_hash(const uint4* __restrict__ a, uint64_t n16, unsigned long long* out) {
+    uint64_t h = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n16;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint4 x = a[i];
+        h += x.x * word_weight(4 * i) + x.y * word_weight(4 * i + 1) + x.z * word_weight(4 * i + 2) +
+             x.w * word_weight(4 * i + 3);
     }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) h += __shfl_down_sync(0xffffffffu, h, d);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)h);
 }
 
 // Picks the batch NTT's register round (radix 2, 4 or 8) by timing each on
-// the plan's own transforms.  Every candidate must reproduce the first
-// candidate's output bytes; a disagreement fails the plan.  Returns the
-// candidates as JSON.
+// the plan's own transforms.  Every candidate's outputs must hash to the
+// first candidate's (a 64-bit position-weighted sum of the output words,
+// so no second copy of the outputs is held); a disagreement fails the
+// plan.  Returns the candidates as JSON.
 std::string tune_ntt_radix(BatchPlan& p, const uint8_t* d_out) {
-    const uint64_t bytes = 32 * p.ntt_elements;
-    DevBuf first, differ;
-    uint8_t* ref = first.as<uint8_t>(bytes);
-    uint32_t* d_differ = differ.as<uint32_t>(1);
+    const uint64_t n16 = 2 * p.ntt_elements;  // 16-byte words of the outputs
+    DevBuf hash;
+    unsigned long long* d_hash = hash.as<unsigned long long>(1);
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n16 + 255) / 256, 4ull * sm_count()));
+    unsigned long long first = 0;
     std::string cands;
     double best_ms = 1e300;
     int best_r = 0;
@@ -132,20 +151,15 @@ std::string tune_ntt_radix(BatchPlan& p, const uint8_t* d_out) {
         ntt_batch_set_radix(p.ntt, r);
         const double ms = time_ntt(p, 3);
         ntt_batch_check(p.ntt, p.stream);
-        if (r == 1) {
-            DV_CUDA(cudaMemcpyAsync(ref, d_out, bytes, cudaMemcpyDeviceToDevice, p.stream));
-        } else {
-            uint32_t h = 0;
-            DV_CUDA(cudaMemsetAsync(d_differ, 0, sizeof(uint32_t), p.stream));
-            const uint64_t words = bytes / 16;
-            const uint32_t grid = (uint32_t)std::min<uint64_t>((words + 255) / 256, 4ull * sm_count());
-            k_words_differ<<<std::max(1u, grid), 256, 0, p.stream>>>((const uint4*)ref, (const uint4*)d_out, words,
-                                                                     d_differ);
-            DV_LAUNCH();
-            DV_CUDA(cudaMemcpyAsync(&h, d_differ, sizeof(uint32_t), cudaMemcpyDeviceToHost, p.stream));
-            DV_CUDA(cudaStreamSynchronize(p.stream));
-            if (h) throw CudaFailure("batch NTT radix " + std::to_string(1 << r) + " disagrees with radix 2");
-        }
+        unsigned long long h = 0;
+        DV_CUDA(cudaMemsetAsync(d_hash, 0, sizeof(unsigned long long), p.stream));
+        k_words_hash<<<grid, 256, 0, p.stream>>>((const uint4*)d_out, n16, d_hash);
+        DV_LAUNCH();
+        DV_CUDA(cudaMemcpyAsync(&h, d_hash, sizeof(h), cudaMemcpyDeviceToHost, p.stream));
+        DV_CUDA(cudaStreamSynchronize(p.stream));
+        if (r == 1) first = h;
+        else if (h != first)
+            throw CudaFailure("batch NTT radix " + std::to_string(1 << r) + " disagrees with radix 2");
         cands += std::string(cands.empty() ? "" : ",") + "{\"radix\":" + std::to_string(1 << r) +
                  ",\"grid\":" + std::to_string(p.ntt.grid) + ",\"ms\":" + std::to_string(ms) + "}";
         if (ms < best_ms) {
