@@ -1301,6 +1301,7 @@ class BatchOp:
                        "ntt_elements_total": self.ntt_elems, "ntt_logs": [min(self.logs), max(self.logs)],
                        "msm_classes": [{"sets": c["sets"], "c": c["best_c"]} for c in self.tune_log["classes"]],
                        "ntt_radix": self.tune_log["ntt"].get("best_radix"),
+                       "ntt_tile": self.tune_log["ntt"].get("best_tile"),
                        "graph_nodes": self.buf.graph_nodes, "graph_kernels": self.buf.graph_kernels}
         self.launches_per_step = self.buf.graph_kernels
         # library kernels run so far (captured launches did not run): a

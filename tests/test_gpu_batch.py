@@ -122,10 +122,12 @@ def test_batch_plan_matches_oracle_and_replays(backend, oracle, dv):
         assert sum(c["sets"] for c in log["classes"]) == len(sizes)
         for c in log["classes"]:
             assert c["best_c"] in [x["c"] for x in c["candidates"]]
-        # the NTT's register round is picked from radix 2, 4 and 8, each
-        # checked against the first on the device while the plan is built
-        radices = [x["radix"] for x in log["ntt"]["candidates"]]
-        assert radices == [2, 4, 8] and log["ntt"]["best_radix"] in radices
+        # the NTT's tile (2^10..2^12 elements) and register round (radix 2,
+        # 4, 8) are picked from every pair, each checked against the first
+        # on the device while the plan is built
+        pairs = [(x["tile"], x["radix"]) for x in log["ntt"]["candidates"]]
+        assert pairs == [(t, r) for t in (1024, 2048, 4096) for r in (2, 4, 8)]
+        assert (log["ntt"]["best_tile"], log["ntt"]["best_radix"]) in pairs
         for rep in range(2):  # the second run replays the graph on new inputs
             scs = [oracle.uniform_fr(5200 + 100 * rep + i, n) for i, n in enumerate(sizes)]
             scs[3] = bytes(32 * sizes[3])  # all-zero scalars: infinity

@@ -133,40 +133,53 @@ __global__ void k_words_hash(const uint4* __restrict__ a, uint64_t n16, unsigned
     if ((threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)h);
 }
 
-// Picks the batch NTT's register round (radix 2, 4 or 8) by timing each on
-// the plan's own transforms.  Every candidate's outputs must hash to the
-// first candidate's (a 64-bit position-weighted sum of the output words,
-// so no second copy of the outputs is held); a disagreement fails the
-// plan.  Returns the candidates as JSON.
-std::string tune_ntt_radix(BatchPlan& p, const uint8_t* d_out) {
+// Picks the batch NTT's tile (2^10, 2^11 or 2^12 elements: 32, 64 or 128 KB
+// of shared memory, hence fewer or more passes and resident blocks) and
+// register round (radix 2, 4 or 8) by timing each pair on the plan's own
+// transforms.  Every candidate's outputs must hash to the first
+// candidate's (a 64-bit position-weighted sum of the output words, so no
+// second copy of the outputs is held); a disagreement fails the plan.
+// Returns the candidates as JSON.
+std::string tune_ntt(BatchPlan& p, const std::vector<NttBatchItem>& items, const uint8_t* d_out) {
     const uint64_t n16 = 2 * p.ntt_elements;  // 16-byte words of the outputs
     DevBuf hash;
     unsigned long long* d_hash = hash.as<unsigned long long>(1);
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n16 + 255) / 256, 4ull * sm_count()));
     unsigned long long first = 0;
+    bool have_first = false;
     std::string cands;
     double best_ms = 1e300;
-    int best_r = 0;
-    for (int r = 1; r <= 3; ++r) {
-        ntt_batch_set_radix(p.ntt, r);
-        const double ms = time_ntt(p, 3);
-        ntt_batch_check(p.ntt, p.stream);
-        unsigned long long h = 0;
-        DV_CUDA(cudaMemsetAsync(d_hash, 0, sizeof(unsigned long long), p.stream));
-        k_words_hash<<<grid, 256, 0, p.stream>>>((const uint4*)d_out, n16, d_hash);
-        DV_LAUNCH();
-        DV_CUDA(cudaMemcpyAsync(&h, d_hash, sizeof(h), cudaMemcpyDeviceToHost, p.stream));
-        DV_CUDA(cudaStreamSynchronize(p.stream));
-        if (r == 1) first = h;
-        else if (h != first)
-            throw CudaFailure("batch NTT radix " + std::to_string(1 << r) + " disagrees with radix 2");
-        cands += std::string(cands.empty() ? "" : ",") + "{\"radix\":" + std::to_string(1 << r) +
-                 ",\"grid\":" + std::to_string(p.ntt.grid) + ",\"ms\":" + std::to_string(ms) + "}";
-        if (ms < best_ms) {
-            best_ms = ms;
-            best_r = r;
+    int best_t = BATCH_TILE_DEFAULT, best_r = 0;
+    for (int t = 10; t <= BATCH_TILE_MAX; ++t) {
+        ntt_batch_prepare(p.ntt_ws, p.ntt, items, p.stream, t);
+        for (int r = 1; r <= 3; ++r) {
+            ntt_batch_set_radix(p.ntt, r);
+            const double ms = time_ntt(p, 3);
+            ntt_batch_check(p.ntt, p.stream);
+            unsigned long long h = 0;
+            DV_CUDA(cudaMemsetAsync(d_hash, 0, sizeof(unsigned long long), p.stream));
+            k_words_hash<<<grid, 256, 0, p.stream>>>((const uint4*)d_out, n16, d_hash);
+            DV_LAUNCH();
+            DV_CUDA(cudaMemcpyAsync(&h, d_hash, sizeof(h), cudaMemcpyDeviceToHost, p.stream));
+            DV_CUDA(cudaStreamSynchronize(p.stream));
+            if (!have_first) {
+                first = h;
+                have_first = true;
+            } else if (h != first) {
+                throw CudaFailure("batch NTT tile 2^" + std::to_string(t) + " radix " + std::to_string(1 << r) +
+                                  " disagrees with the first candidate");
+            }
+            cands += std::string(cands.empty() ? "" : ",") + "{\"tile\":" + std::to_string(1 << t) +
+                     ",\"radix\":" + std::to_string(1 << r) + ",\"grid\":" + std::to_string(p.ntt.grid) +
+                     ",\"tiles\":" + std::to_string(p.ntt.ntiles) + ",\"ms\":" + std::to_string(ms) + "}";
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_t = t;
+                best_r = r;
+            }
         }
     }
+    ntt_batch_prepare(p.ntt_ws, p.ntt, items, p.stream, best_t);
     ntt_batch_set_radix(p.ntt, best_r);
     return cands;
 }
@@ -241,7 +254,7 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
         items.push_back(NttBatchItem{nin + 32 * p.ntt_off[j], nout + 32 * p.ntt_off[j], (int)ntt_logs[j],
                                      ntt_kinds.empty() ? 0 : (int)ntt_kinds[j]});
     ntt_batch_prepare(p.ntt_ws, p.ntt, items, p.stream);
-    const std::string ntt_cands = p.ntt.count ? tune_ntt_radix(p, nout) : std::string();
+    const std::string ntt_cands = p.ntt.count ? tune_ntt(p, items, nout) : std::string();
 
     // ---- classes: set maps, autotuned window width, precomputed table
     log = "{\"classes\":[";
@@ -309,7 +322,8 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
     log += "],\"ntt\":{\"transforms\":" + std::to_string(p.ntt.count) +
            ",\"elements\":" + std::to_string(p.ntt.elements) + ",\"tiles\":" + std::to_string(p.ntt.ntiles) +
            ",\"grid\":" + std::to_string(p.ntt.grid) + ",\"candidates\":[" + ntt_cands +
-           "],\"best_radix\":" + std::to_string(1 << p.ntt.radix_log) + "}";
+           "],\"best_tile\":" + std::to_string(1 << p.ntt.tile_log) +
+           ",\"best_radix\":" + std::to_string(1 << p.ntt.radix_log) + "}";
 
     // ---- one uncaptured run (final workspace sizes), then capture
     enqueue_all(p);

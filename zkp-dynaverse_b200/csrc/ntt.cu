@@ -456,7 +456,6 @@ void ntt_run(NttWorkspace& ws, const uint8_t* d_in, uint8_t* d_out, int logn, in
 // ===================================================================== batches
 namespace {
 
-constexpr int BATCH_TILE_LOG = 11;               // elements per tile: 2^11 (64 KB of shared memory)
 constexpr uint32_t BATCH_SPIN_LIMIT = 1u << 24;  // dependency wait: ~2 s of 128 ns sleeps
 
 struct BatchDesc {
@@ -522,7 +521,9 @@ __global__ void __launch_bounds__(256, R_LOG >= 3 ? 2 : DV_NTT_MINB) k_ntt_batch
 
 }  // namespace
 
-void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttBatchItem>& items, cudaStream_t st) {
+void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttBatchItem>& items, cudaStream_t st,
+                       int tile_log) {
+    if (tile_log < BATCH_TILE_MIN || tile_log > BATCH_TILE_MAX) throw InvalidArgument("batch NTT tile out of range");
     const uint32_t count = (uint32_t)items.size();
     std::vector<BatchDesc> descs(count);
     std::vector<BatchTile> tiles[3];
@@ -545,7 +546,7 @@ void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttB
         d.a = PassArgs{it.in,       work + batch.work_off[i], it.out, sc.tw,    sc.pre_hi, sc.pre_lo,
                        sc.post_hi, sc.post_lo,               sc.post_const,    errs + i, it.logn,  0,
                        0,          1,                        sc.split};
-        d.passes = (it.logn + BATCH_TILE_LOG - 1) / BATCH_TILE_LOG;
+        d.passes = (it.logn + tile_log - 1) / tile_log;  // at most 3: logn <= 24, tile_log >= 8
         for (int p = 0; p < 3; ++p) {
             d.k[p] = d.s0[p] = d.tile_log[p] = 0;
             d.tiles[p] = 0;
@@ -553,12 +554,12 @@ void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttB
         int s0 = 0;
         for (int p = 0; p < d.passes; ++p) {
             const int k = it.logn / d.passes + (p < it.logn % d.passes ? 1 : 0);
-            const int tile_log = std::min(it.logn, BATCH_TILE_LOG);  // 2^(tile_log - k) groups of 2^k per tile
+            const int tl = std::min(it.logn, tile_log);  // 2^(tl - k) groups of 2^k per tile
             const uint64_t groups = 1ull << (it.logn - k);
-            const uint64_t per_tile = 1ull << (tile_log - k);
+            const uint64_t per_tile = 1ull << (tl - k);
             d.k[p] = k;
             d.s0[p] = s0;
-            d.tile_log[p] = tile_log;
+            d.tile_log[p] = tl;
             d.tiles[p] = (uint32_t)(groups / per_tile);
             for (uint64_t g = 0; g < groups; g += per_tile) tiles[p].push_back(BatchTile{i, (uint32_t)p, g});
             s0 += k;
@@ -575,6 +576,7 @@ void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttB
     if (count) DV_CUDA(cudaMemcpyAsync(d_descs, descs.data(), count * sizeof(BatchDesc), cudaMemcpyHostToDevice, st));
     if (!all.empty())
         DV_CUDA(cudaMemcpyAsync(d_tiles, all.data(), all.size() * sizeof(BatchTile), cudaMemcpyHostToDevice, st));
+    batch.tile_log = tile_log;
     ntt_batch_set_radix(batch, DV_NTT_RADIX_LOG);
     // the host descriptor vectors must outlive the copies above
     DV_CUDA(cudaStreamSynchronize(st));
@@ -582,9 +584,11 @@ void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttB
 
 namespace {
 template <int R_LOG>
-uint32_t batch_grid(uint32_t ntiles) {
-    const int smem = 32 << BATCH_TILE_LOG;
-    DV_CUDA(cudaFuncSetAttribute(k_ntt_batch<R_LOG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+uint32_t batch_grid(uint32_t ntiles, int tile_log) {
+    const int smem = 32 << tile_log;
+    // the attribute is a bound shared by every batch: always the largest tile
+    DV_CUDA(cudaFuncSetAttribute(k_ntt_batch<R_LOG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 32 << BATCH_TILE_MAX));
     int per_sm = 0;
     DV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ntt_batch<R_LOG>, 256, smem));
     return (uint32_t)std::max<uint64_t>(
@@ -594,9 +598,9 @@ uint32_t batch_grid(uint32_t ntiles) {
 
 void ntt_batch_set_radix(NttBatch& batch, int radix_log) {
     switch (radix_log) {
-        case 1: batch.grid = batch_grid<1>(batch.ntiles); break;
-        case 2: batch.grid = batch_grid<2>(batch.ntiles); break;
-        case 3: batch.grid = batch_grid<3>(batch.ntiles); break;
+        case 1: batch.grid = batch_grid<1>(batch.ntiles, batch.tile_log); break;
+        case 2: batch.grid = batch_grid<2>(batch.ntiles, batch.tile_log); break;
+        case 3: batch.grid = batch_grid<3>(batch.ntiles, batch.tile_log); break;
         default: throw InvalidArgument("batch NTT radix_log must be 1, 2 or 3");
     }
     batch.radix_log = radix_log;
@@ -609,7 +613,7 @@ void ntt_batch_enqueue(NttBatch& batch, cudaStream_t st) {
     DV_CUDA(cudaMemsetAsync(batch.errs.as<uint32_t>(batch.count), 0xff, batch.count * sizeof(uint32_t), st));
     const BatchDesc* descs = batch.descs.as<BatchDesc>(batch.count);
     const BatchTile* tiles = batch.tiles.as<BatchTile>(batch.ntiles);
-    const int smem = 32 << BATCH_TILE_LOG;
+    const int smem = 32 << batch.tile_log;
     switch (batch.radix_log) {
         case 1: k_ntt_batch<1><<<batch.grid, 256, smem, st>>>(descs, tiles, batch.ntiles, ctl); break;
         case 3: k_ntt_batch<3><<<batch.grid, 256, smem, st>>>(descs, tiles, batch.ntiles, ctl); break;

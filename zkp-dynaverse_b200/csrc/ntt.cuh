@@ -84,15 +84,19 @@ struct NttBatchItem {
 // vectors on the device.  Prepare once, enqueue any number of times (each
 // enqueue = two memsets and one kernel launch, no allocation, no host
 // synchronisation: capturable in a CUDA graph).
+// Elements per tile of the batched NTT: 2^tile_log, staged in 32 << tile_log
+// bytes of shared memory (2^11: 64 KB, three blocks per SM).
+constexpr int BATCH_TILE_MIN = 8, BATCH_TILE_DEFAULT = 11, BATCH_TILE_MAX = 12;
 struct NttBatch {
     DevBuf descs, tiles, ctl, work, errs;
     uint32_t count = 0, ntiles = 0, grid = 0;
     int radix_log = 2;  // register round of the kernel: radix 2, 4 or 8
+    int tile_log = BATCH_TILE_DEFAULT;
     uint64_t elements = 0;
     std::vector<uint64_t> work_off;
 };
 void ntt_batch_prepare(NttWorkspace& ws, NttBatch& batch, const std::vector<NttBatchItem>& items,
-                       cudaStream_t stream);
+                       cudaStream_t stream, int tile_log = BATCH_TILE_DEFAULT);
 void ntt_batch_enqueue(NttBatch& batch, cudaStream_t stream);
 // Selects the kernel's register round (radix_log 1, 2 or 3: radix 2, 4 or
 // 8 butterflies per round) and sizes the persistent grid from that
