@@ -528,10 +528,11 @@ int dvgpu_bn254_ntt_batch_device(void* backend, const uint8_t* d_values, const u
  * the MSMs are grouped into size classes; the autotuner times candidate
  * window widths per class on random scalars, keeps a table of precomputed
  * window multiples for the best one and writes its log (JSON) to log_json.
- * It also times the persistent NTT launch with radix 2, 4 and 8 register
- * rounds on the plan's own transforms, requires every candidate's output to
- * equal the first's (a mismatch fails the call) and keeps the fastest (log
- * keys ntt.candidates, ntt.best_radix).  Each class is one launch sequence
+ * It also times the persistent NTT launch for every pair of tile (2^10,
+ * 2^11, 2^12 elements) and register round (radix 2, 4, 8) on the plan's
+ * own transforms, requires every candidate's output to equal the first's
+ * (a mismatch fails the call) and keeps the fastest (log keys
+ * ntt.candidates, ntt.best_tile, ntt.best_radix).  Each class is one launch sequence
  * over all its MSMs; the NTTs are one persistent launch on a parallel
  * branch of the graph.
  *
