@@ -1299,7 +1299,8 @@ class BatchOp:
         self.config = {"msms": len(self.sizes), "msm_points_total": self.total,
                        "msm_sizes": [min(self.sizes), max(self.sizes)], "ntts": len(self.logs),
                        "ntt_elements_total": self.ntt_elems, "ntt_logs": [min(self.logs), max(self.logs)],
-                       "msm_classes": [{"sets": c["sets"], "c": c["best_c"]} for c in self.tune_log["classes"]],
+                       "msm_classes": [{"sets": c["sets"], "c": c["best_c"], "seg": c.get("best_seg")}
+                                       for c in self.tune_log["classes"]],
                        "ntt_radix": self.tune_log["ntt"].get("best_radix"),
                        "ntt_tile": self.tune_log["ntt"].get("best_tile"),
                        "graph_nodes": self.buf.graph_nodes, "graph_kernels": self.buf.graph_kernels}

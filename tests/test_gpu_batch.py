@@ -122,6 +122,8 @@ def test_batch_plan_matches_oracle_and_replays(backend, oracle, dv):
         assert sum(c["sets"] for c in log["classes"]) == len(sizes)
         for c in log["classes"]:
             assert c["best_c"] in [x["c"] for x in c["candidates"]]
+            # bucket partition: the reduction's segment length, tried around the rule's
+            assert c["best_seg"] in [x["seg"] for x in c["seg_candidates"]]
         # the NTT's tile (2^10..2^12 elements) and register round (radix 2,
         # 4, 8) are picked from every pair, each checked against the first
         # on the device while the plan is built

@@ -311,10 +311,28 @@ std::unique_ptr<BatchPlan> batch_plan_create(const Affine<Fq>* points, uint64_t 
         if (!best_c) throw InvalidArgument("batch MSM class too large for one launch sequence");
         spare.release();
         k->plan = pre_plan(best_c);
+        // bucket partition of the reduction: segments of 2^s buckets around
+        // the rule's choice (the class's c above was timed with the rule's)
+        const int rule = msm_seg_log((uint64_t)cnt * k->plan.buckets, k->plan.buckets, best_c, true);
+        std::string seg_cands = "{\"seg\":" + std::to_string(1 << rule) + ",\"ms\":" + std::to_string(best_ms) + "}";
+        int best_seg = 0;
+        for (int sg = std::max(1, rule - 1); sg <= std::min(best_c - 1, rule + 1); ++sg) {
+            if (sg == rule) continue;
+            k->plan.seg_force = sg;
+            const double ms = time_class(p, *k, 2);
+            seg_cands += ",{\"seg\":" + std::to_string(1 << sg) + ",\"ms\":" + std::to_string(ms) + "}";
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_seg = sg;
+            }
+        }
+        k->plan.seg_force = best_seg;  // 0: the rule's
         log += std::string(first_class ? "" : ",") + "{\"sets\":" + std::to_string(cnt) +
                ",\"max_points\":" + std::to_string(k->max_n) + ",\"points\":" + std::to_string(k->total_n) +
                ",\"model_c\":" + std::to_string(model) + ",\"candidates\":[" + cands +
-               "],\"best_c\":" + std::to_string(best_c) + ",\"best_ms\":" + std::to_string(best_ms) +
+               "],\"best_c\":" + std::to_string(best_c) + ",\"seg_candidates\":[" + seg_cands +
+               "],\"best_seg\":" + std::to_string(1 << (best_seg ? best_seg : rule)) +
+               ",\"best_ms\":" + std::to_string(best_ms) +
                ",\"table_bytes\":" + std::to_string((uint64_t)k->max_n * k->plan.windows * sizeof(G1A)) + "}";
         first_class = false;
         p.classes.push_back(std::move(k));

@@ -589,6 +589,29 @@ static int measured_c(uint64_t n) {
     return 0;
 }
 
+int msm_seg_log(uint64_t all_buckets, uint32_t buckets, int c, bool g1) {
+    // Long windows (a precomputed table's single bucket set of 2^18 or more
+    // G1 buckets) take 16-bucket segments: fewer upper-level entries for a
+    // modest first level (measured 0.86 instead of 1.06 ms at 2^19 buckets);
+    // shorter windows and G2, whose additions cost three times as much,
+    // keep 8.
+    int seg_want = (g1 && buckets >= (1u << 18)) ? DV_SEG_LOG + 1 : DV_SEG_LOG;
+    // Few buckets in all (sparse updates over a precomputed table, small
+    // MSMs): the reduction is a latency chain, so keep about 2^15 first-level
+    // threads and shorten the segments (128 buckets: one bucket each).
+    int room = 0;
+    while ((all_buckets >> (room + 1)) >= (1u << 15)) ++room;
+    // Many buckets in all (a batch of sets over one table, 2^21 buckets or
+    // more): longer segments, up to 64 buckets, while at least 2^17
+    // first-level threads remain (several waves of k_segments at two blocks
+    // per SM).  Each halving of the segment count halves the first upper
+    // level, whose warp-0 phases and doublings leave most lanes idle.
+    int wide = 0;
+    while (wide < 6 && (all_buckets >> (wide + 1)) >= (1u << 17)) ++wide;
+    seg_want = std::min(std::max(seg_want, wide), room);
+    return std::min(seg_want, c - 1);
+}
+
 MsmPlan msm_plan(uint64_t n, int force_c) {
     MsmPlan p;
     int best_c = 4;
@@ -723,27 +746,8 @@ void msm_enqueue(MsmWorkspace& ws, const Affine<F>* d_points, const uint32_t* d_
     int* d_pgid = ws.pgid.as<int>(2ull * T);
     XYZZ<F>* d_ppt = ws.ppt.as<XYZZ<F>>(2ull * T);
 
-    // Long windows (a precomputed table's single bucket set of 2^18 or more
-    // G1 buckets) take 16-bucket segments: fewer upper-level entries for a
-    // modest first level (measured 0.86 instead of 1.06 ms at 2^19 buckets);
-    // shorter windows and G2, whose additions cost three times as much,
-    // keep 8.
-    int seg_want = (sizeof(F) == sizeof(Fq) && B >= (1u << 18)) ? DV_SEG_LOG + 1 : DV_SEG_LOG;
-    // Few buckets in all (sparse updates over a precomputed table, small
-    // MSMs): the reduction is a latency chain, so keep about 2^15 first-level
-    // threads and shorten the segments (128 buckets: one bucket each).
-    const uint64_t all_buckets = (uint64_t)NW * B;
-    int room = 0;
-    while ((all_buckets >> (room + 1)) >= (1u << 15)) ++room;
-    // Many buckets in all (a batch of sets over one table, 2^21 buckets or
-    // more): longer segments, up to 64 buckets, while at least 2^17
-    // first-level threads remain (several waves of k_segments at two blocks
-    // per SM).  Each halving of the segment count halves the first upper
-    // level, whose warp-0 phases and doublings leave most lanes idle.
-    int wide = 0;
-    while (wide < 6 && (all_buckets >> (wide + 1)) >= (1u << 17)) ++wide;
-    seg_want = std::min(std::max(seg_want, wide), room);
-    const int seg_log = std::min(seg_want, c - 1);
+    const int seg_log = plan.seg_force > 0 ? std::min(plan.seg_force, c - 1)
+                                           : msm_seg_log((uint64_t)NW * B, B, c, sizeof(F) == sizeof(Fq));
     const uint32_t S = B >> seg_log;
     XYZZ<F>* d_seg_u = ws.segs.as<XYZZ<F>>(4ull * NW * S);
     XYZZ<F>* d_seg_r = d_seg_u + (size_t)NW * S;

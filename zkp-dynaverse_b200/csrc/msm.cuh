@@ -37,7 +37,12 @@ struct MsmPlan {
     int windows;      // ceil(255 / c): top window never carries out
     uint32_t buckets; // 2^(c-1) signed-digit buckets per window
     int seg_log;      // bucket-reduction segment length = 2^seg_log
+    int seg_force = 0;  // > 0: this segment length (log2) instead of msm_seg_log's
 };
+
+// Bucket-reduction segment length (log2) for a launch of all_buckets
+// buckets, `buckets` per window set, window width c.
+int msm_seg_log(uint64_t all_buckets, uint32_t buckets, int c, bool g1);
 
 // Cost model: windows * (10 * n + 28 * buckets) base-field multiplications
 // (XYZZ mixed add = 10, two full adds per bucket in the reduction = 28).
