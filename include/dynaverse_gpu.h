@@ -527,7 +527,9 @@ int dvgpu_bn254_ntt_batch_device(void* backend, const uint8_t* d_values, const u
  * kinds, captured once into a CUDA graph and replayed per run.  At creation
  * the MSMs are grouped into size classes; the autotuner times candidate
  * window widths per class on random scalars, keeps a table of precomputed
- * window multiples for the best one and writes its log (JSON) to log_json.
+ * window multiples for the best one, then times the bucket partition of the
+ * reduction (segment lengths around the default rule; log keys
+ * seg_candidates, best_seg) and writes its log (JSON) to log_json.
  * It also times the persistent NTT launch for every pair of tile (2^10,
  * 2^11, 2^12 elements) and register round (radix 2, 4, 8) on the plan's
  * own transforms, requires every candidate's output to equal the first's
